@@ -1,0 +1,265 @@
+// Host-side set-up around the GPU path: analytic initial/boundary fields,
+// the modal projection of a field onto the basis (tri_hp::tobasis,
+// tri_hp/tobasis.cpp:14-116), essential boundary values
+// (hp_edge_bdry::setvalues, tri_hp/hp_boundary.cpp:549-619) and the L2/Linf
+// error against a field (tri_hp::l2error, tri_hp/l2error.cpp:13-67).
+//
+// The reference evaluates its fields through muParser expressions; the fields
+// this library's workloads need are built in as closed forms instead:
+//   HP_FIELD_KOVASZNAY  (Testing/tri_hp/ins/Spatial Accuracy/Inputs/run.inpt:21-25,
+//                        re = 1/mu, lda = re/2 - sqrt(re^2/4 + 4 pi^2))
+//   HP_FIELD_SINSIN     sin(pi x) sin(pi y)
+//   HP_FIELD_QUADX      a (x - c)^2          (Testing/tri_hp/conv-diff/Correctness: -(x0-8)^2)
+//   HP_FIELD_LID        u = 1 on y >= 1 - 1e-12, else 0; v = p = 0
+//   HP_FIELD_CONST      prm[n]
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+#include "hp_gpu.h"
+#include "hp_host.h"
+
+namespace {
+
+const int ST = HP_MXGP;
+
+double field_value(const hp_field *f, int n, double x, double y) {
+    switch (f->kind) {
+        case HP_FIELD_KOVASZNAY: {
+            const double PI = 3.14159265358979323846;
+            double re = f->prm[0];
+            double lda = .5 * re - std::sqrt(re * re / 4 + 4 * PI * PI);
+            if (n == 0) return 1.0 - std::cos(2 * PI * y) * std::exp(lda * x);
+            if (n == 1) return lda / (2 * PI) * std::sin(2 * PI * y) * std::exp(lda * x);
+            return -.5 * std::exp(2. * lda * x);
+        }
+        case HP_FIELD_SINSIN: {
+            const double PI = 3.14159265358979323846;
+            return f->prm[0] * std::sin(PI * x) * std::sin(PI * y);
+        }
+        case HP_FIELD_QUADX:
+            return f->prm[0] * (x - f->prm[1]) * (x - f->prm[1]);
+        case HP_FIELD_LID:
+            return (n == 0 && y >= 1.0 - 1e-12) ? 1.0 : 0.0;
+        case HP_FIELD_CONST:
+        default:
+            return f->prm[n < 4 ? n : 3];
+    }
+}
+
+struct Ops {
+    const hp_basis_tables &t;
+    explicit Ops(const hp_basis_tables &tt) : t(tt) {}
+    // value projection with all modes (proj.cpp:121-186) or boundary modes only (proj.cpp:283-331)
+    void proj_val(const double *lin, double *f, bool bdry_only) const {
+        double wk0[HP_MXGP][HP_MXX];
+        const int sm = t.sm, bs1 = sm + 3, bs2 = 2 * sm + 3, bm = t.bm;
+        for (int j = 0; j < t.gpn; ++j) {
+            wk0[j][0] = lin[0] * t.gn[j][0];
+            double l = lin[1] * t.gn[j][1];
+            for (int m = bs2; m < bm; ++m) l += lin[m] * t.gn[j][m];
+            wk0[j][1] = l;
+            l = lin[2] * t.gn[j][2];
+            for (int m = bs1; m < bs2; ++m) l += lin[m] * t.gn[j][m];
+            wk0[j][2] = l;
+            int ind = bm, cnt = sm - 1;
+            for (int m = 3; m < bs1; ++m) {
+                l = lin[m] * t.gn[j][m];
+                if (!bdry_only)
+                    for (int n = 0; n < cnt; ++n) l += lin[ind + n] * t.gn[j][ind + n];
+                ind += cnt--;
+                wk0[j][m] = l;
+            }
+        }
+        for (int i = 0; i < t.gpx; ++i)
+            for (int j = 0; j < t.gpn; ++j) {
+                double l = 0.0;
+                for (int n = 0; n < t.nmodx; ++n) l += wk0[j][n] * t.gx[i][n];
+                f[i * ST + j] = l;
+            }
+    }
+    void proj_lin(double u1, double u2, double u3, double *f) const {
+        for (int i = 0; i < t.gpx; ++i)
+            for (int j = 0; j < t.gpn; ++j)
+                f[i * ST + j] = u1 * t.gx[i][0] * t.gn[j][0] + u2 * t.gx[i][1] * t.gn[j][1] + u3 * t.gx[i][2] * t.gn[j][2];
+    }
+    void intgrt(double *r, const double *f) const {
+        double wk0[HP_MXX][HP_MXGP];
+        const int sm = t.sm, bs1 = sm + 3, bs2 = 2 * sm + 3, bm = t.bm;
+        for (int n = 0; n < t.nmodx; ++n)
+            for (int j = 0; j < t.gpn; ++j) {
+                double l = f[j] * t.gxwtx[n][0];
+                for (int i = 1; i < t.gpx; ++i) l += f[i * ST + j] * t.gxwtx[n][i];
+                wk0[n][j] = l;
+            }
+        auto dot = [&](int m, int col) {
+            double l = 0.0;
+            for (int j = 0; j < t.gpn; ++j) l += t.gnwtn[m][j] * wk0[col][j];
+            return l;
+        };
+        for (int m = 0; m < bs1; ++m) r[m] = dot(m, m);
+        for (int m = bs1; m < bs2; ++m) r[m] = dot(m, 2);
+        for (int m = bs2; m < bm; ++m) r[m] = dot(m, 1);
+        int indx = bm;
+        for (int m = 3; m < sm + 2; ++m)
+            for (int n = 0; n < sm + 2 - m; ++n, ++indx) r[indx] = dot(indx, m);
+    }
+    void proj1d_lin(double u1, double u2, double *f) const {
+        for (int i = 0; i < t.gpx; ++i) f[i] = u1 * t.gx[i][1] + u2 * t.gx[i][2];
+    }
+    void intgrt1d(double *r, const double *f) const {
+        double l = 0.0;
+        for (int i = 0; i < t.gpx; ++i) l += t.gxwtx[1][i] * f[i];
+        r[0] = l;
+        l = 0.0;
+        for (int i = 0; i < t.gpx; ++i) l += t.gxwtx[2][i] * f[i];
+        r[1] = l;
+        for (int n = 3; n < t.nmodx; ++n) {
+            l = 0.0;
+            for (int i = 0; i < t.gpx; ++i) l += t.gxwtx[n][i] * f[i];
+            r[n - 1] = l;
+        }
+    }
+    // LAPACK-style dpbtrs on the reference's band layout [col][kd+1]
+    static void band_solve(int n, int kd, const double *ab, double *x) {
+        const int ld = kd + 1;
+        for (int i = 0; i < n; ++i) {
+            for (int k = std::max(0, i - kd); k < i; ++k) x[i] -= ab[i * ld + kd + k - i] * x[k];
+            x[i] /= ab[i * ld + kd];
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            for (int k = i + 1; k <= std::min(n - 1, i + kd); ++k) x[i] -= ab[k * ld + kd + i - k] * x[k];
+            x[i] /= ab[i * ld + kd];
+        }
+    }
+};
+
+// 1D L2 projection of a field minus the linear vertex interpolant onto the side modes
+// (tobasis.cpp:23-70 / hp_boundary.cpp:567-616).
+void side_modes(const Ops &op, const hp_mesh_desc *m, int NV, const hp_field *fld, const double *ugv, int sind,
+                const int *only_mask, double *ugs) {
+    const hp_basis_tables &t = op.t;
+    int v0 = m->seg_pnt[2 * sind], v1 = m->seg_pnt[2 * sind + 1];
+    double crd[2][HP_MXGP], res[HP_MXGP], lf[HP_MXX];
+    for (int n = 0; n < 2; ++n) op.proj1d_lin(m->pnts[2 * v0 + n], m->pnts[2 * v1 + n], crd[n]);
+    for (int n = 0; n < NV; ++n) {
+        if (only_mask && !(*only_mask & (1 << n))) continue;
+        op.proj1d_lin(ugv[v0 * NV + n], ugv[v1 * NV + n], res);
+        for (int i = 0; i < t.gpx; ++i) res[i] -= field_value(fld, n, crd[0][i], crd[1][i]);
+        op.intgrt1d(lf, res);
+        Ops::band_solve(t.sm, t.sbwth, &t.sdiag1d[0][0], &lf[2]);
+        for (int k = 0; k < t.sm; ++k) ugs[((size_t)sind * t.sm + k) * NV + n] = -lf[2 + k];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int hp_field_eval(const hp_field *f, int n, double x, double y, double *out) {
+    if (!f || !out) return HP_EINVAL;
+    *out = field_value(f, n, x, y);
+    return HP_OK;
+}
+
+int hp_tobasis(const hp_basis_tables *t, const hp_mesh_desc *m, int NV, const hp_field *fld, double *ugv,
+               double *ugs, double *ugi) {
+    if (!t || !m || !fld || !ugv || NV < 1 || NV > 3) return HP_EINVAL;
+    Ops op(*t);
+    for (int i = 0; i < m->npnt; ++i)
+        for (int n = 0; n < NV; ++n) ugv[i * NV + n] = field_value(fld, n, m->pnts[2 * i], m->pnts[2 * i + 1]);
+    if (t->sm == 0) return HP_OK;
+    for (int s = 0; s < m->nseg; ++s) side_modes(op, m, NV, fld, ugv, s, nullptr, ugs);
+    if (t->im == 0) return HP_OK;
+    std::vector<double> uht(HP_MXTM);
+    double u[HP_MXGP * HP_MXGP], crd[2][HP_MXGP * HP_MXGP], lf[HP_MXTM];
+    for (int e = 0; e < m->ntri; ++e) {
+        const int *tp = &m->tri_pnt[3 * e], *ts = &m->tri_seg[3 * e], *tg = &m->tri_sgn[3 * e];
+        for (int n = 0; n < 2; ++n)
+            op.proj_lin(m->pnts[2 * tp[0] + n], m->pnts[2 * tp[1] + n], m->pnts[2 * tp[2] + n], crd[n]);
+        for (int n = 0; n < NV; ++n) {
+            for (int i = 0; i < 3; ++i) uht[i] = ugv[tp[i] * NV + n];
+            int cnt = 3;
+            for (int i = 0; i < 3; ++i) {
+                int msgn = 1;
+                for (int k = 0; k < t->sm; ++k) {
+                    uht[cnt++] = msgn * ugs[((size_t)ts[i] * t->sm + k) * NV + n];
+                    msgn *= tg[i];
+                }
+            }
+            op.proj_val(uht.data(), u, true);
+            for (int i = 0; i < t->gpx; ++i)
+                for (int j = 0; j < t->gpn; ++j)
+                    u[i * ST + j] -= field_value(fld, n, crd[0][i * ST + j], crd[1][i * ST + j]);
+            op.intgrt(lf, u);
+            Ops::band_solve(t->im, t->ibwth, &t->idiag[0][0], &lf[t->bm]);
+            for (int k = 0; k < t->im; ++k) ugi[((size_t)e * t->im + k) * NV + n] = -lf[t->bm + k];
+        }
+    }
+    return HP_OK;
+}
+
+int hp_setvalues(const hp_basis_tables *t, const hp_mesh_desc *m, int NV, const hp_field *fld, double *ugv,
+                 double *ugs) {
+    if (!t || !m || !fld || !ugv) return HP_EINVAL;
+    Ops op(*t);
+    for (int e = 0; e < m->nbseg; ++e) {
+        int mask = m->bseg_kind[e] & 0xFF;
+        if (!mask) continue;
+        int s = m->bseg[e];
+        for (int k = 0; k < 2; ++k) {
+            int v = m->seg_pnt[2 * s + k];
+            for (int n = 0; n < NV; ++n)
+                if (mask & (1 << n)) ugv[v * NV + n] = field_value(fld, n, m->pnts[2 * v], m->pnts[2 * v + 1]);
+        }
+    }
+    if (t->sm == 0) return HP_OK;
+    for (int e = 0; e < m->nbseg; ++e) {
+        int mask = m->bseg_kind[e] & 0xFF;
+        if (mask) side_modes(op, m, NV, fld, ugv, m->bseg[e], &mask, ugs);
+    }
+    return HP_OK;
+}
+
+int hp_l2error(const hp_basis_tables *t, const hp_mesh_desc *m, int NV, const hp_field *fld, const double *ugv,
+               const double *ugs, const double *ugi, double *l2, double *linf) {
+    if (!t || !m || !fld || !ugv || !l2 || !linf) return HP_EINVAL;
+    Ops op(*t);
+    std::vector<double> uht(HP_MXTM);
+    double u[HP_MXGP * HP_MXGP], crd[2][HP_MXGP * HP_MXGP];
+    for (int n = 0; n < NV; ++n) { l2[n] = 0.0; linf[n] = 0.0; }
+    for (int e = 0; e < m->ntri; ++e) {
+        const int *tp = &m->tri_pnt[3 * e], *ts = &m->tri_seg[3 * e], *tg = &m->tri_sgn[3 * e];
+        for (int n = 0; n < 2; ++n)
+            op.proj_lin(m->pnts[2 * tp[0] + n], m->pnts[2 * tp[1] + n], m->pnts[2 * tp[2] + n], crd[n]);
+        double dc00 = 0.5 * (m->pnts[2 * tp[2]] - m->pnts[2 * tp[1]]);
+        double dc01 = 0.5 * (m->pnts[2 * tp[0]] - m->pnts[2 * tp[1]]);
+        double dc10 = 0.5 * (m->pnts[2 * tp[2] + 1] - m->pnts[2 * tp[1] + 1]);
+        double dc11 = 0.5 * (m->pnts[2 * tp[0] + 1] - m->pnts[2 * tp[1] + 1]);
+        double cjcb = dc00 * dc11 - dc10 * dc01;
+        for (int n = 0; n < NV; ++n) {
+            for (int i = 0; i < 3; ++i) uht[i] = ugv[tp[i] * NV + n];
+            int cnt = 3;
+            for (int i = 0; i < 3; ++i) {
+                int msgn = 1;
+                for (int k = 0; k < t->sm; ++k) {
+                    uht[cnt++] = msgn * ugs[((size_t)ts[i] * t->sm + k) * NV + n];
+                    msgn *= tg[i];
+                }
+            }
+            for (int k = 0; k < t->im; ++k) uht[cnt++] = ugi[((size_t)e * t->im + k) * NV + n];
+            op.proj_val(uht.data(), u, false);
+            for (int i = 0; i < t->gpx; ++i)
+                for (int j = 0; j < t->gpn; ++j) {
+                    double err = std::fabs(u[i * ST + j] - field_value(fld, n, crd[0][i * ST + j], crd[1][i * ST + j]));
+                    if (err >= linf[n]) linf[n] = err;
+                    l2[n] += err * err * t->wtx[i] * t->wtn[j] * cjcb;
+                }
+        }
+    }
+    for (int n = 0; n < NV; ++n) l2[n] = std::sqrt(l2[n]);
+    return HP_OK;
+}
+
+}  // extern "C"

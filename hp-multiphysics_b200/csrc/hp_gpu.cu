@@ -1,0 +1,647 @@
+// C-ABI of the B200 library: context set-up, per-(p, physics) dispatch,
+// stream-ordered launches of the element-residual / minvrt / update kernels, and
+// CUDA-graph capture of one multistage update.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <cstdarg>
+#include <vector>
+#include <string>
+#include <algorithm>
+
+#include "hp_gpu.h"
+#include "hp_kernels.cuh"
+
+using namespace hpb;
+
+static thread_local std::string g_err;
+static void set_err(const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+#define CK(call)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return HP_ECUDA;                                                            \
+        }                                                                               \
+    } while (0)
+
+namespace {
+
+template <typename R, int P>
+void fill_tables(const hp_basis_tables &b, DevTables<R, P> &t) {
+    constexpr int G = P + 1, X = P + 2, T = (P + 1) * (P + 2) / 2, SM = P - 1, BM = 3 * P;
+    std::memset(&t, 0, sizeof(t));
+    for (int i = 0; i < G; ++i) {
+        for (int n = 0; n < X; ++n) { t.gx[i][n] = (R)b.gx[i][n]; t.dgx[i][n] = (R)b.dgx[i][n]; }
+        for (int m = 0; m < T; ++m) { t.gn[i][m] = (R)b.gn[i][m]; t.dgn[i][m] = (R)b.dgn[i][m]; }
+        t.x0[i] = (R)b.x0[i]; t.n0[i] = (R)b.n0[i]; t.wtx[i] = (R)b.wtx[i];
+        t.dltx[i] = (R)b.dltx[i]; t.dltn[i] = (R)b.dltn[i];
+        for (int q = 0; q < G; ++q) {
+            t.dltx1[i][q] = (R)b.dltx1[i][q];
+            t.dltn1[i][q] = (R)b.dltn1[i][q];
+            t.dltn2[i][q] = (R)b.dltn2[i][q];
+        }
+    }
+    for (int n = 0; n < X; ++n)
+        for (int i = 0; i < G; ++i) { t.gxwtx[n][i] = (R)b.gxwtx[n][i]; t.dgxwtx[n][i] = (R)b.dgxwtx[n][i]; }
+    for (int m = 0; m < T; ++m)
+        for (int j = 0; j < G; ++j) {
+            t.gnwtn[m][j] = (R)b.gnwtn[m][j];
+            t.gnwtnn0[m][j] = (R)b.gnwtnn0[m][j];
+            t.dgnwtn[m][j] = (R)b.dgnwtn[m][j];
+        }
+    // column structure of the sum factorisation (proj.cpp:46-95, intgrt.cpp:44-76)
+    const int bs1 = SM + 3, bs2 = 2 * SM + 3;
+    std::vector<std::vector<int>> cols(X);
+    cols[0].push_back(0);
+    cols[1].push_back(1);
+    for (int m = bs2; m < BM; ++m) cols[1].push_back(m);
+    if (X > 2) {
+        cols[2].push_back(2);
+        for (int m = bs1; m < bs2; ++m) cols[2].push_back(m);
+    }
+    int ind = BM, cnt = SM - 1;
+    for (int m = 3; m < bs1; ++m) {
+        cols[m].push_back(m);
+        for (int n = 0; n < cnt; ++n) cols[m].push_back(ind + n);
+        ind += cnt--;
+    }
+    int c = 0;
+    for (int n = 0; n < X; ++n) {
+        t.colstart[n] = c;
+        for (int m : cols[n]) { t.colmodes[c++] = m; t.colof[m] = n; }
+    }
+    t.colstart[X] = c;
+}
+
+template <typename R>
+void fill_minv(const hp_basis_tables &b, DevMinv<R> &m) {
+    std::memset(&m, 0, sizeof(m));
+    for (int i = 0; i < 2; ++i)
+        for (int k = 0; k < b.sm; ++k) m.sfmv[i][k] = (R)b.sfmv[i][k];
+    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k < b.sm; ++k) m.vfms[i][k] = (R)b.vfms[i][k];
+    for (int k = 0; k < b.sm; ++k) m.sdiag[k] = (R)b.sdiag[k];
+    for (int a = 0; a < b.sm; ++a)
+        for (int c = 0; c < b.sm; ++c)
+            for (int s = 0; s < 3; ++s) m.sfms[a][c][s] = (R)b.sfms[a][c][s];
+    for (int i = 0; i < b.bm; ++i)
+        for (int k = 0; k < b.im; ++k) { m.ifmb[i][k] = (R)b.ifmb[i][k]; m.bfmi[i][k] = (R)b.bfmi[i][k]; }
+    for (int k = 0; k < b.im; ++k) { m.idiag[k][0] = (R)b.idiag[k][0]; m.idiag[k][1] = (R)b.idiag[k][1]; }
+    m.vdiag = (R)b.vdiag;
+}
+
+inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+// Per-(p, physics) launchers.
+struct Launchers {
+    size_t tab_bytes;
+    void (*fill)(const hp_basis_tables &, void *);
+    void (*elem)(const void *tab, const Mesh &, const State<double> &, const Phys &, int stage, int zero_rr,
+                 int nsm, cudaStream_t);
+    void (*bflux)(const void *tab, const Mesh &, const State<double> &, const Phys &, cudaStream_t);
+    void (*prcn)(const void *tab, const Mesh &, const State<double> &, const Phys &, int *err, cudaStream_t);
+    void (*side)(const Mesh &, const State<double> &, const DevMinv<double> *, int im, int mode, double cfla,
+                 int upd, int fold, cudaStream_t);
+    void (*intr)(const Mesh &, const State<double> &, const DevMinv<double> *, double cfla, int upd, cudaStream_t);
+    void (*vert)(const Mesh &, const State<double> &, const DevMinv<double> *, int sm, int im, double cfla, int upd,
+                 int fold, unsigned long long *slot, cudaStream_t);
+    int elem_smem;
+};
+
+template <int P, int PHYS>
+struct LaunchImpl {
+    using R = double;
+    using C = ElemCfg<R, P, PHYS>;
+    static constexpr int NV = C::NV, SM = P - 1, IM = (P - 1) * (P - 2) / 2;
+    static int smem() {
+        return (int)(((sizeof(DevTables<R, P>) + 15) / 16) * 16 + (size_t)C::WPC * C::S_WARP * sizeof(R));
+    }
+    static void fill(const hp_basis_tables &b, void *out) { fill_tables<R, P>(b, *reinterpret_cast<DevTables<R, P> *>(out)); }
+    static void elem(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int stage, int zero_rr, int nsm,
+                     cudaStream_t st) {
+        int blocks = nblk(m.ntri, C::WPC);
+        const int cap = nsm * 16;
+        if (blocks > cap) blocks = cap;
+        k_rsdl_elem<R, P, PHYS><<<blocks, C::WPC * 32, smem(), st>>>(
+            reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, stage, zero_rr);
+    }
+    static void bflux(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, cudaStream_t st) {
+        if (PHYS == 1 && m.nbseg > 0)
+            k_bdry_flux_ins<R, P><<<nblk(m.nbseg, 128), 128, 0, st>>>(reinterpret_cast<const DevTables<R, P> *>(tab), m,
+                                                                       s, ph);
+    }
+    static void prcn(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int *err, cudaStream_t st) {
+        k_prcn_elem<R, P, PHYS><<<nblk(m.ntri, 128), 128, 0, st>>>(reinterpret_cast<const DevTables<R, P> *>(tab), m, s,
+                                                                   ph, err);
+    }
+    static void side(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, int im, int mode, double cfla, int upd,
+                     int fold, cudaStream_t st) {
+        if constexpr (SM > 0)
+            k_minv_side<R, NV, SM><<<nblk(m.nseg, 128), 128, 0, st>>>(m, s, mt, im, mode, (R)cfla, upd, fold);
+    }
+    static void intr(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, double cfla, int upd, cudaStream_t st) {
+        if constexpr (IM > 0) k_minv_int<R, NV, SM, IM><<<nblk(m.ntri, 128), 128, 0, st>>>(m, s, mt, (R)cfla, upd);
+    }
+    static void vert(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, int sm, int im, double cfla, int upd,
+                     int fold, unsigned long long *slot, cudaStream_t st) {
+        k_minv_vert<R, NV><<<nblk(m.npnt, 128), 128, 0, st>>>(m, s, mt, sm, im, (R)cfla, upd, fold, slot);
+    }
+    static Launchers get() {
+        Launchers L;
+        L.tab_bytes = sizeof(DevTables<R, P>);
+        L.fill = &fill;
+        L.elem = &elem;
+        L.bflux = &bflux;
+        L.prcn = &prcn;
+        L.side = &side;
+        L.intr = &intr;
+        L.vert = &vert;
+        L.elem_smem = smem();
+        return L;
+    }
+};
+
+template <int PHYS>
+static bool get_launchers_phys(int p, Launchers &L) {
+    switch (p) {
+        case 1: L = LaunchImpl<1, PHYS>::get(); return true;
+        case 2: L = LaunchImpl<2, PHYS>::get(); return true;
+        case 3: L = LaunchImpl<3, PHYS>::get(); return true;
+        case 4: L = LaunchImpl<4, PHYS>::get(); return true;
+        case 5: L = LaunchImpl<5, PHYS>::get(); return true;
+        case 6: L = LaunchImpl<6, PHYS>::get(); return true;
+        case 7: L = LaunchImpl<7, PHYS>::get(); return true;
+        case 8: L = LaunchImpl<8, PHYS>::get(); return true;
+    }
+    return false;
+}
+
+template <int P, int PHYS>
+static cudaError_t set_smem_attr() {
+    return cudaFuncSetAttribute(k_rsdl_elem<double, P, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                LaunchImpl<P, PHYS>::smem());
+}
+static cudaError_t set_smem(int p, int phys) {
+#define SM_CASE(PP)                                                            \
+    case PP:                                                                   \
+        return phys ? set_smem_attr<PP, 1>() : set_smem_attr<PP, 0>();
+    switch (p) {
+        SM_CASE(1) SM_CASE(2) SM_CASE(3) SM_CASE(4) SM_CASE(5) SM_CASE(6) SM_CASE(7) SM_CASE(8)
+    }
+#undef SM_CASE
+    return cudaErrorInvalidValue;
+}
+
+struct hp_gpu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int p = 0, NV = 0, npnt = 0, nseg = 0, ntri = 0, nbseg = 0, sm = 0, im = 0, nsm = 148;
+    Phys ph{};
+    Launchers L{};
+    Mesh mesh{};
+    State<double> st{};
+    void *d_tab = nullptr;
+    DevMinv<double> *d_minv = nullptr;
+    double vdiag = 0.0;
+    unsigned long long *d_slot = nullptr;
+    double *d_hist = nullptr;
+    int hist_cap = 0;
+    int *d_iter = nullptr;
+    int *d_err = nullptr;
+    double *d_part = nullptr;
+    int npart = 0;
+    std::vector<void *> allocs;
+    cudaGraphExec_t g_update = nullptr;  // one update() incl. maxres -> hist slot advance
+    bool prcn_ready = false;
+    size_t lv = 0, ls = 0, li = 0;  // element counts of v/s/i arrays
+};
+
+static int dalloc(hp_gpu_ctx *c, void **p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        set_err("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return HP_ENOMEM;
+    }
+    c->allocs.push_back(*p);
+    return HP_OK;
+}
+
+template <typename T>
+static int upload(hp_gpu_ctx *c, T **d, const T *h, size_t n) {
+    int r = dalloc(c, (void **)d, n * sizeof(T));
+    if (r) return r;
+    if (n && h) CK(cudaMemcpyAsync(*d, h, n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    return HP_OK;
+}
+
+extern "C" const char *hp_gpu_last_error(void) { return g_err.c_str(); }
+
+extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, const hp_phys_params *ph, int device,
+                             void *stream, hp_gpu_ctx **out) {
+    g_err.clear();
+    if (!m || !b || !ph || !out) { set_err("null argument"); return HP_EINVAL; }
+    if (b->p < 1 || b->p > HP_MAXP) { set_err("p=%d outside [1,%d]", b->p, HP_MAXP); return HP_EINVAL; }
+    if (ph->physics != HP_PHYS_CD && ph->physics != HP_PHYS_INS) { set_err("unknown physics"); return HP_EINVAL; }
+    if (ph->nstage < 1 || ph->nstage > 7) { set_err("nstage=%d outside [1,7]", ph->nstage); return HP_EINVAL; }
+    if (ph->bd0 != 0.0) { set_err("only steady problems (bd0 = 0) are supported"); return HP_ENOTSUP; }
+    if (m->npnt <= 0 || m->nseg <= 0 || m->ntri <= 0) { set_err("empty mesh"); return HP_EINVAL; }
+    if (ph->physics == HP_PHYS_INS && m->nbseg > 0 && !m->bseg_pibc) {
+        for (int e = 0; e < m->nbseg; ++e)
+            if ((m->bseg_kind[e] & HP_BC_FLUX_MASK) == HP_BC_FLUX_INS_GENERIC) {
+                set_err("ins generic boundary flux needs bseg_pibc");
+                return HP_EINVAL;
+            }
+    }
+    hp_gpu_ctx *c = new hp_gpu_ctx();
+    auto fail = [&](int code) {
+        hp_gpu_destroy(c);
+        return code;
+    };
+    if (device >= 0) {
+        if (cudaSetDevice(device) != cudaSuccess) { set_err("cudaSetDevice(%d) failed", device); delete c; return HP_ECUDA; }
+        c->device = device;
+    } else {
+        cudaGetDevice(&c->device);
+    }
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+    c->nsm = nsm > 0 ? nsm : 148;
+    if (stream) c->stream = (cudaStream_t)stream;
+    else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            set_err("cudaStreamCreate failed");
+            delete c;
+            return HP_ECUDA;
+        }
+        c->own_stream = true;
+    }
+    const int physics = ph->physics;
+    c->p = b->p; c->sm = b->sm; c->im = b->im;
+    c->NV = physics == HP_PHYS_INS ? 3 : 1;
+    c->npnt = m->npnt; c->nseg = m->nseg; c->ntri = m->ntri; c->nbseg = m->nbseg;
+    bool ok = physics ? get_launchers_phys<1>(c->p, c->L) : get_launchers_phys<0>(c->p, c->L);
+    if (!ok) { set_err("p=%d not built", c->p); return fail(HP_ENOTSUP); }
+    if (set_smem(c->p, physics) != cudaSuccess) { set_err("smem attribute (%d bytes) rejected", c->L.elem_smem); return fail(HP_ECUDA); }
+    Phys &P = c->ph;
+    P.physics = physics; P.NV = c->NV; P.nstage = ph->nstage;
+    for (int k = 0; k < 8; ++k) { P.alpha[k] = ph->alpha[k]; P.beta[k] = ph->beta[k]; }
+    P.alpha[ph->nstage] = 1.0; P.beta[ph->nstage] = 1.0;
+    P.cfl = ph->cfl; P.bd0 = ph->bd0; P.adis = ph->adis; P.rho = ph->rho; P.mu = ph->mu;
+    P.rhocv = ph->rhocv; P.kcond = ph->kcond; P.ax = ph->ax; P.ay = ph->ay; P.src = ph->src;
+
+    // host-side mesh preprocessing: seg_loc and vertex incidence
+    const int np = m->npnt, ns = m->nseg, nt = m->ntri;
+    std::vector<int> seg_loc(2 * ns, -1);
+    for (int s = 0; s < ns; ++s)
+        for (int k = 0; k < 2; ++k) {
+            int t = m->seg_tri[2 * s + k];
+            if (t < 0) continue;
+            if (t >= nt) { set_err("seg_tri out of range"); return fail(HP_EINVAL); }
+            for (int i = 0; i < 3; ++i)
+                if (m->tri_seg[3 * t + i] == s) seg_loc[2 * s + k] = i;
+            if (seg_loc[2 * s + k] < 0) { set_err("seg %d not a side of tri %d", s, t); return fail(HP_EINVAL); }
+        }
+    std::vector<int> vs_ptr(np + 1, 0), vt_ptr(np + 1, 0);
+    for (int s = 0; s < ns; ++s)
+        for (int k = 0; k < 2; ++k) {
+            int v = m->seg_pnt[2 * s + k];
+            if (v < 0 || v >= np) { set_err("seg_pnt out of range"); return fail(HP_EINVAL); }
+            vs_ptr[v + 1]++;
+        }
+    for (int t = 0; t < nt; ++t)
+        for (int i = 0; i < 3; ++i) {
+            int v = m->tri_pnt[3 * t + i];
+            if (v < 0 || v >= np) { set_err("tri_pnt out of range"); return fail(HP_EINVAL); }
+            int s = m->tri_seg[3 * t + i];
+            if (s < 0 || s >= ns) { set_err("tri_seg out of range"); return fail(HP_EINVAL); }
+            vt_ptr[v + 1]++;
+        }
+    for (int v = 0; v < np; ++v) { vs_ptr[v + 1] += vs_ptr[v]; vt_ptr[v + 1] += vt_ptr[v]; }
+    std::vector<int> vs_idx(vs_ptr[np]), vt_idx(vt_ptr[np]);
+    {
+        std::vector<int> a(vs_ptr.begin(), vs_ptr.end() - 1), bb(vt_ptr.begin(), vt_ptr.end() - 1);
+        for (int s = 0; s < ns; ++s)
+            for (int k = 0; k < 2; ++k) vs_idx[a[m->seg_pnt[2 * s + k]]++] = 2 * s + k;
+        for (int t = 0; t < nt; ++t)
+            for (int i = 0; i < 3; ++i) vt_idx[bb[m->tri_pnt[3 * t + i]]++] = 4 * t + i;
+    }
+    std::vector<int> vess(np, 0), sess(ns, 0);
+    for (int e = 0; e < m->nbseg; ++e) {
+        int s = m->bseg[e];
+        if (s < 0 || s >= ns) { set_err("bseg out of range"); return fail(HP_EINVAL); }
+        int mask = m->bseg_kind[e] & 0xFF;
+        sess[s] |= mask;
+        vess[m->seg_pnt[2 * s]] |= mask;
+        vess[m->seg_pnt[2 * s + 1]] |= mask;
+    }
+    int r = 0;
+    double *d_pnts;
+    int *d_tp, *d_ts, *d_tg, *d_sp, *d_st, *d_sl, *d_vsp, *d_vsi, *d_vtp, *d_vti, *d_vess, *d_sess, *d_bseg, *d_bkind;
+    double *d_bpibc;
+    if ((r = upload(c, &d_pnts, m->pnts, 2 * (size_t)np))) return fail(r);
+    if ((r = upload(c, &d_tp, m->tri_pnt, 3 * (size_t)nt))) return fail(r);
+    if ((r = upload(c, &d_ts, m->tri_seg, 3 * (size_t)nt))) return fail(r);
+    if ((r = upload(c, &d_tg, m->tri_sgn, 3 * (size_t)nt))) return fail(r);
+    if ((r = upload(c, &d_sp, m->seg_pnt, 2 * (size_t)ns))) return fail(r);
+    if ((r = upload(c, &d_st, m->seg_tri, 2 * (size_t)ns))) return fail(r);
+    if ((r = upload(c, &d_sl, seg_loc.data(), seg_loc.size()))) return fail(r);
+    if ((r = upload(c, &d_vsp, vs_ptr.data(), vs_ptr.size()))) return fail(r);
+    if ((r = upload(c, &d_vsi, vs_idx.data(), vs_idx.size()))) return fail(r);
+    if ((r = upload(c, &d_vtp, vt_ptr.data(), vt_ptr.size()))) return fail(r);
+    if ((r = upload(c, &d_vti, vt_idx.data(), vt_idx.size()))) return fail(r);
+    if ((r = upload(c, &d_vess, vess.data(), vess.size()))) return fail(r);
+    if ((r = upload(c, &d_sess, sess.data(), sess.size()))) return fail(r);
+    if ((r = upload(c, &d_bseg, m->bseg, (size_t)m->nbseg))) return fail(r);
+    if ((r = upload(c, &d_bkind, m->bseg_kind, (size_t)m->nbseg))) return fail(r);
+    std::vector<double> pibc((size_t)std::max(1, m->nbseg) * b->gpx, 0.0);
+    if (m->bseg_pibc) std::copy(m->bseg_pibc, m->bseg_pibc + (size_t)m->nbseg * b->gpx, pibc.begin());
+    if ((r = upload(c, &d_bpibc, pibc.data(), pibc.size()))) return fail(r);
+    Mesh &M = c->mesh;
+    M.npnt = np; M.nseg = ns; M.ntri = nt; M.nbseg = m->nbseg;
+    M.pnts = d_pnts; M.tri_pnt = d_tp; M.tri_seg = d_ts; M.tri_sgn = d_tg;
+    M.seg_pnt = d_sp; M.seg_tri = d_st; M.seg_loc = d_sl;
+    M.vs_ptr = d_vsp; M.vs_idx = d_vsi; M.vt_ptr = d_vtp; M.vt_idx = d_vti;
+    M.vess = d_vess; M.sess = d_sess; M.bseg = d_bseg; M.bkind = d_bkind; M.bpibc = d_bpibc;
+
+    // tables
+    std::vector<unsigned char> htab(c->L.tab_bytes);
+    c->L.fill(*b, htab.data());
+    if ((r = upload(c, (unsigned char **)&c->d_tab, htab.data(), htab.size()))) return fail(r);
+    DevMinv<double> hm;
+    fill_minv<double>(*b, hm);
+    c->vdiag = b->vdiag;
+    if ((r = upload(c, &c->d_minv, &hm, 1))) return fail(r);
+
+    // state
+    const int NV = c->NV;
+    c->lv = (size_t)np * NV; c->ls = (size_t)ns * c->sm * NV; c->li = (size_t)nt * c->im * NV;
+    double **vptrs[] = {&c->st.ugv, &c->st.u0v, &c->st.resv, &c->st.rrv};
+    double **sptrs[] = {&c->st.ugs, &c->st.u0s, &c->st.ress, &c->st.rrs};
+    double **iptrs[] = {&c->st.ugi, &c->st.u0i, &c->st.resi, &c->st.rri};
+    for (auto pp : vptrs) { if ((r = dalloc(c, (void **)pp, c->lv * 8))) return fail(r); CK(cudaMemsetAsync(*pp, 0, c->lv * 8, c->stream)); }
+    for (auto pp : sptrs) { if ((r = dalloc(c, (void **)pp, c->ls * 8))) return fail(r); CK(cudaMemsetAsync(*pp, 0, std::max<size_t>(c->ls, 2) * 8, c->stream)); }
+    for (auto pp : iptrs) { if ((r = dalloc(c, (void **)pp, c->li * 8))) return fail(r); CK(cudaMemsetAsync(*pp, 0, std::max<size_t>(c->li, 2) * 8, c->stream)); }
+    if ((r = dalloc(c, (void **)&c->st.vprcn, (size_t)np * NV * 8))) return fail(r);
+    if ((r = dalloc(c, (void **)&c->st.sprcn, (size_t)ns * NV * 8))) return fail(r);
+    if ((r = dalloc(c, (void **)&c->st.tprcn, (size_t)nt * NV * 8))) return fail(r);
+    if ((r = dalloc(c, (void **)&c->st.tau, (size_t)nt * NV * 8))) return fail(r);
+    if ((r = dalloc(c, (void **)&c->d_slot, 4 * 8))) return fail(r);
+    CK(cudaMemsetAsync(c->d_slot, 0, 32, c->stream));
+    c->hist_cap = 1 << 16;
+    if ((r = dalloc(c, (void **)&c->d_hist, (size_t)c->hist_cap * 8))) return fail(r);
+    if ((r = dalloc(c, (void **)&c->d_iter, 16))) return fail(r);
+    CK(cudaMemsetAsync(c->d_iter, 0, 16, c->stream));
+    if ((r = dalloc(c, (void **)&c->d_err, 16))) return fail(r);
+    c->npart = 4 * c->nsm;
+    if ((r = dalloc(c, (void **)&c->d_part, (size_t)c->npart * 2 * 8))) return fail(r);
+    CK(cudaStreamSynchronize(c->stream));
+    *out = c;
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_destroy(hp_gpu_ctx *c) {
+    if (!c) return HP_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->g_update) cudaGraphExecDestroy(c->g_update);
+    for (void *p : c->allocs) cudaFree(p);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_sizes(const hp_gpu_ctx *c, int *nv, int *sm, int *im) {
+    if (!c) return HP_EINVAL;
+    if (nv) *nv = c->NV;
+    if (sm) *sm = c->sm;
+    if (im) *im = c->im;
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_upload_state(hp_gpu_ctx *c, const double *v, const double *s, const double *i) {
+    if (!c || !v) return HP_EINVAL;
+    CK(cudaMemcpyAsync(c->st.ugv, v, c->lv * 8, cudaMemcpyHostToDevice, c->stream));
+    if (c->ls) { if (!s) return HP_EINVAL; CK(cudaMemcpyAsync(c->st.ugs, s, c->ls * 8, cudaMemcpyHostToDevice, c->stream)); }
+    if (c->li) { if (!i) return HP_EINVAL; CK(cudaMemcpyAsync(c->st.ugi, i, c->li * 8, cudaMemcpyHostToDevice, c->stream)); }
+    CK(cudaStreamSynchronize(c->stream));
+    return HP_OK;
+}
+
+static int download3(hp_gpu_ctx *c, const double *dv, const double *ds, const double *di, double *v, double *s,
+                     double *i) {
+    if (v) CK(cudaMemcpyAsync(v, dv, c->lv * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (s && c->ls) CK(cudaMemcpyAsync(s, ds, c->ls * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (i && c->li) CK(cudaMemcpyAsync(i, di, c->li * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_download_state(hp_gpu_ctx *c, double *v, double *s, double *i) {
+    if (!c) return HP_EINVAL;
+    return download3(c, c->st.ugv, c->st.ugs, c->st.ugi, v, s, i);
+}
+extern "C" int hp_gpu_download_residual(hp_gpu_ctx *c, double *v, double *s, double *i) {
+    if (!c) return HP_EINVAL;
+    return download3(c, c->st.resv, c->st.ress, c->st.resi, v, s, i);
+}
+extern "C" int hp_gpu_download_prcn(hp_gpu_ctx *c, double *vp, double *sp, double *tp, double *tau) {
+    if (!c) return HP_EINVAL;
+    if (vp) CK(cudaMemcpyAsync(vp, c->st.vprcn, (size_t)c->npnt * c->NV * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (sp) CK(cudaMemcpyAsync(sp, c->st.sprcn, (size_t)c->nseg * c->NV * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (tp) CK(cudaMemcpyAsync(tp, c->st.tprcn, (size_t)c->ntri * c->NV * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (tau) CK(cudaMemcpyAsync(tau, c->st.tau, (size_t)c->ntri * c->NV * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return HP_OK;
+}
+extern "C" int hp_gpu_device_ptrs(hp_gpu_ctx *c, double **ugv, double **ugs, double **ugi, double **resv,
+                                  double **ress, double **resi) {
+    if (!c) return HP_EINVAL;
+    if (ugv) *ugv = c->st.ugv;
+    if (ugs) *ugs = c->st.ugs;
+    if (ugi) *ugi = c->st.ugi;
+    if (resv) *resv = c->st.resv;
+    if (ress) *ress = c->st.ress;
+    if (resi) *resi = c->st.resi;
+    return HP_OK;
+}
+
+// Stream-ordered body of rsdl(stage) (no sync, capturable).
+static void enqueue_rsdl(hp_gpu_ctx *c, int stage) {
+    const int nstage = c->ph.nstage;
+    const int zero_rr = (stage >= nstage) ? 1 : 0;
+    const double omb = zero_rr ? 0.0 : 1.0 - c->ph.beta[stage];
+    const long n = (long)(c->lv + c->ls);
+    k_rsdl_pre<double><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>(
+        (int)c->lv, (int)c->ls, c->st.resv, c->st.ress, c->st.rrv, c->st.rrs, omb, zero_rr);
+    c->L.elem(c->d_tab, c->mesh, c->st, c->ph, stage, zero_rr, c->nsm, c->stream);
+    c->L.bflux(c->d_tab, c->mesh, c->st, c->ph, c->stream);
+}
+
+// minvrt (+ update of ug with cflalpha when upd) ; maxres into slot when slot != NULL
+static void enqueue_minvrt(hp_gpu_ctx *c, double cfla, int upd, int fold, unsigned long long *slot) {
+    c->L.vert(c->mesh, c->st, c->d_minv, c->sm, c->im, cfla, upd, fold, slot, c->stream);
+    for (int mode = 0; mode < c->sm; ++mode)
+        c->L.side(c->mesh, c->st, c->d_minv, c->im, mode, cfla, upd, fold, c->stream);
+    if (c->im > 0) c->L.intr(c->mesh, c->st, c->d_minv, cfla, upd, c->stream);
+}
+
+static void enqueue_update(hp_gpu_ctx *c) {
+    cudaMemcpyAsync(c->st.u0v, c->st.ugv, c->lv * 8, cudaMemcpyDeviceToDevice, c->stream);
+    if (c->ls) cudaMemcpyAsync(c->st.u0s, c->st.ugs, c->ls * 8, cudaMemcpyDeviceToDevice, c->stream);
+    if (c->li) cudaMemcpyAsync(c->st.u0i, c->st.ugi, c->li * 8, cudaMemcpyDeviceToDevice, c->stream);
+    for (int stage = 0; stage < c->ph.nstage; ++stage) {
+        enqueue_rsdl(c, stage);
+        const double cfla = c->ph.alpha[stage] * c->ph.cfl;
+        enqueue_minvrt(c, cfla, 1, 1, stage == c->ph.nstage - 1 ? c->d_slot : nullptr);
+    }
+    k_hist_advance<<<1, 32, 0, c->stream>>>(c->d_slot, c->d_hist, c->d_iter, c->NV, c->hist_cap);
+}
+
+static int check_launch(hp_gpu_ctx *c) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { set_err("kernel launch failed: %s", cudaGetErrorString(e)); return HP_ECUDA; }
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_rsdl(hp_gpu_ctx *c, int stage) {
+    if (!c || stage < 0 || stage > c->ph.nstage) { set_err("bad stage"); return HP_EINVAL; }
+    if (c->ph.physics == HP_PHYS_CD && c->ph.beta[stage] > 0.0 && !c->prcn_ready) {
+        set_err("cd rsdl needs tau from setup_preconditioner");
+        return HP_ESTATE;
+    }
+    enqueue_rsdl(c, stage);
+    // the reference's rsdl leaves res = res + res_r (nstage.cpp:76-82); the element kernel
+    // already folded the interiors, fold vertices and sides here for the caller
+    const long n = (long)(c->lv + c->ls);
+    k_rsdl_fold<double><<<nblk(n, 256), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, c->st.resv, c->st.rrv, c->st.ress,
+                                                             c->st.rrs);
+    int r = check_launch(c);
+    if (r) return r;
+    return hp_gpu_sync(c);
+}
+
+extern "C" int hp_gpu_setup_preconditioner(hp_gpu_ctx *c) {
+    if (!c) return HP_EINVAL;
+    CK(cudaMemsetAsync(c->st.vprcn, 0, (size_t)c->npnt * c->NV * 8, c->stream));
+    CK(cudaMemsetAsync(c->st.sprcn, 0, (size_t)c->nseg * c->NV * 8, c->stream));
+    CK(cudaMemsetAsync(c->d_err, 0, 4, c->stream));
+    c->L.prcn(c->d_tab, c->mesh, c->st, c->ph, c->d_err, c->stream);
+    const int nv = c->npnt * c->NV, ns = (c->p > 1 ? c->nseg * c->NV : 0);
+    k_prcn_invert<double><<<nblk(nv + ns, 256), 256, 0, c->stream>>>(nv, ns, c->st.vprcn, c->st.sprcn, c->vdiag);
+    int r = check_launch(c);
+    if (r) return r;
+    int herr = 0;
+    CK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->prcn_ready = true;
+    return herr;
+}
+
+extern "C" int hp_gpu_minvrt(hp_gpu_ctx *c) {
+    if (!c) return HP_EINVAL;
+    if (!c->prcn_ready) { set_err("minvrt before setup_preconditioner"); return HP_ESTATE; }
+    enqueue_minvrt(c, 0.0, 0, 0, nullptr);
+    int r = check_launch(c);
+    if (r) return r;
+    return hp_gpu_sync(c);
+}
+
+static int ensure_update_graph(hp_gpu_ctx *c) {
+    if (c->g_update) return HP_OK;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_update(c);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) { set_err("graph capture failed: %s", cudaGetErrorString(e)); return HP_ECUDA; }
+    e = cudaGraphInstantiate(&c->g_update, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { set_err("graph instantiate failed: %s", cudaGetErrorString(e)); c->g_update = nullptr; return HP_ECUDA; }
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_update(hp_gpu_ctx *c) {
+    if (!c) return HP_EINVAL;
+    if (!c->prcn_ready) { set_err("update before setup_preconditioner"); return HP_ESTATE; }
+    int r = ensure_update_graph(c);
+    if (r) return r;
+    CK(cudaGraphLaunch(c->g_update, c->stream));
+    return hp_gpu_sync(c);
+}
+
+extern "C" int hp_gpu_iterate(hp_gpu_ctx *c, int iters, int prcn_interval, double *hist) {
+    if (!c || iters < 0) return HP_EINVAL;
+    if (iters > c->hist_cap) { set_err("iters > %d", c->hist_cap); return HP_EINVAL; }
+    int r = ensure_update_graph(c);
+    if (r) return r;
+    CK(cudaMemsetAsync(c->d_iter, 0, 4, c->stream));
+    for (int it = 0; it < iters; ++it) {
+        if (!c->prcn_ready || (prcn_interval > 0 && it % prcn_interval == 0 && it > 0)) {
+            r = hp_gpu_setup_preconditioner(c);
+            if (r) return r;
+        }
+        CK(cudaGraphLaunch(c->g_update, c->stream));
+    }
+    if (hist && iters) CK(cudaMemcpyAsync(hist, c->d_hist, (size_t)iters * 8, cudaMemcpyDeviceToHost, c->stream));
+    return hp_gpu_sync(c);
+}
+
+extern "C" int hp_gpu_maxres(hp_gpu_ctx *c, double *out, double *mx) {
+    if (!c) return HP_EINVAL;
+    CK(cudaMemsetAsync(c->d_slot, 0, 32, c->stream));
+    // per-variable max over vertices of |res.v|
+    const int np = c->npnt, NV = c->NV;
+    std::vector<double> hv((size_t)np * NV);
+    CK(cudaMemcpyAsync(hv.data(), c->st.resv, hv.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double m[3] = {0, 0, 0}, e = 0.0;
+    for (int i = 0; i < np; ++i)
+        for (int n = 0; n < NV; ++n) m[n] = std::max(m[n], std::fabs(hv[(size_t)i * NV + n]));
+    for (int n = 0; n < NV; ++n) { if (out) out[n] = m[n]; e = std::max(e, m[n]); }
+    if (mx) *mx = e;
+    return HP_OK;
+}
+
+static int device_norm(hp_gpu_ctx *c, const double *a, size_t n, double &ss, double &mx) {
+    if (n == 0) return HP_OK;
+    int blocks = std::min(c->npart, nblk((long)n, 256));
+    k_norm_partial<double><<<blocks, 256, 0, c->stream>>>(a, n, c->d_part);
+    std::vector<double> h(2 * blocks);
+    CK(cudaMemcpyAsync(h.data(), c->d_part, h.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int b = 0; b < blocks; ++b) { ss += h[2 * b]; mx = std::max(mx, h[2 * b + 1]); }
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_resnorm(hp_gpu_ctx *c, double *l2, double *linf) {
+    if (!c) return HP_EINVAL;
+    int r = hp_gpu_rsdl(c, c->ph.nstage);
+    if (r) return r;
+    double ss = 0.0, mx = 0.0;
+    if ((r = device_norm(c, c->st.resv, c->lv, ss, mx))) return r;
+    if ((r = device_norm(c, c->st.ress, c->ls, ss, mx))) return r;
+    if ((r = device_norm(c, c->st.resi, c->li, ss, mx))) return r;
+    if (l2) *l2 = std::sqrt(ss);
+    if (linf) *linf = mx;
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_sync(hp_gpu_ctx *c) {
+    if (!c) return HP_EINVAL;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { set_err("stream sync: %s", cudaGetErrorString(e)); return HP_ECUDA; }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { set_err("cuda error: %s", cudaGetErrorString(e)); return HP_ECUDA; }
+    return HP_OK;
+}

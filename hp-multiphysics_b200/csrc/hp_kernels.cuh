@@ -1,0 +1,816 @@
+// Device code of the element-residual / multistage-smoothing path (sm_100a).
+//
+// Layout in HBM (element-major blocks, the reference's own blitz layouts):
+//   ug.v/res.v/res_r.v [npnt][NV], ug.s/... [nseg][sm][NV], ug.i/... [ntri][im][NV]
+//   mesh: tri_pnt/tri_seg [ntri][3] int32, tri_sgn packed as 3 bits per element,
+//         seg_pnt/seg_tri/seg_loc [nseg][2], vertex incidence in CSR form.
+// Each element is processed by one warp: the warp gathers the element's modes,
+// runs the sum-factorised contractions (proj -> point fluxes -> intgrtrs,
+// derivr/derivs for the strong residual) through shared memory, and scatters the
+// local residual: vertex and side modes with FP64/FP32 atomics, interior modes
+// with plain stores (they belong to one element).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hpb {
+
+// Compact per-p tables on the device (copied from hp_basis_tables).
+template <typename R, int P>
+struct DevTables {
+    static constexpr int G = P + 1, X = P + 2, T = (P + 1) * (P + 2) / 2, SM = P - 1, IM = (P - 1) * (P - 2) / 2,
+                         BM = 3 * P;
+    R gx[G][X], dgx[G][X], x0[G];
+    R gn[G][T], dgn[G][T], n0[G];
+    R gxwtx[X][G], dgxwtx[X][G];
+    R gnwtn[T][G], gnwtnn0[T][G], dgnwtn[T][G];
+    R dltx[G], dltx1[G][G], dltn[G], dltn1[G][G], dltn2[G][G];
+    R wtx[G];
+    int colstart[X + 1], colmodes[T], colof[T];
+};
+
+// minvrt tables (FP64 or FP32 copies)
+template <typename R>
+struct DevMinv {
+    R sfmv[2][8], vfms[3][8], sdiag[8], sfms[8][8][3];
+    R ifmb[24][21], bfmi[24][21], idiag[21][2];
+    R vdiag;
+};
+
+struct Phys {
+    int physics, NV, nstage;
+    double alpha[8], beta[8];
+    double cfl, bd0, adis, rho, mu, rhocv, kcond, ax, ay, src;
+};
+
+struct Mesh {
+    int npnt, nseg, ntri, nbseg;
+    const double *pnts;  // [npnt][2]
+    const int *tri_pnt, *tri_seg;
+    const int *tri_sgn;  // [ntri][3]
+    const int *seg_pnt, *seg_tri, *seg_loc;  // [nseg][2]
+    const int *vs_ptr, *vs_idx;  // vertex -> (seg*2+end)
+    const int *vt_ptr, *vt_idx;  // vertex -> (tri*4+local)
+    const int *vess, *sess;      // essential masks
+    const int *bseg, *bkind;
+    const double *bpibc;  // [nbseg][G]
+};
+
+template <typename R>
+struct State {
+    R *ugv, *ugs, *ugi;
+    R *u0v, *u0s, *u0i;
+    R *resv, *ress, *resi;
+    R *rrv, *rrs, *rri;
+    R *vprcn, *sprcn, *tprcn, *tau;
+};
+
+__device__ __forceinline__ void atomic_add(double *a, double v) { atomicAdd(a, v); }
+__device__ __forceinline__ void atomic_add(float *a, float v) { atomicAdd(a, v); }
+
+template <typename R>
+__device__ __forceinline__ R rsqrt_(R x);
+template <>
+__device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
+template <>
+__device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+
+// ---------------------------------------------------------------------------
+// Element residual: one warp per element.
+// ---------------------------------------------------------------------------
+template <typename R, int P, int PHYS>
+struct ElemCfg {
+    static constexpr int G = P + 1, X = P + 2, T = (P + 1) * (P + 2) / 2, SM = P - 1, IM = (P - 1) * (P - 2) / 2,
+                         BM = 3 * P;
+    static constexpr int NV = (PHYS == 1 ? 3 : 1);
+    static constexpr int NPAIR = NV;               // flux pairs integrated by intgrtrs
+    static constexpr int NQ = (PHYS == 1 ? 16 : 7);  // per-point scratch values
+    static constexpr int WPC = (P <= 4 ? 8 : 4);   // warps per CTA
+    // per-warp scratch (in R units)
+    static constexpr int S_UHT = NV * T;
+    static constexpr int S_WK = (6 * G * X > 5 * G * X ? 6 * G * X : 5 * G * X);
+    static constexpr int S_PT = (NQ + NV) * G * G;
+    static constexpr int S_WARP = S_UHT + S_WK + S_PT;
+};
+
+// Point-array slot indices (each slot is a [G][G] array)
+// ins: 0..3 cvI (cv00,cv01,cv10,cv11)  4,5 mI  6..9 cvT  10..13 df  14,15 u,v  16..18 res
+// cd : 0,1 cvI  2,3 cvT  4,5 e  6 u      7 res
+
+template <typename R, int P, int PHYS>
+__global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
+    k_rsdl_elem(const DevTables<R, P> *__restrict__ gtab, Mesh mesh, State<R> st, Phys ph, int stage, int zero_rr) {
+    using C = ElemCfg<R, P, PHYS>;
+    constexpr int G = C::G, X = C::X, T = C::T, IM = C::IM, BM = C::BM, NV = C::NV, GG = G * G;
+    constexpr int SM = (C::SM > 0 ? C::SM : 1);  // side-mode stride (unused when p = 1)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    DevTables<R, P> &tb = *reinterpret_cast<DevTables<R, P> *>(smem_raw);
+    R *warp_base = reinterpret_cast<R *>(smem_raw + ((sizeof(DevTables<R, P>) + 15) / 16) * 16);
+    {
+        const int n4 = sizeof(DevTables<R, P>) / 4;
+        const int *src = reinterpret_cast<const int *>(gtab);
+        int *dst = reinterpret_cast<int *>(smem_raw);
+        for (int k = threadIdx.x; k < n4; k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    R *uht = warp_base + warp * C::S_WARP;
+    R *wk = uht + C::S_UHT;
+    R *pt = wk + C::S_WK;
+    auto PT = [&](int q) -> R * { return pt + q * GG; };
+
+    const R beta = (R)ph.beta[stage];
+    const R omb = zero_rr ? (R)0 : (R)1 - beta;
+
+    for (int tind = blockIdx.x * C::WPC + warp; tind < mesh.ntri; tind += gridDim.x * C::WPC) {
+        const int p0 = mesh.tri_pnt[3 * tind], p1 = mesh.tri_pnt[3 * tind + 1], p2 = mesh.tri_pnt[3 * tind + 2];
+        // ---- gather (ugtouht, gtol.cpp:14-55)
+        for (int w = lane; w < NV * T; w += 32) {
+            const int n = w / T, m = w - n * T;
+            R val;
+            if (m < 3) {
+                const int v = (m == 0 ? p0 : (m == 1 ? p1 : p2));
+                val = st.ugv[v * NV + n];
+            } else if (m < BM) {
+                const int i = (m - 3) / SM, k = (m - 3) - i * SM;
+                const int sind = mesh.tri_seg[3 * tind + i], sg = mesh.tri_sgn[3 * tind + i];
+                val = st.ugs[(sind * SM + k) * NV + n];
+                if ((k & 1) && sg < 0) val = -val;
+            } else {
+                val = st.ugi[((size_t)tind * IM + (m - BM)) * NV + n];
+            }
+            uht[n * T + m] = val;
+        }
+        // geometry (straight element): ldcrd(n,0) = (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2
+        const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
+        const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
+        const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
+        const R d00 = (R)(0.5 * (x2d - x1d)), d01 = (R)(0.5 * (x0d - x1d));
+        const R d10 = (R)(0.5 * (y2d - y1d)), d11 = (R)(0.5 * (y0d - y1d));
+        __syncwarp();
+        // ---- proj stage I (proj.cpp:46-95): wk[q][j][n]; q = 2*var (value), 2*var+1 (d/deta)
+        {
+            constexpr int NDV = (PHYS == 1 ? 2 : 1);  // variables projected with derivatives
+            constexpr int NQW = 2 * NDV + (NV - NDV);
+            for (int w = lane; w < NQW * G * X; w += 32) {
+                const int q = w / (G * X), r = w - q * (G * X), j = r / X, n = r - j * X;
+                int var, der;
+                if (q < 2 * NDV) { var = q >> 1; der = q & 1; }
+                else { var = NDV + (q - 2 * NDV); der = 0; }
+                const R *lin = uht + var * T;
+                R acc = 0;
+                for (int c = tb.colstart[n]; c < tb.colstart[n + 1]; ++c) {
+                    const int m = tb.colmodes[c];
+                    acc += lin[m] * (der ? tb.dgn[j][m] : tb.gn[j][m]);
+                }
+                wk[(q * G + j) * X + n] = acc;
+            }
+        }
+        __syncwarp();
+        // ---- proj stage II + pointwise fluxes
+        for (int w = lane; w < GG; w += 32) {
+            const int i = w / G, j = w - i * G;
+            const R oeta = tb.n0[j], xp1 = tb.x0[i];
+            if (PHYS == 1) {
+                R uu[3], dr[2], ds[2];
+                for (int var = 0; var < 2; ++var) {
+                    const R *w0 = wk + ((2 * var) * G + j) * X, *w1 = wk + ((2 * var + 1) * G + j) * X;
+                    R l0 = 0, l1 = 0, l2 = 0;
+                    for (int n = 0; n < X; ++n) {
+                        l0 += w0[n] * tb.gx[i][n];
+                        l1 += w1[n] * tb.gx[i][n];
+                        l2 += (w0[n] * oeta) * tb.dgx[i][n];
+                    }
+                    uu[var] = l0; ds[var] = l1 + xp1 * l2; dr[var] = l2;
+                }
+                {
+                    const R *w0 = wk + (4 * G + j) * X;
+                    R l0 = 0;
+                    for (int n = 0; n < X; ++n) l0 += w0[n] * tb.gx[i][n];
+                    uu[2] = l0;
+                }
+                const R rho = (R)ph.rho;
+                const R fluxx = rho * uu[0], fluxy = rho * uu[1];
+                const R m0 = +d11 * fluxx - d01 * fluxy;
+                const R m1 = -d10 * fluxx + d00 * fluxy;
+                R c00 = uu[0] * m0, c01 = uu[0] * m1, c10 = uu[1] * m0, c11 = uu[1] * m1;
+                c00 += d11 * uu[2];
+                c01 -= d10 * uu[2];
+                c10 -= d01 * uu[2];
+                c11 += d00 * uu[2];
+                PT(0)[w] = c00; PT(1)[w] = c01; PT(2)[w] = c10; PT(3)[w] = c11;
+                PT(4)[w] = m0; PT(5)[w] = m1;
+                if (beta > (R)0) {
+                    const R cjcb = d00 * d11 - d10 * d01;
+                    const R cjcbi = (R)ph.mu / cjcb;
+                    const R v0000 = -cjcbi * ((R)2. * d11 * d11 + d01 * d01);
+                    const R v0011 = -cjcbi * ((R)2. * d10 * d10 + d00 * d00);
+                    const R v0001 = cjcbi * ((R)2. * d11 * d10 + d01 * d00);
+                    const R v1100 = -cjcbi * (d11 * d11 + (R)2. * d01 * d01);
+                    const R v1111 = -cjcbi * (d10 * d10 + (R)2. * d00 * d00);
+                    const R v1101 = cjcbi * (d11 * d10 + (R)2. * d01 * d00);
+                    const R v0100 = cjcbi * d01 * d11;
+                    const R v0111 = cjcbi * d00 * d10;
+                    const R v0101 = -cjcbi * d01 * d10;
+                    const R v0110 = -cjcbi * d00 * d11;
+                    const R f00 = (v0000 * dr[0] + v0100 * dr[1] + v0001 * ds[0] + v0101 * ds[1]);
+                    const R f01 = (v0001 * dr[0] + v0110 * dr[1] + v0011 * ds[0] + v0111 * ds[1]);
+                    const R f10 = (v0100 * dr[0] + v1100 * dr[1] + v0110 * ds[0] + v1101 * ds[1]);
+                    const R f11 = (v0101 * dr[0] + v1101 * dr[1] + v0111 * ds[0] + v1111 * ds[1]);
+                    PT(6)[w] = c00 + f00; PT(7)[w] = c01 + f01; PT(8)[w] = c10 + f10; PT(9)[w] = c11 + f11;
+                    PT(10)[w] = f00; PT(11)[w] = f01; PT(12)[w] = f10; PT(13)[w] = f11;
+                    PT(14)[w] = uu[0]; PT(15)[w] = uu[1];
+                }
+            } else {
+                const R *w0 = wk + (0 * G + j) * X, *w1 = wk + (1 * G + j) * X;
+                R l0 = 0, l1 = 0, l2 = 0;
+                for (int n = 0; n < X; ++n) {
+                    l0 += w0[n] * tb.gx[i][n];
+                    l1 += w1[n] * tb.gx[i][n];
+                    l2 += (w0[n] * oeta) * tb.dgx[i][n];
+                }
+                const R u = l0, ds = l1 + xp1 * l2, dr = l2;
+                const R fluxx = (R)ph.rhocv * (R)ph.ax * u, fluxy = (R)ph.rhocv * (R)ph.ay * u;
+                const R c00 = +d11 * fluxx - d01 * fluxy;
+                const R c01 = -d10 * fluxx + d00 * fluxy;
+                PT(0)[w] = c00; PT(1)[w] = c01;
+                if (beta > (R)0) {
+                    const R cj = d00 * d11 - d10 * d01;
+                    const R kc = (R)ph.kcond / cj;
+                    const R v00 = -kc * (d11 * d11 + d01 * d01);
+                    const R v11 = -kc * (d10 * d10 + d00 * d00);
+                    const R v01 = kc * (d11 * d10 + d01 * d00);
+                    const R e00 = v00 * dr + v01 * ds, e01 = v01 * dr + v11 * ds;
+                    PT(2)[w] = c00 + e00; PT(3)[w] = c01 + e01;
+                    PT(4)[w] = e00; PT(5)[w] = e01;
+                    PT(6)[w] = u;
+                }
+            }
+        }
+        __syncwarp();
+        // ---- intgrtrs of the imaginary fluxes (intgrt.cpp:81-158) -> res (and res.i)
+        // pair k: ins (cv0x,cv0y)=slots(0,1), (cv1x,cv1y)=(2,3), (mx,my)=(4,5); cd (0,1)
+        auto intgrtrs_stageI = [&](int sx0) {
+            for (int w = lane; w < C::NPAIR * X * G; w += 32) {
+                const int k = w / (X * G), r = w - k * (X * G), n = r / G, j = r - n * G;
+                const R *dx = PT(sx0 + 2 * k), *dy = PT(sx0 + 2 * k + 1);
+                R l0 = 0, l1 = 0;
+                for (int i = 0; i < G; ++i) {
+                    const R w2 = dx[i * G + j] + dy[i * G + j] * tb.x0[i];
+                    l0 += w2 * tb.dgxwtx[n][i];
+                    l1 += dy[i * G + j] * tb.gxwtx[n][i];
+                }
+                wk[((2 * k) * X + n) * G + j] = l0;
+                wk[((2 * k + 1) * X + n) * G + j] = l1;
+            }
+        };
+        auto mode_result = [&](int k, int m) -> R {
+            const int col = tb.colof[m];
+            const R *w0 = wk + ((2 * k) * X + col) * G, *w1 = wk + ((2 * k + 1) * X + col) * G;
+            R l0 = 0;
+            for (int j = 0; j < G; ++j) l0 -= tb.gnwtnn0[m][j] * w0[j] + tb.dgnwtn[m][j] * w1[j];
+            return l0;
+        };
+        // scatter of one local coefficient of variable n, mode m (lftog, gtol.cpp:364-402)
+        auto scatter = [&](R *gv, R *gs, int n, int m, R val) {
+            if (m < 3) {
+                const int v = (m == 0 ? p0 : (m == 1 ? p1 : p2));
+                atomic_add(&gv[v * NV + n], val);
+            } else {
+                const int i = (m - 3) / SM, k = (m - 3) - i * SM;
+                const int sind = mesh.tri_seg[3 * tind + i], sg = mesh.tri_sgn[3 * tind + i];
+                if ((k & 1) && sg < 0) val = -val;
+                atomic_add(&gs[(sind * SM + k) * NV + n], val);
+            }
+        };
+        intgrtrs_stageI(0);
+        __syncwarp();
+        for (int w = lane; w < NV * T; w += 32) {
+            const int n = w / T, m = w - n * T;
+            const R val = mode_result(n, m);
+            if (m < BM) {
+                scatter(st.resv, st.ress, n, m, val);
+            } else {
+                const size_t gi = ((size_t)tind * IM + (m - BM)) * NV + n;
+                if (beta > (R)0) st.resi[gi] = val;
+                else st.resi[gi] = val + st.rri[gi] * omb;  // res_r unchanged when beta = 0
+            }
+        }
+        if (beta > (R)0) {
+            // ---- strong residual: res = source + derivr(F_r) + derivs(F_s) (proj.cpp:339-402)
+            __syncwarp();
+            constexpr int SRES = (PHYS == 1 ? 16 : 7);
+            for (int w = lane; w < NV * GG; w += 32) {
+                const int n = w / GG, r = w - n * GG, i = r / G, j = r - i * G;
+                int sr, ss;
+                if (PHYS == 1) { sr = (n < 2 ? 6 + 2 * n : 4); ss = sr + 1; }
+                else { sr = 2; ss = 3; }
+                const R *fr = PT(sr), *fs = PT(ss);
+                R acc;
+                if (PHYS == 1) acc = (R)0;  // rhorbd0*u + dugdt with bd(0) = 0
+                else acc = -(d00 * d11 - d10 * d01) * (R)ph.src;
+                const R ln0 = tb.n0[j];
+                {
+                    const R wi = fr[i * G + j] * tb.dltx[i] * ln0;
+                    for (int q = 0; q < G; ++q)
+                        if (q != i) acc += (wi + fr[q * G + j] * tb.dltx[q] * ln0) * tb.dltx1[i][q];
+                }
+                {
+                    const R wi = fs[i * G + j] * tb.dltx[i] * ln0;
+                    for (int q = 0; q < G; ++q)
+                        if (q != i) acc += (wi + fs[q * G + j] * tb.dltx[q] * ln0) * tb.dltn1[i][q];
+                    const R wj = fs[i * G + j] * tb.dltn[j];
+                    for (int q = 0; q < G; ++q)
+                        if (q != j) acc += (wj + fs[i * G + q] * tb.dltn[q]) * tb.dltn2[j][q];
+                }
+                PT(SRES + n)[r] = acc;
+            }
+            __syncwarp();
+            // ---- pointwise SUPG terms
+            if (PHYS == 1) {
+                // inscribed radius (tri_mesh/tprims.cpp:224-241)
+                const double dx1 = x0d - x2d, dy1 = y0d - y2d, dx2 = x1d - x0d, dy2 = y1d - y0d;
+                const double area = dx1 * dy2 - dy1 * dx2;
+                const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
+                                     sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
+                const R h = (R)((area / perim) / (0.25 * (P + 1) * (P + 1)));
+                const R cjcb = d00 * d11 - d10 * d01;
+                const R nu = (R)(ph.mu / ph.rho);
+                for (int w = lane; w < GG; w += 32) {
+                    const R u0 = PT(14)[w], u1 = PT(15)[w];
+                    const R q = u0 * u0 + u1 * u1;
+                    const R t2 = (R)2. * nu / h;
+                    R gam = (R)3.0 * q + t2 * t2;
+                    if (ph.mu + ph.bd0 == 0.0) gam = (gam > (R)0.1 ? gam : (R)0.1);
+                    const R tau0 = (R)ph.adis * h / (cjcb * rsqrt_<R>(gam));
+                    const R tau2 = rsqrt_<R>(q) * tau0;
+                    const R tr0 = tau0 * PT(16)[w], tr1 = tau0 * PT(17)[w], tr2 = tau2 * PT(18)[w];
+                    PT(10)[w] -= (d11 * ((R)2 * u0) - d01 * u1) * tr0 - d01 * u0 * tr1 + d11 * tr2;
+                    PT(11)[w] -= (-d10 * ((R)2 * u0) + d00 * u1) * tr0 + d00 * u0 * tr1 - d10 * tr2;
+                    PT(12)[w] -= +d11 * u1 * tr0 + (d11 * u0 - d01 * ((R)2. * u1)) * tr1 - d01 * tr2;
+                    PT(13)[w] -= -d10 * u1 * tr0 + (-d10 * u0 + d00 * ((R)2. * u1)) * tr1 + d00 * tr2;
+                    PT(14)[w] = -(d11 * tr0 - d01 * tr1);
+                    PT(15)[w] = -(-d10 * tr0 + d00 * tr1);
+                }
+            } else {
+                const R taue = st.tau[tind];
+                const R ax = (R)ph.ax, ay = (R)ph.ay;
+                for (int w = lane; w < GG; w += 32) {
+                    const R tres = taue * PT(7)[w];
+                    PT(4)[w] -= (d11 * ax - d01 * ay) * tres;
+                    PT(5)[w] -= (-d10 * ax + d00 * ay) * tres;
+                }
+            }
+            __syncwarp();
+            // ---- intgrtrs of the real part -> res_r; ins pairs (10,11),(12,13),(14,15); cd (4,5)
+            intgrtrs_stageI(PHYS == 1 ? 10 : 4);
+            // cd source term: intgrt(res0) with res0 = -cjcb*src (constant over the element)
+            __syncwarp();
+            for (int w = lane; w < NV * T; w += 32) {
+                const int n = w / T, m = w - n * T;
+                R val = mode_result(n, m);
+                if (PHYS == 0 && ph.src != 0.0) {
+                    // intgrt of a constant field c: sum_j gnwtn(m,j) * sum_i c*gxwtx(col,i)
+                    const R cval = -(d00 * d11 - d10 * d01) * (R)ph.src;
+                    const int col = tb.colof[m];
+                    R l0 = 0;
+                    for (int j = 0; j < G; ++j) {
+                        R s = cval * tb.gxwtx[col][0];
+                        for (int i = 1; i < G; ++i) s += cval * tb.gxwtx[col][i];
+                        l0 += tb.gnwtn[m][j] * s;
+                    }
+                    val = l0 + val;
+                }
+                val *= beta;
+                if (m < BM) {
+                    scatter(st.rrv, st.rrs, n, m, val);
+                } else {
+                    const size_t gi = ((size_t)tind * IM + (m - BM)) * NV + n;
+                    const R rr = st.rri[gi] * omb + val;
+                    st.rri[gi] = rr;
+                    st.resi[gi] += rr;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// res.v = res.s = 0 ; res_r.{v,s} *= (1-beta) (or = 0) : nstage.cpp:21-49
+template <typename R>
+__global__ void k_rsdl_pre(int nv_len, int ns_len, R *resv, R *ress, R *rrv, R *rrs, R omb, int zero_rr) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nv_len + ns_len; k += stride) {
+        if (k < nv_len) {
+            resv[k] = (R)0;
+            rrv[k] = zero_rr ? (R)0 : rrv[k] * omb;
+        } else {
+            const int q = k - nv_len;
+            ress[q] = (R)0;
+            rrs[q] = zero_rr ? (R)0 : rrs[q] * omb;
+        }
+    }
+}
+
+// Boundary-edge flux of bdry_ins::generic (hp_boundary.cpp:973-1049, ins/bdry_ins.h:35-50).
+// One thread per boundary edge.
+template <typename R, int P>
+__global__ void k_bdry_flux_ins(const DevTables<R, P> *__restrict__ tb, Mesh mesh, State<R> st, Phys ph) {
+    constexpr int G = P + 1, X = P + 2, SM = P - 1, NV = 3;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= mesh.nbseg) return;
+    if ((mesh.bkind[e] & (0xF << 8)) != (1 << 8)) return;
+    const int sind = mesh.bseg[e];
+    const int v0 = mesh.seg_pnt[2 * sind], v1 = mesh.seg_pnt[2 * sind + 1];
+    R lin[NV][SM + 2];
+    for (int n = 0; n < NV; ++n) {
+        lin[n][0] = st.ugv[v0 * NV + n];
+        lin[n][1] = st.ugv[v1 * NV + n];
+        for (int m = 0; m < SM; ++m) lin[n][m + 2] = st.ugs[(sind * SM + m) * NV + n];
+    }
+    const R xa = (R)mesh.pnts[2 * v0], ya = (R)mesh.pnts[2 * v0 + 1];
+    const R xb = (R)mesh.pnts[2 * v1], yb = (R)mesh.pnts[2 * v1 + 1];
+    R acc[NV][X - 1];
+    for (int n = 0; n < NV; ++n)
+        for (int m = 0; m < X - 1; ++m) acc[n][m] = 0;
+    for (int k = 0; k < G; ++k) {
+        // proj1d of the straight side coordinates: derivative only
+        const R dx = xa * tb->dgx[k][1] + xb * tb->dgx[k][2];
+        const R dy = ya * tb->dgx[k][1] + yb * tb->dgx[k][2];
+        R nrm0 = dy, nrm1 = -dx;
+        const R jcb = rsqrt_<R>(nrm0 * nrm0 + nrm1 * nrm1);
+        nrm0 /= jcb; nrm1 /= jcb;
+        R u[NV];
+        for (int n = 0; n < NV; ++n) {
+            R l0 = lin[n][0] * tb->gx[k][1] + lin[n][1] * tb->gx[k][2];
+            for (int m = 2; m < SM + 2; ++m) l0 += lin[n][m] * tb->gx[k][m + 1];
+            u[n] = l0;
+        }
+        R flx[NV];
+        flx[2] = (R)ph.rho * (u[0] * nrm0 + u[1] * nrm1);
+        const R pb = (R)mesh.bpibc[e * G + k];
+        flx[0] = flx[2] * u[0] + pb * nrm0;
+        flx[1] = flx[2] * u[1] + pb * nrm1;
+        for (int n = 0; n < NV; ++n) {
+            const R r = flx[n] * jcb;
+            acc[n][0] += tb->gxwtx[1][k] * r;
+            acc[n][1] += tb->gxwtx[2][k] * r;
+            for (int m = 3; m < X; ++m) acc[n][m - 1] += tb->gxwtx[m][k] * r;
+        }
+    }
+    for (int n = 0; n < NV; ++n) {
+        atomic_add(&st.resv[v0 * NV + n], acc[n][0]);
+        atomic_add(&st.resv[v1 * NV + n], acc[n][1]);
+        for (int m = 0; m < SM; ++m) atomic_add(&st.ress[(sind * SM + m) * NV + n], acc[n][m + 2]);
+    }
+}
+
+// Order-preserving key of a non-negative floating value (for atomicMax).
+__device__ __forceinline__ unsigned long long ord_key(double v) { return (unsigned long long)__double_as_longlong(v); }
+__device__ __forceinline__ unsigned long long ord_key(float v) { return (unsigned long long)__double_as_longlong((double)v); }
+
+// ---------------------------------------------------------------------------
+// minvrt (setup_preconditioner.cpp:102-373) fused with the stage update
+// (nstage.cpp:387-409).
+// ---------------------------------------------------------------------------
+// Vertex phase: assemble res.v + res_r.v, remove side and interior parts, apply
+// the vertex preconditioner and Dirichlet zeroing, update ug.v, maxres.
+template <typename R, int NV>
+__global__ void k_minv_vert(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, int sm, int im, R cflalpha,
+                            int do_update, int fold, unsigned long long *maxres_slot) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    R r[NV];
+    bool active = v < mesh.npnt;
+    if (active) {
+        for (int n = 0; n < NV; ++n) r[n] = st.resv[v * NV + n] + (fold ? st.rrv[v * NV + n] : (R)0);
+        for (int q = mesh.vs_ptr[v]; q < mesh.vs_ptr[v + 1]; ++q) {
+            const int code = mesh.vs_idx[q], s = code >> 1, end = code & 1;
+            for (int k = 0; k < sm; ++k) {
+                const R f = mt->sfmv[end][k];
+                for (int n = 0; n < NV; ++n) {
+                    const int gi = (s * sm + k) * NV + n;
+                    r[n] -= f * (st.ress[gi] + (fold ? st.rrs[gi] : (R)0));
+                }
+            }
+        }
+        if (im > 0)
+            for (int q = mesh.vt_ptr[v]; q < mesh.vt_ptr[v + 1]; ++q) {
+                const int code = mesh.vt_idx[q], t = code >> 2, i = code & 3;
+                for (int k = 0; k < im; ++k) {
+                    const R f = mt->ifmb[i][k];
+                    for (int n = 0; n < NV; ++n) r[n] -= f * st.resi[((size_t)t * im + k) * NV + n];
+                }
+            }
+        const int ess = mesh.vess[v];
+        for (int n = 0; n < NV; ++n) {
+            r[n] *= st.vprcn[v * NV + n];
+            if (ess & (1 << n)) r[n] = (R)0;
+            st.resv[v * NV + n] = r[n];
+            if (do_update) st.ugv[v * NV + n] = st.u0v[v * NV + n] - cflalpha * r[n];
+        }
+    }
+    if (maxres_slot) {
+        for (int n = 0; n < NV; ++n) {
+            R a = active ? fabs(r[n]) : (R)0;
+            for (int o = 16; o > 0; o >>= 1) {
+                R b = __shfl_xor_sync(0xffffffffu, a, o);
+                a = a > b ? a : b;
+            }
+            if ((threadIdx.x & 31) == 0) atomicMax(&maxres_slot[n], ord_key(a));
+        }
+    }
+}
+
+// Side phase for mode `mode`: mode 0 assembles res.s + res_r.s and removes the
+// interior and vertex parts; mode > 0 removes the finished mode-1 of the three
+// sides of each adjacent element. Then mode `mode` is finished: preconditioner,
+// sdiag, Dirichlet zeroing, update of ug.s.
+template <typename R, int NV, int SM>
+__global__ void k_minv_side(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, int im, int mode, R cflalpha,
+                            int do_update, int fold) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= mesh.nseg) return;
+    R r[SM][NV];
+    if (mode == 0) {
+        for (int k = 0; k < SM; ++k)
+            for (int n = 0; n < NV; ++n) {
+                const int gi = (s * SM + k) * NV + n;
+                r[k][n] = st.ress[gi] + (fold ? st.rrs[gi] : (R)0);
+            }
+    } else {
+        for (int k = mode; k < SM; ++k)
+            for (int n = 0; n < NV; ++n) r[k][n] = st.ress[(s * SM + k) * NV + n];
+    }
+    for (int side = 0; side < 2; ++side) {
+        const int t = mesh.seg_tri[2 * s + side];
+        if (t < 0) continue;
+        const int i = mesh.seg_loc[2 * s + side];
+        const int sgn_i = mesh.tri_sgn[3 * t + i];
+        if (mode == 0) {
+            // interior removal (setup_preconditioner.cpp:131-145)
+            for (int k = 0; k < SM; ++k) {
+                const R msgn = ((k & 1) && sgn_i < 0) ? (R)-1 : (R)1;
+                for (int kk = 0; kk < im; ++kk) {
+                    const R f = msgn * mt->ifmb[3 + i * SM + k][kk];
+                    for (int n = 0; n < NV; ++n) r[k][n] -= f * st.resi[((size_t)t * im + kk) * NV + n];
+                }
+            }
+            // vertex removal (setup_preconditioner.cpp:192-214)
+            for (int j = 0; j < 3; ++j) {
+                const int i1 = (i + j) % 3;
+                const int vv = mesh.tri_pnt[3 * t + i1];
+                for (int n = 0; n < NV; ++n) {
+                    const R uh = st.resv[vv * NV + n] * st.tprcn[t * NV + n];
+                    for (int k = 0; k < SM; ++k) {
+                        const R msgn = ((k & 1) && sgn_i < 0) ? (R)-1 : (R)1;
+                        r[k][n] -= msgn * mt->vfms[j][k] * uh;
+                    }
+                }
+            }
+        } else {
+            // removal of mode-1 from higher modes (setup_preconditioner.cpp:264-284)
+            const int pm = mode - 1;
+            R uh[3][NV];
+            for (int j = 0; j < 3; ++j) {
+                const int sj = mesh.tri_seg[3 * t + j];
+                const int sgj = mesh.tri_sgn[3 * t + j];
+                const R sg = ((pm & 1) && sgj < 0) ? (R)-1 : (R)1;
+                for (int n = 0; n < NV; ++n) uh[j][n] = sg * st.ress[(sj * SM + pm) * NV + n] * st.tprcn[t * NV + n];
+            }
+            R msgn = (((pm + 1) & 1) && sgn_i < 0) ? (R)-1 : (R)1;
+            for (int m = mode; m < SM; ++m) {
+                for (int j = 0; j < 3; ++j) {
+                    const int indx = (i + j) % 3;
+                    const R f = msgn * mt->sfms[pm][m][j];
+                    for (int n = 0; n < NV; ++n) r[m][n] -= f * uh[indx][n];
+                }
+                if (sgn_i < 0) msgn = -msgn;
+            }
+        }
+    }
+    const int ess = mesh.sess[s];
+    for (int n = 0; n < NV; ++n) {
+        R v = r[mode][n] * (st.sprcn[s * NV + n] * mt->sdiag[mode]);
+        if (ess & (1 << n)) v = (R)0;
+        r[mode][n] = v;
+    }
+    const int k0 = (mode == 0 ? 0 : mode);
+    for (int k = k0; k < SM; ++k)
+        for (int n = 0; n < NV; ++n) st.ress[(s * SM + k) * NV + n] = r[k][n];
+    if (do_update)
+        for (int n = 0; n < NV; ++n) {
+            const int gi = (s * SM + mode) * NV + n;
+            st.ugs[gi] = st.u0s[gi] - cflalpha * r[mode][n];
+        }
+}
+
+// Interior phase (setup_preconditioner.cpp:341-370, DPBTRSNU2 as written in
+// utilities/myblas.c:91-120) + update of ug.i.
+template <typename R, int NV, int SM, int IM>
+__global__ void k_minv_int(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha, int do_update) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= mesh.ntri) return;
+    R b[IM][NV];
+    for (int k = 0; k < IM; ++k)
+        for (int n = 0; n < NV; ++n) b[k][n] = st.resi[((size_t)t * IM + k) * NV + n];
+    // DPBTRSNU2(idiag, stride 2, IM, ofdg 1, b, NV)
+    for (int i = 0; i < IM; ++i) {
+        if (i >= 1)
+            for (int n = 0; n < NV; ++n) b[i][n] -= mt->idiag[i][0] * b[0][n];
+        for (int n = 0; n < NV; ++n) b[i][n] /= mt->idiag[i][1];
+    }
+    for (int i = IM - 1; i >= 0; --i) {
+        for (int n = 0; n < NV; ++n) b[i][n] /= mt->idiag[i][1];
+        if (i >= 1)
+            for (int n = 0; n < NV; ++n) b[0][n] -= mt->idiag[i][0] * b[i][n];
+    }
+    R tp[NV];
+    for (int n = 0; n < NV; ++n) tp[n] = st.tprcn[t * NV + n];
+    for (int k = 0; k < IM; ++k)
+        for (int n = 0; n < NV; ++n) b[k][n] /= tp[n];
+    // restouht_bdry and bfmi removal
+    for (int i = 0; i < 3; ++i) {
+        const int vv = mesh.tri_pnt[3 * t + i];
+        for (int n = 0; n < NV; ++n) {
+            const R u = st.resv[vv * NV + n];
+            for (int k = 0; k < IM; ++k) b[k][n] -= mt->bfmi[i][k] * u;
+        }
+    }
+    for (int i = 0; i < 3; ++i) {
+        const int sd = mesh.tri_seg[3 * t + i], sg = mesh.tri_sgn[3 * t + i];
+        for (int m = 0; m < SM; ++m) {
+            const R msgn = ((m & 1) && sg < 0) ? (R)-1 : (R)1;
+            for (int n = 0; n < NV; ++n) {
+                const R u = msgn * st.ress[(sd * SM + m) * NV + n];
+                for (int k = 0; k < IM; ++k) b[k][n] -= mt->bfmi[3 + i * SM + m][k] * u;
+            }
+        }
+    }
+    for (int k = 0; k < IM; ++k)
+        for (int n = 0; n < NV; ++n) {
+            const size_t gi = ((size_t)t * IM + k) * NV + n;
+            st.resi[gi] = b[k][n];
+            if (do_update) st.ugi[gi] = st.u0i[gi] - cflalpha * b[k][n];
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal preconditioner (ins/setup_preconditioner.cpp:9-221 REFINED_WAY,
+// cd/setup_preconditioner.cpp:6-97) with tau, scatter to vprcn/sprcn.
+// ---------------------------------------------------------------------------
+template <typename R, int P, int PHYS>
+__global__ void k_prcn_elem(const DevTables<R, P> *__restrict__ tb, Mesh mesh, State<R> st, Phys ph, int *err) {
+    constexpr int G = P + 1, X = P + 2, T = (P + 1) * (P + 2) / 2, SM = P - 1, BM = 3 * P, NV = (PHYS == 1 ? 3 : 1);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= mesh.ntri) return;
+    const int v[3] = {mesh.tri_pnt[3 * t], mesh.tri_pnt[3 * t + 1], mesh.tri_pnt[3 * t + 2]};
+    const double px[3] = {mesh.pnts[2 * v[0]], mesh.pnts[2 * v[1]], mesh.pnts[2 * v[2]]};
+    const double py[3] = {mesh.pnts[2 * v[0] + 1], mesh.pnts[2 * v[1] + 1], mesh.pnts[2 * v[2] + 1]};
+    // area (tprims.cpp:66-80), 2x triangle area
+    const double dx1 = px[0] - px[2], dy1 = py[0] - py[2], dx2 = px[1] - px[0], dy2 = py[1] - py[0];
+    double jcb = 0.25 * (dx1 * dy2 - dy1 * dx2);
+    double hmax = 0.0;
+    for (int j = 0; j < 3; ++j) {
+        const double ex = px[j] - px[(j + 1) % 3], ey = py[j] - py[(j + 1) % 3];
+        const double h = ex * ex + ey * ey;
+        hmax = (h > hmax ? h : hmax);
+    }
+    const double p1 = 0.25 * (P + 1) * (P + 1);
+    double tp[3];
+    if (PHYS == 0) {
+        hmax = sqrt(hmax);
+        if (!(jcb > 0.0)) { atomicAdd(err, 1); return; }
+        const double h = 4. * jcb / (p1 * hmax);
+        const double q = sqrt(ph.ax * ph.ax + ph.ay * ph.ay);
+        const double alpha = ph.kcond / ph.rhocv;
+        const double lam1 = (q + 1.5 * alpha / h + h * ph.bd0);
+        st.tau[t] = (R)(ph.adis * h / (jcb * lam1));
+        jcb *= ph.rhocv * lam1 / h;
+        tp[0] = jcb;
+    } else {
+        // u, v at Gauss points (values only): proj.cpp:121-186 on the element's modes
+        double lin[2][T];
+        for (int n = 0; n < 2; ++n) {
+            for (int i = 0; i < 3; ++i) lin[n][i] = (double)st.ugv[v[i] * NV + n];
+            for (int i = 0; i < 3; ++i) {
+                const int sd = mesh.tri_seg[3 * t + i], sg = mesh.tri_sgn[3 * t + i];
+                for (int k = 0; k < SM; ++k) {
+                    double val = (double)st.ugs[(sd * SM + k) * NV + n];
+                    if ((k & 1) && sg < 0) val = -val;
+                    lin[n][3 + i * SM + k] = val;
+                }
+            }
+            for (int k = 0; k < T - BM; ++k) lin[n][BM + k] = (double)st.ugi[((size_t)t * (T - BM) + k) * NV + n];
+        }
+        double qmax = 0.0;
+        for (int j = 0; j < G; ++j) {
+            double wk[2][X];
+            for (int n = 0; n < 2; ++n)
+                for (int c = 0; c < X; ++c) {
+                    double acc = 0.0;
+                    for (int q = tb->colstart[c]; q < tb->colstart[c + 1]; ++q) {
+                        const int m = tb->colmodes[q];
+                        acc += lin[n][m] * (double)tb->gn[j][m];
+                    }
+                    wk[n][c] = acc;
+                }
+            for (int i = 0; i < G; ++i) {
+                double u0 = 0.0, u1 = 0.0;
+                for (int c = 0; c < X; ++c) {
+                    u0 += wk[0][c] * (double)tb->gx[i][c];
+                    u1 += wk[1][c] * (double)tb->gx[i][c];
+                }
+                const double q = u0 * u0 + u1 * u1;
+                qmax = (q > qmax ? q : qmax);
+            }
+        }
+        hmax = sqrt(hmax);
+        const double h = 4. * jcb / (p1 * hmax);
+        hmax = hmax / p1;
+        if (!(h > 0.0) || isnan(qmax)) { atomicAdd(err, 1); return; }
+        const double nu = ph.mu / ph.rho;
+        double gam = 3.0 * qmax + (0.5 * hmax * ph.bd0 + 2. * nu / hmax) * (0.5 * hmax * ph.bd0 + 2. * nu / hmax);
+        if (ph.mu + ph.bd0 == 0.0) gam = (gam > 0.1 ? gam : 0.1);
+        const double q = sqrt(qmax);
+        const double lam1 = q + sqrt(qmax + gam);
+        const double tau0 = ph.adis * h / (jcb * sqrt(gam));
+        st.tau[t * NV + 0] = (R)tau0;
+        st.tau[t * NV + 1] = (R)0;
+        st.tau[t * NV + 2] = (R)(qmax * tau0);
+        jcb *= 2. * nu * (1. / (hmax * hmax) + 1. / (h * h)) + 3 * lam1 / h;
+        tp[0] = ph.rho * jcb;
+        tp[1] = ph.rho * jcb;
+        tp[2] = jcb / gam;
+    }
+    for (int n = 0; n < NV; ++n) st.tprcn[t * NV + n] = (R)tp[n];
+    for (int i = 0; i < 3; ++i) {
+        for (int n = 0; n < NV; ++n) atomic_add(&st.vprcn[v[i] * NV + n], (R)tp[n]);
+        if (SM > 0) {
+            const int sd = mesh.tri_seg[3 * t + i];
+            for (int n = 0; n < NV; ++n) atomic_add(&st.sprcn[sd * NV + n], (R)tp[n]);
+        }
+    }
+}
+
+// res.{v,s} += res_r.{v,s} (nstage.cpp:76-82) for callers of the stand-alone rsdl
+template <typename R>
+__global__ void k_rsdl_fold(int n1, int n2, R *resv, const R *rrv, R *ress, const R *rrs) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n1) resv[k] += rrv[k];
+    else if (k < n1 + n2) ress[k - n1] += rrs[k - n1];
+}
+
+template <typename R>
+__global__ void k_prcn_invert(int nv_len, int ns_len, R *vprcn, R *sprcn, R vdiag) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nv_len) vprcn[k] = (R)1.0 / (vdiag * vprcn[k]);
+    else if (k < nv_len + ns_len) sprcn[k - nv_len] = (R)1.0 / sprcn[k - nv_len];
+}
+
+// Sum of squares and max |.| of a vector, block partials into out[2*blockIdx]
+template <typename R>
+__global__ void k_norm_partial(const R *a, size_t n, double *out) {
+    double s = 0.0, mx = 0.0;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const double v = (double)a[k];
+        s += v * v;
+        const double av = fabs(v);
+        mx = av > mx ? av : mx;
+    }
+    __shared__ double ss[32], sx[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        const double b = __shfl_xor_sync(0xffffffffu, mx, o);
+        mx = b > mx ? b : mx;
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { ss[w] = s; sx[w] = mx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a2 = 0.0, m2 = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+            a2 += ss[q];
+            m2 = sx[q] > m2 ? sx[q] : m2;
+        }
+        out[2 * blockIdx.x] = a2;
+        out[2 * blockIdx.x + 1] = m2;
+    }
+}
+
+// History slot bookkeeping for hp_gpu_iterate: maxres of iteration *it goes to
+// hist[*it], then *it advances (all on the device, so one captured graph replays).
+__global__ void k_hist_advance(unsigned long long *slot, double *hist, int *it, int NV, int cap) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double mx = 0.0;
+        for (int n = 0; n < NV; ++n) {
+            const double v = __longlong_as_double((long long)slot[n]);
+            mx = v > mx ? v : mx;
+            slot[n] = 0ull;
+        }
+        const int k = *it;
+        if (k < cap) hist[k] = mx;
+        *it = k + 1;
+    }
+}
+
+}  // namespace hpb

@@ -1,0 +1,137 @@
+"""Triangle meshes in the reference's array form (tri_mesh/tri_mesh.h:46-98).
+
+* ``square_mesh(n)``: [0,1]^2 split into n x n squares, each cut into two
+  counter-clockwise right triangles along the diagonal from the square's
+  upper-left to its lower-right corner -- the triangulation of the reference's
+  Testing/tri_hp/ins/Spatial Accuracy/Inputs/square<k>.grd meshes
+  (square7.grd = 64 x 64 squares = 8,192 triangles).
+* ``read_grd(path)``: the reference's .grd text format (tri_mesh/input.cpp:504-600).
+* ``createsegtri``: segment/triangle connectivity with the reference's
+  conventions (tri_mesh/setup.cpp:76-145): tri.seg(j) is the side opposite
+  tri.pnt(j), tri.sgn(j) = +1 when the segment runs counter-clockwise for the
+  triangle, seg.tri(0) is that triangle, seg.tri(1) the other one (-1 on the
+  boundary). Segments are numbered in order of first appearance.
+"""
+import numpy as np
+
+
+class Mesh:
+    def __init__(self, pnts, tri_pnt, seg_pnt=None):
+        self.pnts = np.ascontiguousarray(pnts, dtype=np.float64)
+        self.tri_pnt = np.ascontiguousarray(tri_pnt, dtype=np.int32)
+        self.npnt = len(self.pnts)
+        self.ntri = len(self.tri_pnt)
+        createsegtri(self, seg_pnt)
+
+    def boundary_segments(self):
+        return np.nonzero(self.seg_tri[:, 1] < 0)[0].astype(np.int32)
+
+    def area2(self):
+        """2 x triangle area (tri_mesh/tprims.cpp:66-80)."""
+        p = self.pnts[self.tri_pnt]
+        dx1 = p[:, 0, 0] - p[:, 2, 0]
+        dy1 = p[:, 0, 1] - p[:, 2, 1]
+        dx2 = p[:, 1, 0] - p[:, 0, 0]
+        dy2 = p[:, 1, 1] - p[:, 0, 1]
+        return dx1 * dy2 - dy1 * dx2
+
+
+def createsegtri(m, seg_pnt=None):
+    """Builds seg_pnt/seg_tri and tri_seg/tri_sgn (tri_mesh/setup.cpp:76-145).
+
+    With seg_pnt given (a mesh file's segment list) the file's segment numbering
+    and orientation are kept, as the reference does; otherwise segments are
+    created in order of first appearance, oriented counter-clockwise for the
+    first triangle that lists them.
+    """
+    t = m.tri_pnt
+    nt = m.ntri
+    # side j of a triangle runs from pnt((j+1)%3) to pnt((j+2)%3)
+    a = np.stack([t[:, 1], t[:, 2], t[:, 0]], axis=1).reshape(-1)
+    b = np.stack([t[:, 2], t[:, 0], t[:, 1]], axis=1).reshape(-1)
+    lo = np.minimum(a, b).astype(np.int64)
+    hi = np.maximum(a, b).astype(np.int64)
+    key = lo * (m.npnt + 1) + hi
+    if seg_pnt is None:
+        ukey, first, inv = np.unique(key, return_index=True, return_inverse=True)
+        order = np.argsort(first, kind="stable")  # number segments by first appearance
+        rank = np.empty_like(order)
+        rank[order] = np.arange(len(order))
+        sid = rank[inv]
+        fo = first[order]
+        seg_pnt = np.stack([a[fo], b[fo]], axis=1)
+    else:
+        seg_pnt = np.asarray(seg_pnt, dtype=np.int64)
+        skey = np.minimum(seg_pnt[:, 0], seg_pnt[:, 1]) * (m.npnt + 1) + np.maximum(seg_pnt[:, 0], seg_pnt[:, 1])
+        srt = np.argsort(skey)
+        pos = np.searchsorted(skey[srt], key)
+        if np.any(pos >= len(srt)) or np.any(skey[srt][np.minimum(pos, len(srt) - 1)] != key):
+            raise ValueError("triangle side without a matching segment")
+        sid = srt[pos]
+    nseg = len(seg_pnt)
+    sgn = np.where(seg_pnt[sid, 0] == a, 1, -1)
+    seg_tri = -np.ones((nseg, 2), dtype=np.int64)
+    tri_of_side = np.repeat(np.arange(nt), 3)
+    slot = np.where(sgn > 0, 0, 1)
+    if np.any(np.bincount(sid * 2 + slot, minlength=2 * nseg) > 1):
+        raise ValueError("non-manifold or inconsistently oriented mesh")
+    seg_tri[sid, slot] = tri_of_side
+    m.nseg = nseg
+    m.seg_pnt = np.ascontiguousarray(seg_pnt, dtype=np.int32)
+    m.seg_tri = np.ascontiguousarray(seg_tri, dtype=np.int32)
+    m.tri_seg = np.ascontiguousarray(sid.reshape(nt, 3), dtype=np.int32)
+    m.tri_sgn = np.ascontiguousarray(sgn.reshape(nt, 3), dtype=np.int32)
+    # a boundary segment must be counter-clockwise for its triangle (outward normal
+    # to its right, as hp_edge_bdry::element_rsdl assumes)
+    bnd = m.seg_tri[:, 0] < 0
+    if np.any(bnd):
+        raise ValueError("boundary segment oriented clockwise for its triangle")
+    return m
+
+
+def square_mesh(n, x0=0.0, x1=1.0, y0=0.0, y1=1.0):
+    """n x n squares, two counter-clockwise triangles each (diagonal upper-left to lower-right)."""
+    xs = np.linspace(x0, x1, n + 1)
+    ys = np.linspace(y0, y1, n + 1)
+    X, Y = np.meshgrid(xs, ys)  # [j][i]
+    pnts = np.stack([X.ravel(), Y.ravel()], axis=1)
+    i = np.arange(n)
+    I, J = np.meshgrid(i, i)
+    I = I.ravel()
+    J = J.ravel()
+    va = J * (n + 1) + I
+    vb = va + 1
+    vd = va + (n + 1)
+    vc = vd + 1
+    t1 = np.stack([va, vb, vd], axis=1)
+    t2 = np.stack([vb, vc, vd], axis=1)
+    tri = np.stack([t1, t2], axis=1).reshape(-1, 3)
+    return Mesh(pnts, tri)
+
+
+def read_grd(path):
+    """Reads the reference's .grd format: header 'nvrtx: N nside: S ntri: T', then
+    N vertex lines 'k: x y', S side lines 'k: p0 p1', T triangle lines 'k: a b c'
+    (tri_mesh/input.cpp:504-600). Boundary groups are returned as
+    {idnum: [segment indices]}."""
+    with open(path) as f:
+        lines = f.read().split("\n")
+    hdr = lines[0].replace(":", " ").split()
+    nv, ns, nt = int(hdr[1]), int(hdr[3]), int(hdr[5])
+    pts = np.array([[float(x) for x in l.split(":")[1].split()[:2]] for l in lines[1:1 + nv]])
+    segs = np.array([[int(x) for x in l.split(":")[1].split()[:2]] for l in lines[1 + nv:1 + nv + ns]])
+    tris = np.array([[int(x) for x in l.split(":")[1].split()[:3]] for l in lines[1 + nv + ns:1 + nv + ns + nt]])
+    groups = {}
+    k = 1 + nv + ns + nt
+    if k < len(lines) and lines[k].startswith("nsbd"):
+        nsbd = int(lines[k].split(":")[1])
+        k += 1
+        for _ in range(nsbd):
+            idnum = int(lines[k].split(":")[1])
+            num = int(lines[k + 1].split(":")[1])
+            ids = [int(l.split(":")[1].split()[0]) for l in lines[k + 2:k + 2 + num]]
+            groups.setdefault(idnum, []).extend(ids)
+            k += 2 + num
+    m = Mesh(pts, tris, seg_pnt=segs)
+    m.groups = groups
+    return m

@@ -1,0 +1,294 @@
+"""Problem set-up around the GPU path, mirroring the reference's tri_hp
+initialisation (tri_hp/allocate.cpp, ins/allocate.cpp, cd/allocate.cpp,
+tobasis.cpp, hp_boundary setvalues) for the workloads this library runs.
+
+A Problem owns the numpy arrays behind an hp_mesh_desc, the basis tables of
+its p, the physics constants and the initial state. ``Problem.gpu()`` opens a
+device context (tri_hp_gpu in the reference's terms) through the C-ABI.
+"""
+import ctypes
+import numpy as np
+
+from . import _lib as L
+from .mesh import square_mesh
+
+# Multistage defaults (tri_mesh/blocks.cpp:1124-1148) and CFL per log2p (tri_hp/allocate.cpp:275)
+ALPHA_DFLT = (0.25, 1.0 / 6.0, 0.375, 0.5, 1.0)
+BETA_DFLT = (1.0, 0.0, 5.0 / 9.0, 0.0, 4.0 / 9.0)
+CFL_DFLT = {0: 2.5, 1: 1.5, 2: 1.0, 3: 0.5}
+
+
+def default_cfl(p):
+    """hp_gbl->cfl(log2p) default; p that is not a power of two takes the next lower entry."""
+    log2p = {1: 0, 2: 1, 3: 1, 4: 2, 5: 2, 6: 2, 7: 2, 8: 3}[p]
+    return CFL_DFLT[log2p]
+
+
+_TABLE_CACHE = {}
+
+
+def basis_tables(p):
+    """hp_basis_tables of tri_basis<p,0> built by the library (hp_basis_build)."""
+    if p not in _TABLE_CACHE:
+        t = L.BasisTables()
+        rc = L.lib().hp_basis_build(p, ctypes.byref(t))
+        if rc != 0:
+            raise RuntimeError(f"hp_basis_build({p}) returned {rc}")
+        _TABLE_CACHE[p] = t
+    return _TABLE_CACHE[p]
+
+
+def splitmix64_uniform(seed, n):
+    """n doubles in [-1, 1) from the splitmix64 sequence started at `seed`."""
+    mask = np.uint64(0xFFFFFFFFFFFFFFFF)
+    with np.errstate(over="ignore"):
+        k = np.arange(1, n + 1, dtype=np.uint64)
+        z = (np.uint64(seed) + k * np.uint64(0x9E3779B97F4A7C15)) & mask
+        z = ((z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & mask
+        z = ((z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & mask
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    return 2.0 * u - 1.0
+
+
+class Problem:
+    def __init__(self, mesh, p, physics, *, rho=1.0, mu=0.01, rhocv=1.0, kcond=1e-3, ax=1.0, ay=0.5, src=0.0,
+                 adis=1.0, nstage=5, alpha=ALPHA_DFLT, beta=BETA_DFLT, cfl=None, field=None, bc=None):
+        self.mesh = mesh
+        self.p = p
+        self.physics = physics
+        self.NV = 3 if physics == L.HP_PHYS_INS else 1
+        self.tab = basis_tables(p)
+        self.sm = self.tab.sm
+        self.im = self.tab.im
+        self.field = field
+        ph = L.PhysParams()
+        ph.physics = physics
+        ph.nstage = nstage
+        for k in range(8):
+            ph.alpha[k] = alpha[k] if k < nstage else 1.0
+            ph.beta[k] = beta[k] if k < nstage else 1.0
+        ph.cfl = default_cfl(p) if cfl is None else cfl
+        ph.bd0 = 0.0
+        ph.adis = adis
+        ph.rho, ph.mu = rho, mu
+        ph.rhocv, ph.kcond, ph.ax, ph.ay, ph.src = rhocv, kcond, ax, ay, src
+        self.phys = ph
+        self._set_bc(bc or [])
+        self._build_desc()
+        self.ugv = np.zeros((mesh.npnt, self.NV))
+        self.ugs = np.zeros((mesh.nseg, self.sm, self.NV))
+        self.ugi = np.zeros((mesh.ntri, self.im, self.NV))
+
+    # --- boundary conditions -------------------------------------------------
+    def _set_bc(self, bc):
+        """bc: list of (segment-index array, kind) with kind = essential mask | flux form."""
+        bsegs, kinds = [], []
+        for segs, kind in bc:
+            segs = np.asarray(segs, dtype=np.int32)
+            bsegs.append(segs)
+            kinds.append(np.full(len(segs), kind, dtype=np.int32))
+        self.bseg = np.ascontiguousarray(np.concatenate(bsegs) if bsegs else np.zeros(0, np.int32))
+        self.bkind = np.ascontiguousarray(np.concatenate(kinds) if kinds else np.zeros(0, np.int32))
+        G = self.tab.gpx
+        self.bpibc = np.zeros((max(len(self.bseg), 1), G))
+        if self.physics == L.HP_PHYS_INS and self.field is not None and len(self.bseg):
+            # ibc->f(NV-1, x) at the side Gauss points of each boundary edge
+            gx1 = np.array([self.tab.gx[k][1] for k in range(G)])
+            gx2 = np.array([self.tab.gx[k][2] for k in range(G)])
+            v0 = self.mesh.seg_pnt[self.bseg, 0]
+            v1 = self.mesh.seg_pnt[self.bseg, 1]
+            X = np.outer(self.mesh.pnts[v0, 0], gx1) + np.outer(self.mesh.pnts[v1, 0], gx2)
+            Y = np.outer(self.mesh.pnts[v0, 1], gx1) + np.outer(self.mesh.pnts[v1, 1], gx2)
+            self.bpibc[: len(self.bseg)] = self.eval_field(2, X, Y)
+        self.bpibc = np.ascontiguousarray(self.bpibc)
+
+    def eval_field(self, n, X, Y):
+        f = self.field
+        out = np.empty_like(X, dtype=np.float64)
+        flat_x, flat_y, flat_o = X.ravel(), Y.ravel(), out.reshape(-1)
+        v = ctypes.c_double()
+        for k in range(flat_x.size):
+            L.lib().hp_field_eval(ctypes.byref(f), n, float(flat_x[k]), float(flat_y[k]), ctypes.byref(v))
+            flat_o[k] = v.value
+        return out
+
+    def _build_desc(self):
+        m = self.mesh
+        d = L.MeshDesc()
+        d.npnt, d.nseg, d.ntri = m.npnt, m.nseg, m.ntri
+        d.pnts = L.dptr(m.pnts)
+        d.seg_pnt, d.seg_tri = L.iptr(m.seg_pnt), L.iptr(m.seg_tri)
+        d.tri_pnt, d.tri_seg, d.tri_sgn = L.iptr(m.tri_pnt), L.iptr(m.tri_seg), L.iptr(m.tri_sgn)
+        d.nbseg = len(self.bseg)
+        d.bseg = L.iptr(self.bseg)
+        d.bseg_kind = L.iptr(self.bkind)
+        d.bseg_pibc = L.dptr(self.bpibc)
+        self.desc = d
+
+    # --- initial state -------------------------------------------------------
+    def tobasis(self, noise=0.0, seed=0):
+        """tri_hp::tobasis of self.field, optional seeded U[-1,1) noise of amplitude
+        `noise` on every v/s/i coefficient, then the essential boundary values are
+        set again (hp_edge_bdry::setvalues), as a time step's tadvance does."""
+        lib = L.lib()
+        rc = lib.hp_tobasis(ctypes.byref(self.tab), ctypes.byref(self.desc), self.NV, ctypes.byref(self.field),
+                            L.ptr(self.ugv), L.ptr(self.ugs), L.ptr(self.ugi))
+        L.check(rc, "hp_tobasis")
+        if noise:
+            nv, ns, ni = self.ugv.size, self.ugs.size, self.ugi.size
+            r = splitmix64_uniform(seed, nv + ns + ni) * noise
+            self.ugv += r[:nv].reshape(self.ugv.shape)
+            self.ugs += r[nv:nv + ns].reshape(self.ugs.shape)
+            self.ugi += r[nv + ns:].reshape(self.ugi.shape)
+        L.check(lib.hp_setvalues(ctypes.byref(self.tab), ctypes.byref(self.desc), self.NV, ctypes.byref(self.field),
+                                 L.ptr(self.ugv), L.ptr(self.ugs)), "hp_setvalues")
+        return self
+
+    def l2error(self, ugv=None, ugs=None, ugi=None):
+        ugv = self.ugv if ugv is None else ugv
+        ugs = self.ugs if ugs is None else ugs
+        ugi = self.ugi if ugi is None else ugi
+        l2 = np.zeros(self.NV)
+        li = np.zeros(self.NV)
+        L.check(L.lib().hp_l2error(ctypes.byref(self.tab), ctypes.byref(self.desc), self.NV, ctypes.byref(self.field),
+                                   L.ptr(np.ascontiguousarray(ugv)), L.ptr(np.ascontiguousarray(ugs)),
+                                   L.ptr(np.ascontiguousarray(ugi)), L.ptr(l2), L.ptr(li)), "hp_l2error")
+        return l2, li
+
+    @property
+    def ndof(self):
+        return self.NV * (self.mesh.npnt + self.mesh.nseg * self.sm + self.mesh.ntri * self.im)
+
+    def gpu(self, device=0, stream=None):
+        return GPULevel(self, device, stream)
+
+
+class GPULevel:
+    """One device context (hp_gpu_ctx) for a Problem: the reference's
+    tri_hp::{rsdl, setup_preconditioner, minvrt, update, maxres} through the C-ABI."""
+
+    def __init__(self, prob, device=0, stream=None):
+        self.prob = prob
+        self.lib = L.lib()
+        h = ctypes.c_void_p()
+        rc = self.lib.hp_gpu_create(ctypes.byref(prob.desc), ctypes.byref(prob.tab), ctypes.byref(prob.phys),
+                                    device, stream, ctypes.byref(h))
+        L.check(rc, "hp_gpu_create")
+        self.h = h
+        self.upload(prob.ugv, prob.ugs, prob.ugi)
+
+    def close(self):
+        if self.h:
+            self.lib.hp_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, v, s, i):
+        v, s, i = (np.ascontiguousarray(a, dtype=np.float64) for a in (v, s, i))
+        L.check(self.lib.hp_gpu_upload_state(self.h, L.ptr(v), L.ptr(s), L.ptr(i)), "upload")
+
+    def state(self):
+        p = self.prob
+        v = np.zeros_like(p.ugv); s = np.zeros_like(p.ugs); i = np.zeros_like(p.ugi)
+        L.check(self.lib.hp_gpu_download_state(self.h, L.ptr(v), L.ptr(s), L.ptr(i)), "download_state")
+        return v, s, i
+
+    def residual(self):
+        p = self.prob
+        v = np.zeros_like(p.ugv); s = np.zeros_like(p.ugs); i = np.zeros_like(p.ugi)
+        L.check(self.lib.hp_gpu_download_residual(self.h, L.ptr(v), L.ptr(s), L.ptr(i)), "download_residual")
+        return v, s, i
+
+    def prcn(self):
+        p = self.prob
+        m = p.mesh
+        vp = np.zeros((m.npnt, p.NV)); sp = np.zeros((m.nseg, p.NV))
+        tp = np.zeros((m.ntri, p.NV)); tau = np.zeros((m.ntri, p.NV))
+        L.check(self.lib.hp_gpu_download_prcn(self.h, L.ptr(vp), L.ptr(sp), L.ptr(tp), L.ptr(tau)), "download_prcn")
+        return vp, sp, tp, tau
+
+    def setup_preconditioner(self):
+        return L.check(self.lib.hp_gpu_setup_preconditioner(self.h), "setup_preconditioner")
+
+    def rsdl(self, stage):
+        L.check(self.lib.hp_gpu_rsdl(self.h, stage), "rsdl")
+
+    def minvrt(self):
+        L.check(self.lib.hp_gpu_minvrt(self.h), "minvrt")
+
+    def update(self):
+        L.check(self.lib.hp_gpu_update(self.h), "update")
+
+    def iterate(self, iters, prcn_interval=0):
+        hist = np.zeros(max(iters, 1))
+        L.check(self.lib.hp_gpu_iterate(self.h, iters, prcn_interval, L.ptr(hist)), "iterate")
+        return hist[:iters]
+
+    def maxres(self):
+        out = np.zeros(self.prob.NV)
+        mx = ctypes.c_double()
+        L.check(self.lib.hp_gpu_maxres(self.h, L.ptr(out), ctypes.byref(mx)), "maxres")
+        return mx.value, out
+
+    def resnorm(self):
+        l2 = ctypes.c_double(); li = ctypes.c_double()
+        L.check(self.lib.hp_gpu_resnorm(self.h, ctypes.byref(l2), ctypes.byref(li)), "resnorm")
+        return l2.value, li.value
+
+
+# --- workloads ---------------------------------------------------------------
+
+def _edges_where(mesh, pred):
+    b = mesh.boundary_segments()
+    mid = 0.5 * (mesh.pnts[mesh.seg_pnt[b, 0]] + mesh.pnts[mesh.seg_pnt[b, 1]])
+    return b[pred(mid[:, 0], mid[:, 1])]
+
+
+def kovasznay_ins(n=64, p=4, re=100.0, noise=1e-3, seed=20261204, **kw):
+    """2D incompressible Navier-Stokes, Kovasznay flow at Re on an n x n split-square
+    mesh of the unit square; inflow (velocity essential) on left/top/bottom,
+    outflow (generic flux with the analytic pressure) on the right; rho = 1, mu = 1/Re."""
+    mesh = square_mesh(n)
+    field = L.Field(L.HP_FIELD_KOVASZNAY, (ctypes.c_double * 4)(re, 0, 0, 0))
+    eps = 1e-12
+    inflow = _edges_where(mesh, lambda x, y: (x < eps) | (y < eps) | (y > 1 - eps))
+    outflow = _edges_where(mesh, lambda x, y: (x > 1 - eps) & (y > eps) & (y < 1 - eps))
+    bc = [(inflow, 0b011 | L.HP_BC_FLUX_INS_GENERIC), (outflow, L.HP_BC_FLUX_INS_GENERIC)]
+    prob = Problem(mesh, p, L.HP_PHYS_INS, rho=1.0, mu=1.0 / re, field=field, bc=bc, **kw)
+    return prob.tobasis(noise=noise, seed=seed)
+
+
+def lid_cavity_ins(n=64, p=4, re=400.0, noise=1e-3, seed=20261206, **kw):
+    """ins lid-driven cavity: u = 1 on the lid, zero on the other walls, velocity essential everywhere."""
+    mesh = square_mesh(n)
+    field = L.Field(L.HP_FIELD_LID, (ctypes.c_double * 4)(0, 0, 0, 0))
+    walls = mesh.boundary_segments()
+    bc = [(walls, 0b011 | L.HP_BC_FLUX_INS_GENERIC)]
+    prob = Problem(mesh, p, L.HP_PHYS_INS, rho=1.0, mu=1.0 / re, field=field, bc=bc, **kw)
+    return prob.tobasis(noise=noise, seed=seed)
+
+
+def cd_sinsin(mesh=None, n=64, p=4, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205, **kw):
+    """Scalar convection-diffusion, velocity (ax, ay), diffusivity kcond, Dirichlet data
+    sin(pi x) sin(pi y) on every boundary edge, initial state the same field plus noise."""
+    mesh = mesh if mesh is not None else square_mesh(n)
+    field = L.Field(L.HP_FIELD_SINSIN, (ctypes.c_double * 4)(1.0, 0, 0, 0))
+    bc = [(mesh.boundary_segments(), 0b1)]
+    prob = Problem(mesh, p, L.HP_PHYS_CD, rhocv=1.0, kcond=kcond, ax=ax, ay=ay, field=field, bc=bc, **kw)
+    return prob.tobasis(noise=noise, seed=seed)
+
+
+def cd_quadratic(n=4, p=2, noise=1e-2, seed=7, **kw):
+    """Exactness case of Testing/tri_hp/conv-diff/Correctness: u = -(x-8)^2, nu = 1,
+    no convection, source 2, Dirichlet everywhere; the p >= 2 discrete solution is exact."""
+    mesh = square_mesh(n)
+    field = L.Field(L.HP_FIELD_QUADX, (ctypes.c_double * 4)(-1.0, 8.0, 0, 0))
+    bc = [(mesh.boundary_segments(), 0b1)]
+    prob = Problem(mesh, p, L.HP_PHYS_CD, rhocv=1.0, kcond=1.0, ax=0.0, ay=0.0, src=2.0, field=field, bc=bc, **kw)
+    return prob.tobasis(noise=noise, seed=seed)

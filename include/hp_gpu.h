@@ -1,0 +1,191 @@
+/*
+ * hp_gpu.h — C-ABI of the B200 element-residual / multistage-smoothing library.
+ *
+ * The library replaces the hot path of hp-multiphysics' 2D solver behind the
+ * same seams the reference exposes through its C++ virtual interfaces:
+ *
+ *   multigrid_interface (tri_mesh/block.h:213-267), implemented by tri_hp
+ *   (tri_hp/tri_hp.h:207-248): setup_preconditioner(), rsdl(), update(),
+ *   mg_restrict(), mg_prolongate(), maxres().
+ *   Physics plug-ins tri_hp_ins / tri_hp_cd: element_rsdl(), setup_preconditioner().
+ *   Basis: tri_basis_interface (tri_basis/tri_basis.h:32-211).
+ *
+ * A reference-side subclass (tri_hp_gpu : tri_hp_ins / tri_hp_cd) overrides
+ * those virtuals and forwards to the calls below, so block::cycle
+ * (tri_mesh/blocks.cpp:1267-1348) stays unchanged. Plain pointers and sizes
+ * only; every call returns an int status: 0 = ok, > 0 = count of bad elements
+ * (setup_preconditioner), < 0 = error (see HP_E*). Host arrays are caller-owned
+ * and copied; device memory is owned by the context. Calls on one context are
+ * stream-ordered on the context's stream; the only host synchronisations are in
+ * the calls that return numbers to the host (maxres, norms, downloads, error
+ * counts).
+ *
+ * Array layouts follow the reference's blitz arrays (row-major):
+ *   ug.v / res.v  [npnt][NV]         (tri_hp.h:71-75)
+ *   ug.s / res.s  [nseg][sm][NV]
+ *   ug.i / res.i  [ntri][im][NV]
+ *   vprcn [npnt][NV], sprcn [nseg][NV], tprcn [ntri][NV]  (tri_hp.h:139-141)
+ */
+#ifndef HP_GPU_H
+#define HP_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HP_MAXP 8
+#define HP_MXGP (HP_MAXP + 1)                      /* Gauss points per direction, p+1 */
+#define HP_MXX (HP_MAXP + 2)                       /* x-direction mode count, p+2 */
+#define HP_MXTM ((HP_MAXP + 1) * (HP_MAXP + 2) / 2) /* total modes */
+#define HP_MXBM (3 * HP_MAXP)                      /* boundary (vertex+side) modes */
+#define HP_MXSM (HP_MAXP - 1)                      /* modes per side */
+#define HP_MXIM ((HP_MAXP - 1) * (HP_MAXP - 2) / 2) /* interior modes */
+
+#define HP_OK 0
+#define HP_EINVAL -1   /* bad argument / size beyond a stated limit */
+#define HP_ECUDA -2    /* a CUDA runtime call failed */
+#define HP_ENOMEM -3   /* device allocation failed */
+#define HP_ENOTSUP -4  /* configuration not built into this library */
+#define HP_ESTATE -5   /* call order violated (e.g. update before setup_preconditioner) */
+
+/* Basis tables of tri_basis<p,0> (tri_basis/tri_basis.h:218-291), stored with
+ * the reference accessors' index order. One instance per polynomial degree. */
+typedef struct hp_basis_tables {
+    int p, sm, im, tm, bm, nmodx, gpx, gpn, ibwth, sbwth;
+    double gx[HP_MXGP][HP_MXX], dgx[HP_MXGP][HP_MXX];
+    double wtx[HP_MXGP], xp[HP_MXGP], x0[HP_MXGP];
+    double gxwtx[HP_MXX][HP_MXGP], dgxwtx[HP_MXX][HP_MXGP];
+    double dltx[HP_MXGP], dltx1[HP_MXGP][HP_MXGP];
+    double gn[HP_MXGP][HP_MXTM], dgn[HP_MXGP][HP_MXTM];
+    double wtn[HP_MXGP], np[HP_MXGP], n0[HP_MXGP];
+    double gnwtn[HP_MXTM][HP_MXGP], gnwtnn0[HP_MXTM][HP_MXGP], dgnwtn[HP_MXTM][HP_MXGP];
+    double dltn[HP_MXGP], dltn1[HP_MXGP][HP_MXGP], dltn2[HP_MXGP][HP_MXGP];
+    double norm[HP_MXTM];
+    /* lumped-mass inversion (tri_basis/initialize.cpp:590-1082) */
+    double sfmv[2][HP_MXSM], ifmb[HP_MXBM][HP_MXIM], vdiag, vfms[3][HP_MXSM], sdiag[HP_MXSM];
+    double sfms[HP_MXSM][HP_MXSM][3], bfmi[HP_MXBM][HP_MXIM], idiag[HP_MXIM][2];
+    /* 1D side mass inversion (tri_basis/initialize.cpp:1085-1232) */
+    double sfmv1d[2][HP_MXSM], vdiag1d, vfms1d[2][HP_MXSM], sdiag1d[HP_MXSM][3];
+} hp_basis_tables;
+
+/* Builds the tables of tri_basis<p,0>, 1 <= p <= HP_MAXP.
+ * Replaces tri_basis<_p,ep>::initialize (tri_basis/initialize.cpp:19-35):
+ * initialize_values (:161-455), lumpinv (:590-1082), lumpinv1d (:1085-1232).
+ * Returns HP_EINVAL for p outside [1, HP_MAXP], > 0 if a factorisation failed. */
+int hp_basis_build(int p, hp_basis_tables *out);
+
+/* Boundary-edge kinds. Bits 0..7: essential (Dirichlet) variable mask, as the
+ * reference's essential_indices (tri_hp/hp_boundary.h:119); bits 8..11: flux
+ * form of hp_edge_bdry::rsdl (tri_hp/hp_boundary.cpp:1028-1049). */
+#define HP_BC_ESSENTIAL(n) (1 << (n))
+#define HP_BC_FLUX_NONE (0 << 8)        /* all-essential edge: flux identically zero */
+#define HP_BC_FLUX_INS_GENERIC (1 << 8) /* bdry_ins::generic::flux (ins/bdry_ins.h:35-50) */
+#define HP_BC_FLUX_MASK (0xF << 8)
+
+/* Mesh, as tri_mesh's pnts / seg / tri arrays (tri_mesh/tri_mesh.h:46-98).
+ * tri.seg(j) is the side opposite tri.pnt(j); tri.sgn(j) = +1 when the segment
+ * runs counter-clockwise for that triangle (tri_mesh/setup.cpp:76-145).
+ * seg.tri(k) = -1 on the domain boundary. Boundary edges: the segments of every
+ * hp_edge_bdry, each with its kind and, for HP_BC_FLUX_INS_GENERIC, the value of
+ * the boundary-condition pressure ibc->f(NV-1, x) at the edge's gpx Gauss points
+ * (bseg_pibc [nbseg][gpx], may be NULL otherwise). */
+typedef struct hp_mesh_desc {
+    int npnt, nseg, ntri;
+    const double *pnts;   /* [npnt][2] */
+    const int *seg_pnt;   /* [nseg][2] */
+    const int *seg_tri;   /* [nseg][2] */
+    const int *tri_pnt;   /* [ntri][3] */
+    const int *tri_seg;   /* [ntri][3] */
+    const int *tri_sgn;   /* [ntri][3] */
+    int nbseg;
+    const int *bseg;      /* [nbseg] segment index */
+    const int *bseg_kind; /* [nbseg] HP_BC_* */
+    const double *bseg_pibc; /* [nbseg][gpx] or NULL */
+} hp_mesh_desc;
+
+#define HP_PHYS_CD 0  /* tri_hp_cd  (tri_hp/cd/tri_hp_cd.h:16, CONST_A) NV=1 */
+#define HP_PHYS_INS 1 /* tri_hp_ins (tri_hp/ins/tri_hp_ins.h:16)          NV=3 */
+
+/* Physics and multistage constants (tri_mesh/blocks.cpp:1124-1148,
+ * tri_hp/allocate.cpp:264-276, ins/allocate.cpp:20-26, cd/allocate.cpp:25-62).
+ * Steady runs only: bd0 = 0 (dtinv = 0), so the mesh velocity and the unsteady
+ * sources are identically zero. */
+typedef struct hp_phys_params {
+    int physics;        /* HP_PHYS_CD | HP_PHYS_INS */
+    int nstage;         /* <= 7 */
+    double alpha[8];    /* alpha(stage), alpha(nstage) = 1 */
+    double beta[8];     /* beta(stage),  beta(nstage)  = 1 */
+    double cfl;         /* hp_gbl->cfl(log2p) of this level */
+    double bd0;         /* must be 0 (steady) */
+    double adis;        /* b0_dissipation */
+    double rho, mu;     /* ins */
+    double rhocv, kcond, ax, ay, src; /* cd: rho*cv, conductivity, constant velocity, constant source */
+} hp_phys_params;
+
+#define HP_PREC_FP64 0
+#define HP_PREC_FP32 1
+
+typedef struct hp_gpu_ctx hp_gpu_ctx;
+
+/* One context per (mesh, p) level. device < 0 selects the current device.
+ * stream == NULL creates a private non-blocking stream. */
+int hp_gpu_create(const hp_mesh_desc *mesh, const hp_basis_tables *basis, const hp_phys_params *phys,
+                  int device, void *stream, hp_gpu_ctx **out);
+int hp_gpu_destroy(hp_gpu_ctx *ctx);
+int hp_gpu_sizes(const hp_gpu_ctx *ctx, int *nv, int *sm, int *im); /* NV, sm, im of the level */
+
+/* State transfer (host <-> device). Layouts as above. */
+int hp_gpu_upload_state(hp_gpu_ctx *ctx, const double *ugv, const double *ugs, const double *ugi);
+int hp_gpu_download_state(hp_gpu_ctx *ctx, double *ugv, double *ugs, double *ugi);
+int hp_gpu_download_residual(hp_gpu_ctx *ctx, double *resv, double *ress, double *resi);
+int hp_gpu_download_prcn(hp_gpu_ctx *ctx, double *vprcn, double *sprcn, double *tprcn, double *tau);
+
+/* Device pointers of the state and residual (for callers that keep data on
+ * the GPU). Any output pointer may be NULL. */
+int hp_gpu_device_ptrs(hp_gpu_ctx *ctx, double **ugv, double **ugs, double **ugi, double **resv,
+                       double **ress, double **resi);
+
+/* tri_hp::rsdl(stage) (tri_hp/nstage.cpp:12-110): residual of the given stage,
+ * 0 <= stage <= nstage (stage == nstage: full residual, res_r reset). */
+int hp_gpu_rsdl(hp_gpu_ctx *ctx, int stage);
+
+/* tri_hp_{ins,cd}::setup_preconditioner + tri_hp::setup_preconditioner
+ * (ins/setup_preconditioner.cpp:9-221, cd/setup_preconditioner.cpp:6-97,
+ * setup_preconditioner.cpp:9-100). Returns the count of bad elements (> 0)
+ * exactly where the reference sets err (non-positive area, NaN velocity). */
+int hp_gpu_setup_preconditioner(hp_gpu_ctx *ctx);
+
+/* tri_hp::minvrt (tri_hp/setup_preconditioner.cpp:102-373) on the current
+ * residual, Dirichlet zeroing included. */
+int hp_gpu_minvrt(hp_gpu_ctx *ctx);
+
+/* tri_hp::update (tri_hp/nstage.cpp:256-427): nstage x (rsdl, minvrt,
+ * ug = ug0 - cfl*alpha*res). */
+int hp_gpu_update(hp_gpu_ctx *ctx);
+
+/* Runs `iters` calls of update() back to back (one CUDA graph per call), with
+ * setup_preconditioner() before every `prcn_interval`-th iteration (0 = only
+ * before the first). Writes tri_hp::maxres of every iteration to hist[iters]
+ * (may be NULL). */
+int hp_gpu_iterate(hp_gpu_ctx *ctx, int iters, int prcn_interval, double *hist);
+
+/* tri_hp::maxres (tri_hp/allocate.cpp:496-525): per-variable max over
+ * vertices of |res.v| as left by the last minvrt; out[NV], returns via *mx the
+ * max over variables. */
+int hp_gpu_maxres(hp_gpu_ctx *ctx, double *out, double *mx);
+
+/* Unpreconditioned residual norm over all modes: computes rsdl(nstage) and
+ * returns sqrt(sum res^2) and max |res| over every v/s/i coefficient. */
+int hp_gpu_resnorm(hp_gpu_ctx *ctx, double *l2, double *linf);
+
+/* Synchronises the context's stream and returns the first sticky error. */
+int hp_gpu_sync(hp_gpu_ctx *ctx);
+
+/* Last error text (thread-local), "" if none. */
+const char *hp_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HP_GPU_H */

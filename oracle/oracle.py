@@ -1,0 +1,137 @@
+"""ctypes access to the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this
+module. It loads oracle/_build/libhp_oracle.so (the C++ restatement in
+hp_oracle.cpp) and, when built, oracle/_ref/libtri_basis_ref.so (the
+reference's own tri_basis compiled here).
+"""
+import ctypes
+import os
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libhp_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libtri_basis_ref.so")
+_o = None
+_r = None
+
+
+def build():
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", HERE, "_build/libhp_oracle.so"])
+
+
+def lib():
+    global _o
+    if _o is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        o = ctypes.CDLL(ORACLE_SO)
+        P = ctypes.c_void_p
+        o.or_create.restype = P
+        o.or_create.argtypes = [P, P, P]
+        o.or_destroy.argtypes = [P]
+        for n in ("or_set_state", "or_get_state", "or_get_res"):
+            getattr(o, n).argtypes = [P, P, P, P]
+        o.or_get_prcn.argtypes = [P, P, P, P, P]
+        o.or_set_prcn.argtypes = [P, P, P, P, P]
+        o.or_rsdl.argtypes = [P, ctypes.c_int]
+        o.or_setup_preconditioner.argtypes = [P]
+        o.or_minvrt.argtypes = [P]
+        o.or_update.argtypes = [P]
+        o.or_maxres.argtypes = [P, P]
+        o.or_maxres.restype = ctypes.c_double
+        for n in ("or_basis_proj",):
+            getattr(o, n).argtypes = [P, P, P, P, P, ctypes.c_int]
+        o.or_basis_proj_val.argtypes = [P, P, P, ctypes.c_int]
+        o.or_basis_derivr.argtypes = [P, P, P, ctypes.c_int]
+        o.or_basis_derivs.argtypes = [P, P, P, ctypes.c_int]
+        o.or_basis_intgrt.argtypes = [P, P, P, ctypes.c_int]
+        o.or_basis_intgrtrs.argtypes = [P, P, P, P, ctypes.c_int]
+        o.or_basis_proj1d.argtypes = [P, P, P, P]
+        o.or_basis_intgrt1d.argtypes = [P, P, P]
+        o.or_dpbtrsnu2.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int]
+        _o = o
+    return _o
+
+
+def ref():
+    """The reference's own tri_basis (oracle/_ref), or None when it was not built."""
+    global _r
+    if _r is None:
+        if not os.path.exists(REF_SO):
+            return None
+        r = ctypes.CDLL(REF_SO)
+        P = ctypes.c_void_p
+        r.ref_tb_get.argtypes = [ctypes.c_int, ctypes.c_char_p, P]
+        r.ref_tb_sizes.argtypes = [ctypes.c_int, P]
+        r.ref_proj.argtypes = [ctypes.c_int, P, P, P, P, ctypes.c_int]
+        r.ref_proj_val.argtypes = [ctypes.c_int, P, P, ctypes.c_int]
+        r.ref_derivr.argtypes = [ctypes.c_int, P, P, ctypes.c_int]
+        r.ref_derivs.argtypes = [ctypes.c_int, P, P, ctypes.c_int]
+        r.ref_intgrt.argtypes = [ctypes.c_int, P, P, ctypes.c_int]
+        r.ref_intgrtrs.argtypes = [ctypes.c_int, P, P, P, ctypes.c_int]
+        r.ref_proj1d.argtypes = [ctypes.c_int, P, P, P]
+        r.ref_intgrt1d.argtypes = [ctypes.c_int, P, P]
+        _r = r
+    return _r
+
+
+def _p(a):
+    return None if a is None or a.size == 0 else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Oracle:
+    """CPU restatement of one tri_hp level (same inputs as the GPU context)."""
+
+    def __init__(self, prob):
+        self.prob = prob
+        self.o = lib()
+        self.h = self.o.or_create(ctypes.addressof(prob.desc), ctypes.addressof(prob.tab), ctypes.addressof(prob.phys))
+        self.set_state(prob.ugv, prob.ugs, prob.ugi)
+
+    def __del__(self):
+        try:
+            self.o.or_destroy(self.h)
+        except Exception:
+            pass
+
+    def set_state(self, v, s, i):
+        v, s, i = (np.ascontiguousarray(a, dtype=np.float64) for a in (v, s, i))
+        self.o.or_set_state(self.h, _p(v), _p(s), _p(i))
+
+    def state(self):
+        p = self.prob
+        v = np.zeros_like(p.ugv); s = np.zeros_like(p.ugs); i = np.zeros_like(p.ugi)
+        self.o.or_get_state(self.h, _p(v), _p(s), _p(i))
+        return v, s, i
+
+    def residual(self):
+        p = self.prob
+        v = np.zeros_like(p.ugv); s = np.zeros_like(p.ugs); i = np.zeros_like(p.ugi)
+        self.o.or_get_res(self.h, _p(v), _p(s), _p(i))
+        return v, s, i
+
+    def prcn(self):
+        p = self.prob
+        m = p.mesh
+        vp = np.zeros((m.npnt, p.NV)); sp = np.zeros((m.nseg, p.NV))
+        tp = np.zeros((m.ntri, p.NV)); tau = np.zeros((m.ntri, p.NV))
+        self.o.or_get_prcn(self.h, _p(vp), _p(sp), _p(tp), _p(tau))
+        return vp, sp, tp, tau
+
+    def setup_preconditioner(self):
+        return self.o.or_setup_preconditioner(self.h)
+
+    def rsdl(self, stage):
+        self.o.or_rsdl(self.h, stage)
+
+    def minvrt(self):
+        self.o.or_minvrt(self.h)
+
+    def update(self):
+        self.o.or_update(self.h)
+
+    def maxres(self):
+        out = np.zeros(self.prob.NV)
+        return self.o.or_maxres(self.h, _p(out)), out
