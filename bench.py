@@ -1,0 +1,307 @@
+#!/usr/bin/env python
+"""Benchmark of the tri_hp element-residual path on B200 (one process per GPU).
+
+Workload (N = 1): scalar convection-diffusion (tri_hp cd, CONST_A), velocity
+(1, 0.5), diffusivity 1e-3, p = 4, Dirichlet data sin(pi x) sin(pi y) on a
+317 x 317 split-square mesh of the unit square (200,978 triangles, 1.61 M
+DOF). Seeded synthetic state: the Dirichlet field projected onto the basis plus
+U[-1,1) * 1e-3 noise (splitmix64). A "step" is one full FP64 residual
+evaluation tri_hp::rsdl(nstage) over the whole mesh; `value` is rsdl GDoF/s
+(whole job, inputs resident in HBM, device time, L2 flushed between steps);
+`e2e` is the same metric through the C-ABI with host buffers (state upload from
+pinned memory + rsdl + residual download every step, wall clock).
+
+--gpus N > 1 runs N independent replicas of the same workload (the path does
+not shard across GPUs in this tier): value = sum over ranks.
+--impl reference times the CPU oracle (the C++ restatement of the reference's
+rsdl) on the host cores with the same metric.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hp-multiphysics_b200"))
+sys.path.insert(0, ROOT)
+
+N_MESH = 317
+P = 4
+METRIC = "rsdl GDoF/s (FP64 tri_hp::rsdl, cd p=4)"
+
+
+def workload_config():
+    return {
+        "workload": f"tri_hp cd rsdl(nstage), p={P}, {N_MESH}x{N_MESH} split-square mesh "
+                    f"({2 * N_MESH * N_MESH} triangles), velocity (1,0.5), kcond 1e-3",
+        "mesh": "structured split squares standing in for the seeded 200k-triangle Delaunay mesh",
+        "p": P, "physics": "cd", "ntri": 2 * N_MESH * N_MESH, "nstage": 5,
+        "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas",
+    }
+
+
+def flops_per_element(p, nv_pairs=1, nv=1, ndv=1):
+    """Loop-count FLOPs of one full-stage element residual of this library's
+    kernel (cd: one variable, projected with derivatives)."""
+    G, X, T = p + 1, p + 2, (p + 1) * (p + 2) // 2
+    nqw = 2 * ndv + (nv - ndv)
+    proj1 = 2 * nqw * G * T
+    proj2 = G * G * (7 * X * ndv + 2 * X * (nv - ndv))
+    intg = 2 * (6 * nv_pairs * X * G * G + 4 * nv * T * G)
+    deriv = 9 * nv * G ** 3
+    point = 40 * G * G
+    return proj1 + proj2 + intg + deriv + point
+
+
+def sample_clocks(stop_file, out):
+    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits", "-lms", "100"]
+    try:
+        return subprocess.Popen(cmd, stdout=open(out, "w"), stderr=subprocess.DEVNULL)
+    except Exception:
+        return None
+
+
+def parse_clocks(path, dev):
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        for line in open(path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or f[0] != str(dev):
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+    except FileNotFoundError:
+        pass
+    sm.sort()
+    return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def cpu_worker(args):
+    """One host core: oracle rsdl(nstage) on a bounded sample mesh for ~secs seconds."""
+    n, p, secs = args
+    sys.path.insert(0, os.path.join(ROOT, "hp-multiphysics_b200"))
+    sys.path.insert(0, ROOT)
+    import hpb
+    from oracle.oracle import Oracle
+    pr = hpb.cd_sinsin(n=n, p=p, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205)
+    o = Oracle(pr)
+    o.setup_preconditioner()
+    o.rsdl(pr.phys.nstage)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        o.rsdl(pr.phys.nstage)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= secs:
+            break
+    return pr.ndof * reps, el
+
+
+def run_cpu(cores, secs, n=60):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(cpu_worker, [(n, P, secs)] * cores)
+    dof = sum(r[0] for r in res)
+    el = max(r[1] for r in res)
+    return dof / el / 1e9, n
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quick", action="store_true",
+                    help="device-timed rsdl steps only (no e2e, update or CPU legs); for profiler runs")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cores = os.cpu_count() or 1
+        secs = 10.0
+        v, n = run_cpu(cores, secs)
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GDoF/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+                "cpu_baseline": {"value": v, "unit": "GDoF/s", "cores": cores, "kind": "port",
+                                 "sample": f"oracle rsdl(nstage) on a {n}x{n} split-square mesh, p={P}, "
+                                           f"{secs:.0f} s per core, one process per core"},
+                "e2e": {"value": v, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import numpy as np
+    import torch
+    import hpb
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()  # a non-default stream: the update graph is captured on it
+    torch.cuda.set_stream(stream)
+
+    pr = hpb.cd_sinsin(n=N_MESH, p=P, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205)
+    lvl = hpb.GPULevel(pr, device=dev, stream=ctypes.c_void_p(stream.cuda_stream))
+    lib = lvl.lib
+    rc = lvl.setup_preconditioner()
+    assert rc == 0
+    ns = pr.phys.nstage
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def enqueue_rsdl():
+        hpb._lib.check(lib.hp_gpu_enqueue_rsdl(lvl.h, ns), "rsdl")
+
+    for _ in range(max(3, args.warmup)):
+        enqueue_rsdl()
+    torch.cuda.synchronize()
+
+    clk_file = os.path.join(ROOT, f"_clocks_{rank}.csv")
+    clk = sample_clocks(None, clk_file)
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        enqueue_rsdl()
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    t_ms = sum(step_ms)
+    if args.quick:
+        if clk:
+            clk.terminate()
+            clk.wait()
+        print(json.dumps({"quick": True, "ms_per_step": t_ms / args.steps,
+                          "value": pr.ndof * args.steps / (t_ms * 1e-3) / 1e9}))
+        lvl.close()
+        return
+
+    # the dominant kernel alone (element residual) for the roofline
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        kev[k][0].record(stream)
+        hpb._lib.check(lib.hp_gpu_enqueue_element_rsdl(lvl.h, ns), "element_rsdl")
+        kev[k][1].record(stream)
+    torch.cuda.synchronize()
+    k_ms = sum(a.elapsed_time(b) for a, b in kev) / args.steps
+
+    # one multistage update (nstage x (rsdl + minvrt + ug update)), for context
+    uev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        uev[k][0].record(stream)
+        hpb._lib.check(lib.hp_gpu_enqueue_update(lvl.h), "update")
+        uev[k][1].record(stream)
+    torch.cuda.synchronize()
+    u_ms = sum(a.elapsed_time(b) for a, b in uev) / args.steps
+    if clk:
+        clk.terminate()
+        clk.wait()
+    clocks = parse_clocks(clk_file, dev)
+    try:
+        os.remove(clk_file)
+    except OSError:
+        pass
+
+    # e2e through the C-ABI with host buffers (pinned)
+    hv = torch.empty(pr.ugv.shape, dtype=torch.float64, pin_memory=True).numpy()
+    hs = torch.empty(pr.ugs.shape, dtype=torch.float64, pin_memory=True).numpy()
+    hi = torch.empty(pr.ugi.shape, dtype=torch.float64, pin_memory=True).numpy()
+    hv[...] = pr.ugv; hs[...] = pr.ugs; hi[...] = pr.ugi
+    rv = torch.empty(pr.ugv.shape, dtype=torch.float64, pin_memory=True).numpy()
+    rs = torch.empty(pr.ugs.shape, dtype=torch.float64, pin_memory=True).numpy()
+    ri = torch.empty(pr.ugi.shape, dtype=torch.float64, pin_memory=True).numpy()
+    P_ = hpb._lib.ptr
+    for _ in range(2):
+        lib.hp_gpu_upload_state(lvl.h, P_(hv), P_(hs), P_(hi))
+        lib.hp_gpu_rsdl(lvl.h, ns)
+        lib.hp_gpu_download_residual(lvl.h, P_(rv), P_(rs), P_(ri))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        hpb._lib.check(lib.hp_gpu_upload_state(lvl.h, P_(hv), P_(hs), P_(hi)), "upload")
+        hpb._lib.check(lib.hp_gpu_rsdl(lvl.h, ns), "rsdl")
+        hpb._lib.check(lib.hp_gpu_download_residual(lvl.h, P_(rv), P_(rs), P_(ri)), "download")
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    io_bytes = hv.nbytes + hs.nbytes + hi.nbytes
+
+    ndof = pr.ndof
+    m = pr.mesh
+    if dist:
+        t = torch.tensor([t_ms, e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms, e2e_s = float(t[0]), float(t[1])
+    value = world * ndof * args.steps / (t_ms * 1e-3) / 1e9
+    e2e = world * ndof / e2e_s / 1e9
+    alg_bytes = 16 * ndof + 36 * m.ntri + 16 * m.npnt
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / (k_ms * 1e-3) / 1e9
+    fl = flops_per_element(P) * m.ntri
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if world == 1:
+        cv, n = run_cpu(1, 10.0)
+        cpu = {"value": cv, "unit": "GDoF/s", "cores": 1, "kind": "port",
+               "sample": f"oracle rsdl(nstage) on a {n}x{n} split-square mesh, p={P}, 10 s, 1 core"}
+    launches_per_step = 3  # k_rsdl_pre, k_rsdl_elem, k_rsdl_fold (cd has no boundary-flux kernel)
+    line = {
+        "metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "kernel": "k_rsdl_elem", "kernel_ms": k_ms,
+                     "algorithmic_bytes": alg_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+                     "fp64_tflops": fl / (k_ms * 1e-3) / 1e12, "flops_per_launch": fl},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": "GDoF/s", "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+        "gpu_launches": launches_per_step * args.steps,
+        "update_ms": u_ms, "update_gdofs_per_stage": ndof * ns / (u_ms * 1e-3) / 1e9,
+        "ndof": ndof, "clocks": clocks,
+    }
+    print(json.dumps(line))
+    lvl.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -515,7 +515,7 @@ static int check_launch(hp_gpu_ctx *c) {
     return HP_OK;
 }
 
-extern "C" int hp_gpu_rsdl(hp_gpu_ctx *c, int stage) {
+extern "C" int hp_gpu_enqueue_rsdl(hp_gpu_ctx *c, int stage) {
     if (!c || stage < 0 || stage > c->ph.nstage) { set_err("bad stage"); return HP_EINVAL; }
     if (c->ph.physics == HP_PHYS_CD && c->ph.beta[stage] > 0.0 && !c->prcn_ready) {
         set_err("cd rsdl needs tau from setup_preconditioner");
@@ -527,7 +527,21 @@ extern "C" int hp_gpu_rsdl(hp_gpu_ctx *c, int stage) {
     const long n = (long)(c->lv + c->ls);
     k_rsdl_fold<double><<<nblk(n, 256), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, c->st.resv, c->st.rrv, c->st.ress,
                                                              c->st.rrs);
-    int r = check_launch(c);
+    return check_launch(c);
+}
+
+extern "C" int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *c, int stage) {
+    if (!c || stage < 0 || stage > c->ph.nstage) { set_err("bad stage"); return HP_EINVAL; }
+    if (c->ph.physics == HP_PHYS_CD && c->ph.beta[stage] > 0.0 && !c->prcn_ready) {
+        set_err("cd rsdl needs tau from setup_preconditioner");
+        return HP_ESTATE;
+    }
+    c->L.elem(c->d_tab, c->mesh, c->st, c->ph, stage, stage >= c->ph.nstage, c->nsm, c->stream);
+    return check_launch(c);
+}
+
+extern "C" int hp_gpu_rsdl(hp_gpu_ctx *c, int stage) {
+    int r = hp_gpu_enqueue_rsdl(c, stage);
     if (r) return r;
     return hp_gpu_sync(c);
 }
@@ -571,12 +585,18 @@ static int ensure_update_graph(hp_gpu_ctx *c) {
     return HP_OK;
 }
 
-extern "C" int hp_gpu_update(hp_gpu_ctx *c) {
+extern "C" int hp_gpu_enqueue_update(hp_gpu_ctx *c) {
     if (!c) return HP_EINVAL;
     if (!c->prcn_ready) { set_err("update before setup_preconditioner"); return HP_ESTATE; }
     int r = ensure_update_graph(c);
     if (r) return r;
     CK(cudaGraphLaunch(c->g_update, c->stream));
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_update(hp_gpu_ctx *c) {
+    int r = hp_gpu_enqueue_update(c);
+    if (r) return r;
     return hp_gpu_sync(c);
 }
 

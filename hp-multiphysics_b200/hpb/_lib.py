@@ -100,6 +100,9 @@ def lib():
         for name in ("hp_gpu_destroy", "hp_gpu_setup_preconditioner", "hp_gpu_minvrt", "hp_gpu_update", "hp_gpu_sync"):
             getattr(L, name).argtypes = [P]
         L.hp_gpu_rsdl.argtypes = [P, _I]
+        L.hp_gpu_enqueue_rsdl.argtypes = [P, _I]
+        L.hp_gpu_enqueue_update.argtypes = [P]
+        L.hp_gpu_enqueue_element_rsdl.argtypes = [P, _I]
         L.hp_gpu_sizes.argtypes = [P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]
         for name in ("hp_gpu_upload_state",):
             getattr(L, name).argtypes = [P, P, P, P]

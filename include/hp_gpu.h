@@ -178,6 +178,15 @@ int hp_gpu_maxres(hp_gpu_ctx *ctx, double *out, double *mx);
  * returns sqrt(sum res^2) and max |res| over every v/s/i coefficient. */
 int hp_gpu_resnorm(hp_gpu_ctx *ctx, double *l2, double *linf);
 
+/* Stream-ordered forms without a host synchronisation (for callers that time or
+ * capture the work themselves): rsdl(stage) with res_r folded into res, and one
+ * update(). */
+int hp_gpu_enqueue_rsdl(hp_gpu_ctx *ctx, int stage);
+int hp_gpu_enqueue_update(hp_gpu_ctx *ctx);
+/* The element-residual kernel alone (the loop over elements of tri_hp::rsdl,
+ * nstage.cpp:52-73: ugtouht, element_rsdl, lftog), for timing it in isolation. */
+int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *ctx, int stage);
+
 /* Synchronises the context's stream and returns the first sticky error. */
 int hp_gpu_sync(hp_gpu_ctx *ctx);
 
