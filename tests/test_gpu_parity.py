@@ -78,3 +78,15 @@ def test_update_iterations(kind, p):
         oh.append(o.maxres()[0])
     assert relerr(g.state(), o.state()) < TOLN
     assert np.max(np.abs(hist - np.array(oh)) / np.array(oh)) < 1e-9
+
+
+def test_gpu_cd_quadratic_exactness_kat():
+    """Testing/tri_hp/conv-diff/Correctness on the GPU: the p = 2 smoother
+    converges to the exact quadratic solution."""
+    pr = hpb.cd_quadratic(n=4, p=2)
+    g = pr.gpu()
+    assert g.setup_preconditioner() == 0
+    hist = g.iterate(300)
+    l2, linf = pr.l2error(*g.state())
+    assert l2[0] < 1e-12 and linf[0] < 1e-11
+    assert hist[-1] < 1e-13
