@@ -1,0 +1,156 @@
+// Residual norm over caller-owned device arrays without any device allocation.
+//
+// hp_gpu_resnorm reduces the residual through a partials buffer that its
+// context allocated with cudaMalloc. Some callers of this library cannot
+// allocate at the moment they need the norm: a solver driver that runs inside a
+// CUDA-graph capture in global capture mode (where cudaMalloc is an illegal
+// call), or an application that gives all device memory to its own pool when it
+// starts and forbids further cudaMalloc/cudaFree. hp_resnorm_noalloc serves
+// them: its only scratch is the file-scope device array below, of fixed size,
+// which every GPU that loads the library keeps until the process exits.
+//
+// Host code must not pass the array's name to a kernel (in host code that name
+// is a host-side stand-in, not a device address): the device address is taken
+// once per device with cudaGetSymbolAddress, with that device current, on the
+// first call made on the device. That first call should therefore come before
+// any stream capture. All calls share the one array, so calls whose work
+// overlaps on the GPU (different streams, or different host threads on the same
+// device) race on it and must be serialised by the caller. Every call writes
+// each partial it reads before reading it, so nothing has to start at zero.
+#include <cuda_runtime.h>
+#include <mutex>
+#include <string>
+#include <cstdio>
+
+#include "hp_gpu.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// [0, 2*MAX): per-chunk (sum of squares, max |x|); [2*MAX, 2*MAX+2): final pair
+static __device__ __align__(256) double g_norm_scratch[2 * HP_NOALLOC_MAX_CHUNKS + 2];
+
+std::mutex g_mu;
+double *g_scratch_dev[64] = {nullptr};  // device address of g_norm_scratch, per device ordinal
+thread_local std::string g_noalloc_err;
+
+__device__ __forceinline__ void block_reduce(double &s, double &m) {
+    __shared__ double ss[kThreads / 32], sx[kThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        const double b = __shfl_xor_sync(0xffffffffu, m, o);
+        m = b > m ? b : m;
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { ss[w] = s; sx[w] = m; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s = 0.0; m = 0.0;
+        for (int q = 0; q < kThreads / 32; ++q) {
+            s += ss[q];
+            m = sx[q] > m ? sx[q] : m;
+        }
+    }
+}
+
+// One block per chunk of HP_NOALLOC_CHUNK elements of the concatenation (a | b | c).
+__global__ void k_chunk_norm(const double *a, long long na, long long ca, const double *b, long long nb, long long cb,
+                             const double *c, long long nc, double *scratch) {
+    long long chunk = blockIdx.x;
+    const double *x;
+    long long n;
+    if (chunk < ca) { x = a; n = na; }
+    else if (chunk < ca + cb) { x = b; n = nb; chunk -= ca; }
+    else { x = c; n = nc; chunk -= ca + cb; }
+    const long long beg = chunk * HP_NOALLOC_CHUNK;
+    long long end = beg + HP_NOALLOC_CHUNK;
+    if (end > n) end = n;
+    double s = 0.0, m = 0.0;
+    for (long long k = beg + threadIdx.x; k < end; k += kThreads) {
+        const double v = x[k];
+        s += v * v;
+        const double av = fabs(v);
+        m = av > m ? av : m;
+    }
+    block_reduce(s, m);
+    if (threadIdx.x == 0) {
+        scratch[2 * blockIdx.x] = s;
+        scratch[2 * blockIdx.x + 1] = m;
+    }
+}
+
+__global__ void k_chunk_final(int nchunks, double *scratch) {
+    double s = 0.0, m = 0.0;
+    for (int k = threadIdx.x; k < nchunks; k += kThreads) {
+        s += scratch[2 * k];
+        const double v = scratch[2 * k + 1];
+        m = v > m ? v : m;
+    }
+    block_reduce(s, m);
+    if (threadIdx.x == 0) {
+        scratch[2 * HP_NOALLOC_MAX_CHUNKS] = sqrt(s);
+        scratch[2 * HP_NOALLOC_MAX_CHUNKS + 1] = m;
+    }
+}
+
+int fail(int code, const char *msg) {
+    g_noalloc_err = msg;
+    return code;
+}
+
+}  // namespace
+
+extern "C" const char *hp_noalloc_last_error(void) { return g_noalloc_err.c_str(); }
+
+extern "C" int hp_resnorm_noalloc(const double *resv, long long nv, const double *ress, long long ns,
+                                  const double *resi, long long ni, double *l2, double *linf, void *stream) {
+    g_noalloc_err.clear();
+    if (!l2 || !linf) return fail(HP_EINVAL, "hp_resnorm_noalloc: null output pointer");
+    if (nv < 0 || ns < 0 || ni < 0) return fail(HP_EINVAL, "hp_resnorm_noalloc: negative length");
+    if ((nv && !resv) || (ns && !ress) || (ni && !resi))
+        return fail(HP_EINVAL, "hp_resnorm_noalloc: null input pointer with non-zero length");
+    const long long ca = (nv + HP_NOALLOC_CHUNK - 1) / HP_NOALLOC_CHUNK;
+    const long long cb = (ns + HP_NOALLOC_CHUNK - 1) / HP_NOALLOC_CHUNK;
+    const long long cc = (ni + HP_NOALLOC_CHUNK - 1) / HP_NOALLOC_CHUNK;
+    const long long nchunks = ca + cb + cc;
+    if (nchunks > HP_NOALLOC_MAX_CHUNKS) {
+        static char msg[160];
+        snprintf(msg, sizeof(msg),
+                 "hp_resnorm_noalloc: %lld values need %lld chunks of %d; the static scratch holds %d "
+                 "(at most %lld values per call)",
+                 nv + ns + ni, nchunks, HP_NOALLOC_CHUNK, HP_NOALLOC_MAX_CHUNKS,
+                 (long long)HP_NOALLOC_MAX_CHUNKS * HP_NOALLOC_CHUNK);
+        return fail(HP_EINVAL, msg);
+    }
+    if (nchunks == 0) {
+        *l2 = 0.0;
+        *linf = 0.0;
+        return HP_OK;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return fail(HP_ECUDA, "hp_resnorm_noalloc: no current CUDA device");
+    double *scratch;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (!g_scratch_dev[dev]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_norm_scratch);
+            if (e != cudaSuccess || !p) return fail(HP_ECUDA, "hp_resnorm_noalloc: cudaGetSymbolAddress failed");
+            g_scratch_dev[dev] = static_cast<double *>(p);
+        }
+        scratch = g_scratch_dev[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_chunk_norm<<<(unsigned)nchunks, kThreads, 0, st>>>(resv, nv, ca, ress, ns, cb, resi, ni, scratch);
+    k_chunk_final<<<1, kThreads, 0, st>>>((int)nchunks, scratch);
+    if (cudaGetLastError() != cudaSuccess) return fail(HP_ECUDA, "hp_resnorm_noalloc: kernel launch failed");
+    double out[2];
+    if (cudaMemcpyAsync(out, scratch + 2 * HP_NOALLOC_MAX_CHUNKS, sizeof(out), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return fail(HP_ECUDA, "hp_resnorm_noalloc: result copy failed");
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(HP_ECUDA, "hp_resnorm_noalloc: stream sync failed");
+    *l2 = out[0];
+    *linf = out[1];
+    return HP_OK;
+}

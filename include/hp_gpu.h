@@ -193,6 +193,25 @@ int hp_gpu_sync(hp_gpu_ctx *ctx);
 /* Last error text (thread-local), "" if none. */
 const char *hp_gpu_last_error(void);
 
+/* Residual norm that allocates nothing. No counterpart in the reference.
+ * For callers that cannot call cudaMalloc when they need the norm: a driver
+ * running inside a CUDA-graph capture in global mode, or an application whose
+ * device memory all belongs to its own pool. Same result as hp_gpu_resnorm's
+ * reduction (sqrt of the sum of squares and max |x| over res.v, res.s, res.i),
+ * but over caller-owned device arrays (e.g. from hp_gpu_device_ptrs) and with a
+ * fixed static device scratch of HP_NOALLOC_MAX_CHUNKS partials, held by every
+ * GPU that loads the library until exit. At most HP_NOALLOC_MAX_CHUNKS chunks
+ * of HP_NOALLOC_CHUNK values per call (nv, ns, ni each rounded up to whole
+ * chunks); larger inputs return HP_EINVAL with a message from
+ * hp_noalloc_last_error(). The first call on a device looks up the scratch's
+ * device address and should come before any stream capture. All calls share
+ * the scratch: calls that overlap on the GPU race. Synchronises `stream`. */
+#define HP_NOALLOC_CHUNK 65536
+#define HP_NOALLOC_MAX_CHUNKS 4096
+int hp_resnorm_noalloc(const double *resv, long long nv, const double *ress, long long ns, const double *resi,
+                       long long ni, double *l2, double *linf, void *stream);
+const char *hp_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
