@@ -103,47 +103,43 @@ inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-// Per-(p, physics) launchers.
+// Per-(precision, p, physics) launchers.
+template <typename R>
 struct Launchers {
     size_t tab_bytes;
     void (*fill)(const hp_basis_tables &, void *);
-    void (*elem)(const void *tab, const Mesh &, const State<double> &, const Phys &, int stage, int zero_rr,
+    void (*elem)(const void *tab, const Mesh &, const State<R> &, const Phys &, int stage, int zero_rr, int diff,
                  int nsm, cudaStream_t);
-    void (*bflux)(const void *tab, const Mesh &, const State<double> &, const Phys &, cudaStream_t);
-    void (*prcn)(const void *tab, const Mesh &, const State<double> &, const Phys &, int *err, cudaStream_t);
-    void (*side)(const Mesh &, const State<double> &, const DevMinv<double> *, int im, int mode, double cfla,
-                 int upd, int fold, cudaStream_t);
-    void (*intr)(const Mesh &, const State<double> &, const DevMinv<double> *, double cfla, int upd, cudaStream_t);
-    void (*vert)(const Mesh &, const State<double> &, const DevMinv<double> *, int sm, int im, double cfla, int upd,
-                 int fold, unsigned long long *slot, cudaStream_t);
+    void (*bflux)(const void *tab, const Mesh &, const State<R> &, const Phys &, int diff, cudaStream_t);
+    void (*side)(const Mesh &, const State<R> &, const DevMinv<R> *, int im, int mode, double cfla, int upd, int fold,
+                 cudaStream_t);
+    void (*intr)(const Mesh &, const State<R> &, const DevMinv<R> *, double cfla, int upd, cudaStream_t);
+    void (*vert)(const Mesh &, const State<R> &, const DevMinv<R> *, int sm, int im, double cfla, int upd, int fold,
+                 unsigned long long *slot, cudaStream_t);
     int elem_smem;
+    cudaError_t (*set_smem)();
 };
 
-template <int P, int PHYS>
+template <typename R, int P, int PHYS>
 struct LaunchImpl {
-    using R = double;
     using C = ElemCfg<R, P, PHYS>;
     static constexpr int NV = C::NV, SM = P - 1, IM = (P - 1) * (P - 2) / 2;
     static int smem() {
         return (int)(((sizeof(DevTables<R, P>) + 15) / 16) * 16 + (size_t)C::WPC * C::S_WARP * sizeof(R));
     }
     static void fill(const hp_basis_tables &b, void *out) { fill_tables<R, P>(b, *reinterpret_cast<DevTables<R, P> *>(out)); }
-    static void elem(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int stage, int zero_rr, int nsm,
-                     cudaStream_t st) {
+    static void elem(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int stage, int zero_rr, int diff,
+                     int nsm, cudaStream_t st) {
         int blocks = nblk(m.ntri, C::WPC);
         const int cap = nsm * 16;
         if (blocks > cap) blocks = cap;
         k_rsdl_elem<R, P, PHYS><<<blocks, C::WPC * 32, smem(), st>>>(
-            reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, stage, zero_rr);
+            reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, stage, zero_rr, diff);
     }
-    static void bflux(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, cudaStream_t st) {
+    static void bflux(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int diff, cudaStream_t st) {
         if (PHYS == 1 && m.nbseg > 0)
             k_bdry_flux_ins<R, P><<<nblk(m.nbseg, 128), 128, 0, st>>>(reinterpret_cast<const DevTables<R, P> *>(tab), m,
-                                                                       s, ph);
-    }
-    static void prcn(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int *err, cudaStream_t st) {
-        k_prcn_elem<R, P, PHYS><<<nblk(m.ntri, 128), 128, 0, st>>>(reinterpret_cast<const DevTables<R, P> *>(tab), m, s,
-                                                                   ph, err);
+                                                                       s, ph, diff);
     }
     static void side(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, int im, int mode, double cfla, int upd,
                      int fold, cudaStream_t st) {
@@ -157,50 +153,58 @@ struct LaunchImpl {
                      int fold, unsigned long long *slot, cudaStream_t st) {
         k_minv_vert<R, NV><<<nblk(m.npnt, 128), 128, 0, st>>>(m, s, mt, sm, im, (R)cfla, upd, fold, slot);
     }
-    static Launchers get() {
-        Launchers L;
+    static cudaError_t set_smem_attr() {
+        return cudaFuncSetAttribute(k_rsdl_elem<R, P, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem());
+    }
+    static Launchers<R> get() {
+        Launchers<R> L;
         L.tab_bytes = sizeof(DevTables<R, P>);
         L.fill = &fill;
         L.elem = &elem;
         L.bflux = &bflux;
-        L.prcn = &prcn;
         L.side = &side;
         L.intr = &intr;
         L.vert = &vert;
         L.elem_smem = smem();
+        L.set_smem = &set_smem_attr;
         return L;
     }
 };
 
-template <int PHYS>
-static bool get_launchers_phys(int p, Launchers &L) {
+template <typename R, int PHYS>
+static bool get_launchers_phys(int p, Launchers<R> &L) {
     switch (p) {
-        case 1: L = LaunchImpl<1, PHYS>::get(); return true;
-        case 2: L = LaunchImpl<2, PHYS>::get(); return true;
-        case 3: L = LaunchImpl<3, PHYS>::get(); return true;
-        case 4: L = LaunchImpl<4, PHYS>::get(); return true;
-        case 5: L = LaunchImpl<5, PHYS>::get(); return true;
-        case 6: L = LaunchImpl<6, PHYS>::get(); return true;
-        case 7: L = LaunchImpl<7, PHYS>::get(); return true;
-        case 8: L = LaunchImpl<8, PHYS>::get(); return true;
+        case 1: L = LaunchImpl<R, 1, PHYS>::get(); return true;
+        case 2: L = LaunchImpl<R, 2, PHYS>::get(); return true;
+        case 3: L = LaunchImpl<R, 3, PHYS>::get(); return true;
+        case 4: L = LaunchImpl<R, 4, PHYS>::get(); return true;
+        case 5: L = LaunchImpl<R, 5, PHYS>::get(); return true;
+        case 6: L = LaunchImpl<R, 6, PHYS>::get(); return true;
+        case 7: L = LaunchImpl<R, 7, PHYS>::get(); return true;
+        case 8: L = LaunchImpl<R, 8, PHYS>::get(); return true;
     }
     return false;
 }
 
-template <int P, int PHYS>
-static cudaError_t set_smem_attr() {
-    return cudaFuncSetAttribute(k_rsdl_elem<double, P, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                LaunchImpl<P, PHYS>::smem());
+template <typename R>
+static bool get_launchers(int p, int phys, Launchers<R> &L) {
+    return phys ? get_launchers_phys<R, 1>(p, L) : get_launchers_phys<R, 0>(p, L);
 }
-static cudaError_t set_smem(int p, int phys) {
-#define SM_CASE(PP)                                                            \
-    case PP:                                                                   \
-        return phys ? set_smem_attr<PP, 1>() : set_smem_attr<PP, 0>();
-    switch (p) {
-        SM_CASE(1) SM_CASE(2) SM_CASE(3) SM_CASE(4) SM_CASE(5) SM_CASE(6) SM_CASE(7) SM_CASE(8)
-    }
-#undef SM_CASE
-    return cudaErrorInvalidValue;
+
+// FP64 preconditioner set-up kernel launch (double only)
+static void launch_prcn(int p, int phys, const void *tab, const Mesh &m, const State<double> &s, const Phys &ph,
+                        int *err, cudaStream_t st) {
+#define PR_CASE(PP)                                                                                           \
+    case PP:                                                                                                  \
+        if (phys)                                                                                             \
+            k_prcn_elem<double, PP, 1><<<nblk(m.ntri, 128), 128, 0, st>>>(                                      \
+                reinterpret_cast<const DevTables<double, PP> *>(tab), m, s, ph, err);                         \
+        else                                                                                                  \
+            k_prcn_elem<double, PP, 0><<<nblk(m.ntri, 128), 128, 0, st>>>(                                      \
+                reinterpret_cast<const DevTables<double, PP> *>(tab), m, s, ph, err);                         \
+        break;
+    switch (p) { PR_CASE(1) PR_CASE(2) PR_CASE(3) PR_CASE(4) PR_CASE(5) PR_CASE(6) PR_CASE(7) PR_CASE(8) }
+#undef PR_CASE
 }
 
 struct hp_gpu_ctx {
@@ -209,11 +213,16 @@ struct hp_gpu_ctx {
     bool own_stream = false;
     int p = 0, NV = 0, npnt = 0, nseg = 0, ntri = 0, nbseg = 0, sm = 0, im = 0, nsm = 148;
     Phys ph{};
-    Launchers L{};
+    Launchers<double> L{};
+    Launchers<float> L32{};
     Mesh mesh{};
     State<double> st{};
-    void *d_tab = nullptr;
+    State<float> s32{};  // correction-form FP32 smoother state (allocated on first mixed solve)
+    bool mixed_ready = false;
+    void *d_tab = nullptr, *d_tab32 = nullptr;
     DevMinv<double> *d_minv = nullptr;
+    DevMinv<float> *d_minv32 = nullptr;
+    cudaGraphExec_t g_update32 = nullptr;
     double vdiag = 0.0;
     unsigned long long *d_slot = nullptr;
     double *d_hist = nullptr;
@@ -292,9 +301,12 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     c->p = b->p; c->sm = b->sm; c->im = b->im;
     c->NV = physics == HP_PHYS_INS ? 3 : 1;
     c->npnt = m->npnt; c->nseg = m->nseg; c->ntri = m->ntri; c->nbseg = m->nbseg;
-    bool ok = physics ? get_launchers_phys<1>(c->p, c->L) : get_launchers_phys<0>(c->p, c->L);
+    bool ok = get_launchers<double>(c->p, physics, c->L) && get_launchers<float>(c->p, physics, c->L32);
     if (!ok) { set_err("p=%d not built", c->p); return fail(HP_ENOTSUP); }
-    if (set_smem(c->p, physics) != cudaSuccess) { set_err("smem attribute (%d bytes) rejected", c->L.elem_smem); return fail(HP_ECUDA); }
+    if (c->L.set_smem() != cudaSuccess || c->L32.set_smem() != cudaSuccess) {
+        set_err("smem attribute (%d bytes) rejected", c->L.elem_smem);
+        return fail(HP_ECUDA);
+    }
     Phys &P = c->ph;
     P.physics = physics; P.NV = c->NV; P.nstage = ph->nstage;
     for (int k = 0; k < 8; ++k) { P.alpha[k] = ph->alpha[k]; P.beta[k] = ph->beta[k]; }
@@ -384,6 +396,12 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     fill_minv<double>(*b, hm);
     c->vdiag = b->vdiag;
     if ((r = upload(c, &c->d_minv, &hm, 1))) return fail(r);
+    std::vector<unsigned char> htab32(c->L32.tab_bytes);
+    c->L32.fill(*b, htab32.data());
+    if ((r = upload(c, (unsigned char **)&c->d_tab32, htab32.data(), htab32.size()))) return fail(r);
+    DevMinv<float> hm32;
+    fill_minv<float>(*b, hm32);
+    if ((r = upload(c, &c->d_minv32, &hm32, 1))) return fail(r);
 
     // state
     const int NV = c->NV;
@@ -416,6 +434,7 @@ extern "C" int hp_gpu_destroy(hp_gpu_ctx *c) {
     if (!c) return HP_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->g_update) cudaGraphExecDestroy(c->g_update);
+    if (c->g_update32) cudaGraphExecDestroy(c->g_update32);
     for (void *p : c->allocs) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -477,35 +496,48 @@ extern "C" int hp_gpu_device_ptrs(hp_gpu_ctx *c, double **ugv, double **ugs, dou
     return HP_OK;
 }
 
-// Stream-ordered body of rsdl(stage) (no sync, capturable).
-static void enqueue_rsdl(hp_gpu_ctx *c, int stage) {
-    const int nstage = c->ph.nstage;
+// Stream-ordered body of rsdl(stage) (no sync, capturable), either precision.
+template <typename R>
+static void enqueue_rsdl_t(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab, const State<R> &st, const Phys &ph,
+                           int stage, int diff) {
+    const int nstage = ph.nstage;
     const int zero_rr = (stage >= nstage) ? 1 : 0;
-    const double omb = zero_rr ? 0.0 : 1.0 - c->ph.beta[stage];
+    const double omb = zero_rr ? 0.0 : 1.0 - ph.beta[stage];
     const long n = (long)(c->lv + c->ls);
-    k_rsdl_pre<double><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>(
-        (int)c->lv, (int)c->ls, c->st.resv, c->st.ress, c->st.rrv, c->st.rrs, omb, zero_rr);
-    c->L.elem(c->d_tab, c->mesh, c->st, c->ph, stage, zero_rr, c->nsm, c->stream);
-    c->L.bflux(c->d_tab, c->mesh, c->st, c->ph, c->stream);
+    k_rsdl_pre<R><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, st.resv, st.ress,
+                                                                           st.rrv, st.rrs, (R)omb, zero_rr);
+    L.elem(tab, c->mesh, st, ph, stage, zero_rr, diff, c->nsm, c->stream);
+    L.bflux(tab, c->mesh, st, ph, diff, c->stream);
 }
+static void enqueue_rsdl(hp_gpu_ctx *c, int stage) { enqueue_rsdl_t<double>(c, c->L, c->d_tab, c->st, c->ph, stage, 0); }
 
 // minvrt (+ update of ug with cflalpha when upd) ; maxres into slot when slot != NULL
+template <typename R>
+static void enqueue_minvrt_t(hp_gpu_ctx *c, const Launchers<R> &L, const State<R> &st, const DevMinv<R> *mt,
+                             double cfla, int upd, int fold, unsigned long long *slot) {
+    L.vert(c->mesh, st, mt, c->sm, c->im, cfla, upd, fold, slot, c->stream);
+    for (int mode = 0; mode < c->sm; ++mode) L.side(c->mesh, st, mt, c->im, mode, cfla, upd, fold, c->stream);
+    if (c->im > 0) L.intr(c->mesh, st, mt, cfla, upd, c->stream);
+}
 static void enqueue_minvrt(hp_gpu_ctx *c, double cfla, int upd, int fold, unsigned long long *slot) {
-    c->L.vert(c->mesh, c->st, c->d_minv, c->sm, c->im, cfla, upd, fold, slot, c->stream);
-    for (int mode = 0; mode < c->sm; ++mode)
-        c->L.side(c->mesh, c->st, c->d_minv, c->im, mode, cfla, upd, fold, c->stream);
-    if (c->im > 0) c->L.intr(c->mesh, c->st, c->d_minv, cfla, upd, c->stream);
+    enqueue_minvrt_t<double>(c, c->L, c->st, c->d_minv, cfla, upd, fold, slot);
+}
+
+template <typename R>
+static void enqueue_update_t(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab, const State<R> &st,
+                             const DevMinv<R> *mt, const Phys &ph, int diff, unsigned long long *slot) {
+    cudaMemcpyAsync(st.u0v, st.ugv, c->lv * sizeof(R), cudaMemcpyDeviceToDevice, c->stream);
+    if (c->ls) cudaMemcpyAsync(st.u0s, st.ugs, c->ls * sizeof(R), cudaMemcpyDeviceToDevice, c->stream);
+    if (c->li) cudaMemcpyAsync(st.u0i, st.ugi, c->li * sizeof(R), cudaMemcpyDeviceToDevice, c->stream);
+    for (int stage = 0; stage < ph.nstage; ++stage) {
+        enqueue_rsdl_t<R>(c, L, tab, st, ph, stage, diff);
+        const double cfla = ph.alpha[stage] * ph.cfl;
+        enqueue_minvrt_t<R>(c, L, st, mt, cfla, 1, 1, stage == ph.nstage - 1 ? slot : nullptr);
+    }
 }
 
 static void enqueue_update(hp_gpu_ctx *c) {
-    cudaMemcpyAsync(c->st.u0v, c->st.ugv, c->lv * 8, cudaMemcpyDeviceToDevice, c->stream);
-    if (c->ls) cudaMemcpyAsync(c->st.u0s, c->st.ugs, c->ls * 8, cudaMemcpyDeviceToDevice, c->stream);
-    if (c->li) cudaMemcpyAsync(c->st.u0i, c->st.ugi, c->li * 8, cudaMemcpyDeviceToDevice, c->stream);
-    for (int stage = 0; stage < c->ph.nstage; ++stage) {
-        enqueue_rsdl(c, stage);
-        const double cfla = c->ph.alpha[stage] * c->ph.cfl;
-        enqueue_minvrt(c, cfla, 1, 1, stage == c->ph.nstage - 1 ? c->d_slot : nullptr);
-    }
+    enqueue_update_t<double>(c, c->L, c->d_tab, c->st, c->d_minv, c->ph, 0, c->d_slot);
     k_hist_advance<<<1, 32, 0, c->stream>>>(c->d_slot, c->d_hist, c->d_iter, c->NV, c->hist_cap);
 }
 
@@ -536,7 +568,7 @@ extern "C" int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *c, int stage) {
         set_err("cd rsdl needs tau from setup_preconditioner");
         return HP_ESTATE;
     }
-    c->L.elem(c->d_tab, c->mesh, c->st, c->ph, stage, stage >= c->ph.nstage, c->nsm, c->stream);
+    c->L.elem(c->d_tab, c->mesh, c->st, c->ph, stage, stage >= c->ph.nstage, 0, c->nsm, c->stream);
     return check_launch(c);
 }
 
@@ -551,7 +583,7 @@ extern "C" int hp_gpu_setup_preconditioner(hp_gpu_ctx *c) {
     CK(cudaMemsetAsync(c->st.vprcn, 0, (size_t)c->npnt * c->NV * 8, c->stream));
     CK(cudaMemsetAsync(c->st.sprcn, 0, (size_t)c->nseg * c->NV * 8, c->stream));
     CK(cudaMemsetAsync(c->d_err, 0, 4, c->stream));
-    c->L.prcn(c->d_tab, c->mesh, c->st, c->ph, c->d_err, c->stream);
+    launch_prcn(c->p, c->ph.physics, c->d_tab, c->mesh, c->st, c->ph, c->d_err, c->stream);
     const int nv = c->npnt * c->NV, ns = (c->p > 1 ? c->nseg * c->NV : 0);
     k_prcn_invert<double><<<nblk(nv + ns, 256), 256, 0, c->stream>>>(nv, ns, c->st.vprcn, c->st.sprcn, c->vdiag);
     int r = check_launch(c);
@@ -664,4 +696,191 @@ extern "C" int hp_gpu_sync(hp_gpu_ctx *c) {
     e = cudaGetLastError();
     if (e != cudaSuccess) { set_err("cuda error: %s", cudaGetErrorString(e)); return HP_ECUDA; }
     return HP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Convergence drivers: plain FP64 smoothing and FP32 correction smoothing with
+// FP64 defect correction.
+// ---------------------------------------------------------------------------
+static int alloc_mixed(hp_gpu_ctx *c) {
+    if (c->mixed_ready) return HP_OK;
+    State<float> &f = c->s32;
+    int r;
+    float **v[] = {&f.ugv, &f.u0v, &f.resv, &f.rrv};
+    float **sp[] = {&f.ugs, &f.u0s, &f.ress, &f.rrs};
+    float **ip[] = {&f.ugi, &f.u0i, &f.resi, &f.rri};
+    for (auto q : v) if ((r = dalloc(c, (void **)q, c->lv * 4))) return r;
+    for (auto q : sp) if ((r = dalloc(c, (void **)q, std::max<size_t>(c->ls, 1) * 4))) return r;
+    for (auto q : ip) if ((r = dalloc(c, (void **)q, std::max<size_t>(c->li, 1) * 4))) return r;
+    float *ubv, *ubs, *ubi, *dv, *ds, *di;
+    if ((r = dalloc(c, (void **)&ubv, c->lv * 4))) return r;
+    if ((r = dalloc(c, (void **)&ubs, std::max<size_t>(c->ls, 1) * 4))) return r;
+    if ((r = dalloc(c, (void **)&ubi, std::max<size_t>(c->li, 1) * 4))) return r;
+    if ((r = dalloc(c, (void **)&dv, c->lv * 4))) return r;
+    if ((r = dalloc(c, (void **)&ds, std::max<size_t>(c->ls, 1) * 4))) return r;
+    if ((r = dalloc(c, (void **)&di, std::max<size_t>(c->li, 1) * 4))) return r;
+    f.ubv = ubv; f.ubs = ubs; f.ubi = ubi;
+    f.dresv = dv; f.dress = ds; f.dresi = c->li ? di : nullptr;
+    if ((r = dalloc(c, (void **)&f.vprcn, (size_t)c->npnt * c->NV * 4))) return r;
+    if ((r = dalloc(c, (void **)&f.sprcn, (size_t)c->nseg * c->NV * 4))) return r;
+    if ((r = dalloc(c, (void **)&f.tprcn, (size_t)c->ntri * c->NV * 4))) return r;
+    if ((r = dalloc(c, (void **)&f.tau, (size_t)c->ntri * c->NV * 4))) return r;
+    // res_r is scaled by (1 - beta) before it is first written: it must start finite
+    CK(cudaMemsetAsync(f.rrv, 0, c->lv * 4, c->stream));
+    if (c->ls) CK(cudaMemsetAsync(f.rrs, 0, c->ls * 4, c->stream));
+    if (c->li) CK(cudaMemsetAsync(f.rri, 0, c->li * 4, c->stream));
+    CK(cudaMemsetAsync(f.resv, 0, c->lv * 4, c->stream));
+    if (c->ls) CK(cudaMemsetAsync(f.ress, 0, c->ls * 4, c->stream));
+    if (c->li) CK(cudaMemsetAsync(f.resi, 0, c->li * 4, c->stream));
+    c->mixed_ready = true;
+    return HP_OK;
+}
+
+template <typename A, typename B>
+static void conv(hp_gpu_ctx *c, long n, const A *src, B *dst) {
+    if (n > 0) k_convert<A, B><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>(n, src, dst);
+}
+
+// FP32 copies of the FP64 preconditioner (computed at the base state)
+static void mixed_prcn(hp_gpu_ctx *c) {
+    State<float> &f = c->s32;
+    conv(c, (long)c->npnt * c->NV, c->st.vprcn, f.vprcn);
+    conv(c, (long)c->nseg * c->NV, c->st.sprcn, f.sprcn);
+    conv(c, (long)c->ntri * c->NV, c->st.tprcn, f.tprcn);
+    conv(c, (long)c->ntri * c->NV, c->st.tau, f.tau);
+}
+
+// Start of one correction cycle: base = fp32(u64), dres = fp32(R64(u64)) (the FP64
+// residual left in res by rsdl(nstage)), correction d = 0, res_r = 0.
+static void mixed_prepare(hp_gpu_ctx *c) {
+    State<float> &f = c->s32;
+    conv(c, (long)c->lv, c->st.ugv, (float *)f.ubv);
+    conv(c, (long)c->ls, c->st.ugs, (float *)f.ubs);
+    conv(c, (long)c->li, c->st.ugi, (float *)f.ubi);
+    conv(c, (long)c->lv, c->st.resv, (float *)f.dresv);
+    conv(c, (long)c->ls, c->st.ress, (float *)f.dress);
+    if (c->li) conv(c, (long)c->li, c->st.resi, (float *)f.dresi);
+    cudaMemsetAsync(f.ugv, 0, c->lv * 4, c->stream);
+    if (c->ls) cudaMemsetAsync(f.ugs, 0, c->ls * 4, c->stream);
+    if (c->li) cudaMemsetAsync(f.ugi, 0, c->li * 4, c->stream);
+}
+
+static void mixed_apply(hp_gpu_ctx *c) {
+    const State<float> &f = c->s32;
+    auto add = [&](long n, const float *src, double *dst) {
+        if (n > 0) k_add_into<float, double><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>(n, src, dst);
+    };
+    add((long)c->lv, f.ugv, c->st.ugv);
+    add((long)c->ls, f.ugs, c->st.ugs);
+    add((long)c->li, f.ugi, c->st.ugi);
+}
+
+static int ensure_update32_graph(hp_gpu_ctx *c) {
+    if (c->g_update32) return HP_OK;
+    Phys ph = c->ph;
+    if (ph.physics == HP_PHYS_CD) ph.src = 0.0;  // the cd residual is affine: R(b+d) - R(b) = R_0(d)
+    const int diff = (ph.physics == HP_PHYS_INS) ? 1 : 0;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_update_t<float>(c, c->L32, c->d_tab32, c->s32, c->d_minv32, ph, diff, nullptr);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) { set_err("graph capture failed: %s", cudaGetErrorString(e)); return HP_ECUDA; }
+    e = cudaGraphInstantiate(&c->g_update32, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { set_err("graph instantiate failed: %s", cudaGetErrorString(e)); c->g_update32 = nullptr; return HP_ECUDA; }
+    return HP_OK;
+}
+
+static int fp64_norm(hp_gpu_ctx *c, double *l2) {
+    int r = hp_gpu_enqueue_rsdl(c, c->ph.nstage);
+    if (r) return r;
+    k_mask_essential<double><<<nblk(c->npnt + c->nseg, 256), 256, 0, c->stream>>>(c->mesh, c->st.resv, c->st.ress,
+                                                                                 c->NV, c->sm);
+    double ss = 0.0, mx = 0.0;
+    if ((r = device_norm(c, c->st.resv, c->lv, ss, mx))) return r;
+    if ((r = device_norm(c, c->st.ress, c->ls, ss, mx))) return r;
+    if ((r = device_norm(c, c->st.resi, c->li, ss, mx))) return r;
+    *l2 = std::sqrt(ss);
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_solve(hp_gpu_ctx *c, int mode, double drop, int max_updates, int inner, int check_every,
+                            int prcn_every, double *hist, int hist_cap, int *n_hist, double *seconds, int *updates) {
+    if (!c || (mode != HP_PREC_FP64 && mode != HP_PREC_FP32) || drop <= 0.0 || max_updates < 1) {
+        set_err("hp_gpu_solve: bad argument");
+        return HP_EINVAL;
+    }
+    if (check_every < 1) check_every = 10;
+    if (inner < 1) inner = 10;
+    int r;
+    if ((r = ensure_update_graph(c))) return r;
+    if (mode == HP_PREC_FP32) {
+        if ((r = alloc_mixed(c))) return r;
+        if ((r = ensure_update32_graph(c))) return r;
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, c->stream));
+    int nh = 0, nupd = 0, nchk = 0;
+    double r0 = 0.0, rn = 0.0;
+    r = hp_gpu_setup_preconditioner(c);
+    if (r) return r < 0 ? r : HP_ESTATE;
+    if ((r = fp64_norm(c, &r0))) return r;
+    if (hist && nh < hist_cap) hist[nh++] = 1.0;
+    if (mode == HP_PREC_FP32) mixed_prcn(c);
+    while (nupd < max_updates) {
+        if (mode == HP_PREC_FP64) {
+            for (int k = 0; k < check_every && nupd < max_updates; ++k, ++nupd) CK(cudaGraphLaunch(c->g_update, c->stream));
+        } else {
+            // the FP64 residual R64(u) is in res from the last norm evaluation
+            mixed_prepare(c);
+            for (int k = 0; k < inner && nupd < max_updates; ++k, ++nupd) CK(cudaGraphLaunch(c->g_update32, c->stream));
+            mixed_apply(c);
+        }
+        ++nchk;
+        if (prcn_every > 0 && nchk % prcn_every == 0) {
+            r = hp_gpu_setup_preconditioner(c);
+            if (r) return r < 0 ? r : HP_ESTATE;
+            if (mode == HP_PREC_FP32) mixed_prcn(c);
+        }
+        if ((r = fp64_norm(c, &rn))) return r;
+        const double d = rn / r0;
+        if (hist && nh < hist_cap) hist[nh++] = d;
+        if (!(d == d)) break;  // NaN
+        if (d <= drop) break;
+    }
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (n_hist) *n_hist = nh;
+    if (seconds) *seconds = ms * 1e-3;
+    if (updates) *updates = nupd;
+    return hp_gpu_sync(c);
+}
+
+// Diagnostic: `n` multistage updates of the FP32 smoother in plain form (the FP32
+// state is fp32(u), no source, no correction), written back to the FP64 state.
+// Lets tests compare the FP32 kernels with the FP64 ones update by update.
+extern "C" int hp_gpu_fp32_updates(hp_gpu_ctx *c, int n) {
+    if (!c || n < 0) return HP_EINVAL;
+    int r;
+    if ((r = alloc_mixed(c))) return r;
+    if (!c->prcn_ready) { set_err("fp32 updates before setup_preconditioner"); return HP_ESTATE; }
+    mixed_prcn(c);
+    State<float> f = c->s32;
+    f.ubv = f.ubs = f.ubi = nullptr;
+    f.dresv = f.dress = f.dresi = nullptr;
+    conv(c, (long)c->lv, c->st.ugv, f.ugv);
+    conv(c, (long)c->ls, c->st.ugs, f.ugs);
+    conv(c, (long)c->li, c->st.ugi, f.ugi);
+    for (int k = 0; k < n; ++k) enqueue_update_t<float>(c, c->L32, c->d_tab32, f, c->d_minv32, c->ph, 0, nullptr);
+    conv(c, (long)c->lv, (const float *)f.ugv, c->st.ugv);
+    conv(c, (long)c->ls, (const float *)f.ugs, c->st.ugs);
+    conv(c, (long)c->li, (const float *)f.ugi, c->st.ugi);
+    if ((r = check_launch(c))) return r;
+    return hp_gpu_sync(c);
 }

@@ -63,6 +63,12 @@ struct State {
     R *resv, *ress, *resi;
     R *rrv, *rrs, *rri;
     R *vprcn, *sprcn, *tprcn, *tau;
+    // Correction (defect) form: ug holds a correction d about the base state ub and
+    // the residual is R(ub + d) - R(ub) + dres (the FP64 residual of the base, as the
+    // reference's mg_source adds dres on coarse levels, nstage.cpp:113-129). NULL
+    // pointers = plain form.
+    const R *ubv, *ubs, *ubi;
+    const R *dresv, *dress, *dresi;
 };
 
 __device__ __forceinline__ void atomic_add(double *a, double v) { atomicAdd(a, v); }
@@ -86,20 +92,25 @@ struct ElemCfg {
     static constexpr int NPAIR = NV;               // flux pairs integrated by intgrtrs
     static constexpr int NQ = (PHYS == 1 ? 16 : 7);  // per-point scratch values
     static constexpr int WPC = (P <= 4 ? 8 : 4);   // warps per CTA
+    static constexpr int NB = (PHYS == 1 ? 2 : 0);  // base-state variables gathered in correction form
     // per-warp scratch (in R units)
-    static constexpr int S_UHT = NV * T;
-    static constexpr int S_WK = (6 * G * X > 5 * G * X ? 6 * G * X : 5 * G * X);
-    static constexpr int S_PT = (NQ + NV) * G * G;
+    static constexpr int S_UHT = (NV + NB) * T;
+    static constexpr int S_WK = (PHYS == 1 ? 7 : 6) * G * X;
+    static constexpr int S_PT = (NQ + NV + 1) * G * G;
     static constexpr int S_WARP = S_UHT + S_WK + S_PT;
 };
 
 // Point-array slot indices (each slot is a [G][G] array)
-// ins: 0..3 cvI (cv00,cv01,cv10,cv11)  4,5 mI  6..9 cvT  10..13 df  14,15 u,v  16..18 res
+// ins: 0..3 cvI (cv00,cv01,cv10,cv11)  4,5 mI  6..9 cvT  10..13 df  14,15 u,v  16..18 res  19 q
 // cd : 0,1 cvI  2,3 cvT  4,5 e  6 u      7 res
+// Correction form (diff != 0, ins): uht holds d, uht+NV*T the base velocity b; the
+// fluxes are the exact differences F(b+d) - F(b) of the convective, pressure and
+// viscous terms, the SUPG term A(b+d) tau(b) res(d) with tau frozen at the base.
 
 template <typename R, int P, int PHYS>
 __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
-    k_rsdl_elem(const DevTables<R, P> *__restrict__ gtab, Mesh mesh, State<R> st, Phys ph, int stage, int zero_rr) {
+    k_rsdl_elem(const DevTables<R, P> *__restrict__ gtab, Mesh mesh, State<R> st, Phys ph, int stage, int zero_rr,
+                int diff) {
     using C = ElemCfg<R, P, PHYS>;
     constexpr int G = C::G, X = C::X, T = C::T, IM = C::IM, BM = C::BM, NV = C::NV, GG = G * G;
     constexpr int SM = (C::SM > 0 ? C::SM : 1);  // side-mode stride (unused when p = 1)
@@ -141,6 +152,24 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
             }
             uht[n * T + m] = val;
         }
+        if (PHYS == 1 && diff) {
+            for (int w = lane; w < 2 * T; w += 32) {
+                const int n = w / T, m = w - n * T;
+                R val;
+                if (m < 3) {
+                    const int v = (m == 0 ? p0 : (m == 1 ? p1 : p2));
+                    val = st.ubv[v * NV + n];
+                } else if (m < BM) {
+                    const int i = (m - 3) / SM, k = (m - 3) - i * SM;
+                    const int sind = mesh.tri_seg[3 * tind + i], sg = mesh.tri_sgn[3 * tind + i];
+                    val = st.ubs[(sind * SM + k) * NV + n];
+                    if ((k & 1) && sg < 0) val = -val;
+                } else {
+                    val = st.ubi[((size_t)tind * IM + (m - BM)) * NV + n];
+                }
+                uht[(NV + n) * T + m] = val;
+            }
+        }
         // geometry (straight element): ldcrd(n,0) = (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2
         const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
         const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
@@ -152,7 +181,8 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
         {
             constexpr int NDV = (PHYS == 1 ? 2 : 1);  // variables projected with derivatives
             constexpr int NQW = 2 * NDV + (NV - NDV);
-            for (int w = lane; w < NQW * G * X; w += 32) {
+            const int nqw = NQW + ((PHYS == 1 && diff) ? 2 : 0);  // + base u, v values
+            for (int w = lane; w < nqw * G * X; w += 32) {
                 const int q = w / (G * X), r = w - q * (G * X), j = r / X, n = r - j * X;
                 int var, der;
                 if (q < 2 * NDV) { var = q >> 1; der = q & 1; }
@@ -193,7 +223,28 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                 const R fluxx = rho * uu[0], fluxy = rho * uu[1];
                 const R m0 = +d11 * fluxx - d01 * fluxy;
                 const R m1 = -d10 * fluxx + d00 * fluxy;
-                R c00 = uu[0] * m0, c01 = uu[0] * m1, c10 = uu[1] * m0, c11 = uu[1] * m1;
+                R c00, c01, c10, c11, uf0 = uu[0], uf1 = uu[1], qt;
+                if (diff) {
+                    R ub[2];
+                    for (int var = 0; var < 2; ++var) {
+                        const R *w0 = wk + ((5 + var) * G + j) * X;
+                        R l0 = 0;
+                        for (int n = 0; n < X; ++n) l0 += w0[n] * tb.gx[i][n];
+                        ub[var] = l0;
+                    }
+                    const R mb0 = +d11 * (rho * ub[0]) - d01 * (rho * ub[1]);
+                    const R mb1 = -d10 * (rho * ub[0]) + d00 * (rho * ub[1]);
+                    uf0 = ub[0] + uu[0];
+                    uf1 = ub[1] + uu[1];
+                    c00 = uf0 * m0 + uu[0] * mb0;
+                    c01 = uf0 * m1 + uu[0] * mb1;
+                    c10 = uf1 * m0 + uu[1] * mb0;
+                    c11 = uf1 * m1 + uu[1] * mb1;
+                    qt = ub[0] * ub[0] + ub[1] * ub[1];
+                } else {
+                    c00 = uu[0] * m0; c01 = uu[0] * m1; c10 = uu[1] * m0; c11 = uu[1] * m1;
+                    qt = uu[0] * uu[0] + uu[1] * uu[1];
+                }
                 c00 += d11 * uu[2];
                 c01 -= d10 * uu[2];
                 c10 -= d01 * uu[2];
@@ -219,7 +270,8 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                     const R f11 = (v0101 * dr[0] + v1101 * dr[1] + v0111 * ds[0] + v1111 * ds[1]);
                     PT(6)[w] = c00 + f00; PT(7)[w] = c01 + f01; PT(8)[w] = c10 + f10; PT(9)[w] = c11 + f11;
                     PT(10)[w] = f00; PT(11)[w] = f01; PT(12)[w] = f10; PT(13)[w] = f11;
-                    PT(14)[w] = uu[0]; PT(15)[w] = uu[1];
+                    PT(14)[w] = uf0; PT(15)[w] = uf1;
+                    PT(19)[w] = qt;
                 }
             } else {
                 const R *w0 = wk + (0 * G + j) * X, *w1 = wk + (1 * G + j) * X;
@@ -292,8 +344,9 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                 scatter(st.resv, st.ress, n, m, val);
             } else {
                 const size_t gi = ((size_t)tind * IM + (m - BM)) * NV + n;
-                if (beta > (R)0) st.resi[gi] = val;
-                else st.resi[gi] = val + st.rri[gi] * omb;  // res_r unchanged when beta = 0
+                const R src = st.dresi ? st.dresi[gi] : (R)0;
+                if (beta > (R)0) st.resi[gi] = val + src;
+                else st.resi[gi] = val + st.rri[gi] * omb + src;  // res_r unchanged when beta = 0
             }
         }
         if (beta > (R)0) {
@@ -338,7 +391,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                 const R nu = (R)(ph.mu / ph.rho);
                 for (int w = lane; w < GG; w += 32) {
                     const R u0 = PT(14)[w], u1 = PT(15)[w];
-                    const R q = u0 * u0 + u1 * u1;
+                    const R q = PT(19)[w];
                     const R t2 = (R)2. * nu / h;
                     R gam = (R)3.0 * q + t2 * t2;
                     if (ph.mu + ph.bd0 == 0.0) gam = (gam > (R)0.1 ? gam : (R)0.1);
@@ -415,18 +468,23 @@ __global__ void k_rsdl_pre(int nv_len, int ns_len, R *resv, R *ress, R *rrv, R *
 // Boundary-edge flux of bdry_ins::generic (hp_boundary.cpp:973-1049, ins/bdry_ins.h:35-50).
 // One thread per boundary edge.
 template <typename R, int P>
-__global__ void k_bdry_flux_ins(const DevTables<R, P> *__restrict__ tb, Mesh mesh, State<R> st, Phys ph) {
+__global__ void k_bdry_flux_ins(const DevTables<R, P> *__restrict__ tb, Mesh mesh, State<R> st, Phys ph, int diff) {
     constexpr int G = P + 1, X = P + 2, SM = P - 1, NV = 3;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= mesh.nbseg) return;
     if ((mesh.bkind[e] & (0xF << 8)) != (1 << 8)) return;
     const int sind = mesh.bseg[e];
     const int v0 = mesh.seg_pnt[2 * sind], v1 = mesh.seg_pnt[2 * sind + 1];
-    R lin[NV][SM + 2];
+    R lin[NV][SM + 2], linb[2][SM + 2];
     for (int n = 0; n < NV; ++n) {
         lin[n][0] = st.ugv[v0 * NV + n];
         lin[n][1] = st.ugv[v1 * NV + n];
         for (int m = 0; m < SM; ++m) lin[n][m + 2] = st.ugs[(sind * SM + m) * NV + n];
+    }
+    for (int n = 0; n < 2; ++n) {
+        linb[n][0] = diff ? st.ubv[v0 * NV + n] : (R)0;
+        linb[n][1] = diff ? st.ubv[v1 * NV + n] : (R)0;
+        for (int m = 0; m < SM; ++m) linb[n][m + 2] = diff ? st.ubs[(sind * SM + m) * NV + n] : (R)0;
     }
     const R xa = (R)mesh.pnts[2 * v0], ya = (R)mesh.pnts[2 * v0 + 1];
     const R xb = (R)mesh.pnts[2 * v1], yb = (R)mesh.pnts[2 * v1 + 1];
@@ -448,9 +506,22 @@ __global__ void k_bdry_flux_ins(const DevTables<R, P> *__restrict__ tb, Mesh mes
         }
         R flx[NV];
         flx[2] = (R)ph.rho * (u[0] * nrm0 + u[1] * nrm1);
-        const R pb = (R)mesh.bpibc[e * G + k];
-        flx[0] = flx[2] * u[0] + pb * nrm0;
-        flx[1] = flx[2] * u[1] + pb * nrm1;
+        if (diff) {
+            // F(b+d) - F(b) = rho (d.n)(b+d) + rho (b.n) d ; the boundary pressure cancels
+            R ub[2];
+            for (int n = 0; n < 2; ++n) {
+                R l0 = linb[n][0] * tb->gx[k][1] + linb[n][1] * tb->gx[k][2];
+                for (int m = 2; m < SM + 2; ++m) l0 += linb[n][m] * tb->gx[k][m + 1];
+                ub[n] = l0;
+            }
+            const R mb = (R)ph.rho * (ub[0] * nrm0 + ub[1] * nrm1);
+            flx[0] = flx[2] * (ub[0] + u[0]) + mb * u[0];
+            flx[1] = flx[2] * (ub[1] + u[1]) + mb * u[1];
+        } else {
+            const R pb = (R)mesh.bpibc[e * G + k];
+            flx[0] = flx[2] * u[0] + pb * nrm0;
+            flx[1] = flx[2] * u[1] + pb * nrm1;
+        }
         for (int n = 0; n < NV; ++n) {
             const R r = flx[n] * jcb;
             acc[n][0] += tb->gxwtx[1][k] * r;
@@ -482,14 +553,15 @@ __global__ void k_minv_vert(Mesh mesh, State<R> st, const DevMinv<R> *__restrict
     R r[NV];
     bool active = v < mesh.npnt;
     if (active) {
-        for (int n = 0; n < NV; ++n) r[n] = st.resv[v * NV + n] + (fold ? st.rrv[v * NV + n] : (R)0);
+        for (int n = 0; n < NV; ++n)
+            r[n] = st.resv[v * NV + n] + (fold ? st.rrv[v * NV + n] : (R)0) + (st.dresv ? st.dresv[v * NV + n] : (R)0);
         for (int q = mesh.vs_ptr[v]; q < mesh.vs_ptr[v + 1]; ++q) {
             const int code = mesh.vs_idx[q], s = code >> 1, end = code & 1;
             for (int k = 0; k < sm; ++k) {
                 const R f = mt->sfmv[end][k];
                 for (int n = 0; n < NV; ++n) {
                     const int gi = (s * sm + k) * NV + n;
-                    r[n] -= f * (st.ress[gi] + (fold ? st.rrs[gi] : (R)0));
+                    r[n] -= f * (st.ress[gi] + (fold ? st.rrs[gi] : (R)0) + (st.dress ? st.dress[gi] : (R)0));
                 }
             }
         }
@@ -535,7 +607,7 @@ __global__ void k_minv_side(Mesh mesh, State<R> st, const DevMinv<R> *__restrict
         for (int k = 0; k < SM; ++k)
             for (int n = 0; n < NV; ++n) {
                 const int gi = (s * SM + k) * NV + n;
-                r[k][n] = st.ress[gi] + (fold ? st.rrs[gi] : (R)0);
+                r[k][n] = st.ress[gi] + (fold ? st.rrs[gi] : (R)0) + (st.dress ? st.dress[gi] : (R)0);
             }
     } else {
         for (int k = mode; k < SM; ++k)
@@ -813,4 +885,36 @@ __global__ void k_hist_advance(unsigned long long *slot, double *hist, int *it, 
     }
 }
 
+// Conversions for the correction form: lo = (lo_t) hi ; hi += (hi_t) lo
+template <typename A, typename B>
+__global__ void k_convert(long n, const A *src, B *dst) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) dst[k] = (B)src[k];
+}
+template <typename A, typename B>
+__global__ void k_add_into(long n, const A *src, B *dst) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) dst[k] += (B)src[k];
+}
+
+}  // namespace hpb
+
+namespace hpb {
+// Zeroes the essential (Dirichlet) components of an unpreconditioned residual,
+// the rows that vdirichlet/sdirichlet replace by the boundary condition
+// (hp_boundary.cpp:680-704), so that its norm measures the equations solved.
+template <typename R>
+__global__ void k_mask_essential(Mesh mesh, R *resv, R *ress, int NV, int sm) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < mesh.npnt) {
+        const int e = mesh.vess[k];
+        if (e)
+            for (int n = 0; n < NV; ++n)
+                if (e & (1 << n)) resv[k * NV + n] = (R)0;
+    } else if (k < mesh.npnt + mesh.nseg && sm > 0) {
+        const int s = k - mesh.npnt, e = mesh.sess[s];
+        if (e)
+            for (int m = 0; m < sm; ++m)
+                for (int n = 0; n < NV; ++n)
+                    if (e & (1 << n)) ress[(s * sm + m) * NV + n] = (R)0;
+    }
+}
 }  // namespace hpb

@@ -113,6 +113,9 @@ def lib():
         L.hp_gpu_iterate.argtypes = [P, _I, _I, P]
         L.hp_gpu_maxres.argtypes = [P, P, P]
         L.hp_gpu_resnorm.argtypes = [P, P, P]
+        L.hp_gpu_fp32_updates.argtypes = [P, _I]
+        L.hp_gpu_solve.argtypes = [P, _I, _D, _I, _I, _I, _I, P, _I, ctypes.POINTER(_I), ctypes.POINTER(_D),
+                                   ctypes.POINTER(_I)]
         L.hp_gpu_last_error.restype = ctypes.c_char_p
         L.hp_field_eval.argtypes = [ctypes.POINTER(Field), _I, _D, _D, P]
         L.hp_tobasis.argtypes = [ctypes.POINTER(BasisTables), ctypes.POINTER(MeshDesc), _I, ctypes.POINTER(Field),

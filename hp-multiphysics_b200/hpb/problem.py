@@ -236,6 +236,16 @@ class GPULevel:
         L.check(self.lib.hp_gpu_maxres(self.h, L.ptr(out), ctypes.byref(mx)), "maxres")
         return mx.value, out
 
+    def solve(self, mixed=False, drop=1e-10, max_updates=20000, inner=20, check_every=10, prcn_every=0):
+        """hp_gpu_solve: smooth until ||R64|| drops by `drop`. Returns (hist, seconds, updates)."""
+        cap = max_updates // max(1, min(inner, check_every)) + 4
+        hist = np.zeros(cap)
+        nh = ctypes.c_int(); sec = ctypes.c_double(); nup = ctypes.c_int()
+        L.check(self.lib.hp_gpu_solve(self.h, 1 if mixed else 0, drop, max_updates, inner, check_every, prcn_every,
+                                      L.ptr(hist), cap, ctypes.byref(nh), ctypes.byref(sec), ctypes.byref(nup)),
+                "solve")
+        return hist[:nh.value], sec.value, nup.value
+
     def resnorm(self):
         l2 = ctypes.c_double(); li = ctypes.c_double()
         L.check(self.lib.hp_gpu_resnorm(self.h, ctypes.byref(l2), ctypes.byref(li)), "resnorm")
@@ -274,11 +284,13 @@ def lid_cavity_ins(n=64, p=4, re=400.0, noise=1e-3, seed=20261206, **kw):
     return prob.tobasis(noise=noise, seed=seed)
 
 
-def cd_sinsin(mesh=None, n=64, p=4, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205, **kw):
+def cd_sinsin(mesh=None, n=64, p=4, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205, field=None, **kw):
     """Scalar convection-diffusion, velocity (ax, ay), diffusivity kcond, Dirichlet data
-    sin(pi x) sin(pi y) on every boundary edge, initial state the same field plus noise."""
+    sin(pi x) sin(pi y) on every boundary edge (or `field`), initial state the same
+    field plus noise."""
     mesh = mesh if mesh is not None else square_mesh(n)
-    field = L.Field(L.HP_FIELD_SINSIN, (ctypes.c_double * 4)(1.0, 0, 0, 0))
+    if field is None:
+        field = L.Field(L.HP_FIELD_SINSIN, (ctypes.c_double * 4)(1.0, 0, 0, 0))
     bc = [(mesh.boundary_segments(), 0b1)]
     prob = Problem(mesh, p, L.HP_PHYS_CD, rhocv=1.0, kcond=kcond, ax=ax, ay=ay, field=field, bc=bc, **kw)
     return prob.tobasis(noise=noise, seed=seed)

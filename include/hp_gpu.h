@@ -187,6 +187,28 @@ int hp_gpu_enqueue_update(hp_gpu_ctx *ctx);
  * nstage.cpp:52-73: ugtouht, element_rsdl, lftog), for timing it in isolation. */
 int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *ctx, int stage);
 
+/* Convergence driver. Runs smoothing until the unpreconditioned FP64 residual
+ * norm ||R64(u)||_2 (all v/s/i modes of rsdl(nstage), without the rows of
+ * essential boundary values, which the boundary condition replaces) has dropped by `drop` from
+ * its value at entry, or `max_updates` multistage updates have run.
+ *   mode HP_PREC_FP64: plain FP64 update() sweeps, the norm checked every
+ *     `check_every` updates (block::cycle with itercrsn sweeps, blocks.cpp:1267).
+ *   mode HP_PREC_FP32: defect correction. Each cycle takes the FP64 residual
+ *     R64(u) as the source of an FP32 smoother that runs `inner` multistage
+ *     updates on a correction d about the base u, with the residual in correction
+ *     form R(u + d) - R(u) + R64(u) (the coarse-level source of mg_source,
+ *     nstage.cpp:113-129); then u += d in FP64 and R64(u) is evaluated again.
+ * setup_preconditioner() runs at entry and every `prcn_every` checks (0: once).
+ * hist[0..*n_hist) receives ||R64|| / ||R64(entry)|| at every check; *seconds is
+ * the device time of the whole solve (CUDA events), *updates the updates run. */
+int hp_gpu_solve(hp_gpu_ctx *ctx, int mode, double drop, int max_updates, int inner, int check_every,
+                 int prcn_every, double *hist, int hist_cap, int *n_hist, double *seconds, int *updates);
+
+/* Diagnostic: n multistage updates of the FP32 smoother in plain form, from
+ * fp32(u), written back to the FP64 state (compares the FP32 kernels with the
+ * FP64 ones update by update). Needs setup_preconditioner() first. */
+int hp_gpu_fp32_updates(hp_gpu_ctx *ctx, int n);
+
 /* Synchronises the context's stream and returns the first sticky error. */
 int hp_gpu_sync(hp_gpu_ctx *ctx);
 
