@@ -122,6 +122,72 @@ def run_cpu(cores, secs, n=60):
     return dof / el / 1e9, n
 
 
+TOL_N = 64
+
+
+def time_to_tolerance(hpb, dev):
+    """Time to a 1e-10 drop of the FP64 residual norm (Dirichlet rows excluded), plain
+    FP64 smoothing against FP32 correction smoothing with FP64 defect correction, on
+    cd p=4 with Dirichlet data -(x-8)^2 on a 64x64 split-square mesh (a size the
+    single-grid smoother converges on in a few thousand updates). Device time of the
+    whole solve (hp_gpu_solve), residual checks included."""
+    import ctypes as C
+    import numpy as np
+    from hpb import _lib as L
+    out = {"workload": f"tri_hp cd p={P}, {TOL_N}x{TOL_N} split-square mesh ({2 * TOL_N * TOL_N} triangles), "
+                       "velocity (1,0.5), kcond 1e-3, Dirichlet -(x-8)^2, cfl 0.5, noise 1e-3",
+           "drop": 1e-10, "criterion": "||R64||_2 / ||R64(u0)||_2 over all non-Dirichlet v/s/i rows"}
+    states = {}
+    for name, mixed in (("fp64", False), ("fp32_defect_correction", True)):
+        f = L.Field(L.HP_FIELD_QUADX, (C.c_double * 4)(-1.0, 8.0, 0, 0))
+        pr = hpb.cd_sinsin(n=TOL_N, p=P, kcond=1e-3, cfl=0.5, field=f, noise=1e-3, seed=20261205)
+        g = pr.gpu(device=dev)
+        hist, sec, upd = g.solve(mixed=mixed, drop=1e-10, max_updates=20000, inner=20, check_every=20)
+        states[name] = g.state()
+        out[name] = {"seconds": sec, "updates": upd, "final_drop": float(hist[-1]),
+                     "reached": bool(hist[-1] <= 1e-10)}
+        g.close()
+    # learned + FP32: a network trained on the GPU from the solver's own residual
+    # histories of 4 other instances of the same family (random velocity and
+    # diffusivity), then attached to the FP32 defect-correction solve
+    import time as _t
+    from hpb import learned as LR
+    t0 = _t.perf_counter()
+    F, T = [], []
+    for s in range(4):
+        r = np.random.default_rng(300 + s)
+        ax, ay = r.uniform(-1, 1, 2)
+        kc = 10 ** r.uniform(-3, -1.5)
+        f = L.Field(L.HP_FIELD_QUADX, (C.c_double * 4)(-1.0, 8.0, 0, 0))
+        fs, ts = LR.solver_samples(lambda: hpb.cd_sinsin(n=TOL_N, p=P, ax=ax, ay=ay, kcond=kc, cfl=0.5, field=f,
+                                                         noise=1e-3, seed=300 + s))
+        F.append(fs)
+        T.append(ts)
+    net, hist = LR.train(np.concatenate(F), np.concatenate(T), steps=400)
+    train_s = _t.perf_counter() - t0
+    f = L.Field(L.HP_FIELD_QUADX, (C.c_double * 4)(-1.0, 8.0, 0, 0))
+    pr = hpb.cd_sinsin(n=TOL_N, p=P, kcond=1e-3, cfl=0.5, field=f, noise=1e-3, seed=20261205)
+    g = pr.gpu(device=dev)
+    LR.attach(g, net, 1.0)
+    hist_l, sec, upd = g.solve(mixed=True, drop=1e-10, max_updates=20000, inner=20, check_every=20)
+    states["learned_fp32"] = g.state()
+    out["learned_fp32"] = {"seconds": sec, "updates": upd, "final_drop": float(hist_l[-1]),
+                           "reached": bool(hist_l[-1] <= 1e-10), "training_seconds_offline": train_s,
+                           "network": "17-64-64-64-1 BF16, FP32 accumulation, 400 Adam steps"}
+    g.close()
+    net.close()
+    out["speedup_learned_fp32_vs_fp64"] = out["fp64"]["seconds"] / out["learned_fp32"]["seconds"]
+    a = states["fp64"]
+    c_ = states["learned_fp32"]
+    out["rel_l2_state_diff_learned"] = float(np.sqrt(sum(np.sum((x - y) ** 2) for x, y in zip(a, c_))) /
+                                             np.sqrt(sum(np.sum(x * x) for x in a)))
+    a, b = states["fp64"], states["fp32_defect_correction"]
+    out["rel_l2_state_diff"] = float(np.sqrt(sum(np.sum((x - y) ** 2) for x, y in zip(a, b))) /
+                                     np.sqrt(sum(np.sum(x * x) for x in a)))
+    out["speedup_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_defect_correction"]["seconds"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -258,6 +324,7 @@ def main():
 
     ndof = pr.ndof
     m = pr.mesh
+    tol = time_to_tolerance(hpb, dev)
     if dist:
         t = torch.tensor([t_ms, e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -295,6 +362,7 @@ def main():
         "e2e": {"value": e2e, "unit": "GDoF/s", "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
         "gpu_launches": launches_per_step * args.steps,
         "update_ms": u_ms, "update_gdofs_per_stage": ndof * ns / (u_ms * 1e-3) / 1e9,
+        "time_to_tol": tol,
         "ndof": ndof, "clocks": clocks,
     }
     print(json.dumps(line))

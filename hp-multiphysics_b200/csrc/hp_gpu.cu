@@ -10,6 +10,7 @@
 #include <algorithm>
 
 #include "hp_gpu.h"
+#include "hp_mlp.h"
 #include "hp_kernels.cuh"
 
 using namespace hpb;
@@ -193,15 +194,15 @@ static bool get_launchers(int p, int phys, Launchers<R> &L) {
 
 // FP64 preconditioner set-up kernel launch (double only)
 static void launch_prcn(int p, int phys, const void *tab, const Mesh &m, const State<double> &s, const Phys &ph,
-                        int *err, cudaStream_t st) {
+                        int *err, const float *lsc, int ld, float clampv, cudaStream_t st) {
 #define PR_CASE(PP)                                                                                           \
     case PP:                                                                                                  \
         if (phys)                                                                                             \
             k_prcn_elem<double, PP, 1><<<nblk(m.ntri, 128), 128, 0, st>>>(                                      \
-                reinterpret_cast<const DevTables<double, PP> *>(tab), m, s, ph, err);                         \
+                reinterpret_cast<const DevTables<double, PP> *>(tab), m, s, ph, err, lsc, ld, clampv);        \
         else                                                                                                  \
             k_prcn_elem<double, PP, 0><<<nblk(m.ntri, 128), 128, 0, st>>>(                                      \
-                reinterpret_cast<const DevTables<double, PP> *>(tab), m, s, ph, err);                         \
+                reinterpret_cast<const DevTables<double, PP> *>(tab), m, s, ph, err, lsc, ld, clampv);        \
         break;
     switch (p) { PR_CASE(1) PR_CASE(2) PR_CASE(3) PR_CASE(4) PR_CASE(5) PR_CASE(6) PR_CASE(7) PR_CASE(8) }
 #undef PR_CASE
@@ -223,6 +224,12 @@ struct hp_gpu_ctx {
     DevMinv<double> *d_minv = nullptr;
     DevMinv<float> *d_minv32 = nullptr;
     cudaGraphExec_t g_update32 = nullptr;
+    // learned preconditioner correction
+    const float *lsc = nullptr;
+    int lsc_ld = 1;
+    float lsc_clamp = 0.f;
+    hp_mlp *net = nullptr;
+    float *d_feat = nullptr, *d_netout = nullptr;
     double vdiag = 0.0;
     unsigned long long *d_slot = nullptr;
     double *d_hist = nullptr;
@@ -583,7 +590,17 @@ extern "C" int hp_gpu_setup_preconditioner(hp_gpu_ctx *c) {
     CK(cudaMemsetAsync(c->st.vprcn, 0, (size_t)c->npnt * c->NV * 8, c->stream));
     CK(cudaMemsetAsync(c->st.sprcn, 0, (size_t)c->nseg * c->NV * 8, c->stream));
     CK(cudaMemsetAsync(c->d_err, 0, 4, c->stream));
-    launch_prcn(c->p, c->ph.physics, c->d_tab, c->mesh, c->st, c->ph, c->d_err, c->stream);
+    if (c->net) {
+        int r0 = hp_gpu_elem_features(c, c->d_feat);
+        if (r0) return r0;
+        if (hp_mlp_forward(c->net, c->d_feat, c->ntri, c->d_netout, c->stream)) {
+            set_err("network forward failed: %s", hp_mlp_last_error());
+            return HP_ECUDA;
+        }
+        c->lsc = c->d_netout;
+    }
+    launch_prcn(c->p, c->ph.physics, c->d_tab, c->mesh, c->st, c->ph, c->d_err, c->lsc, c->lsc_ld, c->lsc_clamp,
+                c->stream);
     const int nv = c->npnt * c->NV, ns = (c->p > 1 ? c->nseg * c->NV : 0);
     k_prcn_invert<double><<<nblk(nv + ns, 256), 256, 0, c->stream>>>(nv, ns, c->st.vprcn, c->st.sprcn, c->vdiag);
     int r = check_launch(c);
@@ -883,4 +900,46 @@ extern "C" int hp_gpu_fp32_updates(hp_gpu_ctx *c, int n) {
     conv(c, (long)c->li, (const float *)f.ugi, c->st.ugi);
     if ((r = check_launch(c))) return r;
     return hp_gpu_sync(c);
+}
+
+// ---------------------------------------------------------------------------
+// Learned preconditioner hooks (include/hp_mlp.h)
+// ---------------------------------------------------------------------------
+extern "C" int hp_gpu_elem_features(hp_gpu_ctx *c, float *d_feat) {
+    if (!c || !d_feat) return HP_EINVAL;
+    k_elem_features<<<nblk(c->ntri, 128), 128, 0, c->stream>>>(c->mesh, c->st, c->ph, c->NV, c->sm, c->im, c->p, d_feat);
+    return check_launch(c);
+}
+
+extern "C" int hp_gpu_elem_resnorm(hp_gpu_ctx *c, double *d_out) {
+    if (!c || !d_out) return HP_EINVAL;
+    k_elem_resnorm<<<nblk(c->ntri, 128), 128, 0, c->stream>>>(c->mesh, c->st, c->NV, c->sm, c->im, d_out);
+    return check_launch(c);
+}
+
+extern "C" int hp_gpu_set_prcn_scale(hp_gpu_ctx *c, const float *d_logscale, int ld, float clampv) {
+    if (!c || (d_logscale && ld < 1)) return HP_EINVAL;
+    c->lsc = d_logscale;
+    c->lsc_ld = ld < 1 ? 1 : ld;
+    c->lsc_clamp = clampv;
+    c->net = nullptr;
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_set_prcn_net(hp_gpu_ctx *c, hp_mlp *net, float clampv) {
+    if (!c) return HP_EINVAL;
+    if (!net) {
+        c->net = nullptr;
+        c->lsc = nullptr;
+        return HP_OK;
+    }
+    int nin = 0, nout = 0;
+    if (hp_mlp_dims(net, &nin, &nout) || nin != HP_NFEAT) { set_err("network must take %d inputs", HP_NFEAT); return HP_EINVAL; }
+    int r;
+    if (!c->d_feat && (r = dalloc(c, (void **)&c->d_feat, (size_t)c->ntri * HP_NFEAT * 4))) return r;
+    if (!c->d_netout && (r = dalloc(c, (void **)&c->d_netout, (size_t)c->ntri * 64 * 4))) return r;
+    c->net = net;
+    c->lsc_ld = nout;
+    c->lsc_clamp = clampv;
+    return HP_OK;
 }

@@ -731,7 +731,8 @@ __global__ void k_minv_int(Mesh mesh, State<R> st, const DevMinv<R> *__restrict_
 // cd/setup_preconditioner.cpp:6-97) with tau, scatter to vprcn/sprcn.
 // ---------------------------------------------------------------------------
 template <typename R, int P, int PHYS>
-__global__ void k_prcn_elem(const DevTables<R, P> *__restrict__ tb, Mesh mesh, State<R> st, Phys ph, int *err) {
+__global__ void k_prcn_elem(const DevTables<R, P> *__restrict__ tb, Mesh mesh, State<R> st, Phys ph, int *err,
+                            const float *__restrict__ lsc, int ld, float clampv) {
     constexpr int G = P + 1, X = P + 2, T = (P + 1) * (P + 2) / 2, SM = P - 1, BM = 3 * P, NV = (PHYS == 1 ? 3 : 1);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= mesh.ntri) return;
@@ -813,6 +814,14 @@ __global__ void k_prcn_elem(const DevTables<R, P> *__restrict__ tb, Mesh mesh, S
         tp[0] = ph.rho * jcb;
         tp[1] = ph.rho * jcb;
         tp[2] = jcb / gam;
+    }
+    if (lsc) {  // learned per-element correction (include/hp_mlp.h)
+        for (int n = 0; n < NV; ++n) {
+            float sc = lsc[(size_t)t * ld + (n < ld ? n : ld - 1)];
+            sc = sc > clampv ? clampv : (sc < -clampv ? -clampv : sc);
+            if (!(sc == sc)) sc = 0.f;
+            tp[n] *= exp((double)sc);
+        }
     }
     for (int n = 0; n < NV; ++n) st.tprcn[t * NV + n] = (R)tp[n];
     for (int i = 0; i < 3; ++i) {
@@ -916,5 +925,69 @@ __global__ void k_mask_essential(Mesh mesh, R *resv, R *ress, int NV, int sm) {
                 for (int n = 0; n < NV; ++n)
                     if (e & (1 << n)) ress[(s * sm + m) * NV + n] = (R)0;
     }
+}
+}  // namespace hpb
+
+namespace hpb {
+// Element features of the learned preconditioner (see include/hp_mlp.h).
+__global__ void k_elem_features(Mesh mesh, State<double> st, Phys ph, int NV, int sm, int im, int p, float *feat) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= mesh.ntri) return;
+    float *f = feat + (size_t)t * 17;
+    const int v[3] = {mesh.tri_pnt[3 * t], mesh.tri_pnt[3 * t + 1], mesh.tri_pnt[3 * t + 2]};
+    double vmax_q = 0.0;
+    for (int n = 0; n < 3; ++n) {
+        if (n >= NV) { f[4 * n] = f[4 * n + 1] = f[4 * n + 2] = f[4 * n + 3] = 0.f; continue; }
+        double a = st.ugv[v[0] * NV + n], b = st.ugv[v[1] * NV + n], c = st.ugv[v[2] * NV + n];
+        double mx = fmax(a, fmax(b, c)), mn = fmin(a, fmin(b, c));
+        double ss = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            const int s = mesh.tri_seg[3 * t + i];
+            for (int m = 0; m < sm; ++m) { const double x = st.ugs[(s * sm + m) * NV + n]; ss += x * x; }
+        }
+        double si = 0.0;
+        for (int k = 0; k < im; ++k) { const double x = st.ugi[((size_t)t * im + k) * NV + n]; si += x * x; }
+        f[4 * n] = (float)((a + b + c) / 3.0);
+        f[4 * n + 1] = (float)(mx - mn);
+        f[4 * n + 2] = (float)(sm > 0 ? sqrt(ss / (3.0 * sm)) : 0.0);
+        f[4 * n + 3] = (float)(im > 0 ? sqrt(si / im) : 0.0);
+    }
+    if (ph.physics == 1) {
+        for (int i = 0; i < 3; ++i) {
+            const double u = st.ugv[v[i] * NV], w = st.ugv[v[i] * NV + 1];
+            vmax_q = fmax(vmax_q, sqrt(u * u + w * w));
+        }
+    } else {
+        vmax_q = sqrt(ph.ax * ph.ax + ph.ay * ph.ay);
+    }
+    const double px[3] = {mesh.pnts[2 * v[0]], mesh.pnts[2 * v[1]], mesh.pnts[2 * v[2]]};
+    const double py[3] = {mesh.pnts[2 * v[0] + 1], mesh.pnts[2 * v[1] + 1], mesh.pnts[2 * v[2] + 1]};
+    const double area2 = (px[0] - px[2]) * (py[1] - py[0]) - (py[0] - py[2]) * (px[1] - px[0]);
+    double h2 = 0.0;
+    for (int j = 0; j < 3; ++j) {
+        const double ex = px[j] - px[(j + 1) % 3], ey = py[j] - py[(j + 1) % 3];
+        h2 = fmax(h2, ex * ex + ey * ey);
+    }
+    const double nu = ph.physics == 1 ? ph.mu / ph.rho : ph.kcond / ph.rhocv;
+    f[12] = (float)log(0.25 * fabs(area2) + 1e-300);
+    f[13] = (float)(0.5 * log(h2 + 1e-300));
+    f[14] = (float)(h2 / (fabs(area2) + 1e-300));
+    f[15] = (float)log1p(vmax_q * sqrt(h2) / (nu > 0 ? nu : 1e-300));
+    f[16] = (float)p / 8.0f;
+}
+
+// Sum of squares of an element's own residual coefficients (vertex, side, interior).
+__global__ void k_elem_resnorm(Mesh mesh, State<double> st, int NV, int sm, int im, double *out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= mesh.ntri) return;
+    double s2 = 0.0;
+    for (int i = 0; i < 3; ++i) {
+        const int v = mesh.tri_pnt[3 * t + i], s = mesh.tri_seg[3 * t + i];
+        for (int n = 0; n < NV; ++n) { const double x = st.resv[v * NV + n]; s2 += x * x; }
+        for (int m = 0; m < sm; ++m)
+            for (int n = 0; n < NV; ++n) { const double x = st.ress[(s * sm + m) * NV + n]; s2 += x * x; }
+    }
+    for (int k = 0; k < im * NV; ++k) { const double x = st.resi[(size_t)t * im * NV + k]; s2 += x * x; }
+    out[t] = s2;
 }
 }  // namespace hpb
