@@ -242,6 +242,15 @@ struct hp_gpu_ctx {
     cudaGraphExec_t g_update = nullptr;  // one update() incl. maxres -> hist slot advance
     bool prcn_ready = false;
     size_t lv = 0, ls = 0, li = 0;  // element counts of v/s/i arrays
+    // multigrid: this context as a coarse level of `fine` (tri_hp's coarse/fine pointers)
+    hp_gpu_ctx *fine = nullptr;
+    int mg_kind = 0;  // 0 none, 1 p-level on the same mesh, 2 h-level (coarser mesh, p = 1)
+    double fadd = 1.0;
+    double *res0v = nullptr, *res0s = nullptr, *res0i = nullptr;  // restricted fine residual
+    double *uc0v = nullptr, *uc0s = nullptr, *uc0i = nullptr;     // state at restriction (vug_frst)
+    double *fasv = nullptr, *fass = nullptr, *fasi = nullptr;     // FAS source dres
+    int *f2c_tri = nullptr, *c2f_tri = nullptr;
+    double *f2c_wt = nullptr, *c2f_wt = nullptr;
 };
 
 static int dalloc(hp_gpu_ctx *c, void **p, size_t bytes) {
@@ -565,7 +574,7 @@ extern "C" int hp_gpu_enqueue_rsdl(hp_gpu_ctx *c, int stage) {
     // already folded the interiors, fold vertices and sides here for the caller
     const long n = (long)(c->lv + c->ls);
     k_rsdl_fold<double><<<nblk(n, 256), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, c->st.resv, c->st.rrv, c->st.ress,
-                                                             c->st.rrs);
+                                                             c->st.rrs, c->st.dresv, c->st.dress);
     return check_launch(c);
 }
 
@@ -942,4 +951,214 @@ extern "C" int hp_gpu_set_prcn_net(hp_gpu_ctx *c, hp_mlp *net, float clampv) {
     c->lsc_ld = nout;
     c->lsc_clamp = clampv;
     return HP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid (tri_hp::mg_restrict / mg_prolongate / mg_source and block::cycle)
+// ---------------------------------------------------------------------------
+static int mg_alloc(hp_gpu_ctx *c) {
+    int r;
+    const size_t lv = std::max<size_t>(c->lv, 1), ls = std::max<size_t>(c->ls, 1), li = std::max<size_t>(c->li, 1);
+    double **v[] = {&c->res0v, &c->uc0v, &c->fasv};
+    double **s[] = {&c->res0s, &c->uc0s, &c->fass};
+    double **i[] = {&c->res0i, &c->uc0i, &c->fasi};
+    for (auto q : v) if (!*q && (r = dalloc(c, (void **)q, lv * 8))) return r;
+    for (auto q : s) if (!*q && (r = dalloc(c, (void **)q, ls * 8))) return r;
+    for (auto q : i) if (!*q && (r = dalloc(c, (void **)q, li * 8))) return r;
+    CK(cudaMemsetAsync(c->fasv, 0, lv * 8, c->stream));
+    CK(cudaMemsetAsync(c->fass, 0, ls * 8, c->stream));
+    CK(cudaMemsetAsync(c->fasi, 0, li * 8, c->stream));
+    // the source enters every stage residual of this level (captured into its update graph)
+    c->st.dresv = c->fasv;
+    c->st.dress = c->ls ? c->fass : nullptr;
+    c->st.dresi = c->li ? c->fasi : nullptr;
+    if (c->g_update) {
+        cudaGraphExecDestroy(c->g_update);
+        c->g_update = nullptr;
+    }
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_mg_attach_p(hp_gpu_ctx *coarse, hp_gpu_ctx *fine, double fadd) {
+    if (!coarse || !fine || coarse == fine) return HP_EINVAL;
+    if (coarse->npnt != fine->npnt || coarse->nseg != fine->nseg || coarse->ntri != fine->ntri ||
+        coarse->NV != fine->NV || coarse->p >= fine->p) {
+        set_err("p-level must share the mesh and physics of its fine level and have a lower p");
+        return HP_EINVAL;
+    }
+    coarse->fine = fine;
+    coarse->mg_kind = 1;
+    coarse->fadd = fadd;
+    return mg_alloc(coarse);
+}
+
+extern "C" int hp_gpu_mg_attach_h(hp_gpu_ctx *coarse, hp_gpu_ctx *fine, const int *f2c_tri, const double *f2c_wt,
+                                  const int *c2f_tri, const double *c2f_wt, double fadd) {
+    if (!coarse || !fine || !f2c_tri || !f2c_wt || !c2f_tri || !c2f_wt) return HP_EINVAL;
+    if (coarse->p != 1 || coarse->NV != fine->NV) {
+        set_err("h-level must be p = 1 with the physics of its fine level");
+        return HP_EINVAL;
+    }
+    for (int i = 0; i < fine->npnt; ++i)
+        if (f2c_tri[i] < 0 || f2c_tri[i] >= coarse->ntri) { set_err("f2c_tri out of range"); return HP_EINVAL; }
+    for (int i = 0; i < coarse->npnt; ++i)
+        if (c2f_tri[i] < 0 || c2f_tri[i] >= fine->ntri) { set_err("c2f_tri out of range"); return HP_EINVAL; }
+    int r;
+    if ((r = upload(coarse, &coarse->f2c_tri, f2c_tri, (size_t)fine->npnt))) return r;
+    if ((r = upload(coarse, &coarse->f2c_wt, f2c_wt, (size_t)fine->npnt * 3))) return r;
+    if ((r = upload(coarse, &coarse->c2f_tri, c2f_tri, (size_t)coarse->npnt))) return r;
+    if ((r = upload(coarse, &coarse->c2f_wt, c2f_wt, (size_t)coarse->npnt * 3))) return r;
+    coarse->fine = fine;
+    coarse->mg_kind = 2;
+    coarse->fadd = fadd;
+    return mg_alloc(coarse);
+}
+
+// Transfers the fine level's current full residual (rsdl(nstage), folded) and
+// state to this coarse level and sets its FAS source.
+static int mg_restrict_enqueue(hp_gpu_ctx *c) {
+    hp_gpu_ctx *f = c->fine;
+    if (!f || !c->mg_kind) { set_err("not a coarse level"); return HP_ESTATE; }
+    // both levels run on the fine level's stream order: make the coarse stream wait
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, f->stream));
+    CK(cudaStreamWaitEvent(c->stream, ev, 0));
+    cudaEventDestroy(ev);
+    const int NV = c->NV;
+    if (c->mg_kind == 1) {
+        const long tot = (long)(c->lv + c->ls + c->li);
+        const int g = std::min(nblk(tot, 256), c->nsm * 8);
+        k_mg_truncate<<<g, 256, 0, c->stream>>>(c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im, f->st.resv,
+                                                f->st.ress, f->st.resi, c->res0v, c->res0s, c->res0i);
+        k_mg_truncate<<<g, 256, 0, c->stream>>>(c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im, f->st.ugv,
+                                                f->st.ugs, f->st.ugi, c->st.ugv, c->st.ugs, c->st.ugi);
+        CK(cudaMemcpyAsync(c->uc0v, c->st.ugv, c->lv * 8, cudaMemcpyDeviceToDevice, c->stream));
+        if (c->ls) CK(cudaMemcpyAsync(c->uc0s, c->st.ugs, c->ls * 8, cudaMemcpyDeviceToDevice, c->stream));
+        if (c->li) CK(cudaMemcpyAsync(c->uc0i, c->st.ugi, c->li * 8, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        CK(cudaMemsetAsync(c->res0v, 0, c->lv * 8, c->stream));
+        k_mg_restrict_hres<<<nblk(f->npnt, 128), 128, 0, c->stream>>>(f->npnt, NV, c->f2c_tri, c->f2c_wt,
+                                                                        c->mesh.tri_pnt, f->st.resv, c->res0v);
+        k_mg_restrict_hstate<<<nblk(c->npnt, 128), 128, 0, c->stream>>>(c->npnt, NV, c->c2f_tri, c->c2f_wt,
+                                                                          f->mesh.tri_pnt, f->st.ugv, c->st.ugv,
+                                                                          c->uc0v);
+    }
+    // res(first) of the coarse level without its source, then dres = fadd*res0 - res(first)
+    State<double> plain = c->st;
+    plain.dresv = plain.dress = plain.dresi = nullptr;
+    enqueue_rsdl_t<double>(c, c->L, c->d_tab, plain, c->ph, c->ph.nstage, 0);
+    const long n2 = (long)(c->lv + c->ls);
+    k_rsdl_fold<double><<<nblk(n2, 256), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, c->st.resv, c->st.rrv,
+                                                              c->st.ress, c->st.rrs, nullptr, nullptr);
+    const int g2 = c->nsm * 8;
+    k_fas_source<<<g2, 256, 0, c->stream>>>((long)c->lv, c->fadd, c->res0v, c->st.resv, c->fasv);
+    if (c->ls) k_fas_source<<<g2, 256, 0, c->stream>>>((long)c->ls, c->fadd, c->res0s, c->st.ress, c->fass);
+    if (c->li) k_fas_source<<<g2, 256, 0, c->stream>>>((long)c->li, c->fadd, c->res0i, c->st.resi, c->fasi);
+    return check_launch(c);
+}
+
+static int mg_prolong_enqueue(hp_gpu_ctx *c) {
+    hp_gpu_ctx *f = c->fine;
+    if (!f || !c->mg_kind) { set_err("not a coarse level"); return HP_ESTATE; }
+    const int NV = c->NV;
+    if (c->mg_kind == 1) {
+        const long tot = (long)(c->lv + c->ls + c->li);
+        k_mg_prolong_p<<<std::min(nblk(tot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+            c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im, c->st.ugv, c->st.ugs, c->st.ugi, c->uc0v,
+            c->uc0s, c->uc0i, f->st.ugv, f->st.ugs, f->st.ugi);
+    } else {
+        k_mg_prolong_h<<<nblk(f->npnt, 128), 128, 0, c->stream>>>(f->npnt, NV, c->f2c_tri, c->f2c_wt, c->mesh.tri_pnt,
+                                                                    c->st.ugv, c->uc0v, f->st.ugv);
+    }
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, c->stream));
+    CK(cudaStreamWaitEvent(f->stream, ev, 0));
+    cudaEventDestroy(ev);
+    return check_launch(c);
+}
+
+extern "C" int hp_gpu_mg_restrict(hp_gpu_ctx *coarse) {
+    int r = mg_restrict_enqueue(coarse);
+    if (r) return r;
+    return hp_gpu_sync(coarse);
+}
+
+extern "C" int hp_gpu_mg_prolongate(hp_gpu_ctx *coarse) {
+    int r = mg_prolong_enqueue(coarse);
+    if (r) return r;
+    return hp_gpu_sync(coarse->fine);
+}
+
+// block::cycle (tri_mesh/blocks.cpp:1267-1348) over levels[0] (finest) .. levels[n-1]
+static int cycle(hp_gpu_ctx **lv, int n, int lvl, int vw, int itercrsn, int iterrfne, int eval_prcn) {
+    hp_gpu_ctx *c = lv[lvl];
+    int r;
+    for (int vc = 0; vc < vw; ++vc) {
+        if (eval_prcn) {
+            r = hp_gpu_setup_preconditioner(c);
+            if (r) return r < 0 ? r : HP_ESTATE;
+        }
+        if ((r = ensure_update_graph(c))) return r;
+        for (int it = 0; it < itercrsn; ++it) CK(cudaGraphLaunch(c->g_update, c->stream));
+        if (lvl == n - 1) return HP_OK;
+        if ((r = hp_gpu_enqueue_rsdl(c, c->ph.nstage))) return r;
+        if ((r = mg_restrict_enqueue(lv[lvl + 1]))) return r;
+        if ((r = cycle(lv, n, lvl + 1, vw, itercrsn, iterrfne, eval_prcn))) return r;
+        if ((r = mg_prolong_enqueue(lv[lvl + 1]))) return r;
+        if (eval_prcn && iterrfne) {
+            r = hp_gpu_setup_preconditioner(c);
+            if (r) return r < 0 ? r : HP_ESTATE;
+        }
+        for (int it = 0; it < iterrfne; ++it) CK(cudaGraphLaunch(c->g_update, c->stream));
+    }
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_vcycle(hp_gpu_ctx **levels, int nlevels, int vw, int itercrsn, int iterrfne, int eval_prcn) {
+    if (!levels || nlevels < 1 || vw < 1 || itercrsn < 0 || iterrfne < 0) return HP_EINVAL;
+    for (int l = 1; l < nlevels; ++l)
+        if (!levels[l] || levels[l]->fine != levels[l - 1]) { set_err("level %d is not attached to level %d", l, l - 1); return HP_EINVAL; }
+    int r = cycle(levels, nlevels, 0, vw, itercrsn, iterrfne, eval_prcn);
+    if (r) return r;
+    return hp_gpu_sync(levels[0]);
+}
+
+extern "C" int hp_gpu_solve_mg(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
+                               int iterrfne, int prcn_every, double *hist, int hist_cap, int *n_hist,
+                               double *seconds, int *cycles) {
+    if (!levels || nlevels < 1 || drop <= 0.0 || max_cycles < 1) return HP_EINVAL;
+    hp_gpu_ctx *f = levels[0];
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, f->stream));
+    double r0 = 0.0, rn = 0.0;
+    int nh = 0, nc = 0, r;
+    r = hp_gpu_setup_preconditioner(f);
+    if (r) return r < 0 ? r : HP_ESTATE;
+    if ((r = fp64_norm(f, &r0))) return r;
+    if (hist && nh < hist_cap) hist[nh++] = 1.0;
+    while (nc < max_cycles) {
+        // every level's preconditioner is evaluated at its state on the first cycle
+        // and then every prcn_every cycles (block::cycle's evaluate_preconditioner)
+        const int eval = (nc == 0 || (prcn_every > 0 && nc % prcn_every == 0)) ? 1 : 0;
+        if ((r = cycle(levels, nlevels, 0, vw, itercrsn, iterrfne, eval))) return r;
+        ++nc;
+        if ((r = fp64_norm(f, &rn))) return r;
+        const double d = rn / r0;
+        if (hist && nh < hist_cap) hist[nh++] = d;
+        if (!(d == d) || d <= drop) break;
+    }
+    CK(cudaEventRecord(e1, f->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (n_hist) *n_hist = nh;
+    if (seconds) *seconds = ms * 1e-3;
+    if (cycles) *cycles = nc;
+    return hp_gpu_sync(f);
 }

@@ -835,10 +835,116 @@ __global__ void k_prcn_elem(const DevTables<R, P> *__restrict__ tb, Mesh mesh, S
 
 // res.{v,s} += res_r.{v,s} (nstage.cpp:76-82) for callers of the stand-alone rsdl
 template <typename R>
-__global__ void k_rsdl_fold(int n1, int n2, R *resv, const R *rrv, R *ress, const R *rrs) {
+__global__ void k_rsdl_fold(int n1, int n2, R *resv, const R *rrv, R *ress, const R *rrs, const R *dv, const R *ds) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n1) resv[k] += rrv[k];
-    else if (k < n1 + n2) ress[k - n1] += rrs[k - n1];
+    if (k < n1) resv[k] += rrv[k] + (dv ? dv[k] : (R)0);
+    else if (k < n1 + n2) ress[k - n1] += rrs[k - n1] + (ds ? ds[k - n1] : (R)0);
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid transfers (tri_hp/movco.cpp:4-106, movfin.cpp:7-82).
+// p-levels: the hierarchical basis makes the coarse modes a subset of the fine
+// ones: all vertices, the first smc side modes, interior modes (m, k) with the
+// fine index offset_f(m) + k. h-levels: barycentric weights of each point in a
+// triangle of the other mesh (tri_mesh::mgconnect, connect.cpp:49-87).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int interior_fine_index(int kc, int smc, int smf) {
+    // coarse interior index kc -> (m, k) with rows of length smc - m, m = 1..smc-1
+    int m = 1, off_c = 0, off_f = 0;
+    while (kc >= off_c + (smc - m)) {
+        off_c += smc - m;
+        off_f += smf - m;
+        ++m;
+    }
+    return off_f + (kc - off_c);
+}
+
+// dst_c = src_f restricted (truncate) ; mode 0: copy, 1: dst_c += src_f (unused)
+__global__ void k_mg_truncate(int npnt, int nseg, int ntri, int NV, int smf, int imf, int smc, int imc,
+                              const double *fv, const double *fs, const double *fi, double *cv, double *cs, double *ci) {
+    const long nv = (long)npnt * NV, ns = (long)nseg * smc * NV, ni = (long)ntri * imc * NV;
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < nv + ns + ni; k += (long)gridDim.x * blockDim.x) {
+        if (k < nv) {
+            cv[k] = fv[k];
+        } else if (k < nv + ns) {
+            const long q = k - nv;
+            const long s = q / (smc * NV), r = q - s * smc * NV, m = r / NV, n = r - m * NV;
+            cs[q] = fs[(s * smf + m) * NV + n];
+        } else {
+            const long q = k - nv - ns;
+            const long t = q / (imc * NV), r = q - t * imc * NV, kc = r / NV, n = r - kc * NV;
+            ci[q] = fi[(t * imf + interior_fine_index((int)kc, smc, smf)) * NV + n];
+        }
+    }
+}
+
+// fine low modes += (coarse state - coarse state at restriction)
+__global__ void k_mg_prolong_p(int npnt, int nseg, int ntri, int NV, int smf, int imf, int smc, int imc,
+                               const double *cv, const double *cs, const double *ci, const double *c0v,
+                               const double *c0s, const double *c0i, double *fv, double *fs, double *fi) {
+    const long nv = (long)npnt * NV, ns = (long)nseg * smc * NV, ni = (long)ntri * imc * NV;
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < nv + ns + ni; k += (long)gridDim.x * blockDim.x) {
+        if (k < nv) {
+            fv[k] += cv[k] - c0v[k];
+        } else if (k < nv + ns) {
+            const long q = k - nv;
+            const long s = q / (smc * NV), r = q - s * smc * NV, m = r / NV, n = r - m * NV;
+            fs[(s * smf + m) * NV + n] += cs[q] - c0s[q];
+        } else {
+            const long q = k - nv - ns;
+            const long t = q / (imc * NV), r = q - t * imc * NV, kc = r / NV, n = r - kc * NV;
+            fi[(t * imf + interior_fine_index((int)kc, smc, smf)) * NV + n] += ci[q] - c0i[q];
+        }
+    }
+}
+
+// h restriction of the vertex residual: res0_c(v0) += wt * res_f(i) over fine vertices i
+__global__ void k_mg_restrict_hres(int nfine, int NV, const int *f2c_tri, const double *f2c_wt, const int *ctri_pnt,
+                                   const double *resf, double *res0c) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfine) return;
+    const int t = f2c_tri[i];
+    for (int j = 0; j < 3; ++j) {
+        const int v0 = ctri_pnt[3 * t + j];
+        const double w = f2c_wt[3 * i + j];
+        for (int n = 0; n < NV; ++n) atomicAdd(&res0c[v0 * NV + n], w * resf[i * NV + n]);
+    }
+}
+
+// h interpolation of the vertex state: u_c(i) = sum_j wt_j u_f(fine tri pnt j)
+__global__ void k_mg_restrict_hstate(int ncoarse, int NV, const int *c2f_tri, const double *c2f_wt,
+                                     const int *ftri_pnt, const double *uf, double *uc, double *uc0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncoarse) return;
+    const int t = c2f_tri[i];
+    for (int n = 0; n < NV; ++n) {
+        double a = 0.0;
+        for (int j = 0; j < 3; ++j) a += c2f_wt[3 * i + j] * uf[ftri_pnt[3 * t + j] * NV + n];
+        uc[i * NV + n] = a;
+        uc0[i * NV + n] = a;
+    }
+}
+
+// h prolongation: u_f(i) += sum_j wt_j (u_c - u_c0)(coarse tri pnt j)
+__global__ void k_mg_prolong_h(int nfine, int NV, const int *f2c_tri, const double *f2c_wt, const int *ctri_pnt,
+                               const double *uc, const double *uc0, double *uf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfine) return;
+    const int t = f2c_tri[i];
+    for (int n = 0; n < NV; ++n) {
+        double a = 0.0;
+        for (int j = 0; j < 3; ++j) {
+            const int v0 = ctri_pnt[3 * t + j];
+            a += f2c_wt[3 * i + j] * (uc[v0 * NV + n] - uc0[v0 * NV + n]);
+        }
+        uf[i * NV + n] += a;
+    }
+}
+
+// FAS source (tri_hp::mg_source, nstage.cpp:113-129): dres = fadd*res0 - res(first)
+__global__ void k_fas_source(long n, double fadd, const double *res0, const double *res, double *dres) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+        dres[k] = fadd * res0[k] - res[k];
 }
 
 template <typename R>

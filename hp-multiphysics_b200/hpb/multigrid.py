@@ -1,0 +1,168 @@
+"""Multigrid hierarchies over the GPU contexts (block::cycle with p- and
+h-levels, tri_mesh/blocks.cpp:1267-1348).
+
+p-levels share the fine mesh at a lower polynomial degree (p -> p/2 -> ... -> 1,
+as the reference halves log2p; p = 6 goes 6 -> 3 -> 1). h-levels are coarser
+split-square meshes at p = 1 whose transfer weights are each point's containing
+triangle in the other mesh with barycentric weights (tri_mesh::mgconnect).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from .problem import GPULevel
+
+P = ctypes.c_void_p
+_bound = False
+
+
+def _bind():
+    global _bound
+    lib = L.lib()
+    if not _bound:
+        lib.hp_gpu_mg_attach_p.argtypes = [P, P, ctypes.c_double]
+        lib.hp_gpu_mg_attach_h.argtypes = [P, P, P, P, P, P, ctypes.c_double]
+        lib.hp_gpu_mg_restrict.argtypes = [P]
+        lib.hp_gpu_mg_prolongate.argtypes = [P]
+        lib.hp_gpu_vcycle.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int]
+        lib.hp_gpu_solve_mg.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_int)]
+        _bound = True
+    return lib
+
+
+def barycentric(pnts, tri_pnt, tris, pts):
+    """Barycentric weights of points pts[k] in triangles tris[k]."""
+    a = pnts[tri_pnt[tris, 0]]
+    b = pnts[tri_pnt[tris, 1]]
+    c = pnts[tri_pnt[tris, 2]]
+    v0, v1, v2 = b - a, c - a, pts - a
+    d = v0[:, 0] * v1[:, 1] - v0[:, 1] * v1[:, 0]
+    w1 = (v2[:, 0] * v1[:, 1] - v2[:, 1] * v1[:, 0]) / d
+    w2 = (v0[:, 0] * v2[:, 1] - v0[:, 1] * v2[:, 0]) / d
+    return np.stack([1.0 - w1 - w2, w1, w2], axis=1)
+
+
+def locate(mesh, pts):
+    """Containing triangle of each point (tri_mesh::findtri) and its barycentric
+    weights (getwgts). Uses a uniform bucket grid over the triangles."""
+    pts = np.asarray(pts, dtype=np.float64)
+    P_ = mesh.pnts
+    T = mesh.tri_pnt
+    lo = P_.min(axis=0)
+    hi = P_.max(axis=0)
+    nb = max(1, int(np.sqrt(mesh.ntri / 2)))
+    span = np.maximum(hi - lo, 1e-300)
+    tmin = ((P_[T].min(axis=1) - lo) / span * nb).astype(np.int64).clip(0, nb - 1)
+    tmax = ((P_[T].max(axis=1) - lo) / span * nb).astype(np.int64).clip(0, nb - 1)
+    # (cell, tri) pairs
+    cells, tris = [], []
+    for di in range(int((tmax - tmin)[:, 0].max()) + 1):
+        for dj in range(int((tmax - tmin)[:, 1].max()) + 1):
+            ok = (tmin[:, 0] + di <= tmax[:, 0]) & (tmin[:, 1] + dj <= tmax[:, 1])
+            t = np.nonzero(ok)[0]
+            cells.append((tmin[t, 0] + di) * nb + tmin[t, 1] + dj)
+            tris.append(t)
+    cells = np.concatenate(cells)
+    tris = np.concatenate(tris)
+    order = np.argsort(cells, kind="stable")
+    cells, tris = cells[order], tris[order]
+    start = np.searchsorted(cells, np.arange(nb * nb))
+    end = np.searchsorted(cells, np.arange(nb * nb), side="right")
+    pc = ((pts - lo) / span * nb).astype(np.int64).clip(0, nb - 1)
+    pcell = pc[:, 0] * nb + pc[:, 1]
+    best_t = np.full(len(pts), -1, dtype=np.int64)
+    best_w = np.full((len(pts), 3), np.nan)
+    best_m = np.full(len(pts), -np.inf)
+    maxc = int((end - start).max())
+    for k in range(maxc):
+        idx = start[pcell] + k
+        valid = idx < end[pcell]
+        if not np.any(valid):
+            break
+        q = np.nonzero(valid)[0]
+        t = tris[idx[q]]
+        w = barycentric(P_, T, t, pts[q])
+        m = w.min(axis=1)
+        better = m > best_m[q]
+        qq = q[better]
+        best_m[qq] = m[better]
+        best_t[qq] = t[better]
+        best_w[qq] = w[better]
+    if np.any(best_t < 0) or np.any(best_m < -1e-6):
+        raise ValueError("point outside the mesh")
+    return best_t.astype(np.int32), np.ascontiguousarray(best_w)
+
+
+class Hierarchy:
+    """levels[0] is the finest GPULevel; each next one is attached to the previous."""
+
+    def __init__(self, probs, kinds, stream=None, fadd=1.0):
+        lib = _bind()
+        self.probs = probs
+        self.levels = [GPULevel(pr, 0, stream) for pr in probs]
+        self._keep = []
+        for l in range(1, len(probs)):
+            c, f = self.levels[l], self.levels[l - 1]
+            if kinds[l] == "p":
+                L.check(lib.hp_gpu_mg_attach_p(c.h, f.h, fadd), "mg_attach_p")
+            else:
+                fm, cm = probs[l - 1].mesh, probs[l].mesh
+                f2c_t, f2c_w = locate(cm, fm.pnts)
+                c2f_t, c2f_w = locate(fm, cm.pnts)
+                self._keep += [f2c_t, f2c_w, c2f_t, c2f_w]
+                L.check(lib.hp_gpu_mg_attach_h(c.h, f.h, L.ptr(f2c_t), L.ptr(f2c_w), L.ptr(c2f_t), L.ptr(c2f_w),
+                                               fadd), "mg_attach_h")
+        self.lib = lib
+
+    def handles(self):
+        arr = (P * len(self.levels))(*[lv.h for lv in self.levels])
+        return arr
+
+    def solve(self, drop=1e-10, max_cycles=500, vw=1, itercrsn=2, iterrfne=2, prcn_every=0):
+        cap = max_cycles + 2
+        hist = np.zeros(cap)
+        nh = ctypes.c_int(); sec = ctypes.c_double(); nc = ctypes.c_int()
+        L.check(self.lib.hp_gpu_solve_mg(self.handles(), len(self.levels), drop, max_cycles, vw, itercrsn, iterrfne,
+                                         prcn_every, L.ptr(hist), cap, ctypes.byref(nh), ctypes.byref(sec),
+                                         ctypes.byref(nc)), "solve_mg")
+        return hist[:nh.value], sec.value, nc.value
+
+    def close(self):
+        for lv in self.levels:
+            lv.close()
+
+
+def p_sequence(p):
+    """p-levels below p: halving (the reference's log2p hierarchy), then 1."""
+    seq = []
+    q = p
+    while q > 1:
+        q = max(1, q // 2)
+        seq.append(q)
+    return seq
+
+
+def build(factory, n, p, hlevels=0, stream=None, cfl=None, **kw):
+    """Hierarchy for a workload factory(n=..., p=...): p-levels of the fine mesh
+    down to p = 1, then `hlevels` split-square meshes of n/2, n/4, ... at p = 1.
+    cfl: None (the per-log2p defaults), a number, or a dict p -> cfl."""
+    def cf(q):
+        if cfl is None:
+            return {}
+        return {"cfl": cfl[q] if isinstance(cfl, dict) else cfl}
+    probs = [factory(n=n, p=p, **cf(p), **kw)]
+    kinds = ["fine"]
+    for q in p_sequence(p):
+        probs.append(factory(n=n, p=q, **cf(q), **kw))
+        kinds.append("p")
+    m = n
+    for _ in range(hlevels):
+        m //= 2
+        probs.append(factory(n=m, p=1, **cf(1), **kw))
+        kinds.append("h")
+    return Hierarchy(probs, kinds, stream=stream)

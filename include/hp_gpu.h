@@ -204,6 +204,36 @@ int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *ctx, int stage);
 int hp_gpu_solve(hp_gpu_ctx *ctx, int mode, double drop, int max_updates, int inner, int check_every,
                  int prcn_every, double *hist, int hist_cap, int *n_hist, double *seconds, int *updates);
 
+/* Multigrid. A coarse context is attached to its fine context either as a
+ * p-level (same mesh, lower p: the hierarchical basis makes its modes a subset
+ * of the fine ones, tri_hp/movco.cpp:17-39) or as an h-level (a coarser mesh at
+ * p = 1, with each fine vertex's containing coarse triangle and barycentric
+ * weights f2c_tri/f2c_wt [fine npnt][3], and each coarse vertex's containing fine
+ * triangle c2f_tri/c2f_wt [coarse npnt][3]: tri_mesh::mgconnect,
+ * tri_mesh/connect.cpp:49-87). Attaching gives the coarse level a FAS source
+ * dres = fadd*res0 - res(first) that enters every stage residual
+ * (tri_hp::mg_source, nstage.cpp:113-129; hp_fadd default 1). */
+int hp_gpu_mg_attach_p(hp_gpu_ctx *coarse, hp_gpu_ctx *fine, double fadd);
+int hp_gpu_mg_attach_h(hp_gpu_ctx *coarse, hp_gpu_ctx *fine, const int *f2c_tri, const double *f2c_wt,
+                       const int *c2f_tri, const double *c2f_wt, double fadd);
+/* tri_hp::mg_restrict (movco.cpp:4-106): needs the fine level's full residual
+ * (hp_gpu_rsdl(fine, nstage)); sets the coarse state, its copy at entry
+ * (vug_frst) and the FAS source. */
+int hp_gpu_mg_restrict(hp_gpu_ctx *coarse);
+/* tri_hp::mg_prolongate (movfin.cpp:7-82): fine state += coarse correction. */
+int hp_gpu_mg_prolongate(hp_gpu_ctx *coarse);
+/* block::cycle (tri_mesh/blocks.cpp:1267-1348) over levels[0] (finest) ..
+ * levels[nlevels-1], each attached to the previous one: vw cycles per level,
+ * itercrsn updates before and iterrfne after the coarse-grid correction,
+ * setup_preconditioner() on entry to each level when eval_prcn. */
+int hp_gpu_vcycle(hp_gpu_ctx **levels, int nlevels, int vw, int itercrsn, int iterrfne, int eval_prcn);
+/* Cycles until ||R64|| on levels[0] (as in hp_gpu_solve) drops by `drop` or
+ * max_cycles ran; preconditioners on the first cycle and every prcn_every
+ * cycles. hist gets the drop after each cycle; *seconds device time. */
+int hp_gpu_solve_mg(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
+                    int iterrfne, int prcn_every, double *hist, int hist_cap, int *n_hist, double *seconds,
+                    int *cycles);
+
 /* Diagnostic: n multistage updates of the FP32 smoother in plain form, from
  * fp32(u), written back to the FP64 state (compares the FP32 kernels with the
  * FP64 ones update by update). Needs setup_preconditioner() first. */

@@ -1,0 +1,104 @@
+"""Multigrid on the GPU: the p- and h-transfers against numpy restatements of
+tri_hp::mg_restrict / mg_prolongate (movco.cpp, movfin.cpp), the FAS source
+(mg_source), and convergence of V-cycles."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import hpb
+from hpb import _lib as L
+from hpb import multigrid as MG
+
+pytestmark = pytest.mark.gpu
+
+
+def interior_map(smc, smf):
+    out = []
+    off_f = 0
+    for m in range(1, smf):
+        for k in range(smf - m):
+            if m < smc and k < smc - m:
+                out.append(off_f + k)
+        off_f += smf - m
+    return np.array(out, dtype=int)
+
+
+def test_p_restriction_and_fas_source():
+    H = MG.build(lambda n, p, **kw: hpb.kovasznay_ins(n=n, p=p, **kw), n=6, p=4)
+    f, c = H.levels[0], H.levels[1]
+    assert f.setup_preconditioner() == 0
+    f.rsdl(f.prob.phys.nstage)
+    rf = f.residual()
+    uf = f.state()
+    L.check(H.lib.hp_gpu_mg_restrict(c.h), "restrict")
+    uc = c.state()
+    smc, imc = c.prob.sm, c.prob.im
+    imap = interior_map(smc, f.prob.sm)
+    assert np.array_equal(uc[0], uf[0])
+    assert np.array_equal(uc[1], uf[1][:, :smc, :])
+    assert np.array_equal(uc[2], uf[2][:, imap, :])
+    # the coarse residual with the FAS source at the restricted state is fadd*res0
+    assert c.setup_preconditioner() == 0
+    c.rsdl(c.prob.phys.nstage)
+    rc = c.residual()
+    want = (rf[0], rf[1][:, :smc, :], rf[2][:, imap, :])
+    for a, b in zip(rc, want):
+        if b.size:
+            assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b)))
+    H.close()
+
+
+def test_h_restriction_and_prolongation():
+    H = MG.build(lambda n, p, **kw: hpb.kovasznay_ins(n=n, p=p, **kw), n=8, p=1, hlevels=1)
+    f, c = H.levels[0], H.levels[1]
+    fm, cm = f.prob.mesh, c.prob.mesh
+    assert f.setup_preconditioner() == 0
+    f.rsdl(f.prob.phys.nstage)
+    rf = f.residual()[0]
+    uf = f.state()[0]
+    L.check(H.lib.hp_gpu_mg_restrict(c.h), "restrict")
+    uc = c.state()[0]
+    t_c2f, w_c2f = MG.locate(fm, cm.pnts)
+    want_u = np.einsum("kj,kjn->kn", w_c2f, uf[fm.tri_pnt[t_c2f]])
+    assert np.max(np.abs(uc - want_u)) < 1e-13
+    t_f2c, w_f2c = MG.locate(cm, fm.pnts)
+    res0 = np.zeros_like(uc)
+    for j in range(3):
+        np.add.at(res0, cm.tri_pnt[t_f2c, j], w_f2c[:, j:j + 1] * rf)
+    assert c.setup_preconditioner() == 0
+    c.rsdl(c.prob.phys.nstage)
+    rc = c.residual()[0]
+    assert np.max(np.abs(rc - res0)) <= 1e-12 * np.max(np.abs(res0))
+    # prolongation adds the interpolated coarse correction to the fine vertices
+    c.update()
+    duc = c.state()[0] - uc
+    L.check(H.lib.hp_gpu_mg_prolongate(c.h), "prolongate")
+    want = uf + np.einsum("kj,kjn->kn", w_f2c, duc[cm.tri_pnt[t_f2c]])
+    assert np.max(np.abs(f.state()[0] - want)) < 1e-12
+    H.close()
+
+
+def quad():
+    return L.Field(L.HP_FIELD_QUADX, (ctypes.c_double * 4)(-1.0, 8.0, 0, 0))
+
+
+def test_vcycle_converges_faster_than_single_grid_cd():
+    mk = lambda n, p, **kw: hpb.cd_sinsin(n=n, p=p, kcond=1e-2, field=quad(), **kw)
+    H = MG.build(mk, n=16, p=4, hlevels=2, cfl={4: 0.5, 2: 0.75, 1: 1.0})
+    hist, sec, cycles = H.solve(drop=1e-10, max_cycles=300, itercrsn=2, iterrfne=2)
+    assert hist[-1] <= 1e-10
+    fine_updates_mg = 4 * cycles
+    g = mk(n=16, p=4, cfl=0.5).gpu()
+    h1, s1, upd = g.solve(drop=1e-10, max_updates=20000, check_every=10)
+    assert h1[-1] <= 1e-10
+    assert fine_updates_mg < upd
+    H.close()
+
+
+def test_vcycle_converges_ins_kovasznay():
+    mk = lambda n, p, **kw: hpb.kovasznay_ins(n=n, p=p, re=100.0, **kw)
+    H = MG.build(mk, n=16, p=4, hlevels=2)
+    hist, sec, cycles = H.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2)
+    assert hist[-1] <= 1e-10, hist[-5:]
+    H.close()
