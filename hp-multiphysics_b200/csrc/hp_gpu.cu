@@ -251,6 +251,8 @@ struct hp_gpu_ctx {
     double *fasv = nullptr, *fass = nullptr, *fasi = nullptr;     // FAS source dres
     int *f2c_tri = nullptr, *c2f_tri = nullptr;
     double *f2c_wt = nullptr, *c2f_wt = nullptr;
+    // FP32 multigrid on the correction equation: restricted residual and entry state
+    float *r0v32 = nullptr, *r0s32 = nullptr, *r0i32 = nullptr, *c0v32 = nullptr, *c0s32 = nullptr, *c0i32 = nullptr;
 };
 
 static int dalloc(hp_gpu_ctx *c, void **p, size_t bytes) {
@@ -1019,28 +1021,29 @@ extern "C" int hp_gpu_mg_attach_h(hp_gpu_ctx *coarse, hp_gpu_ctx *fine, const in
 static int mg_restrict_enqueue(hp_gpu_ctx *c) {
     hp_gpu_ctx *f = c->fine;
     if (!f || !c->mg_kind) { set_err("not a coarse level"); return HP_ESTATE; }
-    // both levels run on the fine level's stream order: make the coarse stream wait
-    cudaEvent_t ev;
-    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    CK(cudaEventRecord(ev, f->stream));
-    CK(cudaStreamWaitEvent(c->stream, ev, 0));
-    cudaEventDestroy(ev);
+    if (c->stream != f->stream) {  // order the coarse stream after the fine one
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev, f->stream));
+        CK(cudaStreamWaitEvent(c->stream, ev, 0));
+        cudaEventDestroy(ev);
+    }
     const int NV = c->NV;
     if (c->mg_kind == 1) {
         const long tot = (long)(c->lv + c->ls + c->li);
         const int g = std::min(nblk(tot, 256), c->nsm * 8);
-        k_mg_truncate<<<g, 256, 0, c->stream>>>(c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im, f->st.resv,
+        k_mg_truncate<double><<<g, 256, 0, c->stream>>>(c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im, f->st.resv,
                                                 f->st.ress, f->st.resi, c->res0v, c->res0s, c->res0i);
-        k_mg_truncate<<<g, 256, 0, c->stream>>>(c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im, f->st.ugv,
+        k_mg_truncate<double><<<g, 256, 0, c->stream>>>(c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im, f->st.ugv,
                                                 f->st.ugs, f->st.ugi, c->st.ugv, c->st.ugs, c->st.ugi);
         CK(cudaMemcpyAsync(c->uc0v, c->st.ugv, c->lv * 8, cudaMemcpyDeviceToDevice, c->stream));
         if (c->ls) CK(cudaMemcpyAsync(c->uc0s, c->st.ugs, c->ls * 8, cudaMemcpyDeviceToDevice, c->stream));
         if (c->li) CK(cudaMemcpyAsync(c->uc0i, c->st.ugi, c->li * 8, cudaMemcpyDeviceToDevice, c->stream));
     } else {
         CK(cudaMemsetAsync(c->res0v, 0, c->lv * 8, c->stream));
-        k_mg_restrict_hres<<<nblk(f->npnt, 128), 128, 0, c->stream>>>(f->npnt, NV, c->f2c_tri, c->f2c_wt,
+        k_mg_restrict_hres<double><<<nblk(f->npnt, 128), 128, 0, c->stream>>>(f->npnt, NV, c->f2c_tri, c->f2c_wt,
                                                                         c->mesh.tri_pnt, f->st.resv, c->res0v);
-        k_mg_restrict_hstate<<<nblk(c->npnt, 128), 128, 0, c->stream>>>(c->npnt, NV, c->c2f_tri, c->c2f_wt,
+        k_mg_restrict_hstate<double><<<nblk(c->npnt, 128), 128, 0, c->stream>>>(c->npnt, NV, c->c2f_tri, c->c2f_wt,
                                                                           f->mesh.tri_pnt, f->st.ugv, c->st.ugv,
                                                                           c->uc0v);
     }
@@ -1052,9 +1055,9 @@ static int mg_restrict_enqueue(hp_gpu_ctx *c) {
     k_rsdl_fold<double><<<nblk(n2, 256), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, c->st.resv, c->st.rrv,
                                                               c->st.ress, c->st.rrs, nullptr, nullptr);
     const int g2 = c->nsm * 8;
-    k_fas_source<<<g2, 256, 0, c->stream>>>((long)c->lv, c->fadd, c->res0v, c->st.resv, c->fasv);
-    if (c->ls) k_fas_source<<<g2, 256, 0, c->stream>>>((long)c->ls, c->fadd, c->res0s, c->st.ress, c->fass);
-    if (c->li) k_fas_source<<<g2, 256, 0, c->stream>>>((long)c->li, c->fadd, c->res0i, c->st.resi, c->fasi);
+    k_fas_source<double><<<g2, 256, 0, c->stream>>>((long)c->lv, c->fadd, c->res0v, c->st.resv, c->fasv);
+    if (c->ls) k_fas_source<double><<<g2, 256, 0, c->stream>>>((long)c->ls, c->fadd, c->res0s, c->st.ress, c->fass);
+    if (c->li) k_fas_source<double><<<g2, 256, 0, c->stream>>>((long)c->li, c->fadd, c->res0i, c->st.resi, c->fasi);
     return check_launch(c);
 }
 
@@ -1064,18 +1067,20 @@ static int mg_prolong_enqueue(hp_gpu_ctx *c) {
     const int NV = c->NV;
     if (c->mg_kind == 1) {
         const long tot = (long)(c->lv + c->ls + c->li);
-        k_mg_prolong_p<<<std::min(nblk(tot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+        k_mg_prolong_p<double><<<std::min(nblk(tot, 256), c->nsm * 8), 256, 0, c->stream>>>(
             c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im, c->st.ugv, c->st.ugs, c->st.ugi, c->uc0v,
             c->uc0s, c->uc0i, f->st.ugv, f->st.ugs, f->st.ugi);
     } else {
-        k_mg_prolong_h<<<nblk(f->npnt, 128), 128, 0, c->stream>>>(f->npnt, NV, c->f2c_tri, c->f2c_wt, c->mesh.tri_pnt,
+        k_mg_prolong_h<double><<<nblk(f->npnt, 128), 128, 0, c->stream>>>(f->npnt, NV, c->f2c_tri, c->f2c_wt, c->mesh.tri_pnt,
                                                                     c->st.ugv, c->uc0v, f->st.ugv);
     }
-    cudaEvent_t ev;
-    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    CK(cudaEventRecord(ev, c->stream));
-    CK(cudaStreamWaitEvent(f->stream, ev, 0));
-    cudaEventDestroy(ev);
+    if (c->stream != f->stream) {
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev, c->stream));
+        CK(cudaStreamWaitEvent(f->stream, ev, 0));
+        cudaEventDestroy(ev);
+    }
     return check_launch(c);
 }
 
@@ -1145,6 +1150,286 @@ extern "C" int hp_gpu_solve_mg(hp_gpu_ctx **levels, int nlevels, double drop, in
         // and then every prcn_every cycles (block::cycle's evaluate_preconditioner)
         const int eval = (nc == 0 || (prcn_every > 0 && nc % prcn_every == 0)) ? 1 : 0;
         if ((r = cycle(levels, nlevels, 0, vw, itercrsn, iterrfne, eval))) return r;
+        ++nc;
+        if ((r = fp64_norm(f, &rn))) return r;
+        const double d = rn / r0;
+        if (hist && nh < hist_cap) hist[nh++] = d;
+        if (!(d == d) || d <= drop) break;
+    }
+    CK(cudaEventRecord(e1, f->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (n_hist) *n_hist = nh;
+    if (seconds) *seconds = ms * 1e-3;
+    if (cycles) *cycles = nc;
+    return hp_gpu_sync(f);
+}
+
+// One V/W-cycle captured as a single CUDA graph (all levels must share one
+// stream). The preconditioners are evaluated before capture and frozen inside it;
+// the level updates are enqueued as plain kernels so the whole cycle is one graph.
+static int cycle_enqueue(hp_gpu_ctx **lv, int n, int lvl, int vw, int itercrsn, int iterrfne) {
+    hp_gpu_ctx *c = lv[lvl];
+    int r;
+    for (int vc = 0; vc < vw; ++vc) {
+        for (int it = 0; it < itercrsn; ++it) enqueue_update(c);
+        if (lvl == n - 1) return HP_OK;
+        if ((r = hp_gpu_enqueue_rsdl(c, c->ph.nstage))) return r;
+        if ((r = mg_restrict_enqueue(lv[lvl + 1]))) return r;
+        if ((r = cycle_enqueue(lv, n, lvl + 1, vw, itercrsn, iterrfne))) return r;
+        if ((r = mg_prolong_enqueue(lv[lvl + 1]))) return r;
+        for (int it = 0; it < iterrfne; ++it) enqueue_update(c);
+    }
+    return HP_OK;
+}
+
+struct VGraph {
+    cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" int hp_gpu_capture_vcycle(hp_gpu_ctx **levels, int nlevels, int vw, int itercrsn, int iterrfne,
+                                     void **graph_out) {
+    if (!levels || nlevels < 1 || !graph_out) return HP_EINVAL;
+    for (int l = 0; l < nlevels; ++l) {
+        if (levels[l]->stream != levels[0]->stream) { set_err("all levels must share one stream"); return HP_EINVAL; }
+        if (l > 0 && levels[l]->fine != levels[l - 1]) { set_err("levels not attached in order"); return HP_EINVAL; }
+        if (!levels[l]->prcn_ready) { set_err("setup_preconditioner every level before capture"); return HP_ESTATE; }
+    }
+    cudaStream_t s = levels[0]->stream;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int r = cycle_enqueue(levels, nlevels, 0, vw, itercrsn, iterrfne);
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (r) return r;
+    if (e != cudaSuccess) { set_err("V-cycle capture failed: %s", cudaGetErrorString(e)); return HP_ECUDA; }
+    VGraph *vg = new VGraph();
+    e = cudaGraphInstantiate(&vg->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { delete vg; set_err("V-cycle instantiate failed: %s", cudaGetErrorString(e)); return HP_ECUDA; }
+    *graph_out = vg;
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_launch_vcycle(void *graph, hp_gpu_ctx *finest, int count) {
+    if (!graph || !finest || count < 0) return HP_EINVAL;
+    VGraph *vg = static_cast<VGraph *>(graph);
+    for (int k = 0; k < count; ++k) CK(cudaGraphLaunch(vg->exec, finest->stream));
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_destroy_vcycle(void *graph) {
+    if (!graph) return HP_OK;
+    VGraph *vg = static_cast<VGraph *>(graph);
+    if (vg->exec) cudaGraphExecDestroy(vg->exec);
+    delete vg;
+    return HP_OK;
+}
+
+// hp_gpu_solve_mg with the cycle replayed from one captured graph (preconditioners
+// frozen at the entry state: preconditioner_interval = 0).
+extern "C" int hp_gpu_solve_mg_graph(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycles, int vw,
+                                     int itercrsn, int iterrfne, int check_every, double *hist, int hist_cap,
+                                     int *n_hist, double *seconds, int *cycles) {
+    if (!levels || nlevels < 1 || drop <= 0.0 || max_cycles < 1) return HP_EINVAL;
+    if (check_every < 1) check_every = 1;
+    hp_gpu_ctx *f = levels[0];
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, f->stream));
+    int r, nh = 0, nc = 0;
+    double r0 = 0.0, rn = 0.0;
+    r = hp_gpu_setup_preconditioner(f);
+    if (r) return r < 0 ? r : HP_ESTATE;
+    if ((r = fp64_norm(f, &r0))) return r;
+    if (hist && nh < hist_cap) hist[nh++] = 1.0;
+    // first cycle evaluates every level's preconditioner at its own state
+    if ((r = cycle(levels, nlevels, 0, vw, itercrsn, iterrfne, 1))) return r;
+    ++nc;
+    void *vg = nullptr;
+    if ((r = hp_gpu_capture_vcycle(levels, nlevels, vw, itercrsn, iterrfne, &vg))) return r;
+    while (true) {
+        if ((r = fp64_norm(f, &rn))) break;
+        const double d = rn / r0;
+        if (hist && nh < hist_cap) hist[nh++] = d;
+        if (!(d == d) || d <= drop || nc >= max_cycles) break;
+        const int k = std::min(check_every, max_cycles - nc);
+        if ((r = hp_gpu_launch_vcycle(vg, f, k))) break;
+        nc += k;
+    }
+    hp_gpu_destroy_vcycle(vg);
+    if (r) return r;
+    CK(cudaEventRecord(e1, f->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (n_hist) *n_hist = nh;
+    if (seconds) *seconds = ms * 1e-3;
+    if (cycles) *cycles = nc;
+    return hp_gpu_sync(f);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 multigrid on the correction equation, inside FP64 defect correction.
+// Every level l carries a base state b_l (fp32 of its FP64 state: the fine u,
+// or u restricted down the hierarchy) and a correction d_l; its residual is the
+// correction form F_l(d) = R_l(b_l + d) - R_l(b_l) + s_l with s_fine = R64(u)
+// and s_coarse the FAS source fadd*restrict(F_fine) - F_coarse(d_entry).
+// ---------------------------------------------------------------------------
+static int alloc_mixed_mg(hp_gpu_ctx *c) {
+    int r;
+    if ((r = alloc_mixed(c))) return r;
+    if (c->r0v32) return HP_OK;
+    const size_t lv = std::max<size_t>(c->lv, 1), ls = std::max<size_t>(c->ls, 1), li = std::max<size_t>(c->li, 1);
+    if ((r = dalloc(c, (void **)&c->r0v32, lv * 4)) || (r = dalloc(c, (void **)&c->r0s32, ls * 4)) ||
+        (r = dalloc(c, (void **)&c->r0i32, li * 4)) || (r = dalloc(c, (void **)&c->c0v32, lv * 4)) ||
+        (r = dalloc(c, (void **)&c->c0s32, ls * 4)) || (r = dalloc(c, (void **)&c->c0i32, li * 4)))
+        return r;
+    return HP_OK;
+}
+
+static Phys phys32(const hp_gpu_ctx *c) {
+    Phys ph = c->ph;
+    if (ph.physics == HP_PHYS_CD) ph.src = 0.0;
+    return ph;
+}
+
+// F(d) of this level folded into s32.res (the source included when `with_src`)
+static void rsdl32_folded(hp_gpu_ctx *c, bool with_src) {
+    State<float> st = c->s32;
+    if (!with_src) st.dresv = st.dress = st.dresi = nullptr;
+    const int diff = (c->ph.physics == HP_PHYS_INS) ? 1 : 0;
+    enqueue_rsdl_t<float>(c, c->L32, c->d_tab32, st, phys32(c), c->ph.nstage, diff);
+    const long n = (long)(c->lv + c->ls);
+    k_rsdl_fold<float><<<nblk(n, 256), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, st.resv, st.rrv, st.ress, st.rrs,
+                                                            st.dresv, st.dress);
+}
+
+static int mg_restrict32(hp_gpu_ctx *c) {
+    hp_gpu_ctx *f = c->fine;
+    const int NV = c->NV;
+    State<float> &fs = f->s32, &cs = c->s32;
+    rsdl32_folded(f, true);  // F_fine(d) with its source
+    if (c->mg_kind == 1) {
+        const long tot = (long)(c->lv + c->ls + c->li);
+        const int g = std::min(nblk(tot, 256), c->nsm * 8);
+        k_mg_truncate<float><<<g, 256, 0, c->stream>>>(c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im,
+                                                       fs.resv, fs.ress, fs.resi, c->r0v32, c->r0s32, c->r0i32);
+        k_mg_truncate<float><<<g, 256, 0, c->stream>>>(c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im,
+                                                       fs.ugv, fs.ugs, fs.ugi, cs.ugv, cs.ugs, cs.ugi);
+        CK(cudaMemcpyAsync(c->c0v32, cs.ugv, c->lv * 4, cudaMemcpyDeviceToDevice, c->stream));
+        if (c->ls) CK(cudaMemcpyAsync(c->c0s32, cs.ugs, c->ls * 4, cudaMemcpyDeviceToDevice, c->stream));
+        if (c->li) CK(cudaMemcpyAsync(c->c0i32, cs.ugi, c->li * 4, cudaMemcpyDeviceToDevice, c->stream));
+    } else {
+        CK(cudaMemsetAsync(c->r0v32, 0, c->lv * 4, c->stream));
+        k_mg_restrict_hres<float><<<nblk(f->npnt, 128), 128, 0, c->stream>>>(f->npnt, NV, c->f2c_tri, c->f2c_wt,
+                                                                               c->mesh.tri_pnt, fs.resv, c->r0v32);
+        k_mg_restrict_hstate<float><<<nblk(c->npnt, 128), 128, 0, c->stream>>>(c->npnt, NV, c->c2f_tri, c->c2f_wt,
+                                                                                 f->mesh.tri_pnt, fs.ugv, cs.ugv,
+                                                                                 c->c0v32);
+    }
+    rsdl32_folded(c, false);  // F_coarse(d_entry) without source
+    const int g2 = c->nsm * 8;
+    k_fas_source<float><<<g2, 256, 0, c->stream>>>((long)c->lv, c->fadd, c->r0v32, cs.resv, (float *)cs.dresv);
+    if (c->ls) k_fas_source<float><<<g2, 256, 0, c->stream>>>((long)c->ls, c->fadd, c->r0s32, cs.ress, (float *)cs.dress);
+    if (c->li) k_fas_source<float><<<g2, 256, 0, c->stream>>>((long)c->li, c->fadd, c->r0i32, cs.resi, (float *)cs.dresi);
+    return check_launch(c);
+}
+
+static int mg_prolong32(hp_gpu_ctx *c) {
+    hp_gpu_ctx *f = c->fine;
+    const int NV = c->NV;
+    State<float> &fs = f->s32, &cs = c->s32;
+    if (c->mg_kind == 1) {
+        const long tot = (long)(c->lv + c->ls + c->li);
+        k_mg_prolong_p<float><<<std::min(nblk(tot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+            c->npnt, c->nseg, c->ntri, NV, f->sm, f->im, c->sm, c->im, cs.ugv, cs.ugs, cs.ugi, c->c0v32, c->c0s32,
+            c->c0i32, fs.ugv, fs.ugs, fs.ugi);
+    } else {
+        k_mg_prolong_h<float><<<nblk(f->npnt, 128), 128, 0, c->stream>>>(f->npnt, NV, c->f2c_tri, c->f2c_wt,
+                                                                           c->mesh.tri_pnt, cs.ugv, c->c0v32, fs.ugv);
+    }
+    return check_launch(c);
+}
+
+static int cycle32(hp_gpu_ctx **lv, int n, int lvl, int vw, int itercrsn, int iterrfne) {
+    hp_gpu_ctx *c = lv[lvl];
+    int r;
+    if ((r = ensure_update32_graph(c))) return r;
+    for (int vc = 0; vc < vw; ++vc) {
+        for (int it = 0; it < itercrsn; ++it) CK(cudaGraphLaunch(c->g_update32, c->stream));
+        if (lvl == n - 1) return HP_OK;
+        if ((r = mg_restrict32(lv[lvl + 1]))) return r;
+        if ((r = cycle32(lv, n, lvl + 1, vw, itercrsn, iterrfne))) return r;
+        if ((r = mg_prolong32(lv[lvl + 1]))) return r;
+        for (int it = 0; it < iterrfne; ++it) CK(cudaGraphLaunch(c->g_update32, c->stream));
+    }
+    return HP_OK;
+}
+
+// FP64 states of the coarse levels from the fine one (no FAS), their FP64
+// preconditioners, and the FP32 copies (prcn and base states) of every level.
+static int mixed_levels_setup(hp_gpu_ctx **lv, int n, bool prcn) {
+    int r;
+    for (int l = 1; l < n; ++l) {
+        hp_gpu_ctx *c = lv[l], *f = lv[l - 1];
+        if (c->mg_kind == 1) {
+            const long tot = (long)(c->lv + c->ls + c->li);
+            k_mg_truncate<double><<<std::min(nblk(tot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+                c->npnt, c->nseg, c->ntri, c->NV, f->sm, f->im, c->sm, c->im, f->st.ugv, f->st.ugs, f->st.ugi,
+                c->st.ugv, c->st.ugs, c->st.ugi);
+        } else {
+            k_mg_restrict_hstate<double><<<nblk(c->npnt, 128), 128, 0, c->stream>>>(
+                c->npnt, c->NV, c->c2f_tri, c->c2f_wt, f->mesh.tri_pnt, f->st.ugv, c->st.ugv, (double *)nullptr);
+        }
+    }
+    for (int l = 0; l < n; ++l) {
+        hp_gpu_ctx *c = lv[l];
+        if (prcn || !c->prcn_ready) {
+            r = hp_gpu_setup_preconditioner(c);
+            if (r) return r < 0 ? r : HP_ESTATE;
+            mixed_prcn(c);
+        }
+        State<float> &f = c->s32;
+        conv(c, (long)c->lv, c->st.ugv, (float *)f.ubv);
+        conv(c, (long)c->ls, c->st.ugs, (float *)f.ubs);
+        conv(c, (long)c->li, c->st.ugi, (float *)f.ubi);
+    }
+    return check_launch(lv[0]);
+}
+
+extern "C" int hp_gpu_solve_mg_mixed(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycles, int vw,
+                                     int itercrsn, int iterrfne, int prcn_every, double *hist, int hist_cap,
+                                     int *n_hist, double *seconds, int *cycles) {
+    if (!levels || nlevels < 1 || drop <= 0.0 || max_cycles < 1) return HP_EINVAL;
+    for (int l = 1; l < nlevels; ++l)
+        if (!levels[l] || levels[l]->fine != levels[l - 1]) { set_err("levels not attached in order"); return HP_EINVAL; }
+    hp_gpu_ctx *f = levels[0];
+    int r;
+    for (int l = 0; l < nlevels; ++l)
+        if ((r = alloc_mixed_mg(levels[l]))) return r;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, f->stream));
+    int nh = 0, nc = 0;
+    double r0 = 0.0, rn = 0.0;
+    r = hp_gpu_setup_preconditioner(f);
+    if (r) return r < 0 ? r : HP_ESTATE;
+    if ((r = fp64_norm(f, &r0))) return r;
+    if (hist && nh < hist_cap) hist[nh++] = 1.0;
+    while (nc < max_cycles) {
+        const bool eval = (nc == 0) || (prcn_every > 0 && nc % prcn_every == 0);
+        if ((r = mixed_levels_setup(levels, nlevels, eval))) return r;
+        // the FP64 residual R64(u) from the last norm evaluation is the fine source
+        mixed_prepare(f);
+        if ((r = cycle32(levels, nlevels, 0, vw, itercrsn, iterrfne))) return r;
+        mixed_apply(f);
         ++nc;
         if ((r = fp64_norm(f, &rn))) return r;
         const double d = rn / r0;

@@ -859,9 +859,10 @@ __device__ __forceinline__ int interior_fine_index(int kc, int smc, int smf) {
     return off_f + (kc - off_c);
 }
 
-// dst_c = src_f restricted (truncate) ; mode 0: copy, 1: dst_c += src_f (unused)
+// dst_c = src_f restricted to the coarse modes
+template <typename R>
 __global__ void k_mg_truncate(int npnt, int nseg, int ntri, int NV, int smf, int imf, int smc, int imc,
-                              const double *fv, const double *fs, const double *fi, double *cv, double *cs, double *ci) {
+                              const R *fv, const R *fs, const R *fi, R *cv, R *cs, R *ci) {
     const long nv = (long)npnt * NV, ns = (long)nseg * smc * NV, ni = (long)ntri * imc * NV;
     for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < nv + ns + ni; k += (long)gridDim.x * blockDim.x) {
         if (k < nv) {
@@ -879,9 +880,10 @@ __global__ void k_mg_truncate(int npnt, int nseg, int ntri, int NV, int smf, int
 }
 
 // fine low modes += (coarse state - coarse state at restriction)
+template <typename R>
 __global__ void k_mg_prolong_p(int npnt, int nseg, int ntri, int NV, int smf, int imf, int smc, int imc,
-                               const double *cv, const double *cs, const double *ci, const double *c0v,
-                               const double *c0s, const double *c0i, double *fv, double *fs, double *fi) {
+                               const R *cv, const R *cs, const R *ci, const R *c0v, const R *c0s, const R *c0i, R *fv,
+                               R *fs, R *fi) {
     const long nv = (long)npnt * NV, ns = (long)nseg * smc * NV, ni = (long)ntri * imc * NV;
     for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < nv + ns + ni; k += (long)gridDim.x * blockDim.x) {
         if (k < nv) {
@@ -899,35 +901,38 @@ __global__ void k_mg_prolong_p(int npnt, int nseg, int ntri, int NV, int smf, in
 }
 
 // h restriction of the vertex residual: res0_c(v0) += wt * res_f(i) over fine vertices i
+template <typename R>
 __global__ void k_mg_restrict_hres(int nfine, int NV, const int *f2c_tri, const double *f2c_wt, const int *ctri_pnt,
-                                   const double *resf, double *res0c) {
+                                   const R *resf, R *res0c) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nfine) return;
     const int t = f2c_tri[i];
     for (int j = 0; j < 3; ++j) {
         const int v0 = ctri_pnt[3 * t + j];
         const double w = f2c_wt[3 * i + j];
-        for (int n = 0; n < NV; ++n) atomicAdd(&res0c[v0 * NV + n], w * resf[i * NV + n]);
+        for (int n = 0; n < NV; ++n) atomic_add(&res0c[v0 * NV + n], (R)(w * (double)resf[i * NV + n]));
     }
 }
 
 // h interpolation of the vertex state: u_c(i) = sum_j wt_j u_f(fine tri pnt j)
+template <typename R>
 __global__ void k_mg_restrict_hstate(int ncoarse, int NV, const int *c2f_tri, const double *c2f_wt,
-                                     const int *ftri_pnt, const double *uf, double *uc, double *uc0) {
+                                     const int *ftri_pnt, const R *uf, R *uc, R *uc0) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ncoarse) return;
     const int t = c2f_tri[i];
     for (int n = 0; n < NV; ++n) {
         double a = 0.0;
-        for (int j = 0; j < 3; ++j) a += c2f_wt[3 * i + j] * uf[ftri_pnt[3 * t + j] * NV + n];
-        uc[i * NV + n] = a;
-        uc0[i * NV + n] = a;
+        for (int j = 0; j < 3; ++j) a += c2f_wt[3 * i + j] * (double)uf[ftri_pnt[3 * t + j] * NV + n];
+        uc[i * NV + n] = (R)a;
+        if (uc0) uc0[i * NV + n] = (R)a;
     }
 }
 
 // h prolongation: u_f(i) += sum_j wt_j (u_c - u_c0)(coarse tri pnt j)
+template <typename R>
 __global__ void k_mg_prolong_h(int nfine, int NV, const int *f2c_tri, const double *f2c_wt, const int *ctri_pnt,
-                               const double *uc, const double *uc0, double *uf) {
+                               const R *uc, const R *uc0, R *uf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nfine) return;
     const int t = f2c_tri[i];
@@ -935,16 +940,17 @@ __global__ void k_mg_prolong_h(int nfine, int NV, const int *f2c_tri, const doub
         double a = 0.0;
         for (int j = 0; j < 3; ++j) {
             const int v0 = ctri_pnt[3 * t + j];
-            a += f2c_wt[3 * i + j] * (uc[v0 * NV + n] - uc0[v0 * NV + n]);
+            a += f2c_wt[3 * i + j] * (double)(uc[v0 * NV + n] - uc0[v0 * NV + n]);
         }
-        uf[i * NV + n] += a;
+        uf[i * NV + n] += (R)a;
     }
 }
 
 // FAS source (tri_hp::mg_source, nstage.cpp:113-129): dres = fadd*res0 - res(first)
-__global__ void k_fas_source(long n, double fadd, const double *res0, const double *res, double *dres) {
+template <typename R>
+__global__ void k_fas_source(long n, double fadd, const R *res0, const R *res, R *dres) {
     for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
-        dres[k] = fadd * res0[k] - res[k];
+        dres[k] = (R)fadd * res0[k] - res[k];
 }
 
 template <typename R>

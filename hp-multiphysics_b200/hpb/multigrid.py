@@ -27,6 +27,14 @@ def _bind():
         lib.hp_gpu_mg_prolongate.argtypes = [P]
         lib.hp_gpu_vcycle.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int]
+        lib.hp_gpu_solve_mg_graph.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_int)]
+        lib.hp_gpu_solve_mg_mixed.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_int)]
         lib.hp_gpu_solve_mg.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
@@ -104,6 +112,11 @@ class Hierarchy:
     def __init__(self, probs, kinds, stream=None, fadd=1.0):
         lib = _bind()
         self.probs = probs
+        if stream is None:
+            # one stream for every level: the whole cycle can then be one CUDA graph
+            import torch
+            self._stream = torch.cuda.Stream()
+            stream = ctypes.c_void_p(self._stream.cuda_stream)
         self.levels = [GPULevel(pr, 0, stream) for pr in probs]
         self._keep = []
         for l in range(1, len(probs)):
@@ -123,13 +136,26 @@ class Hierarchy:
         arr = (P * len(self.levels))(*[lv.h for lv in self.levels])
         return arr
 
-    def solve(self, drop=1e-10, max_cycles=500, vw=1, itercrsn=2, iterrfne=2, prcn_every=0):
+    def solve(self, drop=1e-10, max_cycles=500, vw=1, itercrsn=2, iterrfne=2, prcn_every=0, graph=False,
+              check_every=1, mixed=False):
+        """Cycles until the FP64 residual drops by `drop`; returns (hist, seconds, cycles).
+        graph=True replays one captured CUDA graph per cycle (preconditioners frozen);
+        mixed=True runs FP32 cycles on the correction equation inside FP64 defect correction."""
         cap = max_cycles + 2
         hist = np.zeros(cap)
         nh = ctypes.c_int(); sec = ctypes.c_double(); nc = ctypes.c_int()
-        L.check(self.lib.hp_gpu_solve_mg(self.handles(), len(self.levels), drop, max_cycles, vw, itercrsn, iterrfne,
-                                         prcn_every, L.ptr(hist), cap, ctypes.byref(nh), ctypes.byref(sec),
-                                         ctypes.byref(nc)), "solve_mg")
+        if mixed:
+            L.check(self.lib.hp_gpu_solve_mg_mixed(self.handles(), len(self.levels), drop, max_cycles, vw, itercrsn,
+                                                   iterrfne, prcn_every, L.ptr(hist), cap, ctypes.byref(nh),
+                                                   ctypes.byref(sec), ctypes.byref(nc)), "solve_mg_mixed")
+        elif graph:
+            L.check(self.lib.hp_gpu_solve_mg_graph(self.handles(), len(self.levels), drop, max_cycles, vw, itercrsn,
+                                                   iterrfne, check_every, L.ptr(hist), cap, ctypes.byref(nh),
+                                                   ctypes.byref(sec), ctypes.byref(nc)), "solve_mg_graph")
+        else:
+            L.check(self.lib.hp_gpu_solve_mg(self.handles(), len(self.levels), drop, max_cycles, vw, itercrsn,
+                                             iterrfne, prcn_every, L.ptr(hist), cap, ctypes.byref(nh),
+                                             ctypes.byref(sec), ctypes.byref(nc)), "solve_mg")
         return hist[:nh.value], sec.value, nc.value
 
     def close(self):
@@ -147,17 +173,19 @@ def p_sequence(p):
     return seq
 
 
-def build(factory, n, p, hlevels=0, stream=None, cfl=None, **kw):
+def build(factory, n, p, hlevels=0, stream=None, cfl=None, plevels=True, **kw):
     """Hierarchy for a workload factory(n=..., p=...): p-levels of the fine mesh
-    down to p = 1, then `hlevels` split-square meshes of n/2, n/4, ... at p = 1.
-    cfl: None (the per-log2p defaults), a number, or a dict p -> cfl."""
+    down to p = 1 (unless plevels=False: the fine level goes straight to the h-levels,
+    as the reference does with extra_finest_levels = 0), then `hlevels` split-square
+    meshes of n/2, n/4, ... at p = 1. cfl: None (the per-log2p defaults), a number,
+    or a dict p -> cfl."""
     def cf(q):
         if cfl is None:
             return {}
         return {"cfl": cfl[q] if isinstance(cfl, dict) else cfl}
     probs = [factory(n=n, p=p, **cf(p), **kw)]
     kinds = ["fine"]
-    for q in p_sequence(p):
+    for q in (p_sequence(p) if plevels else []):
         probs.append(factory(n=n, p=q, **cf(q), **kw))
         kinds.append("p")
     m = n

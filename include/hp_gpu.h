@@ -234,6 +234,31 @@ int hp_gpu_solve_mg(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycle
                     int iterrfne, int prcn_every, double *hist, int hist_cap, int *n_hist, double *seconds,
                     int *cycles);
 
+/* One whole cycle of block::cycle as a single CUDA graph (all levels created on
+ * one stream, every level's preconditioner set up before capture and frozen
+ * inside the graph). The opaque handle is replayed with hp_gpu_launch_vcycle
+ * (count cycles back to back on the finest level's stream) and freed with
+ * hp_gpu_destroy_vcycle. */
+int hp_gpu_capture_vcycle(hp_gpu_ctx **levels, int nlevels, int vw, int itercrsn, int iterrfne, void **graph);
+int hp_gpu_launch_vcycle(void *graph, hp_gpu_ctx *finest, int count);
+int hp_gpu_destroy_vcycle(void *graph);
+/* hp_gpu_solve_mg with the cycle replayed from one captured graph: the first
+ * cycle runs level by level with the preconditioners evaluated, the rest replay
+ * the graph, `check_every` cycles between residual checks. */
+int hp_gpu_solve_mg_graph(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
+                          int iterrfne, int check_every, double *hist, int hist_cap, int *n_hist, double *seconds,
+                          int *cycles);
+
+/* Multigrid inside FP64 defect correction: each cycle evaluates the FP64
+ * residual R64(u) on levels[0], runs one FP32 cycle of the hierarchy on the
+ * correction equation (every level in correction form about its base state,
+ * fp32 of u restricted down the levels, FP32 FAS sources between levels), and
+ * adds the fine correction to u in FP64. Preconditioners (FP64, copied to FP32)
+ * on the first cycle and every prcn_every cycles. Arguments as hp_gpu_solve_mg. */
+int hp_gpu_solve_mg_mixed(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
+                          int iterrfne, int prcn_every, double *hist, int hist_cap, int *n_hist, double *seconds,
+                          int *cycles);
+
 /* Diagnostic: n multistage updates of the FP32 smoother in plain form, from
  * fp32(u), written back to the FP64 state (compares the FP32 kernels with the
  * FP64 ones update by update). Needs setup_preconditioner() first. */

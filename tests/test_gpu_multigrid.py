@@ -102,3 +102,45 @@ def test_vcycle_converges_ins_kovasznay():
     hist, sec, cycles = H.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2)
     assert hist[-1] <= 1e-10, hist[-5:]
     H.close()
+
+
+@pytest.mark.parametrize("kind", ["cd", "ins"])
+def test_mixed_multigrid_matches_fp64_multigrid(kind):
+    """FP32 cycles on the correction equation inside FP64 defect correction reach
+    the 1e-10 drop of the FP64 residual and the FP64 multigrid solution."""
+    if kind == "cd":
+        mk = lambda n, p, **kw: hpb.cd_sinsin(n=n, p=p, kcond=1e-2, field=quad(), **kw)
+        cfl = {4: 0.5, 2: 0.75, 1: 1.0}
+    else:
+        mk = lambda n, p, **kw: hpb.kovasznay_ins(n=n, p=p, re=100.0, **kw)
+        cfl = None
+    H1 = MG.build(mk, n=16, p=4, hlevels=2, cfl=cfl)
+    h1, s1, c1 = H1.solve(drop=1e-10, max_cycles=400)
+    u1 = H1.levels[0].state()
+    H1.close()
+    H2 = MG.build(mk, n=16, p=4, hlevels=2, cfl=cfl)
+    h2, s2, c2 = H2.solve(drop=1e-10, max_cycles=400, mixed=True)
+    u2 = H2.levels[0].state()
+    H2.close()
+    assert h1[-1] <= 1e-10 and h2[-1] <= 1e-10, (h1[-3:], h2[-3:])
+    num = np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u1, u2)))
+    den = np.sqrt(sum(np.sum(a * a) for a in u1))
+    assert num / den < 1e-9
+
+
+def test_vcycle_graph_matches_level_by_level():
+    mk = lambda n, p, **kw: hpb.kovasznay_ins(n=n, p=p, re=100.0, **kw)
+    H1 = MG.build(mk, n=16, p=4, hlevels=2)
+    h1, s1, c1 = H1.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2)
+    u1 = H1.levels[0].state()
+    H1.close()
+    H2 = MG.build(mk, n=16, p=4, hlevels=2)
+    h2, s2, c2 = H2.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2, graph=True)
+    u2 = H2.levels[0].state()
+    H2.close()
+    assert h2[-1] <= 1e-10
+    # the graph freezes the preconditioners after the first cycle, as prcn_every=0 does
+    assert abs(c1 - c2) <= 2
+    num = np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u1, u2)))
+    den = np.sqrt(sum(np.sum(a * a) for a in u1))
+    assert num / den < 1e-8
