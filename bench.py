@@ -196,6 +196,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quick", action="store_true",
                     help="device-timed rsdl steps only (no e2e, update or CPU legs); for profiler runs")
+    ap.add_argument("--profile", choices=["update64", "update32"], default=None,
+                    help="run `steps` multistage updates of the workload in FP64 or FP32 (for profiler runs)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -242,6 +244,17 @@ def main():
 
     def enqueue_rsdl():
         hpb._lib.check(lib.hp_gpu_enqueue_rsdl(lvl.h, ns), "rsdl")
+
+    if args.profile:
+        for k in range(args.warmup + args.steps):
+            if args.profile == "update64":
+                hpb._lib.check(lib.hp_gpu_enqueue_update(lvl.h), "update")
+            else:
+                hpb._lib.check(lib.hp_gpu_fp32_updates(lvl.h, 1), "fp32 update")
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "updates": args.warmup + args.steps}))
+        lvl.close()
+        return
 
     for _ in range(max(3, args.warmup)):
         enqueue_rsdl()

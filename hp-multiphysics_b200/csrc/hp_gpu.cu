@@ -119,6 +119,12 @@ struct Launchers {
                  unsigned long long *slot, cudaStream_t);
     int elem_smem;
     cudaError_t (*set_smem)();
+    // cd element operators: length of one operator array, build, apply
+    size_t (*emat_len)(long ntri);
+    void (*emat_build)(const void *tab, const Mesh &, const State<R> &, const Phys &, ElemMat<R>, int nsm,
+                       cudaStream_t);
+    void (*emat_apply)(ElemMat<R>, const Mesh &, const State<R> &, const Phys &, int stage, int zero_rr, int nsm,
+                       cudaStream_t);
 };
 
 template <typename R, int P, int PHYS>
@@ -135,7 +141,33 @@ struct LaunchImpl {
         const int cap = nsm * 16;
         if (blocks > cap) blocks = cap;
         k_rsdl_elem<R, P, PHYS><<<blocks, C::WPC * 32, smem(), st>>>(
-            reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, stage, zero_rr, diff);
+            reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, stage, zero_rr, diff, ElemMat<R>{});
+    }
+    static size_t emat_len(long ntri) { return EmatCfg<P>::len(ntri); }
+    // one warp item per (element, column j <= T) at beta(nstage) = 1
+    static void emat_build(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, ElemMat<R> em, int nsm,
+                           cudaStream_t st) {
+        if constexpr (PHYS == 0) {
+            const long items = (long)m.ntri * (C::T + 1);
+            long blocks = (items + C::WPC - 1) / C::WPC;
+            if (blocks > (long)nsm * 16) blocks = (long)nsm * 16;
+            k_rsdl_elem<R, P, PHYS><<<(int)blocks, C::WPC * 32, smem(), st>>>(
+                reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, ph.nstage, 1, 0, em);
+        }
+    }
+    static void emat_apply(ElemMat<R> em, const Mesh &m, const State<R> &s, const Phys &ph, int stage, int zero_rr,
+                           int nsm, cudaStream_t st) {
+        if constexpr (PHYS == 0) {
+            using E = EmatCfg<P>;
+            const long ntiles = ((long)m.ntri + E::EB - 1) / E::EB;
+            if (ph.beta[stage] > 0.0) {
+                const long blocks = std::min(ntiles, (long)nsm * (2048 / E::THREADS_RE));
+                k_rsdl_emat<R, P, true><<<(int)blocks, E::THREADS_RE, 0, st>>>(em, m, s, ph, stage, zero_rr);
+            } else {
+                const long blocks = std::min(ntiles, (long)nsm * (2048 / E::THREADS_IM));
+                k_rsdl_emat<R, P, false><<<(int)blocks, E::THREADS_IM, 0, st>>>(em, m, s, ph, stage, zero_rr);
+            }
+        }
     }
     static void bflux(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int diff, cudaStream_t st) {
         if (PHYS == 1 && m.nbseg > 0)
@@ -168,6 +200,9 @@ struct LaunchImpl {
         L.vert = &vert;
         L.elem_smem = smem();
         L.set_smem = &set_smem_attr;
+        L.emat_len = &emat_len;
+        L.emat_build = &emat_build;
+        L.emat_apply = &emat_apply;
         return L;
     }
 };
@@ -251,6 +286,10 @@ struct hp_gpu_ctx {
     double *fasv = nullptr, *fass = nullptr, *fasi = nullptr;     // FAS source dres
     int *f2c_tri = nullptr, *c2f_tri = nullptr;
     double *f2c_wt = nullptr, *c2f_wt = nullptr;
+    // cd element operators (FP64 built by the element kernel, FP32 converted copy)
+    bool emat_on = false, emat_built = false;
+    ElemMat<double> em{};
+    ElemMat<float> em32{};
     // FP32 multigrid on the correction equation: restricted residual and entry state
     float *r0v32 = nullptr, *r0s32 = nullptr, *r0i32 = nullptr, *c0v32 = nullptr, *c0s32 = nullptr, *c0i32 = nullptr;
 };
@@ -514,6 +553,20 @@ extern "C" int hp_gpu_device_ptrs(hp_gpu_ctx *c, double **ugv, double **ugs, dou
     return HP_OK;
 }
 
+static ElemMat<double> emat_of(hp_gpu_ctx *c, double) { return c->em; }
+static ElemMat<float> emat_of(hp_gpu_ctx *c, float) { return c->em32; }
+
+// Element part of rsdl(stage): the stored cd element operators once built, else the
+// matrix-free element kernel.
+template <typename R>
+static void launch_elem(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab, const State<R> &st, const Phys &ph,
+                        int stage, int zero_rr, int diff) {
+    if (c->emat_on && c->emat_built && ph.physics == HP_PHYS_CD && !diff)
+        L.emat_apply(emat_of(c, R()), c->mesh, st, ph, stage, zero_rr, c->nsm, c->stream);
+    else
+        L.elem(tab, c->mesh, st, ph, stage, zero_rr, diff, c->nsm, c->stream);
+}
+
 // Stream-ordered body of rsdl(stage) (no sync, capturable), either precision.
 template <typename R>
 static void enqueue_rsdl_t(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab, const State<R> &st, const Phys &ph,
@@ -524,7 +577,7 @@ static void enqueue_rsdl_t(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab
     const long n = (long)(c->lv + c->ls);
     k_rsdl_pre<R><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, st.resv, st.ress,
                                                                            st.rrv, st.rrs, (R)omb, zero_rr);
-    L.elem(tab, c->mesh, st, ph, stage, zero_rr, diff, c->nsm, c->stream);
+    launch_elem<R>(c, L, tab, st, ph, stage, zero_rr, diff);
     L.bflux(tab, c->mesh, st, ph, diff, c->stream);
 }
 static void enqueue_rsdl(hp_gpu_ctx *c, int stage) { enqueue_rsdl_t<double>(c, c->L, c->d_tab, c->st, c->ph, stage, 0); }
@@ -559,6 +612,11 @@ static void enqueue_update(hp_gpu_ctx *c) {
     k_hist_advance<<<1, 32, 0, c->stream>>>(c->d_slot, c->d_hist, c->d_iter, c->NV, c->hist_cap);
 }
 
+template <typename A, typename B>
+static void conv(hp_gpu_ctx *c, long n, const A *src, B *dst) {
+    if (n > 0) k_convert<A, B><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>(n, src, dst);
+}
+
 static int check_launch(hp_gpu_ctx *c) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) { set_err("kernel launch failed: %s", cudaGetErrorString(e)); return HP_ECUDA; }
@@ -586,7 +644,7 @@ extern "C" int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *c, int stage) {
         set_err("cd rsdl needs tau from setup_preconditioner");
         return HP_ESTATE;
     }
-    c->L.elem(c->d_tab, c->mesh, c->st, c->ph, stage, stage >= c->ph.nstage, 0, c->nsm, c->stream);
+    launch_elem<double>(c, c->L, c->d_tab, c->st, c->ph, stage, stage >= c->ph.nstage, 0);
     return check_launch(c);
 }
 
@@ -594,6 +652,51 @@ extern "C" int hp_gpu_rsdl(hp_gpu_ctx *c, int stage) {
     int r = hp_gpu_enqueue_rsdl(c, stage);
     if (r) return r;
     return hp_gpu_sync(c);
+}
+
+static void drop_update_graphs(hp_gpu_ctx *c) {
+    if (c->g_update) { cudaGraphExecDestroy(c->g_update); c->g_update = nullptr; }
+    if (c->g_update32) { cudaGraphExecDestroy(c->g_update32); c->g_update32 = nullptr; }
+}
+
+// The cd element operators depend on the geometry, the fixed physics parameters and
+// tau; cd tau is a function of the geometry and those parameters alone (steady
+// problems), so one build after the first preconditioner set-up stays valid.
+static int build_element_matrices(hp_gpu_ctx *c) {
+    const size_t n = c->L.emat_len(c->ntri), nb = (size_t)c->ntri * ((c->p + 1) * (c->p + 2) / 2);
+    int r;
+    if (!c->em.aim) {
+        if ((r = dalloc(c, (void **)&c->em.aim, n * 8))) return r;
+        if ((r = dalloc(c, (void **)&c->em.are, n * 8))) return r;
+        if ((r = dalloc(c, (void **)&c->em.bre, nb * 8))) return r;
+        if ((r = dalloc(c, (void **)&c->em32.aim, n * 4))) return r;
+        if ((r = dalloc(c, (void **)&c->em32.are, n * 4))) return r;
+        if ((r = dalloc(c, (void **)&c->em32.bre, nb * 4))) return r;
+        CK(cudaMemsetAsync(c->em.aim, 0, n * 8, c->stream));  // padding of the last tile
+        CK(cudaMemsetAsync(c->em.are, 0, n * 8, c->stream));
+    }
+    c->L.emat_build(c->d_tab, c->mesh, c->st, c->ph, c->em, c->nsm, c->stream);
+    conv(c, (long)n, c->em.aim, c->em32.aim);
+    conv(c, (long)n, c->em.are, c->em32.are);
+    conv(c, (long)nb, c->em.bre, c->em32.bre);
+    if ((r = check_launch(c))) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    c->emat_built = true;
+    drop_update_graphs(c);
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_set_element_matrices(hp_gpu_ctx *c, int on) {
+    if (!c) return HP_EINVAL;
+    if (on && c->ph.physics != HP_PHYS_CD) {
+        set_err("element operators are built for the linear cd residual only");
+        return HP_ENOTSUP;
+    }
+    if ((bool)on == c->emat_on) return HP_OK;
+    c->emat_on = on != 0;
+    drop_update_graphs(c);
+    if (c->emat_on && !c->emat_built && c->prcn_ready) return build_element_matrices(c);
+    return HP_OK;
 }
 
 extern "C" int hp_gpu_setup_preconditioner(hp_gpu_ctx *c) {
@@ -620,6 +723,7 @@ extern "C" int hp_gpu_setup_preconditioner(hp_gpu_ctx *c) {
     CK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->prcn_ready = true;
+    if (herr == 0 && c->emat_on && !c->emat_built && (r = build_element_matrices(c))) return r;
     return herr;
 }
 
@@ -670,6 +774,7 @@ extern "C" int hp_gpu_iterate(hp_gpu_ctx *c, int iters, int prcn_interval, doubl
         if (!c->prcn_ready || (prcn_interval > 0 && it % prcn_interval == 0 && it > 0)) {
             r = hp_gpu_setup_preconditioner(c);
             if (r) return r;
+            if ((r = ensure_update_graph(c))) return r;  // a first set-up may switch the element path
         }
         CK(cudaGraphLaunch(c->g_update, c->stream));
     }
@@ -764,11 +869,6 @@ static int alloc_mixed(hp_gpu_ctx *c) {
     return HP_OK;
 }
 
-template <typename A, typename B>
-static void conv(hp_gpu_ctx *c, long n, const A *src, B *dst) {
-    if (n > 0) k_convert<A, B><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>(n, src, dst);
-}
-
 // FP32 copies of the FP64 preconditioner (computed at the base state)
 static void mixed_prcn(hp_gpu_ctx *c) {
     State<float> &f = c->s32;
@@ -854,6 +954,9 @@ extern "C" int hp_gpu_solve(hp_gpu_ctx *c, int mode, double drop, int max_update
     double r0 = 0.0, rn = 0.0;
     r = hp_gpu_setup_preconditioner(c);
     if (r) return r < 0 ? r : HP_ESTATE;
+    // the first set-up may have built element operators and dropped the update graphs
+    if ((r = ensure_update_graph(c))) return r;
+    if (mode == HP_PREC_FP32 && (r = ensure_update32_graph(c))) return r;
     if ((r = fp64_norm(c, &r0))) return r;
     if (hist && nh < hist_cap) hist[nh++] = 1.0;
     if (mode == HP_PREC_FP32) mixed_prcn(c);

@@ -2,7 +2,7 @@
 //
 // Layout in HBM (element-major blocks, the reference's own blitz layouts):
 //   ug.v/res.v/res_r.v [npnt][NV], ug.s/... [nseg][sm][NV], ug.i/... [ntri][im][NV]
-//   mesh: tri_pnt/tri_seg [ntri][3] int32, tri_sgn packed as 3 bits per element,
+//   mesh: tri_pnt/tri_seg/tri_sgn [ntri][3] int32,
 //         seg_pnt/seg_tri/seg_loc [nseg][2], vertex incidence in CSR form.
 // Each element is processed by one warp: the warp gathers the element's modes,
 // runs the sum-factorised contractions (proj -> point fluxes -> intgrtrs,
@@ -107,10 +107,32 @@ struct ElemCfg {
 // fluxes are the exact differences F(b+d) - F(b) of the convective, pressure and
 // viscous terms, the SUPG term A(b+d) tau(b) res(d) with tau frozen at the base.
 
+// Element operators of the linear cd residual. For uht = e_j, aim(t, j, m) = lf_im(m)
+// and are(t, j, m) = lf_re(m) at beta = 1; bre[t][m] = lf_re(m) of the source alone
+// (uht = 0). Storage is in tiles of EB elements, column-major inside a tile, so that
+// the EB*T entries of one column j that a CTA reads together are contiguous:
+//   index(t, j, m) = ((t / EB) * T + j) * (EB * T) + (t % EB) * T + m.
+template <typename R>
+struct ElemMat {
+    R *aim, *are, *bre;
+};
+
+template <int P>
+struct EmatCfg {
+    static constexpr int T = (P + 1) * (P + 2) / 2;
+    static constexpr int EB = (128 / T > 0 ? 128 / T : 1);                  // elements per tile
+    static constexpr int THREADS_RE = ((2 * EB * T + 31) / 32) * 32;       // beta > 0: A_im and A_re rows
+    static constexpr int THREADS_IM = ((EB * T + 31) / 32) * 32;           // beta = 0: A_im rows only
+    __host__ __device__ static size_t idx(long t, int j, int m) {
+        return ((size_t)(t / EB) * T + j) * (size_t)(EB * T) + (size_t)(t % EB) * T + m;
+    }
+    static size_t len(long ntri) { return (size_t)((ntri + EB - 1) / EB) * T * (size_t)(EB * T); }
+};
+
 template <typename R, int P, int PHYS>
 __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
     k_rsdl_elem(const DevTables<R, P> *__restrict__ gtab, Mesh mesh, State<R> st, Phys ph, int stage, int zero_rr,
-                int diff) {
+                int diff, ElemMat<R> build) {
     using C = ElemCfg<R, P, PHYS>;
     constexpr int G = C::G, X = C::X, T = C::T, IM = C::IM, BM = C::BM, NV = C::NV, GG = G * G;
     constexpr int SM = (C::SM > 0 ? C::SM : 1);  // side-mode stride (unused when p = 1)
@@ -133,13 +155,20 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
     const R beta = (R)ph.beta[stage];
     const R omb = zero_rr ? (R)0 : (R)1 - beta;
 
-    for (int tind = blockIdx.x * C::WPC + warp; tind < mesh.ntri; tind += gridDim.x * C::WPC) {
+    // build mode (cd): one item per (element, column j) with uht = e_j, j = T: uht = 0
+    const bool bmode = (PHYS == 0) && build.aim != nullptr;
+    const long nitems = bmode ? (long)mesh.ntri * (T + 1) : (long)mesh.ntri;
+    for (long item = (long)blockIdx.x * C::WPC + warp; item < nitems; item += (long)gridDim.x * C::WPC) {
+        const int tind = bmode ? (int)(item / (T + 1)) : (int)item;
+        const int bcol = bmode ? (int)(item - (long)tind * (T + 1)) : -1;
         const int p0 = mesh.tri_pnt[3 * tind], p1 = mesh.tri_pnt[3 * tind + 1], p2 = mesh.tri_pnt[3 * tind + 2];
         // ---- gather (ugtouht, gtol.cpp:14-55)
         for (int w = lane; w < NV * T; w += 32) {
             const int n = w / T, m = w - n * T;
             R val;
-            if (m < 3) {
+            if (bmode) {
+                val = (m == bcol) ? (R)1 : (R)0;
+            } else if (m < 3) {
                 const int v = (m == 0 ? p0 : (m == 1 ? p1 : p2));
                 val = st.ugv[v * NV + n];
             } else if (m < BM) {
@@ -337,10 +366,14 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
         };
         intgrtrs_stageI(0);
         __syncwarp();
+        // the cd source enters only the uht = 0 column of the build
+        const R srcv = (bmode && bcol < T) ? (R)0 : (R)ph.src;
         for (int w = lane; w < NV * T; w += 32) {
             const int n = w / T, m = w - n * T;
             const R val = mode_result(n, m);
-            if (m < BM) {
+            if (bmode) {
+                if (bcol < T) build.aim[EmatCfg<P>::idx(tind, bcol, m)] = val;
+            } else if (m < BM) {
                 scatter(st.resv, st.ress, n, m, val);
             } else {
                 const size_t gi = ((size_t)tind * IM + (m - BM)) * NV + n;
@@ -361,7 +394,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                 const R *fr = PT(sr), *fs = PT(ss);
                 R acc;
                 if (PHYS == 1) acc = (R)0;  // rhorbd0*u + dugdt with bd(0) = 0
-                else acc = -(d00 * d11 - d10 * d01) * (R)ph.src;
+                else acc = -(d00 * d11 - d10 * d01) * srcv;
                 const R ln0 = tb.n0[j];
                 {
                     const R wi = fr[i * G + j] * tb.dltx[i] * ln0;
@@ -422,9 +455,9 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
             for (int w = lane; w < NV * T; w += 32) {
                 const int n = w / T, m = w - n * T;
                 R val = mode_result(n, m);
-                if (PHYS == 0 && ph.src != 0.0) {
+                if (PHYS == 0 && srcv != (R)0) {
                     // intgrt of a constant field c: sum_j gnwtn(m,j) * sum_i c*gxwtx(col,i)
-                    const R cval = -(d00 * d11 - d10 * d01) * (R)ph.src;
+                    const R cval = -(d00 * d11 - d10 * d01) * srcv;
                     const int col = tb.colof[m];
                     R l0 = 0;
                     for (int j = 0; j < G; ++j) {
@@ -435,7 +468,10 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                     val = l0 + val;
                 }
                 val *= beta;
-                if (m < BM) {
+                if (bmode) {
+                    if (bcol < T) build.are[EmatCfg<P>::idx(tind, bcol, m)] = val;
+                    else build.bre[(size_t)tind * T + m] = val;
+                } else if (m < BM) {
                     scatter(st.rrv, st.rrs, n, m, val);
                 } else {
                     const size_t gi = ((size_t)tind * IM + (m - BM)) * NV + n;
@@ -446,6 +482,93 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
             }
         }
         __syncwarp();
+    }
+}
+
+// Linear cd residual from the stored element operators: lf_im = A_im uht and
+// lf_re = beta (A_re uht + b_re), with the gather, scatter, res_r mixing and dres of
+// k_rsdl_elem (tri_hp/cd/rsdl.cpp:14-154 through tri_hp/nstage.cpp:21-82). One CTA
+// per tile of EB elements: gather the tile's coefficients to shared memory, one
+// thread per operator row (RE: A_im and A_re rows; otherwise A_im only) streams its
+// T contiguous-by-tile column entries, then one thread per (element, mode) scatters.
+template <typename R, int P, bool RE>
+__global__ void __launch_bounds__(RE ? EmatCfg<P>::THREADS_RE : EmatCfg<P>::THREADS_IM)
+    k_rsdl_emat(ElemMat<R> em, Mesh mesh, State<R> st, Phys ph, int stage, int zero_rr) {
+    using E = EmatCfg<P>;
+    constexpr int T = E::T, EB = E::EB, BM = 3 * P, IM = (P - 1) * (P - 2) / 2;
+    constexpr int SM = (P > 1 ? P - 1 : 1);  // side-mode stride (unused when p = 1)
+    constexpr int NH = RE ? 2 : 1;
+    __shared__ R su[EB * T];
+    __shared__ R sr[NH * EB * T];
+    const R beta = (R)ph.beta[stage];
+    const R omb = zero_rr ? (R)0 : (R)1 - beta;
+    const bool src = RE && ph.src != 0.0;
+    const long ntiles = ((long)mesh.ntri + EB - 1) / EB;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long t0 = tile * EB;
+        for (int w = threadIdx.x; w < EB * T; w += blockDim.x) {
+            const int e = w / T, m = w - e * T;
+            const long t = t0 + e;
+            R val = (R)0;
+            if (t < mesh.ntri) {
+                if (m < 3) {
+                    val = st.ugv[mesh.tri_pnt[3 * t + m]];
+                } else if (m < BM) {
+                    const int i = (m - 3) / SM, k = (m - 3) - i * SM;
+                    val = st.ugs[mesh.tri_seg[3 * t + i] * SM + k];
+                    if ((k & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
+                } else {
+                    val = st.ugi[t * IM + (m - BM)];
+                }
+            }
+            su[w] = val;
+        }
+        __syncthreads();
+        for (int w = threadIdx.x; w < NH * EB * T; w += blockDim.x) {
+            const int h = w / (EB * T), q = w - h * (EB * T), e = q / T;
+            if (t0 + e < mesh.ntri) {
+                const R *a = (h ? em.are : em.aim) + (size_t)tile * T * (EB * T) + q;
+                const R *u = su + e * T;
+                R acc = (R)0;
+#pragma unroll
+                for (int j = 0; j < T; ++j) acc = fma(__ldg(a + (size_t)j * (EB * T)), u[j], acc);
+                if (h) {
+                    if (src) acc += __ldg(em.bre + (size_t)t0 * T + q);
+                    acc *= beta;
+                }
+                sr[w] = acc;
+            }
+        }
+        __syncthreads();
+        for (int w = threadIdx.x; w < EB * T; w += blockDim.x) {
+            const int e = w / T, m = w - e * T;
+            const long t = t0 + e;
+            if (t >= mesh.ntri) continue;
+            const R vim = sr[w];
+            const R vre = RE ? sr[EB * T + w] : (R)0;
+            if (m < 3) {
+                const int v = mesh.tri_pnt[3 * t + m];
+                atomic_add(&st.resv[v], vim);
+                if (RE) atomic_add(&st.rrv[v], vre);
+            } else if (m < BM) {
+                const int i = (m - 3) / SM, k = (m - 3) - i * SM;
+                const int g = mesh.tri_seg[3 * t + i] * SM + k;
+                const bool flip = (k & 1) && mesh.tri_sgn[3 * t + i] < 0;
+                atomic_add(&st.ress[g], flip ? -vim : vim);
+                if (RE) atomic_add(&st.rrs[g], flip ? -vre : vre);
+            } else {
+                const size_t gi = (size_t)t * IM + (m - BM);
+                const R d = st.dresi ? st.dresi[gi] : (R)0;
+                if (RE) {
+                    const R rr = st.rri[gi] * omb + vre;
+                    st.rri[gi] = rr;
+                    st.resi[gi] = vim + d + rr;
+                } else {
+                    st.resi[gi] = vim + st.rri[gi] * omb + d;  // res_r unchanged when beta = 0
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 

@@ -132,6 +132,11 @@ class Hierarchy:
                                                fadd), "mg_attach_h")
         self.lib = lib
 
+    def element_matrices(self, on=True):
+        """cd: every level's rsdl from stored element operators (hp_gpu_set_element_matrices)."""
+        for lv in self.levels:
+            lv.element_matrices(on)
+
     def handles(self):
         arr = (P * len(self.levels))(*[lv.h for lv in self.levels])
         return arr

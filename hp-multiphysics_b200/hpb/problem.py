@@ -219,6 +219,10 @@ class GPULevel:
     def rsdl(self, stage):
         L.check(self.lib.hp_gpu_rsdl(self.h, stage), "rsdl")
 
+    def element_matrices(self, on=True):
+        """cd only: rsdl from stored element operators (hp_gpu_set_element_matrices)."""
+        L.check(self.lib.hp_gpu_set_element_matrices(self.h, 1 if on else 0), "set_element_matrices")
+
     def minvrt(self):
         L.check(self.lib.hp_gpu_minvrt(self.h), "minvrt")
 

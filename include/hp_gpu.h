@@ -187,6 +187,18 @@ int hp_gpu_enqueue_update(hp_gpu_ctx *ctx);
  * nstage.cpp:52-73: ugtouht, element_rsdl, lftog), for timing it in isolation. */
 int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *ctx, int stage);
 
+/* Stored element operators for the linear cd residual. No counterpart in the
+ * reference: tri_hp::rsdl (nstage.cpp:52-73) recomputes element_rsdl
+ * (tri_hp/cd/rsdl.cpp:14-154) every call; for cd the element residual is affine
+ * in the element's coefficients, lf_im = A_im u and lf_re = beta (A_re u + b_re),
+ * so on = 1 builds A_im, A_re, b_re of every element once (FP64 by the element
+ * kernel applied to unit vectors, plus an FP32 copy for the FP32 smoother) at the
+ * first setup_preconditioner() (or at once if that has run), and every later
+ * rsdl of either precision becomes a streamed batched mat-vec with the same
+ * result up to rounding. on = 0 returns to the matrix-free kernel (the storage
+ * is kept until hp_gpu_destroy). HP_ENOTSUP for ins. */
+int hp_gpu_set_element_matrices(hp_gpu_ctx *ctx, int on);
+
 /* Convergence driver. Runs smoothing until the unpreconditioned FP64 residual
  * norm ||R64(u)||_2 (all v/s/i modes of rsdl(nstage), without the rows of
  * essential boundary values, which the boundary condition replaces) has dropped by `drop` from
