@@ -6,7 +6,9 @@ Workload (N = 1): scalar convection-diffusion (tri_hp cd, CONST_A), velocity
 317 x 317 split-square mesh of the unit square (200,978 triangles, 1.61 M
 DOF). Seeded synthetic state: the Dirichlet field projected onto the basis plus
 U[-1,1) * 1e-3 noise (splitmix64). A "step" is one full FP64 residual
-evaluation tri_hp::rsdl(nstage) over the whole mesh; `value` is rsdl GDoF/s
+evaluation tri_hp::rsdl(nstage) over the whole mesh, computed from the stored
+cd element operators (built once before the timed steps; the matrix-free
+element kernel is timed beside it); `value` is rsdl GDoF/s
 (whole job, inputs resident in HBM, device time, L2 flushed between steps);
 `e2e` is the same metric through the C-ABI with host buffers (state upload from
 pinned memory + rsdl + residual download every step, wall clock).
@@ -123,68 +125,101 @@ def run_cpu(cores, secs, n=60):
 
 
 TOL_N = 64
+MG_N = 320
+
+
+def _rel(a, b):
+    import numpy as np
+    return float(np.sqrt(sum(np.sum((x - y) ** 2) for x, y in zip(a, b))) / np.sqrt(sum(np.sum(x * x) for x in a)))
 
 
 def time_to_tolerance(hpb, dev):
-    """Time to a 1e-10 drop of the FP64 residual norm (Dirichlet rows excluded), plain
-    FP64 smoothing against FP32 correction smoothing with FP64 defect correction, on
-    cd p=4 with Dirichlet data -(x-8)^2 on a 64x64 split-square mesh (a size the
-    single-grid smoother converges on in a few thousand updates). Device time of the
-    whole solve (hp_gpu_solve), residual checks included."""
+    """Time to a 1e-10 drop of the FP64 residual norm (Dirichlet rows excluded) on cd p=4
+    with Dirichlet data -(x-8)^2, velocity (1,0.5), kcond 1e-3, noise 1e-3. `seconds` is
+    the device time of the whole solve (preconditioner set-up and residual checks
+    included) plus, for the arms with stored element operators, the wall time of their
+    one-time build (allocation included). Arms: plain FP64 (matrix-free element kernel, the reference's algorithm),
+    FP64 with stored element operators, FP32 correction smoothing inside FP64 defect
+    correction (stored operators), and that plus the learned preconditioner correction.
+    Two drivers: single-grid smoothing on a 64x64 split-square mesh, and V-cycles
+    (p 4 -> 2 -> 1, then 4 h-levels) on a 320x320 mesh (204,800 triangles)."""
     import ctypes as C
+    import time as _t
     import numpy as np
     from hpb import _lib as L
-    out = {"workload": f"tri_hp cd p={P}, {TOL_N}x{TOL_N} split-square mesh ({2 * TOL_N * TOL_N} triangles), "
-                       "velocity (1,0.5), kcond 1e-3, Dirichlet -(x-8)^2, cfl 0.5, noise 1e-3",
-           "drop": 1e-10, "criterion": "||R64||_2 / ||R64(u0)||_2 over all non-Dirichlet v/s/i rows"}
-    states = {}
-    for name, mixed in (("fp64", False), ("fp32_defect_correction", True)):
-        f = L.Field(L.HP_FIELD_QUADX, (C.c_double * 4)(-1.0, 8.0, 0, 0))
-        pr = hpb.cd_sinsin(n=TOL_N, p=P, kcond=1e-3, cfl=0.5, field=f, noise=1e-3, seed=20261205)
-        g = pr.gpu(device=dev)
-        hist, sec, upd = g.solve(mixed=mixed, drop=1e-10, max_updates=20000, inner=20, check_every=20)
-        states[name] = g.state()
-        out[name] = {"seconds": sec, "updates": upd, "final_drop": float(hist[-1]),
-                     "reached": bool(hist[-1] <= 1e-10)}
-        g.close()
-    # learned + FP32: a network trained on the GPU from the solver's own residual
-    # histories of 4 other instances of the same family (random velocity and
-    # diffusivity), then attached to the FP32 defect-correction solve
-    import time as _t
     from hpb import learned as LR
+    from hpb import multigrid as MG
+
+    def field():
+        return L.Field(L.HP_FIELD_QUADX, (C.c_double * 4)(-1.0, 8.0, 0, 0))
+
+    # the network: trained on the GPU from the solver's own residual histories of 4
+    # other instances of the same family (random velocity and diffusivity)
     t0 = _t.perf_counter()
     F, T = [], []
     for s in range(4):
         r = np.random.default_rng(300 + s)
         ax, ay = r.uniform(-1, 1, 2)
         kc = 10 ** r.uniform(-3, -1.5)
-        f = L.Field(L.HP_FIELD_QUADX, (C.c_double * 4)(-1.0, 8.0, 0, 0))
-        fs, ts = LR.solver_samples(lambda: hpb.cd_sinsin(n=TOL_N, p=P, ax=ax, ay=ay, kcond=kc, cfl=0.5, field=f,
-                                                         noise=1e-3, seed=300 + s))
+        fs, ts = LR.solver_samples(lambda: hpb.cd_sinsin(n=TOL_N, p=P, ax=ax, ay=ay, kcond=kc, cfl=0.5,
+                                                         field=field(), noise=1e-3, seed=300 + s))
         F.append(fs)
         T.append(ts)
-    net, hist = LR.train(np.concatenate(F), np.concatenate(T), steps=400)
+    net, _ = LR.train(np.concatenate(F), np.concatenate(T), steps=400)
     train_s = _t.perf_counter() - t0
-    f = L.Field(L.HP_FIELD_QUADX, (C.c_double * 4)(-1.0, 8.0, 0, 0))
-    pr = hpb.cd_sinsin(n=TOL_N, p=P, kcond=1e-3, cfl=0.5, field=f, noise=1e-3, seed=20261205)
-    g = pr.gpu(device=dev)
-    LR.attach(g, net, 1.0)
-    hist_l, sec, upd = g.solve(mixed=True, drop=1e-10, max_updates=20000, inner=20, check_every=20)
-    states["learned_fp32"] = g.state()
-    out["learned_fp32"] = {"seconds": sec, "updates": upd, "final_drop": float(hist_l[-1]),
-                           "reached": bool(hist_l[-1] <= 1e-10), "training_seconds_offline": train_s,
-                           "network": "17-64-64-64-1 BF16, FP32 accumulation, 400 Adam steps"}
-    g.close()
+
+    arms = (("fp64", False, False, False), ("fp64_elem_ops", False, True, False),
+            ("fp32_defect_correction", True, True, False), ("learned_fp32", True, True, True))
+    out = {"drop": 1e-10, "criterion": "||R64||_2 / ||R64(u0)||_2 over all non-Dirichlet v/s/i rows",
+           "network": {"widths": "17-64-64-64-1", "dtype": "BF16 weights, FP32 accumulation",
+                       "training": "400 Adam steps on the GPU, 4 solver-generated instances",
+                       "training_seconds_offline": train_s}}
+    sg = {"workload": f"single grid: cd p={P}, {TOL_N}x{TOL_N} split-square mesh ({2 * TOL_N * TOL_N} triangles), "
+                      "cfl 0.5, 20 updates per defect-correction cycle"}
+    states = {}
+    for name, mixed, em, learned in arms:
+        g = hpb.cd_sinsin(n=TOL_N, p=P, kcond=1e-3, cfl=0.5, field=field(), noise=1e-3, seed=20261205).gpu(device=dev)
+        tb = 0.0
+        if em:
+            t0 = _t.perf_counter()
+            g.element_matrices(True)
+            tb = _t.perf_counter() - t0
+        if learned:
+            LR.attach(g, net, 1.0)
+        hist, sec, upd = g.solve(mixed=mixed, drop=1e-10, max_updates=20000, inner=20, check_every=20)
+        states[name] = g.state()
+        sg[name] = {"seconds": sec + tb, "solve_seconds": sec, "operator_build_seconds": tb, "updates": upd,
+                    "final_drop": float(hist[-1]), "reached": bool(hist[-1] <= 1e-10),
+                    "rel_l2_state_diff_vs_fp64": _rel(states["fp64"], states[name])}
+        g.close()
+    sg["speedup_learned_fp32_vs_fp64"] = sg["fp64"]["seconds"] / sg["learned_fp32"]["seconds"]
+    sg["speedup_learned_fp32_vs_fp64_elem_ops"] = sg["fp64_elem_ops"]["seconds"] / sg["learned_fp32"]["seconds"]
+    out["single_grid"] = sg
+
+    mg = {"workload": f"multigrid: cd p={P}, {MG_N}x{MG_N} split-square mesh ({2 * MG_N * MG_N} triangles), levels "
+                      f"p=4,2,1 then h-levels {MG_N // 2},{MG_N // 4},{MG_N // 8},{MG_N // 16} at p=1, V-cycle with "
+                      "2+2 updates per level, cfl 0.5/0.75/1.0 for p=4/2/1; learned correction on the finest level"}
+    mk = lambda n, p, **kw: hpb.cd_sinsin(n=n, p=p, kcond=1e-3, field=field(), **kw)
+    states = {}
+    for name, mixed, em, learned in arms:
+        H = MG.build(mk, n=MG_N, p=P, hlevels=4, cfl={4: 0.5, 2: 0.75, 1: 1.0})
+        tb = 0.0
+        if em:
+            t0 = _t.perf_counter()
+            H.element_matrices(True)
+            tb = _t.perf_counter() - t0
+        if learned:
+            LR.attach(H.levels[0], net, 1.0)
+        hist, sec, cyc = H.solve(drop=1e-10, max_cycles=400, mixed=mixed)
+        states[name] = H.levels[0].state()
+        mg[name] = {"seconds": sec + tb, "solve_seconds": sec, "operator_build_seconds": tb, "cycles": cyc,
+                    "final_drop": float(hist[-1]), "reached": bool(hist[-1] <= 1e-10),
+                    "rel_l2_state_diff_vs_fp64": _rel(states["fp64"], states[name])}
+        H.close()
+    mg["speedup_learned_fp32_vs_fp64"] = mg["fp64"]["seconds"] / mg["learned_fp32"]["seconds"]
+    mg["speedup_learned_fp32_vs_fp64_elem_ops"] = mg["fp64_elem_ops"]["seconds"] / mg["learned_fp32"]["seconds"]
+    out["multigrid"] = mg
     net.close()
-    out["speedup_learned_fp32_vs_fp64"] = out["fp64"]["seconds"] / out["learned_fp32"]["seconds"]
-    a = states["fp64"]
-    c_ = states["learned_fp32"]
-    out["rel_l2_state_diff_learned"] = float(np.sqrt(sum(np.sum((x - y) ** 2) for x, y in zip(a, c_))) /
-                                             np.sqrt(sum(np.sum(x * x) for x in a)))
-    a, b = states["fp64"], states["fp32_defect_correction"]
-    out["rel_l2_state_diff"] = float(np.sqrt(sum(np.sum((x - y) ** 2) for x, y in zip(a, b))) /
-                                     np.sqrt(sum(np.sum(x * x) for x in a)))
-    out["speedup_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_defect_correction"]["seconds"]
     return out
 
 
@@ -194,8 +229,12 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mesh", type=int, default=N_MESH,
+                    help="split-square mesh size n (2 n^2 triangles); smaller cases are for profiler runs")
     ap.add_argument("--quick", action="store_true",
                     help="device-timed rsdl steps only (no e2e, update or CPU legs); for profiler runs")
+    ap.add_argument("--matrix-free", action="store_true",
+                    help="with --quick / --profile: the matrix-free element kernel instead of stored operators")
     ap.add_argument("--profile", choices=["update64", "update32"], default=None,
                     help="run `steps` multistage updates of the workload in FP64 or FP32 (for profiler runs)")
     args = ap.parse_args()
@@ -222,6 +261,7 @@ def main():
     import numpy as np
     import torch
     import hpb
+    from hpb._lib import check
 
     dist = None
     if world > 1:
@@ -234,7 +274,7 @@ def main():
     stream = torch.cuda.Stream()  # a non-default stream: the update graph is captured on it
     torch.cuda.set_stream(stream)
 
-    pr = hpb.cd_sinsin(n=N_MESH, p=P, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205)
+    pr = hpb.cd_sinsin(n=args.mesh, p=P, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205)
     lvl = hpb.GPULevel(pr, device=dev, stream=ctypes.c_void_p(stream.cuda_stream))
     lib = lvl.lib
     rc = lvl.setup_preconditioner()
@@ -242,22 +282,62 @@ def main():
     ns = pr.phys.nstage
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def enqueue_rsdl():
-        hpb._lib.check(lib.hp_gpu_enqueue_rsdl(lvl.h, ns), "rsdl")
-
-    if args.profile:
-        for k in range(args.warmup + args.steps):
-            if args.profile == "update64":
-                hpb._lib.check(lib.hp_gpu_enqueue_update(lvl.h), "update")
-            else:
-                hpb._lib.check(lib.hp_gpu_fp32_updates(lvl.h, 1), "fp32 update")
+    def timed(fn, n):
+        """Device ms of each of n calls of fn on the bench stream, L2 flushed before each."""
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            fn()
+            b.record(stream)
         torch.cuda.synchronize()
-        print(json.dumps({"profile": args.profile, "updates": args.warmup + args.steps}))
+        return [a.elapsed_time(b) for a, b in evs]
+
+    def rsdl():
+        check(lib.hp_gpu_enqueue_rsdl(lvl.h, ns), "rsdl")
+
+    def elem():
+        check(lib.hp_gpu_enqueue_element_rsdl(lvl.h, ns), "element_rsdl")
+
+    def update():
+        check(lib.hp_gpu_enqueue_update(lvl.h), "update")
+
+    if args.profile or args.quick:
+        if not args.matrix_free:
+            lvl.element_matrices(True)
+        if args.profile:
+            for k in range(args.warmup + args.steps):
+                if args.profile == "update64":
+                    update()
+                else:
+                    check(lib.hp_gpu_fp32_updates(lvl.h, 1), "fp32 update")
+            torch.cuda.synchronize()
+            print(json.dumps({"profile": args.profile, "updates": args.warmup + args.steps}))
+        else:
+            for _ in range(max(3, args.warmup)):
+                rsdl()
+            ms = timed(rsdl, args.steps)
+            print(json.dumps({"quick": True, "matrix_free": args.matrix_free, "ntri": pr.mesh.ntri,
+                              "ms_per_step": sum(ms) / args.steps,
+                              "value": pr.ndof * args.steps / (sum(ms) * 1e-3) / 1e9}))
         lvl.close()
         return
 
+    # matrix-free element kernel (the reference's per-call element_rsdl), for comparison
+    for _ in range(3):
+        rsdl()
+    torch.cuda.synchronize()
+    mf_ms = sum(timed(rsdl, args.steps)) / args.steps
+    mf_k = sum(timed(elem, args.steps)) / args.steps
+    mf_u = sum(timed(update, args.steps)) / args.steps
+
+    # stored element operators: built once, then every rsdl is a streamed batched mat-vec
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lvl.element_matrices(True)
+    build_ms = (time.perf_counter() - t0) * 1e3
     for _ in range(max(3, args.warmup)):
-        enqueue_rsdl()
+        rsdl()
     torch.cuda.synchronize()
 
     clk_file = os.path.join(ROOT, f"_clocks_{rank}.csv")
@@ -266,45 +346,16 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.zero_()
-        evs[k][0].record(stream)
-        enqueue_rsdl()
-        evs[k][1].record(stream)
-    torch.cuda.synchronize()
+    step_ms = timed(rsdl, args.steps)
     if dist:
         dist.barrier()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
     t_ms = sum(step_ms)
-    if args.quick:
-        if clk:
-            clk.terminate()
-            clk.wait()
-        print(json.dumps({"quick": True, "ms_per_step": t_ms / args.steps,
-                          "value": pr.ndof * args.steps / (t_ms * 1e-3) / 1e9}))
-        lvl.close()
-        return
-
-    # the dominant kernel alone (element residual) for the roofline
-    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.zero_()
-        kev[k][0].record(stream)
-        hpb._lib.check(lib.hp_gpu_enqueue_element_rsdl(lvl.h, ns), "element_rsdl")
-        kev[k][1].record(stream)
-    torch.cuda.synchronize()
-    k_ms = sum(a.elapsed_time(b) for a, b in kev) / args.steps
-
-    # one multistage update (nstage x (rsdl + minvrt + ug update)), for context
-    uev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.zero_()
-        uev[k][0].record(stream)
-        hpb._lib.check(lib.hp_gpu_enqueue_update(lvl.h), "update")
-        uev[k][1].record(stream)
-    torch.cuda.synchronize()
-    u_ms = sum(a.elapsed_time(b) for a, b in uev) / args.steps
+    # the dominant kernel alone (k_rsdl_emat) for the roofline
+    k_ms = sum(timed(elem, args.steps)) / args.steps
+    # one multistage update (nstage x (rsdl + minvrt + ug update)), FP64 and FP32
+    u_ms = sum(timed(update, args.steps)) / args.steps
+    check(lib.hp_gpu_fp32_updates(lvl.h, 10), "fp32 updates")  # FP32 buffers and graph outside the timing
+    u32_ms = sum(timed(lambda: check(lib.hp_gpu_fp32_updates(lvl.h, 10), "fp32 updates"), 3)) / 30
     if clk:
         clk.terminate()
         clk.wait()
@@ -313,7 +364,6 @@ def main():
         os.remove(clk_file)
     except OSError:
         pass
-
     # e2e through the C-ABI with host buffers (pinned)
     hv = torch.empty(pr.ugv.shape, dtype=torch.float64, pin_memory=True).numpy()
     hs = torch.empty(pr.ugs.shape, dtype=torch.float64, pin_memory=True).numpy()
@@ -337,6 +387,7 @@ def main():
 
     ndof = pr.ndof
     m = pr.mesh
+    T = (P + 1) * (P + 2) // 2
     tol = time_to_tolerance(hpb, dev)
     if dist:
         t = torch.tensor([t_ms, e2e_s], device="cuda", dtype=torch.float64)
@@ -344,14 +395,27 @@ def main():
         t_ms, e2e_s = float(t[0]), float(t[1])
     value = world * ndof * args.steps / (t_ms * 1e-3) / 1e9
     e2e = world * ndof / e2e_s / 1e9
-    alg_bytes = 16 * ndof + 36 * m.ntri + 16 * m.npnt
+    # algorithmic bytes of one k_rsdl_emat launch at beta = 1: both element operators and
+    # b_re (ntri (2 T^2 + T) FP64), the state read once, res and res_r written once, and
+    # the element connectivity (tri_pnt, tri_seg, tri_sgn: 9 int32 per triangle)
+    op_bytes = m.ntri * (2 * T * T + T) * 8
+    alg_bytes = op_bytes + 3 * ndof * 8 + 36 * m.ntri
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
-    hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm = peaks.get("hbm_gbs")
+    peak_source = "MEASURED_PEAKS.json hbm_gbs (measured)"
+    if hbm is None:
+        hbm, peak_source = 6650.0, "fallback 6.65 TB/s (no measured peak file)"
     achieved = alg_bytes / (k_ms * 1e-3) / 1e9
+    traffic = None
+    try:  # DRAM bytes per triangle of k_rsdl_emat from an ncu capture, scaled to this launch
+        tr = json.load(open(os.path.join(ROOT, "profiles", "k_rsdl_emat_cd_p4_traffic.json")))
+        traffic = tr["dram_bytes_per_triangle"] * m.ntri
+    except Exception:
+        pass
     fl = flops_per_element(P) * m.ntri
     if rank != 0:
         if dist:
@@ -362,19 +426,27 @@ def main():
         cv, n = run_cpu(1, 10.0)
         cpu = {"value": cv, "unit": "GDoF/s", "cores": 1, "kind": "port",
                "sample": f"oracle rsdl(nstage) on a {n}x{n} split-square mesh, p={P}, 10 s, 1 core"}
-    launches_per_step = 3  # k_rsdl_pre, k_rsdl_elem, k_rsdl_fold (cd has no boundary-flux kernel)
+    launches_per_step = 3  # k_rsdl_pre, k_rsdl_emat, k_rsdl_fold (cd has no boundary-flux kernel)
+    cfg = workload_config()
+    cfg["element_operators"] = ("stored: built once by the element kernel on unit vectors "
+                                f"({build_ms:.1f} ms, {2 * op_bytes / 1e9:.2f} GB FP64 + FP32 copy), "
+                                "outside the timed steps")
     line = {
         "metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "kernel": "k_rsdl_elem", "kernel_ms": k_ms,
-                     "algorithmic_bytes": alg_bytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
-                     "fp64_tflops": fl / (k_ms * 1e-3) / 1e12, "flops_per_launch": fl},
+                     "traffic": traffic, "kernel": "k_rsdl_emat<double,4,beta>0>", "kernel_ms": k_ms,
+                     "algorithmic_bytes": alg_bytes, "peak_source": peak_source},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "GDoF/s", "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
         "gpu_launches": launches_per_step * args.steps,
+        "elem_operator_build_ms": build_ms,
         "update_ms": u_ms, "update_gdofs_per_stage": ndof * ns / (u_ms * 1e-3) / 1e9,
+        "fp32_update_ms": u32_ms,
+        "matrix_free": {"value": ndof / (mf_ms * 1e-3) / 1e9, "ms_per_step": mf_ms, "kernel": "k_rsdl_elem",
+                        "kernel_ms": mf_k, "fp64_tflops": fl / (mf_k * 1e-3) / 1e12, "flops_per_launch": fl,
+                        "update_ms": mf_u},
         "time_to_tol": tol,
         "ndof": ndof, "clocks": clocks,
     }

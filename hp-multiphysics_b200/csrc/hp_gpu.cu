@@ -8,6 +8,9 @@
 #include <vector>
 #include <string>
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <cstdint>
 
 #include "hp_gpu.h"
 #include "hp_mlp.h"
@@ -274,6 +277,7 @@ struct hp_gpu_ctx {
     double *d_part = nullptr;
     int npart = 0;
     std::vector<void *> allocs;
+    cudaMemPool_t pool = nullptr;
     cudaGraphExec_t g_update = nullptr;  // one update() incl. maxres -> hist slot advance
     bool prcn_ready = false;
     size_t lv = 0, ls = 0, li = 0;  // element counts of v/s/i arrays
@@ -281,6 +285,7 @@ struct hp_gpu_ctx {
     hp_gpu_ctx *fine = nullptr;
     int mg_kind = 0;  // 0 none, 1 p-level on the same mesh, 2 h-level (coarser mesh, p = 1)
     double fadd = 1.0;
+    bool fas_pending = false;  // restricted, driving term not formed yet (tri_hp::isfrst)
     double *res0v = nullptr, *res0s = nullptr, *res0i = nullptr;  // restricted fine residual
     double *uc0v = nullptr, *uc0s = nullptr, *uc0i = nullptr;     // state at restriction (vug_frst)
     double *fasv = nullptr, *fass = nullptr, *fasi = nullptr;     // FAS source dres
@@ -294,14 +299,43 @@ struct hp_gpu_ctx {
     float *r0v32 = nullptr, *r0s32 = nullptr, *r0i32 = nullptr, *c0v32 = nullptr, *c0s32 = nullptr, *c0i32 = nullptr;
 };
 
+// Device memory comes from one library-private stream-ordered pool per device: a
+// context's buffers return to the pool when it is destroyed and the next context
+// reuses them without a driver allocation (creating and destroying whole solver
+// hierarchies stays cheap). The pool keeps up to 16 GiB reserved between uses.
+static cudaMemPool_t pool_for(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = 16ull << 30;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[device] = pool;
+    return pool;
+}
+
 static int dalloc(hp_gpu_ctx *c, void **p, size_t bytes) {
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = c->pool ? cudaMallocFromPoolAsync(p, bytes, c->pool, c->stream) : cudaErrorInvalidValue;
     if (e != cudaSuccess) {
-        set_err("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        set_err("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
         return HP_ENOMEM;
     }
     c->allocs.push_back(*p);
+    // every buffer starts zeroed: nothing reads leftovers of an earlier allocation
+    e = cudaMemsetAsync(*p, 0, bytes, c->stream);
+    if (e != cudaSuccess) {
+        set_err("cudaMemsetAsync(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return HP_ECUDA;
+    }
     return HP_OK;
 }
 
@@ -354,6 +388,8 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
         }
         c->own_stream = true;
     }
+    c->pool = pool_for(c->device);
+    if (!c->pool) { set_err("cudaMemPoolCreate failed on device %d", c->device); return fail(HP_ECUDA); }
     const int physics = ph->physics;
     c->p = b->p; c->sm = b->sm; c->im = b->im;
     c->NV = physics == HP_PHYS_INS ? 3 : 1;
@@ -492,7 +528,8 @@ extern "C" int hp_gpu_destroy(hp_gpu_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->g_update) cudaGraphExecDestroy(c->g_update);
     if (c->g_update32) cudaGraphExecDestroy(c->g_update32);
-    for (void *p : c->allocs) cudaFree(p);
+    for (void *p : c->allocs) cudaFreeAsync(p, c->stream);
+    if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return HP_OK;
@@ -623,12 +660,26 @@ static int check_launch(hp_gpu_ctx *c) {
     return HP_OK;
 }
 
+static int mg_source_enqueue(hp_gpu_ctx *c);
+
+// A coarse level's first residual evaluation after mg_restrict forms its driving term.
+static int fas_first(hp_gpu_ctx *c) {
+    if (!c->fas_pending) return HP_OK;
+    if (!c->prcn_ready) {
+        set_err("coarse level: setup_preconditioner before its first residual after mg_restrict");
+        return HP_ESTATE;
+    }
+    return mg_source_enqueue(c);
+}
+
 extern "C" int hp_gpu_enqueue_rsdl(hp_gpu_ctx *c, int stage) {
     if (!c || stage < 0 || stage > c->ph.nstage) { set_err("bad stage"); return HP_EINVAL; }
     if (c->ph.physics == HP_PHYS_CD && c->ph.beta[stage] > 0.0 && !c->prcn_ready) {
         set_err("cd rsdl needs tau from setup_preconditioner");
         return HP_ESTATE;
     }
+    int r = fas_first(c);
+    if (r) return r;
     enqueue_rsdl(c, stage);
     // the reference's rsdl leaves res = res + res_r (nstage.cpp:76-82); the element kernel
     // already folded the interiors, fold vertices and sides here for the caller
@@ -661,7 +712,7 @@ static void drop_update_graphs(hp_gpu_ctx *c) {
 
 // The cd element operators depend on the geometry, the fixed physics parameters and
 // tau; cd tau is a function of the geometry and those parameters alone (steady
-// problems), so one build after the first preconditioner set-up stays valid.
+// problems), so one build stays valid for every later state.
 static int build_element_matrices(hp_gpu_ctx *c) {
     const size_t n = c->L.emat_len(c->ntri), nb = (size_t)c->ntri * ((c->p + 1) * (c->p + 2) / 2);
     int r;
@@ -695,7 +746,13 @@ extern "C" int hp_gpu_set_element_matrices(hp_gpu_ctx *c, int on) {
     if ((bool)on == c->emat_on) return HP_OK;
     c->emat_on = on != 0;
     drop_update_graphs(c);
-    if (c->emat_on && !c->emat_built && c->prcn_ready) return build_element_matrices(c);
+    if (c->emat_on && !c->emat_built) {
+        if (!c->prcn_ready) {  // tau
+            int r = hp_gpu_setup_preconditioner(c);
+            if (r) return r < 0 ? r : HP_ESTATE;
+        }
+        return build_element_matrices(c);
+    }
     return HP_OK;
 }
 
@@ -723,7 +780,6 @@ extern "C" int hp_gpu_setup_preconditioner(hp_gpu_ctx *c) {
     CK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->prcn_ready = true;
-    if (herr == 0 && c->emat_on && !c->emat_built && (r = build_element_matrices(c))) return r;
     return herr;
 }
 
@@ -752,8 +808,9 @@ static int ensure_update_graph(hp_gpu_ctx *c) {
 extern "C" int hp_gpu_enqueue_update(hp_gpu_ctx *c) {
     if (!c) return HP_EINVAL;
     if (!c->prcn_ready) { set_err("update before setup_preconditioner"); return HP_ESTATE; }
-    int r = ensure_update_graph(c);
+    int r = fas_first(c);
     if (r) return r;
+    if ((r = ensure_update_graph(c))) return r;
     CK(cudaGraphLaunch(c->g_update, c->stream));
     return HP_OK;
 }
@@ -776,6 +833,7 @@ extern "C" int hp_gpu_iterate(hp_gpu_ctx *c, int iters, int prcn_interval, doubl
             if (r) return r;
             if ((r = ensure_update_graph(c))) return r;  // a first set-up may switch the element path
         }
+        if ((r = fas_first(c))) return r;
         CK(cudaGraphLaunch(c->g_update, c->stream));
     }
     if (hist && iters) CK(cudaMemcpyAsync(hist, c->d_hist, (size_t)iters * 8, cudaMemcpyDeviceToHost, c->stream));
@@ -1150,7 +1208,17 @@ static int mg_restrict_enqueue(hp_gpu_ctx *c) {
                                                                           f->mesh.tri_pnt, f->st.ugv, c->st.ugv,
                                                                           c->uc0v);
     }
-    // res(first) of the coarse level without its source, then dres = fadd*res0 - res(first)
+    // the driving term is formed at the coarse level's first residual evaluation (isfrst)
+    c->fas_pending = true;
+    return check_launch(c);
+}
+
+// tri_hp::mg_source on first entry (nstage.cpp:113-129): res(first) of the coarse level
+// at the restricted state without its source, then dres = fadd*res0 - res(first). Runs
+// where the reference's first coarse rsdl runs: after that level's own preconditioner
+// set-up, so that res(first) uses its tau.
+static int mg_source_enqueue(hp_gpu_ctx *c) {
+    c->fas_pending = false;
     State<double> plain = c->st;
     plain.dresv = plain.dress = plain.dresi = nullptr;
     enqueue_rsdl_t<double>(c, c->L, c->d_tab, plain, c->ph, c->ph.nstage, 0);
@@ -1208,6 +1276,7 @@ static int cycle(hp_gpu_ctx **lv, int n, int lvl, int vw, int itercrsn, int iter
             r = hp_gpu_setup_preconditioner(c);
             if (r) return r < 0 ? r : HP_ESTATE;
         }
+        if ((r = fas_first(c))) return r;
         if ((r = ensure_update_graph(c))) return r;
         for (int it = 0; it < itercrsn; ++it) CK(cudaGraphLaunch(c->g_update, c->stream));
         if (lvl == n - 1) return HP_OK;
@@ -1238,12 +1307,14 @@ extern "C" int hp_gpu_solve_mg(hp_gpu_ctx **levels, int nlevels, double drop, in
                                double *seconds, int *cycles) {
     if (!levels || nlevels < 1 || drop <= 0.0 || max_cycles < 1) return HP_EINVAL;
     hp_gpu_ctx *f = levels[0];
+    int nh = 0, nc = 0, r;
+    for (int l = 0; l < nlevels; ++l)  // graph instantiation is set-up, outside the solve time
+        if ((r = ensure_update_graph(levels[l]))) return r;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     CK(cudaEventRecord(e0, f->stream));
     double r0 = 0.0, rn = 0.0;
-    int nh = 0, nc = 0, r;
     r = hp_gpu_setup_preconditioner(f);
     if (r) return r < 0 ? r : HP_ESTATE;
     if ((r = fp64_norm(f, &r0))) return r;
@@ -1282,6 +1353,7 @@ static int cycle_enqueue(hp_gpu_ctx **lv, int n, int lvl, int vw, int itercrsn, 
         if (lvl == n - 1) return HP_OK;
         if ((r = hp_gpu_enqueue_rsdl(c, c->ph.nstage))) return r;
         if ((r = mg_restrict_enqueue(lv[lvl + 1]))) return r;
+        if ((r = mg_source_enqueue(lv[lvl + 1]))) return r;  // preconditioners frozen in the graph
         if ((r = cycle_enqueue(lv, n, lvl + 1, vw, itercrsn, iterrfne))) return r;
         if ((r = mg_prolong_enqueue(lv[lvl + 1]))) return r;
         for (int it = 0; it < iterrfne; ++it) enqueue_update(c);
@@ -1339,6 +1411,10 @@ extern "C" int hp_gpu_solve_mg_graph(hp_gpu_ctx **levels, int nlevels, double dr
     if (!levels || nlevels < 1 || drop <= 0.0 || max_cycles < 1) return HP_EINVAL;
     if (check_every < 1) check_every = 1;
     hp_gpu_ctx *f = levels[0];
+    for (int l = 0; l < nlevels; ++l) {
+        int r0_ = ensure_update_graph(levels[l]);
+        if (r0_) return r0_;
+    }
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -1515,7 +1591,7 @@ extern "C" int hp_gpu_solve_mg_mixed(hp_gpu_ctx **levels, int nlevels, double dr
     hp_gpu_ctx *f = levels[0];
     int r;
     for (int l = 0; l < nlevels; ++l)
-        if ((r = alloc_mixed_mg(levels[l]))) return r;
+        if ((r = alloc_mixed_mg(levels[l])) || (r = ensure_update32_graph(levels[l]))) return r;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

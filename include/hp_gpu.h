@@ -192,11 +192,13 @@ int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *ctx, int stage);
  * (tri_hp/cd/rsdl.cpp:14-154) every call; for cd the element residual is affine
  * in the element's coefficients, lf_im = A_im u and lf_re = beta (A_re u + b_re),
  * so on = 1 builds A_im, A_re, b_re of every element once (FP64 by the element
- * kernel applied to unit vectors, plus an FP32 copy for the FP32 smoother) at the
- * first setup_preconditioner() (or at once if that has run), and every later
- * rsdl of either precision becomes a streamed batched mat-vec with the same
- * result up to rounding. on = 0 returns to the matrix-free kernel (the storage
- * is kept until hp_gpu_destroy). HP_ENOTSUP for ins. */
+ * kernel applied to unit vectors, plus an FP32 copy for the FP32 smoother), and
+ * every later rsdl of either precision becomes a streamed batched mat-vec with
+ * the same result up to rounding. The build needs tau: it runs
+ * setup_preconditioner() first when that has not run (cd tau depends on the
+ * geometry and the fixed parameters only, so the operators stay valid for every
+ * later state). on = 0 returns to the matrix-free kernel (the storage is kept
+ * until hp_gpu_destroy). HP_ENOTSUP for ins. */
 int hp_gpu_set_element_matrices(hp_gpu_ctx *ctx, int on);
 
 /* Convergence driver. Runs smoothing until the unpreconditioned FP64 residual
@@ -230,7 +232,10 @@ int hp_gpu_mg_attach_h(hp_gpu_ctx *coarse, hp_gpu_ctx *fine, const int *f2c_tri,
                        const int *c2f_tri, const double *c2f_wt, double fadd);
 /* tri_hp::mg_restrict (movco.cpp:4-106): needs the fine level's full residual
  * (hp_gpu_rsdl(fine, nstage)); sets the coarse state, its copy at entry
- * (vug_frst) and the FAS source. */
+ * (vug_frst) and the restricted residual res0. As the reference's isfrst, the
+ * FAS source is formed at the coarse level's first residual evaluation after
+ * this call (rsdl, update, iterate or a cycle), which therefore needs that
+ * level's setup_preconditioner() first (its tau enters res(first)). */
 int hp_gpu_mg_restrict(hp_gpu_ctx *coarse);
 /* tri_hp::mg_prolongate (movfin.cpp:7-82): fine state += coarse correction. */
 int hp_gpu_mg_prolongate(hp_gpu_ctx *coarse);

@@ -49,6 +49,27 @@ def test_p_restriction_and_fas_source():
     H.close()
 
 
+def test_coarse_driving_term_waits_for_coarse_preconditioner():
+    """As the reference's isfrst (nstage.cpp:113-129), the FAS source is formed at the
+    coarse level's first residual after restriction, with that level's own tau."""
+    H = MG.build(lambda n, p, **kw: hpb.cd_sinsin(n=n, p=p, kcond=1e-2, cfl=0.5, **kw), n=6, p=4)
+    f, c = H.levels[0], H.levels[1]
+    assert f.setup_preconditioner() == 0
+    f.rsdl(f.prob.phys.nstage)
+    L.check(H.lib.hp_gpu_mg_restrict(c.h), "restrict")
+    with pytest.raises(RuntimeError):
+        c.rsdl(c.prob.phys.nstage)
+    assert c.setup_preconditioner() == 0
+    c.rsdl(c.prob.phys.nstage)
+    rf = f.residual()
+    imap = interior_map(c.prob.sm, f.prob.sm)
+    want = (rf[0], rf[1][:, :c.prob.sm, :], rf[2][:, imap, :])
+    for a, b in zip(c.residual(), want):
+        if b.size:
+            assert np.max(np.abs(a - b)) <= 1e-12 * max(1.0, np.max(np.abs(b)))
+    H.close()
+
+
 def test_h_restriction_and_prolongation():
     H = MG.build(lambda n, p, **kw: hpb.kovasznay_ins(n=n, p=p, **kw), n=8, p=1, hlevels=1)
     f, c = H.levels[0], H.levels[1]
