@@ -124,6 +124,18 @@ def run_cpu(cores, secs, n=60):
     return dof / el / 1e9, n
 
 
+def replica_totals(dist, world, ndof, steps, t_ms, e2e_s, device):
+    """Whole-job figures of N independent replicas: each rank processed `ndof` per step,
+    and the slowest rank bounds the job (max over ranks of the timed region and of the
+    e2e step time). Returns (value GDoF/s, e2e GDoF/s, t_ms, e2e_s)."""
+    if dist is not None:
+        import torch
+        t = torch.tensor([t_ms, e2e_s], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms, e2e_s = float(t[0]), float(t[1])
+    return world * ndof * steps / (t_ms * 1e-3) / 1e9, world * ndof / e2e_s / 1e9, t_ms, e2e_s
+
+
 TOL_N = 64
 MG_N = 320
 
@@ -389,12 +401,7 @@ def main():
     m = pr.mesh
     T = (P + 1) * (P + 2) // 2
     tol = time_to_tolerance(hpb, dev)
-    if dist:
-        t = torch.tensor([t_ms, e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms, e2e_s = float(t[0]), float(t[1])
-    value = world * ndof * args.steps / (t_ms * 1e-3) / 1e9
-    e2e = world * ndof / e2e_s / 1e9
+    value, e2e, t_ms, e2e_s = replica_totals(dist, world, ndof, args.steps, t_ms, e2e_s, "cuda")
     # algorithmic bytes of one k_rsdl_emat launch at beta = 1: both element operators and
     # b_re (ntri (2 T^2 + T) FP64), the state read once, res and res_r written once, and
     # the element connectivity (tri_pnt, tri_seg, tri_sgn: 9 int32 per triangle)
