@@ -138,6 +138,99 @@ def replica_totals(dist, world, ndof, steps, t_ms, e2e_s, device):
 
 TOL_N = 64
 MG_N = 320
+CD_CFL = {8: 0.3, 6: 0.35, 4: 0.5, 3: 0.6, 2: 0.75, 1: 1.0}
+
+
+def timed_factory(torch, flush):
+    def timed(fn, n, stream):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            fn()
+            b.record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in evs]
+    return timed
+
+
+def c2_sweep(hpb, dev, n, ps, steps, timed):
+    """cd, velocity (1, 0.5), kcond 1e-3, Dirichlet sin(pi x) sin(pi y) (so the converged
+    state is 0; the initial state is that field projected plus 1e-3 noise) on the seeded
+    Delaunay mesh delaunay_square(n) (n = 317: ~200k triangles, min angle >= 20 deg).
+    Per p: FP64 rsdl GDoF/s matrix-free and from stored operators (with the operator
+    kernel's HBM fraction), then time to a 1e-10 drop of the FP64 residual norm by V-cycles
+    (p-levels p -> ... -> 1, then 4 Delaunay h-levels of n/2 .. n/16) for plain FP64
+    (matrix-free), FP64 with stored operators and FP32 defect correction with stored
+    operators, with the L2 difference of the converged states."""
+    import ctypes as C
+    import time as _t
+    import numpy as np
+    import torch
+    from hpb import multigrid as MG
+    from hpb._lib import check
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    meshes = {}
+
+    def mesh(m):
+        if m not in meshes:
+            meshes[m] = hpb.delaunay_square(m, seed=20261205 + m)
+        return meshes[m]
+
+    def mk(n, p, **kw):
+        return hpb.cd_sinsin(mesh=mesh(n), p=p, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205, **kw)
+
+    for p in ps:
+        T = (p + 1) * (p + 2) // 2
+        st = torch.cuda.Stream()
+        pr = mk(n, p, cfl=CD_CFL[p])
+        g = hpb.GPULevel(pr, device=dev, stream=C.c_void_p(st.cuda_stream))
+        g.setup_preconditioner()
+        ns = pr.phys.nstage
+        rs = lambda: check(g.lib.hp_gpu_enqueue_rsdl(g.h, ns), "rsdl")
+        el = lambda: check(g.lib.hp_gpu_enqueue_element_rsdl(g.h, ns), "element_rsdl")
+        for _ in range(3):
+            rs()
+        mf = sum(timed(rs, steps, st)) / steps
+        t0 = _t.perf_counter()
+        g.element_matrices(True)
+        build = _t.perf_counter() - t0
+        for _ in range(3):
+            rs()
+        em = sum(timed(rs, steps, st)) / steps
+        ek = sum(timed(el, steps, st)) / steps
+        alg = pr.mesh.ntri * (2 * T * T + T) * 8 + 3 * pr.ndof * 8 + 36 * pr.mesh.ntri
+        g.close()
+        line = {"sweep": "c2", "p": p, "mesh": f"seeded Delaunay, {pr.mesh.ntri} triangles, min angle "
+                                               f"{mesh(n).min_angle:.1f} deg", "ndof": pr.ndof,
+                "rsdl_gdofs_matrix_free": pr.ndof / (mf * 1e-3) / 1e9, "rsdl_ms_matrix_free": mf,
+                "rsdl_gdofs": pr.ndof / (em * 1e-3) / 1e9, "rsdl_ms": em, "operator_build_s": build,
+                "k_rsdl_emat_ms": ek, "k_rsdl_emat_gbs": alg / (ek * 1e-3) / 1e9,
+                "k_rsdl_emat_hbm_frac": alg / (ek * 1e-3) / 1e9 / hbm}
+        states = {}
+        for name, mixed, ops in (("fp64", False, False), ("fp64_elem_ops", False, True),
+                                 ("fp32_defect_correction", True, True)):
+            H = MG.build(mk, n=n, p=p, hlevels=4, cfl=CD_CFL)
+            tb = 0.0
+            if ops:
+                t0 = _t.perf_counter()
+                H.element_matrices(True)
+                tb = _t.perf_counter() - t0
+            hist, sec, cyc = H.solve(drop=1e-10, max_cycles=400, mixed=mixed)
+            states[name] = H.levels[0].state()
+            H.close()
+            d = float(np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(states["fp64"], states[name]))))
+            line[name] = {"seconds": sec + tb, "solve_seconds": sec, "operator_build_seconds": tb, "cycles": cyc,
+                          "final_drop": float(hist[-1]), "reached": bool(hist[-1] <= 1e-10),
+                          "l2_coeff_diff_vs_fp64": d}
+        line["state_l2_fp64"] = float(np.sqrt(sum(np.sum(a * a) for a in states["fp64"])))
+        line["speedup_fp32_vs_fp64"] = line["fp64"]["seconds"] / line["fp32_defect_correction"]["seconds"]
+        print(json.dumps(line), flush=True)
 
 
 def _rel(a, b):
@@ -249,6 +342,10 @@ def main():
                     help="with --quick / --profile: the matrix-free element kernel instead of stored operators")
     ap.add_argument("--profile", choices=["update64", "update32"], default=None,
                     help="run `steps` multistage updates of the workload in FP64 or FP32 (for profiler runs)")
+    ap.add_argument("--sweep", choices=["c2"], default=None,
+                    help="c2: cd on the seeded 200k-triangle Delaunay mesh, p = 2, 4, 6, 8: rsdl GDoF/s and time "
+                         "to a 1e-10 drop, plain FP64 vs FP32 defect correction (one JSON line per p)")
+    ap.add_argument("--p", type=int, nargs="*", default=None, help="with --sweep: the p values")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -285,6 +382,11 @@ def main():
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream()  # a non-default stream: the update graph is captured on it
     torch.cuda.set_stream(stream)
+
+    if args.sweep == "c2":
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        c2_sweep(hpb, dev, args.mesh, args.p or [2, 4, 6, 8], args.steps, timed_factory(torch, flush))
+        return
 
     pr = hpb.cd_sinsin(n=args.mesh, p=P, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205)
     lvl = hpb.GPULevel(pr, device=dev, stream=ctypes.c_void_p(stream.cuda_stream))

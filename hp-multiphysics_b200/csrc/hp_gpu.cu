@@ -107,19 +107,27 @@ inline int nblk(long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
+// Launch shapes chosen per context (per mesh level) and precision by hp_gpu_autotune.
+struct Tune {
+    int elem_cap = 16;       // matrix-free element kernel: CTAs per SM at most
+    int emat_tpp = 1;        // stored-operator kernel: tiles per pipeline phase (1 or 2)
+    int emat_ctas = 0;       // stored-operator kernel: CTAs per SM (0 = as many as fit)
+    int minv_threads = 128;  // minvrt kernels: threads per CTA
+};
+
 // Per-(precision, p, physics) launchers.
 template <typename R>
 struct Launchers {
     size_t tab_bytes;
     void (*fill)(const hp_basis_tables &, void *);
     void (*elem)(const void *tab, const Mesh &, const State<R> &, const Phys &, int stage, int zero_rr, int diff,
-                 int nsm, cudaStream_t);
+                 int nsm, const Tune &, cudaStream_t);
     void (*bflux)(const void *tab, const Mesh &, const State<R> &, const Phys &, int diff, cudaStream_t);
     void (*side)(const Mesh &, const State<R> &, const DevMinv<R> *, int im, int mode, double cfla, int upd, int fold,
-                 cudaStream_t);
-    void (*intr)(const Mesh &, const State<R> &, const DevMinv<R> *, double cfla, int upd, cudaStream_t);
+                 int threads, cudaStream_t);
+    void (*intr)(const Mesh &, const State<R> &, const DevMinv<R> *, double cfla, int upd, int threads, cudaStream_t);
     void (*vert)(const Mesh &, const State<R> &, const DevMinv<R> *, int sm, int im, double cfla, int upd, int fold,
-                 unsigned long long *slot, cudaStream_t);
+                 unsigned long long *slot, int threads, cudaStream_t);
     int elem_smem;
     cudaError_t (*set_smem)();
     // cd element operators: length of one operator array, build, apply
@@ -127,7 +135,7 @@ struct Launchers {
     void (*emat_build)(const void *tab, const Mesh &, const State<R> &, const Phys &, ElemMat<R>, int nsm,
                        cudaStream_t);
     void (*emat_apply)(ElemMat<R>, const Mesh &, const State<R> &, const Phys &, int stage, int zero_rr, int nsm,
-                       cudaStream_t);
+                       const Tune &, cudaStream_t);
 };
 
 template <typename R, int P, int PHYS>
@@ -139,9 +147,9 @@ struct LaunchImpl {
     }
     static void fill(const hp_basis_tables &b, void *out) { fill_tables<R, P>(b, *reinterpret_cast<DevTables<R, P> *>(out)); }
     static void elem(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int stage, int zero_rr, int diff,
-                     int nsm, cudaStream_t st) {
+                     int nsm, const Tune &tn, cudaStream_t st) {
         int blocks = nblk(m.ntri, C::WPC);
-        const int cap = nsm * 16;
+        const int cap = nsm * tn.elem_cap;
         if (blocks > cap) blocks = cap;
         k_rsdl_elem<R, P, PHYS><<<blocks, C::WPC * 32, smem(), st>>>(
             reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, stage, zero_rr, diff, ElemMat<R>{});
@@ -158,18 +166,29 @@ struct LaunchImpl {
                 reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, ph.nstage, 1, 0, em);
         }
     }
+    template <bool RE>
+    static void emat_launch(ElemMat<R> em, const Mesh &m, const State<R> &s, const Phys &ph, int stage, int zero_rr,
+                            int nsm, const Tune &tn, cudaStream_t st) {
+        using E = EmatCfg<P>;
+        constexpr int TH = RE ? E::THREADS_RE : E::THREADS_IM;
+        const long ntiles = ((long)m.ntri + E::EB - 1) / E::EB;
+        const int tpp = tn.emat_tpp == 2 ? 2 : 1;
+        const int maxc = std::max(1, 2048 / TH / tpp);
+        const int cps = (tn.emat_ctas > 0 && tn.emat_ctas < maxc) ? tn.emat_ctas : maxc;
+        const long groups = (ntiles + tpp - 1) / tpp;
+        const int blocks = (int)std::min(groups, (long)nsm * cps);
+        if (tpp == 2)
+            k_rsdl_emat<R, P, RE, 2><<<blocks, TH, 0, st>>>(em, m, s, ph, stage, zero_rr);
+        else
+            k_rsdl_emat<R, P, RE, 1><<<blocks, TH, 0, st>>>(em, m, s, ph, stage, zero_rr);
+    }
     static void emat_apply(ElemMat<R> em, const Mesh &m, const State<R> &s, const Phys &ph, int stage, int zero_rr,
-                           int nsm, cudaStream_t st) {
+                           int nsm, const Tune &tn, cudaStream_t st) {
         if constexpr (PHYS == 0) {
-            using E = EmatCfg<P>;
-            const long ntiles = ((long)m.ntri + E::EB - 1) / E::EB;
-            if (ph.beta[stage] > 0.0) {
-                const long blocks = std::min(ntiles, (long)nsm * (2048 / E::THREADS_RE));
-                k_rsdl_emat<R, P, true><<<(int)blocks, E::THREADS_RE, 0, st>>>(em, m, s, ph, stage, zero_rr);
-            } else {
-                const long blocks = std::min(ntiles, (long)nsm * (2048 / E::THREADS_IM));
-                k_rsdl_emat<R, P, false><<<(int)blocks, E::THREADS_IM, 0, st>>>(em, m, s, ph, stage, zero_rr);
-            }
+            if (ph.beta[stage] > 0.0)
+                emat_launch<true>(em, m, s, ph, stage, zero_rr, nsm, tn, st);
+            else
+                emat_launch<false>(em, m, s, ph, stage, zero_rr, nsm, tn, st);
         }
     }
     static void bflux(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int diff, cudaStream_t st) {
@@ -178,16 +197,17 @@ struct LaunchImpl {
                                                                        s, ph, diff);
     }
     static void side(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, int im, int mode, double cfla, int upd,
-                     int fold, cudaStream_t st) {
+                     int fold, int th, cudaStream_t st) {
         if constexpr (SM > 0)
-            k_minv_side<R, NV, SM><<<nblk(m.nseg, 128), 128, 0, st>>>(m, s, mt, im, mode, (R)cfla, upd, fold);
+            k_minv_side<R, NV, SM><<<nblk(m.nseg, th), th, 0, st>>>(m, s, mt, im, mode, (R)cfla, upd, fold);
     }
-    static void intr(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, double cfla, int upd, cudaStream_t st) {
-        if constexpr (IM > 0) k_minv_int<R, NV, SM, IM><<<nblk(m.ntri, 128), 128, 0, st>>>(m, s, mt, (R)cfla, upd);
+    static void intr(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, double cfla, int upd, int th,
+                     cudaStream_t st) {
+        if constexpr (IM > 0) k_minv_int<R, NV, SM, IM><<<nblk(m.ntri, th), th, 0, st>>>(m, s, mt, (R)cfla, upd);
     }
     static void vert(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, int sm, int im, double cfla, int upd,
-                     int fold, unsigned long long *slot, cudaStream_t st) {
-        k_minv_vert<R, NV><<<nblk(m.npnt, 128), 128, 0, st>>>(m, s, mt, sm, im, (R)cfla, upd, fold, slot);
+                     int fold, unsigned long long *slot, int th, cudaStream_t st) {
+        k_minv_vert<R, NV><<<nblk(m.npnt, th), th, 0, st>>>(m, s, mt, sm, im, (R)cfla, upd, fold, slot);
     }
     static cudaError_t set_smem_attr() {
         return cudaFuncSetAttribute(k_rsdl_elem<R, P, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem());
@@ -291,6 +311,8 @@ struct hp_gpu_ctx {
     double *fasv = nullptr, *fass = nullptr, *fasi = nullptr;     // FAS source dres
     int *f2c_tri = nullptr, *c2f_tri = nullptr;
     double *f2c_wt = nullptr, *c2f_wt = nullptr;
+    Tune tune[2];  // launch shapes for FP64 [0] and FP32 [1]
+    float tune_ms[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // tuned element-part and minvrt times
     // cd element operators (FP64 built by the element kernel, FP32 converted copy)
     bool emat_on = false, emat_built = false;
     ElemMat<double> em{};
@@ -592,6 +614,8 @@ extern "C" int hp_gpu_device_ptrs(hp_gpu_ctx *c, double **ugv, double **ugs, dou
 
 static ElemMat<double> emat_of(hp_gpu_ctx *c, double) { return c->em; }
 static ElemMat<float> emat_of(hp_gpu_ctx *c, float) { return c->em32; }
+static const Tune &tune_of(hp_gpu_ctx *c, double) { return c->tune[0]; }
+static const Tune &tune_of(hp_gpu_ctx *c, float) { return c->tune[1]; }
 
 // Element part of rsdl(stage): the stored cd element operators once built, else the
 // matrix-free element kernel.
@@ -599,9 +623,9 @@ template <typename R>
 static void launch_elem(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab, const State<R> &st, const Phys &ph,
                         int stage, int zero_rr, int diff) {
     if (c->emat_on && c->emat_built && ph.physics == HP_PHYS_CD && !diff)
-        L.emat_apply(emat_of(c, R()), c->mesh, st, ph, stage, zero_rr, c->nsm, c->stream);
+        L.emat_apply(emat_of(c, R()), c->mesh, st, ph, stage, zero_rr, c->nsm, tune_of(c, R()), c->stream);
     else
-        L.elem(tab, c->mesh, st, ph, stage, zero_rr, diff, c->nsm, c->stream);
+        L.elem(tab, c->mesh, st, ph, stage, zero_rr, diff, c->nsm, tune_of(c, R()), c->stream);
 }
 
 // Stream-ordered body of rsdl(stage) (no sync, capturable), either precision.
@@ -623,9 +647,10 @@ static void enqueue_rsdl(hp_gpu_ctx *c, int stage) { enqueue_rsdl_t<double>(c, c
 template <typename R>
 static void enqueue_minvrt_t(hp_gpu_ctx *c, const Launchers<R> &L, const State<R> &st, const DevMinv<R> *mt,
                              double cfla, int upd, int fold, unsigned long long *slot) {
-    L.vert(c->mesh, st, mt, c->sm, c->im, cfla, upd, fold, slot, c->stream);
-    for (int mode = 0; mode < c->sm; ++mode) L.side(c->mesh, st, mt, c->im, mode, cfla, upd, fold, c->stream);
-    if (c->im > 0) L.intr(c->mesh, st, mt, cfla, upd, c->stream);
+    const int th = tune_of(c, R()).minv_threads;
+    L.vert(c->mesh, st, mt, c->sm, c->im, cfla, upd, fold, slot, th, c->stream);
+    for (int mode = 0; mode < c->sm; ++mode) L.side(c->mesh, st, mt, c->im, mode, cfla, upd, fold, th, c->stream);
+    if (c->im > 0) L.intr(c->mesh, st, mt, cfla, upd, th, c->stream);
 }
 static void enqueue_minvrt(hp_gpu_ctx *c, double cfla, int upd, int fold, unsigned long long *slot) {
     enqueue_minvrt_t<double>(c, c->L, c->st, c->d_minv, cfla, upd, fold, slot);
@@ -723,9 +748,14 @@ static int build_element_matrices(hp_gpu_ctx *c) {
         if ((r = dalloc(c, (void **)&c->em32.aim, n * 4))) return r;
         if ((r = dalloc(c, (void **)&c->em32.are, n * 4))) return r;
         if ((r = dalloc(c, (void **)&c->em32.bre, nb * 4))) return r;
-        CK(cudaMemsetAsync(c->em.aim, 0, n * 8, c->stream));  // padding of the last tile
-        CK(cudaMemsetAsync(c->em.are, 0, n * 8, c->stream));
     }
+    // operator tiles start on 16-byte boundaries
+    for (const void *q : {(const void *)c->em.aim, (const void *)c->em.are, (const void *)c->em32.aim,
+                          (const void *)c->em32.are})
+        if ((uintptr_t)q % 16) {
+            set_err("element operator storage not 16-byte aligned");
+            return HP_ECUDA;
+        }
     c->L.emat_build(c->d_tab, c->mesh, c->st, c->ph, c->em, c->nsm, c->stream);
     conv(c, (long)n, c->em.aim, c->em32.aim);
     conv(c, (long)n, c->em.are, c->em32.are);
@@ -1625,4 +1655,96 @@ extern "C" int hp_gpu_solve_mg_mixed(hp_gpu_ctx **levels, int nlevels, double dr
     if (seconds) *seconds = ms * 1e-3;
     if (cycles) *cycles = nc;
     return hp_gpu_sync(f);
+}
+
+// ---------------------------------------------------------------------------
+// Launch-shape autotuner. Each context is one mesh level at one p, so the best
+// shapes differ between the levels of a hierarchy: the tuner times the candidate
+// shapes of this context's element part (matrix-free kernel: CTAs per SM; stored
+// operators: tiles per phase x CTAs per SM) and of its minvrt kernels (threads per
+// CTA) on its own mesh, in FP64 and FP32, and keeps the fastest of each.
+// ---------------------------------------------------------------------------
+template <typename R>
+static int tune_prec(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab, const State<R> &st, const Phys &ph,
+                     const DevMinv<R> *mt, int diff, Tune &tn, int reps, float *ms_out) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto time = [&](auto &&fn) -> float {
+        fn();  // warm
+        cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < reps; ++r) fn();
+        cudaEventRecord(e1, c->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms / reps;
+    };
+    const int ns = ph.nstage;
+    auto elem = [&]() { launch_elem<R>(c, L, tab, st, ph, ns, 1, diff); };
+    Tune keep = tn;
+    float best = 1e30f;
+    if (c->emat_on && c->emat_built && ph.physics == HP_PHYS_CD && !diff) {
+        const int tpps[2] = {1, 2}, ctas[3] = {0, 4, 2};
+        for (int a : tpps)
+            for (int b : ctas) {
+                tn.emat_tpp = a;
+                tn.emat_ctas = b;
+                const float t = time(elem);
+                if (t < best) { best = t; keep = tn; }
+            }
+    } else {
+        const int caps[3] = {4, 8, 16};
+        for (int a : caps) {
+            tn.elem_cap = a;
+            const float t = time(elem);
+            if (t < best) { best = t; keep = tn; }
+        }
+    }
+    tn = keep;
+    ms_out[0] = best;
+    best = 1e30f;
+    const int ths[3] = {64, 128, 256};
+    for (int a : ths) {
+        tn.minv_threads = a;
+        const float t = time([&]() { enqueue_minvrt_t<R>(c, L, st, mt, 0.0, 0, 0, nullptr); });
+        if (t < best) { best = t; keep = tn; }
+    }
+    tn = keep;
+    ms_out[1] = best;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return check_launch(c);
+}
+
+extern "C" int hp_gpu_autotune(hp_gpu_ctx *c, int reps) {
+    if (!c) return HP_EINVAL;
+    if (!c->prcn_ready) { set_err("autotune before setup_preconditioner"); return HP_ESTATE; }
+    if (reps < 1) reps = 5;
+    int r;
+    if ((r = tune_prec<double>(c, c->L, c->d_tab, c->st, c->ph, c->d_minv, 0, c->tune[0], reps, c->tune_ms[0])))
+        return r;
+    if ((r = alloc_mixed(c))) return r;
+    mixed_prcn(c);
+    const Phys p32 = phys32(c);
+    if ((r = tune_prec<float>(c, c->L32, c->d_tab32, c->s32, p32, c->d_minv32, c->ph.physics == HP_PHYS_INS ? 1 : 0,
+                              c->tune[1], reps, c->tune_ms[1])))
+        return r;
+    drop_update_graphs(c);  // captured graphs hold the old shapes
+    return hp_gpu_sync(c);
+}
+
+extern "C" int hp_gpu_get_tuning(const hp_gpu_ctx *c, int *shapes, float *ms) {
+    if (!c) return HP_EINVAL;
+    for (int k = 0; k < 2; ++k) {
+        const Tune &t = c->tune[k];
+        if (shapes) {
+            shapes[4 * k] = t.elem_cap;
+            shapes[4 * k + 1] = t.emat_tpp;
+            shapes[4 * k + 2] = t.emat_ctas;
+            shapes[4 * k + 3] = t.minv_threads;
+        }
+        if (ms) { ms[2 * k] = c->tune_ms[k][0]; ms[2 * k + 1] = c->tune_ms[k][1]; }
+    }
+    return HP_OK;
 }

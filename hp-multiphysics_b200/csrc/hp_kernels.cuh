@@ -109,9 +109,10 @@ struct ElemCfg {
 
 // Element operators of the linear cd residual. For uht = e_j, aim(t, j, m) = lf_im(m)
 // and are(t, j, m) = lf_re(m) at beta = 1; bre[t][m] = lf_re(m) of the source alone
-// (uht = 0). Storage is in tiles of EB elements, column-major inside a tile, so that
-// the EB*T entries of one column j that a CTA reads together are contiguous:
-//   index(t, j, m) = ((t / EB) * T + j) * (EB * T) + (t % EB) * T + m.
+// (uht = 0). Storage is in tiles of EB elements, column-major inside a tile (the EB*T
+// entries of one column that a CTA reads together are contiguous), each tile padded to
+// a 16-byte multiple:
+//   index(t, j, m) = (t / EB) * TS + j * (EB * T) + (t % EB) * T + m,  TS >= T * EB * T.
 template <typename R>
 struct ElemMat {
     R *aim, *are, *bre;
@@ -120,13 +121,14 @@ struct ElemMat {
 template <int P>
 struct EmatCfg {
     static constexpr int T = (P + 1) * (P + 2) / 2;
-    static constexpr int EB = (128 / T > 0 ? 128 / T : 1);                  // elements per tile
-    static constexpr int THREADS_RE = ((2 * EB * T + 31) / 32) * 32;       // beta > 0: A_im and A_re rows
-    static constexpr int THREADS_IM = ((EB * T + 31) / 32) * 32;           // beta = 0: A_im rows only
+    static constexpr int EB = (128 / T > 0 ? 128 / T : 1);            // elements per tile
+    static constexpr int TS = ((T * EB * T + 3) / 4) * 4;             // tile stride (entries)
+    static constexpr int THREADS_RE = ((2 * EB * T + 31) / 32) * 32;  // beta > 0: A_im and A_re rows
+    static constexpr int THREADS_IM = ((EB * T + 31) / 32) * 32;      // beta = 0: A_im rows only
     __host__ __device__ static size_t idx(long t, int j, int m) {
-        return ((size_t)(t / EB) * T + j) * (size_t)(EB * T) + (size_t)(t % EB) * T + m;
+        return (size_t)(t / EB) * TS + (size_t)j * (EB * T) + (size_t)(t % EB) * T + m;
     }
-    static size_t len(long ntri) { return (size_t)((ntri + EB - 1) / EB) * T * (size_t)(EB * T); }
+    static size_t len(long ntri) { return (size_t)((ntri + EB - 1) / EB) * TS; }
 };
 
 template <typename R, int P, int PHYS>
@@ -487,89 +489,122 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
 
 // Linear cd residual from the stored element operators: lf_im = A_im uht and
 // lf_re = beta (A_re uht + b_re), with the gather, scatter, res_r mixing and dres of
-// k_rsdl_elem (tri_hp/cd/rsdl.cpp:14-154 through tri_hp/nstage.cpp:21-82). One CTA
-// per tile of EB elements: gather the tile's coefficients to shared memory, one
-// thread per operator row (RE: A_im and A_re rows; otherwise A_im only) streams its
-// T contiguous-by-tile column entries, then one thread per (element, mode) scatters.
-template <typename R, int P, bool RE>
-__global__ void __launch_bounds__(RE ? EmatCfg<P>::THREADS_RE : EmatCfg<P>::THREADS_IM)
+// k_rsdl_elem (tri_hp/cd/rsdl.cpp:14-154 through tri_hp/nstage.cpp:21-82). Persistent
+// CTAs walk tiles of EB elements. Each thread owns one operator row (A_im rows, plus the
+// A_re rows when beta > 0) and at most one (element, mode) slot. The work of three tiles
+// is software-pipelined across one barrier per tile: in the phase of tile k a thread
+// scatters its slot of tile k-1, forms its row's dot product for tile k (the operator
+// entries stream from HBM, coalesced across the CTA) and gathers its slot of tile k+1,
+// so the dependent index -> value gather loads and the scatter atomics overlap the
+// operator stream instead of separating it. TPP tiles (consecutive, one contiguous
+// operator run) go through each phase together: TPP rows and slots per thread, more
+// loads in flight per barrier, at more registers per thread (a per-level tuning choice).
+template <typename R, int P, bool RE, int TPP>
+__global__ void __launch_bounds__(RE ? EmatCfg<P>::THREADS_RE : EmatCfg<P>::THREADS_IM,
+                                  2048 / (RE ? EmatCfg<P>::THREADS_RE : EmatCfg<P>::THREADS_IM) / TPP)
     k_rsdl_emat(ElemMat<R> em, Mesh mesh, State<R> st, Phys ph, int stage, int zero_rr) {
     using E = EmatCfg<P>;
-    constexpr int T = E::T, EB = E::EB, BM = 3 * P, IM = (P - 1) * (P - 2) / 2;
+    constexpr int T = E::T, EB = E::EB, TS = E::TS, BM = 3 * P, IM = (P - 1) * (P - 2) / 2;
     constexpr int SM = (P > 1 ? P - 1 : 1);  // side-mode stride (unused when p = 1)
     constexpr int NH = RE ? 2 : 1;
-    __shared__ R su[EB * T];
-    __shared__ R sr[NH * EB * T];
+    constexpr int ROWS = NH * EB * T, SLOTS = EB * T;
+    __shared__ R su[2][TPP * SLOTS];
+    __shared__ R sr[2][TPP * ROWS];
     const R beta = (R)ph.beta[stage];
     const R omb = zero_rr ? (R)0 : (R)1 - beta;
     const bool src = RE && ph.src != 0.0;
     const long ntiles = ((long)mesh.ntri + EB - 1) / EB;
-    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long t0 = tile * EB;
-        for (int w = threadIdx.x; w < EB * T; w += blockDim.x) {
-            const int e = w / T, m = w - e * T;
-            const long t = t0 + e;
-            R val = (R)0;
-            if (t < mesh.ntri) {
-                if (m < 3) {
-                    val = st.ugv[mesh.tri_pnt[3 * t + m]];
-                } else if (m < BM) {
-                    const int i = (m - 3) / SM, k = (m - 3) - i * SM;
-                    val = st.ugs[mesh.tri_seg[3 * t + i] * SM + k];
-                    if ((k & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
-                } else {
-                    val = st.ugi[t * IM + (m - BM)];
-                }
-            }
-            su[w] = val;
-        }
-        __syncthreads();
-        for (int w = threadIdx.x; w < NH * EB * T; w += blockDim.x) {
-            const int h = w / (EB * T), q = w - h * (EB * T), e = q / T;
-            if (t0 + e < mesh.ntri) {
-                const R *a = (h ? em.are : em.aim) + (size_t)tile * T * (EB * T) + q;
-                const R *u = su + e * T;
-                R acc = (R)0;
-#pragma unroll
-                for (int j = 0; j < T; ++j) acc = fma(__ldg(a + (size_t)j * (EB * T)), u[j], acc);
-                if (h) {
-                    if (src) acc += __ldg(em.bre + (size_t)t0 * T + q);
-                    acc *= beta;
-                }
-                sr[w] = acc;
-            }
-        }
-        __syncthreads();
-        for (int w = threadIdx.x; w < EB * T; w += blockDim.x) {
-            const int e = w / T, m = w - e * T;
-            const long t = t0 + e;
-            if (t >= mesh.ntri) continue;
-            const R vim = sr[w];
-            const R vre = RE ? sr[EB * T + w] : (R)0;
-            if (m < 3) {
-                const int v = mesh.tri_pnt[3 * t + m];
-                atomic_add(&st.resv[v], vim);
-                if (RE) atomic_add(&st.rrv[v], vre);
-            } else if (m < BM) {
-                const int i = (m - 3) / SM, k = (m - 3) - i * SM;
-                const int g = mesh.tri_seg[3 * t + i] * SM + k;
-                const bool flip = (k & 1) && mesh.tri_sgn[3 * t + i] < 0;
-                atomic_add(&st.ress[g], flip ? -vim : vim);
-                if (RE) atomic_add(&st.rrs[g], flip ? -vre : vre);
+    const long step = gridDim.x;
+    const int w = threadIdx.x;
+    const int hr = w / SLOTS, qr = w - hr * SLOTS, er = qr / T;  // operator row (w < ROWS)
+    const int es = w / T, ms = w - es * T;                       // gather / scatter slot (w < SLOTS)
+    auto gather = [&](long tile) -> R {
+        const long t = tile * EB + es;
+        R val = (R)0;
+        if (w < SLOTS && t < mesh.ntri) {
+            if (ms < 3) {
+                val = st.ugv[mesh.tri_pnt[3 * t + ms]];
+            } else if (ms < BM) {
+                const int i = (ms - 3) / SM, kk = (ms - 3) - i * SM;
+                val = st.ugs[mesh.tri_seg[3 * t + i] * SM + kk];
+                if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
             } else {
-                const size_t gi = (size_t)t * IM + (m - BM);
-                const R d = st.dresi ? st.dresi[gi] : (R)0;
-                if (RE) {
-                    const R rr = st.rri[gi] * omb + vre;
-                    st.rri[gi] = rr;
-                    st.resi[gi] = vim + d + rr;
-                } else {
-                    st.resi[gi] = vim + st.rri[gi] * omb + d;  // res_r unchanged when beta = 0
-                }
+                val = st.ugi[t * IM + (ms - BM)];
             }
+        }
+        return val;
+    };
+    auto matvec = [&](long tile, const R *u_s, R *r_s) {
+        if (w >= ROWS || tile * EB + er >= mesh.ntri) return;
+        const R *a = (hr ? em.are : em.aim) + (size_t)tile * TS + qr;
+        const R *u = u_s + er * T;
+        R acc = (R)0;
+#pragma unroll
+        for (int j = 0; j < T; ++j) acc = fma(__ldg(a + (size_t)j * SLOTS), u[j], acc);
+        if (hr) {
+            if (src) acc += __ldg(em.bre + (size_t)tile * EB * T + qr);
+            acc *= beta;
+        }
+        r_s[w] = acc;
+    };
+    auto scatter = [&](long tile, const R *r_s) {
+        if (w >= SLOTS) return;
+        const long t = tile * EB + es;
+        if (t >= mesh.ntri) return;
+        const R vim = r_s[w];
+        const R vre = RE ? r_s[SLOTS + w] : (R)0;
+        if (ms < 3) {
+            const int v = mesh.tri_pnt[3 * t + ms];
+            atomic_add(&st.resv[v], vim);
+            if (RE) atomic_add(&st.rrv[v], vre);
+        } else if (ms < BM) {
+            const int i = (ms - 3) / SM, kk = (ms - 3) - i * SM;
+            const int g = mesh.tri_seg[3 * t + i] * SM + kk;
+            const bool flip = (kk & 1) && mesh.tri_sgn[3 * t + i] < 0;
+            atomic_add(&st.ress[g], flip ? -vim : vim);
+            if (RE) atomic_add(&st.rrs[g], flip ? -vre : vre);
+        } else {
+            const size_t gi = (size_t)t * IM + (ms - BM);
+            const R d = st.dresi ? st.dresi[gi] : (R)0;
+            if (RE) {
+                const R rr = st.rri[gi] * omb + vre;
+                st.rri[gi] = rr;
+                st.resi[gi] = vim + d + rr;
+            } else {
+                st.resi[gi] = vim + st.rri[gi] * omb + d;  // res_r unchanged when beta = 0
+            }
+        }
+    };
+    const long ngroups = (ntiles + TPP - 1) / TPP;
+    long grp = blockIdx.x;
+    if (grp >= ngroups) return;
+#pragma unroll
+    for (int i = 0; i < TPP; ++i)
+        if (w < SLOTS) su[0][i * SLOTS + w] = gather(grp * TPP + i);
+    __syncthreads();
+    int k = 0;
+    for (; grp < ngroups; grp += step, ++k) {
+        const int b = k & 1;
+        // the next group's gather loads are issued first and stored last, so their
+        // index -> value latency runs under the scatter and the operator stream
+        R g[TPP];
+        const bool more = grp + step < ngroups;
+#pragma unroll
+        for (int i = 0; i < TPP; ++i) g[i] = more ? gather((grp + step) * TPP + i) : (R)0;
+        if (k > 0) {
+#pragma unroll
+            for (int i = 0; i < TPP; ++i) scatter((grp - step) * TPP + i, sr[b ^ 1] + i * ROWS);
+        }
+#pragma unroll
+        for (int i = 0; i < TPP; ++i) matvec(grp * TPP + i, su[b] + i * SLOTS, sr[b] + i * ROWS);
+        if (w < SLOTS) {
+#pragma unroll
+            for (int i = 0; i < TPP; ++i) su[b ^ 1][i * SLOTS + w] = g[i];
         }
         __syncthreads();
     }
+#pragma unroll
+    for (int i = 0; i < TPP; ++i) scatter((grp - step) * TPP + i, sr[(k - 1) & 1] + i * ROWS);
 }
 
 // res.v = res.s = 0 ; res_r.{v,s} *= (1-beta) (or = 0) : nstage.cpp:21-49

@@ -104,6 +104,8 @@ def lib():
         L.hp_gpu_enqueue_update.argtypes = [P]
         L.hp_gpu_enqueue_element_rsdl.argtypes = [P, _I]
         L.hp_gpu_set_element_matrices.argtypes = [P, _I]
+        L.hp_gpu_autotune.argtypes = [P, _I]
+        L.hp_gpu_get_tuning.argtypes = [P, P, P]
         L.hp_gpu_sizes.argtypes = [P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]
         for name in ("hp_gpu_upload_state",):
             getattr(L, name).argtypes = [P, P, P, P]

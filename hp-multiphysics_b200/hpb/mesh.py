@@ -5,6 +5,8 @@
   upper-left to its lower-right corner -- the triangulation of the reference's
   Testing/tri_hp/ins/Spatial Accuracy/Inputs/square<k>.grd meshes
   (square7.grd = 64 x 64 squares = 8,192 triangles).
+* ``delaunay_square(n, seed)``: a seeded Delaunay triangulation of the unit
+  square with about 2 n^2 triangles and a checked minimum angle.
 * ``read_grd(path)``: the reference's .grd text format (tri_mesh/input.cpp:504-600).
 * ``createsegtri``: segment/triangle connectivity with the reference's
   conventions (tri_mesh/setup.cpp:76-145): tri.seg(j) is the side opposite
@@ -87,6 +89,79 @@ def createsegtri(m, seg_pnt=None):
     if np.any(bnd):
         raise ValueError("boundary segment oriented clockwise for its triangle")
     return m
+
+
+def splitmix64_uniform(seed, n):
+    """n doubles in [-1, 1) from the splitmix64 sequence started at `seed`."""
+    mask = np.uint64(0xFFFFFFFFFFFFFFFF)
+    with np.errstate(over="ignore"):
+        k = np.arange(1, n + 1, dtype=np.uint64)
+        z = (np.uint64(seed) + k * np.uint64(0x9E3779B97F4A7C15)) & mask
+        z = ((z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & mask
+        z = ((z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & mask
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    return 2.0 * u - 1.0
+
+
+def delaunay_square(n, seed=20261205, jitter=0.12, margin=0.7, min_angle=20.0):
+    """Seeded Delaunay triangulation of the unit square with about 2 n^2 triangles
+    (the split-square mesh's count) and uniform vertex density: a hexagonal lattice of
+    spacing h = sqrt(2/sqrt(3))/n whose points are jittered by splitmix64 uniforms of
+    +-jitter*h, interior points kept at least margin*h from the boundary, boundary
+    points evenly spaced at about h, triangulated by scipy's Delaunay (Qhull) and
+    oriented counter-clockwise; vertices and triangles are numbered along a Z-curve, as a
+    mesh generator's renumbering pass would. Raises if the smallest angle is below
+    min_angle degrees."""
+    from scipy.spatial import Delaunay
+    h = np.sqrt(2.0 / np.sqrt(3.0)) / n
+    m = int(np.ceil(1.0 / h))
+    s = np.linspace(0.0, 1.0, m + 1)[:-1]
+    z, o = np.zeros(m), np.ones(m)
+    bnd = np.concatenate([np.stack([s, z], 1), np.stack([o, s], 1), np.stack([1 - s, o], 1), np.stack([z, 1 - s], 1)])
+    dy = h * np.sqrt(3.0) / 2.0
+    rows = []
+    for j in range(int(np.ceil(1.0 / dy)) + 2):
+        xs = np.arange(-1, int(1.0 / h) + 2) * h + (0.5 * h if j % 2 else 0.0)
+        rows.append(np.stack([xs, np.full_like(xs, j * dy)], 1))
+    pts = np.concatenate(rows)
+    pts = pts + jitter * h * splitmix64_uniform(seed, pts.size).reshape(pts.shape)
+    keep = np.all((pts > margin * h) & (pts < 1.0 - margin * h), axis=1)
+    pts = np.concatenate([bnd, pts[keep]])
+    pts = pts[np.argsort(morton_key(pts), kind="stable")]  # vertices numbered along a Z-curve
+    tri = Delaunay(pts).simplices.astype(np.int64)
+    tri = tri[np.argsort(morton_key(pts[tri].mean(axis=1)), kind="stable")]  # triangles too
+    a = pts[tri]
+    ar = (a[:, 1, 0] - a[:, 0, 0]) * (a[:, 2, 1] - a[:, 0, 1]) - (a[:, 1, 1] - a[:, 0, 1]) * (a[:, 2, 0] - a[:, 0, 0])
+    tri[ar < 0] = tri[ar < 0][:, [0, 2, 1]]
+    mesh = Mesh(pts, tri)
+    mesh.min_angle = float(min_angles(mesh).min())
+    if mesh.min_angle < min_angle:
+        raise ValueError(f"Delaunay mesh min angle {mesh.min_angle:.2f} < {min_angle}")
+    return mesh
+
+
+def morton_key(xy, bits=16):
+    """Z-order (Morton) key of points in the unit square: neighbouring keys are nearby
+    points, so arrays numbered by it keep an element's gathers close in memory."""
+    q = np.clip((np.asarray(xy) * (1 << bits)).astype(np.int64), 0, (1 << bits) - 1)
+    key = np.zeros(len(q), dtype=np.int64)
+    for b in range(bits):
+        key |= ((q[:, 0] >> b) & 1) << (2 * b)
+        key |= ((q[:, 1] >> b) & 1) << (2 * b + 1)
+    return key
+
+
+def min_angles(mesh):
+    """Smallest interior angle (degrees) of every triangle."""
+    a = mesh.pnts[mesh.tri_pnt]
+    out = np.full(mesh.ntri, 180.0)
+    for k in range(3):
+        u = a[:, (k + 1) % 3] - a[:, k]
+        v = a[:, (k + 2) % 3] - a[:, k]
+        c = np.sum(u * v, axis=1) / (np.linalg.norm(u, axis=1) * np.linalg.norm(v, axis=1))
+        out = np.minimum(out, np.degrees(np.arccos(np.clip(c, -1.0, 1.0))))
+    return out
 
 
 def square_mesh(n, x0=0.0, x1=1.0, y0=0.0, y1=1.0):

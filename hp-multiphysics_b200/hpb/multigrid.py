@@ -137,6 +137,14 @@ class Hierarchy:
         for lv in self.levels:
             lv.element_matrices(on)
 
+    def autotune(self, reps=5):
+        """Per-level launch shapes (hp_gpu_autotune on every level); returns them per level."""
+        out = []
+        for lv in self.levels:
+            lv.setup_preconditioner()
+            out.append(lv.autotune(reps))
+        return out
+
     def handles(self):
         arr = (P * len(self.levels))(*[lv.h for lv in self.levels])
         return arr

@@ -10,7 +10,7 @@ import ctypes
 import numpy as np
 
 from . import _lib as L
-from .mesh import square_mesh
+from .mesh import square_mesh, splitmix64_uniform
 
 # Multistage defaults (tri_mesh/blocks.cpp:1124-1148) and CFL per log2p (tri_hp/allocate.cpp:275)
 ALPHA_DFLT = (0.25, 1.0 / 6.0, 0.375, 0.5, 1.0)
@@ -38,17 +38,6 @@ def basis_tables(p):
     return _TABLE_CACHE[p]
 
 
-def splitmix64_uniform(seed, n):
-    """n doubles in [-1, 1) from the splitmix64 sequence started at `seed`."""
-    mask = np.uint64(0xFFFFFFFFFFFFFFFF)
-    with np.errstate(over="ignore"):
-        k = np.arange(1, n + 1, dtype=np.uint64)
-        z = (np.uint64(seed) + k * np.uint64(0x9E3779B97F4A7C15)) & mask
-        z = ((z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & mask
-        z = ((z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & mask
-        z = z ^ (z >> np.uint64(31))
-    u = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
-    return 2.0 * u - 1.0
 
 
 class Problem:
@@ -218,6 +207,20 @@ class GPULevel:
 
     def rsdl(self, stage):
         L.check(self.lib.hp_gpu_rsdl(self.h, stage), "rsdl")
+
+    def autotune(self, reps=5):
+        """hp_gpu_autotune; returns the chosen shapes and tuned times of FP64 and FP32."""
+        L.check(self.lib.hp_gpu_autotune(self.h, reps), "autotune")
+        return self.tuning()
+
+    def tuning(self):
+        sh = np.zeros(8, dtype=np.int32)
+        ms = np.zeros(4, dtype=np.float32)
+        L.check(self.lib.hp_gpu_get_tuning(self.h, L.ptr(sh), L.ptr(ms)), "get_tuning")
+        keys = ("elem_cap", "emat_tpp", "emat_ctas", "minv_threads")
+        return {prec: dict({k: int(sh[4 * i + j]) for j, k in enumerate(keys)},
+                           elem_ms=float(ms[2 * i]), minv_ms=float(ms[2 * i + 1]))
+                for i, prec in enumerate(("fp64", "fp32"))}
 
     def element_matrices(self, on=True):
         """cd only: rsdl from stored element operators (hp_gpu_set_element_matrices)."""

@@ -281,6 +281,23 @@ int hp_gpu_solve_mg_mixed(hp_gpu_ctx **levels, int nlevels, double drop, int max
  * FP64 ones update by update). Needs setup_preconditioner() first. */
 int hp_gpu_fp32_updates(hp_gpu_ctx *ctx, int n);
 
+/* Launch-shape autotuner (no counterpart in the reference; the north star's
+ * per-level tile-shape choice). Each context is one mesh level at one p, so the
+ * fastest launch shapes differ between the levels of a hierarchy. Times, on this
+ * context's own mesh, `reps` launches of each candidate shape of
+ *   the element part: matrix-free kernel CTAs per SM in {4, 8, 16}, or with stored
+ *     cd operators tiles per pipeline phase {1, 2} x CTAs per SM {all that fit, 4, 2};
+ *   the minvrt kernels: threads per CTA {64, 128, 256};
+ * in FP64 and in FP32 (allocating the FP32 smoother state), and keeps the fastest
+ * for every later launch of that precision. Results do not depend on the shapes
+ * beyond rounding of the atomic scatter. Needs setup_preconditioner(); leaves the
+ * state unchanged and the residual arrays unspecified. */
+int hp_gpu_autotune(hp_gpu_ctx *ctx, int reps);
+/* The shapes in use: shapes[8] = {elem_cap, emat_tpp, emat_ctas, minv_threads} for
+ * FP64 then FP32 (emat_ctas 0 = all that fit); ms[4] = the tuned element-part and
+ * minvrt times (ms) for FP64 then FP32 (0 before hp_gpu_autotune). Either may be NULL. */
+int hp_gpu_get_tuning(const hp_gpu_ctx *ctx, int *shapes, float *ms);
+
 /* Synchronises the context's stream and returns the first sticky error. */
 int hp_gpu_sync(hp_gpu_ctx *ctx);
 

@@ -165,3 +165,13 @@ def test_vcycle_graph_matches_level_by_level():
     num = np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u1, u2)))
     den = np.sqrt(sum(np.sum(a * a) for a in u1))
     assert num / den < 1e-8
+
+
+def test_vcycle_on_delaunay_meshes():
+    """Non-nested h-levels: each level is its own seeded Delaunay mesh; the transfers
+    locate every point in the other mesh (mgconnect semantics)."""
+    mk = lambda n, p, **kw: hpb.cd_sinsin(mesh=hpb.delaunay_square(n, seed=n), p=p, kcond=1e-2, field=quad(), **kw)
+    H = MG.build(mk, n=24, p=4, hlevels=2, cfl={4: 0.5, 2: 0.75, 1: 1.0})
+    hist, sec, cycles = H.solve(drop=1e-10, max_cycles=300)
+    assert hist[-1] <= 1e-10
+    H.close()

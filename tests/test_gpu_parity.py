@@ -90,3 +90,28 @@ def test_gpu_cd_quadratic_exactness_kat():
     l2, linf = pr.l2error(*g.state())
     assert l2[0] < 1e-12 and linf[0] < 1e-11
     assert hist[-1] < 1e-13
+
+
+@pytest.mark.parametrize("p", [2, 4, 6])
+@pytest.mark.parametrize("ops", [False, True])
+def test_unstructured_delaunay_cd(p, ops):
+    """Seeded Delaunay mesh (irregular valences and side orientations): rsdl, minvrt and
+    four updates against the oracle, matrix-free and with stored element operators."""
+    pr = hpb.cd_sinsin(mesh=hpb.delaunay_square(10, seed=3), p=p, kcond=1e-2, cfl=0.5, src=0.4)
+    g = pr.gpu()
+    o = Oracle(pr)
+    if ops:
+        g.element_matrices(True)
+    assert g.setup_preconditioner() == 0
+    assert o.setup_preconditioner() == 0
+    for stage in (pr.phys.nstage, 0, 1):
+        g.rsdl(stage)
+        o.rsdl(stage)
+        assert relerr(g.residual(), o.residual()) < TOL1, f"rsdl stage {stage}"
+    g.minvrt()
+    o.minvrt()
+    assert relerr(g.residual(), o.residual()) < tol1(p)
+    g.iterate(4)
+    for _ in range(4):
+        o.update()
+    assert relerr(g.state(), o.state()) < TOLN
