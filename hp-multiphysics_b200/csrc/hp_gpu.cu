@@ -786,11 +786,11 @@ extern "C" int hp_gpu_set_element_matrices(hp_gpu_ctx *c, int on) {
     return HP_OK;
 }
 
-extern "C" int hp_gpu_setup_preconditioner(hp_gpu_ctx *c) {
-    if (!c) return HP_EINVAL;
+// Stream-ordered body of setup_preconditioner (capturable: no host synchronisation).
+// Bad elements are counted into d_err, which the caller zeroes and reads.
+static int enqueue_prcn(hp_gpu_ctx *c) {
     CK(cudaMemsetAsync(c->st.vprcn, 0, (size_t)c->npnt * c->NV * 8, c->stream));
     CK(cudaMemsetAsync(c->st.sprcn, 0, (size_t)c->nseg * c->NV * 8, c->stream));
-    CK(cudaMemsetAsync(c->d_err, 0, 4, c->stream));
     if (c->net) {
         int r0 = hp_gpu_elem_features(c, c->d_feat);
         if (r0) return r0;
@@ -804,7 +804,13 @@ extern "C" int hp_gpu_setup_preconditioner(hp_gpu_ctx *c) {
                 c->stream);
     const int nv = c->npnt * c->NV, ns = (c->p > 1 ? c->nseg * c->NV : 0);
     k_prcn_invert<double><<<nblk(nv + ns, 256), 256, 0, c->stream>>>(nv, ns, c->st.vprcn, c->st.sprcn, c->vdiag);
-    int r = check_launch(c);
+    return check_launch(c);
+}
+
+extern "C" int hp_gpu_setup_preconditioner(hp_gpu_ctx *c) {
+    if (!c) return HP_EINVAL;
+    CK(cudaMemsetAsync(c->d_err, 0, 4, c->stream));
+    int r = enqueue_prcn(c);
     if (r) return r;
     int herr = 0;
     CK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1375,17 +1381,22 @@ extern "C" int hp_gpu_solve_mg(hp_gpu_ctx **levels, int nlevels, double drop, in
 // One V/W-cycle captured as a single CUDA graph (all levels must share one
 // stream). The preconditioners are evaluated before capture and frozen inside it;
 // the level updates are enqueued as plain kernels so the whole cycle is one graph.
-static int cycle_enqueue(hp_gpu_ctx **lv, int n, int lvl, int vw, int itercrsn, int iterrfne) {
+// block::cycle as stream operations only (for capture). With eval_prcn the
+// preconditioners are set up at the same points as in cycle(); bad elements then
+// accumulate in each level's d_err, which the driver checks between replays.
+static int cycle_enqueue(hp_gpu_ctx **lv, int n, int lvl, int vw, int itercrsn, int iterrfne, int eval_prcn) {
     hp_gpu_ctx *c = lv[lvl];
     int r;
     for (int vc = 0; vc < vw; ++vc) {
+        if (eval_prcn && (r = enqueue_prcn(c))) return r;
+        if (c->fas_pending && (r = mg_source_enqueue(c))) return r;
         for (int it = 0; it < itercrsn; ++it) enqueue_update(c);
         if (lvl == n - 1) return HP_OK;
         if ((r = hp_gpu_enqueue_rsdl(c, c->ph.nstage))) return r;
         if ((r = mg_restrict_enqueue(lv[lvl + 1]))) return r;
-        if ((r = mg_source_enqueue(lv[lvl + 1]))) return r;  // preconditioners frozen in the graph
-        if ((r = cycle_enqueue(lv, n, lvl + 1, vw, itercrsn, iterrfne))) return r;
+        if ((r = cycle_enqueue(lv, n, lvl + 1, vw, itercrsn, iterrfne, eval_prcn))) return r;
         if ((r = mg_prolong_enqueue(lv[lvl + 1]))) return r;
+        if (eval_prcn && iterrfne && (r = enqueue_prcn(c))) return r;
         for (int it = 0; it < iterrfne; ++it) enqueue_update(c);
     }
     return HP_OK;
@@ -1396,7 +1407,7 @@ struct VGraph {
 };
 
 extern "C" int hp_gpu_capture_vcycle(hp_gpu_ctx **levels, int nlevels, int vw, int itercrsn, int iterrfne,
-                                     void **graph_out) {
+                                     int eval_prcn, void **graph_out) {
     if (!levels || nlevels < 1 || !graph_out) return HP_EINVAL;
     for (int l = 0; l < nlevels; ++l) {
         if (levels[l]->stream != levels[0]->stream) { set_err("all levels must share one stream"); return HP_EINVAL; }
@@ -1406,7 +1417,7 @@ extern "C" int hp_gpu_capture_vcycle(hp_gpu_ctx **levels, int nlevels, int vw, i
     cudaStream_t s = levels[0]->stream;
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    int r = cycle_enqueue(levels, nlevels, 0, vw, itercrsn, iterrfne);
+    int r = cycle_enqueue(levels, nlevels, 0, vw, itercrsn, iterrfne, eval_prcn);
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (r) return r;
     if (e != cudaSuccess) { set_err("V-cycle capture failed: %s", cudaGetErrorString(e)); return HP_ECUDA; }
@@ -1433,11 +1444,12 @@ extern "C" int hp_gpu_destroy_vcycle(void *graph) {
     return HP_OK;
 }
 
-// hp_gpu_solve_mg with the cycle replayed from one captured graph (preconditioners
-// frozen at the entry state: preconditioner_interval = 0).
+// hp_gpu_solve_mg with every cycle after the first replayed from a captured graph:
+// one with the preconditioner set-ups inside (cycles where nc % prcn_every == 0) and
+// one with them frozen (prcn_every = 0: every cycle).
 extern "C" int hp_gpu_solve_mg_graph(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycles, int vw,
-                                     int itercrsn, int iterrfne, int check_every, double *hist, int hist_cap,
-                                     int *n_hist, double *seconds, int *cycles) {
+                                     int itercrsn, int iterrfne, int check_every, int prcn_every, double *hist,
+                                     int hist_cap, int *n_hist, double *seconds, int *cycles) {
     if (!levels || nlevels < 1 || drop <= 0.0 || max_cycles < 1) return HP_EINVAL;
     if (check_every < 1) check_every = 1;
     hp_gpu_ctx *f = levels[0];
@@ -1458,18 +1470,32 @@ extern "C" int hp_gpu_solve_mg_graph(hp_gpu_ctx **levels, int nlevels, double dr
     // first cycle evaluates every level's preconditioner at its own state
     if ((r = cycle(levels, nlevels, 0, vw, itercrsn, iterrfne, 1))) return r;
     ++nc;
-    void *vg = nullptr;
-    if ((r = hp_gpu_capture_vcycle(levels, nlevels, vw, itercrsn, iterrfne, &vg))) return r;
+    void *g_frozen = nullptr, *g_eval = nullptr;
+    if ((r = hp_gpu_capture_vcycle(levels, nlevels, vw, itercrsn, iterrfne, 0, &g_frozen))) return r;
+    if (prcn_every > 0 && (r = hp_gpu_capture_vcycle(levels, nlevels, vw, itercrsn, iterrfne, 1, &g_eval))) {
+        hp_gpu_destroy_vcycle(g_frozen);
+        return r;
+    }
+    for (int l = 0; l < nlevels; ++l) cudaMemsetAsync(levels[l]->d_err, 0, 4, f->stream);
+    std::vector<int> bad(nlevels, 0);
     while (true) {
         if ((r = fp64_norm(f, &rn))) break;
+        for (int l = 0; l < nlevels && g_eval; ++l)
+            cudaMemcpyAsync(&bad[l], levels[l]->d_err, 4, cudaMemcpyDeviceToHost, f->stream);
+        if (g_eval) cudaStreamSynchronize(f->stream);
+        int nbad = 0;
+        for (int l = 0; l < nlevels; ++l) nbad += bad[l];
+        if (nbad) { r = nbad; set_err("%d bad elements in a preconditioner set-up", nbad); break; }
         const double d = rn / r0;
         if (hist && nh < hist_cap) hist[nh++] = d;
         if (!(d == d) || d <= drop || nc >= max_cycles) break;
         const int k = std::min(check_every, max_cycles - nc);
-        if ((r = hp_gpu_launch_vcycle(vg, f, k))) break;
-        nc += k;
+        for (int q = 0; q < k && !r; ++q, ++nc)
+            r = hp_gpu_launch_vcycle((g_eval && nc % prcn_every == 0) ? g_eval : g_frozen, f, 1);
+        if (r) break;
     }
-    hp_gpu_destroy_vcycle(vg);
+    hp_gpu_destroy_vcycle(g_frozen);
+    hp_gpu_destroy_vcycle(g_eval);
     if (r) return r;
     CK(cudaEventRecord(e1, f->stream));
     CK(cudaEventSynchronize(e1));

@@ -28,9 +28,13 @@ def _bind():
         lib.hp_gpu_vcycle.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int]
         lib.hp_gpu_solve_mg_graph.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_double, ctypes.c_int,
-                                              ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int,
-                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
-                                              ctypes.POINTER(ctypes.c_int)]
+                                              ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P,
+                                              ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
+        lib.hp_gpu_capture_vcycle.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)]
+        lib.hp_gpu_launch_vcycle.argtypes = [P, P, ctypes.c_int]
+        lib.hp_gpu_destroy_vcycle.argtypes = [P]
         lib.hp_gpu_solve_mg_mixed.argtypes = [ctypes.POINTER(P), ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                               ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int,
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
@@ -149,10 +153,13 @@ class Hierarchy:
         arr = (P * len(self.levels))(*[lv.h for lv in self.levels])
         return arr
 
-    def solve(self, drop=1e-10, max_cycles=500, vw=1, itercrsn=2, iterrfne=2, prcn_every=0, graph=False,
+    def solve(self, drop=1e-10, max_cycles=500, vw=1, itercrsn=2, iterrfne=2, prcn_every=1, graph=False,
               check_every=1, mixed=False):
         """Cycles until the FP64 residual drops by `drop`; returns (hist, seconds, cycles).
-        graph=True replays one captured CUDA graph per cycle (preconditioners frozen);
+        Preconditioners are evaluated every `prcn_every` cycles (the reference's
+        preconditioner_interval, default 1: blocks.cpp:1170,1492); 0 = first cycle only.
+        graph=True replays one captured CUDA graph per cycle (preconditioner set-ups inside
+        every prcn_every cycles, frozen when prcn_every = 0);
         mixed=True runs FP32 cycles on the correction equation inside FP64 defect correction."""
         cap = max_cycles + 2
         hist = np.zeros(cap)
@@ -163,8 +170,9 @@ class Hierarchy:
                                                    ctypes.byref(sec), ctypes.byref(nc)), "solve_mg_mixed")
         elif graph:
             L.check(self.lib.hp_gpu_solve_mg_graph(self.handles(), len(self.levels), drop, max_cycles, vw, itercrsn,
-                                                   iterrfne, check_every, L.ptr(hist), cap, ctypes.byref(nh),
-                                                   ctypes.byref(sec), ctypes.byref(nc)), "solve_mg_graph")
+                                                   iterrfne, check_every, prcn_every, L.ptr(hist), cap,
+                                                   ctypes.byref(nh), ctypes.byref(sec), ctypes.byref(nc)),
+                    "solve_mg_graph")
         else:
             L.check(self.lib.hp_gpu_solve_mg(self.handles(), len(self.levels), drop, max_cycles, vw, itercrsn,
                                              iterrfne, prcn_every, L.ptr(hist), cap, ctypes.byref(nh),

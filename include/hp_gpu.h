@@ -252,19 +252,26 @@ int hp_gpu_solve_mg(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycle
                     int *cycles);
 
 /* One whole cycle of block::cycle as a single CUDA graph (all levels created on
- * one stream, every level's preconditioner set up before capture and frozen
- * inside the graph). The opaque handle is replayed with hp_gpu_launch_vcycle
- * (count cycles back to back on the finest level's stream) and freed with
- * hp_gpu_destroy_vcycle. */
-int hp_gpu_capture_vcycle(hp_gpu_ctx **levels, int nlevels, int vw, int itercrsn, int iterrfne, void **graph);
+ * one stream, every level's preconditioner set up before capture). With
+ * eval_prcn the graph also re-evaluates every level's preconditioner at the
+ * points where block::cycle does (evaluate_preconditioner, blocks.cpp:1279,1335;
+ * bad elements accumulate in the context's count, read by the solve driver);
+ * without, the preconditioners stay frozen inside the graph. The opaque handle is
+ * replayed with hp_gpu_launch_vcycle (count cycles back to back on the finest
+ * level's stream) and freed with hp_gpu_destroy_vcycle. */
+int hp_gpu_capture_vcycle(hp_gpu_ctx **levels, int nlevels, int vw, int itercrsn, int iterrfne, int eval_prcn,
+                          void **graph);
 int hp_gpu_launch_vcycle(void *graph, hp_gpu_ctx *finest, int count);
 int hp_gpu_destroy_vcycle(void *graph);
-/* hp_gpu_solve_mg with the cycle replayed from one captured graph: the first
- * cycle runs level by level with the preconditioners evaluated, the rest replay
- * the graph, `check_every` cycles between residual checks. */
+/* hp_gpu_solve_mg with the cycle replayed from captured graphs: the first cycle
+ * runs level by level with the preconditioners evaluated; later cycles replay the
+ * graph with the preconditioner set-ups inside when nc % prcn_every == 0 (the
+ * reference's preconditioner_interval), else the frozen one (prcn_every = 0:
+ * always); `check_every` cycles between residual checks. Returns > 0 (bad-element
+ * count) if a preconditioner set-up inside the graph met bad elements. */
 int hp_gpu_solve_mg_graph(hp_gpu_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
-                          int iterrfne, int check_every, double *hist, int hist_cap, int *n_hist, double *seconds,
-                          int *cycles);
+                          int iterrfne, int check_every, int prcn_every, double *hist, int hist_cap, int *n_hist,
+                          double *seconds, int *cycles);
 
 /* Multigrid inside FP64 defect correction: each cycle evaluates the FP64
  * residual R64(u) on levels[0], runs one FP32 cycle of the hierarchy on the

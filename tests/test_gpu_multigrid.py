@@ -149,18 +149,21 @@ def test_mixed_multigrid_matches_fp64_multigrid(kind):
     assert num / den < 1e-9
 
 
-def test_vcycle_graph_matches_level_by_level():
+@pytest.mark.parametrize("prcn_every", [0, 1])
+def test_vcycle_graph_matches_level_by_level(prcn_every):
+    """The captured V-cycle replays the level-by-level cycle: with the preconditioner
+    set-ups inside the graph (prcn_every = 1, the reference's default interval) or
+    frozen after the first cycle (prcn_every = 0)."""
     mk = lambda n, p, **kw: hpb.kovasznay_ins(n=n, p=p, re=100.0, **kw)
     H1 = MG.build(mk, n=16, p=4, hlevels=2)
-    h1, s1, c1 = H1.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2)
+    h1, s1, c1 = H1.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2, prcn_every=prcn_every)
     u1 = H1.levels[0].state()
     H1.close()
     H2 = MG.build(mk, n=16, p=4, hlevels=2)
-    h2, s2, c2 = H2.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2, graph=True)
+    h2, s2, c2 = H2.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2, graph=True, prcn_every=prcn_every)
     u2 = H2.levels[0].state()
     H2.close()
-    assert h2[-1] <= 1e-10
-    # the graph freezes the preconditioners after the first cycle, as prcn_every=0 does
+    assert h1[-1] <= 1e-10 and h2[-1] <= 1e-10
     assert abs(c1 - c2) <= 2
     num = np.sqrt(sum(np.sum((a - b) ** 2) for a, b in zip(u1, u2)))
     den = np.sqrt(sum(np.sum(a * a) for a in u1))
