@@ -141,6 +141,43 @@ MG_N = 320
 CD_CFL = {8: 0.3, 6: 0.35, 4: 0.5, 3: 0.6, 2: 0.75, 1: 1.0}
 
 
+def c3_sweep(hpb, dev, n, p, cycles):
+    """ins lid-driven cavity, Re 400 (rho 1, mu 1/400), p on an n x n split-square mesh
+    (n = 512: 524,288 triangles, 28.3 M DOF at p = 6); u = 1 on the lid, velocity
+    Dirichlet on every wall, initial state the boundary field projected plus 1e-3 noise.
+    Hierarchy: p-levels p -> ... -> 1 on the fine mesh, then h-levels n/2, n/4, n/8 at
+    p = 1 (the 524k/131k/32k/8k-triangle meshes). `cycles` V-cycles (2+2 updates per
+    level, preconditioners every cycle) per arm; reports seconds per cycle and the FP64
+    residual drop reached. The h-levels-only hierarchy of the reference's
+    extra_finest_levels = 0 is run as a last arm."""
+    import time as _t
+    from hpb import multigrid as MG
+    mk = lambda n, p, **kw: hpb.lid_cavity_ins(n=n, p=p, re=400.0, **kw)
+    line = {"sweep": "c3", "workload": f"ins lid cavity Re 400, p={p}, {n}x{n} split squares", "cycles": cycles}
+    for name, kw, plev in (("fp64_level_by_level", {}, True), ("fp64_graph", {"graph": True}, True),
+                           ("fp64_graph_autotuned", {"graph": True, "tune": True}, True),
+                           ("fp32_defect_correction", {"mixed": True}, True),
+                           ("fp32_defect_correction_autotuned", {"mixed": True, "tune": True}, True),
+                           ("fp64_h_levels_only", {}, False)):
+        t0 = _t.perf_counter()
+        H = MG.build(mk, n=n, p=p, hlevels=3, plevels=plev)
+        setup = _t.perf_counter() - t0
+        kw = dict(kw)
+        shapes = H.autotune(reps=3) if kw.pop("tune", False) else None
+        hist, sec, cyc = H.solve(drop=1e-10, max_cycles=cycles, prcn_every=1, **kw)
+        line[name] = {"seconds": sec, "cycles": cyc, "ms_per_cycle": 1e3 * sec / max(cyc, 1),
+                      "drop": float(hist[-1]), "drop_history": [float(h) for h in hist[::max(1, cycles // 10)]],
+                      "levels": [f"{len(lv.prob.mesh.tri_pnt)} tri p={lv.prob.p}" for lv in H.levels],
+                      "setup_seconds_host": setup}
+        if shapes:
+            line[name]["shapes"] = shapes
+        if name == "fp64_level_by_level":
+            line["ndof"] = H.probs[0].ndof
+        H.close()
+        print(json.dumps({"arm": name, **line[name]}), flush=True)
+    print(json.dumps(line), flush=True)
+
+
 def timed_factory(torch, flush):
     def timed(fn, n, stream):
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
@@ -344,9 +381,11 @@ def main():
                     help="with --quick / --profile: the matrix-free element kernel instead of stored operators")
     ap.add_argument("--profile", choices=["update64", "update32"], default=None,
                     help="run `steps` multistage updates of the workload in FP64 or FP32 (for profiler runs)")
-    ap.add_argument("--sweep", choices=["c2"], default=None,
+    ap.add_argument("--sweep", choices=["c2", "c3"], default=None,
                     help="c2: cd on the seeded 200k-triangle Delaunay mesh, p = 2, 4, 6, 8: rsdl GDoF/s and time "
-                         "to a 1e-10 drop, plain FP64 vs FP32 defect correction (one JSON line per p)")
+                         "to a 1e-10 drop, plain FP64 vs FP32 defect correction (one JSON line per p); "
+                         "c3: ins lid-driven cavity Re 400, p = 6, 512x512 split squares, V-cycles for --steps "
+                         "cycles: level by level, one CUDA graph, autotuned graph, FP32 defect correction")
     ap.add_argument("--p", type=int, nargs="*", default=None, help="with --sweep: the p values")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -388,6 +427,9 @@ def main():
     if args.sweep == "c2":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         c2_sweep(hpb, dev, args.mesh, args.p or [2, 4, 6, 8], args.steps, timed_factory(torch, flush))
+        return
+    if args.sweep == "c3":
+        c3_sweep(hpb, dev, args.mesh if args.mesh != N_MESH else 512, (args.p or [6])[0], args.steps)
         return
 
     pr = hpb.cd_sinsin(n=args.mesh, p=P, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205)
