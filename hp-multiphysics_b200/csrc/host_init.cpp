@@ -42,6 +42,11 @@ double field_value(const hp_field *f, int n, double x, double y) {
             return f->prm[0] * (x - f->prm[1]) * (x - f->prm[1]);
         case HP_FIELD_LID:
             return (n == 0 && y >= 1.0 - 1e-12) ? 1.0 : 0.0;
+        case HP_FIELD_CYLINDER: {
+            // free stream u = 1 outside the cylinder, rest on and inside it
+            const double d = std::hypot(x - f->prm[0], y - f->prm[1]);
+            return (n == 0 && d > f->prm[2] * (1.0 + 1e-9)) ? 1.0 : 0.0;
+        }
         case HP_FIELD_CONST:
         default:
             return f->prm[n < 4 ? n : 3];
@@ -156,6 +161,24 @@ void side_modes(const Ops &op, const hp_mesh_desc *m, int NV, const hp_field *fl
 }  // namespace
 
 extern "C" {
+
+int hp_curved_side_modes(const hp_basis_tables *t, int nside, const double *ends, const double *curve,
+                         double *modes) {
+    if (!t || nside < 0 || (nside && (!ends || !curve || !modes))) return HP_EINVAL;
+    Ops op(*t);
+    double crd[HP_MXGP], lf[HP_MXX];
+    for (int k = 0; k < nside; ++k) {
+        const double *e = ends + 4 * k;
+        for (int n = 0; n < 2; ++n) {
+            op.proj1d_lin(e[n], e[2 + n], crd);
+            for (int i = 0; i < t->gpx; ++i) crd[i] -= curve[((size_t)k * t->gpx + i) * 2 + n];
+            op.intgrt1d(lf, crd);
+            if (t->sm > 0) Ops::band_solve(t->sm, t->sbwth, &t->sdiag1d[0][0], &lf[2]);
+            for (int m = 0; m < t->sm; ++m) modes[((size_t)k * t->sm + m) * 2 + n] = -lf[2 + m];
+        }
+    }
+    return HP_OK;
+}
 
 int hp_field_eval(const hp_field *f, int n, double x, double y, double *out) {
     if (!f || !out) return HP_EINVAL;

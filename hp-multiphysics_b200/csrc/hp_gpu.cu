@@ -151,19 +151,31 @@ struct LaunchImpl {
         int blocks = nblk(m.ntri, C::WPC);
         const int cap = nsm * tn.elem_cap;
         if (blocks > cap) blocks = cap;
-        k_rsdl_elem<R, P, PHYS><<<blocks, C::WPC * 32, smem(), st>>>(
-            reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, stage, zero_rr, diff, ElemMat<R>{});
+        const auto *t = reinterpret_cast<const DevTables<R, P> *>(tab);
+        k_rsdl_elem<R, P, PHYS, false><<<blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, stage, zero_rr, diff,
+                                                                           ElemMat<R>{});
+        if (m.ncurved > 0)
+            k_rsdl_elem<R, P, PHYS, true><<<std::min(nblk(m.ncurved, C::WPC), cap), C::WPC * 32, smem(), st>>>(
+                t, m, s, ph, stage, zero_rr, diff, ElemMat<R>{});
     }
     static size_t emat_len(long ntri) { return EmatCfg<P>::len(ntri); }
     // one warp item per (element, column j <= T) at beta(nstage) = 1
     static void emat_build(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, ElemMat<R> em, int nsm,
                            cudaStream_t st) {
         if constexpr (PHYS == 0) {
-            const long items = (long)m.ntri * (C::T + 1);
-            long blocks = (items + C::WPC - 1) / C::WPC;
-            if (blocks > (long)nsm * 16) blocks = (long)nsm * 16;
-            k_rsdl_elem<R, P, PHYS><<<(int)blocks, C::WPC * 32, smem(), st>>>(
-                reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, ph.nstage, 1, 0, em);
+            const auto *t = reinterpret_cast<const DevTables<R, P> *>(tab);
+            for (int cv = 0; cv < 2; ++cv) {
+                const long items = (cv ? (long)m.ncurved : (long)m.ntri) * (C::T + 1);
+                if (items == 0) continue;
+                long blocks = (items + C::WPC - 1) / C::WPC;
+                if (blocks > (long)nsm * 16) blocks = (long)nsm * 16;
+                if (cv)
+                    k_rsdl_elem<R, P, PHYS, true><<<(int)blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, ph.nstage, 1, 0,
+                                                                                            em);
+                else
+                    k_rsdl_elem<R, P, PHYS, false><<<(int)blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, ph.nstage, 1,
+                                                                                             0, em);
+            }
         }
     }
     template <bool RE>
@@ -210,7 +222,10 @@ struct LaunchImpl {
         k_minv_vert<R, NV><<<nblk(m.npnt, th), th, 0, st>>>(m, s, mt, sm, im, (R)cfla, upd, fold, slot);
     }
     static cudaError_t set_smem_attr() {
-        return cudaFuncSetAttribute(k_rsdl_elem<R, P, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem());
+        cudaError_t e = cudaFuncSetAttribute(k_rsdl_elem<R, P, PHYS, false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem());
+        if (e != cudaSuccess) return e;
+        return cudaFuncSetAttribute(k_rsdl_elem<R, P, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem());
     }
     static Launchers<R> get() {
         Launchers<R> L;
@@ -271,6 +286,7 @@ struct hp_gpu_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int p = 0, NV = 0, npnt = 0, nseg = 0, ntri = 0, nbseg = 0, sm = 0, im = 0, nsm = 148;
+    int ncurved = 0;  // curved elements (tri.info > -1)
     Phys ph{};
     Launchers<double> L{};
     Launchers<float> L32{};
@@ -502,6 +518,54 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     M.seg_pnt = d_sp; M.seg_tri = d_st; M.seg_loc = d_sl;
     M.vs_ptr = d_vsp; M.vs_idx = d_vsi; M.vt_ptr = d_vtp; M.vt_idx = d_vti;
     M.vess = d_vess; M.sess = d_sess; M.bseg = d_bseg; M.bkind = d_bkind; M.bpibc = d_bpibc;
+    M.tri_cv = nullptr; M.crv_cht = nullptr; M.bcrd = nullptr; M.ncurved = 0; M.crv_tri = nullptr;
+
+    // curved elements (tri_hp::metric::setinfo, metric.cpp:44-70, for p > 1): the
+    // owner triangle of every boundary side with non-zero position modes, with its
+    // vertex and side position modes (crdtocht, gtol.cpp:204-248)
+    if (m->bseg_crd && b->sm > 0 && m->nbseg > 0) {
+        const int sm = b->sm, bmv = b->bm;
+        std::vector<int> tri_cv(nt, -1);
+        std::vector<const double *> side_modes((size_t)3 * nt, nullptr);
+        int ncv = 0;
+        for (int e = 0; e < m->nbseg; ++e) {
+            const double *md = m->bseg_crd + (size_t)e * sm * 2;
+            bool nz = false;
+            for (int k = 0; k < 2 * sm; ++k) nz = nz || md[k] != 0.0;
+            if (!nz) continue;
+            const int sg = m->bseg[e], t = m->seg_tri[2 * sg], i = seg_loc[2 * sg];
+            if (t < 0 || i < 0) { set_err("curved boundary side %d has no triangle", sg); return fail(HP_EINVAL); }
+            side_modes[3 * (size_t)t + i] = md;
+            if (tri_cv[t] < 0) tri_cv[t] = ncv++;
+        }
+        if (ncv > 0) {
+            std::vector<double> cht((size_t)ncv * 2 * bmv, 0.0);
+            std::vector<int> crv_tri(ncv);
+            for (int t = 0; t < nt; ++t) {
+                if (tri_cv[t] < 0) continue;
+                crv_tri[tri_cv[t]] = t;
+                double *cc = &cht[(size_t)tri_cv[t] * 2 * bmv];
+                for (int n = 0; n < 2; ++n) {
+                    for (int k = 0; k < 3; ++k) cc[n * bmv + k] = m->pnts[2 * m->tri_pnt[3 * t + k] + n];
+                    for (int i = 0; i < 3; ++i) {
+                        const double *md = side_modes[3 * (size_t)t + i];
+                        if (!md) continue;
+                        const int sgn = m->tri_sgn[3 * t + i];
+                        for (int k = 0; k < sm; ++k)
+                            cc[n * bmv + 3 + i * sm + k] = ((k & 1) && sgn < 0 ? -1.0 : 1.0) * md[k * 2 + n];
+                    }
+                }
+            }
+            int *d_cv, *d_ctri;
+            double *d_cht, *d_bcrd;
+            if ((r = upload(c, &d_cv, tri_cv.data(), tri_cv.size()))) return fail(r);
+            if ((r = upload(c, &d_cht, cht.data(), cht.size()))) return fail(r);
+            if ((r = upload(c, &d_bcrd, m->bseg_crd, (size_t)m->nbseg * sm * 2))) return fail(r);
+            if ((r = upload(c, &d_ctri, crv_tri.data(), crv_tri.size()))) return fail(r);
+            M.tri_cv = d_cv; M.crv_cht = d_cht; M.bcrd = d_bcrd; M.ncurved = ncv; M.crv_tri = d_ctri;
+            c->ncurved = ncv;
+        }
+    }
 
     // tables
     std::vector<unsigned char> htab(c->L.tab_bytes);

@@ -54,6 +54,14 @@ struct Mesh {
     const int *vess, *sess;      // essential masks
     const int *bseg, *bkind;
     const double *bpibc;  // [nbseg][G]
+    // curved elements (tri.info > -1): tri_cv[t] = index into crv_cht or -1;
+    // crv_cht[cv][2][BM] = vertex and side position modes (crdtocht); bcrd[e][sm][2] =
+    // side position modes of boundary edge e (NULL: all straight)
+    const int *tri_cv;
+    const double *crv_cht;
+    const double *bcrd;
+    int ncurved;         // number of curved elements
+    const int *crv_tri;  // [ncurved] their triangle indices (crv_cht order)
 };
 
 template <typename R>
@@ -131,8 +139,53 @@ struct EmatCfg {
     static size_t len(long ntri) { return (size_t)((ntri + EB - 1) / EB) * TS; }
 };
 
-template <typename R, int P, int PHYS>
-__global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
+// Isoparametric metrics of a curved element at quadrature point (i, j): the r and s
+// derivatives of x and y from the element's vertex and side position modes (interior
+// modes zero), dcrd(n,0) = d x_n / dr and dcrd(n,1) = d x_n / ds (proj_bdry with
+// derivatives, tri_basis/proj.cpp:201-281, of crdtocht, tri_hp/gtol.cpp:204-248).
+template <typename R, int P>
+__device__ __forceinline__ void curved_metrics(const DevTables<R, P> &tb, const double *cht, int i, int j, R &d00,
+                                               R &d01, R &d10, R &d11) {
+    constexpr int X = P + 2, BM = 3 * P;
+    R l1[2] = {(R)0, (R)0}, l2[2] = {(R)0, (R)0};
+    const R oeta = tb.n0[j];
+    for (int n = 0; n < X; ++n) {
+        R w0[2] = {(R)0, (R)0}, w1[2] = {(R)0, (R)0};
+        for (int c = tb.colstart[n]; c < tb.colstart[n + 1]; ++c) {
+            const int m = tb.colmodes[c];
+            if (m >= BM) continue;
+            for (int k = 0; k < 2; ++k) {
+                const R v = (R)cht[k * BM + m];
+                w0[k] += v * tb.gn[j][m];
+                w1[k] += v * tb.dgn[j][m];
+            }
+        }
+        for (int k = 0; k < 2; ++k) {
+            l1[k] += w1[k] * tb.gx[i][n];
+            l2[k] += (w0[k] * oeta) * tb.dgx[i][n];
+        }
+    }
+    d00 = l2[0];
+    d01 = l1[0] + tb.x0[i] * l2[0];
+    d10 = l2[1];
+    d11 = l1[1] + tb.x0[i] * l2[1];
+}
+
+// CTAs per SM the straight-element kernel keeps resident (caps its registers): cd 64
+// registers a thread; ins 85 (FP64, 8 warps), 128 (FP64, 4 warps), 64 (FP32).
+template <typename R, int P, int PHYS, bool CURVED>
+struct ElemMinBlocks {
+    static constexpr int WPC = ElemCfg<R, P, PHYS>::WPC;
+    static constexpr int value = CURVED ? 1
+                                 : PHYS == 0 ? 256 / WPC / 8
+                                 : sizeof(R) == 8 ? (WPC == 8 ? 3 : 4)
+                                                  : (WPC == 8 ? 4 : 8);
+};
+
+// CURVED = false: the straight elements (curved ones are skipped); CURVED = true: the
+// mesh's curved elements only (mesh.crv_tri), with metrics at every quadrature point.
+template <typename R, int P, int PHYS, bool CURVED>
+__global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R, P, PHYS, CURVED>::value)
     k_rsdl_elem(const DevTables<R, P> *__restrict__ gtab, Mesh mesh, State<R> st, Phys ph, int stage, int zero_rr,
                 int diff, ElemMat<R> build) {
     using C = ElemCfg<R, P, PHYS>;
@@ -159,10 +212,13 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
 
     // build mode (cd): one item per (element, column j) with uht = e_j, j = T: uht = 0
     const bool bmode = (PHYS == 0) && build.aim != nullptr;
-    const long nitems = bmode ? (long)mesh.ntri * (T + 1) : (long)mesh.ntri;
+    const long nel = CURVED ? (long)mesh.ncurved : (long)mesh.ntri;
+    const long nitems = bmode ? nel * (T + 1) : nel;
     for (long item = (long)blockIdx.x * C::WPC + warp; item < nitems; item += (long)gridDim.x * C::WPC) {
-        const int tind = bmode ? (int)(item / (T + 1)) : (int)item;
-        const int bcol = bmode ? (int)(item - (long)tind * (T + 1)) : -1;
+        const int eidx = bmode ? (int)(item / (T + 1)) : (int)item;
+        const int bcol = bmode ? (int)(item - (long)eidx * (T + 1)) : -1;
+        const int tind = CURVED ? mesh.crv_tri[eidx] : eidx;
+        if (!CURVED && mesh.tri_cv && mesh.tri_cv[tind] >= 0) continue;  // done by the curved launch
         const int p0 = mesh.tri_pnt[3 * tind], p1 = mesh.tri_pnt[3 * tind + 1], p2 = mesh.tri_pnt[3 * tind + 2];
         // ---- gather (ugtouht, gtol.cpp:14-55)
         for (int w = lane; w < NV * T; w += 32) {
@@ -205,8 +261,14 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
         const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
         const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
         const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
-        const R d00 = (R)(0.5 * (x2d - x1d)), d01 = (R)(0.5 * (x0d - x1d));
-        const R d10 = (R)(0.5 * (y2d - y1d)), d11 = (R)(0.5 * (y0d - y1d));
+        const R g00 = (R)(0.5 * (x2d - x1d)), g01 = (R)(0.5 * (x0d - x1d));
+        const R g10 = (R)(0.5 * (y2d - y1d)), g11 = (R)(0.5 * (y0d - y1d));
+        // curved element: metrics at every point from its position modes (rsdl.cpp:83-258)
+        const double *cht = CURVED ? mesh.crv_cht + (size_t)eidx * 2 * BM : nullptr;
+        auto metric = [&](int i, int j, R &a, R &b, R &c, R &d) {
+            if constexpr (CURVED) curved_metrics<R, P>(tb, cht, i, j, a, b, c, d);
+            else { a = g00; b = g01; c = g10; d = g11; }
+        };
         __syncwarp();
         // ---- proj stage I (proj.cpp:46-95): wk[q][j][n]; q = 2*var (value), 2*var+1 (d/deta)
         {
@@ -232,6 +294,8 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
         for (int w = lane; w < GG; w += 32) {
             const int i = w / G, j = w - i * G;
             const R oeta = tb.n0[j], xp1 = tb.x0[i];
+            R d00, d01, d10, d11;
+            metric(i, j, d00, d01, d10, d11);
             if (PHYS == 1) {
                 R uu[3], dr[2], ds[2];
                 for (int var = 0; var < 2; ++var) {
@@ -396,7 +460,12 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                 const R *fr = PT(sr), *fs = PT(ss);
                 R acc;
                 if (PHYS == 1) acc = (R)0;  // rhorbd0*u + dugdt with bd(0) = 0
-                else acc = -(d00 * d11 - d10 * d01) * srcv;
+                else {
+                    R d00, d01, d10, d11;
+                    metric(i, j, d00, d01, d10, d11);
+                    acc = -(d00 * d11 - d10 * d01) * srcv;
+                    if (CURVED) PT(8)[r] = acc;  // the source field, integrated below
+                }
                 const R ln0 = tb.n0[j];
                 {
                     const R wi = fr[i * G + j] * tb.dltx[i] * ln0;
@@ -422,9 +491,11 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                 const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
                                      sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
                 const R h = (R)((area / perim) / (0.25 * (P + 1) * (P + 1)));
-                const R cjcb = d00 * d11 - d10 * d01;
                 const R nu = (R)(ph.mu / ph.rho);
                 for (int w = lane; w < GG; w += 32) {
+                    R d00, d01, d10, d11;
+                    metric(w / G, w - (w / G) * G, d00, d01, d10, d11);
+                    const R cjcb = d00 * d11 - d10 * d01;
                     const R u0 = PT(14)[w], u1 = PT(15)[w];
                     const R q = PT(19)[w];
                     const R t2 = (R)2. * nu / h;
@@ -444,6 +515,8 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                 const R taue = st.tau[tind];
                 const R ax = (R)ph.ax, ay = (R)ph.ay;
                 for (int w = lane; w < GG; w += 32) {
+                    R d00, d01, d10, d11;
+                    metric(w / G, w - (w / G) * G, d00, d01, d10, d11);
                     const R tres = taue * PT(7)[w];
                     PT(4)[w] -= (d11 * ax - d01 * ay) * tres;
                     PT(5)[w] -= (-d10 * ax + d00 * ay) * tres;
@@ -458,13 +531,14 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32)
                 const int n = w / T, m = w - n * T;
                 R val = mode_result(n, m);
                 if (PHYS == 0 && srcv != (R)0) {
-                    // intgrt of a constant field c: sum_j gnwtn(m,j) * sum_i c*gxwtx(col,i)
-                    const R cval = -(d00 * d11 - d10 * d01) * srcv;
+                    // intgrt (intgrt.cpp:22-78) of res0 = -cjcb*src: sum_j gnwtn(m,j) sum_i
+                    // res0(i,j) gxwtx(col,i); constant over a straight element
+                    const R cval = -(g00 * g11 - g10 * g01) * srcv;
                     const int col = tb.colof[m];
                     R l0 = 0;
                     for (int j = 0; j < G; ++j) {
-                        R s = cval * tb.gxwtx[col][0];
-                        for (int i = 1; i < G; ++i) s += cval * tb.gxwtx[col][i];
+                        R s = (CURVED ? PT(8)[j] : cval) * tb.gxwtx[col][0];
+                        for (int i = 1; i < G; ++i) s += (CURVED ? PT(8)[i * G + j] : cval) * tb.gxwtx[col][i];
                         l0 += tb.gnwtn[m][j] * s;
                     }
                     val = l0 + val;
@@ -650,9 +724,15 @@ __global__ void k_bdry_flux_ins(const DevTables<R, P> *__restrict__ tb, Mesh mes
     for (int n = 0; n < NV; ++n)
         for (int m = 0; m < X - 1; ++m) acc[n][m] = 0;
     for (int k = 0; k < G; ++k) {
-        // proj1d of the straight side coordinates: derivative only
-        const R dx = xa * tb->dgx[k][1] + xb * tb->dgx[k][2];
-        const R dy = ya * tb->dgx[k][1] + yb * tb->dgx[k][2];
+        // proj1d of the side coordinates: derivative only
+        R dx = xa * tb->dgx[k][1] + xb * tb->dgx[k][2];
+        R dy = ya * tb->dgx[k][1] + yb * tb->dgx[k][2];
+        if (mesh.bcrd) {  // curved side: its position modes (crdtocht1d)
+            for (int m = 0; m < SM; ++m) {
+                dx += (R)mesh.bcrd[((size_t)e * SM + m) * 2] * tb->dgx[k][m + 3];
+                dy += (R)mesh.bcrd[((size_t)e * SM + m) * 2 + 1] * tb->dgx[k][m + 3];
+            }
+        }
         R nrm0 = dy, nrm1 = -dx;
         const R jcb = rsqrt_<R>(nrm0 * nrm0 + nrm1 * nrm1);
         nrm0 /= jcb; nrm1 /= jcb;
@@ -955,9 +1035,31 @@ __global__ void k_prcn_elem(const DevTables<R, P> *__restrict__ tb, Mesh mesh, S
                 qmax = (q > qmax ? q : qmax);
             }
         }
-        hmax = sqrt(hmax);
-        const double h = 4. * jcb / (p1 * hmax);
-        hmax = hmax / p1;
+        double h;
+        const int cvi = mesh.tri_cv ? mesh.tri_cv[t] : -1;
+        if (cvi >= 0) {
+            // curved element (setup_preconditioner.cpp:45-87): smallest point Jacobian and
+            // longest side tangent over the quadrature points
+            const double *cht = mesh.crv_cht + (size_t)cvi * 2 * BM;
+            double jcbmin = jcb, hm = 0.0;
+            for (int i = 0; i < G; ++i)
+                for (int j = 0; j < G; ++j) {
+                    R a, b, c, d;
+                    curved_metrics<R, P>(*tb, cht, i, j, a, b, c, d);
+                    const double d00 = a, d01 = b, d10 = c, d11 = d;
+                    jcbmin = fmin(jcbmin, d00 * d11 - d10 * d01);
+                    hm = fmax(hm, d00 * d00 + d10 * d10);
+                    hm = fmax(hm, d01 * d01 + d11 * d11);
+                    hm = fmax(hm, (d01 - d00) * (d01 - d00) + (d11 - d10) * (d11 - d10));
+                }
+            hmax = 2. * sqrt(hm);
+            h = 4. * jcbmin / (p1 * hmax);
+            hmax = hmax / p1;
+        } else {
+            hmax = sqrt(hmax);
+            h = 4. * jcb / (p1 * hmax);
+            hmax = hmax / p1;
+        }
         if (!(h > 0.0) || isnan(qmax)) { atomicAdd(err, 1); return; }
         const double nu = ph.mu / ph.rho;
         double gam = 3.0 * qmax + (0.5 * hmax * ph.bd0 + 2. * nu / hmax) * (0.5 * hmax * ph.bd0 + 2. * nu / hmax);

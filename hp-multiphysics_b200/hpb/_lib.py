@@ -25,6 +25,7 @@ HP_FIELD_KOVASZNAY = 1
 HP_FIELD_SINSIN = 2
 HP_FIELD_QUADX = 3
 HP_FIELD_LID = 4
+HP_FIELD_CYLINDER = 5
 
 _D = ctypes.c_double
 _I = ctypes.c_int
@@ -64,7 +65,7 @@ class MeshDesc(ctypes.Structure):
         ("seg_pnt", ctypes.POINTER(_I)), ("seg_tri", ctypes.POINTER(_I)),
         ("tri_pnt", ctypes.POINTER(_I)), ("tri_seg", ctypes.POINTER(_I)), ("tri_sgn", ctypes.POINTER(_I)),
         ("nbseg", _I), ("bseg", ctypes.POINTER(_I)), ("bseg_kind", ctypes.POINTER(_I)),
-        ("bseg_pibc", ctypes.POINTER(_D)),
+        ("bseg_pibc", ctypes.POINTER(_D)), ("bseg_crd", ctypes.POINTER(_D)),
     ]
 
 
@@ -123,6 +124,7 @@ def lib():
         L.hp_field_eval.argtypes = [ctypes.POINTER(Field), _I, _D, _D, P]
         L.hp_tobasis.argtypes = [ctypes.POINTER(BasisTables), ctypes.POINTER(MeshDesc), _I, ctypes.POINTER(Field),
                                  P, P, P]
+        L.hp_curved_side_modes.argtypes = [ctypes.POINTER(BasisTables), _I, P, P, P]
         L.hp_setvalues.argtypes = [ctypes.POINTER(BasisTables), ctypes.POINTER(MeshDesc), _I, ctypes.POINTER(Field),
                                    P, P]
         L.hp_l2error.argtypes = [ctypes.POINTER(BasisTables), ctypes.POINTER(MeshDesc), _I, ctypes.POINTER(Field),

@@ -7,6 +7,8 @@
   (square7.grd = 64 x 64 squares = 8,192 triangles).
 * ``delaunay_square(n, seed)``: a seeded Delaunay triangulation of the unit
   square with about 2 n^2 triangles and a checked minimum angle.
+* ``channel_hole(...)``: a graded Delaunay mesh of a channel with a circular hole
+  (its hole sides are made curved by the workload's boundary curve).
 * ``read_grd(path)``: the reference's .grd text format (tri_mesh/input.cpp:504-600).
 * ``createsegtri``: segment/triangle connectivity with the reference's
   conventions (tri_mesh/setup.cpp:76-145): tri.seg(j) is the side opposite
@@ -138,6 +140,77 @@ def delaunay_square(n, seed=20261205, jitter=0.12, margin=0.7, min_angle=20.0):
     mesh.min_angle = float(min_angles(mesh).min())
     if mesh.min_angle < min_angle:
         raise ValueError(f"Delaunay mesh min angle {mesh.min_angle:.2f} < {min_angle}")
+    return mesh
+
+
+def channel_hole(L=20.0, H=10.0, cx=5.0, cy=5.0, r=0.5, hmin=0.02, hmax=0.2, grade=0.0085, seed=20261207,
+                 jitter=0.05, margin=0.6, min_angle=15.0):
+    """Graded Delaunay mesh of the channel [0,L] x [0,H] with a circular hole of radius r
+    at (cx, cy). Local edge length h(d) = min(hmax, hmin + grade * d), d the distance
+    from the hole. Points: rings around the hole at radius steps h*sqrt(3)/2 holding
+    2*pi*radius/h points each (alternate rings offset by half a spacing; the first ring
+    on the circle itself), ring points closer than margin*h to a wall dropped, the walls
+    sampled at the local h; interior points jittered by splitmix64 uniforms of
+    +-jitter*h; Qhull Delaunay, triangles inside the hole removed, counter-clockwise,
+    Z-curve numbering. Defaults: ~150k triangles. Raises below min_angle degrees."""
+    from scipy.spatial import Delaunay
+
+    def hf(d):
+        return np.minimum(hmax, hmin + grade * np.maximum(d, 0.0))
+
+    rings = []
+    rk, k = r, 0
+    rmax = np.hypot(max(cx, L - cx), max(cy, H - cy))
+    while rk < rmax + hmax:
+        h = float(hf(rk - r))
+        n = max(8, int(round(2.0 * np.pi * rk / h)))
+        th = (np.arange(n) + 0.5 * (k % 2)) * 2.0 * np.pi / n
+        rings.append(np.stack([cx + rk * np.cos(th), cy + rk * np.sin(th)], 1))
+        rk += h * np.sqrt(3.0) / 2.0
+        k += 1
+    n0 = len(rings[0])
+    pts = np.concatenate(rings)
+    d = np.hypot(pts[:, 0] - cx, pts[:, 1] - cy) - r
+    hp = hf(d)
+    jit = jitter * hp[:, None] * splitmix64_uniform(seed, pts.size).reshape(pts.shape)
+    jit[:n0] = 0.0  # the hole's own points stay on the circle
+    pts = pts + jit
+    wall = np.minimum(np.minimum(pts[:, 0], L - pts[:, 0]), np.minimum(pts[:, 1], H - pts[:, 1]))
+    keep = np.arange(len(pts)) < n0
+    keep |= wall > margin * hp
+    pts = pts[keep]
+    walls = []
+    for (x0, y0, x1, y1) in ((0.0, 0.0, L, 0.0), (L, 0.0, L, H), (L, H, 0.0, H), (0.0, H, 0.0, 0.0)):
+        seg = np.hypot(x1 - x0, y1 - y0)
+        ts, t = [0.0], 0.0
+        while True:
+            x, y = x0 + (x1 - x0) * t / seg, y0 + (y1 - y0) * t / seg
+            step = float(hf(np.hypot(x - cx, y - cy) - r))
+            t += step
+            if t >= seg - 0.3 * step:
+                break
+            ts.append(t)
+        ts = np.array(ts)
+        walls.append(np.stack([x0 + (x1 - x0) * ts / seg, y0 + (y1 - y0) * ts / seg], 1))
+    pts = np.concatenate([pts] + walls)
+    span = max(L, H)
+    pts = pts[np.argsort(morton_key(pts / span), kind="stable")]
+    tri = Delaunay(pts).simplices.astype(np.int64)
+    cen = pts[tri].mean(axis=1)
+    tri = tri[np.hypot(cen[:, 0] - cx, cen[:, 1] - cy) > r]
+    a = pts[tri]
+    ar = (a[:, 1, 0] - a[:, 0, 0]) * (a[:, 2, 1] - a[:, 0, 1]) - (a[:, 1, 1] - a[:, 0, 1]) * (a[:, 2, 0] - a[:, 0, 0])
+    tri[ar < 0] = tri[ar < 0][:, [0, 2, 1]]
+    tri = tri[np.argsort(morton_key(pts[tri].mean(axis=1) / span), kind="stable")]
+    used = np.unique(tri)
+    remap = np.full(len(pts), -1, dtype=np.int64)
+    remap[used] = np.arange(len(used))
+    mesh = Mesh(pts[used], remap[tri])
+    mesh.min_angle = float(min_angles(mesh).min())
+    mesh.hole = (cx, cy, r)
+    mesh.box = (L, H)
+    if mesh.min_angle < min_angle:
+        raise ValueError(f"channel mesh min angle {mesh.min_angle:.2f} < {min_angle}")
     return mesh
 
 

@@ -10,7 +10,7 @@ import ctypes
 import numpy as np
 
 from . import _lib as L
-from .mesh import square_mesh, splitmix64_uniform
+from .mesh import square_mesh, channel_hole, splitmix64_uniform
 
 # Multistage defaults (tri_mesh/blocks.cpp:1124-1148) and CFL per log2p (tri_hp/allocate.cpp:275)
 ALPHA_DFLT = (0.25, 1.0 / 6.0, 0.375, 0.5, 1.0)
@@ -71,24 +71,50 @@ class Problem:
 
     # --- boundary conditions -------------------------------------------------
     def _set_bc(self, bc):
-        """bc: list of (segment-index array, kind) with kind = essential mask | flux form."""
-        bsegs, kinds = [], []
-        for segs, kind in bc:
+        """bc: list of (segment-index array, kind[, curve]) with kind = essential mask |
+        flux form; `curve(X, Y) -> (Xc, Yc)` maps points near the boundary onto it (the
+        reference's mvpttobdry) and makes those sides curved (p > 1)."""
+        bsegs, kinds, curved = [], [], []
+        off = 0
+        for entry in bc:
+            segs, kind = entry[0], entry[1]
+            curve = entry[2] if len(entry) > 2 else None
             segs = np.asarray(segs, dtype=np.int32)
             bsegs.append(segs)
             kinds.append(np.full(len(segs), kind, dtype=np.int32))
+            curved.append((off, len(segs), curve))
+            off += len(segs)
         self.bseg = np.ascontiguousarray(np.concatenate(bsegs) if bsegs else np.zeros(0, np.int32))
         self.bkind = np.ascontiguousarray(np.concatenate(kinds) if kinds else np.zeros(0, np.int32))
         G = self.tab.gpx
+        gx = np.array([[self.tab.gx[k][n] for n in range(self.tab.nmodx)] for k in range(G)])
+        v0 = self.mesh.seg_pnt[self.bseg, 0]
+        v1 = self.mesh.seg_pnt[self.bseg, 1]
+        # straight chord at the side Gauss points
+        X = np.outer(self.mesh.pnts[v0, 0], gx[:, 1]) + np.outer(self.mesh.pnts[v1, 0], gx[:, 2])
+        Y = np.outer(self.mesh.pnts[v0, 1], gx[:, 1]) + np.outer(self.mesh.pnts[v1, 1], gx[:, 2])
+        self.bcrd = None
+        if self.sm > 0 and any(c is not None for _, _, c in curved):
+            # hp_edge_bdry::curv_init: side modes of (curve - chord)
+            self.bcrd = np.zeros((len(self.bseg), self.sm, 2))
+            for o, cnt, curve in curved:
+                if curve is None or cnt == 0:
+                    continue
+                sl = slice(o, o + cnt)
+                xc, yc = curve(X[sl], Y[sl])
+                ends = np.ascontiguousarray(np.stack([self.mesh.pnts[v0[sl]], self.mesh.pnts[v1[sl]]], 1))
+                cur = np.ascontiguousarray(np.stack([xc, yc], -1), dtype=np.float64)
+                out = np.zeros((cnt, self.sm, 2))
+                L.check(L.lib().hp_curved_side_modes(ctypes.byref(self.tab), cnt, L.ptr(ends), L.ptr(cur),
+                                                     L.ptr(out)), "hp_curved_side_modes")
+                self.bcrd[sl] = out
+            self.bcrd = np.ascontiguousarray(self.bcrd)
+            # positions on the curved sides (proj1d of the position modes)
+            X = X + np.einsum("em,km->ek", self.bcrd[:, :, 0], gx[:, 3:3 + self.sm])
+            Y = Y + np.einsum("em,km->ek", self.bcrd[:, :, 1], gx[:, 3:3 + self.sm])
         self.bpibc = np.zeros((max(len(self.bseg), 1), G))
         if self.physics == L.HP_PHYS_INS and self.field is not None and len(self.bseg):
             # ibc->f(NV-1, x) at the side Gauss points of each boundary edge
-            gx1 = np.array([self.tab.gx[k][1] for k in range(G)])
-            gx2 = np.array([self.tab.gx[k][2] for k in range(G)])
-            v0 = self.mesh.seg_pnt[self.bseg, 0]
-            v1 = self.mesh.seg_pnt[self.bseg, 1]
-            X = np.outer(self.mesh.pnts[v0, 0], gx1) + np.outer(self.mesh.pnts[v1, 0], gx2)
-            Y = np.outer(self.mesh.pnts[v0, 1], gx1) + np.outer(self.mesh.pnts[v1, 1], gx2)
             self.bpibc[: len(self.bseg)] = self.eval_field(2, X, Y)
         self.bpibc = np.ascontiguousarray(self.bpibc)
 
@@ -113,6 +139,7 @@ class Problem:
         d.bseg = L.iptr(self.bseg)
         d.bseg_kind = L.iptr(self.bkind)
         d.bseg_pibc = L.dptr(self.bpibc)
+        d.bseg_crd = L.dptr(self.bcrd) if self.bcrd is not None else None
         self.desc = d
 
     # --- initial state -------------------------------------------------------
@@ -300,6 +327,41 @@ def cd_sinsin(mesh=None, n=64, p=4, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed
         field = L.Field(L.HP_FIELD_SINSIN, (ctypes.c_double * 4)(1.0, 0, 0, 0))
     bc = [(mesh.boundary_segments(), 0b1)]
     prob = Problem(mesh, p, L.HP_PHYS_CD, rhocv=1.0, kcond=kcond, ax=ax, ay=ay, field=field, bc=bc, **kw)
+    return prob.tobasis(noise=noise, seed=seed)
+
+
+def circle_curve(cx, cy, r):
+    """mvpttobdry of a circular boundary: radial projection onto the circle."""
+    def curve(X, Y):
+        dx, dy = X - cx, Y - cy
+        d = np.hypot(dx, dy)
+        return cx + r * dx / d, cy + r * dy / d
+    return curve
+
+
+def channel_cylinder_ins(scale=1.0, p=4, re=100.0, noise=1e-3, seed=20261207, curved=True, mesh=None, **kw):
+    """ins flow past a cylinder: channel [0,20] x [0,10] with a hole of radius 0.5 at
+    (5, 5) (diameter 1, so Re = 1/mu at rho = 1 and free-stream speed 1), graded mesh
+    channel_hole with edge lengths scaled by `scale` (1: ~150k triangles), or `mesh` (a
+    channel_hole mesh). Free stream (velocity essential + generic flux) on the left, top
+    and bottom walls, outflow (generic flux, p = 0) on the right, no-slip (velocity
+    essential + generic flux) on the hole, whose sides are curved (isoparametric, p > 1)
+    unless curved=False. Initial state: free stream u = 1 outside the cylinder plus
+    seeded noise."""
+    if mesh is None:
+        mesh = channel_hole(hmin=0.02 * scale, hmax=0.2 * scale, grade=0.0085 * scale)
+    cx, cy, r = mesh.hole
+    field = L.Field(L.HP_FIELD_CYLINDER, (ctypes.c_double * 4)(cx, cy, r, 0))
+    b = mesh.boundary_segments()
+    mid = 0.5 * (mesh.pnts[mesh.seg_pnt[b, 0]] + mesh.pnts[mesh.seg_pnt[b, 1]])
+    Lx, Hy = mesh.box
+    eps = 1e-9
+    hole = np.hypot(mid[:, 0] - cx, mid[:, 1] - cy) < r + eps
+    outflow = (~hole) & (mid[:, 0] > Lx - eps)
+    inflow = (~hole) & (~outflow)
+    bc = [(b[inflow], 0b011 | L.HP_BC_FLUX_INS_GENERIC), (b[outflow], L.HP_BC_FLUX_INS_GENERIC),
+          (b[hole], 0b011 | L.HP_BC_FLUX_INS_GENERIC, circle_curve(cx, cy, r) if curved else None)]
+    prob = Problem(mesh, p, L.HP_PHYS_INS, rho=1.0, mu=1.0 / re, field=field, bc=bc, **kw)
     return prob.tobasis(noise=noise, seed=seed)
 
 

@@ -101,6 +101,14 @@ typedef struct hp_mesh_desc {
     const int *bseg;      /* [nbseg] segment index */
     const int *bseg_kind; /* [nbseg] HP_BC_* */
     const double *bseg_pibc; /* [nbseg][gpx] or NULL */
+    /* Curved boundary sides: the side modes of the boundary position, the
+     * reference's hp_edge_bdry::crds(indx, m, n) ([nbseg][sm][2], NULL = every side
+     * straight; hp_curved_side_modes computes them as curv_init does). A triangle
+     * with a side whose modes are not all zero is a curved element (tri.info > -1,
+     * tri_hp::metric::setinfo, metric.cpp:44-70): its residual and preconditioner
+     * use the isoparametric metrics at every quadrature point (proj_bdry of the
+     * vertex and side position modes, crdtocht, gtol.cpp:204-248). */
+    const double *bseg_crd;
 } hp_mesh_desc;
 
 #define HP_PHYS_CD 0  /* tri_hp_cd  (tri_hp/cd/tri_hp_cd.h:16, CONST_A) NV=1 */

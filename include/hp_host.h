@@ -20,6 +20,8 @@ extern "C" {
 #define HP_FIELD_SINSIN 2    /* prm[0] * sin(pi x) sin(pi y) */
 #define HP_FIELD_QUADX 3     /* prm[0] * (x - prm[1])^2 ; conv-diff/Correctness/Inputs/run.inpt ibc0 */
 #define HP_FIELD_LID 4       /* u = 1 on the lid y = 1, 0 elsewhere; v = p = 0 */
+#define HP_FIELD_CYLINDER 5  /* u = 1 outside the circle of centre (prm[0], prm[1]), radius prm[2], 0 on and
+                                inside it; v = p = 0 (free stream past a cylinder at rest) */
 
 typedef struct hp_field {
     int kind;
@@ -41,6 +43,15 @@ int hp_tobasis(const hp_basis_tables *t, const hp_mesh_desc *m, int NV, const hp
  * variables of every boundary edge of m (bseg_kind bits 0..7). */
 int hp_setvalues(const hp_basis_tables *t, const hp_mesh_desc *m, int NV, const hp_field *f, double *ugv,
                  double *ugs);
+
+/* hp_edge_bdry::curv_init (tri_hp/hp_boundary.cpp:621-678): side modes of curved
+ * boundary positions. For each of nside sides, ends[k] = {x0, y0, x1, y1} are its
+ * end vertices and curve[k][i] = {x, y} the boundary point that
+ * base.mvpttobdry maps the straight chord's i-th Gauss point (parameter xp(i)) to;
+ * modes[k][m] = {x, y} receives the L2 projection of (curve - chord) onto the side
+ * modes (1D intgrt with the sdiag1d band inversion), the bseg_crd input of
+ * hp_mesh_desc. */
+int hp_curved_side_modes(const hp_basis_tables *t, int nside, const double *ends, const double *curve, double *modes);
 
 /* tri_hp::l2error (tri_hp/l2error.cpp:13-67): per-variable L2 and Linf error of
  * the state against f at the Gauss points. */

@@ -283,6 +283,9 @@ struct or_ctx {
     std::vector<int> bseg, bkind;
     std::vector<double> bpibc;
     std::vector<int> vess, sess;  // essential masks
+    std::vector<double> bcrd;     // [nbseg][sm][2] curved side position modes (empty: straight)
+    std::vector<int> seg_bdry;    // [nseg] boundary index e of a segment or -1
+    std::vector<char> curved;     // [ntri] tri.info > -1
     // vsi arrays
     std::vector<double> ugv, ugs, ugi, resv, ress, resi, rrv, rrs, rri, u0v, u0s, u0i;
     std::vector<double> vprcn, sprcn, tprcn, tau;  // tau [ntri][NV] (cd uses column 0)
@@ -304,6 +307,51 @@ static double inscribedradius(const or_ctx *c, int t) {  // tri_mesh/tprims.cpp:
     double perim = std::sqrt(dx1 * dx1 + dy1 * dy1) + std::sqrt(dx2 * dx2 + dy2 * dy2) +
                    std::sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
     return area / perim;
+}
+
+static bool side_is_curved(const or_ctx *c, int e) {
+    if (c->bcrd.empty() || e < 0) return false;
+    for (int k = 0; k < 2 * c->sm; ++k)
+        if (c->bcrd[(size_t)e * c->sm * 2 + k] != 0.0) return true;
+    return false;
+}
+
+// tri_hp::crdtocht (gtol.cpp:204-248): vertex coordinates, then per side the boundary
+// side's position modes (hp_ebdry->crds) on curved sides and 0 elsewhere; interior 0
+static void crdtocht(const or_ctx *c, int tind, double (*cht)[HP_MXTM]) {
+    for (int n = 0; n < 2; ++n)
+        for (int m = 0; m < HP_MXTM; ++m) cht[n][m] = 0.0;
+    for (int i = 0; i < 3; ++i)
+        for (int n = 0; n < 2; ++n) cht[n][i] = c->pnts[2 * c->tri_pnt[3 * tind + i] + n];
+    int cnt = 3;
+    for (int i = 0; i < 3; ++i) {
+        const int sind = c->tri_seg[3 * tind + i];
+        const int e = c->seg_bdry[sind];
+        const bool cv = c->seg_tri[2 * sind + 1] < 0 && side_is_curved(c, e);
+        for (int m = 0; m < c->sm; ++m, ++cnt)
+            for (int n = 0; n < 2; ++n) cht[n][cnt] = cv ? c->bcrd[((size_t)e * c->sm + m) * 2 + n] : 0.0;
+    }
+}
+
+// Metrics at the quadrature points: curved element (tri.info > -1) from proj_bdry of
+// crdtocht (metric.cpp:12-20, proj.cpp:201-281: the projection of a coefficient vector
+// whose interior modes are zero), straight element the constant ldcrd.
+static void element_metrics(const or_ctx *c, int tind, PtArr (*dc)[2]) {
+    const Basis &B = *c->B;
+    if (c->curved[tind]) {
+        double cht[2][HP_MXTM];
+        static PtArr crd;
+        crdtocht(c, tind, cht);
+        for (int n = 0; n < 2; ++n) B.proj(cht[n], &crd[0][0], &dc[n][0][0][0], &dc[n][1][0][0], MXGP);
+        return;
+    }
+    const int v[3] = {c->tri_pnt[3 * tind], c->tri_pnt[3 * tind + 1], c->tri_pnt[3 * tind + 2]};
+    for (int n = 0; n < 2; ++n) {
+        const double a = 0.5 * (c->pnts[2 * v[2] + n] - c->pnts[2 * v[1] + n]);
+        const double b = 0.5 * (c->pnts[2 * v[0] + n] - c->pnts[2 * v[1] + n]);
+        for (int i = 0; i < c->gpx; ++i)
+            for (int j = 0; j < c->gpn; ++j) { dc[n][0][i][j] = a; dc[n][1][i][j] = b; }
+    }
 }
 
 // tri_hp/gtol.cpp:14-55 (fine level: sm == sm0)
@@ -351,20 +399,17 @@ static void lftog(or_ctx *c, int tind, double (*lfl)[HP_MXTM], double *gv, doubl
     }
 }
 
-// tri_hp/cd/rsdl.cpp:14-154 (CONST_A, straight element, steady)
+// tri_hp/cd/rsdl.cpp:14-154 (CONST_A, steady; curved elements with the metrics of calc_metrics)
 static void element_rsdl_cd(or_ctx *c, int tind, int stage, double (*lf_re)[HP_MXTM], double (*lf_im)[HP_MXTM]) {
     const Basis &B = *c->B;
     const int gpx = c->gpx, gpn = c->gpn;
     const hp_phys_params &ph = c->ph;
     static PtArr crd[2], u, du0, du1, res, cjcb, cv00, cv01, e00, e01;
-    double dcrd[2][2];
+    static PtArr dc[2][2];
     int v[3] = {c->tri_pnt[3 * tind], c->tri_pnt[3 * tind + 1], c->tri_pnt[3 * tind + 2]};
     for (int n = 0; n < 2; ++n)
         B.proj(c->pnts[2 * v[0] + n], c->pnts[2 * v[1] + n], c->pnts[2 * v[2] + n], &crd[n][0][0], MXGP);
-    for (int n = 0; n < 2; ++n) {
-        dcrd[n][0] = 0.5 * (c->pnts[2 * v[2] + n] - c->pnts[2 * v[1] + n]);
-        dcrd[n][1] = 0.5 * (c->pnts[2 * v[0] + n] - c->pnts[2 * v[1] + n]);
-    }
+    element_metrics(c, tind, dc);
     const double mv0 = 0.0, mv1 = 0.0;  // bd(0)*(crd - dxdt) with bd(0) = 0
     B.proj(&c->uht[0][0], &u[0][0], &du0[0][0], &du1[0][0], MXGP);
     for (int i = 0; i < B.tm; ++i) { lf_re[0][i] = 0.0; lf_im[0][i] = 0.0; }
@@ -372,15 +417,15 @@ static void element_rsdl_cd(or_ctx *c, int tind, int stage, double (*lf_re)[HP_M
         for (int j = 0; j < gpn; ++j) {
             double fluxx = ph.rhocv * (ph.ax - mv0) * u[i][j];
             double fluxy = ph.rhocv * (ph.ay - mv1) * u[i][j];
-            cv00[i][j] = +dcrd[1][1] * fluxx - dcrd[0][1] * fluxy;
-            cv01[i][j] = -dcrd[1][0] * fluxx + dcrd[0][0] * fluxy;
+            cv00[i][j] = +dc[1][1][i][j] * fluxx - dc[0][1][i][j] * fluxy;
+            cv01[i][j] = -dc[1][0][i][j] * fluxx + dc[0][0][i][j] * fluxy;
         }
     B.intgrtrs(&lf_im[0][0], &cv00[0][0], &cv01[0][0], MXGP);
     const double beta = ph.beta[stage];
     if (beta > 0.0) {
         for (int i = 0; i < gpx; ++i)
             for (int j = 0; j < gpn; ++j) {
-                cjcb[i][j] = dcrd[0][0] * dcrd[1][1] - dcrd[1][0] * dcrd[0][1];
+                cjcb[i][j] = dc[0][0][i][j] * dc[1][1][i][j] - dc[1][0][i][j] * dc[0][1][i][j];
                 res[i][j] = ph.rhocv * ph.bd0 * u[i][j] * cjcb[i][j] + 0.0;
                 res[i][j] -= cjcb[i][j] * ph.src;
             }
@@ -388,9 +433,9 @@ static void element_rsdl_cd(or_ctx *c, int tind, int stage, double (*lf_re)[HP_M
         for (int i = 0; i < gpx; ++i)
             for (int j = 0; j < gpn; ++j) {
                 cjcb[i][j] = ph.kcond / cjcb[i][j];
-                double v0000 = -cjcb[i][j] * (dcrd[1][1] * dcrd[1][1] + dcrd[0][1] * dcrd[0][1]);
-                double v0011 = -cjcb[i][j] * (dcrd[1][0] * dcrd[1][0] + dcrd[0][0] * dcrd[0][0]);
-                double v0001 = cjcb[i][j] * (dcrd[1][1] * dcrd[1][0] + dcrd[0][1] * dcrd[0][0]);
+                double v0000 = -cjcb[i][j] * (dc[1][1][i][j] * dc[1][1][i][j] + dc[0][1][i][j] * dc[0][1][i][j]);
+                double v0011 = -cjcb[i][j] * (dc[1][0][i][j] * dc[1][0][i][j] + dc[0][0][i][j] * dc[0][0][i][j]);
+                double v0001 = cjcb[i][j] * (dc[1][1][i][j] * dc[1][0][i][j] + dc[0][1][i][j] * dc[0][0][i][j]);
                 e00[i][j] = +v0000 * du0[i][j] + v0001 * du1[i][j];
                 e01[i][j] = +v0001 * du0[i][j] + v0011 * du1[i][j];
                 cv00[i][j] += e00[i][j];
@@ -401,29 +446,27 @@ static void element_rsdl_cd(or_ctx *c, int tind, int stage, double (*lf_re)[HP_M
         for (int i = 0; i < gpx; ++i)
             for (int j = 0; j < gpn; ++j) {
                 double tres = c->tau[tind * c->NV] * res[i][j];
-                e00[i][j] -= (dcrd[1][1] * (ph.ax - mv0) - dcrd[0][1] * (ph.ay - mv1)) * tres;
-                e01[i][j] -= (-dcrd[1][0] * (ph.ax - mv0) + dcrd[0][0] * (ph.ay - mv1)) * tres;
+                e00[i][j] -= (dc[1][1][i][j] * (ph.ax - mv0) - dc[0][1][i][j] * (ph.ay - mv1)) * tres;
+                e01[i][j] -= (-dc[1][0][i][j] * (ph.ax - mv0) + dc[0][0][i][j] * (ph.ay - mv1)) * tres;
             }
         B.intgrtrs(&lf_re[0][0], &e00[0][0], &e01[0][0], MXGP);
         for (int i = 0; i < B.tm; ++i) lf_re[0][i] *= beta;
     }
 }
 
-// tri_hp/ins/rsdl.cpp:17-80 + straight-element branch :259-433 (CALC_TAU2, steady)
+// tri_hp/ins/rsdl.cpp:17-80 + the curved (:83-258) and straight (:259-433) branches (CALC_TAU2,
+// steady); both are the same arithmetic on metrics per point, constant when straight
 static void element_rsdl_ins(or_ctx *c, int tind, int stage, double (*lf_re)[HP_MXTM], double (*lf_im)[HP_MXTM]) {
     const Basis &B = *c->B;
     const int NV = 3, gpx = c->gpx, gpn = c->gpn;
     const hp_phys_params &ph = c->ph;
     static PtArr crd[2], u[3], du[3][2], res[3], cv[2][2], df[2][2], mvel[2];
-    double ldcrd[2][2];
+    static PtArr dc[2][2];
     int v[3] = {c->tri_pnt[3 * tind], c->tri_pnt[3 * tind + 1], c->tri_pnt[3 * tind + 2]};
     const double rhobd0 = ph.rho * ph.bd0, lmu = ph.mu;
     for (int n = 0; n < 2; ++n)
         B.proj(c->pnts[2 * v[0] + n], c->pnts[2 * v[1] + n], c->pnts[2 * v[2] + n], &crd[n][0][0], MXGP);
-    for (int n = 0; n < 2; ++n) {
-        ldcrd[n][0] = 0.5 * (c->pnts[2 * v[2] + n] - c->pnts[2 * v[1] + n]);
-        ldcrd[n][1] = 0.5 * (c->pnts[2 * v[0] + n] - c->pnts[2 * v[1] + n]);
-    }
+    element_metrics(c, tind, dc);
     for (int i = 0; i < gpx; ++i)
         for (int j = 0; j < gpn; ++j) { mvel[0][i][j] = 0.0; mvel[1][i][j] = 0.0; }
     const double beta = ph.beta[stage];
@@ -440,42 +483,44 @@ static void element_rsdl_ins(or_ctx *c, int tind, int stage, double (*lf_re)[HP_
         for (int j = 0; j < gpn; ++j) {
             double fluxx = ph.rho * (u[0][i][j] - mvel[0][i][j]);
             double fluxy = ph.rho * (u[1][i][j] - mvel[1][i][j]);
-            du[NV - 1][0][i][j] = +ldcrd[1][1] * fluxx - ldcrd[0][1] * fluxy;
-            du[NV - 1][1][i][j] = -ldcrd[1][0] * fluxx + ldcrd[0][0] * fluxy;
+            du[NV - 1][0][i][j] = +dc[1][1][i][j] * fluxx - dc[0][1][i][j] * fluxy;
+            du[NV - 1][1][i][j] = -dc[1][0][i][j] * fluxx + dc[0][0][i][j] * fluxy;
             for (int n = 0; n < NV - 1; ++n) {
                 cv[n][0][i][j] = u[n][i][j] * du[NV - 1][0][i][j];
                 cv[n][1][i][j] = u[n][i][j] * du[NV - 1][1][i][j];
             }
-            cv[0][0][i][j] += ldcrd[1][1] * u[NV - 1][i][j];
-            cv[0][1][i][j] -= ldcrd[1][0] * u[NV - 1][i][j];
-            cv[1][0][i][j] -= ldcrd[0][1] * u[NV - 1][i][j];
-            cv[1][1][i][j] += ldcrd[0][0] * u[NV - 1][i][j];
+            cv[0][0][i][j] += dc[1][1][i][j] * u[NV - 1][i][j];
+            cv[0][1][i][j] -= dc[1][0][i][j] * u[NV - 1][i][j];
+            cv[1][0][i][j] -= dc[0][1][i][j] * u[NV - 1][i][j];
+            cv[1][1][i][j] += dc[0][0][i][j] * u[NV - 1][i][j];
         }
     for (int n = 0; n < NV - 1; ++n) B.intgrtrs(&lf_im[n][0], &cv[n][0][0][0], &cv[n][1][0][0], MXGP);
     B.intgrtrs(&lf_im[NV - 1][0], &du[NV - 1][0][0][0], &du[NV - 1][1][0][0], MXGP);
 
     if (beta > 0.0) {
-        double cjcb = ldcrd[0][0] * ldcrd[1][1] - ldcrd[1][0] * ldcrd[0][1];
-        double cjcbi = lmu / cjcb;
-        double lrhorbd0 = rhobd0 * cjcb;
-        double visc[2][2][2][2];
-        visc[0][0][0][0] = -cjcbi * (2. * ldcrd[1][1] * ldcrd[1][1] + ldcrd[0][1] * ldcrd[0][1]);
-        visc[0][0][1][1] = -cjcbi * (2. * ldcrd[1][0] * ldcrd[1][0] + ldcrd[0][0] * ldcrd[0][0]);
-        visc[0][0][0][1] = cjcbi * (2. * ldcrd[1][1] * ldcrd[1][0] + ldcrd[0][1] * ldcrd[0][0]);
-        visc[1][1][0][0] = -cjcbi * (ldcrd[1][1] * ldcrd[1][1] + 2. * ldcrd[0][1] * ldcrd[0][1]);
-        visc[1][1][1][1] = -cjcbi * (ldcrd[1][0] * ldcrd[1][0] + 2. * ldcrd[0][0] * ldcrd[0][0]);
-        visc[1][1][0][1] = cjcbi * (ldcrd[1][1] * ldcrd[1][0] + 2. * ldcrd[0][1] * ldcrd[0][0]);
-        visc[0][1][0][0] = cjcbi * ldcrd[0][1] * ldcrd[1][1];
-        visc[0][1][1][1] = cjcbi * ldcrd[0][0] * ldcrd[1][0];
-        visc[0][1][0][1] = -cjcbi * ldcrd[0][1] * ldcrd[1][0];
-        visc[0][1][1][0] = -cjcbi * ldcrd[0][0] * ldcrd[1][1];
-        const double v0010 = visc[0][0][0][1];  // viscI0II0II1II0I
-        const double v1110 = visc[1][1][0][1];  // viscI1II1II1II0I
-        const double v1000 = visc[0][1][0][0], v1011 = visc[0][1][1][1], v1001 = visc[0][1][1][0],
-                     v1010 = visc[0][1][0][1];
+        static PtArr cjcbp;
         for (int i = 0; i < gpx; ++i)
             for (int j = 0; j < gpn; ++j) {
-                double rhorbd0 = lrhorbd0;
+                const double cjcb = dc[0][0][i][j] * dc[1][1][i][j] - dc[1][0][i][j] * dc[0][1][i][j];
+                cjcbp[i][j] = cjcb;
+                const double cjcbi = lmu / cjcb;
+                double rhorbd0 = rhobd0 * cjcb;
+                double visc[2][2][2][2];
+                visc[0][0][0][0] = -cjcbi * (2. * dc[1][1][i][j] * dc[1][1][i][j] + dc[0][1][i][j] * dc[0][1][i][j]);
+                visc[0][0][1][1] = -cjcbi * (2. * dc[1][0][i][j] * dc[1][0][i][j] + dc[0][0][i][j] * dc[0][0][i][j]);
+                visc[0][0][0][1] = cjcbi * (2. * dc[1][1][i][j] * dc[1][0][i][j] + dc[0][1][i][j] * dc[0][0][i][j]);
+                visc[1][1][0][0] = -cjcbi * (dc[1][1][i][j] * dc[1][1][i][j] + 2. * dc[0][1][i][j] * dc[0][1][i][j]);
+                visc[1][1][1][1] = -cjcbi * (dc[1][0][i][j] * dc[1][0][i][j] + 2. * dc[0][0][i][j] * dc[0][0][i][j]);
+                visc[1][1][0][1] = cjcbi * (dc[1][1][i][j] * dc[1][0][i][j] + 2. * dc[0][1][i][j] * dc[0][0][i][j]);
+                visc[0][1][0][0] = cjcbi * dc[0][1][i][j] * dc[1][1][i][j];
+                visc[0][1][1][1] = cjcbi * dc[0][0][i][j] * dc[1][0][i][j];
+                visc[0][1][0][1] = -cjcbi * dc[0][1][i][j] * dc[1][0][i][j];
+                visc[0][1][1][0] = -cjcbi * dc[0][0][i][j] * dc[1][1][i][j];
+                const double v0010 = visc[0][0][0][1];  // viscI0II0II1II0I
+                const double v1110 = visc[1][1][0][1];  // viscI1II1II1II0I
+                const double v1000 = visc[0][1][0][0], v1011 = visc[0][1][1][1], v1001 = visc[0][1][1][0],
+                             v1010 = visc[0][1][0][1];
+
                 for (int n = 0; n < NV - 1; ++n) res[n][i][j] = rhorbd0 * u[n][i][j] + 0.0;
                 res[NV - 1][i][j] = rhorbd0 + 0.0;
                 df[0][0][i][j] = (+visc[0][0][0][0] * du[0][0][i][j] + visc[0][1][0][0] * du[1][0][i][j] +
@@ -506,23 +551,23 @@ static void element_rsdl_ins(or_ctx *c, int tind, int stage, double (*lf_re)[HP_
                 double rho = ph.rho, nu = ph.mu / rho;
                 double gam = 3.0 * q + (0.5 * h * ph.bd0 + 2. * nu / h) * (0.5 * h * ph.bd0 + 2. * nu / h);
                 if (ph.mu + ph.bd0 == 0.0) gam = std::max(gam, 0.1);
-                double tau0 = ph.adis * h / (cjcb * std::sqrt(gam));
+                double tau0 = ph.adis * h / (cjcbp[i][j] * std::sqrt(gam));
                 double tau2 = std::sqrt(q) * tau0;
                 c->tau[tind * 3 + 0] = tau0;
                 c->tau[tind * 3 + NV - 1] = tau2;
                 double tr0 = tau0 * res[0][i][j], tr1 = tau0 * res[1][i][j], tr2 = tau2 * res[NV - 1][i][j];
-                df[0][0][i][j] -= (ldcrd[1][1] * (2 * u[0][i][j] - mvel[0][i][j]) - ldcrd[0][1] * (u[1][i][j] - mvel[1][i][j])) * tr0 -
-                                  ldcrd[0][1] * u[0][i][j] * tr1 + ldcrd[1][1] * tr2;
-                df[0][1][i][j] -= (-ldcrd[1][0] * (2 * u[0][i][j] - mvel[0][i][j]) + ldcrd[0][0] * (u[1][i][j] - mvel[1][i][j])) * tr0 +
-                                  ldcrd[0][0] * u[0][i][j] * tr1 - ldcrd[1][0] * tr2;
-                df[1][0][i][j] -= +ldcrd[1][1] * u[1][i][j] * tr0 +
-                                  (ldcrd[1][1] * (u[0][i][j] - mvel[0][i][j]) - ldcrd[0][1] * (2. * u[1][i][j] - mvel[1][i][j])) * tr1 -
-                                  ldcrd[0][1] * tr2;
-                df[1][1][i][j] -= -ldcrd[1][0] * u[1][i][j] * tr0 +
-                                  (-ldcrd[1][0] * (u[0][i][j] - mvel[0][i][j]) + ldcrd[0][0] * (2. * u[1][i][j] - mvel[1][i][j])) * tr1 +
-                                  ldcrd[0][0] * tr2;
-                du[NV - 1][0][i][j] = -(ldcrd[1][1] * tr0 - ldcrd[0][1] * tr1);
-                du[NV - 1][1][i][j] = -(-ldcrd[1][0] * tr0 + ldcrd[0][0] * tr1);
+                df[0][0][i][j] -= (dc[1][1][i][j] * (2 * u[0][i][j] - mvel[0][i][j]) - dc[0][1][i][j] * (u[1][i][j] - mvel[1][i][j])) * tr0 -
+                                  dc[0][1][i][j] * u[0][i][j] * tr1 + dc[1][1][i][j] * tr2;
+                df[0][1][i][j] -= (-dc[1][0][i][j] * (2 * u[0][i][j] - mvel[0][i][j]) + dc[0][0][i][j] * (u[1][i][j] - mvel[1][i][j])) * tr0 +
+                                  dc[0][0][i][j] * u[0][i][j] * tr1 - dc[1][0][i][j] * tr2;
+                df[1][0][i][j] -= +dc[1][1][i][j] * u[1][i][j] * tr0 +
+                                  (dc[1][1][i][j] * (u[0][i][j] - mvel[0][i][j]) - dc[0][1][i][j] * (2. * u[1][i][j] - mvel[1][i][j])) * tr1 -
+                                  dc[0][1][i][j] * tr2;
+                df[1][1][i][j] -= -dc[1][0][i][j] * u[1][i][j] * tr0 +
+                                  (-dc[1][0][i][j] * (u[0][i][j] - mvel[0][i][j]) + dc[0][0][i][j] * (2. * u[1][i][j] - mvel[1][i][j])) * tr1 +
+                                  dc[0][0][i][j] * tr2;
+                du[NV - 1][0][i][j] = -(dc[1][1][i][j] * tr0 - dc[0][1][i][j] * tr1);
+                du[NV - 1][1][i][j] = -(-dc[1][0][i][j] * tr0 + dc[0][0][i][j] * tr1);
             }
         for (int n = 0; n < NV - 1; ++n) B.intgrtrs(&lf_re[n][0], &df[n][0][0][0], &df[n][1][0][0], MXGP);
         B.intgrtrs(&lf_re[NV - 1][0], &du[NV - 1][0][0][0], &du[NV - 1][1][0][0], MXGP);
@@ -545,10 +590,11 @@ static void bdry_rsdl(or_ctx *c) {
             u1d[n][1] = c->ugv[v1 * NV + n];
             for (int m = 0; m < sm; ++m) u1d[n][m + 2] = c->ugs[(sind * sm + m) * NV + n];
         }
-        for (int n = 0; n < 2; ++n) {
+        const bool cv = side_is_curved(c, e);
+        for (int n = 0; n < 2; ++n) {  // crdtocht1d (gtol.cpp:296-327)
             cht[n][0] = c->pnts[2 * v0 + n];
             cht[n][1] = c->pnts[2 * v1 + n];
-            for (int m = 0; m < sm; ++m) cht[n][m + 2] = 0.0;  // straight side
+            for (int m = 0; m < sm; ++m) cht[n][m + 2] = cv ? c->bcrd[((size_t)e * sm + m) * 2 + n] : 0.0;
         }
         double crd[2][HP_MXGP], dcrd[2][HP_MXGP], uu[3][HP_MXGP], dum[HP_MXGP], rr[3][HP_MXGP], lf1[3][HP_MXX];
         for (int n = 0; n < 2; ++n) B.proj1d(cht[n], crd[n], dcrd[n]);
@@ -593,6 +639,13 @@ or_ctx *or_create(const hp_mesh_desc *m, const hp_basis_tables *b, const hp_phys
     c->bkind.assign(m->bseg_kind, m->bseg_kind + m->nbseg);
     if (m->bseg_pibc) c->bpibc.assign(m->bseg_pibc, m->bseg_pibc + m->nbseg * b->gpx);
     else c->bpibc.assign(m->nbseg * b->gpx, 0.0);
+    c->seg_bdry.assign(m->nseg, -1);
+    for (int e = 0; e < m->nbseg; ++e) c->seg_bdry[m->bseg[e]] = e;
+    if (m->bseg_crd && b->sm > 0) c->bcrd.assign(m->bseg_crd, m->bseg_crd + (size_t)m->nbseg * b->sm * 2);
+    // tri_hp::metric::setinfo (metric.cpp:44-70): owners of curved boundary sides, p > 1
+    c->curved.assign(m->ntri, 0);
+    for (int e = 0; e < m->nbseg; ++e)
+        if (side_is_curved(c, e)) c->curved[m->seg_tri[2 * m->bseg[e]]] = 1;
     c->vess.assign(m->npnt, 0);
     c->sess.assign(m->nseg, 0);
     for (int e = 0; e < m->nbseg; ++e) {
@@ -716,9 +769,32 @@ int or_setup_preconditioner(or_ctx *c) {
                     double q = std::pow(u[0][i][j] - 0.5 * 0.0, 2.0) + std::pow(u[1][i][j] - 0.5 * 0.0, 2.0);
                     qmax = std::max(qmax, q);
                 }
-            hmax = std::sqrt(hmax);
-            h = 4. * jcb / (p1 * hmax);
-            hmax = hmax / p1;
+            if (c->curved[tind]) {
+                // curved element (ins/setup_preconditioner.cpp:45-87)
+                static PtArr dc[2][2];
+                element_metrics(c, tind, dc);
+                double jcbmin = jcb, hm = 0.0;
+                for (int i = 0; i < c->gpx; ++i)
+                    for (int j = 0; j < c->gpn; ++j) {
+                        jcbmin = std::min(jcbmin, dc[0][0][i][j] * dc[1][1][i][j] - dc[1][0][i][j] * dc[0][1][i][j]);
+                        double hh = 0.0;
+                        for (int n = 0; n < 2; ++n) hh += dc[n][0][i][j] * dc[n][0][i][j];
+                        hm = std::max(hh, hm);
+                        hh = 0.0;
+                        for (int n = 0; n < 2; ++n) hh += dc[n][1][i][j] * dc[n][1][i][j];
+                        hm = std::max(hh, hm);
+                        hh = 0.0;
+                        for (int n = 0; n < 2; ++n) hh += (dc[n][1][i][j] - dc[n][0][i][j]) * (dc[n][1][i][j] - dc[n][0][i][j]);
+                        hm = std::max(hh, hm);
+                    }
+                hmax = 2. * std::sqrt(hm);
+                h = 4. * jcbmin / (p1 * hmax);
+                hmax = hmax / p1;
+            } else {
+                hmax = std::sqrt(hmax);
+                h = 4. * jcb / (p1 * hmax);
+                hmax = hmax / p1;
+            }
             if (!(h > 0.0)) { err = 1; break; }
             if (std::isnan(qmax)) { err = 1; break; }
             double nu = ph.mu / ph.rho;

@@ -73,6 +73,7 @@ def ref():
         r.ref_intgrtrs.argtypes = [ctypes.c_int, P, P, P, ctypes.c_int]
         r.ref_proj1d.argtypes = [ctypes.c_int, P, P, P]
         r.ref_intgrt1d.argtypes = [ctypes.c_int, P, P]
+        r.ref_proj_bdry.argtypes = [ctypes.c_int, P, P, P, P, ctypes.c_int]
         _r = r
     return _r
 

@@ -231,3 +231,73 @@ def test_abi_exports_every_declared_symbol():
     lib = L.lib()
     missing = [n for n in sorted(names) if not hasattr(lib, n)]
     assert not missing, missing
+
+
+@needs_ref
+@pytest.mark.parametrize("p", [2, 3, 4, 6, 8])
+def test_curved_metrics_projection_matches_reference_proj_bdry(p):
+    """The curved-element metrics project the vertex and side position modes (interior
+    modes zero) with derivatives: the oracle's projection of such a vector equals the
+    reference's own tri_basis::proj_bdry (tri_basis/proj.cpp:201-281)."""
+    r = O.ref()
+    o = O.lib()
+    t = hpb.basis_tables(p)
+    G, T, S = p + 1, (p + 1) * (p + 2) // 2, 9
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    lin = _rand(T, 31 + p)
+    lin[3 * p:] = 0.0
+    f1, dx1, dy1 = (np.zeros((G, S)) for _ in range(3))
+    f2, dx2, dy2 = (np.zeros((G, S)) for _ in range(3))
+    o.or_basis_proj(ctypes.addressof(t), P(lin), P(f1), P(dx1), P(dy1), S)
+    r.ref_proj_bdry(p, P(lin), P(f2), P(dx2), P(dy2), S)
+    for a, b in ((f1, f2), (dx1, dx2), (dy1, dy2)):
+        assert np.max(np.abs(a - b)) <= 1e-13 * max(1.0, np.max(np.abs(b)))
+
+
+@pytest.mark.parametrize("p", [2, 4, 6])
+def test_curved_side_modes(p):
+    """hp_curved_side_modes (hp_edge_bdry::curv_init): a boundary that is a polynomial of
+    degree <= p along the side is reproduced exactly at the side's Gauss points; a circle
+    is approximated to O(h^(p+1))."""
+    from hpb import _lib as L
+    t = hpb.basis_tables(p)
+    G, sm = p + 1, p - 1
+    gx = np.array([[t.gx[k][n] for n in range(t.nmodx)] for k in range(G)])
+    x0, x1 = np.array([0.2, 0.1]), np.array([0.9, 0.4])
+    xp = np.array([t.xp[k] for k in range(G)])
+    chord = np.outer(gx[:, 1], x0) + np.outer(gx[:, 2], x1)
+    nrm = np.array([-(x1 - x0)[1], (x1 - x0)[0]])
+    curve = chord + np.outer(0.3 * (1 - xp ** 2) * (1 + 0.5 * xp), nrm)  # cubic bump, zero at the ends
+    ends = np.ascontiguousarray(np.concatenate([x0, x1])[None])
+    modes = np.zeros((1, sm, 2))
+    L.check(L.lib().hp_curved_side_modes(ctypes.byref(t), 1, L.ptr(ends), L.ptr(np.ascontiguousarray(curve[None])),
+                                         L.ptr(modes)), "curved modes")
+    rec = chord + gx[:, 3:3 + sm] @ modes[0]
+    if p >= 3:
+        assert np.max(np.abs(rec - curve)) < 1e-13
+    # circle of radius 1: a side spanning 0.2 rad
+    th0, th1 = 0.3, 0.5
+    c0, c1 = np.array([np.cos(th0), np.sin(th0)]), np.array([np.cos(th1), np.sin(th1)])
+    chord = np.outer(gx[:, 1], c0) + np.outer(gx[:, 2], c1)
+    onc = chord / np.linalg.norm(chord, axis=1)[:, None]
+    ends = np.ascontiguousarray(np.concatenate([c0, c1])[None])
+    L.check(L.lib().hp_curved_side_modes(ctypes.byref(t), 1, L.ptr(ends), L.ptr(np.ascontiguousarray(onc[None])),
+                                         L.ptr(modes)), "curved modes")
+    rec = chord + gx[:, 3:3 + sm] @ modes[0]
+    assert np.max(np.abs(np.linalg.norm(rec, axis=1) - 1.0)) < 0.2 ** (p + 1)
+
+
+def test_channel_hole_mesh():
+    """The graded channel-with-hole mesh: hole points on the circle, all triangles
+    counter-clockwise and outside the hole, and its area equals the channel minus the
+    inscribed polygon of the hole."""
+    m = hpb.channel_hole(L=4.0, H=2.0, cx=1.0, cy=1.0, r=0.25, hmin=0.08, hmax=0.3, grade=0.2)
+    assert np.all(m.area2() > 0)
+    bs = m.boundary_segments()
+    mid = 0.5 * (m.pnts[m.seg_pnt[bs, 0]] + m.pnts[m.seg_pnt[bs, 1]])
+    hole = np.hypot(mid[:, 0] - 1.0, mid[:, 1] - 1.0) < 0.25 + 1e-9
+    ends = m.pnts[m.seg_pnt[bs[hole]].ravel()]
+    assert np.max(np.abs(np.hypot(ends[:, 0] - 1.0, ends[:, 1] - 1.0) - 0.25)) < 1e-12
+    k = hole.sum()
+    poly = 0.5 * k * 0.25 ** 2 * np.sin(2 * np.pi / k)
+    assert abs(0.5 * np.sum(m.area2()) - (8.0 - poly)) < 1e-9
