@@ -178,6 +178,69 @@ def c3_sweep(hpb, dev, n, p, cycles):
     print(json.dumps(line), flush=True)
 
 
+def c4_sweep(hpb, dev, scale, cycles):
+    """ins past a cylinder: channel [0,20] x [0,10], hole of diameter 1 at (5, 5) with
+    curved (isoparametric) sides, graded Delaunay mesh channel_hole scaled by `scale`
+    (1: ~150k triangles), p = 4, free stream in, outflow p = 0 out, no-slip hole. The
+    learned correction is trained on the GPU on solver-generated samples of 4 training
+    instances with Re drawn from U[20, 200] (snapshot states after 0, 200, 1000 and 3000
+    plain updates, every element of every snapshot one sample) and judged on 2 held-out
+    Re by the FP64 residual after `cycles` V-cycles (p 4 -> 2 -> 1, then channel meshes at
+    2x, 4x, 8x the edge lengths at p = 1; preconditioners every cycle): plain FP64, FP32
+    defect correction, and FP32 defect correction with the learned correction."""
+    import time as _t
+    import numpy as np
+    from hpb import learned as LR
+    from hpb import multigrid as MG
+    meshes = {k: hpb.channel_hole(hmin=0.02 * scale * k, hmax=0.2 * scale * k, grade=0.0085 * scale * k)
+              for k in (1, 2, 4, 8)}
+    rng = np.random.default_rng(20261208)
+    train_re = rng.uniform(20.0, 200.0, 4)
+    test_re = rng.uniform(20.0, 200.0, 2)
+    t0 = _t.perf_counter()
+    F, T = [], []
+    for k, re in enumerate(train_re):
+        f, tg = LR.solver_samples(lambda: hpb.channel_cylinder_ins(mesh=meshes[1], p=4, re=float(re), seed=400 + k),
+                                  snapshots=(0, 200, 1000, 3000))
+        F.append(f)
+        T.append(tg)
+    F, T = np.concatenate(F), np.concatenate(T)
+    net, hist = LR.train(F, T, steps=600)
+    train_s = _t.perf_counter() - t0
+    line = {"sweep": "c4", "workload": f"ins cylinder in a channel, p=4, curved hole, {meshes[1].ntri} triangles",
+            "train_re": [float(x) for x in train_re], "test_re": [float(x) for x in test_re],
+            "samples": int(len(T)), "snapshots": 16, "nonzero_targets": float(np.mean(T != 0)),
+            "training_seconds": train_s, "loss_first_last": [float(hist[0]), float(hist[-1])], "cycles": cycles,
+            "levels": [f"{meshes[k].ntri} tri" for k in (1, 2, 4, 8)]}
+
+    def hierarchy(re):
+        probs = [hpb.channel_cylinder_ins(mesh=meshes[1], p=4, re=re, seed=900)]
+        kinds = ["fine"]
+        for q in (2, 1):
+            probs.append(hpb.channel_cylinder_ins(mesh=meshes[1], p=q, re=re, seed=900))
+            kinds.append("p")
+        for k in (2, 4, 8):
+            probs.append(hpb.channel_cylinder_ins(mesh=meshes[k], p=1, re=re, seed=900))
+            kinds.append("h")
+        return MG.Hierarchy(probs, kinds)
+
+    for re in test_re:
+        res = {}
+        for name, mixed, learned in (("fp64", False, False), ("fp32_defect_correction", True, False),
+                                     ("learned_fp32", True, True)):
+            H = hierarchy(float(re))
+            if learned:
+                LR.attach(H.levels[0], net, 1.0)
+            h, sec, cyc = H.solve(drop=1e-10, max_cycles=cycles, mixed=mixed, prcn_every=1)
+            res[name] = {"seconds": sec, "cycles": cyc, "drop": float(h[-1]),
+                         "min_drop": float(np.min(h)), "drop_history": [float(x) for x in h[::max(1, cycles // 10)]]}
+            H.close()
+        line[f"re_{re:.1f}"] = res
+        print(json.dumps({"re": float(re), **{k: (v["drop"], v["seconds"]) for k, v in res.items()}}), flush=True)
+    net.close()
+    print(json.dumps(line), flush=True)
+
+
 def timed_factory(torch, flush):
     def timed(fn, n, stream):
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
@@ -381,11 +444,15 @@ def main():
                     help="with --quick / --profile: the matrix-free element kernel instead of stored operators")
     ap.add_argument("--profile", choices=["update64", "update32"], default=None,
                     help="run `steps` multistage updates of the workload in FP64 or FP32 (for profiler runs)")
-    ap.add_argument("--sweep", choices=["c2", "c3"], default=None,
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="with --sweep c4: edge-length scale of the channel mesh (1: ~150k triangles)")
+    ap.add_argument("--sweep", choices=["c2", "c3", "c4"], default=None,
                     help="c2: cd on the seeded 200k-triangle Delaunay mesh, p = 2, 4, 6, 8: rsdl GDoF/s and time "
                          "to a 1e-10 drop, plain FP64 vs FP32 defect correction (one JSON line per p); "
                          "c3: ins lid-driven cavity Re 400, p = 6, 512x512 split squares, V-cycles for --steps "
-                         "cycles: level by level, one CUDA graph, autotuned graph, FP32 defect correction")
+                         "cycles: level by level, one CUDA graph, autotuned graph, FP32 defect correction; "
+                         "c4: ins past a cylinder in a channel (curved hole, graded ~150k triangles), learned "
+                         "preconditioner trained on Re in [20, 200], judged on held-out Re by the FP64 residual")
     ap.add_argument("--p", type=int, nargs="*", default=None, help="with --sweep: the p values")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -427,6 +494,9 @@ def main():
     if args.sweep == "c2":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         c2_sweep(hpb, dev, args.mesh, args.p or [2, 4, 6, 8], args.steps, timed_factory(torch, flush))
+        return
+    if args.sweep == "c4":
+        c4_sweep(hpb, dev, args.scale, args.steps)
         return
     if args.sweep == "c3":
         c3_sweep(hpb, dev, args.mesh if args.mesh != N_MESH else 512, (args.p or [6])[0], args.steps)

@@ -113,6 +113,7 @@ def elem_features(level):
     lib = _bind()
     m = level.prob.mesh
     d = torch.empty((m.ntri, 17), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()  # the buffer is written on the context's own stream
     L.check(lib.hp_gpu_elem_features(level.h, P(d.data_ptr())), "elem_features")
     L.check(lib.hp_gpu_sync(level.h), "sync")
     return d.cpu().numpy()
@@ -125,39 +126,56 @@ def elem_resnorm(level):
     m = level.prob.mesh
     level.rsdl(level.prob.phys.nstage)
     d = torch.empty(m.ntri, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()  # the buffer is written on the context's own stream
     L.check(lib.hp_gpu_elem_resnorm(level.h, P(d.data_ptr())), "elem_resnorm")
     L.check(lib.hp_gpu_sync(level.h), "sync")
     return d.cpu().numpy()
 
 
-def solver_samples(prob_factory, scales=(-1.0, -0.6, -0.3, 0.0, 0.3), k_updates=8, margin=0.02):
-    """(features, targets) from one problem instance, generated by the solver."""
+def solver_samples(prob_factory, scales=(-1.0, -0.6, -0.3, 0.0, 0.3), k_updates=8, margin=0.02, snapshots=(0,)):
+    """(features, targets) from one problem instance, generated by the solver. With
+    `snapshots` (cumulative plain-update counts), the instance is first smoothed by the
+    plain method to each snapshot and every snapshot state gives one sample per element,
+    so the network also sees the states later in a solve."""
     import torch
     lib = _bind()
     pr = prob_factory()
     g = pr.gpu()
-    init = (pr.ugv.copy(), pr.ugs.copy(), pr.ugi.copy())
-    feats = elem_features(g)
+    state = (pr.ugv.copy(), pr.ugs.copy(), pr.ugi.copy())
     ntri = pr.mesh.ntri
-    ratios = []
-    for c in scales:
-        g.upload(*init)
-        sc = torch.full((ntri, 1), float(c), dtype=torch.float32, device="cuda")
-        L.check(lib.hp_gpu_set_prcn_scale(g.h, P(sc.data_ptr()), 1, 1.5), "set_prcn_scale")
-        assert g.setup_preconditioner() == 0
-        r0 = elem_resnorm(g)
-        g.iterate(k_updates, prcn_interval=0)
-        rk = elem_resnorm(g)
-        ratios.append(np.sqrt(rk / np.maximum(r0, 1e-300)))
-        L.check(lib.hp_gpu_set_prcn_scale(g.h, None, 1, 0.0), "set_prcn_scale")
-        del sc
+    F, Tg = [], []
+    done = 0
+    for snap in sorted(snapshots):
+        if snap > done:
+            g.upload(*state)
+            assert g.setup_preconditioner() == 0
+            g.iterate(snap - done, prcn_interval=0)
+            state = g.state()
+            done = snap
+        g.upload(*state)
+        feats = elem_features(g)
+        ratios = []
+        for c in scales:
+            g.upload(*state)
+            sc = torch.full((ntri, 1), float(c), dtype=torch.float32, device="cuda")
+            torch.cuda.synchronize()  # the context reads it on its own stream
+            L.check(lib.hp_gpu_set_prcn_scale(g.h, P(sc.data_ptr()), 1, 1.5), "set_prcn_scale")
+            assert g.setup_preconditioner() == 0
+            r0 = elem_resnorm(g)
+            g.iterate(k_updates, prcn_interval=0)
+            rk = elem_resnorm(g)
+            ratios.append(np.sqrt(rk / np.maximum(r0, 1e-300)))
+            L.check(lib.hp_gpu_set_prcn_scale(g.h, None, 1, 0.0), "set_prcn_scale")
+            del sc
+        R = np.array(ratios)  # [nscales][ntri]
+        base = R[list(scales).index(0.0)]
+        best = np.argmin(R, axis=0)
+        tgt = np.array(scales)[best]
+        tgt[(R[best, np.arange(ntri)] > (1.0 - margin) * base) | ~np.isfinite(R).all(axis=0)] = 0.0
+        F.append(feats)
+        Tg.append(tgt.astype(np.float32))
     g.close()
-    R = np.array(ratios)  # [nscales][ntri]
-    base = R[list(scales).index(0.0)]
-    best = np.argmin(R, axis=0)
-    tgt = np.array(scales)[best]
-    tgt[(R[best, np.arange(ntri)] > (1.0 - margin) * base) | ~np.isfinite(R).all(axis=0)] = 0.0
-    return feats, tgt.astype(np.float32)
+    return np.concatenate(F), np.concatenate(Tg)
 
 
 def train(feats, targets, widths=(17, 64, 64, 64, 1), steps=400, batch=4096, lr=2e-3, seed=1, log=None):
