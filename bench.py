@@ -440,6 +440,9 @@ def main():
                     help="split-square mesh size n (2 n^2 triangles); smaller cases are for profiler runs")
     ap.add_argument("--quick", action="store_true",
                     help="device-timed rsdl steps only (no e2e, update or CPU legs); for profiler runs")
+    ap.add_argument("--physics", choices=["cd", "ins"], default="cd",
+                    help="with --quick / --profile: ins runs the Kovasznay workload (Re 100, p = 4) on the "
+                         "--mesh split-square mesh with the matrix-free ins element kernel")
     ap.add_argument("--matrix-free", action="store_true",
                     help="with --quick / --profile: the matrix-free element kernel instead of stored operators")
     ap.add_argument("--profile", choices=["update64", "update32"], default=None,
@@ -502,7 +505,12 @@ def main():
         c3_sweep(hpb, dev, args.mesh if args.mesh != N_MESH else 512, (args.p or [6])[0], args.steps)
         return
 
-    pr = hpb.cd_sinsin(n=args.mesh, p=P, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205)
+    if args.physics == "ins":
+        if not (args.quick or args.profile):
+            raise SystemExit("--physics ins is for --quick / --profile runs")
+        pr = hpb.kovasznay_ins(n=args.mesh, p=P, re=100.0)
+    else:
+        pr = hpb.cd_sinsin(n=args.mesh, p=P, ax=1.0, ay=0.5, kcond=1e-3, noise=1e-3, seed=20261205)
     lvl = hpb.GPULevel(pr, device=dev, stream=ctypes.c_void_p(stream.cuda_stream))
     lib = lvl.lib
     rc = lvl.setup_preconditioner()
@@ -531,7 +539,7 @@ def main():
         check(lib.hp_gpu_enqueue_update(lvl.h), "update")
 
     if args.profile or args.quick:
-        if not args.matrix_free:
+        if not args.matrix_free and args.physics == "cd":
             lvl.element_matrices(True)
         if args.profile:
             for k in range(args.warmup + args.steps):
@@ -545,7 +553,7 @@ def main():
             for _ in range(max(3, args.warmup)):
                 rsdl()
             ms = timed(rsdl, args.steps)
-            print(json.dumps({"quick": True, "matrix_free": args.matrix_free, "ntri": pr.mesh.ntri,
+            print(json.dumps({"quick": True, "matrix_free": args.matrix_free or args.physics == "ins", "ntri": pr.mesh.ntri,
                               "ms_per_step": sum(ms) / args.steps,
                               "value": pr.ndof * args.steps / (sum(ms) * 1e-3) / 1e9}))
         lvl.close()
