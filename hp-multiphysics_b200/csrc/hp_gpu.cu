@@ -208,10 +208,19 @@ struct LaunchImpl {
             k_bdry_flux_ins<R, P><<<nblk(m.nbseg, 128), 128, 0, st>>>(reinterpret_cast<const DevTables<R, P> *>(tab), m,
                                                                        s, ph, diff);
     }
+    template <int MODE>
+    static void side_mode(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, int im, int mode, double cfla,
+                          int upd, int fold, int th, cudaStream_t st) {
+        if constexpr (MODE < SM) {
+            if (mode == MODE)
+                k_minv_side<R, NV, SM, MODE><<<nblk(m.nseg, th), th, 0, st>>>(m, s, mt, im, (R)cfla, upd, fold);
+            else
+                side_mode<MODE + 1>(m, s, mt, im, mode, cfla, upd, fold, th, st);
+        }
+    }
     static void side(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, int im, int mode, double cfla, int upd,
                      int fold, int th, cudaStream_t st) {
-        if constexpr (SM > 0)
-            k_minv_side<R, NV, SM><<<nblk(m.nseg, th), th, 0, st>>>(m, s, mt, im, mode, (R)cfla, upd, fold);
+        if constexpr (SM > 0) side_mode<0>(m, s, mt, im, mode, cfla, upd, fold, th, st);
     }
     static void intr(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, double cfla, int upd, int th,
                      cudaStream_t st) {

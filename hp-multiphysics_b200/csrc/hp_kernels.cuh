@@ -835,9 +835,12 @@ __global__ void k_minv_vert(Mesh mesh, State<R> st, const DevMinv<R> *__restrict
 // interior and vertex parts; mode > 0 removes the finished mode-1 of the three
 // sides of each adjacent element. Then mode `mode` is finished: preconditioner,
 // sdiag, Dirichlet zeroing, update of ug.s.
-template <typename R, int NV, int SM>
-__global__ void k_minv_side(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, int im, int mode, R cflalpha,
+// The side mode is a template parameter so that every index into r is a compile-time
+// constant and r stays in registers.
+template <typename R, int NV, int SM, int MODE>
+__global__ void k_minv_side(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, int im, R cflalpha,
                             int do_update, int fold) {
+    constexpr int mode = MODE;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= mesh.nseg) return;
     R r[SM][NV];
@@ -880,19 +883,22 @@ __global__ void k_minv_side(Mesh mesh, State<R> st, const DevMinv<R> *__restrict
         } else {
             // removal of mode-1 from higher modes (setup_preconditioner.cpp:264-284)
             const int pm = mode - 1;
-            R uh[3][NV];
+            R uh[3][NV];  // uh[j]: mode pm of the triangle's side (i + j) % 3
+#pragma unroll
             for (int j = 0; j < 3; ++j) {
-                const int sj = mesh.tri_seg[3 * t + j];
-                const int sgj = mesh.tri_sgn[3 * t + j];
+                const int sidx = (i + j) % 3;
+                const int sj = mesh.tri_seg[3 * t + sidx];
+                const int sgj = mesh.tri_sgn[3 * t + sidx];
                 const R sg = ((pm & 1) && sgj < 0) ? (R)-1 : (R)1;
                 for (int n = 0; n < NV; ++n) uh[j][n] = sg * st.ress[(sj * SM + pm) * NV + n] * st.tprcn[t * NV + n];
             }
             R msgn = (((pm + 1) & 1) && sgn_i < 0) ? (R)-1 : (R)1;
+#pragma unroll
             for (int m = mode; m < SM; ++m) {
+#pragma unroll
                 for (int j = 0; j < 3; ++j) {
-                    const int indx = (i + j) % 3;
                     const R f = msgn * mt->sfms[pm][m][j];
-                    for (int n = 0; n < NV; ++n) r[m][n] -= f * uh[indx][n];
+                    for (int n = 0; n < NV; ++n) r[m][n] -= f * uh[j][n];
                 }
                 if (sgn_i < 0) msgn = -msgn;
             }
