@@ -139,6 +139,23 @@ struct EmatCfg {
     static size_t len(long ntri) { return (size_t)((ntri + EB - 1) / EB) * TS; }
 };
 
+// Column of mode m in the sum factorisation (proj.cpp:46-95, intgrt.cpp:44-76): vertex
+// modes 0, 1, 2 own columns 0, 1, 2; side-0 modes own columns 3 .. sm+2; side-1 modes
+// join column 2, side-2 modes column 1; interior blocks of sm-1, sm-2, ... modes join
+// columns 3, 4, .... A compile-time function of p, so unrolled loops index registers.
+template <int P>
+struct ModeCols {
+    static constexpr int SM = P - 1, BM = 3 * P, BS1 = SM + 3, BS2 = 2 * SM + 3;
+    __host__ __device__ static constexpr int col(int m) {
+        if (m < BS1) return m;
+        if (m < BS2) return 2;
+        if (m < BM) return 1;
+        int idx = m - BM, c = 3, cnt = SM - 1;
+        while (idx >= cnt) { idx -= cnt; --cnt; ++c; }
+        return c;
+    }
+};
+
 // Isoparametric metrics of a curved element at quadrature point (i, j): the r and s
 // derivatives of x and y from the element's vertex and side position modes (interior
 // modes zero), dcrd(n,0) = d x_n / dr and dcrd(n,1) = d x_n / ds (proj_bdry with
@@ -275,18 +292,22 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
             constexpr int NDV = (PHYS == 1 ? 2 : 1);  // variables projected with derivatives
             constexpr int NQW = 2 * NDV + (NV - NDV);
             const int nqw = NQW + ((PHYS == 1 && diff) ? 2 : 0);  // + base u, v values
-            for (int w = lane; w < nqw * G * X; w += 32) {
-                const int q = w / (G * X), r = w - q * (G * X), j = r / X, n = r - j * X;
+            // one lane per (quantity, eta point): all X column sums in registers, modes in
+            // increasing order within each column (the order of the column lists)
+            for (int w = lane; w < nqw * G; w += 32) {
+                const int q = w / G, j = w - q * G;
                 int var, der;
                 if (q < 2 * NDV) { var = q >> 1; der = q & 1; }
                 else { var = NDV + (q - 2 * NDV); der = 0; }
                 const R *lin = uht + var * T;
-                R acc = 0;
-                for (int c = tb.colstart[n]; c < tb.colstart[n + 1]; ++c) {
-                    const int m = tb.colmodes[c];
-                    acc += lin[m] * (der ? tb.dgn[j][m] : tb.gn[j][m]);
-                }
-                wk[(q * G + j) * X + n] = acc;
+                const R *g = der ? &tb.dgn[j][0] : &tb.gn[j][0];
+                R acc[X];
+#pragma unroll
+                for (int n = 0; n < X; ++n) acc[n] = (R)0;
+#pragma unroll
+                for (int m = 0; m < T; ++m) acc[ModeCols<P>::col(m)] += lin[m] * g[m];
+#pragma unroll
+                for (int n = 0; n < X; ++n) wk[(q * G + j) * X + n] = acc[n];
             }
         }
         __syncwarp();
