@@ -182,7 +182,7 @@ struct LaunchImpl {
     static void emat_launch(ElemMat<R> em, const Mesh &m, const State<R> &s, const Phys &ph, int stage, int zero_rr,
                             int nsm, const Tune &tn, cudaStream_t st) {
         using E = EmatCfg<P>;
-        constexpr int TH = RE ? E::THREADS_RE : E::THREADS_IM;
+        constexpr int TH = EmatShape<R, P, RE>::THREADS;
         const long ntiles = ((long)m.ntri + E::EB - 1) / E::EB;
         const int tpp = tn.emat_tpp == 2 ? 2 : 1;
         const int maxc = std::max(1, 2048 / TH / tpp);

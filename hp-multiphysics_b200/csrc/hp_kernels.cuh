@@ -131,8 +131,6 @@ struct EmatCfg {
     static constexpr int T = (P + 1) * (P + 2) / 2;
     static constexpr int EB = (128 / T > 0 ? 128 / T : 1);            // elements per tile
     static constexpr int TS = ((T * EB * T + 3) / 4) * 4;             // tile stride (entries)
-    static constexpr int THREADS_RE = ((2 * EB * T + 31) / 32) * 32;  // beta > 0: A_im and A_re rows
-    static constexpr int THREADS_IM = ((EB * T + 31) / 32) * 32;      // beta = 0: A_im rows only
     __host__ __device__ static size_t idx(long t, int j, int m) {
         return (size_t)(t / EB) * TS + (size_t)j * (EB * T) + (size_t)(t % EB) * T + m;
     }
@@ -594,15 +592,30 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
 // operator stream instead of separating it. TPP tiles (consecutive, one contiguous
 // operator run) go through each phase together: TPP rows and slots per thread, more
 // loads in flight per barrier, at more registers per thread (a per-level tuning choice).
+// Threads of one CTA: at p <= 2 FP32 threads own two adjacent operator rows (one 8-byte
+// load per column, so each request moves as many bytes as an FP64 row's; 9% faster FP32
+// updates at p = 2), otherwise one row (at p = 4 and 6 the paired rows measured 3% and 11%
+// slower: fewer threads to hide the gather latency, and spills at p = 6); at least one
+// thread per (element, mode) slot of the tile.
+template <typename R, int P, bool RE>
+struct EmatShape {
+    static constexpr int VW = (sizeof(R) == 4 && P <= 2) ? 2 : 1;
+    static constexpr int SLOTS = EmatCfg<P>::EB * EmatCfg<P>::T;
+    static constexpr int ROWS = (RE ? 2 : 1) * SLOTS;
+    static constexpr int RT = ROWS / VW;  // row groups
+    static constexpr int THREADS = (((RT > SLOTS ? RT : SLOTS) + 31) / 32) * 32;
+};
+
 template <typename R, int P, bool RE, int TPP>
-__global__ void __launch_bounds__(RE ? EmatCfg<P>::THREADS_RE : EmatCfg<P>::THREADS_IM,
-                                  2048 / (RE ? EmatCfg<P>::THREADS_RE : EmatCfg<P>::THREADS_IM) / TPP)
+__global__ void __launch_bounds__(EmatShape<R, P, RE>::THREADS, 2048 / EmatShape<R, P, RE>::THREADS / TPP)
     k_rsdl_emat(ElemMat<R> em, Mesh mesh, State<R> st, Phys ph, int stage, int zero_rr) {
     using E = EmatCfg<P>;
+    using S = EmatShape<R, P, RE>;
     constexpr int T = E::T, EB = E::EB, TS = E::TS, BM = 3 * P, IM = (P - 1) * (P - 2) / 2;
     constexpr int SM = (P > 1 ? P - 1 : 1);  // side-mode stride (unused when p = 1)
     constexpr int NH = RE ? 2 : 1;
-    constexpr int ROWS = NH * EB * T, SLOTS = EB * T;
+    constexpr int ROWS = NH * EB * T, SLOTS = EB * T, VW = S::VW, RT = S::RT;
+    static_assert(SLOTS % 2 == 0, "row pairs must not straddle the A_im / A_re halves");
     __shared__ R su[2][TPP * SLOTS];
     __shared__ R sr[2][TPP * ROWS];
     const R beta = (R)ph.beta[stage];
@@ -611,7 +624,7 @@ __global__ void __launch_bounds__(RE ? EmatCfg<P>::THREADS_RE : EmatCfg<P>::THRE
     const long ntiles = ((long)mesh.ntri + EB - 1) / EB;
     const long step = gridDim.x;
     const int w = threadIdx.x;
-    const int hr = w / SLOTS, qr = w - hr * SLOTS, er = qr / T;  // operator row (w < ROWS)
+    const int r0 = w * VW, hr = r0 / SLOTS, qr = r0 - hr * SLOTS, er = qr / T;  // first operator row (w < RT)
     const int es = w / T, ms = w - es * T;                       // gather / scatter slot (w < SLOTS)
     auto gather = [&](long tile) -> R {
         const long t = tile * EB + es;
@@ -630,17 +643,42 @@ __global__ void __launch_bounds__(RE ? EmatCfg<P>::THREADS_RE : EmatCfg<P>::THRE
         return val;
     };
     auto matvec = [&](long tile, const R *u_s, R *r_s) {
-        if (w >= ROWS || tile * EB + er >= mesh.ntri) return;
+        if (w >= RT || tile * EB + er >= mesh.ntri) return;
         const R *a = (hr ? em.are : em.aim) + (size_t)tile * TS + qr;
-        const R *u = u_s + er * T;
-        R acc = (R)0;
+        if constexpr (VW == 1) {
+            const R *u = u_s + er * T;
+            R acc = (R)0;
 #pragma unroll
-        for (int j = 0; j < T; ++j) acc = fma(__ldg(a + (size_t)j * SLOTS), u[j], acc);
-        if (hr) {
-            if (src) acc += __ldg(em.bre + (size_t)tile * EB * T + qr);
-            acc *= beta;
+            for (int j = 0; j < T; ++j) acc = fma(__ldg(a + (size_t)j * SLOTS), u[j], acc);
+            if (hr) {
+                if (src) acc += __ldg(em.bre + (size_t)tile * EB * T + qr);
+                acc *= beta;
+            }
+            r_s[w] = acc;
+        } else {
+            // rows qr, qr+1 of every column: one aligned 8-byte load (tile stride and
+            // column length are even); the two rows may belong to consecutive elements
+            const float2 *a2 = reinterpret_cast<const float2 *>(a);
+            const R *u0 = u_s + er * T, *u1 = u_s + ((qr + 1) / T) * T;
+            R acc0 = (R)0, acc1 = (R)0;
+#pragma unroll
+            for (int j = 0; j < T; ++j) {
+                const float2 x = __ldg(a2 + (size_t)j * (SLOTS / 2));
+                acc0 = fmaf(x.x, u0[j], acc0);
+                acc1 = fmaf(x.y, u1[j], acc1);
+            }
+            const bool row1 = tile * EB + (qr + 1) / T < mesh.ntri;  // b_re holds ntri * T entries
+            if (hr) {
+                if (src) {
+                    acc0 += __ldg(em.bre + (size_t)tile * EB * T + qr);
+                    if (row1) acc1 += __ldg(em.bre + (size_t)tile * EB * T + qr + 1);
+                }
+                acc0 *= beta;
+                acc1 *= beta;
+            }
+            r_s[r0] = acc0;
+            if (row1) r_s[r0 + 1] = acc1;
         }
-        r_s[w] = acc;
     };
     auto scatter = [&](long tile, const R *r_s) {
         if (w >= SLOTS) return;

@@ -50,6 +50,25 @@ def test_rsdl_minvrt_from_element_operators(p):
     assert relerr(g.residual(), o.residual()) < tol1(p), "minvrt"
 
 
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_fp32_updates_from_element_operators_match_matrix_free(p):
+    """The FP32 operator copy (paired 8-byte row loads at p <= 2; at p = 1 a pair can
+    span two elements) against the FP32 matrix-free kernels, on a mesh whose last
+    tile is partial; both start from fp32(u), so they differ by FP32 rounding only."""
+    pr = hpb.cd_sinsin(n=7, p=p, kcond=1e-2, cfl=0.5, src=0.7)
+    a, b = pr.gpu(), pr.gpu()
+    b.element_matrices(True)
+    for g in (a, b):
+        assert g.setup_preconditioner() == 0
+    u0 = a.state()
+    for g in (a, b):
+        L.check(g.lib.hp_gpu_fp32_updates(g.h, 3))
+    ua, ub = a.state(), b.state()
+    moved, diff = relerr(ua, u0), relerr(ub, ua)
+    assert moved > 1e-3
+    assert diff < 1e-5  # measured 6e-8 (p = 1) to 2.1e-6 (p = 8)
+
+
 def test_update_iterations_from_element_operators():
     pr = hpb.cd_sinsin(n=6, p=4, kcond=1e-2, cfl=0.5)
     g = pr.gpu()
