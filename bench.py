@@ -146,19 +146,20 @@ def c3_sweep(hpb, dev, n, p, cycles):
     (n = 512: 524,288 triangles, 28.3 M DOF at p = 6); u = 1 on the lid, velocity
     Dirichlet on every wall, initial state the boundary field projected plus 1e-3 noise.
     Hierarchy: p-levels p -> ... -> 1 on the fine mesh, then h-levels n/2, n/4, n/8 at
-    p = 1 (the 524k/131k/32k/8k-triangle meshes). `cycles` V-cycles (2+2 updates per
-    level, preconditioners every cycle) per arm; reports seconds per cycle and the FP64
-    residual drop reached. The h-levels-only hierarchy of the reference's
-    extra_finest_levels = 0 is run as a last arm."""
+    p = 1 (the 524k/131k/32k/8k-triangle meshes). At most `cycles` W-cycles (vwcycle 2,
+    the reference's ins Convergence test input; 2+2 updates per level, preconditioners
+    every cycle) per arm, stopping at a 1e-10 drop of the FP64 residual; reports seconds,
+    seconds per cycle and the drop reached. A V-cycle arm and the h-levels-only
+    hierarchy of the reference's extra_finest_levels = 0 are run last."""
     import time as _t
     from hpb import multigrid as MG
     mk = lambda n, p, **kw: hpb.lid_cavity_ins(n=n, p=p, re=400.0, **kw)
     line = {"sweep": "c3", "workload": f"ins lid cavity Re 400, p={p}, {n}x{n} split squares", "cycles": cycles}
-    for name, kw, plev in (("fp64_level_by_level", {}, True), ("fp64_graph", {"graph": True}, True),
-                           ("fp64_graph_autotuned", {"graph": True, "tune": True}, True),
-                           ("fp32_defect_correction", {"mixed": True}, True),
-                           ("fp32_defect_correction_autotuned", {"mixed": True, "tune": True}, True),
-                           ("fp64_h_levels_only", {}, False)):
+    for name, kw, plev in (("fp64_level_by_level", {"vw": 2}, True), ("fp64_graph", {"vw": 2, "graph": True}, True),
+                           ("fp64_graph_autotuned", {"vw": 2, "graph": True, "tune": True}, True),
+                           ("fp32_defect_correction", {"vw": 2, "mixed": True}, True),
+                           ("fp32_defect_correction_autotuned", {"vw": 2, "mixed": True, "tune": True}, True),
+                           ("fp64_v_cycle", {"vw": 1}, True), ("fp64_h_levels_only", {"vw": 2}, False)):
         t0 = _t.perf_counter()
         H = MG.build(mk, n=n, p=p, hlevels=3, plevels=plev)
         setup = _t.perf_counter() - t0
@@ -166,7 +167,8 @@ def c3_sweep(hpb, dev, n, p, cycles):
         shapes = H.autotune(reps=3) if kw.pop("tune", False) else None
         hist, sec, cyc = H.solve(drop=1e-10, max_cycles=cycles, prcn_every=1, **kw)
         line[name] = {"seconds": sec, "cycles": cyc, "ms_per_cycle": 1e3 * sec / max(cyc, 1),
-                      "drop": float(hist[-1]), "drop_history": [float(h) for h in hist[::max(1, cycles // 10)]],
+                      "drop": float(hist[-1]), "reached": bool(hist[-1] <= 1e-10),
+                      "drop_history": [float(h) for h in hist[::max(1, cycles // 10)]],
                       "levels": [f"{len(lv.prob.mesh.tri_pnt)} tri p={lv.prob.p}" for lv in H.levels],
                       "setup_seconds_host": setup}
         if shapes:
@@ -185,9 +187,11 @@ def c4_sweep(hpb, dev, scale, cycles):
     learned correction is trained on the GPU on solver-generated samples of 4 training
     instances with Re drawn from U[20, 200] (snapshot states after 0, 200, 1000 and 3000
     plain updates, every element of every snapshot one sample) and judged on 2 held-out
-    Re by the FP64 residual after `cycles` V-cycles (p 4 -> 2 -> 1, then channel meshes at
-    2x, 4x, 8x the edge lengths at p = 1; preconditioners every cycle): plain FP64, FP32
-    defect correction, and FP32 defect correction with the learned correction."""
+    Re by the time to a 1e-10 drop of the FP64 residual, at most `cycles` W-cycles
+    (vwcycle 2, the cycle of the reference's ins Convergence test input; p 4 -> 2 -> 1,
+    then channel meshes at 2x, 4x, 8x the edge lengths at p = 1; preconditioners every
+    cycle): plain FP64, FP32 defect correction, and FP32 defect correction with the
+    learned correction."""
     import time as _t
     import numpy as np
     from hpb import learned as LR
@@ -231,12 +235,15 @@ def c4_sweep(hpb, dev, scale, cycles):
             H = hierarchy(float(re))
             if learned:
                 LR.attach(H.levels[0], net, 1.0)
-            h, sec, cyc = H.solve(drop=1e-10, max_cycles=cycles, mixed=mixed, prcn_every=1)
-            res[name] = {"seconds": sec, "cycles": cyc, "drop": float(h[-1]),
+            h, sec, cyc = H.solve(drop=1e-10, max_cycles=cycles, vw=2, mixed=mixed, prcn_every=1)
+            res[name] = {"seconds": sec, "cycles": cyc, "drop": float(h[-1]), "reached": bool(h[-1] <= 1e-10),
                          "min_drop": float(np.min(h)), "drop_history": [float(x) for x in h[::max(1, cycles // 10)]]}
             H.close()
+        res["speedup_learned_fp32_vs_fp64"] = res["fp64"]["seconds"] / res["learned_fp32"]["seconds"]
+        res["speedup_fp32_vs_fp64"] = res["fp64"]["seconds"] / res["fp32_defect_correction"]["seconds"]
         line[f"re_{re:.1f}"] = res
-        print(json.dumps({"re": float(re), **{k: (v["drop"], v["seconds"]) for k, v in res.items()}}), flush=True)
+        print(json.dumps({"re": float(re), **{k: ((v["drop"], v["seconds"], v["cycles"]) if isinstance(v, dict) else v)
+                                               for k, v in res.items()}}), flush=True)
     net.close()
     print(json.dumps(line), flush=True)
 

@@ -3,8 +3,9 @@ h-levels, tri_mesh/blocks.cpp:1267-1348).
 
 p-levels share the fine mesh at a lower polynomial degree (p -> p/2 -> ... -> 1,
 as the reference halves log2p; p = 6 goes 6 -> 3 -> 1). h-levels are coarser
-split-square meshes at p = 1 whose transfer weights are each point's containing
-triangle in the other mesh with barycentric weights (tri_mesh::mgconnect).
+meshes at p = 1 whose transfer weights are each point's containing triangle in the
+other mesh with barycentric weights, boundary points re-connected along the other
+mesh's boundary sides (tri_mesh::mgconnect).
 """
 import ctypes
 
@@ -110,6 +111,48 @@ def locate(mesh, pts):
     return best_t.astype(np.int32), np.ascontiguousarray(best_w)
 
 
+def boundary_reconnect(src, tgt, t, w, chunk=4096):
+    """Boundary points of src re-connected along tgt's boundary sides
+    (edge_bdry::mgconnect, tri_mesh/tri_boundary.cpp:164-201, with the side search of
+    edge_bdry::findbdrypt, tri_boundary.cpp:95-160): each boundary point takes the
+    nearest boundary side of tgt, weights 0.5(1-psi) and 0.5(1+psi) on its end points
+    and 0 on the triangle's third vertex; a point beyond the ends of the sides (a
+    convex corner) takes the nearer end point. Boundary values, essential conditions
+    included, then move between the levels through boundary values only: on a curved
+    boundary, whose coarse sides are chords, the containing triangle would also weight
+    an interior vertex and every prolongation would move the fine essential values.
+    t, w: containing-triangle weights of every src point (locate), updated in place."""
+    sb = src.boundary_segments()
+    bp = np.unique(src.seg_pnt[sb].ravel())
+    tb = tgt.boundary_segments()
+    a = tgt.pnts[tgt.seg_pnt[tb, 0]]
+    d = tgt.pnts[tgt.seg_pnt[tb, 1]] - a
+    l2 = np.einsum("ij,ij->i", d, d)
+    for c0 in range(0, len(bp), chunk):
+        q = bp[c0:c0 + chunk]
+        x = src.pnts[q][:, None, :] - a[None, :, :]
+        sv = np.clip(np.einsum("kij,ij->ki", x, d) / l2, 0.0, 1.0)
+        r = x - sv[..., None] * d[None, :, :]
+        k = np.argmin(np.einsum("kij,kij->ki", r, r), axis=1)
+        seg = tb[k]
+        s = sv[np.arange(len(q)), k]
+        tri = tgt.seg_tri[seg, 0]
+        tp = tgt.tri_pnt[tri]
+        p0 = tgt.seg_pnt[seg, 0][:, None]
+        p1 = tgt.seg_pnt[seg, 1][:, None]
+        t[q] = tri
+        w[q] = np.where(tp == p0, (1.0 - s)[:, None], 0.0) + np.where(tp == p1, s[:, None], 0.0)
+    return t, w
+
+
+def connect(src, tgt):
+    """Transfer weights of every src point in tgt (tri_mesh::mgconnect,
+    tri_mesh/connect.cpp:49-86): the containing triangle with barycentric weights,
+    then boundary points re-connected along tgt's boundary sides."""
+    t, w = locate(tgt, src.pnts)
+    return boundary_reconnect(src, tgt, t, w)
+
+
 class Hierarchy:
     """levels[0] is the finest GPULevel; each next one is attached to the previous."""
 
@@ -129,8 +172,8 @@ class Hierarchy:
                 L.check(lib.hp_gpu_mg_attach_p(c.h, f.h, fadd), "mg_attach_p")
             else:
                 fm, cm = probs[l - 1].mesh, probs[l].mesh
-                f2c_t, f2c_w = locate(cm, fm.pnts)
-                c2f_t, c2f_w = locate(fm, cm.pnts)
+                f2c_t, f2c_w = connect(fm, cm)
+                c2f_t, c2f_w = connect(cm, fm)
                 self._keep += [f2c_t, f2c_w, c2f_t, c2f_w]
                 L.check(lib.hp_gpu_mg_attach_h(c.h, f.h, L.ptr(f2c_t), L.ptr(f2c_w), L.ptr(c2f_t), L.ptr(c2f_w),
                                                fadd), "mg_attach_h")

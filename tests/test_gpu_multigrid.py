@@ -80,10 +80,10 @@ def test_h_restriction_and_prolongation():
     uf = f.state()[0]
     L.check(H.lib.hp_gpu_mg_restrict(c.h), "restrict")
     uc = c.state()[0]
-    t_c2f, w_c2f = MG.locate(fm, cm.pnts)
+    t_c2f, w_c2f = MG.connect(cm, fm)
     want_u = np.einsum("kj,kjn->kn", w_c2f, uf[fm.tri_pnt[t_c2f]])
     assert np.max(np.abs(uc - want_u)) < 1e-13
-    t_f2c, w_f2c = MG.locate(cm, fm.pnts)
+    t_f2c, w_f2c = MG.connect(fm, cm)
     res0 = np.zeros_like(uc)
     for j in range(3):
         np.add.at(res0, cm.tri_pnt[t_f2c, j], w_f2c[:, j:j + 1] * rf)
@@ -177,4 +177,24 @@ def test_vcycle_on_delaunay_meshes():
     H = MG.build(mk, n=24, p=4, hlevels=2, cfl={4: 0.5, 2: 0.75, 1: 1.0})
     hist, sec, cycles = H.solve(drop=1e-10, max_cycles=300)
     assert hist[-1] <= 1e-10
+    H.close()
+
+
+def test_curved_hole_cycles_keep_essential_values_and_converge():
+    """ins past a curved hole with h-levels on coarser, non-nested channel meshes: the
+    boundary re-connection keeps the fine no-slip values exact through every
+    prolongation, and W-cycles (vwcycle 2) reach the 1e-10 drop."""
+    ms = [hpb.channel_hole(L=4.0, H=2.0, cx=1.0, cy=1.0, r=0.25, hmin=0.04 * k, hmax=0.15 * k, grade=0.1 * k)
+          for k in (1, 2)]
+    probs = [hpb.channel_cylinder_ins(mesh=ms[0], p=2, re=20.0), hpb.channel_cylinder_ins(mesh=ms[0], p=1, re=20.0),
+             hpb.channel_cylinder_ins(mesh=ms[1], p=1, re=20.0)]
+    H = MG.Hierarchy(probs, ["fine", "p", "h"])
+    hist, sec, cycles = H.solve(drop=1e-10, max_cycles=300, vw=2)
+    assert hist[-1] <= 1e-10, hist[-5:]
+    m = ms[0]
+    cx, cy, r = m.hole
+    on_hole = np.abs(np.hypot(m.pnts[:, 0] - cx, m.pnts[:, 1] - cy) - r) < 1e-9
+    assert np.count_nonzero(on_hole) > 8
+    uv = H.levels[0].state()[0][on_hole, :2]
+    assert np.max(np.abs(uv)) == 0.0
     H.close()
