@@ -143,19 +143,20 @@ struct LaunchImpl {
     using C = ElemCfg<R, P, PHYS>;
     static constexpr int NV = C::NV, SM = P - 1, IM = (P - 1) * (P - 2) / 2;
     static int smem() {
-        return (int)(((sizeof(DevTables<R, P>) + 15) / 16) * 16 + (size_t)C::WPC * C::S_WARP * sizeof(R));
+        return (int)(((sizeof(DevTables<R, P>) + 15) / 16) * 16 + (size_t)C::WPC * C::EPW * C::S_WARP * sizeof(R));
     }
     static void fill(const hp_basis_tables &b, void *out) { fill_tables<R, P>(b, *reinterpret_cast<DevTables<R, P> *>(out)); }
     static void elem(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, int stage, int zero_rr, int diff,
                      int nsm, const Tune &tn, cudaStream_t st) {
-        int blocks = nblk(m.ntri, C::WPC);
+        constexpr int EPC = C::WPC * C::EPW;  // elements per CTA and pass
+        int blocks = nblk(m.ntri, EPC);
         const int cap = nsm * tn.elem_cap;
         if (blocks > cap) blocks = cap;
         const auto *t = reinterpret_cast<const DevTables<R, P> *>(tab);
         k_rsdl_elem<R, P, PHYS, false><<<blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, stage, zero_rr, diff,
                                                                            ElemMat<R>{});
         if (m.ncurved > 0)
-            k_rsdl_elem<R, P, PHYS, true><<<std::min(nblk(m.ncurved, C::WPC), cap), C::WPC * 32, smem(), st>>>(
+            k_rsdl_elem<R, P, PHYS, true><<<std::min(nblk(m.ncurved, EPC), cap), C::WPC * 32, smem(), st>>>(
                 t, m, s, ph, stage, zero_rr, diff, ElemMat<R>{});
     }
     static size_t emat_len(long ntri) { return EmatCfg<P>::len(ntri); }
@@ -167,7 +168,7 @@ struct LaunchImpl {
             for (int cv = 0; cv < 2; ++cv) {
                 const long items = (cv ? (long)m.ncurved : (long)m.ntri) * (C::T + 1);
                 if (items == 0) continue;
-                long blocks = (items + C::WPC - 1) / C::WPC;
+                long blocks = (items + C::WPC * C::EPW - 1) / (C::WPC * C::EPW);
                 if (blocks > (long)nsm * 16) blocks = (long)nsm * 16;
                 if (cv)
                     k_rsdl_elem<R, P, PHYS, true><<<(int)blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, ph.nstage, 1, 0,

@@ -100,6 +100,7 @@ struct ElemCfg {
     static constexpr int NPAIR = NV;               // flux pairs integrated by intgrtrs
     static constexpr int NQ = (PHYS == 1 ? 16 : 7);  // per-point scratch values
     static constexpr int WPC = (P <= 4 ? 8 : 4);   // warps per CTA
+    static constexpr int EPW = (P == 1 ? 4 : (P == 2 ? 2 : 1));  // elements per warp (lane groups)
     static constexpr int NB = (PHYS == 1 ? 2 : 0);  // base-state variables gathered in correction form
     // per-warp scratch (in R units)
     static constexpr int S_UHT = (NV + NB) * T;
@@ -217,7 +218,11 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    R *uht = warp_base + warp * C::S_WARP;
+    // EPW elements per warp, one group of LW lanes each (all groups pass the same
+    // __syncwarp sequence; a group without an element idles through it)
+    constexpr int EPW = C::EPW, LW = 32 / EPW;
+    const int grp = lane / LW, sl = lane - grp * LW;
+    R *uht = warp_base + (warp * EPW + grp) * C::S_WARP;
     R *wk = uht + C::S_UHT;
     R *pt = wk + C::S_WK;
     auto PT = [&](int q) -> R * { return pt + q * GG; };
@@ -229,14 +234,18 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
     const bool bmode = (PHYS == 0) && build.aim != nullptr;
     const long nel = CURVED ? (long)mesh.ncurved : (long)mesh.ntri;
     const long nitems = bmode ? nel * (T + 1) : nel;
-    for (long item = (long)blockIdx.x * C::WPC + warp; item < nitems; item += (long)gridDim.x * C::WPC) {
+    for (long wbase = ((long)blockIdx.x * C::WPC + warp) * EPW; wbase < nitems;
+         wbase += (long)gridDim.x * C::WPC * EPW) {
+        const long item = (wbase + grp < nitems) ? wbase + grp : wbase;
         const int eidx = bmode ? (int)(item / (T + 1)) : (int)item;
         const int bcol = bmode ? (int)(item - (long)eidx * (T + 1)) : -1;
         const int tind = CURVED ? mesh.crv_tri[eidx] : eidx;
-        if (!CURVED && mesh.tri_cv && mesh.tri_cv[tind] >= 0) continue;  // done by the curved launch
+        // curved elements are done by the curved launch
+        const bool act = (wbase + grp < nitems) && (CURVED || !mesh.tri_cv || mesh.tri_cv[tind] < 0);
+        if (EPW == 1 && !act) continue;
         const int p0 = mesh.tri_pnt[3 * tind], p1 = mesh.tri_pnt[3 * tind + 1], p2 = mesh.tri_pnt[3 * tind + 2];
         // ---- gather (ugtouht, gtol.cpp:14-55)
-        for (int w = lane; w < NV * T; w += 32) {
+        for (int w = sl; act && w < NV * T; w += LW) {
             const int n = w / T, m = w - n * T;
             R val;
             if (bmode) {
@@ -255,7 +264,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
             uht[n * T + m] = val;
         }
         if (PHYS == 1 && diff) {
-            for (int w = lane; w < 2 * T; w += 32) {
+            for (int w = sl; act && w < 2 * T; w += LW) {
                 const int n = w / T, m = w - n * T;
                 R val;
                 if (m < 3) {
@@ -292,7 +301,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
             const int nqw = NQW + ((PHYS == 1 && diff) ? 2 : 0);  // + base u, v values
             // one lane per (quantity, eta point): all X column sums in registers, modes in
             // increasing order within each column (the order of the column lists)
-            for (int w = lane; w < nqw * G; w += 32) {
+            for (int w = sl; act && w < nqw * G; w += LW) {
                 const int q = w / G, j = w - q * G;
                 int var, der;
                 if (q < 2 * NDV) { var = q >> 1; der = q & 1; }
@@ -310,7 +319,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
         }
         __syncwarp();
         // ---- proj stage II + pointwise fluxes
-        for (int w = lane; w < GG; w += 32) {
+        for (int w = sl; act && w < GG; w += LW) {
             const int i = w / G, j = w - i * G;
             const R oeta = tb.n0[j], xp1 = tb.x0[i];
             R d00, d01, d10, d11;
@@ -417,7 +426,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
         // ---- intgrtrs of the imaginary fluxes (intgrt.cpp:81-158) -> res (and res.i)
         // pair k: ins (cv0x,cv0y)=slots(0,1), (cv1x,cv1y)=(2,3), (mx,my)=(4,5); cd (0,1)
         auto intgrtrs_stageI = [&](int sx0) {
-            for (int w = lane; w < C::NPAIR * X * G; w += 32) {
+            for (int w = sl; act && w < C::NPAIR * X * G; w += LW) {
                 const int k = w / (X * G), r = w - k * (X * G), n = r / G, j = r - n * G;
                 const R *dx = PT(sx0 + 2 * k), *dy = PT(sx0 + 2 * k + 1);
                 R l0 = 0, l1 = 0;
@@ -453,7 +462,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
         __syncwarp();
         // the cd source enters only the uht = 0 column of the build
         const R srcv = (bmode && bcol < T) ? (R)0 : (R)ph.src;
-        for (int w = lane; w < NV * T; w += 32) {
+        for (int w = sl; act && w < NV * T; w += LW) {
             const int n = w / T, m = w - n * T;
             const R val = mode_result(n, m);
             if (bmode) {
@@ -471,7 +480,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
             // ---- strong residual: res = source + derivr(F_r) + derivs(F_s) (proj.cpp:339-402)
             __syncwarp();
             constexpr int SRES = (PHYS == 1 ? 16 : 7);
-            for (int w = lane; w < NV * GG; w += 32) {
+            for (int w = sl; act && w < NV * GG; w += LW) {
                 const int n = w / GG, r = w - n * GG, i = r / G, j = r - i * G;
                 int sr, ss;
                 if (PHYS == 1) { sr = (n < 2 ? 6 + 2 * n : 4); ss = sr + 1; }
@@ -511,7 +520,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
                                      sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
                 const R h = (R)((area / perim) / (0.25 * (P + 1) * (P + 1)));
                 const R nu = (R)(ph.mu / ph.rho);
-                for (int w = lane; w < GG; w += 32) {
+                for (int w = sl; act && w < GG; w += LW) {
                     R d00, d01, d10, d11;
                     metric(w / G, w - (w / G) * G, d00, d01, d10, d11);
                     const R cjcb = d00 * d11 - d10 * d01;
@@ -533,7 +542,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
             } else {
                 const R taue = st.tau[tind];
                 const R ax = (R)ph.ax, ay = (R)ph.ay;
-                for (int w = lane; w < GG; w += 32) {
+                for (int w = sl; act && w < GG; w += LW) {
                     R d00, d01, d10, d11;
                     metric(w / G, w - (w / G) * G, d00, d01, d10, d11);
                     const R tres = taue * PT(7)[w];
@@ -546,7 +555,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
             intgrtrs_stageI(PHYS == 1 ? 10 : 4);
             // cd source term: intgrt(res0) with res0 = -cjcb*src (constant over the element)
             __syncwarp();
-            for (int w = lane; w < NV * T; w += 32) {
+            for (int w = sl; act && w < NV * T; w += LW) {
                 const int n = w / T, m = w - n * T;
                 R val = mode_result(n, m);
                 if (PHYS == 0 && srcv != (R)0) {
