@@ -605,3 +605,253 @@ extern "C" int hp_basis_build(int p, hp_basis_tables *out) {
     e += b.lumpinv1d();
     return e;
 }
+
+// ---------------------------------------------------------------------------
+// Modal tetrahedral basis (tet_basis, runtime p <= 4).
+//
+// Restates tet_basis::initialize_values (tet_basis/initialize.cpp:73-380) and the
+// 1D functions of tet_basis::ptvalues_deriv (tet_basis/ptvalues.cpp:154-330) with
+// the recurrence and Gauss routines above, then forms dense per-point operators
+// from the factorisation that tet_basis::proj (proj.cpp:22-265) applies: every
+// mode is sgn * gx(x_i, mx) gy(y_j, my) gz(z_k, mz) in the collapsed coordinates.
+// ---------------------------------------------------------------------------
+#include "hp_tet.h"
+
+namespace {
+
+// Monic three-term recurrence value and derivative, p_0 = 1, from (a, b).
+struct Rec {
+    double pk = 1.0, pkm = 0.0, dpk = 0.0, dpkm = 0.0;
+    void step(double x, double a, double b) {
+        const double pkp = (x - a) * pk - b * pkm;
+        const double dpkp = pk + (x - a) * dpk - b * dpkm;
+        dpkm = dpk;
+        dpk = dpkp;
+        pkm = pk;
+        pk = pkp;
+    }
+};
+
+struct TetRecur {
+    int em;
+    std::vector<double> a22, b22;              // Jacobi(2,2): edges
+    std::vector<std::vector<double>> af, bf;   // Jacobi(2m+3,2), m = 1..em: faces
+    std::vector<std::vector<double>> ai, bi;   // Jacobi(2n+2m+4,2): interiors
+    explicit TetRecur(int em_) : em(em_) {
+        const int n = em + 1;
+        a22.resize(n); b22.resize(n);
+        jacobi_recur(n, 2.0, 2.0, a22.data(), b22.data());
+        af.assign(em + 1, std::vector<double>(n)); bf = af;
+        for (int m = 1; m <= em; ++m) jacobi_recur(n, 2.0 * m + 3.0, 2.0, af[m].data(), bf[m].data());
+        for (int nn = 1; nn <= em - 1; ++nn)
+            for (int m = 1; m <= em - nn; ++m) {
+                ai.emplace_back(n); bi.emplace_back(n);
+                jacobi_recur(n, 2.0 * nn + 2.0 * m + 4.0, 2.0, ai.back().data(), bi.back().data());
+            }
+    }
+    // x direction: vertex 0,1 / edge 4; vertex 2 etc.; vertex 3 etc.; edge 1 bubbles
+    void fx(double x, double *g, double *dg) const {
+        int k = 0;
+        g[k] = 1.0; dg[k++] = 0.0;
+        g[k] = 0.5 * (1 - x); dg[k++] = -0.5;
+        g[k] = 0.5 * (1 + x); dg[k++] = 0.5;
+        Rec r;
+        for (int m = 0; m < em; ++m) {
+            g[k] = 0.25 * (1.0 + x) * (1.0 - x) * r.pk;
+            dg[k++] = -x * 0.5 * r.pk + (1.0 + x) * (1.0 - x) * 0.25 * r.dpk;
+            r.step(x, a22[m], b22[m]);
+        }
+    }
+    void fy(double y, double *g, double *dg) const {
+        int k = 0;
+        g[k] = 1.0; dg[k++] = 0.0;
+        g[k] = (1 + y) * 0.5; dg[k++] = 0.5;
+        g[k] = (1 - y) * 0.5; dg[k++] = -0.5;
+        for (int m = 2; m <= em + 1; ++m) {
+            g[k] = std::pow(0.5 * (1 - y), m);
+            dg[k++] = -0.5 * m * std::pow(0.5 * (1. - y), m - 1);
+        }
+        Rec r;
+        for (int n = 0; n < em; ++n) {
+            g[k] = (1.0 - y) * (1.0 + y) * 0.25 * r.pk;
+            dg[k++] = -0.5 * y * r.pk + (1.0 - y) * (1.0 + y) * 0.25 * r.dpk;
+            r.step(y, a22[n], b22[n]);
+        }
+        for (int m = 1; m <= em - 1; ++m) {
+            Rec q;
+            for (int kk = 1; kk <= em - m; ++kk) {
+                g[k] = std::pow(0.5 * (1.0 - y), m + 1) * 0.5 * (1.0 + y) * q.pk;
+                dg[k++] = -0.25 * (m + 1.0) * std::pow(0.5 * (1.0 - y), m) * (1.0 + y) * q.pk +
+                          std::pow(0.5 * (1.0 - y), m + 1) * 0.5 * (q.pk + (1.0 + y) * q.dpk);
+                q.step(y, af[m][kk - 1], bf[m][kk - 1]);
+            }
+        }
+    }
+    void fz(double z, double *g, double *dg) const {
+        int k = 0;
+        g[k] = (1 + z) * 0.5; dg[k++] = 0.5;
+        g[k] = (1 - z) * 0.5; dg[k++] = -0.5;
+        for (int m = 2; m <= em + 1; ++m) {
+            g[k] = std::pow(0.5 * (1 - z), m);
+            dg[k++] = -0.5 * m * std::pow(0.5 * (1. - z), m - 1);
+        }
+        Rec r;
+        for (int n = 0; n < em; ++n) {
+            g[k] = (1.0 - z) * (1.0 + z) * 0.25 * r.pk;
+            dg[k++] = -0.5 * z * r.pk + (1.0 - z) * (1.0 + z) * 0.25 * r.dpk;
+            r.step(z, a22[n], b22[n]);
+        }
+        for (int m = 1; m <= em - 1; ++m) {
+            Rec q;
+            for (int kk = 1; kk <= em - m; ++kk) {
+                g[k] = std::pow(0.5 * (1.0 - z), m + 1) * 0.5 * (1.0 + z) * q.pk;
+                dg[k++] = -0.25 * (m + 1.0) * std::pow(0.5 * (1.0 - z), m) * (1.0 + z) * q.pk +
+                          std::pow(.5 * (1.0 - z), m + 1) * .5 * (q.pk + (1.0 + z) * q.dpk);
+                q.step(z, af[m][kk - 1], bf[m][kk - 1]);
+            }
+        }
+        int ind2 = 0;
+        for (int n = 1; n <= em - 1; ++n)
+            for (int m = 1; m <= em - n; ++m) {
+                Rec q;
+                for (int kk = 1; kk <= em - m - n; ++kk) {
+                    g[k] = std::pow(0.5 * (1.0 - z), m + n + 1) * 0.5 * (1.0 + z) * q.pk;
+                    dg[k++] = -0.25 * (m + n + 1) * std::pow(0.5 * (1.0 - z), m + n) * (1.0 + z) * q.pk +
+                              std::pow(.5 * (1.0 - z), m + n + 1) * .5 * (q.pk + (1. + z) * q.dpk);
+                    q.step(z, ai[ind2][kk - 1], bi[ind2][kk - 1]);
+                }
+                ++ind2;
+            }
+    }
+};
+
+// Lagrange-derivative factors of one Gauss direction (initialize.cpp:157-180):
+// d(i) = 1 / prod_{k != i} (x_i - x_k); d2(i,n) = prod_{k != i}(x_i - x_k) / (x_i - x_n);
+// d3 = d2 (1 + x_i) / 2 (on the raw nodes).
+void lagrange_factors(int g, const double *x, double *d, double (*d2)[HP_TET_MAXG], double (*d3)[HP_TET_MAXG]) {
+    for (int i = 0; i < g; ++i) {
+        double pr = 1.0;
+        for (int k = 0; k < g; ++k)
+            if (k != i) pr *= (x[i] - x[k]);
+        for (int n = 0; n < g; ++n) {
+            d2[i][n] = (n == i) ? 0.0 : pr / (x[i] - x[n]);
+            if (d3) d3[i][n] = (n == i) ? 0.0 : d2[i][n] * (1. + x[i]) / 2.;
+        }
+        d[i] = 1.0 / pr;
+    }
+}
+
+// (A f)(i) = sum_n A(i,n) f(n) equal to sum_{n != i} (f_i d_i + f_n d_n) c(i,n)
+// (the pairwise form of derivr / derivs / derivt, proj.cpp:781-911).
+void deriv_operator(int g, const double *d, const double (*c)[HP_TET_MAXG], double (*A)[HP_TET_MAXG]) {
+    for (int i = 0; i < g; ++i) {
+        double diag = 0.0;
+        for (int n = 0; n < g; ++n) {
+            if (n == i) continue;
+            diag += c[i][n];
+            A[i][n] = d[n] * c[i][n];
+        }
+        A[i][i] = d[i] * diag;
+    }
+}
+
+}  // namespace
+
+extern "C" int hp_tet_basis_build(int p, hp_tet_tables *out) {
+    if (!out || p < 1 || p > HP_TET_MAXP) return -1;
+    hp_tet_tables &t = *out;
+    std::memset(&t, 0, sizeof(t));
+    const int G = p + 1, em = p - 1, fm = std::max((p - 1) * (p - 2) / 2, 0);
+    const int T = (p + 1) * (p + 2) * (p + 3) / 6;
+    const int im = std::max(T - 4 * fm - 6 * em - 4, 0);
+    t.p = p; t.G = G; t.T = T; t.em = em; t.fm = fm; t.im = im; t.bm = 4 + 6 * em + 4 * fm;
+    t.nmodx = em + 3; t.nmody = 3 + 2 * em + fm; t.nmodz = 2 + 2 * em + fm + im;
+    // Gauss rules: Legendre in x, Jacobi(1,0) in y (weights / 2), Jacobi(2,0) in z (weights / 4)
+    std::vector<double> a(G + 1), b(G + 1);
+    legendre_recur(G + 1, a.data(), b.data());
+    gauss_rule(G, a.data(), b.data(), t.xp, t.wtx);
+    jacobi_recur(G + 1, 1.0, 0.0, a.data(), b.data());
+    gauss_rule(G, a.data(), b.data(), t.yp, t.wty);
+    jacobi_recur(G + 1, 2.0, 0.0, a.data(), b.data());
+    gauss_rule(G, a.data(), b.data(), t.zp, t.wtz);
+    for (int i = 0; i < G; ++i) {
+        t.wty[i] *= 0.5;
+        t.wtz[i] *= 0.25;
+    }
+    lagrange_factors(G, t.xp, t.dltx, t.dltx2, t.dltx3);
+    lagrange_factors(G, t.yp, t.dlty, t.dlty2, t.dlty3);
+    lagrange_factors(G, t.zp, t.dltz, t.dltz2, nullptr);
+    TetRecur rc(em);
+    for (int i = 0; i < G; ++i) {
+        rc.fx(t.xp[i], t.gx[i], t.dgx[i]);
+        rc.fy(t.yp[i], t.gy[i], t.dgy[i]);
+        rc.fz(t.zp[i], t.gz[i], t.dgz[i]);
+        t.x0[i] = 0.5 * (1 + t.xp[i]);
+        t.y0[i] = 2.0 / (1 - t.yp[i]);
+        t.y1[i] = 0.5 * (1 + t.yp[i]);
+        t.z0[i] = 2.0 / (1 - t.zp[i]);
+    }
+    // mode -> (x, y, z function, sign), in the order of tet_basis::proj
+    auto set = [&](int m, int ix, int iy, int iz, double s) {
+        t.mx[m] = ix; t.my[m] = iy; t.mz[m] = iz; t.msg[m] = s;
+    };
+    const int be1 = 4, be2 = be1 + em, be3 = be2 + em, be4 = be3 + em, be5 = be4 + em, be6 = be5 + em;
+    const int bf0 = be6 + em, bf1 = bf0 + fm, bf2 = bf1 + fm, bf3 = bf2 + fm, bi = bf3 + fm;
+    set(0, 0, 0, 0, 1.0);
+    set(1, 0, 1, 1, 1.0);
+    set(2, 1, 2, 1, 1.0);
+    set(3, 2, 2, 1, 1.0);
+    for (int i = 0; i < em; ++i) {
+        set(be4 + i, 0, 1, 2 + em + i, 1.0);
+        set(be5 + i, 1, 2, 2 + em + i, 1.0);
+        set(be6 + i, 2, 2, 2 + em + i, 1.0);
+    }
+    for (int i = 1; i <= em; ++i) {
+        set(be1 + i - 1, i + 2, i + 2, i + 1, 1.0);
+        set(be2 + i - 1, 2, 2 + em + i, i + 1, 1.0);
+        set(be3 + i - 1, 1, 2 + em + i, i + 1, 1.0);
+    }
+    {
+        int ind2 = 0;
+        double s = 1.0;
+        for (int i = 1; i <= em; ++i, s = -s)
+            for (int j = 1; j <= em - i; ++j, ++ind2) {
+                set(bf1 + ind2, i + 2, i + 2, 2 + 2 * em + ind2, s);
+                set(bf2 + ind2, 2, 2 + em + i, 2 + 2 * em + ind2, s);
+                set(bf3 + ind2, 1, 2 + em + i, 2 + 2 * em + ind2, 1.0);
+            }
+    }
+    {
+        int ind2 = 0, ind3 = 0;
+        for (int i = 1; i <= em - 1; ++i)
+            for (int j = 1; j <= em - i; ++j, ++ind2) {
+                set(bf0 + ind2, i + 2, 3 + 2 * em + ind2, i + j + 1, 1.0);
+                for (int k = 1; k <= em - i - j; ++k, ++ind3)
+                    set(bi + ind3, i + 2, 3 + 2 * em + ind2, 2 + 2 * em + fm + ind3, 1.0);
+            }
+    }
+    // dense operators of proj (r, s, t derivatives through the collapsed coordinates)
+    for (int i = 0; i < G; ++i)
+        for (int j = 0; j < G; ++j)
+            for (int k = 0; k < G; ++k) {
+                const int q = (i * G + j) * G + k;
+                t.w[q] = t.wtx[i] * t.wty[j] * t.wtz[k];
+                for (int m = 0; m < T; ++m) {
+                    const double s = t.msg[m];
+                    const double gx = t.gx[i][t.mx[m]], dgx = t.dgx[i][t.mx[m]];
+                    const double gy = t.gy[j][t.my[m]], dgy = t.dgy[j][t.my[m]];
+                    const double gz = t.gz[k][t.mz[m]], dgz = t.dgz[k][t.mz[m]];
+                    const double dx = s * dgx * gy * gz * t.y0[j] * t.z0[k];
+                    t.F[q][m] = s * gx * gy * gz;
+                    t.DX[q][m] = dx;
+                    t.DY[q][m] = s * gx * dgy * gz * t.z0[k] + t.x0[i] * dx;
+                    t.DZ[q][m] = s * (gx * gy * dgz + t.y1[j] * gx * dgy * gz * t.z0[k]) + t.x0[i] * dx;
+                }
+            }
+    deriv_operator(G, t.dltx, t.dltx2, t.Ax);
+    deriv_operator(G, t.dltx, t.dltx3, t.Bx);
+    deriv_operator(G, t.dlty, t.dlty2, t.Ay);
+    deriv_operator(G, t.dlty, t.dlty3, t.By);
+    deriv_operator(G, t.dltz, t.dltz2, t.Az);
+    return 0;
+}

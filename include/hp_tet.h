@@ -1,0 +1,68 @@
+/*
+ * hp_tet.h — C ABI of the 3D (tet_hp) path: modal tetrahedral basis tables and
+ * the ins element residual on tetrahedra.
+ *
+ * Replaces, for the 3D hot path:
+ *   tet_basis::initialize / initialize_values   tet_basis/initialize.cpp:21-520
+ *   tet_basis::proj / intgrt / intgrtrst        tet_basis/proj.cpp:22-265, intgrt.cpp:23-609
+ *   tet_basis::derivr / derivs / derivt         tet_basis/proj.cpp:781-911
+ *   tet_hp::rsdl + tet_hp_ins::element_rsdl     tet_hp/update.cpp:9, tet_hp/ins/rsdl.cpp:15-785
+ *   tet_hp_ins::setup_preconditioner (tau)      tet_hp/ins/setup_preconditioner.cpp
+ */
+#ifndef HP_TET_H
+#define HP_TET_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HP_TET_MAXP 4  /* tet_basis.h:26 MAXP */
+#define HP_TET_MAXG 5  /* Gauss points per direction, p + 1 */
+#define HP_TET_MAXT 35 /* modes, (p+1)(p+2)(p+3)/6 */
+#define HP_TET_MAXQ 125
+#define HP_TET_MAXM 12 /* 1D functions per collapsed direction */
+
+/* Tables of tet_basis for one p (gpx = gpy = gpz = G = p + 1). Point arrays use
+ * the compact index q = (i * G + j) * G + k for Gauss point (x_i, y_j, z_k) of the
+ * collapsed coordinates. Mode order: 4 vertices, 6 edges x em, 4 faces x fm,
+ * interior (tet_basis.h:33-40).
+ *
+ * Dense operators (rows q, columns mode m): F = value, DX / DY / DZ = the r, s, t
+ * derivatives that tet_basis::proj returns, w = wtx * wty * wtz, so that
+ *   proj:      f(q) = sum_m F(q,m) u(m), and likewise dr, ds, dt;
+ *   intgrt:    r(m) = sum_q w(q) F(q,m) f(q);
+ *   intgrtrst: r(m) -= sum_q w(q) (DX(q,m) fr(q) + DY(q,m) fs(q) + DZ(q,m) ft(q)).
+ * The point-derivative operators of derivr / derivs / derivt act along one
+ * collapsed direction each: (Ax f)(i) = sum_n Ax(i,n) f(n) along x, and so on;
+ *   derivr: dr += y0(j) z0(k) Ax_x f
+ *   derivs: ds += y0(j) z0(k) Bx_x f + z0(k) Ay_y f
+ *   derivt: dt += y0(j) z0(k) Bx_x f + z0(k) By_y f + Az_z f. */
+typedef struct hp_tet_tables {
+    int p, G, T, em, fm, im, bm, nmodx, nmody, nmodz;
+    double gx[HP_TET_MAXG][HP_TET_MAXM], dgx[HP_TET_MAXG][HP_TET_MAXM];
+    double gy[HP_TET_MAXG][HP_TET_MAXM], dgy[HP_TET_MAXG][HP_TET_MAXM];
+    double gz[HP_TET_MAXG][HP_TET_MAXM], dgz[HP_TET_MAXG][HP_TET_MAXM];
+    double wtx[HP_TET_MAXG], wty[HP_TET_MAXG], wtz[HP_TET_MAXG];
+    double xp[HP_TET_MAXG], yp[HP_TET_MAXG], zp[HP_TET_MAXG];
+    double x0[HP_TET_MAXG], y0[HP_TET_MAXG], y1[HP_TET_MAXG], z0[HP_TET_MAXG];
+    double dltx[HP_TET_MAXG], dlty[HP_TET_MAXG], dltz[HP_TET_MAXG];
+    double dltx2[HP_TET_MAXG][HP_TET_MAXG], dltx3[HP_TET_MAXG][HP_TET_MAXG];
+    double dlty2[HP_TET_MAXG][HP_TET_MAXG], dlty3[HP_TET_MAXG][HP_TET_MAXG];
+    double dltz2[HP_TET_MAXG][HP_TET_MAXG];
+    int mx[HP_TET_MAXT], my[HP_TET_MAXT], mz[HP_TET_MAXT]; /* 1D function of each mode */
+    double msg[HP_TET_MAXT];                               /* its sign */
+    double w[HP_TET_MAXQ];
+    double F[HP_TET_MAXQ][HP_TET_MAXT], DX[HP_TET_MAXQ][HP_TET_MAXT];
+    double DY[HP_TET_MAXQ][HP_TET_MAXT], DZ[HP_TET_MAXQ][HP_TET_MAXT];
+    double Ax[HP_TET_MAXG][HP_TET_MAXG], Bx[HP_TET_MAXG][HP_TET_MAXG];
+    double Ay[HP_TET_MAXG][HP_TET_MAXG], By[HP_TET_MAXG][HP_TET_MAXG];
+    double Az[HP_TET_MAXG][HP_TET_MAXG];
+} hp_tet_tables;
+
+/* Builds the tables for 1 <= p <= 4. Returns 0, or -1 for an unsupported p. */
+int hp_tet_basis_build(int p, hp_tet_tables *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -78,6 +78,28 @@ def ref():
     return _r
 
 
+_rt = None
+REF_TET_SO = os.path.join(os.path.dirname(REF_SO), "libtet_basis_ref.so")
+
+
+def ref_tet():
+    """The reference's own tet_basis (oracle/_ref), or None when it was not built."""
+    global _rt
+    if _rt is None:
+        if not os.path.exists(REF_TET_SO):
+            return None
+        r = ctypes.CDLL(REF_TET_SO)
+        P, I = ctypes.c_void_p, ctypes.c_int
+        r.ref_tet_sizes.argtypes = [I, P]
+        r.ref_tet_get.argtypes = [I, ctypes.c_char_p, P]
+        r.ref_tet_proj.argtypes = [I, P, P, P, P, P]
+        r.ref_tet_intgrt.argtypes = [I, P, P]
+        r.ref_tet_intgrtrst.argtypes = [I, P, P, P, P]
+        r.ref_tet_deriv.argtypes = [I, I, P, P]
+        _rt = r
+    return _rt
+
+
 def _p(a):
     return None if a is None or a.size == 0 else a.ctypes.data_as(ctypes.c_void_p)
 

@@ -1,11 +1,16 @@
 /*
  * Minimal container subset with the blitz++ names that the reference's
- * tri_basis sources use outside their BZ_DEBUG blocks: TinyVector, TinyMatrix
- * (fixed size, row-major) and Array<T,R> (R = 1..3, row-major, resizable).
+ * tri_basis and tet_basis sources use outside their BZ_DEBUG blocks: TinyVector,
+ * TinyMatrix (fixed size, row-major), Array<T,R> (R = 1..4, row-major,
+ * resizable, fill by scalar assignment) and Range::all() for the one column
+ * assignment tet_basis makes. Every allocation carries PAD spare elements: the
+ * reference's tet_basis::lumpinv writes idiag(0) for p < 4 where idiag has no
+ * element (blitz without bounds checks lets that pass), and the spare elements
+ * absorb such writes.
  *
  * TEST INFRASTRUCTURE ONLY. This header exists so that the reference's own
- * tri_basis/*.cpp files compile unmodified, where they lie, into the checker
- * library oracle/_ref/libtri_basis_ref.so. Nothing in the shipped library
+ * tri_basis/*.cpp and tet_basis/*.cpp files compile unmodified, where they lie,
+ * into the checker libraries under oracle/_ref/. Nothing in the shipped library
  * includes it.
  */
 #ifndef HPB_ORACLE_BLITZ_SHIM_H
@@ -52,27 +57,51 @@ public:
     }
 };
 
+struct Range {
+    static Range all() { return Range(); }
+};
+
 template <class T, int R>
 class Array {
+    static constexpr size_t PAD = 16;
     std::vector<T> v_;
-    int e_[3] = {0, 0, 0};
+    int e_[4] = {0, 0, 0, 0};
 
 public:
+    /* column view of a rank-2 array: a(Range::all(), j) = value */
+    struct Column {
+        Array *a;
+        int j;
+        Column &operator=(T v) {
+            for (int i = 0; i < a->e_[0]; ++i) (*a)(i, j) = v;
+            return *this;
+        }
+    };
+    Column operator()(Range, int j) { return Column{this, j}; }
+    Array &operator=(T v) {
+        for (size_t i = 0; i + PAD < v_.size(); ++i) v_[i] = v;
+        return *this;
+    }
     Array() {}
     explicit Array(int n0) { resize(n0); }
     Array(int n0, int n1) { resize(n0, n1); }
     Array(int n0, int n1, int n2) { resize(n0, n1, n2); }
+    Array(int n0, int n1, int n2, int n3) { resize(n0, n1, n2, n3); }
     void resize(int n0) {
-        e_[0] = n0; e_[1] = 1; e_[2] = 1;
-        v_.assign((size_t)n0, T());
+        e_[0] = n0; e_[1] = 1; e_[2] = 1; e_[3] = 1;
+        v_.assign((size_t)n0 + PAD, T());
     }
     void resize(int n0, int n1) {
-        e_[0] = n0; e_[1] = n1; e_[2] = 1;
-        v_.assign((size_t)n0 * n1, T());
+        e_[0] = n0; e_[1] = n1; e_[2] = 1; e_[3] = 1;
+        v_.assign((size_t)n0 * n1 + PAD, T());
     }
     void resize(int n0, int n1, int n2) {
-        e_[0] = n0; e_[1] = n1; e_[2] = n2;
-        v_.assign((size_t)n0 * n1 * n2, T());
+        e_[0] = n0; e_[1] = n1; e_[2] = n2; e_[3] = 1;
+        v_.assign((size_t)n0 * n1 * n2 + PAD, T());
+    }
+    void resize(int n0, int n1, int n2, int n3) {
+        e_[0] = n0; e_[1] = n1; e_[2] = n2; e_[3] = n3;
+        v_.assign((size_t)n0 * n1 * n2 * n3 + PAD, T());
     }
     int extent(int d) const { return e_[d]; }
     T &operator()(int i) { return v_[i]; }
@@ -81,6 +110,10 @@ public:
     const T &operator()(int i, int j) const { return v_[(size_t)i * e_[1] + j]; }
     T &operator()(int i, int j, int k) { return v_[((size_t)i * e_[1] + j) * e_[2] + k]; }
     const T &operator()(int i, int j, int k) const { return v_[((size_t)i * e_[1] + j) * e_[2] + k]; }
+    T &operator()(int i, int j, int k, int l) { return v_[(((size_t)i * e_[1] + j) * e_[2] + k) * e_[3] + l]; }
+    const T &operator()(int i, int j, int k, int l) const {
+        return v_[(((size_t)i * e_[1] + j) * e_[2] + k) * e_[3] + l];
+    }
     T *data() { return v_.data(); }
     const T *data() const { return v_.data(); }
 };

@@ -1,0 +1,70 @@
+"""The tet basis tables and dense operators (hp_tet_basis_build) against the
+reference's own tet_basis compiled here (oracle/_ref/libtet_basis_ref.so):
+1D tables of initialize_values / ptvalues_deriv, and the dense F / DX / DY / DZ /
+w and derivative operators against the reference's sum-factorised proj, intgrt,
+intgrtrst and derivr / derivs / derivt (tet_basis/proj.cpp, intgrt.cpp)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from hpb import tet as TB
+from oracle import oracle as O
+
+needs_ref = pytest.mark.skipif(O.ref_tet() is None, reason="oracle/_ref not built (reference tree absent)")
+
+
+def ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@needs_ref
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_tet_tables_match_reference(p):
+    r = O.ref_tet()
+    t = TB.tables(p)
+    sz = np.zeros(10, np.int32)
+    assert r.ref_tet_sizes(p, ptr(sz)) == 0
+    assert list(sz) == [t.p, t.em, t.fm, t.im, t.bm, t.T, t.nmodx, t.nmody, t.nmodz, t.G]
+    buf = np.zeros(4096)
+    for name in ("gx", "dgx", "gy", "dgy", "gz", "dgz", "wtx", "wty", "wtz", "xp", "yp", "zp", "x0", "y0", "y1",
+                 "z0", "dltx", "dlty", "dltz", "dltx2", "dltx3", "dlty2", "dlty3", "dltz2"):
+        n = r.ref_tet_get(p, name.encode(), ptr(buf))
+        mine = TB.arr(t, name)
+        assert n == mine.size, name
+        assert rel(mine.ravel(), buf[:n]) < 1e-13, name
+
+
+@needs_ref
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_tet_dense_operators_match_reference_sum_factorisation(p):
+    r = O.ref_tet()
+    t = TB.tables(p)
+    G, T = t.G, t.T
+    Q = G ** 3
+    F, DX, DY, DZ, w = (TB.arr(t, n) for n in ("F", "DX", "DY", "DZ", "w"))
+    rng = np.random.default_rng(p)
+    for _ in range(3):
+        lin = rng.uniform(-1, 1, T)
+        f, dx, dy, dz = (np.zeros(Q) for _ in range(4))
+        r.ref_tet_proj(p, ptr(lin), ptr(f), ptr(dx), ptr(dy), ptr(dz))
+        assert rel(F @ lin, f) < 1e-13
+        assert rel(DX @ lin, dx) < 1e-13
+        assert rel(DY @ lin, dy) < 1e-13
+        assert rel(DZ @ lin, dz) < 1e-13
+        g = [rng.uniform(-1, 1, Q) for _ in range(3)]
+        res = np.zeros(T)
+        r.ref_tet_intgrt(p, ptr(res), ptr(g[0]))
+        assert rel(F.T @ (w * g[0]), res) < 1e-13
+        res = np.zeros(T)
+        r.ref_tet_intgrtrst(p, ptr(res), ptr(g[0]), ptr(g[1]), ptr(g[2]))
+        mine = -(DX.T @ (w * g[0]) + DY.T @ (w * g[1]) + DZ.T @ (w * g[2]))  # intgrtrst subtracts
+        assert rel(mine, res) < 1e-13
+        for d in range(3):
+            out = np.zeros(Q)
+            r.ref_tet_deriv(p, d, ptr(g[d]), ptr(out))
+            assert rel(TB.deriv(t, d, g[d]), out) < 1e-13, d
