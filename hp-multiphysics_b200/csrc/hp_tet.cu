@@ -1,0 +1,633 @@
+// 3D (tet_hp) ins residual path on the GPU: context, preconditioner set-up (tau and
+// the diagonal element terms) and tet_hp::rsdl with tet_hp_ins::element_rsdl for
+// straight tetrahedra.
+//
+// Reference path (tet_hp/update.cpp:9-118, tet_hp/ins/rsdl.cpp:442-781,
+// tet_hp/ins/setup_preconditioner.cpp, tet_hp/gtol.cpp:16-82 and 815-873). The
+// basis operators are the dense per-point forms of tet_basis::proj / intgrtrst and
+// the 1D operators of derivr / derivs / derivt (include/hp_tet.h), pinned against
+// the reference's own tet_basis.
+//
+// Layout in HBM: one buffer per field (state, res, res_r) holding the vertex, edge,
+// face and interior sections back to back, each [entity][mode][4 variables]; the
+// dense operators (G^3 x T each) are read through the read-only path and stay in
+// L1 / L2. One warp per tetrahedron: lanes own quadrature points for the
+// projection and the pointwise fluxes and (variable, mode) pairs for the
+// integrations; the per-point arrays live in the warp's shared-memory slice.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hp_gpu.h"
+#include "hp_tet.h"
+
+namespace {
+
+thread_local std::string g_err;
+void set_err(const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+#define TCK(call)                                                                                    \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess) {                                                                     \
+            set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);     \
+            return HP_ECUDA;                                                                         \
+        }                                                                                            \
+    } while (0)
+
+constexpr int NV = 4;
+
+template <int P>
+struct TetCfg {
+    static constexpr int G = P + 1, Q = G * G * G, T = (P + 1) * (P + 2) * (P + 3) / 6;
+    static constexpr int EM = P - 1, FM = (P - 1) * (P - 2) / 2, IM = T - 4 - 6 * EM - 4 * FM;
+    static constexpr int BM = 4 + 6 * EM + 4 * FM;
+    static constexpr int WPC = 4;                 // warps (tetrahedra in flight) per CTA
+    static constexpr int QL = (Q + 31) / 32;      // quadrature points per lane
+    // per-warp scratch: uht [NV][T]; u [NV][Q]; cvi [3][3][Q]; c3 [3][Q]; df [3][3][Q]
+    static constexpr int S_WARP = NV * T + 25 * Q;
+};
+
+template <typename R, int P>
+struct TetSmall {  // by-value kernel parameter: the 1D derivative operators and factors
+    R Ax[P + 1][P + 1], Bx[P + 1][P + 1], Ay[P + 1][P + 1], By[P + 1][P + 1], Az[P + 1][P + 1];
+    R y0[P + 1], z0[P + 1];
+};
+
+template <typename R>
+struct TetOps {  // dense operators in device memory, row-major [q][m]; WD* = w * D*
+    const R *F, *DX, *DY, *DZ, *WDX, *WDY, *WDZ;
+};
+
+struct TetMeshD {
+    int npnt, nseg, ntri, ntet;
+    const double *pnts, *vol;
+    const int *tp, *ts, *tsg, *tt, *trot;
+};
+
+template <typename R>
+struct TetFields {
+    R *v, *e, *f, *i;
+};
+
+// The global location and sign of local mode m of tetrahedron tind (ugtouht / lftog).
+template <typename R, int P>
+__device__ __forceinline__ R *mode_slot(const TetMeshD &m, const TetFields<R> &g, int tind, int mode, int n,
+                                        R &sgn) {
+    using C = TetCfg<P>;
+    constexpr int EM = C::EM > 0 ? C::EM : 1, FM = C::FM > 0 ? C::FM : 1, IM = C::IM > 0 ? C::IM : 1;
+    sgn = (R)1;
+    if (mode < 4) return g.v + (size_t)m.tp[4 * tind + mode] * NV + n;
+    if (mode < 4 + 6 * C::EM) {
+        const int i = (mode - 4) / EM, k = (mode - 4) - i * EM;
+        if ((k & 1) && m.tsg[6 * tind + i] < 0) sgn = (R)-1;
+        return g.e + ((size_t)m.ts[6 * tind + i] * EM + k) * NV + n;
+    }
+    if (mode < C::BM) {
+        const int r = mode - 4 - 6 * C::EM, i = r / FM, idx = r - i * FM;
+        // row of face mode idx: rows 1 .. EM-1 hold EM-1, EM-2, ... modes
+        int row = 1, left = idx;
+        while (left >= C::EM - row) {
+            left -= C::EM - row;
+            ++row;
+        }
+        if (((row - 1) & 1) && m.trot[4 * tind + i] > 0) sgn = (R)-1;  // (-rot)^(row-1)
+        return g.f + ((size_t)m.tt[4 * tind + i] * FM + idx) * NV + n;
+    }
+    return g.i + ((size_t)tind * IM + (mode - C::BM)) * NV + n;
+}
+
+__device__ __forceinline__ void atomic_add_r(double *a, double v) { atomicAdd(a, v); }
+__device__ __forceinline__ void atomic_add_r(float *a, float v) { atomicAdd(a, v); }
+
+// tet_hp::rsdl element loop: res (imaginary terms) and res_r (beta-scaled real terms)
+template <typename R, int P>
+__global__ void __launch_bounds__(TetCfg<P>::WPC * 32)
+    k_tet_rsdl(TetOps<R> ops, TetSmall<R, P> sm, TetMeshD mesh, TetFields<R> ug, TetFields<R> res,
+               TetFields<R> rr, const R *__restrict__ tau, R rho, R mu, R beta) {
+    using C = TetCfg<P>;
+    constexpr int G = C::G, Q = C::Q, T = C::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    R *uht = reinterpret_cast<R *>(smem_raw) + warp * C::S_WARP;
+    R *u = uht + NV * T;   // [NV][Q]
+    R *cvi = u + NV * Q;   // [3][3][Q] convective + pressure fluxes
+    R *c3 = cvi + 9 * Q;   // [3][Q] continuity flux, then its SUPG term
+    R *df = c3 + 3 * Q;    // [3][3][Q] viscous flux, then viscous + SUPG
+    for (long tind = (long)blockIdx.x * C::WPC + warp; tind < mesh.ntet; tind += (long)gridDim.x * C::WPC) {
+        const int t = (int)tind;
+        for (int w = lane; w < NV * T; w += 32) {
+            const int n = w / T, m = w - n * T;
+            R s;
+            const R *src = mode_slot<R, P>(mesh, ug, t, m, n, s);
+            uht[n * T + m] = s * *src;
+        }
+        // straight element: ldcrd(n, .) = (v3 - v2, v1 - v2, v0 - v2) / 2
+        R ld[3][3];
+        {
+            const int v0 = mesh.tp[4 * t], v1 = mesh.tp[4 * t + 1], v2 = mesh.tp[4 * t + 2], v3 = mesh.tp[4 * t + 3];
+            for (int n = 0; n < 3; ++n) {
+                const double c2 = mesh.pnts[3 * v2 + n];
+                ld[n][0] = (R)(0.5 * (mesh.pnts[3 * v3 + n] - c2));
+                ld[n][1] = (R)(0.5 * (mesh.pnts[3 * v1 + n] - c2));
+                ld[n][2] = (R)(0.5 * (mesh.pnts[3 * v0 + n] - c2));
+            }
+        }
+        R d[3][3];
+        d[0][0] = ld[1][1] * ld[2][2] - ld[1][2] * ld[2][1];
+        d[0][1] = -ld[0][1] * ld[2][2] + ld[0][2] * ld[2][1];
+        d[0][2] = ld[0][1] * ld[1][2] - ld[0][2] * ld[1][1];
+        d[1][0] = -ld[1][0] * ld[2][2] + ld[1][2] * ld[2][0];
+        d[1][1] = ld[0][0] * ld[2][2] - ld[0][2] * ld[2][0];
+        d[1][2] = -ld[0][0] * ld[1][2] + ld[0][2] * ld[1][0];
+        d[2][0] = ld[1][0] * ld[2][1] - ld[1][1] * ld[2][0];
+        d[2][1] = -ld[0][0] * ld[2][1] + ld[0][1] * ld[2][0];
+        d[2][2] = ld[0][0] * ld[1][1] - ld[0][1] * ld[1][0];
+        const R cjcb = ld[0][0] * (ld[1][1] * ld[2][2] - ld[1][2] * ld[2][1]) -
+                       ld[0][1] * (ld[1][0] * ld[2][2] - ld[2][0] * ld[1][2]) +
+                       ld[0][2] * (ld[1][0] * ld[2][1] - ld[2][0] * ld[1][1]);
+        __syncwarp();
+        // ---- projection and pointwise fluxes (lanes own points)
+        for (int k = 0; k < C::QL; ++k) {
+            const int q = lane + 32 * k;
+            if (q >= Q) break;
+            R uu[NV] = {0, 0, 0, 0}, du[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            const R *fq = ops.F + (size_t)q * T, *xq = ops.DX + (size_t)q * T, *yq = ops.DY + (size_t)q * T,
+                    *zq = ops.DZ + (size_t)q * T;
+#pragma unroll 4
+            for (int m = 0; m < T; ++m) {
+                const R f = __ldg(fq + m);
+                const R a = __ldg(xq + m), b = __ldg(yq + m), c = __ldg(zq + m);
+#pragma unroll
+                for (int n = 0; n < NV; ++n) uu[n] += f * uht[n * T + m];
+#pragma unroll
+                for (int n = 0; n < 3; ++n) {
+                    const R x = uht[n * T + m];
+                    du[n][0] += a * x;
+                    du[n][1] += b * x;
+                    du[n][2] += c * x;
+                }
+            }
+#pragma unroll
+            for (int n = 0; n < NV; ++n) u[n * Q + q] = uu[n];
+            const R fx = rho * uu[0], fy = rho * uu[1], fz = rho * uu[2];
+            R f3[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                f3[c] = d[c][0] * fx + d[c][1] * fy + d[c][2] * fz;
+                c3[c * Q + q] = f3[c];
+            }
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) cvi[(n * 3 + c) * Q + q] = uu[n] * f3[c] + d[c][n] * uu[3];
+            if (beta > (R)0) {
+                // df(a,c) = sum_{b,e} visc(a,b)(c,e) du(b,e)  (rsdl.cpp:521-612, 632-670), with
+                // visc(a,a)(c,e) = -mu/J (sum_f d(c)(f) d(e)(f) + d(c)(a) d(e)(a)) and
+                // visc(a,b)(c,e) = -mu/J d(c)(b) d(e)(a) for b != a
+                const R cjcbi = mu / cjcb;
+                R h[3][3];  // h(b,a) = sum_e d(e)(a) du(b,e)
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) h[b][a] = d[0][a] * du[b][0] + d[1][a] * du[b][1] + d[2][a] * du[b][2];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        R s = (R)0;
+#pragma unroll
+                        for (int e = 0; e < 3; ++e) {
+                            const R gce = d[c][0] * d[e][0] + d[c][1] * d[e][1] + d[c][2] * d[e][2];
+                            s += gce * du[a][e];
+                        }
+                        s += d[c][0] * h[0][a] + d[c][1] * h[1][a] + d[c][2] * h[2][a];
+                        df[(a * 3 + c) * Q + q] = -cjcbi * s;
+                    }
+            }
+        }
+        __syncwarp();
+        // ---- imaginary terms: intgrtrst of (cvi, c3), scattered into res
+        for (int w = lane; w < NV * T; w += 32) {
+            const int n = w / T, m = w - n * T;
+            const R *fr = n < 3 ? cvi + (n * 3) * Q : c3;
+            R s = (R)0;
+            for (int q = 0; q < Q; ++q)
+                s += __ldg(ops.WDX + (size_t)q * T + m) * fr[q] + __ldg(ops.WDY + (size_t)q * T + m) * fr[Q + q] +
+                     __ldg(ops.WDZ + (size_t)q * T + m) * fr[2 * Q + q];
+            R sg;
+            R *dst = mode_slot<R, P>(mesh, res, t, m, n, sg);
+            if (m < C::BM) atomic_add_r(dst, -sg * s);
+            else *dst = -s;  // interiors: one writer, res cleared before
+        }
+        if (beta > (R)0) {
+            // ---- strong residual at the owned points: derivatives of the total fluxes
+            R rsd[C::QL][NV];
+            for (int k = 0; k < C::QL; ++k) {
+                const int q = lane + 32 * k;
+                if (q >= Q) break;
+                const int i = q / (G * G), j = (q / G) % G, kk = q % G;
+                const R yz = sm.y0[j] * sm.z0[kk], zz = sm.z0[kk];
+                for (int n = 0; n < NV; ++n) {
+                    // flux component c of variable n at point (i2, j2, k2)
+                    auto fl = [&](int c, int i2, int j2, int k2) -> R {
+                        const int q2 = (i2 * G + j2) * G + k2;
+                        return n < 3 ? cvi[(n * 3 + c) * Q + q2] + df[(n * 3 + c) * Q + q2] : c3[c * Q + q2];
+                    };
+                    R ax = 0, bxs = 0, bxt = 0, ays = 0, byt = 0, azt = 0;
+#pragma unroll
+                    for (int l = 0; l < G; ++l) {
+                        ax += sm.Ax[i][l] * fl(0, l, j, kk);
+                        bxs += sm.Bx[i][l] * fl(1, l, j, kk);
+                        bxt += sm.Bx[i][l] * fl(2, l, j, kk);
+                        ays += sm.Ay[j][l] * fl(1, i, l, kk);
+                        byt += sm.By[j][l] * fl(2, i, l, kk);
+                        azt += sm.Az[kk][l] * fl(2, i, j, l);
+                    }
+                    rsd[k][n] = yz * ax + (yz * bxs + zz * ays) + (yz * bxt + zz * byt + azt);
+                }
+            }
+            __syncwarp();
+            // ---- SUPG terms (rsdl.cpp:693-766), mesh velocity zero
+            const R tau0 = tau[2 * t], tau3 = tau[2 * t + 1];
+            for (int k = 0; k < C::QL; ++k) {
+                const int q = lane + 32 * k;
+                if (q >= Q) break;
+                R tr[NV], uq[3];
+#pragma unroll
+                for (int n = 0; n < 3; ++n) {
+                    tr[n] = tau0 * rsd[k][n];
+                    uq[n] = u[n * Q + q];
+                }
+                tr[3] = tau3 * rsd[k][3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        R s = d[c][a] * ((R)2 * uq[a]);
+#pragma unroll
+                        for (int b = 0; b < 3; ++b)
+                            if (b != a) s += d[c][b] * uq[b];
+                        R r = s * tr[a];
+#pragma unroll
+                        for (int b = 0; b < 3; ++b)
+                            if (b != a) r += d[c][b] * uq[a] * tr[b];
+                        r += d[c][a] * tr[3];
+                        df[(a * 3 + c) * Q + q] -= r;
+                    }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) c3[c * Q + q] = -d[c][0] * tr[0] - d[c][1] * tr[1] - d[c][2] * tr[2];
+            }
+            __syncwarp();
+            // ---- real terms: beta * intgrtrst of (df, c3), scattered into res_r
+            for (int w = lane; w < NV * T; w += 32) {
+                const int n = w / T, m = w - n * T;
+                const R *fr = n < 3 ? df + (n * 3) * Q : c3;
+                R s = (R)0;
+                for (int q = 0; q < Q; ++q)
+                    s += __ldg(ops.WDX + (size_t)q * T + m) * fr[q] + __ldg(ops.WDY + (size_t)q * T + m) * fr[Q + q] +
+                         __ldg(ops.WDZ + (size_t)q * T + m) * fr[2 * Q + q];
+                R sg;
+                R *dst = mode_slot<R, P>(mesh, rr, t, m, n, sg);
+                if (m < C::BM) atomic_add_r(dst, -beta * sg * s);
+                else *dst += -beta * s;
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// res = 0; res_r *= 1 - beta  (tet_hp::rsdl prologue)
+template <typename R>
+__global__ void k_tet_pre(long n, R *res, R *rr, R omb) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        res[k] = (R)0;
+        rr[k] *= omb;
+    }
+}
+
+// res += res_r
+template <typename R>
+__global__ void k_tet_fold(long n, R *res, const R *rr) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+        res[k] += rr[k];
+}
+
+// tet_hp_ins::setup_preconditioner, diagonal branch, steady, mesh velocity zero
+__global__ void k_tet_prcn(TetMeshD mesh, const double *ugv, double *tau, double *iprcn, double *vprcn,
+                           double *eprcn, double *fprcn, int p, int em, int fm, double rho, double mu, double adis,
+                           double bd0, int *err) {
+    const int VF[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};
+    const double nu = mu / rho;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mesh.ntet; t += gridDim.x * blockDim.x) {
+        double jcb = 0.125 * mesh.vol[t];
+        const int *v = mesh.tp + 4 * t;
+        double amin = 1.0e99, amax = 0.0;
+        for (int j = 0; j < 4; ++j) {
+            const double *a = mesh.pnts + 3 * v[VF[j][0]], *b = mesh.pnts + 3 * v[VF[j][1]],
+                         *c = mesh.pnts + 3 * v[VF[j][2]];
+            const double v1[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+            const double v2[3] = {a[0] - c[0], a[1] - c[1], a[2] - c[2]};
+            const double cr[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2],
+                                  v1[0] * v2[1] - v1[1] * v2[0]};
+            const double ar = .5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+            amax = ar > amax ? ar : amax;
+            amin = ar < amin ? ar : amin;
+        }
+        const double h = 4.0 * jcb / (0.25 * (p + 1) * (p + 1) * amax);
+        const double hmax = 4.0 * jcb / (0.25 * (p + 1) * (p + 1) * amin);
+        double qmax = 0.0;
+        for (int j = 0; j < 4; ++j) {
+            const double *uu = ugv + (size_t)v[j] * NV;
+            const double q = uu[0] * uu[0] + uu[1] * uu[1] + uu[2] * uu[2];
+            qmax = q > qmax ? q : qmax;
+        }
+        if (!(jcb > 0.0) || !(qmax >= 0.0)) atomicAdd(err, 1);
+        const double tm = 0.5 * hmax * bd0 + 2. * nu / hmax;
+        double gam = 3.0 * qmax + tm * tm;
+        if (mu + bd0 == 0.0) gam = gam > 0.1 ? gam : 0.1;
+        const double q = sqrt(qmax);
+        const double lam1 = q + sqrt(qmax + gam);
+        tau[2 * t] = adis * h / (jcb * sqrt(gam));
+        tau[2 * t + 1] = qmax * tau[2 * t];
+        jcb *= 2. * nu * (1. / (h * h) + 1. / (h * h) + 1. / (h * h)) + 3 * lam1 / h;
+        const double ip[NV] = {rho * jcb, rho * jcb, rho * jcb, jcb / gam};
+        for (int n = 0; n < NV; ++n) iprcn[(size_t)t * NV + n] = ip[n];
+        for (int i = 0; i < 4; ++i)
+            for (int n = 0; n < NV; ++n) atomicAdd(vprcn + (size_t)v[i] * NV + n, ip[n]);
+        if (em > 0)
+            for (int i = 0; i < 6; ++i)
+                for (int n = 0; n < NV; ++n) atomicAdd(eprcn + (size_t)mesh.ts[6 * t + i] * NV + n, ip[n]);
+        if (fm > 0)
+            for (int i = 0; i < 4; ++i)
+                for (int n = 0; n < NV; ++n) atomicAdd(fprcn + (size_t)mesh.tt[4 * t + i] * NV + n, ip[n]);
+    }
+}
+
+int nblk(long n, int b) { return (int)std::max<long>(1, (n + b - 1) / b); }
+
+}  // namespace
+
+struct hp_tet_ctx {
+    int device = 0, nsm = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int p = 0, em = 0, fm = 0, im = 0, T = 0, Q = 0;
+    hp_phys_params ph{};
+    TetMeshD mesh{};
+    size_t lv = 0, le = 0, lf = 0, li = 0, ltot = 0;  // section lengths (values)
+    std::vector<void *> allocs;
+    double *U = nullptr, *RES = nullptr, *RR = nullptr;  // [v | e | f | i]
+    double *tau = nullptr, *iprcn = nullptr, *vprcn = nullptr, *eprcn = nullptr, *fprcn = nullptr;
+    int *d_err = nullptr;
+    double *ops = nullptr;  // F, DX, DY, DZ, WDX, WDY, WDZ  [Q*T] each
+    hp_tet_tables tab{};
+    bool prcn_ready = false;
+    TetFields<double> fields(double *base) const {
+        return TetFields<double>{base, base + lv, base + lv + le, base + lv + le + lf};
+    }
+};
+
+namespace {
+
+int talloc(hp_tet_ctx *c, void **p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        set_err("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+        return HP_ECUDA;
+    }
+    c->allocs.push_back(*p);
+    return HP_OK;
+}
+
+template <int P>
+int launch_rsdl(hp_tet_ctx *c, int stage) {
+    using C = TetCfg<P>;
+    static_assert(C::S_WARP * C::WPC * 8 <= 227 * 1024, "scratch exceeds shared memory");
+    const size_t smem = (size_t)C::S_WARP * C::WPC * sizeof(double);
+    static bool attr_set = false;
+    if (!attr_set) {
+        TCK(cudaFuncSetAttribute(k_tet_rsdl<double, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    TetSmall<double, P> sm;
+    const hp_tet_tables &t = c->tab;
+    for (int i = 0; i <= P; ++i) {
+        for (int j = 0; j <= P; ++j) {
+            sm.Ax[i][j] = t.Ax[i][j];
+            sm.Bx[i][j] = t.Bx[i][j];
+            sm.Ay[i][j] = t.Ay[i][j];
+            sm.By[i][j] = t.By[i][j];
+            sm.Az[i][j] = t.Az[i][j];
+        }
+        sm.y0[i] = t.y0[i];
+        sm.z0[i] = t.z0[i];
+    }
+    const size_t qt = (size_t)C::Q * C::T;
+    TetOps<double> ops{c->ops, c->ops + qt, c->ops + 2 * qt, c->ops + 3 * qt, c->ops + 4 * qt, c->ops + 5 * qt,
+                       c->ops + 6 * qt};
+    const double omb = stage >= c->ph.nstage ? 0.0 : 1.0 - c->ph.beta[stage];
+    const double beta = c->ph.beta[stage];
+    k_tet_pre<double><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>((long)c->ltot, c->RES,
+                                                                                           c->RR, omb);
+    int blocks = std::min(nblk(c->mesh.ntet, C::WPC), c->nsm * 16);
+    k_tet_rsdl<double, P><<<blocks, C::WPC * 32, smem, c->stream>>>(ops, sm, c->mesh, c->fields(c->U),
+                                                                    c->fields(c->RES), c->fields(c->RR), c->tau,
+                                                                    c->ph.rho, c->ph.mu, beta);
+    k_tet_fold<double><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>((long)c->ltot, c->RES,
+                                                                                            c->RR);
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+}  // namespace
+
+extern "C" const char *hp_tet_last_error(void) { return g_err.c_str(); }
+
+extern "C" int hp_tet_create(const hp_tet_mesh_desc *m, const hp_tet_tables *b, const hp_phys_params *ph, int device,
+                             void *stream, hp_tet_ctx **out) {
+    if (!m || !b || !ph || !out || b->p < 1 || b->p > HP_TET_MAXP || m->ntet < 1) {
+        set_err("hp_tet_create: bad arguments");
+        return HP_EINVAL;
+    }
+    if (ph->physics != HP_PHYS_INS || ph->nstage < 1 || ph->nstage > 7) {
+        set_err("hp_tet_create: ins physics with 1..7 stages only");
+        return HP_EINVAL;
+    }
+    auto *c = new hp_tet_ctx;
+    if (device >= 0) TCK(cudaSetDevice(device));
+    TCK(cudaGetDevice(&c->device));
+    TCK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
+    if (stream) c->stream = (cudaStream_t)stream;
+    else {
+        TCK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    c->tab = *b;
+    c->p = b->p; c->em = b->em; c->fm = b->fm; c->im = b->im; c->T = b->T; c->Q = b->G * b->G * b->G;
+    c->ph = *ph;
+    c->lv = (size_t)m->npnt * NV; c->le = (size_t)m->nseg * c->em * NV;
+    c->lf = (size_t)m->ntri * c->fm * NV; c->li = (size_t)m->ntet * c->im * NV;
+    c->ltot = c->lv + c->le + c->lf + c->li;
+    int r;
+    void *p;
+    auto up = [&](const void *src, size_t bytes, void **dst) -> int {
+        if ((r = talloc(c, dst, bytes))) return r;
+        if (bytes) TCK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        return HP_OK;
+    };
+    TetMeshD &md = c->mesh;
+    md.npnt = m->npnt; md.nseg = m->nseg; md.ntri = m->ntri; md.ntet = m->ntet;
+    if ((r = up(m->pnts, 24 * (size_t)m->npnt, &p))) { hp_tet_destroy(c); return r; }
+    md.pnts = (const double *)p;
+    if ((r = up(m->vol, 8 * (size_t)m->ntet, &p))) { hp_tet_destroy(c); return r; }
+    md.vol = (const double *)p;
+    if ((r = up(m->tet_pnt, 16 * (size_t)m->ntet, &p))) { hp_tet_destroy(c); return r; }
+    md.tp = (const int *)p;
+    if ((r = up(m->tet_seg, 24 * (size_t)m->ntet, &p))) { hp_tet_destroy(c); return r; }
+    md.ts = (const int *)p;
+    if ((r = up(m->tet_sgn, 24 * (size_t)m->ntet, &p))) { hp_tet_destroy(c); return r; }
+    md.tsg = (const int *)p;
+    if ((r = up(m->tet_tri, 16 * (size_t)m->ntet, &p))) { hp_tet_destroy(c); return r; }
+    md.tt = (const int *)p;
+    if ((r = up(m->tet_rot, 16 * (size_t)m->ntet, &p))) { hp_tet_destroy(c); return r; }
+    md.trot = (const int *)p;
+    for (double **f : {&c->U, &c->RES, &c->RR}) {
+        if ((r = talloc(c, (void **)f, 8 * c->ltot))) { hp_tet_destroy(c); return r; }
+        TCK(cudaMemset(*f, 0, 8 * c->ltot));
+    }
+    if ((r = talloc(c, (void **)&c->tau, 16 * (size_t)m->ntet)) ||
+        (r = talloc(c, (void **)&c->iprcn, 32 * (size_t)m->ntet)) ||
+        (r = talloc(c, (void **)&c->vprcn, 32 * (size_t)m->npnt)) ||
+        (r = talloc(c, (void **)&c->eprcn, 32 * (size_t)m->nseg)) ||
+        (r = talloc(c, (void **)&c->fprcn, 32 * (size_t)m->ntri)) || (r = talloc(c, (void **)&c->d_err, 16))) {
+        hp_tet_destroy(c);
+        return r;
+    }
+    TCK(cudaMemset(c->tau, 0, 16 * (size_t)m->ntet));
+    // dense operators; WD* = w(q) * D*(q, m)
+    const int Q = c->Q, T = c->T;
+    std::vector<double> h((size_t)7 * Q * T);
+    for (int q = 0; q < Q; ++q)
+        for (int mm = 0; mm < T; ++mm) {
+            const size_t k = (size_t)q * T + mm, qt = (size_t)Q * T;
+            h[k] = b->F[q][mm];
+            h[qt + k] = b->DX[q][mm];
+            h[2 * qt + k] = b->DY[q][mm];
+            h[3 * qt + k] = b->DZ[q][mm];
+            h[4 * qt + k] = b->w[q] * b->DX[q][mm];
+            h[5 * qt + k] = b->w[q] * b->DY[q][mm];
+            h[6 * qt + k] = b->w[q] * b->DZ[q][mm];
+        }
+    if ((r = up(h.data(), 8 * h.size(), (void **)&c->ops))) { hp_tet_destroy(c); return r; }
+    *out = c;
+    return HP_OK;
+}
+
+extern "C" int hp_tet_destroy(hp_tet_ctx *c) {
+    if (!c) return HP_EINVAL;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void *p : c->allocs) cudaFree(p);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return HP_OK;
+}
+
+extern "C" int hp_tet_sync(hp_tet_ctx *c) {
+    if (!c) return HP_EINVAL;
+    TCK(cudaStreamSynchronize(c->stream));
+    return HP_OK;
+}
+
+static int copy_fields(hp_tet_ctx *c, double *dev, const double *v, const double *e, const double *f, const double *i,
+                       double *ov, double *oe, double *of, double *oi) {
+    const size_t len[4] = {c->lv, c->le, c->lf, c->li};
+    size_t off = 0;
+    const double *src[4] = {v, e, f, i};
+    double *dst[4] = {ov, oe, of, oi};
+    for (int k = 0; k < 4; ++k) {
+        if (len[k]) {
+            if (src[k]) TCK(cudaMemcpyAsync(dev + off, src[k], 8 * len[k], cudaMemcpyHostToDevice, c->stream));
+            if (dst[k]) TCK(cudaMemcpyAsync(dst[k], dev + off, 8 * len[k], cudaMemcpyDeviceToHost, c->stream));
+        }
+        off += len[k];
+    }
+    TCK(cudaStreamSynchronize(c->stream));
+    return HP_OK;
+}
+
+extern "C" int hp_tet_upload_state(hp_tet_ctx *c, const double *v, const double *e, const double *f, const double *i) {
+    if (!c || !v) return HP_EINVAL;
+    return copy_fields(c, c->U, v, e, f, i, nullptr, nullptr, nullptr, nullptr);
+}
+
+extern "C" int hp_tet_download_state(hp_tet_ctx *c, double *v, double *e, double *f, double *i) {
+    if (!c) return HP_EINVAL;
+    return copy_fields(c, c->U, nullptr, nullptr, nullptr, nullptr, v, e, f, i);
+}
+
+extern "C" int hp_tet_download_residual(hp_tet_ctx *c, int which, double *v, double *e, double *f, double *i) {
+    if (!c || which < 0 || which > 1) return HP_EINVAL;
+    return copy_fields(c, which ? c->RR : c->RES, nullptr, nullptr, nullptr, nullptr, v, e, f, i);
+}
+
+extern "C" int hp_tet_setup_preconditioner(hp_tet_ctx *c) {
+    if (!c) return HP_EINVAL;
+    TCK(cudaMemsetAsync(c->d_err, 0, 4, c->stream));
+    TCK(cudaMemsetAsync(c->vprcn, 0, 32 * (size_t)c->mesh.npnt, c->stream));
+    TCK(cudaMemsetAsync(c->eprcn, 0, 32 * (size_t)c->mesh.nseg, c->stream));
+    TCK(cudaMemsetAsync(c->fprcn, 0, 32 * (size_t)c->mesh.ntri, c->stream));
+    k_tet_prcn<<<std::min(nblk(c->mesh.ntet, 128), c->nsm * 16), 128, 0, c->stream>>>(
+        c->mesh, c->U, c->tau, c->iprcn, c->vprcn, c->eprcn, c->fprcn, c->p, c->em, c->fm, c->ph.rho, c->ph.mu,
+        c->ph.adis, c->ph.bd0, c->d_err);
+    TCK(cudaGetLastError());
+    int herr = 0;
+    TCK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream));
+    TCK(cudaStreamSynchronize(c->stream));
+    c->prcn_ready = true;
+    return herr;
+}
+
+extern "C" int hp_tet_download_prcn(hp_tet_ctx *c, double *tau, double *iprcn) {
+    if (!c || !tau || !iprcn) return HP_EINVAL;
+    TCK(cudaMemcpyAsync(tau, c->tau, 16 * (size_t)c->mesh.ntet, cudaMemcpyDeviceToHost, c->stream));
+    TCK(cudaMemcpyAsync(iprcn, c->iprcn, 32 * (size_t)c->mesh.ntet, cudaMemcpyDeviceToHost, c->stream));
+    TCK(cudaStreamSynchronize(c->stream));
+    return HP_OK;
+}
+
+extern "C" int hp_tet_enqueue_rsdl(hp_tet_ctx *c, int stage) {
+    if (!c || stage < 0 || stage > c->ph.nstage) return HP_EINVAL;
+    if (c->ph.beta[stage] > 0.0 && !c->prcn_ready) {
+        set_err("tet rsdl with beta > 0 needs tau from hp_tet_setup_preconditioner");
+        return HP_ESTATE;
+    }
+    switch (c->p) {
+        case 1: return launch_rsdl<1>(c, stage);
+        case 2: return launch_rsdl<2>(c, stage);
+        case 3: return launch_rsdl<3>(c, stage);
+        case 4: return launch_rsdl<4>(c, stage);
+    }
+    return HP_EINVAL;
+}
+
+extern "C" int hp_tet_rsdl(hp_tet_ctx *c, int stage) {
+    int r = hp_tet_enqueue_rsdl(c, stage);
+    if (r) return r;
+    return hp_tet_sync(c);
+}

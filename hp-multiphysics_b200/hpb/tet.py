@@ -64,3 +64,167 @@ def deriv(t, direction, f):
     if direction == 1:
         return (y0 * z0 * ax(arr(t, "Bx")) + z0 * ay(arr(t, "Ay"))).ravel()
     return (y0 * z0 * ax(arr(t, "Bx")) + z0 * ay(arr(t, "By")) + az(arr(t, "Az"))).ravel()
+
+
+def beltrami(X, Y, Z, re=100.0, a=np.pi / 4, d=np.pi / 2, t=0.0):
+    """The Ethier-Steinman 3D Beltrami solution of incompressible Navier-Stokes
+    (rho = 1, nu = 1/re): velocity (u, v, w) and pressure at time t."""
+    nu = 1.0 / re
+    e1 = np.exp(-nu * d * d * t)
+    u = -a * (np.exp(a * X) * np.sin(a * Y + d * Z) + np.exp(a * Z) * np.cos(a * X + d * Y)) * e1
+    v = -a * (np.exp(a * Y) * np.sin(a * Z + d * X) + np.exp(a * X) * np.cos(a * Y + d * Z)) * e1
+    w = -a * (np.exp(a * Z) * np.sin(a * X + d * Y) + np.exp(a * Y) * np.cos(a * Z + d * X)) * e1
+    p = -0.5 * a * a * (np.exp(2 * a * X) + np.exp(2 * a * Y) + np.exp(2 * a * Z) +
+                        2 * np.sin(a * X + d * Y) * np.cos(a * Z + d * X) * np.exp(a * (Y + Z)) +
+                        2 * np.sin(a * Y + d * Z) * np.cos(a * X + d * Y) * np.exp(a * (Z + X)) +
+                        2 * np.sin(a * Z + d * X) * np.cos(a * Y + d * Z) * np.exp(a * (X + Y))) * e1 * e1
+    return np.stack([u, v, w, p], axis=-1)
+
+
+class TetProblem:
+    """One tet_hp ins level: mesh (hpb.tetmesh.TetMesh), p <= 4, physics and the
+    modal state (vertices [npnt][4], edges [nseg][em][4], faces [ntri][fm][4],
+    interiors [ntet][im][4]; variables u, v, w, p)."""
+
+    NV = 4
+
+    def __init__(self, mesh, p, *, rho=1.0, mu=0.01, adis=1.0, nstage=5, alpha=None, beta=None, cfl=1.0):
+        from .problem import ALPHA_DFLT, BETA_DFLT
+        alpha = ALPHA_DFLT if alpha is None else alpha
+        beta = BETA_DFLT if beta is None else beta
+        self.mesh, self.p = mesh, p
+        self.tab = tables(p)
+        t = self.tab
+        ph = L.PhysParams()
+        ph.physics = L.HP_PHYS_INS
+        ph.nstage = nstage
+        for k in range(8):
+            ph.alpha[k] = alpha[k] if k < nstage else 1.0
+            ph.beta[k] = beta[k] if k < nstage else 1.0
+        ph.cfl, ph.bd0, ph.adis, ph.rho, ph.mu = cfl, 0.0, adis, rho, mu
+        self.phys = ph
+        self.ugv = np.zeros((mesh.npnt, 4))
+        self.uge = np.zeros((mesh.nseg, t.em, 4))
+        self.ugf = np.zeros((mesh.ntri, t.fm, 4))
+        self.ugi = np.zeros((mesh.ntet, t.im, 4))
+
+    @property
+    def state(self):
+        return self.ugv, self.uge, self.ugf, self.ugi
+
+    @property
+    def ndof(self):
+        return sum(a.size for a in self.state)
+
+    def set_beltrami(self, re=100.0, noise=1e-3, seed=20261209):
+        """Vertex values of the Beltrami field, high-order modes zero, plus seeded
+        U[-1,1) noise of amplitude `noise` on every coefficient."""
+        from .mesh import splitmix64_uniform
+        P = self.mesh.pnts
+        self.ugv[:] = beltrami(P[:, 0], P[:, 1], P[:, 2], re=re)
+        for a in (self.uge, self.ugf, self.ugi):
+            a[:] = 0.0
+        if noise:
+            n = self.ndof
+            r = splitmix64_uniform(seed, n) * noise
+            k = 0
+            for a in self.state:
+                a += r[k:k + a.size].reshape(a.shape)
+                k += a.size
+        return self
+
+
+class TetMeshDesc(ctypes.Structure):
+    _fields_ = [("npnt", _I), ("nseg", _I), ("ntri", _I), ("ntet", _I), ("pnts", ctypes.c_void_p),
+                ("tet_pnt", ctypes.c_void_p), ("tet_seg", ctypes.c_void_p), ("tet_sgn", ctypes.c_void_p),
+                ("tet_tri", ctypes.c_void_p), ("tet_rot", ctypes.c_void_p), ("vol", ctypes.c_void_p)]
+
+
+_bound = False
+
+
+def _bind():
+    global _bound
+    lib = L.lib()
+    if not _bound:
+        P = ctypes.c_void_p
+        lib.hp_tet_create.argtypes = [ctypes.POINTER(TetMeshDesc), ctypes.POINTER(TetTables),
+                                      ctypes.POINTER(L.PhysParams), _I, P, ctypes.POINTER(P)]
+        lib.hp_tet_destroy.argtypes = [P]
+        lib.hp_tet_upload_state.argtypes = [P, P, P, P, P]
+        lib.hp_tet_download_state.argtypes = [P, P, P, P, P]
+        lib.hp_tet_download_residual.argtypes = [P, _I, P, P, P, P]
+        lib.hp_tet_setup_preconditioner.argtypes = [P]
+        lib.hp_tet_download_prcn.argtypes = [P, P, P]
+        lib.hp_tet_enqueue_rsdl.argtypes = [P, _I]
+        lib.hp_tet_rsdl.argtypes = [P, _I]
+        lib.hp_tet_sync.argtypes = [P]
+        lib.hp_tet_last_error.restype = ctypes.c_char_p
+        _bound = True
+    return lib
+
+
+def _check(lib, rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed with status {rc}: {lib.hp_tet_last_error().decode()}")
+
+
+class TetGPU:
+    """A hp_tet_ctx for a TetProblem (the C ABI of include/hp_tet.h)."""
+
+    def __init__(self, prob, device=0, stream=None):
+        self.lib = lib = _bind()
+        self.prob = prob
+        m = prob.mesh
+        ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self._keep = m
+        self.desc = TetMeshDesc(m.npnt, m.nseg, m.ntri, m.ntet, ptr(m.pnts), ptr(m.tet_pnt), ptr(m.tet_seg),
+                                ptr(m.tet_sgn), ptr(m.tet_tri), ptr(m.tet_rot), ptr(m.vol))
+        h = ctypes.c_void_p()
+        _check(lib, lib.hp_tet_create(ctypes.byref(self.desc), ctypes.byref(prob.tab), ctypes.byref(prob.phys),
+                                      device, stream, ctypes.byref(h)), "hp_tet_create")
+        self.h = h
+        self.upload(*prob.state)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hp_tet_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    @staticmethod
+    def _p(a):
+        return None if a is None or a.size == 0 else a.ctypes.data_as(ctypes.c_void_p)
+
+    def upload(self, v, e, f, i):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (v, e, f, i)]
+        _check(self.lib, self.lib.hp_tet_upload_state(self.h, *[self._p(a) for a in arrs]), "upload")
+
+    def _out(self):
+        return [np.zeros_like(a) for a in self.prob.state]
+
+    def state(self):
+        out = self._out()
+        _check(self.lib, self.lib.hp_tet_download_state(self.h, *[self._p(a) for a in out]), "download_state")
+        return out
+
+    def residual(self, which=0):
+        out = self._out()
+        _check(self.lib, self.lib.hp_tet_download_residual(self.h, which, *[self._p(a) for a in out]),
+               "download_residual")
+        return out
+
+    def setup_preconditioner(self):
+        return self.lib.hp_tet_setup_preconditioner(self.h)
+
+    def prcn(self):
+        m = self.prob.mesh
+        tau = np.zeros((m.ntet, 2))
+        ip = np.zeros((m.ntet, 4))
+        _check(self.lib, self.lib.hp_tet_download_prcn(self.h, self._p(tau), self._p(ip)), "download_prcn")
+        return tau, ip
+
+    def rsdl(self, stage):
+        _check(self.lib, self.lib.hp_tet_rsdl(self.h, stage), "rsdl")

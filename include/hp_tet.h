@@ -62,6 +62,44 @@ typedef struct hp_tet_tables {
 /* Builds the tables for 1 <= p <= 4. Returns 0, or -1 for an unsupported p. */
 int hp_tet_basis_build(int p, hp_tet_tables *out);
 
+/* Tetrahedral mesh in the reference's conventions (tet_mesh/setup.cpp:14-374):
+ * pnts [npnt][3]; tet_pnt [ntet][4] (v0 < v1 by index, positively oriented);
+ * tet_seg / tet_sgn [ntet][6] (local edge i joins local vertices (2,3), (3,1),
+ * (2,1), (1,0), (2,0), (3,0)); tet_tri / tet_rot [ntet][4] (face i opposite vertex
+ * i, rot +1 in the tetrahedron that numbered the face, -1 in the other); vol
+ * [ntet] = |triple product| = 6 x volume (tet(tind).vol). */
+typedef struct hp_tet_mesh_desc {
+    int npnt, nseg, ntri, ntet;
+    const double *pnts;
+    const int *tet_pnt, *tet_seg, *tet_sgn, *tet_tri, *tet_rot;
+    const double *vol;
+} hp_tet_mesh_desc;
+
+typedef struct hp_tet_ctx hp_tet_ctx;
+struct hp_phys_params;
+
+/* One tet_hp ins level on one GPU (device < 0: the current one; stream NULL: a
+ * private stream). State and residual layouts, 4 variables (u, v, w, p):
+ * vertices [npnt][4], edges [nseg][em][4], faces [ntri][fm][4], interiors
+ * [ntet][im][4]; edge and face modes in the global orientation (tet_hp::ug). */
+int hp_tet_create(const hp_tet_mesh_desc *mesh, const hp_tet_tables *basis, const struct hp_phys_params *phys,
+                  int device, void *stream, hp_tet_ctx **out);
+int hp_tet_destroy(hp_tet_ctx *ctx);
+int hp_tet_upload_state(hp_tet_ctx *ctx, const double *ugv, const double *uge, const double *ugf, const double *ugi);
+int hp_tet_download_state(hp_tet_ctx *ctx, double *ugv, double *uge, double *ugf, double *ugi);
+/* which = 0: res (tet_hp::rsdl's output, res_r folded in); 1: res_r */
+int hp_tet_download_residual(hp_tet_ctx *ctx, int which, double *v, double *e, double *f, double *i);
+/* tet_hp_ins::setup_preconditioner (diagonal): tau and the element diagonals
+ * iprcn, summed into vertex / edge / face diagonals. Returns > 0 if an element has
+ * a non-positive volume or the state has NaNs. */
+int hp_tet_setup_preconditioner(hp_tet_ctx *ctx);
+int hp_tet_download_prcn(hp_tet_ctx *ctx, double *tau, double *iprcn); /* [ntet][2], [ntet][4] */
+/* tet_hp::rsdl(stage) (tet_hp/update.cpp:9-118): enqueue only / enqueue and wait */
+int hp_tet_enqueue_rsdl(hp_tet_ctx *ctx, int stage);
+int hp_tet_rsdl(hp_tet_ctx *ctx, int stage);
+int hp_tet_sync(hp_tet_ctx *ctx);
+const char *hp_tet_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,374 @@
+// CPU oracle of the 3D (tet_hp, ins) residual path. TEST INFRASTRUCTURE ONLY:
+// only tests/, __graft_entry__.smoke() and bench.py's CPU baseline use it.
+//
+// Restates, element by element in plain loops:
+//   tet_hp::rsdl                        tet_hp/update.cpp:9-118
+//   tet_hp::ugtouht / lftog             tet_hp/gtol.cpp:16-82, 815-873
+//   tet_hp_ins::element_rsdl (straight) tet_hp/ins/rsdl.cpp:442-781
+//   tet_hp_ins::setup_preconditioner    tet_hp/ins/setup_preconditioner.cpp (diagonal: tau, iprcn)
+// with the basis operators of tet_basis in the dense form of hp_tet_tables
+// (pinned against the reference's own proj / intgrt / intgrtrst / derivr / derivs /
+// derivt by tests/test_tet_basis_pin.py). Parity: the stages of the reference's
+// loops are kept; sums over points and modes run in the natural order.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../include/hp_gpu.h"
+#include "../include/hp_tet.h"
+
+namespace {
+
+constexpr int NV = 4;
+
+struct OT {
+    hp_tet_tables t;
+    hp_phys_params ph;
+    int npnt, nseg, ntri, ntet;
+    std::vector<double> pnts, vol;
+    std::vector<int> tp, ts, tsg, tt, trot;
+    std::vector<double> ugv, uge, ugf, ugi;           // state
+    std::vector<double> rv, re, rf, ri;               // res
+    std::vector<double> rrv, rre, rrf, rri;           // res_r
+    std::vector<double> tau;                          // [ntet][2]: tau(tind,0), tau(tind,NV-1)
+    std::vector<double> iprcn;                        // [ntet][NV]
+    std::vector<double> vprcn, eprcn, fprcn;          // accumulated diagonals
+};
+
+// the face vertices of local face i (tet_mesh/setup.cpp:307-310)
+const int VF[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};
+
+void gather(const OT &o, int tind, double uht[NV][HP_TET_MAXT]) {
+    const hp_tet_tables &t = o.t;
+    for (int i = 0; i < 4; ++i)
+        for (int n = 0; n < NV; ++n) uht[n][i] = o.ugv[(size_t)o.tp[4 * tind + i] * NV + n];
+    int cnt = 4;
+    for (int i = 0; i < 6; ++i) {
+        const int e = o.ts[6 * tind + i], sg = o.tsg[6 * tind + i];
+        int msgn = 1;
+        for (int m = 0; m < t.em; ++m, ++cnt) {
+            for (int n = 0; n < NV; ++n) uht[n][cnt] = msgn * o.uge[((size_t)e * t.em + m) * NV + n];
+            msgn *= sg;
+        }
+    }
+    for (int i = 0; i < 4; ++i) {
+        const int f = o.tt[4 * tind + i], sg = -o.trot[4 * tind + i];
+        int msgn = 1, indx = 0;
+        for (int m = 1; m <= t.em - 1; ++m) {
+            for (int k = 1; k <= t.em - m; ++k, ++cnt, ++indx)
+                for (int n = 0; n < NV; ++n) uht[n][cnt] = msgn * o.ugf[((size_t)f * t.fm + indx) * NV + n];
+            msgn *= sg;
+        }
+    }
+    for (int m = 0; m < t.im; ++m, ++cnt)
+        for (int n = 0; n < NV; ++n) uht[n][cnt] = o.ugi[((size_t)tind * t.im + m) * NV + n];
+}
+
+void scatter(const OT &o, int tind, const double lf[NV][HP_TET_MAXT], double *gv, double *ge, double *gf,
+             double *gi) {
+    const hp_tet_tables &t = o.t;
+    for (int i = 0; i < 4; ++i)
+        for (int n = 0; n < NV; ++n) gv[(size_t)o.tp[4 * tind + i] * NV + n] += lf[n][i];
+    int indx = 4;
+    for (int i = 0; i < 6; ++i) {
+        const int e = o.ts[6 * tind + i], sg = o.tsg[6 * tind + i];
+        int msgn = 1;
+        for (int m = 0; m < t.em; ++m, ++indx) {
+            for (int n = 0; n < NV; ++n) ge[((size_t)e * t.em + m) * NV + n] += msgn * lf[n][indx];
+            msgn *= sg;
+        }
+    }
+    for (int i = 0; i < 4; ++i) {
+        const int f = o.tt[4 * tind + i], sg = -o.trot[4 * tind + i];
+        int msgn = 1, gindx = 0;
+        for (int m = 1; m <= t.em - 1; ++m) {
+            for (int j = 1; j <= t.em - m; ++j, ++gindx, ++indx)
+                for (int n = 0; n < NV; ++n) gf[((size_t)f * t.fm + gindx) * NV + n] += msgn * lf[n][indx];
+            msgn *= sg;
+        }
+    }
+    for (int m = 0; m < t.im; ++m, ++indx)
+        for (int n = 0; n < NV; ++n) gi[((size_t)tind * t.im + m) * NV + n] += lf[n][indx];
+}
+
+// r(m) -= sum_q w (DX fr + DY fs + DZ ft)  (tet_basis::intgrtrst)
+void intgrtrst(const hp_tet_tables &t, double *r, const double *fr, const double *fs, const double *ft) {
+    const int Q = t.G * t.G * t.G;
+    for (int m = 0; m < t.T; ++m) {
+        double s = 0.0;
+        for (int q = 0; q < Q; ++q) s += t.w[q] * (t.DX[q][m] * fr[q] + t.DY[q][m] * fs[q] + t.DZ[q][m] * ft[q]);
+        r[m] -= s;
+    }
+}
+
+// dst += derivative `dir` (0 r, 1 s, 2 t) of point values f  (tet_basis::derivr/s/t)
+void deriv(const hp_tet_tables &t, int dir, const double *f, double *dst) {
+    const int G = t.G;
+    for (int i = 0; i < G; ++i)
+        for (int j = 0; j < G; ++j)
+            for (int k = 0; k < G; ++k) {
+                const int q = (i * G + j) * G + k;
+                double ax = 0.0, bx = 0.0, ay = 0.0, by = 0.0, az = 0.0;
+                for (int n = 0; n < G; ++n) {
+                    const double fx = f[(n * G + j) * G + k], fy = f[(i * G + n) * G + k], fz = f[(i * G + j) * G + n];
+                    ax += t.Ax[i][n] * fx;
+                    bx += t.Bx[i][n] * fx;
+                    ay += t.Ay[j][n] * fy;
+                    by += t.By[j][n] * fy;
+                    az += t.Az[k][n] * fz;
+                }
+                const double yz = t.y0[j] * t.z0[k], z = t.z0[k];
+                if (dir == 0) dst[q] += yz * ax;
+                else if (dir == 1) dst[q] += yz * bx + z * ay;
+                else dst[q] += yz * bx + z * by + az;
+            }
+}
+
+void element_rsdl(const OT &o, int tind, int stage, double lf_re[NV][HP_TET_MAXT], double lf_im[NV][HP_TET_MAXT]) {
+    const hp_tet_tables &t = o.t;
+    const int Q = t.G * t.G * t.G, T = t.T;
+    double uht[NV][HP_TET_MAXT];
+    gather(o, tind, uht);
+    // straight element: ldcrd(n, 0..2) = (v3 - v2, v1 - v2, v0 - v2) / 2
+    const int *v = &o.tp[4 * tind];
+    double ld[3][3];
+    for (int n = 0; n < 3; ++n) {
+        ld[n][0] = 0.5 * (o.pnts[3 * v[3] + n] - o.pnts[3 * v[2] + n]);
+        ld[n][1] = 0.5 * (o.pnts[3 * v[1] + n] - o.pnts[3 * v[2] + n]);
+        ld[n][2] = 0.5 * (o.pnts[3 * v[0] + n] - o.pnts[3 * v[2] + n]);
+    }
+    double d[3][3];
+    d[0][0] = ld[1][1] * ld[2][2] - ld[1][2] * ld[2][1];
+    d[0][1] = -ld[0][1] * ld[2][2] + ld[0][2] * ld[2][1];
+    d[0][2] = ld[0][1] * ld[1][2] - ld[0][2] * ld[1][1];
+    d[1][0] = -ld[1][0] * ld[2][2] + ld[1][2] * ld[2][0];
+    d[1][1] = ld[0][0] * ld[2][2] - ld[0][2] * ld[2][0];
+    d[1][2] = -ld[0][0] * ld[1][2] + ld[0][2] * ld[1][0];
+    d[2][0] = ld[1][0] * ld[2][1] - ld[1][1] * ld[2][0];
+    d[2][1] = -ld[0][0] * ld[2][1] + ld[0][1] * ld[2][0];
+    d[2][2] = ld[0][0] * ld[1][1] - ld[0][1] * ld[1][0];
+    const double cjcb = ld[0][0] * (ld[1][1] * ld[2][2] - ld[1][2] * ld[2][1]) -
+                        ld[0][1] * (ld[1][0] * ld[2][2] - ld[2][0] * ld[1][2]) +
+                        ld[0][2] * (ld[1][0] * ld[2][1] - ld[2][0] * ld[1][1]);
+    const double beta = o.ph.beta[stage], rho = o.ph.rho;
+    // proj (with r, s, t derivatives of u, v, w when beta > 0)
+    std::vector<double> u(NV * Q, 0.0), du(NV * 3 * Q, 0.0);
+    auto U = [&](int n, int q) -> double & { return u[n * Q + q]; };
+    auto DU = [&](int n, int c, int q) -> double & { return du[(n * 3 + c) * Q + q]; };
+    for (int q = 0; q < Q; ++q)
+        for (int n = 0; n < NV; ++n) {
+            double f = 0, dr = 0, ds = 0, dt = 0;
+            for (int m = 0; m < T; ++m) {
+                f += t.F[q][m] * uht[n][m];
+                dr += t.DX[q][m] * uht[n][m];
+                ds += t.DY[q][m] * uht[n][m];
+                dt += t.DZ[q][m] * uht[n][m];
+            }
+            U(n, q) = f;
+            if (beta > 0.0 && n < NV - 1) { DU(n, 0, q) = dr; DU(n, 1, q) = ds; DU(n, 2, q) = dt; }
+        }
+    for (int n = 0; n < NV; ++n)
+        for (int m = 0; m < T; ++m) lf_re[n][m] = lf_im[n][m] = 0.0;
+    // convective, continuity and pressure fluxes (imaginary part)
+    std::vector<double> cv(3 * 3 * Q), df(3 * 3 * Q), res(NV * Q);
+    auto CV = [&](int n, int c, int q) -> double & { return cv[(n * 3 + c) * Q + q]; };
+    auto DF = [&](int n, int c, int q) -> double & { return df[(n * 3 + c) * Q + q]; };
+    for (int q = 0; q < Q; ++q) {
+        const double fx = rho * U(0, q), fy = rho * U(1, q), fz = rho * U(2, q);
+        for (int c = 0; c < 3; ++c) DU(NV - 1, c, q) = d[c][0] * fx + d[c][1] * fy + d[c][2] * fz;
+        for (int n = 0; n < NV - 1; ++n)
+            for (int c = 0; c < 3; ++c) CV(n, c, q) = U(n, q) * DU(NV - 1, c, q) + d[c][n] * U(NV - 1, q);
+    }
+    for (int n = 0; n < NV - 1; ++n) intgrtrst(t, lf_im[n], &CV(n, 0, 0), &CV(n, 1, 0), &CV(n, 2, 0));
+    intgrtrst(t, lf_im[NV - 1], &DU(NV - 1, 0, 0), &DU(NV - 1, 1, 0), &DU(NV - 1, 2, 0));
+    if (!(beta > 0.0)) return;
+    // viscous tensor visc(a,b)(c,e) (rsdl.cpp:521-612)
+    const double cjcbi = o.ph.mu / cjcb;
+    double visc[3][3][3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+            for (int c = 0; c < 3; ++c)
+                for (int e = 0; e < 3; ++e) {
+                    if (a == b) {
+                        double s = d[c][a] * d[e][a];
+                        for (int f = 0; f < 3; ++f) s += d[c][f] * d[e][f];
+                        visc[a][b][c][e] = -cjcbi * s;
+                    } else {
+                        visc[a][b][c][e] = -cjcbi * d[c][b] * d[e][a];
+                    }
+                }
+    // steady: res = rho*bd0*cjcb*u + dugdt = 0, intgrt of it into lf_re = 0
+    for (int q = 0; q < Q; ++q) {
+        for (int n = 0; n < NV; ++n) res[n * Q + q] = 0.0;
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 3; ++c) {
+                double s = 0.0;
+                for (int b = 0; b < 3; ++b)
+                    for (int e = 0; e < 3; ++e) s += visc[a][b][c][e] * DU(b, e, q);
+                DF(a, c, q) = s;
+                CV(a, c, q) += s;
+            }
+    }
+    // strong residual: derivatives of the total fluxes
+    for (int n = 0; n < NV - 1; ++n)
+        for (int c = 0; c < 3; ++c) deriv(t, c, &CV(n, c, 0), &res[n * Q]);
+    for (int c = 0; c < 3; ++c) deriv(t, c, &DU(NV - 1, c, 0), &res[(NV - 1) * Q]);
+    // SUPG (rsdl.cpp:693-766), mesh velocity zero
+    const double tau0 = o.tau[2 * tind], tau3 = o.tau[2 * tind + 1];
+    for (int q = 0; q < Q; ++q) {
+        double tr[NV];
+        for (int n = 0; n < NV - 1; ++n) tr[n] = tau0 * res[n * Q + q];
+        tr[NV - 1] = tau3 * res[(NV - 1) * Q + q];
+        for (int a = 0; a < 3; ++a)
+            for (int c = 0; c < 3; ++c) {
+                double s = d[c][a] * (2.0 * U(a, q));
+                for (int b = 0; b < 3; ++b)
+                    if (b != a) s += d[c][b] * U(b, q);
+                double r = s * tr[a];
+                for (int b = 0; b < 3; ++b)
+                    if (b != a) r += d[c][b] * U(a, q) * tr[b];
+                r += d[c][a] * tr[NV - 1];
+                DF(a, c, q) -= r;
+            }
+        for (int c = 0; c < 3; ++c) DU(NV - 1, c, q) = -d[c][0] * tr[0] - d[c][1] * tr[1] - d[c][2] * tr[2];
+    }
+    for (int n = 0; n < NV - 1; ++n) intgrtrst(t, lf_re[n], &DF(n, 0, 0), &DF(n, 1, 0), &DF(n, 2, 0));
+    intgrtrst(t, lf_re[NV - 1], &DU(NV - 1, 0, 0), &DU(NV - 1, 1, 0), &DU(NV - 1, 2, 0));
+    for (int n = 0; n < NV; ++n)
+        for (int m = 0; m < T; ++m) lf_re[n][m] *= beta;
+}
+
+}  // namespace
+
+extern "C" {
+
+void *ot_create(const hp_tet_tables *t, const hp_phys_params *ph, int npnt, int nseg, int ntri, int ntet,
+                const double *pnts, const int *tet_pnt, const int *tet_seg, const int *tet_sgn, const int *tet_tri,
+                const int *tet_rot, const double *vol) {
+    OT *o = new OT;
+    o->t = *t;
+    o->ph = *ph;
+    o->npnt = npnt; o->nseg = nseg; o->ntri = ntri; o->ntet = ntet;
+    o->pnts.assign(pnts, pnts + 3 * (size_t)npnt);
+    o->vol.assign(vol, vol + ntet);
+    o->tp.assign(tet_pnt, tet_pnt + 4 * (size_t)ntet);
+    o->ts.assign(tet_seg, tet_seg + 6 * (size_t)ntet);
+    o->tsg.assign(tet_sgn, tet_sgn + 6 * (size_t)ntet);
+    o->tt.assign(tet_tri, tet_tri + 4 * (size_t)ntet);
+    o->trot.assign(tet_rot, tet_rot + 4 * (size_t)ntet);
+    const size_t lv = (size_t)npnt * NV, le = (size_t)nseg * t->em * NV, lf = (size_t)ntri * t->fm * NV,
+                 li = (size_t)ntet * t->im * NV;
+    for (auto *a : {&o->ugv, &o->rv, &o->rrv}) a->assign(lv, 0.0);
+    for (auto *a : {&o->uge, &o->re, &o->rre}) a->assign(le, 0.0);
+    for (auto *a : {&o->ugf, &o->rf, &o->rrf}) a->assign(lf, 0.0);
+    for (auto *a : {&o->ugi, &o->ri, &o->rri}) a->assign(li, 0.0);
+    o->tau.assign(2 * (size_t)ntet, 0.0);
+    o->iprcn.assign(NV * (size_t)ntet, 0.0);
+    o->vprcn.assign(lv, 0.0);
+    o->eprcn.assign((size_t)nseg * NV, 0.0);
+    o->fprcn.assign((size_t)ntri * NV, 0.0);
+    return o;
+}
+
+void ot_destroy(void *h) { delete static_cast<OT *>(h); }
+
+void ot_set_state(void *h, const double *v, const double *e, const double *f, const double *i) {
+    OT &o = *static_cast<OT *>(h);
+    std::memcpy(o.ugv.data(), v, o.ugv.size() * 8);
+    if (!o.uge.empty()) std::memcpy(o.uge.data(), e, o.uge.size() * 8);
+    if (!o.ugf.empty()) std::memcpy(o.ugf.data(), f, o.ugf.size() * 8);
+    if (!o.ugi.empty()) std::memcpy(o.ugi.data(), i, o.ugi.size() * 8);
+}
+
+// which: 0 res, 1 res_r, 2 state
+void ot_get(void *h, int which, double *v, double *e, double *f, double *i) {
+    OT &o = *static_cast<OT *>(h);
+    const std::vector<double> *a[4];
+    if (which == 0) { a[0] = &o.rv; a[1] = &o.re; a[2] = &o.rf; a[3] = &o.ri; }
+    else if (which == 1) { a[0] = &o.rrv; a[1] = &o.rre; a[2] = &o.rrf; a[3] = &o.rri; }
+    else { a[0] = &o.ugv; a[1] = &o.uge; a[2] = &o.ugf; a[3] = &o.ugi; }
+    double *dst[4] = {v, e, f, i};
+    for (int k = 0; k < 4; ++k)
+        if (dst[k] && !a[k]->empty()) std::memcpy(dst[k], a[k]->data(), a[k]->size() * 8);
+}
+
+// tau [ntet][2], iprcn [ntet][4]
+void ot_get_prcn(void *h, double *tau, double *iprcn) {
+    OT &o = *static_cast<OT *>(h);
+    std::memcpy(tau, o.tau.data(), o.tau.size() * 8);
+    std::memcpy(iprcn, o.iprcn.data(), o.iprcn.size() * 8);
+}
+
+// tet_hp_ins::setup_preconditioner, diagonal branch, steady (bd0 = 0), mesh velocity 0
+int ot_setup_preconditioner(void *h) {
+    OT &o = *static_cast<OT *>(h);
+    const double nu = o.ph.mu / o.ph.rho;
+    const int p = o.t.p;
+    int err = 0;
+    std::fill(o.vprcn.begin(), o.vprcn.end(), 0.0);
+    std::fill(o.eprcn.begin(), o.eprcn.end(), 0.0);
+    std::fill(o.fprcn.begin(), o.fprcn.end(), 0.0);
+    for (int tind = 0; tind < o.ntet; ++tind) {
+        double jcb = 0.125 * o.vol[tind];
+        const int *v = &o.tp[4 * tind];
+        double amin = 1.0e99, amax = 0.0;
+        for (int j = 0; j < 4; ++j) {
+            const double *a = &o.pnts[3 * v[VF[j][0]]], *b = &o.pnts[3 * v[VF[j][1]]], *c = &o.pnts[3 * v[VF[j][2]]];
+            const double v1[3] = {a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+            const double v2[3] = {a[0] - c[0], a[1] - c[1], a[2] - c[2]};
+            const double cr[3] = {v1[1] * v2[2] - v1[2] * v2[1], v1[2] * v2[0] - v1[0] * v2[2],
+                                  v1[0] * v2[1] - v1[1] * v2[0]};
+            const double ar = .5 * std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+            amax = ar > amax ? ar : amax;
+            amin = ar < amin ? ar : amin;
+        }
+        const double h = 4.0 * jcb / (0.25 * (p + 1) * (p + 1) * amax);
+        const double hmax = 4.0 * jcb / (0.25 * (p + 1) * (p + 1) * amin);
+        double qmax = 0.0;
+        for (int j = 0; j < 4; ++j) {
+            const double *uu = &o.ugv[(size_t)v[j] * NV];
+            const double q = uu[0] * uu[0] + uu[1] * uu[1] + uu[2] * uu[2];
+            qmax = q > qmax ? q : qmax;
+        }
+        if (!(jcb > 0.0) || !(qmax >= 0.0)) err = 1;
+        double gam = 3.0 * qmax + (0.5 * hmax * o.ph.bd0 + 2. * nu / hmax) * (0.5 * hmax * o.ph.bd0 + 2. * nu / hmax);
+        if (o.ph.mu + o.ph.bd0 == 0.0) gam = gam > 0.1 ? gam : 0.1;
+        const double q = std::sqrt(qmax);
+        const double lam1 = q + std::sqrt(qmax + gam);
+        o.tau[2 * tind] = o.ph.adis * h / (jcb * std::sqrt(gam));
+        o.tau[2 * tind + 1] = qmax * o.tau[2 * tind];
+        jcb *= 2. * nu * (1. / (h * h) + 1. / (h * h) + 1. / (h * h)) + 3 * lam1 / h;
+        double ip[NV] = {o.ph.rho * jcb, o.ph.rho * jcb, o.ph.rho * jcb, jcb / gam};
+        for (int n = 0; n < NV; ++n) o.iprcn[(size_t)tind * NV + n] = ip[n];
+        for (int i = 0; i < 4; ++i)
+            for (int n = 0; n < NV; ++n) o.vprcn[(size_t)v[i] * NV + n] += ip[n];
+        if (o.t.em > 0)
+            for (int i = 0; i < 6; ++i)
+                for (int n = 0; n < NV; ++n) o.eprcn[(size_t)o.ts[6 * tind + i] * NV + n] += ip[n];
+        if (o.t.fm > 0)
+            for (int i = 0; i < 4; ++i)
+                for (int n = 0; n < NV; ++n) o.fprcn[(size_t)o.tt[4 * tind + i] * NV + n] += ip[n];
+    }
+    return err;
+}
+
+// tet_hp::rsdl (update.cpp:9-118) without boundary fluxes and coarse-level terms
+void ot_rsdl(void *h, int stage) {
+    OT &o = *static_cast<OT *>(h);
+    const double omb = 1.0 - o.ph.beta[stage];
+    for (auto *a : {&o.rv, &o.re, &o.rf, &o.ri}) std::fill(a->begin(), a->end(), 0.0);
+    for (auto *a : {&o.rrv, &o.rre, &o.rrf, &o.rri})
+        for (auto &x : *a) x *= omb;
+    double lf_re[NV][HP_TET_MAXT], lf_im[NV][HP_TET_MAXT];
+    for (int tind = 0; tind < o.ntet; ++tind) {
+        element_rsdl(o, tind, stage, lf_re, lf_im);
+        scatter(o, tind, lf_im, o.rv.data(), o.re.data(), o.rf.data(), o.ri.data());
+        scatter(o, tind, lf_re, o.rrv.data(), o.rre.data(), o.rrf.data(), o.rri.data());
+    }
+    for (size_t k = 0; k < o.rv.size(); ++k) o.rv[k] += o.rrv[k];
+    for (size_t k = 0; k < o.re.size(); ++k) o.re[k] += o.rre[k];
+    for (size_t k = 0; k < o.rf.size(); ++k) o.rf[k] += o.rrf[k];
+    for (size_t k = 0; k < o.ri.size(); ++k) o.ri[k] += o.rri[k];
+}
+
+}  // extern "C"

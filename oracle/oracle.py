@@ -51,6 +51,15 @@ def lib():
         o.or_basis_proj1d.argtypes = [P, P, P, P]
         o.or_basis_intgrt1d.argtypes = [P, P, P]
         o.or_dpbtrsnu2.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int]
+        I = ctypes.c_int
+        o.ot_create.restype = P
+        o.ot_create.argtypes = [P, P, I, I, I, I, P, P, P, P, P, P, P]
+        o.ot_destroy.argtypes = [P]
+        o.ot_set_state.argtypes = [P, P, P, P, P]
+        o.ot_get.argtypes = [P, I, P, P, P, P]
+        o.ot_get_prcn.argtypes = [P, P, P]
+        o.ot_setup_preconditioner.argtypes = [P]
+        o.ot_rsdl.argtypes = [P, I]
         _o = o
     return _o
 
@@ -158,3 +167,52 @@ class Oracle:
     def maxres(self):
         out = np.zeros(self.prob.NV)
         return self.o.or_maxres(self.h, _p(out)), out
+
+
+class OracleTet:
+    """CPU restatement of the tet ins residual path (hp_oracle_tet.cpp) for a
+    hpb.tet.TetProblem. Test infrastructure only."""
+
+    def __init__(self, prob):
+        o = lib()
+        m = prob.mesh
+        self.prob = prob
+        self.h = o.ot_create(ctypes.byref(prob.tab), ctypes.byref(prob.phys), m.npnt, m.nseg, m.ntri, m.ntet,
+                             _p(m.pnts), _p(m.tet_pnt), _p(m.tet_seg), _p(m.tet_sgn), _p(m.tet_tri), _p(m.tet_rot),
+                             _p(m.vol))
+        self.set_state(*prob.state)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ot_destroy(self.h)
+            self.h = None
+
+    def set_state(self, v, e, f, i):
+        lib().ot_set_state(self.h, _p(v), _p(e), _p(f), _p(i))
+
+    def _get(self, which):
+        out = [np.zeros_like(a) for a in self.prob.state]
+        lib().ot_get(self.h, which, *[_p(a) for a in out])
+        return out
+
+    def residual(self):
+        return self._get(0)
+
+    def residual_r(self):
+        return self._get(1)
+
+    def state(self):
+        return self._get(2)
+
+    def setup_preconditioner(self):
+        return lib().ot_setup_preconditioner(self.h)
+
+    def prcn(self):
+        m = self.prob.mesh
+        tau = np.zeros((m.ntet, 2))
+        ip = np.zeros((m.ntet, 4))
+        lib().ot_get_prcn(self.h, _p(tau), _p(ip))
+        return tau, ip
+
+    def rsdl(self, stage):
+        lib().ot_rsdl(self.h, stage)

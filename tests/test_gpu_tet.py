@@ -1,0 +1,35 @@
+"""The tet_hp ins residual on the GPU (include/hp_tet.h) against the CPU oracle
+(oracle/hp_oracle_tet.cpp): tau and the element diagonals of
+tet_hp_ins::setup_preconditioner, and tet_hp::rsdl (res and res_r) at every kind of
+stage, p = 1..4, on a cube of 3^3 x 6 tetrahedra with a Beltrami state plus noise.
+The GPU sums points and modes in another order than the oracle: 1e-12 of max|oracle|."""
+import numpy as np
+import pytest
+
+from hpb.tet import TetGPU, TetProblem
+from hpb.tetmesh import cube_tets
+from oracle.oracle import OracleTet
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    a = np.concatenate([np.ravel(x) for x in a])
+    b = np.concatenate([np.ravel(x) for x in b])
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_tet_rsdl_matches_oracle(p):
+    pr = TetProblem(cube_tets(3), p, mu=0.01).set_beltrami()
+    g, o = TetGPU(pr), OracleTet(pr)
+    assert g.setup_preconditioner() == 0 and o.setup_preconditioner() == 0
+    gt, gi = g.prcn()
+    ot, oi = o.prcn()
+    assert relerr([gt, gi], [ot, oi]) < 1e-13
+    for stage in (pr.phys.nstage, 0, 1, 2):
+        g.rsdl(stage)
+        o.rsdl(stage)
+        assert relerr(g.residual(), o.residual()) < 1e-12, f"res stage {stage}"
+        assert relerr(g.residual(1), o.residual_r()) < 1e-12, f"res_r stage {stage}"
+    g.close()
