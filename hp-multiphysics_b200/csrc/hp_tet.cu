@@ -310,6 +310,295 @@ __global__ void __launch_bounds__(TetCfg<P>::WPC * 32)
     }
 }
 
+// FP64 tensor-core (DMMA, mma.m8n8k4.f64) form of k_tet_rsdl: one warp takes two
+// tetrahedra, so the 8 rows of an A fragment are (tetrahedron, variable) pairs.
+//   projection:  C[8 x Q] = U[8 x T] * Op^T[T x Q]   for Op = F, DX, DY, DZ
+//   intgrtrst:   C[8 x T] = Flux[8 x 3Q] * WD[3Q x T] (WD = w * (DX; DY; DZ))
+// The B operands are constant: the host stores them in fragment order (one 8-byte
+// coalesced load per lane per MMA). The pointwise fluxes, the strong residual and
+// the SUPG terms stay scalar, lanes owning (tetrahedron, point) pairs.
+template <int P>
+struct TetMma {
+    using C = TetCfg<P>;
+    static constexpr int KS = (C::T + 3) / 4;        // projection k-steps
+    static constexpr int NT = (C::Q + 7) / 8;        // projection n-tiles
+    static constexpr int KS2 = (3 * C::Q + 3) / 4;   // intgrtrst k-steps
+    static constexpr int NT2 = (C::T + 7) / 8;       // intgrtrst n-tiles
+    static constexpr int WPC = 2;
+    // strides padded to 4 (mod 16) doubles: the 4 rows (variables) a half-warp reads
+    // in one fragment load fall on distinct shared-memory banks
+    static constexpr int pad4(int x) { return x + ((4 - x % 16) + 16) % 16; }
+    static constexpr int QP = pad4(C::Q);       // u [NV][QP]
+    static constexpr int VS = pad4(3 * C::Q);   // fim / fre [NV][VS], component c at c * Q
+    // per tetrahedron: uht [NV][T], u [NV][QP], fim [NV][VS], fre [NV][VS]
+    static constexpr int S_EL = NV * C::T + NV * QP + 2 * NV * VS;
+    static constexpr int NG = NT < 8 ? NT : 8;  // projection n-tiles accumulated together
+    static constexpr int S_WARP = 2 * S_EL;
+    static constexpr size_t PROJ_LEN = (size_t)4 * NT * KS * 32, INT_LEN = (size_t)NT2 * KS2 * 32;
+};
+
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <int P>
+__global__ void __launch_bounds__(TetMma<P>::WPC * 32)
+    k_tet_rsdl_mma(const double *__restrict__ projB, const double *__restrict__ intB, TetSmall<double, P> sm,
+                   TetMeshD mesh, TetFields<double> ug, TetFields<double> res, TetFields<double> rr,
+                   const double *__restrict__ tau, double rho, double mu, double beta) {
+    using C = TetCfg<P>;
+    using M = TetMma<P>;
+    constexpr int G = C::G, Q = C::Q, T = C::T;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grow = lane >> 2, gcol = lane & 3;  // fragment row / column group
+    double *base = reinterpret_cast<double *>(smem_raw) + warp * M::S_WARP;
+    constexpr int QP = M::QP, VS = M::VS;
+    auto UHT = [&](int e) { return base + e * M::S_EL; };
+    auto UQ = [&](int e) { return base + e * M::S_EL + NV * T; };
+    auto FIM = [&](int e) { return base + e * M::S_EL + NV * T + NV * QP; };
+    auto FRE = [&](int e) { return base + e * M::S_EL + NV * T + NV * QP + NV * VS; };
+    const long npair = ((long)mesh.ntet + 1) / 2;
+    for (long pr = (long)blockIdx.x * M::WPC + warp; pr < npair; pr += (long)gridDim.x * M::WPC) {
+        const int t0 = (int)(2 * pr);
+        const bool has1 = t0 + 1 < mesh.ntet;
+        // ---- gather both tetrahedra (a missing second one gets zeros)
+        for (int w = lane; w < 2 * NV * T; w += 32) {
+            const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
+            double v = 0.0;
+            if (e == 0 || has1) {
+                double s;
+                const double *src = mode_slot<double, P>(mesh, ug, t0 + e, m, n, s);
+                v = s * *src;
+            }
+            UHT(e)[n * T + m] = v;
+        }
+        // geometry of both (the missing one repeats the first)
+        double d[2][3][3], cj[2];
+        for (int e = 0; e < 2; ++e) {
+            const int t = (e == 1 && has1) ? t0 + 1 : t0;
+            const int v0 = mesh.tp[4 * t], v1 = mesh.tp[4 * t + 1], v2 = mesh.tp[4 * t + 2], v3 = mesh.tp[4 * t + 3];
+            double ld[3][3];
+            for (int n = 0; n < 3; ++n) {
+                const double c2 = mesh.pnts[3 * v2 + n];
+                ld[n][0] = 0.5 * (mesh.pnts[3 * v3 + n] - c2);
+                ld[n][1] = 0.5 * (mesh.pnts[3 * v1 + n] - c2);
+                ld[n][2] = 0.5 * (mesh.pnts[3 * v0 + n] - c2);
+            }
+            d[e][0][0] = ld[1][1] * ld[2][2] - ld[1][2] * ld[2][1];
+            d[e][0][1] = -ld[0][1] * ld[2][2] + ld[0][2] * ld[2][1];
+            d[e][0][2] = ld[0][1] * ld[1][2] - ld[0][2] * ld[1][1];
+            d[e][1][0] = -ld[1][0] * ld[2][2] + ld[1][2] * ld[2][0];
+            d[e][1][1] = ld[0][0] * ld[2][2] - ld[0][2] * ld[2][0];
+            d[e][1][2] = -ld[0][0] * ld[1][2] + ld[0][2] * ld[1][0];
+            d[e][2][0] = ld[1][0] * ld[2][1] - ld[1][1] * ld[2][0];
+            d[e][2][1] = -ld[0][0] * ld[2][1] + ld[0][1] * ld[2][0];
+            d[e][2][2] = ld[0][0] * ld[1][1] - ld[0][1] * ld[1][0];
+            cj[e] = ld[0][0] * (ld[1][1] * ld[2][2] - ld[1][2] * ld[2][1]) -
+                    ld[0][1] * (ld[1][0] * ld[2][2] - ld[2][0] * ld[1][2]) +
+                    ld[0][2] * (ld[1][0] * ld[2][1] - ld[2][0] * ld[1][1]);
+        }
+        __syncwarp();
+        // ---- projection on the tensor cores: row (e, n) = (grow >> 2, grow & 3)
+        {
+            const int e = grow >> 2, n = grow & 3;
+            double a[M::KS];
+#pragma unroll
+            for (int ks = 0; ks < M::KS; ++ks) {
+                const int m = ks * 4 + gcol;
+                a[ks] = m < T ? UHT(e)[n * T + m] : 0.0;
+            }
+            const bool needd = beta > 0.0;
+            for (int op = 0; op < (needd ? 4 : 1); ++op) {
+                double *dst = op == 0 ? UQ(e) + n * QP : (n < 3 ? FRE(e) + n * VS + (op - 1) * Q : nullptr);
+                for (int nt0 = 0; nt0 < M::NT; nt0 += M::NG) {
+                    // NG independent accumulator chains
+                    double c[M::NG][2];
+#pragma unroll
+                    for (int g = 0; g < M::NG; ++g) c[g][0] = c[g][1] = 0.0;
+                    const double *b = projB + ((size_t)(op * M::NT + nt0) * M::KS) * 32 + lane;
+#pragma unroll
+                    for (int ks = 0; ks < M::KS; ++ks)
+#pragma unroll
+                        for (int g = 0; g < M::NG; ++g)
+                            if (nt0 + g < M::NT) dmma(c[g][0], c[g][1], a[ks], __ldg(b + ((size_t)g * M::KS + ks) * 32));
+                    if (dst) {
+#pragma unroll
+                        for (int g = 0; g < M::NG; ++g) {
+                            const int q = (nt0 + g) * 8 + gcol * 2;
+                            if (q < Q) dst[q] = c[g][0];
+                            if (q + 1 < Q) dst[q + 1] = c[g][1];
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        // ---- pointwise fluxes, lanes own (e, q): fim = convective + pressure / continuity;
+        //      fre = viscous flux from the velocity derivatives stored there
+        for (int w = lane; w < 2 * Q; w += 32) {
+            const int e = w / Q, q = w - e * Q;
+            const double *uq = UQ(e);
+            double *fim = FIM(e), *fre = FRE(e);
+            const double uu[4] = {uq[q], uq[QP + q], uq[2 * QP + q], uq[3 * QP + q]};
+            const double fx = rho * uu[0], fy = rho * uu[1], fz = rho * uu[2];
+            double f3[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                f3[c] = d[e][c][0] * fx + d[e][c][1] * fy + d[e][c][2] * fz;
+                fim[3 * VS + c * Q + q] = f3[c];
+            }
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) fim[n * VS + c * Q + q] = uu[n] * f3[c] + d[e][c][n] * uu[3];
+            if (beta > 0.0) {
+                double du[3][3];
+#pragma unroll
+                for (int n = 0; n < 3; ++n)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) du[n][c] = fre[n * VS + c * Q + q];
+                const double cjcbi = mu / cj[e];
+                double h[3][3];
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        h[b][a] = d[e][0][a] * du[b][0] + d[e][1][a] * du[b][1] + d[e][2][a] * du[b][2];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        double s = 0.0;
+#pragma unroll
+                        for (int ee = 0; ee < 3; ++ee) {
+                            const double gce = d[e][c][0] * d[e][ee][0] + d[e][c][1] * d[e][ee][1] + d[e][c][2] * d[e][ee][2];
+                            s += gce * du[a][ee];
+                        }
+                        s += d[e][c][0] * h[0][a] + d[e][c][1] * h[1][a] + d[e][c][2] * h[2][a];
+                        fre[a * VS + c * Q + q] = -cjcbi * s;
+                    }
+            }
+        }
+        __syncwarp();
+        if (beta > 0.0) {
+            // ---- strong residual at the owned points
+            constexpr int NW = (2 * Q + 31) / 32;
+            double rsd[NW][NV];
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                const int w = lane + 32 * k;
+                if (w >= 2 * Q) break;
+                const int e = w / Q, q = w - e * Q;
+                const int i = q / (G * G), j = (q / G) % G, kk = q % G;
+                const double yz = sm.y0[j] * sm.z0[kk], zz = sm.z0[kk];
+                const double *fim = FIM(e), *fre = FRE(e);
+#pragma unroll
+                for (int n = 0; n < NV; ++n) {
+                    auto fl = [&](int c, int i2, int j2, int k2) -> double {
+                        const int q2 = (i2 * G + j2) * G + k2;
+                        return n < 3 ? fim[n * VS + c * Q + q2] + fre[n * VS + c * Q + q2] : fim[3 * VS + c * Q + q2];
+                    };
+                    double ax = 0, bxs = 0, bxt = 0, ays = 0, byt = 0, azt = 0;
+#pragma unroll
+                    for (int l = 0; l < G; ++l) {
+                        ax += sm.Ax[i][l] * fl(0, l, j, kk);
+                        bxs += sm.Bx[i][l] * fl(1, l, j, kk);
+                        bxt += sm.Bx[i][l] * fl(2, l, j, kk);
+                        ays += sm.Ay[j][l] * fl(1, i, l, kk);
+                        byt += sm.By[j][l] * fl(2, i, l, kk);
+                        azt += sm.Az[kk][l] * fl(2, i, j, l);
+                    }
+                    rsd[k][n] = yz * ax + (yz * bxs + zz * ays) + (yz * bxt + zz * byt + azt);
+                }
+            }
+            __syncwarp();
+            // ---- SUPG terms into fre (viscous + SUPG; variable 3: the continuity SUPG term)
+#pragma unroll
+            for (int k = 0; k < NW; ++k) {
+                const int w = lane + 32 * k;
+                if (w >= 2 * Q) break;
+                const int e = w / Q, q = w - e * Q;
+                const int t = (e == 1 && has1) ? t0 + 1 : t0;
+                const double tau0 = tau[2 * t], tau3 = tau[2 * t + 1];
+                double *fre = FRE(e);
+                const double *uq = UQ(e);
+                double tr[NV], uu[3];
+#pragma unroll
+                for (int n = 0; n < 3; ++n) {
+                    tr[n] = tau0 * rsd[k][n];
+                    uu[n] = uq[n * QP + q];
+                }
+                tr[3] = tau3 * rsd[k][3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        double s2 = d[e][c][a] * (2.0 * uu[a]);
+#pragma unroll
+                        for (int b = 0; b < 3; ++b)
+                            if (b != a) s2 += d[e][c][b] * uu[b];
+                        double r = s2 * tr[a];
+#pragma unroll
+                        for (int b = 0; b < 3; ++b)
+                            if (b != a) r += d[e][c][b] * uu[a] * tr[b];
+                        r += d[e][c][a] * tr[3];
+                        fre[a * VS + c * Q + q] -= r;
+                    }
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    fre[3 * VS + c * Q + q] = -d[e][c][0] * tr[0] - d[e][c][1] * tr[1] - d[e][c][2] * tr[2];
+            }
+            __syncwarp();
+        }
+        // ---- intgrtrst on the tensor cores (imaginary into res, real * beta into res_r)
+        {
+            const int e = grow >> 2, n = grow & 3;
+            for (int part = 0; part < (beta > 0.0 ? 2 : 1); ++part) {
+                const double *fa = (part == 0 ? FIM(e) : FRE(e)) + n * VS;  // [3][Q] = k order
+                // all NT2 n-tiles share each A fragment; two K halves -> 2 * NT2 chains
+                double c[2][M::NT2][2];
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh)
+#pragma unroll
+                    for (int nt = 0; nt < M::NT2; ++nt) c[hh][nt][0] = c[hh][nt][1] = 0.0;
+#pragma unroll 2
+                for (int ks = 0; ks < M::KS2; ++ks) {
+                    const int k = ks * 4 + gcol;
+                    const double av = k < 3 * Q ? fa[k] : 0.0;
+#pragma unroll
+                    for (int nt = 0; nt < M::NT2; ++nt)
+                        dmma(c[ks & 1][nt][0], c[ks & 1][nt][1], av, __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane));
+                }
+                const bool ok = (e == 0 || has1);
+                for (int nt = 0; nt < M::NT2; ++nt) {
+                    // row grow = (e, n); columns m = nt*8 + gcol*2 + {0, 1}
+                    const double c0 = c[0][nt][0] + c[1][nt][0], c1 = c[0][nt][1] + c[1][nt][1];
+#pragma unroll
+                    for (int h2 = 0; h2 < 2; ++h2) {
+                        const int m = nt * 8 + gcol * 2 + h2;
+                        if (!ok || m >= T) continue;
+                        const double val = -(h2 ? c1 : c0);
+                        double sg;
+                        if (part == 0) {
+                            double *dst = mode_slot<double, P>(mesh, res, t0 + e, m, n, sg);
+                            if (m < C::BM) atomicAdd(dst, sg * val);
+                            else *dst = val;
+                        } else {
+                            double *dst = mode_slot<double, P>(mesh, rr, t0 + e, m, n, sg);
+                            if (m < C::BM) atomicAdd(dst, beta * sg * val);
+                            else *dst += beta * val;
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // res = 0; res_r *= 1 - beta  (tet_hp::rsdl prologue)
 template <typename R>
 __global__ void k_tet_pre(long n, R *res, R *rr, R omb) {
@@ -394,6 +683,7 @@ struct hp_tet_ctx {
     double *tau = nullptr, *iprcn = nullptr, *vprcn = nullptr, *eprcn = nullptr, *fprcn = nullptr;
     int *d_err = nullptr;
     double *ops = nullptr;  // F, DX, DY, DZ, WDX, WDY, WDZ  [Q*T] each
+    double *projB = nullptr, *intB = nullptr;  // the same operators in DMMA fragment order
     hp_tet_tables tab{};
     bool prcn_ready = false;
     TetFields<double> fields(double *base) const {
@@ -412,6 +702,34 @@ int talloc(hp_tet_ctx *c, void **p, size_t bytes) {
     }
     c->allocs.push_back(*p);
     return HP_OK;
+}
+
+// DMMA B fragments (lane = 4 * group + column): projection B[k = mode][n = point]
+// = Op(q, m) at [op][nt][ks][lane]; intgrtrst B[k = (c, q)][n = mode] = w(q) Dc(q, m)
+// at [nt][ks][lane]; zero beyond T, Q, 3Q.
+template <int P>
+void tet_fragments(const hp_tet_tables &b, std::vector<double> &proj, std::vector<double> &intg) {
+    using C = TetCfg<P>;
+    using M = TetMma<P>;
+    proj.assign(M::PROJ_LEN, 0.0);
+    intg.assign(M::INT_LEN, 0.0);
+    const double(*ops[4])[HP_TET_MAXT] = {b.F, b.DX, b.DY, b.DZ};
+    for (int op = 0; op < 4; ++op)
+        for (int nt = 0; nt < M::NT; ++nt)
+            for (int ks = 0; ks < M::KS; ++ks)
+                for (int lane = 0; lane < 32; ++lane) {
+                    const int q = nt * 8 + (lane >> 2), m = ks * 4 + (lane & 3);
+                    if (q < C::Q && m < C::T)
+                        proj[(((size_t)op * M::NT + nt) * M::KS + ks) * 32 + lane] = ops[op][q][m];
+                }
+    for (int nt = 0; nt < M::NT2; ++nt)
+        for (int ks = 0; ks < M::KS2; ++ks)
+            for (int lane = 0; lane < 32; ++lane) {
+                const int k = ks * 4 + (lane & 3), m = nt * 8 + (lane >> 2);
+                if (k >= 3 * C::Q || m >= C::T) continue;
+                const int c = k / C::Q, q = k - c * C::Q;
+                intg[((size_t)nt * M::KS2 + ks) * 32 + lane] = b.w[q] * ops[1 + c][q][m];
+            }
 }
 
 template <int P>
@@ -444,10 +762,19 @@ int launch_rsdl(hp_tet_ctx *c, int stage) {
     const double beta = c->ph.beta[stage];
     k_tet_pre<double><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>((long)c->ltot, c->RES,
                                                                                            c->RR, omb);
-    int blocks = std::min(nblk(c->mesh.ntet, C::WPC), c->nsm * 16);
-    k_tet_rsdl<double, P><<<blocks, C::WPC * 32, smem, c->stream>>>(ops, sm, c->mesh, c->fields(c->U),
-                                                                    c->fields(c->RES), c->fields(c->RR), c->tau,
-                                                                    c->ph.rho, c->ph.mu, beta);
+    using M = TetMma<P>;
+    const size_t smem2 = (size_t)M::S_WARP * M::WPC * sizeof(double);
+    static bool attr2 = false;
+    if (!attr2) {
+        TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+        attr2 = true;
+    }
+    (void)ops;
+    const long npair = ((long)c->mesh.ntet + 1) / 2;
+    int blocks = std::min(nblk(npair, M::WPC), c->nsm * 32);
+    k_tet_rsdl_mma<P><<<blocks, M::WPC * 32, smem2, c->stream>>>(c->projB, c->intB, sm, c->mesh, c->fields(c->U),
+                                                                 c->fields(c->RES), c->fields(c->RR), c->tau,
+                                                                 c->ph.rho, c->ph.mu, beta);
     k_tet_fold<double><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>((long)c->ltot, c->RES,
                                                                                             c->RR);
     TCK(cudaGetLastError());
@@ -534,6 +861,20 @@ extern "C" int hp_tet_create(const hp_tet_mesh_desc *m, const hp_tet_tables *b, 
             h[6 * qt + k] = b->w[q] * b->DZ[q][mm];
         }
     if ((r = up(h.data(), 8 * h.size(), (void **)&c->ops))) { hp_tet_destroy(c); return r; }
+    {
+        std::vector<double> pb, ib;
+        switch (c->p) {
+            case 1: tet_fragments<1>(*b, pb, ib); break;
+            case 2: tet_fragments<2>(*b, pb, ib); break;
+            case 3: tet_fragments<3>(*b, pb, ib); break;
+            case 4: tet_fragments<4>(*b, pb, ib); break;
+        }
+        if ((r = up(pb.data(), 8 * pb.size(), (void **)&c->projB)) ||
+            (r = up(ib.data(), 8 * ib.size(), (void **)&c->intB))) {
+            hp_tet_destroy(c);
+            return r;
+        }
+    }
     *out = c;
     return HP_OK;
 }
