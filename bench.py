@@ -248,6 +248,73 @@ def c4_sweep(hpb, dev, scale, cycles):
     print(json.dumps(line), flush=True)
 
 
+def tet_flops_per_element(p, beta_positive=True):
+    """Multiply-adds of the dense basis operators per tetrahedron and residual,
+    x 2 flops: projection of u, v, w with r, s, t derivatives and p by value
+    (13 operator rows x Q x T when beta > 0, 4 otherwise) and intgrtrst of the four
+    3-component fluxes (4 x 3Q x T) for the imaginary part and again for the real
+    part. Pointwise flux, derivative and SUPG arithmetic is not counted."""
+    G = p + 1
+    Q, T = G ** 3, (p + 1) * (p + 2) * (p + 3) // 6
+    proj = (13 if beta_positive else 4) * Q * T
+    intg = (2 if beta_positive else 1) * 4 * 3 * Q * T
+    return 2 * (proj + intg)
+
+
+def c5_sweep(torch, dev, n, p, steps, warmup, timed):
+    """3D tet_hp ins: the unit cube split into n^3 hexahedra x 6 tetrahedra (n = 64:
+    1,572,864 tetrahedra), p = 3, Re 100, the Ethier-Steinman Beltrami state at the
+    vertices plus 1e-3 seeded noise on every coefficient. Times tet_hp::rsdl(nstage)
+    (FP64, beta = 1: both parts of element_rsdl) on the GPU with CUDA events (the
+    state, 230 MB at n = 64, exceeds L2; L2 flushed between steps anyway), the CPU
+    oracle on a bounded 6^3 x 6 sample, and the FP64 tensor-core throughput of the
+    GPU for the roofline."""
+    import time as _t
+    from hpb.tet import TetGPU, TetProblem
+    from hpb.tetmesh import cube_tets
+    from oracle.oracle import OracleTet
+    t0 = _t.perf_counter()
+    mesh = cube_tets(n)
+    pr = TetProblem(mesh, p, mu=1.0 / 100.0).set_beltrami(re=100.0)
+    import ctypes
+    cur = torch.cuda.current_stream()
+    g = TetGPU(pr, device=dev, stream=ctypes.c_void_p(cur.cuda_stream))  # events and kernels on one stream
+    host_s = _t.perf_counter() - t0
+    assert g.setup_preconditioner() == 0
+    ns = pr.phys.nstage
+    for _ in range(warmup):
+        g.lib.hp_tet_enqueue_rsdl(g.h, ns)
+    g.lib.hp_tet_sync(g.h)
+    ms = timed(lambda: g.lib.hp_tet_enqueue_rsdl(g.h, ns), steps, cur)
+    ms0 = timed(lambda: g.lib.hp_tet_enqueue_rsdl(g.h, 1), steps, cur)
+    rsdl_ms = sum(ms) / len(ms)
+    peak = ctypes.c_double()
+    g.lib.hp_tet_fp64_mma_peak.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    g.lib.hp_tet_fp64_mma_peak(dev, 200.0, ctypes.byref(peak))
+    fl = tet_flops_per_element(p) * mesh.ntet
+    achieved = fl / (rsdl_ms * 1e-3) / 1e12
+    line = {"sweep": "c5", "workload": f"tet ins p={p}, {n}^3 x 6 = {mesh.ntet} tetrahedra, Re 100 Beltrami + 1e-3 noise",
+            "ndof": pr.ndof, "ntet": mesh.ntet, "host_setup_seconds": host_s, "steps": steps, "warmup": warmup,
+            "rsdl_ms": rsdl_ms, "rsdl_gdofs": pr.ndof / rsdl_ms / 1e6, "rsdl_beta0_ms": sum(ms0) / len(ms0),
+            "operator_flops_per_tet": tet_flops_per_element(p), "l2_flushed": True,
+            "roofline": {"bound": "fp64_tensor", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value,
+                         "peak_source": "hp_tet_fp64_mma_peak: mma.m8n8k4.f64 chains on every SM, measured in this run"}}
+    g.close()
+    # CPU oracle on a bounded sample
+    ps = TetProblem(cube_tets(6), p, mu=1.0 / 100.0).set_beltrami(re=100.0)
+    o = OracleTet(ps)
+    o.setup_preconditioner()
+    reps, t2 = 0, _t.perf_counter()
+    while _t.perf_counter() - t2 < 10.0:
+        o.rsdl(ns)
+        reps += 1
+    cpu_s = (_t.perf_counter() - t2) / reps
+    line["cpu_baseline"] = {"value": ps.ndof / cpu_s / 1e9, "unit": "GDoF/s", "cores": 1, "kind": "port",
+                            "sample": f"oracle tet rsdl(nstage), 6^3 x 6 tetrahedra p={p}, {reps} repetitions"}
+    print(json.dumps(line), flush=True)
+
+
 def timed_factory(torch, flush):
     def timed(fn, n, stream):
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
@@ -456,7 +523,7 @@ def main():
                     help="run `steps` multistage updates of the workload in FP64 or FP32 (for profiler runs)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="with --sweep c4: edge-length scale of the channel mesh (1: ~150k triangles)")
-    ap.add_argument("--sweep", choices=["c2", "c3", "c4"], default=None,
+    ap.add_argument("--sweep", choices=["c2", "c3", "c4", "c5"], default=None,
                     help="c2: cd on the seeded 200k-triangle Delaunay mesh, p = 2, 4, 6, 8: rsdl GDoF/s and time "
                          "to a 1e-10 drop, plain FP64 vs FP32 defect correction (one JSON line per p); "
                          "c3: ins lid-driven cavity Re 400, p = 6, 512x512 split squares, V-cycles for --steps "
@@ -510,6 +577,11 @@ def main():
         return
     if args.sweep == "c3":
         c3_sweep(hpb, dev, args.mesh if args.mesh != N_MESH else 512, (args.p or [6])[0], args.steps)
+        return
+    if args.sweep == "c5":
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        c5_sweep(torch, dev, args.mesh if args.mesh != N_MESH else 64, (args.p or [3])[0], args.steps, args.warmup,
+                 timed_factory(torch, flush))
         return
 
     if args.physics == "ins":

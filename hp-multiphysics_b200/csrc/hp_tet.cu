@@ -972,3 +972,49 @@ extern "C" int hp_tet_rsdl(hp_tet_ctx *c, int stage) {
     if (r) return r;
     return hp_tet_sync(c);
 }
+
+namespace {
+// 8 independent accumulator pairs per warp; out keeps the compiler from dropping them
+__global__ void k_dmma_peak(long iters, double *out) {
+    double c[8][2];
+    for (int g = 0; g < 8; ++g) c[g][0] = c[g][1] = 0.0;
+    const double a = 1.0 + 1e-9 * threadIdx.x, b = 1.0 - 1e-9 * threadIdx.x;
+    for (long it = 0; it < iters; ++it)
+#pragma unroll
+        for (int g = 0; g < 8; ++g) dmma(c[g][0], c[g][1], a, b);
+    double s = 0.0;
+    for (int g = 0; g < 8; ++g) s += c[g][0] + c[g][1];
+    if (s == -1.0) out[0] = s;  // never true; keeps the chains live
+}
+}  // namespace
+
+extern "C" int hp_tet_fp64_mma_peak(int device, double ms, double *tflops) {
+    if (!tflops || ms <= 0) return HP_EINVAL;
+    if (device >= 0) TCK(cudaSetDevice(device));
+    int dev, nsm;
+    TCK(cudaGetDevice(&dev));
+    TCK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    double *out;
+    TCK(cudaMalloc(&out, 8));
+    cudaEvent_t e0, e1;
+    TCK(cudaEventCreate(&e0));
+    TCK(cudaEventCreate(&e1));
+    const int blocks = nsm * 4, threads = 256;
+    long iters = 1000;
+    float el = 0.f;
+    for (int tries = 0; tries < 12; ++tries) {
+        TCK(cudaEventRecord(e0));
+        k_dmma_peak<<<blocks, threads>>>(iters, out);
+        TCK(cudaEventRecord(e1));
+        TCK(cudaEventSynchronize(e1));
+        TCK(cudaEventElapsedTime(&el, e0, e1));
+        if (el >= ms) break;
+        iters = (long)(iters * std::min(16.0, 1.2 * ms / std::max(el, 0.01f)));
+    }
+    const double mmas = (double)blocks * (threads / 32) * iters * 8;
+    *tflops = mmas * 8 * 8 * 4 * 2 / (el * 1e-3) / 1e12;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    return HP_OK;
+}

@@ -100,6 +100,11 @@ int hp_tet_rsdl(hp_tet_ctx *ctx, int stage);
 int hp_tet_sync(hp_tet_ctx *ctx);
 const char *hp_tet_last_error(void);
 
+/* Measurement helper (no counterpart in the reference): the FP64 tensor-core
+ * (mma.m8n8k4.f64) throughput of this GPU, from independent accumulation chains
+ * on every SM for about `ms` milliseconds. Writes TFLOP/s (2 flops per multiply-add). */
+int hp_tet_fp64_mma_peak(int device, double ms, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif
