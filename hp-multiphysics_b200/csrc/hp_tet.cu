@@ -335,6 +335,7 @@ struct TetMma {
     static constexpr int NG = NT < 8 ? NT : 8;  // projection n-tiles accumulated together
     static constexpr int S_WARP = 2 * S_EL;
     static constexpr size_t PROJ_LEN = (size_t)4 * NT * KS * 32, INT_LEN = (size_t)NT2 * KS2 * 32;
+    static constexpr size_t SMEM = (size_t)S_WARP * WPC * sizeof(double);
 };
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
@@ -343,14 +344,21 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-template <int P>
+// MODE 0: tet_hp::rsdl element loop (res, res_r). MODE 1: the stage-0 element residual
+// lf_re + lf_im of every tetrahedron into rbar [ntet][T][NV]. MODE 2: tet_hp::
+// jacobian_diagonal (tet_hp/jacobi.cpp:32-111): one item per (tetrahedron, mode m,
+// variable n) with uht(n)(m) raised by dw; (lf(n)(m) - rbar) / dw is added, without the
+// edge / face sign (its square is 1), to the global diagonal jd.
+template <int P, int MODE>
 __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
     k_tet_rsdl_mma(const double *__restrict__ projB, const double *__restrict__ intB, TetSmall<double, P> sm,
                    TetMeshD mesh, TetFields<double> ug, TetFields<double> res, TetFields<double> rr,
-                   const double *__restrict__ tau, double rho, double mu, double beta) {
+                   const double *__restrict__ tau, double rho, double mu, double beta, double *rbar,
+                   TetFields<double> jd) {
     using C = TetCfg<P>;
     using M = TetMma<P>;
     constexpr int G = C::G, Q = C::Q, T = C::T;
+    constexpr int NJ = NV * T;  // items per tetrahedron in MODE 2
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int grow = lane >> 2, gcol = lane & 3;  // fragment row / column group
@@ -360,25 +368,51 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
     auto UQ = [&](int e) { return base + e * M::S_EL + NV * T; };
     auto FIM = [&](int e) { return base + e * M::S_EL + NV * T + NV * QP; };
     auto FRE = [&](int e) { return base + e * M::S_EL + NV * T + NV * QP + NV * VS; };
-    const long npair = ((long)mesh.ntet + 1) / 2;
+    const long nitems = MODE == 2 ? (long)mesh.ntet * NJ : (long)mesh.ntet;
+    const long npair = (nitems + 1) / 2;
     for (long pr = (long)blockIdx.x * M::WPC + warp; pr < npair; pr += (long)gridDim.x * M::WPC) {
-        const int t0 = (int)(2 * pr);
-        const bool has1 = t0 + 1 < mesh.ntet;
+        const long it0 = 2 * pr;
+        const bool has1 = it0 + 1 < nitems;
+        // tetrahedron of item e (a missing second item repeats the first)
+        int te[2];
+        for (int e = 0; e < 2; ++e) {
+            const long it = (e == 1 && has1) ? it0 + 1 : it0;
+            te[e] = MODE == 2 ? (int)(it / NJ) : (int)it;
+        }
         // ---- gather both tetrahedra (a missing second one gets zeros)
         for (int w = lane; w < 2 * NV * T; w += 32) {
             const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
             double v = 0.0;
             if (e == 0 || has1) {
                 double s;
-                const double *src = mode_slot<double, P>(mesh, ug, t0 + e, m, n, s);
+                const double *src = mode_slot<double, P>(mesh, ug, te[e], m, n, s);
                 v = s * *src;
             }
             UHT(e)[n * T + m] = v;
         }
+        double dw[2] = {0.0, 0.0};
+        int jm[2] = {0, 0}, jn[2] = {0, 0};
+        if constexpr (MODE == 2) {
+            __syncwarp();
+            // dw = 1e-6 sum over the 4 vertex modes of all variables + 1e-10, the same for
+            // every variable (jacobi.cpp:63-67)
+            for (int e = 0; e < 2; ++e) {
+                double sdw = 0.0;
+                for (int n = 0; n < NV; ++n)
+                    for (int i = 0; i < 4; ++i) sdw += fabs(UHT(e)[n * T + i]);
+                dw[e] = sdw * 1.0e-6 + 1.0e-10;
+                const long it = (e == 1 && has1) ? it0 + 1 : it0;
+                const int j = (int)(it - (long)te[e] * NJ);
+                jm[e] = j / NV;
+                jn[e] = j - jm[e] * NV;
+            }
+            __syncwarp();
+            if (lane < 2 && (lane == 0 || has1)) UHT(lane)[jn[lane] * T + jm[lane]] += dw[lane];
+        }
         // geometry of both (the missing one repeats the first)
         double d[2][3][3], cj[2];
         for (int e = 0; e < 2; ++e) {
-            const int t = (e == 1 && has1) ? t0 + 1 : t0;
+            const int t = te[e];
             const int v0 = mesh.tp[4 * t], v1 = mesh.tp[4 * t + 1], v2 = mesh.tp[4 * t + 2], v3 = mesh.tp[4 * t + 3];
             double ld[3][3];
             for (int n = 0; n < 3; ++n) {
@@ -521,7 +555,7 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
                 const int w = lane + 32 * k;
                 if (w >= 2 * Q) break;
                 const int e = w / Q, q = w - e * Q;
-                const int t = (e == 1 && has1) ? t0 + 1 : t0;
+                const int t = te[e];
                 const double tau0 = tau[2 * t], tau3 = tau[2 * t + 1];
                 double *fre = FRE(e);
                 const double *uq = UQ(e);
@@ -556,6 +590,9 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
         // ---- intgrtrst on the tensor cores (imaginary into res, real * beta into res_r)
         {
             const int e = grow >> 2, n = grow & 3;
+            double tot[M::NT2][2];
+#pragma unroll
+            for (int nt = 0; nt < M::NT2; ++nt) tot[nt][0] = tot[nt][1] = 0.0;
             for (int part = 0; part < (beta > 0.0 ? 2 : 1); ++part) {
                 const double *fa = (part == 0 ? FIM(e) : FRE(e)) + n * VS;  // [3][Q] = k order
                 // all NT2 n-tiles share each A fragment; two K halves -> 2 * NT2 chains
@@ -581,18 +618,41 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
                         const int m = nt * 8 + gcol * 2 + h2;
                         if (!ok || m >= T) continue;
                         const double val = -(h2 ? c1 : c0);
+                        if constexpr (MODE != 0) {
+                            tot[nt][h2] += part == 0 ? val : beta * val;
+                            continue;
+                        }
                         double sg;
                         if (part == 0) {
-                            double *dst = mode_slot<double, P>(mesh, res, t0 + e, m, n, sg);
+                            double *dst = mode_slot<double, P>(mesh, res, te[e], m, n, sg);
                             if (m < C::BM) atomicAdd(dst, sg * val);
                             else *dst = val;
                         } else {
-                            double *dst = mode_slot<double, P>(mesh, rr, t0 + e, m, n, sg);
+                            double *dst = mode_slot<double, P>(mesh, rr, te[e], m, n, sg);
                             if (m < C::BM) atomicAdd(dst, beta * sg * val);
                             else *dst += beta * val;
                         }
                     }
                 }
+            }
+            if constexpr (MODE != 0) {
+                const bool ok = (e == 0 || has1);
+#pragma unroll
+                for (int nt = 0; nt < M::NT2; ++nt)
+#pragma unroll
+                    for (int h2 = 0; h2 < 2; ++h2) {
+                        const int m = nt * 8 + gcol * 2 + h2;
+                        if (!ok || m >= T) continue;
+                        const size_t rb = ((size_t)te[e] * T + m) * NV + n;
+                        if constexpr (MODE == 1) {
+                            rbar[rb] = tot[nt][h2];
+                        } else {
+                            if (m != jm[e] || n != jn[e]) continue;
+                            double sg;
+                            double *dst = mode_slot<double, P>(mesh, jd, te[e], m, n, sg);
+                            atomicAdd(dst, (tot[nt][h2] - rbar[rb]) / dw[e]);
+                        }
+                    }
             }
         }
         __syncwarp();
@@ -666,6 +726,32 @@ __global__ void k_tet_prcn(TetMeshD mesh, const double *ugv, double *tau, double
     }
 }
 
+// tet_hp::update stage, JACOBI build (update.cpp:206-390, jacobi.cpp:14-30): essential rows
+// zeroed, res = 0.5 res / jacob_diag, ug = ug0 - cflalpha res
+__global__ void k_tet_relax(long n, double *res, const double *jd, const unsigned char *mask, double *u,
+                            const double *u0, double ca) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        const double r = mask[k] ? 0.0 : 0.5 * res[k] / jd[k];
+        res[k] = r;
+        u[k] = u0[k] - ca * r;
+    }
+}
+
+// per-block sums of squares of the unmasked residual entries (fixed grid: deterministic)
+__global__ void k_tet_sq(long n, const double *res, const unsigned char *mask, double *part) {
+    __shared__ double sh[256];
+    double s = 0.0;
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+        if (!mask[k]) s += res[k] * res[k];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
 int nblk(long n, int b) { return (int)std::max<long>(1, (n + b - 1) / b); }
 
 }  // namespace
@@ -684,6 +770,9 @@ struct hp_tet_ctx {
     int *d_err = nullptr;
     double *ops = nullptr;  // F, DX, DY, DZ, WDX, WDY, WDZ  [Q*T] each
     double *projB = nullptr, *intB = nullptr;  // the same operators in DMMA fragment order
+    double *U0 = nullptr, *JD = nullptr, *rbar = nullptr, *part = nullptr;  // update, jacob_diag
+    unsigned char *mask = nullptr;  // 1: row fixed by an essential condition
+    bool jd_ready = false;
     hp_tet_tables tab{};
     bool prcn_ready = false;
     TetFields<double> fields(double *base) const {
@@ -766,17 +855,51 @@ int launch_rsdl(hp_tet_ctx *c, int stage) {
     const size_t smem2 = (size_t)M::S_WARP * M::WPC * sizeof(double);
     static bool attr2 = false;
     if (!attr2) {
-        TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+        TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+        TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+        TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
         attr2 = true;
     }
     (void)ops;
     const long npair = ((long)c->mesh.ntet + 1) / 2;
     int blocks = std::min(nblk(npair, M::WPC), c->nsm * 32);
-    k_tet_rsdl_mma<P><<<blocks, M::WPC * 32, smem2, c->stream>>>(c->projB, c->intB, sm, c->mesh, c->fields(c->U),
-                                                                 c->fields(c->RES), c->fields(c->RR), c->tau,
-                                                                 c->ph.rho, c->ph.mu, beta);
+    k_tet_rsdl_mma<P, 0><<<blocks, M::WPC * 32, smem2, c->stream>>>(
+        c->projB, c->intB, sm, c->mesh, c->fields(c->U), c->fields(c->RES), c->fields(c->RR), c->tau, c->ph.rho,
+        c->ph.mu, beta, nullptr, TetFields<double>{});
     k_tet_fold<double><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>((long)c->ltot, c->RES,
                                                                                             c->RR);
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+template <int P>
+int launch_jacdiag(hp_tet_ctx *c) {
+    using C = TetCfg<P>;
+    using M = TetMma<P>;
+    int r = launch_rsdl<P>(c, c->ph.nstage);  // sets the kernel attributes on first use
+    if (r) return r;
+    TetSmall<double, P> sm;
+    const hp_tet_tables &t = c->tab;
+    for (int i = 0; i <= P; ++i) {
+        for (int j = 0; j <= P; ++j) {
+            sm.Ax[i][j] = t.Ax[i][j];
+            sm.Bx[i][j] = t.Bx[i][j];
+            sm.Ay[i][j] = t.Ay[i][j];
+            sm.By[i][j] = t.By[i][j];
+            sm.Az[i][j] = t.Az[i][j];
+        }
+        sm.y0[i] = t.y0[i];
+        sm.z0[i] = t.z0[i];
+    }
+    const double beta0 = c->ph.beta[0];
+    const long n1 = ((long)c->mesh.ntet + 1) / 2, n2 = ((long)c->mesh.ntet * NV * C::T + 1) / 2;
+    k_tet_rsdl_mma<P, 1><<<std::min(nblk(n1, M::WPC), c->nsm * 32), M::WPC * 32, M::SMEM, c->stream>>>(
+        c->projB, c->intB, sm, c->mesh, c->fields(c->U), c->fields(c->RES), c->fields(c->RR), c->tau, c->ph.rho,
+        c->ph.mu, beta0, c->rbar, c->fields(c->JD));
+    TCK(cudaMemsetAsync(c->JD, 0, 8 * c->ltot, c->stream));
+    k_tet_rsdl_mma<P, 2><<<std::min(nblk(n2, M::WPC), c->nsm * 32), M::WPC * 32, M::SMEM, c->stream>>>(
+        c->projB, c->intB, sm, c->mesh, c->fields(c->U), c->fields(c->RES), c->fields(c->RR), c->tau, c->ph.rho,
+        c->ph.mu, beta0, c->rbar, c->fields(c->JD));
     TCK(cudaGetLastError());
     return HP_OK;
 }
@@ -875,6 +998,12 @@ extern "C" int hp_tet_create(const hp_tet_mesh_desc *m, const hp_tet_tables *b, 
             return r;
         }
     }
+    if ((r = talloc(c, (void **)&c->U0, 8 * c->ltot)) || (r = talloc(c, (void **)&c->JD, 8 * c->ltot)) ||
+        (r = talloc(c, (void **)&c->mask, c->ltot)) || (r = talloc(c, (void **)&c->part, 8 * 1024))) {
+        hp_tet_destroy(c);
+        return r;
+    }
+    TCK(cudaMemset(c->mask, 0, c->ltot));
     *out = c;
     return HP_OK;
 }
@@ -1016,5 +1145,128 @@ extern "C" int hp_tet_fp64_mma_peak(int device, double ms, double *tflops) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(out);
+    return HP_OK;
+}
+
+extern "C" int hp_tet_set_dirichlet(hp_tet_ctx *c, const unsigned char *mv, const unsigned char *me,
+                                    const unsigned char *mf) {
+    if (!c || !mv) return HP_EINVAL;
+    std::vector<unsigned char> h(c->ltot, 0);
+    for (size_t k = 0; k < c->lv; ++k) h[k] = mv[k] ? 1 : 0;
+    if (c->em && me)
+        for (int e = 0; e < c->mesh.nseg; ++e)
+            for (int m = 0; m < c->em; ++m)
+                for (int n = 0; n < NV; ++n) h[c->lv + ((size_t)e * c->em + m) * NV + n] = me[(size_t)e * NV + n] ? 1 : 0;
+    if (c->fm && mf)
+        for (int f = 0; f < c->mesh.ntri; ++f)
+            for (int m = 0; m < c->fm; ++m)
+                for (int n = 0; n < NV; ++n)
+                    h[c->lv + c->le + ((size_t)f * c->fm + m) * NV + n] = mf[(size_t)f * NV + n] ? 1 : 0;
+    TCK(cudaMemcpyAsync(c->mask, h.data(), c->ltot, cudaMemcpyHostToDevice, c->stream));
+    TCK(cudaStreamSynchronize(c->stream));
+    return HP_OK;
+}
+
+extern "C" int hp_tet_jacobian_diagonal(hp_tet_ctx *c) {
+    if (!c) return HP_EINVAL;
+    if (!c->prcn_ready) {
+        set_err("hp_tet_jacobian_diagonal needs tau from hp_tet_setup_preconditioner");
+        return HP_ESTATE;
+    }
+    if (!c->rbar) {
+        int r = talloc(c, (void **)&c->rbar, 8 * (size_t)c->mesh.ntet * c->T * NV);
+        if (r) return r;
+    }
+    int r = HP_EINVAL;
+    switch (c->p) {
+        case 1: r = launch_jacdiag<1>(c); break;
+        case 2: r = launch_jacdiag<2>(c); break;
+        case 3: r = launch_jacdiag<3>(c); break;
+        case 4: r = launch_jacdiag<4>(c); break;
+    }
+    if (r) return r;
+    TCK(cudaStreamSynchronize(c->stream));
+    c->jd_ready = true;
+    return HP_OK;
+}
+
+extern "C" int hp_tet_download_jacobian_diagonal(hp_tet_ctx *c, double *v, double *e, double *f, double *i) {
+    if (!c || !c->jd_ready) return HP_ESTATE;
+    return copy_fields(c, c->JD, nullptr, nullptr, nullptr, nullptr, v, e, f, i);
+}
+
+extern "C" int hp_tet_enqueue_update(hp_tet_ctx *c) {
+    if (!c) return HP_EINVAL;
+    if (!c->jd_ready) {
+        set_err("hp_tet_update needs hp_tet_jacobian_diagonal first");
+        return HP_ESTATE;
+    }
+    TCK(cudaMemcpyAsync(c->U0, c->U, 8 * c->ltot, cudaMemcpyDeviceToDevice, c->stream));
+    for (int stage = 0; stage < c->ph.nstage; ++stage) {
+        int r = hp_tet_enqueue_rsdl(c, stage);
+        if (r) return r;
+        const double ca = c->ph.alpha[stage] * c->ph.cfl;
+        k_tet_relax<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+            (long)c->ltot, c->RES, c->JD, c->mask, c->U, c->U0, ca);
+    }
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+extern "C" int hp_tet_update(hp_tet_ctx *c) {
+    int r = hp_tet_enqueue_update(c);
+    if (r) return r;
+    return hp_tet_sync(c);
+}
+
+extern "C" int hp_tet_resnorm(hp_tet_ctx *c, double *l2) {
+    if (!c || !l2) return HP_EINVAL;
+    int r = hp_tet_enqueue_rsdl(c, c->ph.nstage);
+    if (r) return r;
+    const int nb = 1024;
+    k_tet_sq<<<nb, 256, 0, c->stream>>>((long)c->ltot, c->RES, c->mask, c->part);
+    std::vector<double> h(nb);
+    TCK(cudaMemcpyAsync(h.data(), c->part, 8 * nb, cudaMemcpyDeviceToHost, c->stream));
+    TCK(cudaStreamSynchronize(c->stream));
+    double s2 = 0.0;
+    for (int k = 0; k < nb; ++k) s2 += h[k];
+    *l2 = std::sqrt(s2);
+    return HP_OK;
+}
+
+// Smooths until the residual norm falls by `drop` (checked every check_every updates) or
+// max_updates; the preconditioner (tau and the Jacobian diagonal) is set up once.
+extern "C" int hp_tet_solve(hp_tet_ctx *c, double drop, int max_updates, int check_every, double *hist, int cap,
+                            int *nhist, double *seconds, int *updates) {
+    if (!c || drop <= 0 || max_updates < 1 || check_every < 1 || !hist || cap < 1) return HP_EINVAL;
+    cudaEvent_t e0, e1;
+    TCK(cudaEventCreate(&e0));
+    TCK(cudaEventCreate(&e1));
+    TCK(cudaEventRecord(e0, c->stream));
+    int r = hp_tet_setup_preconditioner(c);
+    if (r) return r < 0 ? r : HP_ESTATE;
+    if ((r = hp_tet_jacobian_diagonal(c))) return r;
+    double r0;
+    if ((r = hp_tet_resnorm(c, &r0))) return r;
+    int nh = 0, nu = 0;
+    hist[nh++] = 1.0;
+    while (nu < max_updates) {
+        for (int k = 0; k < check_every && nu < max_updates; ++k, ++nu)
+            if ((r = hp_tet_enqueue_update(c))) return r;
+        double rn;
+        if ((r = hp_tet_resnorm(c, &rn))) return r;
+        const double d = r0 > 0 ? rn / r0 : 0.0;
+        if (nh < cap) hist[nh++] = d;
+        if (!(d == d) || d <= drop) break;
+    }
+    TCK(cudaEventRecord(e1, c->stream));
+    TCK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    TCK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (nhist) *nhist = nh;
+    if (seconds) *seconds = ms * 1e-3;
+    if (updates) *updates = nu;
     return HP_OK;
 }

@@ -116,6 +116,19 @@ class TetProblem:
     def ndof(self):
         return sum(a.size for a in self.state)
 
+    def dirichlet_masks(self, faces=None):
+        """Velocity rows fixed on the boundary faces (bdry_ins::inflow: u, v, w essential,
+        pressure free): masks [npnt][4], [nseg][4], [ntri][4]."""
+        m = self.mesh
+        v, e, f = m.boundary_entities(faces)
+        mv = np.zeros((m.npnt, 4), np.uint8)
+        me = np.zeros((m.nseg, 4), np.uint8)
+        mf = np.zeros((m.ntri, 4), np.uint8)
+        mv[v, :3] = 1
+        me[e, :3] = 1
+        mf[f, :3] = 1
+        return mv, me, mf
+
     def set_beltrami(self, re=100.0, noise=1e-3, seed=20261209):
         """Vertex values of the Beltrami field, high-order modes zero, plus seeded
         U[-1,1) noise of amplitude `noise` on every coefficient."""
@@ -160,6 +173,15 @@ def _bind():
         lib.hp_tet_rsdl.argtypes = [P, _I]
         lib.hp_tet_sync.argtypes = [P]
         lib.hp_tet_last_error.restype = ctypes.c_char_p
+        lib.hp_tet_set_dirichlet.argtypes = [P, P, P, P]
+        lib.hp_tet_jacobian_diagonal.argtypes = [P]
+        lib.hp_tet_download_jacobian_diagonal.argtypes = [P, P, P, P, P]
+        lib.hp_tet_enqueue_update.argtypes = [P]
+        lib.hp_tet_update.argtypes = [P]
+        lib.hp_tet_resnorm.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+        lib.hp_tet_solve.argtypes = [P, ctypes.c_double, _I, _I, P, _I, ctypes.POINTER(_I),
+                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I)]
+        lib.hp_tet_fp64_mma_peak.argtypes = [_I, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
         _bound = True
     return lib
 
@@ -228,3 +250,32 @@ class TetGPU:
 
     def rsdl(self, stage):
         _check(self.lib, self.lib.hp_tet_rsdl(self.h, stage), "rsdl")
+
+    def set_dirichlet(self, masks):
+        mv, me, mf = (np.ascontiguousarray(a, dtype=np.uint8) for a in masks)
+        _check(self.lib, self.lib.hp_tet_set_dirichlet(self.h, self._p(mv), self._p(me), self._p(mf)),
+               "set_dirichlet")
+
+    def jacobian_diagonal(self):
+        _check(self.lib, self.lib.hp_tet_jacobian_diagonal(self.h), "jacobian_diagonal")
+        out = self._out()
+        _check(self.lib, self.lib.hp_tet_download_jacobian_diagonal(self.h, *[self._p(a) for a in out]),
+               "download_jacobian_diagonal")
+        return out
+
+    def update(self):
+        _check(self.lib, self.lib.hp_tet_update(self.h), "update")
+
+    def resnorm(self):
+        r = ctypes.c_double()
+        _check(self.lib, self.lib.hp_tet_resnorm(self.h, ctypes.byref(r)), "resnorm")
+        return r.value
+
+    def solve(self, drop=1e-10, max_updates=20000, check_every=20):
+        cap = max_updates // check_every + 4
+        hist = np.zeros(cap)
+        nh, nu = ctypes.c_int(), ctypes.c_int()
+        sec = ctypes.c_double()
+        _check(self.lib, self.lib.hp_tet_solve(self.h, drop, max_updates, check_every, self._p(hist), cap,
+                                               ctypes.byref(nh), ctypes.byref(sec), ctypes.byref(nu)), "solve")
+        return hist[:nh.value], sec.value, nu.value

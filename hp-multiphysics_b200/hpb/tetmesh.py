@@ -87,6 +87,20 @@ class TetMesh:
     def boundary_faces(self):
         return np.nonzero(self.tri_tet[:, 1] < 0)[0].astype(np.int32)
 
+    def boundary_entities(self, faces=None):
+        """Vertices, edges and faces on the given boundary faces (default: all):
+        each face's local edges are found in its tetrahedron (the edges whose two
+        local vertices both lie on the face)."""
+        faces = self.boundary_faces() if faces is None else np.asarray(faces)
+        t = self.tri_tet[faces, 0]
+        loc = np.argmax(self.tet_tri[t] == faces[:, None], axis=1)
+        verts = np.unique(self.tri_pnt[faces].ravel())
+        on = np.zeros((len(faces), 4), bool)
+        on[np.arange(len(faces))[:, None], VF[loc]] = True
+        edge_on = on[:, VS[:, 0]] & on[:, VS[:, 1]]          # (nf, 6)
+        edges = np.unique(self.tet_seg[t][edge_on])
+        return verts, edges, np.unique(faces)
+
 
 def cube_tets(n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
     """[lo, hi] box, n^3 hexahedra x 6 tetrahedra around each main diagonal."""

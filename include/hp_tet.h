@@ -100,6 +100,27 @@ int hp_tet_rsdl(hp_tet_ctx *ctx, int stage);
 int hp_tet_sync(hp_tet_ctx *ctx);
 const char *hp_tet_last_error(void);
 
+/* Rows fixed by essential conditions (bdry_ins::inflow on boundary faces,
+ * tet_hp/ins/bdry_ins.h:141-183): masks [npnt][4], [nseg][4], [ntri][4], 1 = zero the
+ * residual of that (entity, variable) in every mode. */
+int hp_tet_set_dirichlet(hp_tet_ctx *ctx, const unsigned char *mv, const unsigned char *me,
+                         const unsigned char *mf);
+/* tet_hp::jacobian_diagonal (tet_hp/jacobi.cpp:32-111): finite-difference diagonal of every
+ * element Jacobian at stage 0, summed into the global diagonal. Needs tau. */
+int hp_tet_jacobian_diagonal(hp_tet_ctx *ctx);
+int hp_tet_download_jacobian_diagonal(hp_tet_ctx *ctx, double *v, double *e, double *f, double *i);
+/* tet_hp::update of the reference's JACOBI build (tet_hp/update.cpp:181-390 with
+ * jacobi_relaxation, jacobi.cpp:14-30): nstage stages of rsdl, essential rows zeroed,
+ * res = 0.5 res / jacob_diag, ug = ug0 - alpha(stage) cfl res. */
+int hp_tet_enqueue_update(hp_tet_ctx *ctx);
+int hp_tet_update(hp_tet_ctx *ctx);
+/* L2 norm of rsdl(nstage) over the rows no essential condition fixes */
+int hp_tet_resnorm(hp_tet_ctx *ctx, double *l2);
+/* setup_preconditioner + jacobian_diagonal, then updates until the residual norm has
+ * dropped by `drop` (checked every check_every updates) or max_updates */
+int hp_tet_solve(hp_tet_ctx *ctx, double drop, int max_updates, int check_every, double *hist, int cap,
+                 int *nhist, double *seconds, int *updates);
+
 /* Measurement helper (no counterpart in the reference): the FP64 tensor-core
  * (mma.m8n8k4.f64) throughput of this GPU, from independent accumulation chains
  * on every SM for about `ms` milliseconds. Writes TFLOP/s (2 flops per multiply-add). */

@@ -33,6 +33,9 @@ struct OT {
     std::vector<double> tau;                          // [ntet][2]: tau(tind,0), tau(tind,NV-1)
     std::vector<double> iprcn;                        // [ntet][NV]
     std::vector<double> vprcn, eprcn, fprcn;          // accumulated diagonals
+    std::vector<double> jv, je, jf, ji;               // jacob_diag (tet_hp/jacobi.cpp)
+    std::vector<unsigned char> mv, me, mf;            // 1 where a boundary condition fixes the row
+    std::vector<double> u0v, u0e, u0f, u0i;           // ug0 of the nstage update
 };
 
 // the face vertices of local face i (tet_mesh/setup.cpp:307-310)
@@ -124,11 +127,10 @@ void deriv(const hp_tet_tables &t, int dir, const double *f, double *dst) {
             }
 }
 
-void element_rsdl(const OT &o, int tind, int stage, double lf_re[NV][HP_TET_MAXT], double lf_im[NV][HP_TET_MAXT]) {
+void element_rsdl_uht(const OT &o, int tind, int stage, const double uht[NV][HP_TET_MAXT],
+                      double lf_re[NV][HP_TET_MAXT], double lf_im[NV][HP_TET_MAXT]) {
     const hp_tet_tables &t = o.t;
     const int Q = t.G * t.G * t.G, T = t.T;
-    double uht[NV][HP_TET_MAXT];
-    gather(o, tind, uht);
     // straight element: ldcrd(n, 0..2) = (v3 - v2, v1 - v2, v0 - v2) / 2
     const int *v = &o.tp[4 * tind];
     double ld[3][3];
@@ -236,6 +238,29 @@ void element_rsdl(const OT &o, int tind, int stage, double lf_re[NV][HP_TET_MAXT
     intgrtrst(t, lf_re[NV - 1], &DU(NV - 1, 0, 0), &DU(NV - 1, 1, 0), &DU(NV - 1, 2, 0));
     for (int n = 0; n < NV; ++n)
         for (int m = 0; m < T; ++m) lf_re[n][m] *= beta;
+}
+
+void element_rsdl(const OT &o, int tind, int stage, double lf_re[NV][HP_TET_MAXT], double lf_im[NV][HP_TET_MAXT]) {
+    double uht[NV][HP_TET_MAXT];
+    gather(o, tind, uht);
+    element_rsdl_uht(o, tind, stage, uht, lf_re, lf_im);
+}
+
+// lftog without the edge / face signs (for diagonal entries: sign * sign = 1)
+void scatter_unsigned(const OT &o, int tind, const double lf[NV][HP_TET_MAXT], double *gv, double *ge, double *gf,
+                      double *gi) {
+    const hp_tet_tables &t = o.t;
+    for (int i = 0; i < 4; ++i)
+        for (int n = 0; n < NV; ++n) gv[(size_t)o.tp[4 * tind + i] * NV + n] += lf[n][i];
+    int indx = 4;
+    for (int i = 0; i < 6; ++i)
+        for (int m = 0; m < t.em; ++m, ++indx)
+            for (int n = 0; n < NV; ++n) ge[((size_t)o.ts[6 * tind + i] * t.em + m) * NV + n] += lf[n][indx];
+    for (int i = 0; i < 4; ++i)
+        for (int m = 0; m < t.fm; ++m, ++indx)
+            for (int n = 0; n < NV; ++n) gf[((size_t)o.tt[4 * tind + i] * t.fm + m) * NV + n] += lf[n][indx];
+    for (int m = 0; m < t.im; ++m, ++indx)
+        for (int n = 0; n < NV; ++n) gi[((size_t)tind * t.im + m) * NV + n] += lf[n][indx];
 }
 
 }  // namespace
@@ -350,6 +375,106 @@ int ot_setup_preconditioner(void *h) {
                 for (int n = 0; n < NV; ++n) o.fprcn[(size_t)o.tt[4 * tind + i] * NV + n] += ip[n];
     }
     return err;
+}
+
+// Rows fixed by essential (velocity) conditions: mask arrays over vertices [npnt][NV],
+// edges [nseg][NV], faces [ntri][NV] (1 = zero this row; the boundary faces' vdirichlet /
+// edirichlet / fdirichlet of bdry_ins::inflow, tet_hp/ins/bdry_ins.h:141-183).
+void ot_set_dirichlet(void *h, const unsigned char *mv, const unsigned char *me, const unsigned char *mf) {
+    OT &o = *static_cast<OT *>(h);
+    o.mv.assign(mv, mv + (size_t)o.npnt * NV);
+    o.me.assign(me, me + (size_t)o.nseg * NV);
+    o.mf.assign(mf, mf + (size_t)o.ntri * NV);
+}
+
+static void all_dirichlet(OT &o) {
+    if (o.mv.empty()) return;
+    for (size_t k = 0; k < o.rv.size(); ++k)
+        if (o.mv[k]) o.rv[k] = 0.0;
+    for (int e = 0; e < o.nseg; ++e)
+        for (int m = 0; m < o.t.em; ++m)
+            for (int n = 0; n < NV; ++n)
+                if (o.me[(size_t)e * NV + n]) o.re[((size_t)e * o.t.em + m) * NV + n] = 0.0;
+    for (int f = 0; f < o.ntri; ++f)
+        for (int m = 0; m < o.t.fm; ++m)
+            for (int n = 0; n < NV; ++n)
+                if (o.mf[(size_t)f * NV + n]) o.rf[((size_t)f * o.t.fm + m) * NV + n] = 0.0;
+}
+
+// tet_hp::jacobian_diagonal (jacobi.cpp:32-111): finite-difference diagonal of every
+// element's Jacobian at stage 0, summed into the global diagonal.
+void ot_jacobian_diagonal(void *h) {
+    OT &o = *static_cast<OT *>(h);
+    const hp_tet_tables &t = o.t;
+    const int T = t.T;
+    o.jv.assign(o.ugv.size(), 0.0);
+    o.je.assign(o.uge.size(), 0.0);
+    o.jf.assign(o.ugf.size(), 0.0);
+    o.ji.assign(o.ugi.size(), 0.0);
+    const double eps_r = 1.0e-6, eps_a = 1.0e-10;
+    double lf_re[NV][HP_TET_MAXT], lf_im[NV][HP_TET_MAXT], rbar[NV][HP_TET_MAXT], lf[NV][HP_TET_MAXT];
+    std::vector<double> kd((size_t)T * NV);
+    for (int tind = 0; tind < o.ntet; ++tind) {
+        double uht[NV][HP_TET_MAXT];
+        gather(o, tind, uht);
+        double dw = 0.0;  // the same for every variable (jacobi.cpp:63-67 adds to all entries)
+        for (int i = 0; i < 4; ++i)
+            for (int n = 0; n < NV; ++n) dw += std::fabs(uht[n][i]);
+        dw = dw * eps_r + eps_a;
+        element_rsdl_uht(o, tind, 0, uht, lf_re, lf_im);
+        for (int i = 0; i < T; ++i)
+            for (int n = 0; n < NV; ++n) rbar[n][i] = lf_re[n][i] + lf_im[n][i];
+        int ind = 0;
+        for (int i = 0; i < T; ++i)
+            for (int n = 0; n < NV; ++n) {
+                uht[n][i] += dw;
+                element_rsdl_uht(o, tind, 0, uht, lf_re, lf_im);
+                kd[ind++] = (lf_re[n][i] + lf_im[n][i] - rbar[n][i]) / dw;
+                uht[n][i] -= dw;
+            }
+        // kd is in (mode, variable) order; add to the global diagonal (no signs: sign^2 = 1)
+        for (int i = 0; i < T; ++i)
+            for (int n = 0; n < NV; ++n) lf[n][i] = kd[(size_t)i * NV + n];
+        scatter_unsigned(o, tind, lf, o.jv.data(), o.je.data(), o.jf.data(), o.ji.data());
+    }
+}
+
+// tet_hp::jacobi_relaxation (jacobi.cpp:14-30): res = omega res / jacob_diag, then the
+// essential rows are zeroed.
+static void jacobi_relaxation(OT &o) {
+    const double omega = 0.5;
+    for (size_t k = 0; k < o.rv.size(); ++k) o.rv[k] = omega * o.rv[k] / o.jv[k];
+    for (size_t k = 0; k < o.re.size(); ++k) o.re[k] = omega * o.re[k] / o.je[k];
+    for (size_t k = 0; k < o.rf.size(); ++k) o.rf[k] = omega * o.rf[k] / o.jf[k];
+    for (size_t k = 0; k < o.ri.size(); ++k) o.ri[k] = omega * o.ri[k] / o.ji[k];
+    all_dirichlet(o);
+}
+
+void ot_rsdl(void *h, int stage);
+
+// tet_hp::update, JACOBI build (update.cpp:181-390): nstage stages of rsdl, boundary
+// zeroing, Jacobi relaxation and ug = ug0 - alpha(stage) cfl res.
+void ot_update(void *h) {
+    OT &o = *static_cast<OT *>(h);
+    o.u0v = o.ugv; o.u0e = o.uge; o.u0f = o.ugf; o.u0i = o.ugi;
+    for (int stage = 0; stage < o.ph.nstage; ++stage) {
+        ot_rsdl(h, stage);
+        all_dirichlet(o);
+        jacobi_relaxation(o);
+        const double ca = o.ph.alpha[stage] * o.ph.cfl;
+        for (size_t k = 0; k < o.ugv.size(); ++k) o.ugv[k] = o.u0v[k] - ca * o.rv[k];
+        for (size_t k = 0; k < o.uge.size(); ++k) o.uge[k] = o.u0e[k] - ca * o.re[k];
+        for (size_t k = 0; k < o.ugf.size(); ++k) o.ugf[k] = o.u0f[k] - ca * o.rf[k];
+        for (size_t k = 0; k < o.ugi.size(); ++k) o.ugi[k] = o.u0i[k] - ca * o.ri[k];
+    }
+}
+
+void ot_get_jacobian_diagonal(void *h, double *v, double *e, double *f, double *i) {
+    OT &o = *static_cast<OT *>(h);
+    std::memcpy(v, o.jv.data(), o.jv.size() * 8);
+    if (!o.je.empty()) std::memcpy(e, o.je.data(), o.je.size() * 8);
+    if (!o.jf.empty()) std::memcpy(f, o.jf.data(), o.jf.size() * 8);
+    if (!o.ji.empty()) std::memcpy(i, o.ji.data(), o.ji.size() * 8);
 }
 
 // tet_hp::rsdl (update.cpp:9-118) without boundary fluxes and coarse-level terms

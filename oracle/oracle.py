@@ -60,6 +60,10 @@ def lib():
         o.ot_get_prcn.argtypes = [P, P, P]
         o.ot_setup_preconditioner.argtypes = [P]
         o.ot_rsdl.argtypes = [P, I]
+        o.ot_set_dirichlet.argtypes = [P, P, P, P]
+        o.ot_jacobian_diagonal.argtypes = [P]
+        o.ot_get_jacobian_diagonal.argtypes = [P, P, P, P, P]
+        o.ot_update.argtypes = [P]
         _o = o
     return _o
 
@@ -216,3 +220,16 @@ class OracleTet:
 
     def rsdl(self, stage):
         lib().ot_rsdl(self.h, stage)
+
+    def set_dirichlet(self, masks):
+        mv, me, mf = (np.ascontiguousarray(a, dtype=np.uint8) for a in masks)
+        lib().ot_set_dirichlet(self.h, _p(mv), _p(me), _p(mf))
+
+    def jacobian_diagonal(self):
+        lib().ot_jacobian_diagonal(self.h)
+        out = [np.zeros_like(a) for a in self.prob.state]
+        lib().ot_get_jacobian_diagonal(self.h, *[_p(a) for a in out])
+        return out
+
+    def update(self):
+        lib().ot_update(self.h)
