@@ -752,6 +752,60 @@ __global__ void k_tet_sq(long n, const double *res, const unsigned char *mask, d
     if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
+// ---- multigrid transfers (tet_hp/mg_restrict.cpp, mg_prolongate.cpp) ----
+// p-levels share the mesh: coarse entry c is fine entry map[c] (mode truncation)
+__global__ void k_tet_p_restrict(long n, const int *map, const double *fu, const double *fres, double *u,
+                                 double *uf, double *res0) {
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
+        const double v = fu[map[c]];
+        u[c] = v;
+        uf[c] = v;
+        res0[c] = fres[map[c]];
+    }
+}
+__global__ void k_tet_p_prolong(long n, const int *map, const double *u, const double *uf, double *fu) {
+    for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
+        fu[map[c]] += u[c] - uf[c];
+}
+// h-levels at p = 1: vertex values, each point in a tetrahedron of the other mesh
+__global__ void k_tet_h_restrict_state(int ncp, const int *tet, const double *w, const int *ftp, const double *fu,
+                                       double *u, double *uf) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < ncp; v += gridDim.x * blockDim.x)
+        for (int n = 0; n < NV; ++n) {
+            double s = 0.0;
+            for (int j = 0; j < 4; ++j) s += w[4 * v + j] * fu[(size_t)ftp[4 * tet[v] + j] * NV + n];
+            u[(size_t)v * NV + n] = s;
+            uf[(size_t)v * NV + n] = s;
+        }
+}
+__global__ void k_tet_h_restrict_res(int nfp, const int *tet, const double *w, const int *ctp, const double *fres,
+                                     double *res0) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nfp; v += gridDim.x * blockDim.x)
+        for (int j = 0; j < 4; ++j)
+            for (int n = 0; n < NV; ++n)
+                atomicAdd(res0 + (size_t)ctp[4 * tet[v] + j] * NV + n, w[4 * v + j] * fres[(size_t)v * NV + n]);
+}
+__global__ void k_tet_h_prolong(int nfp, const int *tet, const double *w, const int *ctp, const double *u,
+                                const double *uf, double *fu) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nfp; v += gridDim.x * blockDim.x)
+        for (int n = 0; n < NV; ++n) {
+            double s = 0.0;
+            for (int j = 0; j < 4; ++j) {
+                const size_t c = (size_t)ctp[4 * tet[v] + j] * NV + n;
+                s += w[4 * v + j] * (u[c] - uf[c]);
+            }
+            fu[(size_t)v * NV + n] += s;
+        }
+}
+// FAS driving term (tet_hp::rsdl, update.cpp:97-117): on the first residual after a
+// restriction dres = fadd res0 - res; every coarse residual then adds dres
+__global__ void k_tet_fas(long n, double *res, const double *res0, double *dres, double fadd, int first) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        if (first) dres[k] = fadd * res0[k] - res[k];
+        res[k] += dres[k];
+    }
+}
+
 int nblk(long n, int b) { return (int)std::max<long>(1, (n + b - 1) / b); }
 
 }  // namespace
@@ -773,6 +827,15 @@ struct hp_tet_ctx {
     double *U0 = nullptr, *JD = nullptr, *rbar = nullptr, *part = nullptr;  // update, jacob_diag
     unsigned char *mask = nullptr;  // 1: row fixed by an essential condition
     bool jd_ready = false;
+    // multigrid: this level is coarser than `fine` (kind 1: p-level, 2: h-level)
+    hp_tet_ctx *fine = nullptr;
+    int kind = 0;
+    double fadd = 1.0;
+    bool fas_pending = false;
+    int *pmap = nullptr;                    // p-level: fine index of every coarse entry
+    int *c2f_tet = nullptr, *f2c_tet = nullptr;
+    double *c2f_w = nullptr, *f2c_w = nullptr;
+    double *RES0 = nullptr, *DRES = nullptr, *UF = nullptr;
     hp_tet_tables tab{};
     bool prcn_ready = false;
     TetFields<double> fields(double *base) const {
@@ -821,6 +884,19 @@ void tet_fragments(const hp_tet_tables &b, std::vector<double> &proj, std::vecto
             }
 }
 
+// dynamic shared memory above 48 KB for every instantiation, once per process
+template <int P>
+int ensure_attrs() {
+    using M = TetMma<P>;
+    static bool done = false;
+    if (done) return HP_OK;
+    TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::SMEM));
+    TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::SMEM));
+    TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::SMEM));
+    done = true;
+    return HP_OK;
+}
+
 template <int P>
 int launch_rsdl(hp_tet_ctx *c, int stage) {
     using C = TetCfg<P>;
@@ -853,13 +929,7 @@ int launch_rsdl(hp_tet_ctx *c, int stage) {
                                                                                            c->RR, omb);
     using M = TetMma<P>;
     const size_t smem2 = (size_t)M::S_WARP * M::WPC * sizeof(double);
-    static bool attr2 = false;
-    if (!attr2) {
-        TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-        TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-        TCK(cudaFuncSetAttribute(k_tet_rsdl_mma<P, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-        attr2 = true;
-    }
+    if (int r = ensure_attrs<P>()) return r;
     (void)ops;
     const long npair = ((long)c->mesh.ntet + 1) / 2;
     int blocks = std::min(nblk(npair, M::WPC), c->nsm * 32);
@@ -868,6 +938,11 @@ int launch_rsdl(hp_tet_ctx *c, int stage) {
         c->ph.mu, beta, nullptr, TetFields<double>{});
     k_tet_fold<double><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>((long)c->ltot, c->RES,
                                                                                             c->RR);
+    if (c->fine) {
+        k_tet_fas<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+            (long)c->ltot, c->RES, c->RES0, c->DRES, c->fadd, c->fas_pending ? 1 : 0);
+        c->fas_pending = false;
+    }
     TCK(cudaGetLastError());
     return HP_OK;
 }
@@ -876,7 +951,7 @@ template <int P>
 int launch_jacdiag(hp_tet_ctx *c) {
     using C = TetCfg<P>;
     using M = TetMma<P>;
-    int r = launch_rsdl<P>(c, c->ph.nstage);  // sets the kernel attributes on first use
+    int r = ensure_attrs<P>();
     if (r) return r;
     TetSmall<double, P> sm;
     const hp_tet_tables &t = c->tab;
@@ -1268,5 +1343,186 @@ extern "C" int hp_tet_solve(hp_tet_ctx *c, double drop, int max_updates, int che
     if (nhist) *nhist = nh;
     if (seconds) *seconds = ms * 1e-3;
     if (updates) *updates = nu;
+    return HP_OK;
+}
+
+namespace {
+int attach_common(hp_tet_ctx *c, hp_tet_ctx *f, double fadd) {
+    int r;
+    c->fine = f;
+    c->fadd = fadd;
+    for (double **b : {&c->RES0, &c->DRES, &c->UF}) {
+        if (!*b && (r = talloc(c, (void **)b, 8 * c->ltot))) return r;
+        TCK(cudaMemset(*b, 0, 8 * c->ltot));
+    }
+    return HP_OK;
+}
+}  // namespace
+
+// p-level: coarse has the fine level's mesh at a lower p (mode truncation of the
+// hierarchical basis: edge mode k, face mode (row m, k), interior (m, k, j) keep their
+// indices; tet_hp/mg_restrict.cpp:9-57)
+extern "C" int hp_tet_mg_attach_p(hp_tet_ctx *coarse, hp_tet_ctx *fine, double fadd) {
+    if (!coarse || !fine || coarse->p >= fine->p || coarse->mesh.ntet != fine->mesh.ntet) return HP_EINVAL;
+    hp_tet_ctx *c = coarse, *f = fine;
+    std::vector<int> map(c->ltot);
+    size_t k = 0;
+    for (size_t v = 0; v < c->lv; ++v) map[k++] = (int)v;
+    for (int e = 0; e < c->mesh.nseg; ++e)
+        for (int m = 0; m < c->em; ++m)
+            for (int n = 0; n < NV; ++n) map[k++] = (int)(f->lv + ((size_t)e * f->em + m) * NV + n);
+    auto face_index = [](int em, int row, int col) {  // (row m >= 1, col k >= 1) -> index
+        int idx = 0;
+        for (int m = 1; m < row; ++m) idx += em - m;
+        return idx + col - 1;
+    };
+    for (int t = 0; t < c->mesh.ntri; ++t)
+        for (int m = 1; m <= c->em - 1; ++m)
+            for (int kk = 1; kk <= c->em - m; ++kk)
+                for (int n = 0; n < NV; ++n)
+                    map[k++] = (int)(f->lv + f->le + ((size_t)t * f->fm + face_index(f->em, m, kk)) * NV + n);
+    auto int_index = [](int em, int a, int b, int cc) {
+        int idx = 0;
+        for (int m = 1; m <= em - 1; ++m)
+            for (int kk = 1; kk <= em - m; ++kk)
+                for (int j = 1; j <= em - m - kk; ++j) {
+                    if (m == a && kk == b && j == cc) return idx;
+                    ++idx;
+                }
+        return -1;
+    };
+    for (int t = 0; t < c->mesh.ntet; ++t)
+        for (int m = 1; m <= c->em - 1; ++m)
+            for (int kk = 1; kk <= c->em - m; ++kk)
+                for (int j = 1; j <= c->em - m - kk; ++j)
+                    for (int n = 0; n < NV; ++n)
+                        map[k++] = (int)(f->lv + f->le + f->lf + ((size_t)t * f->im + int_index(f->em, m, kk, j)) * NV + n);
+    if (k != c->ltot) {
+        set_err("p-level map size mismatch");
+        return HP_EINVAL;
+    }
+    int r;
+    if (!c->pmap && (r = talloc(c, (void **)&c->pmap, 4 * c->ltot))) return r;
+    TCK(cudaMemcpy(c->pmap, map.data(), 4 * c->ltot, cudaMemcpyHostToDevice));
+    c->kind = 1;
+    return attach_common(c, f, fadd);
+}
+
+// h-level at p = 1: f2c [fine npnt] tetrahedron of the coarse mesh holding each fine
+// vertex with its 4 barycentric weights (tet_mesh ccnnct), c2f [coarse npnt] likewise in
+// the fine mesh (fcnnct)
+extern "C" int hp_tet_mg_attach_h(hp_tet_ctx *coarse, hp_tet_ctx *fine, const int *f2c_tet, const double *f2c_w,
+                                  const int *c2f_tet, const double *c2f_w, double fadd) {
+    if (!coarse || !fine || coarse->p != 1 || fine->p != 1 || !f2c_tet || !f2c_w || !c2f_tet || !c2f_w)
+        return HP_EINVAL;
+    hp_tet_ctx *c = coarse;
+    int r;
+    const size_t nf = fine->mesh.npnt, nc = c->mesh.npnt;
+    if ((r = talloc(c, (void **)&c->f2c_tet, 4 * nf)) || (r = talloc(c, (void **)&c->f2c_w, 32 * nf)) ||
+        (r = talloc(c, (void **)&c->c2f_tet, 4 * nc)) || (r = talloc(c, (void **)&c->c2f_w, 32 * nc)))
+        return r;
+    TCK(cudaMemcpy(c->f2c_tet, f2c_tet, 4 * nf, cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(c->f2c_w, f2c_w, 32 * nf, cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(c->c2f_tet, c2f_tet, 4 * nc, cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(c->c2f_w, c2f_w, 32 * nc, cudaMemcpyHostToDevice));
+    c->kind = 2;
+    return attach_common(c, fine, fadd);
+}
+
+// mg_restrict: the fine residual (rsdl(nstage) already enqueued on the fine level) and
+// state onto this level; the next residual evaluation here forms the FAS term
+static int tet_mg_restrict(hp_tet_ctx *c) {
+    hp_tet_ctx *f = c->fine;
+    if (c->kind == 1) {
+        k_tet_p_restrict<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+            (long)c->ltot, c->pmap, f->U, f->RES, c->U, c->UF, c->RES0);
+    } else {
+        k_tet_h_restrict_state<<<nblk(c->mesh.npnt, 128), 128, 0, c->stream>>>(c->mesh.npnt, c->c2f_tet, c->c2f_w,
+                                                                             f->mesh.tp, f->U, c->U, c->UF);
+        TCK(cudaMemsetAsync(c->RES0, 0, 8 * c->ltot, c->stream));
+        k_tet_h_restrict_res<<<nblk(f->mesh.npnt, 128), 128, 0, c->stream>>>(f->mesh.npnt, c->f2c_tet, c->f2c_w,
+                                                                          c->mesh.tp, f->RES, c->RES0);
+    }
+    TCK(cudaGetLastError());
+    c->fas_pending = true;
+    return HP_OK;
+}
+
+static int tet_mg_prolongate(hp_tet_ctx *c) {
+    hp_tet_ctx *f = c->fine;
+    if (c->kind == 1)
+        k_tet_p_prolong<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>((long)c->ltot, c->pmap,
+                                                                                             c->U, c->UF, f->U);
+    else
+        k_tet_h_prolong<<<nblk(f->mesh.npnt, 128), 128, 0, c->stream>>>(f->mesh.npnt, c->f2c_tet, c->f2c_w,
+                                                                     c->mesh.tp, c->U, c->UF, f->U);
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+// block::cycle (tri_mesh/blocks.cpp:1267-1348) over levels[0] (finest) .. levels[n-1];
+// a level's preconditioner (tau and the Jacobian diagonal) is set up on its first visit
+static int tet_cycle(hp_tet_ctx **lv, int n, int lvl, int vw, int itercrsn, int iterrfne) {
+    hp_tet_ctx *c = lv[lvl];
+    int r;
+    for (int vc = 0; vc < vw; ++vc) {
+        if (!c->jd_ready) {
+            r = hp_tet_setup_preconditioner(c);
+            if (r) return r < 0 ? r : HP_ESTATE;
+            if ((r = hp_tet_jacobian_diagonal(c))) return r;
+        }
+        for (int it = 0; it < itercrsn; ++it)
+            if ((r = hp_tet_enqueue_update(c))) return r;
+        if (lvl == n - 1) return HP_OK;
+        if ((r = hp_tet_enqueue_rsdl(c, c->ph.nstage))) return r;
+        if ((r = tet_mg_restrict(lv[lvl + 1]))) return r;
+        if ((r = tet_cycle(lv, n, lvl + 1, vw, itercrsn, iterrfne))) return r;
+        if ((r = tet_mg_prolongate(lv[lvl + 1]))) return r;
+        for (int it = 0; it < iterrfne; ++it)
+            if ((r = hp_tet_enqueue_update(c))) return r;
+    }
+    return HP_OK;
+}
+
+extern "C" int hp_tet_solve_mg(hp_tet_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
+                               int iterrfne, double *hist, int cap, int *nhist, double *seconds, int *cycles) {
+    if (!levels || nlevels < 1 || drop <= 0 || max_cycles < 1 || vw < 1 || !hist || cap < 1) return HP_EINVAL;
+    for (int l = 1; l < nlevels; ++l)
+        if (!levels[l]->fine || levels[l]->fine != levels[l - 1] || levels[l]->stream != levels[0]->stream) {
+            set_err("hp_tet_solve_mg: levels must be attached in order and share one stream");
+            return HP_EINVAL;
+        }
+    hp_tet_ctx *f = levels[0];
+    cudaEvent_t e0, e1;
+    TCK(cudaEventCreate(&e0));
+    TCK(cudaEventCreate(&e1));
+    TCK(cudaEventRecord(e0, f->stream));
+    int r;
+    if (!f->prcn_ready) {
+        r = hp_tet_setup_preconditioner(f);
+        if (r) return r < 0 ? r : HP_ESTATE;
+    }
+    double r0;
+    if ((r = hp_tet_resnorm(f, &r0))) return r;
+    int nh = 0, nc = 0;
+    hist[nh++] = 1.0;
+    while (nc < max_cycles) {
+        if ((r = tet_cycle(levels, nlevels, 0, vw, itercrsn, iterrfne))) return r;
+        ++nc;
+        double rn;
+        if ((r = hp_tet_resnorm(f, &rn))) return r;
+        const double d = r0 > 0 ? rn / r0 : 0.0;
+        if (nh < cap) hist[nh++] = d;
+        if (!(d == d) || d <= drop) break;
+    }
+    TCK(cudaEventRecord(e1, f->stream));
+    TCK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    TCK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (nhist) *nhist = nh;
+    if (seconds) *seconds = ms * 1e-3;
+    if (cycles) *cycles = nc;
     return HP_OK;
 }

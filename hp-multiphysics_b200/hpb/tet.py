@@ -279,3 +279,90 @@ class TetGPU:
         _check(self.lib, self.lib.hp_tet_solve(self.h, drop, max_updates, check_every, self._p(hist), cap,
                                                ctypes.byref(nh), ctypes.byref(sec), ctypes.byref(nu)), "solve")
         return hist[:nh.value], sec.value, nu.value
+
+
+def locate_cube(mesh, n, pts, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
+    """The tetrahedron of cube_tets(n) holding each point (tet_mesh::findtet) and its 4
+    barycentric weights in that tetrahedron's vertex order (getwgts): the point's
+    hexahedron is found by index, then the best of its 6 tetrahedra. Weights below
+    1e-13 are dropped and the rest renormalised, so points on a face of the box take
+    weights from that face only."""
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    pts = np.asarray(pts, float)
+    ijk = np.clip(np.floor((pts - lo) / ((hi - lo) / n)).astype(np.int64), 0, n - 1)
+    hexi = (ijk[:, 0] * n + ijk[:, 1]) * n + ijk[:, 2]
+    best_t = np.zeros(len(pts), np.int64)
+    best_w = np.zeros((len(pts), 4))
+    best_m = np.full(len(pts), -np.inf)
+    P = mesh.pnts
+    for k in range(6):
+        t = hexi * 6 + k
+        v = mesh.tet_pnt[t]
+        A = np.stack([P[v[:, 1]] - P[v[:, 0]], P[v[:, 2]] - P[v[:, 0]], P[v[:, 3]] - P[v[:, 0]]], axis=2)
+        lam = np.linalg.solve(A, (pts - P[v[:, 0]])[:, :, None])[:, :, 0]
+        w = np.concatenate([1.0 - lam.sum(1, keepdims=True), lam], axis=1)
+        m = w.min(1)
+        better = m > best_m
+        best_m[better], best_t[better], best_w[better] = m[better], t[better], w[better]
+    if np.any(best_m < -1e-9):
+        raise ValueError("point outside the mesh")
+    best_w[np.abs(best_w) < 1e-13] = 0.0
+    best_w /= best_w.sum(1, keepdims=True)
+    return best_t.astype(np.int32), np.ascontiguousarray(best_w)
+
+
+class TetHierarchy:
+    """tet multigrid on the unit cube: p-levels p, p-1, ..., 1 on cube_tets(n), then
+    h-levels cube_tets(n/2), cube_tets(n/4), ... at p = 1 (the reference decrements
+    log2p = p - 1 for tetrahedra; h-levels as tet_mesh coarsening). Every level takes the
+    Beltrami state, essential velocity on the six faces, and `cfl[p]`."""
+
+    def __init__(self, n, p, hlevels=2, mu=0.01, cfl=None, re=100.0, noise=1e-3, stream=None, fadd=1.0):
+        import torch
+        from .tetmesh import cube_tets
+        cfl = cfl or {1: 2.2, 2: 1.5, 3: 1.0, 4: 0.5}
+        if stream is None:
+            self._stream = torch.cuda.Stream()
+            stream = ctypes.c_void_p(self._stream.cuda_stream)
+        meshes = [(cube_tets(n), n)] + [(cube_tets(n >> k), n >> k) for k in range(1, hlevels + 1)]
+        specs = [(0, q) for q in range(p, 0, -1)] + [(k, 1) for k in range(1, hlevels + 1)]
+        self.probs, self.levels, self.kinds = [], [], []
+        for li, (mi, q) in enumerate(specs):
+            pr = TetProblem(meshes[mi][0], q, mu=mu, cfl=cfl[q]).set_beltrami(re=re, noise=noise)
+            g = TetGPU(pr, stream=stream)
+            g.set_dirichlet(pr.dirichlet_masks())
+            self.probs.append(pr)
+            self.levels.append(g)
+        lib = self.levels[0].lib
+        lib.hp_tet_mg_attach_p.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
+        P_ = ctypes.c_void_p
+        lib.hp_tet_mg_attach_h.argtypes = [P_, P_, P_, P_, P_, P_, ctypes.c_double]
+        lib.hp_tet_solve_mg.argtypes = [ctypes.POINTER(P_), _I, ctypes.c_double, _I, _I, _I, _I, P_, _I,
+                                        ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I)]
+        self._keep = []
+        for li in range(1, len(specs)):
+            c, f = self.levels[li], self.levels[li - 1]
+            if specs[li][0] == specs[li - 1][0]:
+                _check(lib, lib.hp_tet_mg_attach_p(c.h, f.h, fadd), "mg_attach_p")
+            else:
+                (fm, fn), (cm, cn) = meshes[specs[li - 1][0]], meshes[specs[li][0]]
+                f2c = locate_cube(cm, cn, fm.pnts)
+                c2f = locate_cube(fm, fn, cm.pnts)
+                self._keep += [f2c, c2f]
+                _check(lib, lib.hp_tet_mg_attach_h(c.h, f.h, f2c[0].ctypes.data, f2c[1].ctypes.data,
+                                                   c2f[0].ctypes.data, c2f[1].ctypes.data, fadd), "mg_attach_h")
+        self.lib = lib
+
+    def solve(self, drop=1e-10, max_cycles=300, vw=1, itercrsn=2, iterrfne=2):
+        hs = (ctypes.c_void_p * len(self.levels))(*[g.h for g in self.levels])
+        hist = np.zeros(max_cycles + 2)
+        nh, nc = ctypes.c_int(), ctypes.c_int()
+        sec = ctypes.c_double()
+        _check(self.lib, self.lib.hp_tet_solve_mg(hs, len(self.levels), drop, max_cycles, vw, itercrsn, iterrfne,
+                                                  hist.ctypes.data, len(hist), ctypes.byref(nh), ctypes.byref(sec),
+                                                  ctypes.byref(nc)), "solve_mg")
+        return hist[:nh.value], sec.value, nc.value
+
+    def close(self):
+        for g in self.levels:
+            g.close()

@@ -121,6 +121,20 @@ int hp_tet_resnorm(hp_tet_ctx *ctx, double *l2);
 int hp_tet_solve(hp_tet_ctx *ctx, double drop, int max_updates, int check_every, double *hist, int cap,
                  int *nhist, double *seconds, int *updates);
 
+/* Multigrid (tet_hp/mg_restrict.cpp, mg_prolongate.cpp, tri_mesh/blocks.cpp:1267 cycle).
+ * p-level: `coarse` has fine's mesh at a lower p (the hierarchical modes truncate).
+ * h-level (both p = 1): f2c_tet / f2c_w [fine npnt][4]: the coarse tetrahedron holding
+ * each fine vertex and its barycentric weights; c2f_tet / c2f_w [coarse npnt][4] the
+ * same in the fine mesh. fadd scales the FAS source dres = fadd res0 - res. */
+int hp_tet_mg_attach_p(hp_tet_ctx *coarse, hp_tet_ctx *fine, double fadd);
+int hp_tet_mg_attach_h(hp_tet_ctx *coarse, hp_tet_ctx *fine, const int *f2c_tet, const double *f2c_w,
+                       const int *c2f_tet, const double *c2f_w, double fadd);
+/* vw cycles per level (1 V, 2 W), itercrsn / iterrfne updates before / after the coarse
+ * correction, until the finest residual norm drops by `drop` or max_cycles; each level's
+ * preconditioner is set up on its first visit. Levels share one stream. */
+int hp_tet_solve_mg(hp_tet_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
+                    int iterrfne, double *hist, int cap, int *nhist, double *seconds, int *cycles);
+
 /* Measurement helper (no counterpart in the reference): the FP64 tensor-core
  * (mma.m8n8k4.f64) throughput of this GPU, from independent accumulation chains
  * on every SM for about `ms` milliseconds. Writes TFLOP/s (2 flops per multiply-add). */

@@ -66,3 +66,20 @@ def test_tet_jacobi_updates_match_oracle(p):
     mv = masks[0].astype(bool)
     assert np.array_equal(g.state()[0][mv], u0[mv])
     g.close()
+
+
+def test_tet_multigrid_reduces_residual_and_keeps_essential_values():
+    """p-levels 3, 2, 1 and two h-levels (tet_hp mg_restrict / mg_prolongate with the
+    FAS source): the residual falls, and the velocity on the boundary faces (essential)
+    is unchanged by smoothing and by every prolongation."""
+    from hpb.tet import TetHierarchy
+    H = TetHierarchy(8, 3, hlevels=2, mu=0.01, cfl={1: 0.5, 2: 0.5, 3: 0.5})
+    u0 = [a.copy() for a in H.probs[0].state]
+    hist, sec, cycles = H.solve(drop=1e-10, max_cycles=30, vw=1)
+    assert np.all(np.isfinite(hist)) and hist[-1] < 0.2
+    mv, me, mf = (m.astype(bool) for m in H.probs[0].dirichlet_masks())
+    u = H.levels[0].state()
+    assert np.array_equal(u[0][mv], u0[0][mv])
+    assert np.array_equal(u[1][np.broadcast_to(me[:, None, :], u[1].shape)],
+                          u0[1][np.broadcast_to(me[:, None, :], u0[1].shape)])
+    H.close()
