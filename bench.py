@@ -301,6 +301,34 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed):
                          "frac": achieved / peak.value,
                          "peak_source": "hp_tet_fp64_mma_peak: mma.m8n8k4.f64 chains on every SM, measured in this run"}}
     g.close()
+    # smoothing legs: the JACOBI build's update (finite-difference Jacobian diagonal,
+    # omega 0.5) with the velocity fixed on the six faces; cfl 0.5 on every level (the
+    # reference's tet defaults 2.2 / 1.5 / 1.0 for p = 1 / 2 / 3 diverge with this smoother
+    # at p >= 2)
+    from hpb.tet import TetHierarchy
+    cfl = {1: 0.5, 2: 0.5, 3: 0.5, 4: 0.5}
+    small = 8
+    ps = TetProblem(cube_tets(small), p, mu=1.0 / 100.0, cfl=cfl[p]).set_beltrami(re=100.0)
+    gs = TetGPU(ps, device=dev, stream=ctypes.c_void_p(cur.cuda_stream))
+    gs.set_dirichlet(ps.dirichlet_masks())
+    h, sec, nu = gs.solve(drop=1e-10, max_updates=20000, check_every=100)
+    line["solve_single_grid_small"] = {"mesh": f"{small}^3 x 6", "ndof": ps.ndof, "seconds": sec, "updates": nu,
+                                       "drop": float(h[-1]), "reached": bool(h[-1] <= 1e-10)}
+    gs.close()
+    H = TetHierarchy(small, p, hlevels=2, mu=1.0 / 100.0, cfl=cfl, stream=ctypes.c_void_p(cur.cuda_stream))
+    h, sec, nc = H.solve(drop=1e-10, max_cycles=400, vw=1)
+    line["solve_multigrid_small"] = {"mesh": f"{small}^3 x 6", "levels": f"p {p}..1, then {small // 2}^3, "
+                                     f"{small // 4}^3 at p = 1", "seconds": sec, "cycles": nc,
+                                     "drop": float(h[-1]), "reached": bool(h[-1] <= 1e-10)}
+    H.close()
+    H = TetHierarchy(n, p, hlevels=3, mu=1.0 / 100.0, cfl=cfl, stream=ctypes.c_void_p(cur.cuda_stream))
+    ncyc = max(steps, 10)
+    h, sec, nc = H.solve(drop=1e-10, max_cycles=ncyc, vw=1)
+    line["multigrid_full"] = {"mesh": f"{n}^3 x 6", "levels": f"p {p}..1, then {n // 2}^3, {n // 4}^3, {n // 8}^3 "
+                              "at p = 1", "seconds_incl_preconditioner_setup": sec, "cycles": nc,
+                              "ms_per_cycle_incl_setup": 1e3 * sec / max(nc, 1), "drop": float(h[-1]),
+                              "drop_history": [float(x) for x in h[::max(1, len(h) // 10)]]}
+    H.close()
     # CPU oracle on a bounded sample
     ps = TetProblem(cube_tets(6), p, mu=1.0 / 100.0).set_beltrami(re=100.0)
     o = OracleTet(ps)
