@@ -331,7 +331,12 @@ struct TetMma {
     static constexpr int QP = pad4(C::Q);       // u [NV][QP]
     static constexpr int VS = pad4(3 * C::Q);   // fim / fre [NV][VS], component c at c * Q
     // per tetrahedron: uht [NV][T], u [NV][QP], fim [NV][VS], fre [NV][VS]
-    static constexpr int S_EL = NV * C::T + NV * QP + 2 * NV * VS;
+    // per tetrahedron: u [3][QP] (u, v, w), fim [NV][VS], fre [NV][VS]; the gathered modes
+    // uht [NV][T] and then the pressure at the points share fre's variable-3 slot, which
+    // holds nothing else until the SUPG phase (uht is read into registers before the
+    // projection stores anything; the pressure values are last read by the pointwise phase)
+    static constexpr int S_EL = 3 * QP + 2 * NV * VS;
+    static_assert(NV * C::T <= VS && C::Q <= VS, "uht / pressure must fit fre's variable-3 slot");
     static constexpr int NG = NT < 8 ? NT : 8;  // projection n-tiles accumulated together
     static constexpr int S_WARP = 2 * S_EL;
     static constexpr size_t PROJ_LEN = (size_t)4 * NT * KS * 32, INT_LEN = (size_t)NT2 * KS2 * 32;
@@ -364,10 +369,11 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
     const int grow = lane >> 2, gcol = lane & 3;  // fragment row / column group
     double *base = reinterpret_cast<double *>(smem_raw) + warp * M::S_WARP;
     constexpr int QP = M::QP, VS = M::VS;
-    auto UHT = [&](int e) { return base + e * M::S_EL; };
-    auto UQ = [&](int e) { return base + e * M::S_EL + NV * T; };
-    auto FIM = [&](int e) { return base + e * M::S_EL + NV * T + NV * QP; };
-    auto FRE = [&](int e) { return base + e * M::S_EL + NV * T + NV * QP + NV * VS; };
+    auto UQ = [&](int e) { return base + e * M::S_EL; };
+    auto FIM = [&](int e) { return base + e * M::S_EL + 3 * QP; };
+    auto FRE = [&](int e) { return base + e * M::S_EL + 3 * QP + NV * VS; };
+    auto UHT = [&](int e) { return FRE(e) + 3 * VS; };
+    auto PV = [&](int e) { return FRE(e) + 3 * VS; };
     const long nitems = MODE == 2 ? (long)mesh.ntet * NJ : (long)mesh.ntet;
     const long npair = (nitems + 1) / 2;
     for (long pr = (long)blockIdx.x * M::WPC + warp; pr < npair; pr += (long)gridDim.x * M::WPC) {
@@ -444,9 +450,11 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
                 const int m = ks * 4 + gcol;
                 a[ks] = m < T ? UHT(e)[n * T + m] : 0.0;
             }
+            __syncwarp();  // uht is dead from here: its slot takes the pressure values
             const bool needd = beta > 0.0;
             for (int op = 0; op < (needd ? 4 : 1); ++op) {
-                double *dst = op == 0 ? UQ(e) + n * QP : (n < 3 ? FRE(e) + n * VS + (op - 1) * Q : nullptr);
+                double *dst = op == 0 ? (n < 3 ? UQ(e) + n * QP : PV(e))
+                                      : (n < 3 ? FRE(e) + n * VS + (op - 1) * Q : nullptr);
                 for (int nt0 = 0; nt0 < M::NT; nt0 += M::NG) {
                     // NG independent accumulator chains
                     double c[M::NG][2];
@@ -476,7 +484,7 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
             const int e = w / Q, q = w - e * Q;
             const double *uq = UQ(e);
             double *fim = FIM(e), *fre = FRE(e);
-            const double uu[4] = {uq[q], uq[QP + q], uq[2 * QP + q], uq[3 * QP + q]};
+            const double uu[4] = {uq[q], uq[QP + q], uq[2 * QP + q], PV(e)[q]};
             const double fx = rho * uu[0], fy = rho * uu[1], fz = rho * uu[2];
             double f3[3];
 #pragma unroll
