@@ -136,6 +136,8 @@ struct Launchers {
                        cudaStream_t);
     void (*emat_apply)(ElemMat<R>, const Mesh &, const State<R> &, const Phys &, int stage, int zero_rr, int nsm,
                        const Tune &, cudaStream_t);
+    void (*elem_jac)(const void *tab, const Mesh &, const State<R> &, const Phys &, R *K, R *rbar, int nsm,
+                     cudaStream_t);
 };
 
 template <typename R, int P, int PHYS>
@@ -154,10 +156,30 @@ struct LaunchImpl {
         if (blocks > cap) blocks = cap;
         const auto *t = reinterpret_cast<const DevTables<R, P> *>(tab);
         k_rsdl_elem<R, P, PHYS, false><<<blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, stage, zero_rr, diff,
-                                                                           ElemMat<R>{});
+                                                                           ElemMat<R>{}, ElemJac<R>{});
         if (m.ncurved > 0)
             k_rsdl_elem<R, P, PHYS, true><<<std::min(nblk(m.ncurved, EPC), cap), C::WPC * 32, smem(), st>>>(
-                t, m, s, ph, stage, zero_rr, diff, ElemMat<R>{});
+                t, m, s, ph, stage, zero_rr, diff, ElemMat<R>{}, ElemJac<R>{});
+    }
+    // finite-difference element Jacobians at stage 0: pass 0 (rbar) then pass 1 (columns)
+    static void elem_jac(const void *tab, const Mesh &m, const State<R> &s, const Phys &ph, R *K, R *rbar, int nsm,
+                         cudaStream_t st) {
+        const auto *t = reinterpret_cast<const DevTables<R, P> *>(tab);
+        constexpr int EPC = C::WPC * C::EPW, NJ = NV * C::T;
+        for (int pass = 0; pass < 2; ++pass)
+            for (int cv = 0; cv < 2; ++cv) {
+                const long nel = cv ? (long)m.ncurved : (long)m.ntri;
+                if (nel == 0) continue;
+                const long items = pass ? nel * NJ : nel;
+                const int blocks = (int)std::min<long>((items + EPC - 1) / EPC, (long)nsm * 16);
+                const ElemJac<R> jac{K, rbar, pass};
+                if (cv)
+                    k_rsdl_elem<R, P, PHYS, true><<<blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, 0, 1, 0,
+                                                                                       ElemMat<R>{}, jac);
+                else
+                    k_rsdl_elem<R, P, PHYS, false><<<blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, 0, 1, 0,
+                                                                                        ElemMat<R>{}, jac);
+            }
     }
     static size_t emat_len(long ntri) { return EmatCfg<P>::len(ntri); }
     // one warp item per (element, column j <= T) at beta(nstage) = 1
@@ -172,10 +194,10 @@ struct LaunchImpl {
                 if (blocks > (long)nsm * 16) blocks = (long)nsm * 16;
                 if (cv)
                     k_rsdl_elem<R, P, PHYS, true><<<(int)blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, ph.nstage, 1, 0,
-                                                                                            em);
+                                                                                            em, ElemJac<R>{});
                 else
                     k_rsdl_elem<R, P, PHYS, false><<<(int)blocks, C::WPC * 32, smem(), st>>>(t, m, s, ph, ph.nstage, 1,
-                                                                                             0, em);
+                                                                                             0, em, ElemJac<R>{});
             }
         }
     }
@@ -251,6 +273,7 @@ struct LaunchImpl {
         L.emat_len = &emat_len;
         L.emat_build = &emat_build;
         L.emat_apply = &emat_apply;
+        L.elem_jac = &elem_jac;
         return L;
     }
 };
@@ -1845,6 +1868,36 @@ extern "C" int hp_gpu_get_tuning(const hp_gpu_ctx *c, int *shapes, float *ms) {
             shapes[4 * k + 3] = t.minv_threads;
         }
         if (ms) { ms[2 * k] = c->tune_ms[k][0]; ms[2 * k + 1] = c->tune_ms[k][1]; }
+    }
+    return HP_OK;
+}
+
+// tri_hp::element_jacobian (nstage.cpp:131-165, fixed mesh) of every element, batched:
+// one pass for the stage-0 residuals, one item per (element, column) for the columns.
+extern "C" int hp_gpu_element_jacobian(hp_gpu_ctx *c, double *K) {
+    if (!c || !K) return HP_EINVAL;
+    if (!c->prcn_ready) {
+        set_err("hp_gpu_element_jacobian needs tau from setup_preconditioner");
+        return HP_ESTATE;
+    }
+    const size_t T = (size_t)(c->p + 1) * (c->p + 2) / 2, NJ = (size_t)c->NV * T;
+    const size_t kb = (size_t)c->ntri * NJ * NJ * sizeof(double), rb = (size_t)c->ntri * NJ * sizeof(double);
+    double *dK = nullptr, *dR = nullptr;
+    if (!c->pool || cudaMallocFromPoolAsync((void **)&dK, kb, c->pool, c->stream) != cudaSuccess ||
+        cudaMallocFromPoolAsync((void **)&dR, rb, c->pool, c->stream) != cudaSuccess) {
+        if (dK) cudaFreeAsync(dK, c->stream);
+        set_err("device allocation of %zu bytes for the element Jacobians failed", kb + rb);
+        return HP_ENOMEM;
+    }
+    c->L.elem_jac(c->d_tab, c->mesh, c->st, c->ph, dK, dR, c->nsm, c->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(K, dK, kb, cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(dK, c->stream);
+    cudaFreeAsync(dR, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        set_err("element Jacobians: %s", cudaGetErrorString(e));
+        return HP_ECUDA;
     }
     return HP_OK;
 }

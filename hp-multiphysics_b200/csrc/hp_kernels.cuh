@@ -122,6 +122,17 @@ struct ElemCfg {
 // entries of one column that a CTA reads together are contiguous), each tile padded to
 // a 16-byte multiple:
 //   index(t, j, m) = (t / EB) * TS + j * (EB * T) + (t % EB) * T + m,  TS >= T * EB * T.
+// Finite-difference element Jacobians (tri_hp::element_jacobian, nstage.cpp:131-165, fixed
+// mesh): pass 0 stores every element's stage-0 residual lf_re + lf_im in rbar [ntri][T][NV];
+// pass 1 runs one item per (element, column kcol = mode * NV + var) with that unknown raised
+// by dw(var) = 1e-8 sum_{i<3} |uht(var)(i)| + 1e-8 and writes
+// K[tind][krow = i * NV + n][kcol] = (lf_re(n)(i) + lf_im(n)(i) - rbar) / dw(var).
+template <typename R>
+struct ElemJac {
+    R *K, *rbar;
+    int pass;
+};
+
 template <typename R>
 struct ElemMat {
     R *aim, *are, *bre;
@@ -203,7 +214,7 @@ struct ElemMinBlocks {
 template <typename R, int P, int PHYS, bool CURVED>
 __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R, P, PHYS, CURVED>::value)
     k_rsdl_elem(const DevTables<R, P> *__restrict__ gtab, Mesh mesh, State<R> st, Phys ph, int stage, int zero_rr,
-                int diff, ElemMat<R> build) {
+                int diff, ElemMat<R> build, ElemJac<R> jac) {
     using C = ElemCfg<R, P, PHYS>;
     constexpr int G = C::G, X = C::X, T = C::T, IM = C::IM, BM = C::BM, NV = C::NV, GG = G * G;
     constexpr int SM = (C::SM > 0 ? C::SM : 1);  // side-mode stride (unused when p = 1)
@@ -232,13 +243,16 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
 
     // build mode (cd): one item per (element, column j) with uht = e_j, j = T: uht = 0
     const bool bmode = (PHYS == 0) && build.aim != nullptr;
+    const bool jmode = jac.rbar != nullptr, jcols = jmode && jac.pass == 1;
+    constexpr int NJ = NV * T;  // Jacobian columns per element
     const long nel = CURVED ? (long)mesh.ncurved : (long)mesh.ntri;
-    const long nitems = bmode ? nel * (T + 1) : nel;
+    const long nitems = bmode ? nel * (T + 1) : (jcols ? nel * NJ : nel);
     for (long wbase = ((long)blockIdx.x * C::WPC + warp) * EPW; wbase < nitems;
          wbase += (long)gridDim.x * C::WPC * EPW) {
         const long item = (wbase + grp < nitems) ? wbase + grp : wbase;
-        const int eidx = bmode ? (int)(item / (T + 1)) : (int)item;
+        const int eidx = bmode ? (int)(item / (T + 1)) : (jcols ? (int)(item / NJ) : (int)item);
         const int bcol = bmode ? (int)(item - (long)eidx * (T + 1)) : -1;
+        const int jcol = jcols ? (int)(item - (long)eidx * NJ) : 0;
         const int tind = CURVED ? mesh.crv_tri[eidx] : eidx;
         // curved elements are done by the curved launch
         const bool act = (wbase + grp < nitems) && (CURVED || !mesh.tri_cv || mesh.tri_cv[tind] < 0);
@@ -280,6 +294,14 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
                 }
                 uht[(NV + n) * T + m] = val;
             }
+        }
+        R jdw = (R)1;
+        if (jcols) {
+            __syncwarp();
+            const int jm = jcol / NV, jn = jcol - jm * NV;
+            jdw = (R)1e-8 * (fabs(uht[jn * T]) + fabs(uht[jn * T + 1]) + fabs(uht[jn * T + 2])) + (R)1e-8;
+            __syncwarp();
+            if (act && sl == 0) uht[jn * T + jm] += jdw;
         }
         // geometry (straight element): ldcrd(n,0) = (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2
         const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
@@ -467,6 +489,8 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
             const R val = mode_result(n, m);
             if (bmode) {
                 if (bcol < T) build.aim[EmatCfg<P>::idx(tind, bcol, m)] = val;
+            } else if (jmode) {
+                uht[n * T + m] = val;  // uht is dead after stage I: lf_im collects there
             } else if (m < BM) {
                 scatter(st.resv, st.ress, n, m, val);
             } else {
@@ -575,6 +599,8 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
                 if (bmode) {
                     if (bcol < T) build.are[EmatCfg<P>::idx(tind, bcol, m)] = val;
                     else build.bre[(size_t)tind * T + m] = val;
+                } else if (jmode) {
+                    uht[n * T + m] += val;
                 } else if (m < BM) {
                     scatter(st.rrv, st.rrs, n, m, val);
                 } else {
@@ -583,6 +609,15 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
                     st.rri[gi] = rr;
                     st.resi[gi] += rr;
                 }
+            }
+        }
+        if (jmode) {
+            __syncwarp();
+            for (int w = sl; act && w < NJ; w += LW) {
+                const int n = w / T, m = w - n * T;
+                const size_t rb = ((size_t)tind * T + m) * NV + n;
+                if (!jcols) jac.rbar[rb] = uht[n * T + m];
+                else jac.K[((size_t)tind * NJ + (m * NV + n)) * NJ + jcol] = (uht[n * T + m] - jac.rbar[rb]) / jdw;
             }
         }
         __syncwarp();

@@ -385,8 +385,13 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
             const long it = (e == 1 && has1) ? it0 + 1 : it0;
             te[e] = MODE == 2 ? (int)(it / NJ) : (int)it;
         }
-        // ---- gather both tetrahedra (a missing second one gets zeros)
-        for (int w = lane; w < 2 * NV * T; w += 32) {
+        // ---- gather both tetrahedra (a missing second one gets zeros); unrolled so that
+        //      the dependent index -> value loads of a lane's entries overlap
+        constexpr int NGATH = (2 * NV * T + 31) / 32;
+#pragma unroll
+        for (int k = 0; k < NGATH; ++k) {
+            const int w = lane + 32 * k;
+            if (w >= 2 * NV * T) break;
             const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
             double v = 0.0;
             if (e == 0 || has1) {

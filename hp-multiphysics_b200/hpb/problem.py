@@ -249,6 +249,16 @@ class GPULevel:
                            elem_ms=float(ms[2 * i]), minv_ms=float(ms[2 * i + 1]))
                 for i, prec in enumerate(("fp64", "fp32"))}
 
+    def element_jacobians(self):
+        """tri_hp::element_jacobian of every element (hp_gpu_element_jacobian):
+        K [ntri][tm*NV][tm*NV], row i*NV + n, column mode*NV + var."""
+        tm = (self.prob.p + 1) * (self.prob.p + 2) // 2
+        nj = tm * self.prob.NV
+        K = np.zeros((self.prob.mesh.ntri, nj, nj))
+        self.lib.hp_gpu_element_jacobian.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.check(self.lib.hp_gpu_element_jacobian(self.h, L.ptr(K)), "element_jacobian")
+        return K
+
     def element_matrices(self, on=True):
         """cd only: rsdl from stored element operators (hp_gpu_set_element_matrices)."""
         L.check(self.lib.hp_gpu_set_element_matrices(self.h, 1 if on else 0), "set_element_matrices")

@@ -209,6 +209,15 @@ int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *ctx, int stage);
  * until hp_gpu_destroy). HP_ENOTSUP for ins. */
 int hp_gpu_set_element_matrices(hp_gpu_ctx *ctx, int on);
 
+/* tri_hp::element_jacobian (tri_hp/nstage.cpp:131-165, fixed mesh) of every element,
+ * batched on the GPU: the finite-difference Jacobian of the stage-0 element residual
+ * lf_re + lf_im with respect to the element's coefficients, column (mode, var) from the
+ * residual with uht(var)(mode) raised by dw(var) = 1e-8 sum_{i<3} |uht(var)(i)| + 1e-8.
+ * K (host) [ntri][tm*NV][tm*NV], row i*NV + n, column mode*NV + var. Needs
+ * setup_preconditioner (tau). Device scratch of ntri*(tm*NV)^2 doubles is taken from
+ * the context's pool for the call. */
+int hp_gpu_element_jacobian(hp_gpu_ctx *ctx, double *K);
+
 /* Convergence driver. Runs smoothing until the unpreconditioned FP64 residual
  * norm ||R64(u)||_2 (all v/s/i modes of rsdl(nstage), without the rows of
  * essential boundary values, which the boundary condition replaces) has dropped by `drop` from

@@ -962,6 +962,43 @@ double or_maxres(or_ctx *c, double *out) {
 }
 
 // Basis-operator probes for pinning against the reference's tri_basis.
+// tri_hp::element_jacobian (nstage.cpp:131-165), fixed mesh: K [ntri][tm*NV][tm*NV], row
+// i*NV + n, column mode*NV + var = (lf_re + lf_im - Rbar) / dw(var) at stage 0, the column's
+// unknown raised by dw(var) = eps_r sum_{i<3} |uht(var)(i)| + eps_a (eps_r = eps_a = 1e-8,
+// tri_hp/hp_boundary.h:22) and lowered again afterwards, as the reference does.
+void or_element_jacobian(or_ctx *c, double *K) {
+    const int NV = c->NV, tm = c->tm, NJ = NV * tm;
+    const double eps_r = 1.0e-8, eps_a = 1.0e-8;
+    double lf_re[3][HP_MXTM], lf_im[3][HP_MXTM], rbar[3][HP_MXTM];
+    auto elem = [&](int tind) {
+        if (c->ph.physics == HP_PHYS_INS) element_rsdl_ins(c, tind, 0, lf_re, lf_im);
+        else element_rsdl_cd(c, tind, 0, lf_re, lf_im);
+    };
+    for (int tind = 0; tind < c->ntri; ++tind) {
+        ugtouht(c, tind);
+        double dw[3];
+        for (int n = 0; n < NV; ++n) {
+            dw[n] = 0.0;
+            for (int i = 0; i < 3; ++i) dw[n] += std::fabs(c->uht[n][i]);
+            dw[n] = dw[n] * eps_r + eps_a;
+        }
+        elem(tind);
+        for (int i = 0; i < tm; ++i)
+            for (int n = 0; n < NV; ++n) rbar[n][i] = lf_re[n][i] + lf_im[n][i];
+        int kcol = 0;
+        for (int mode = 0; mode < tm; ++mode)
+            for (int var = 0; var < NV; ++var, ++kcol) {
+                c->uht[var][mode] += dw[var];
+                elem(tind);
+                int krow = 0;
+                for (int i = 0; i < tm; ++i)
+                    for (int n = 0; n < NV; ++n, ++krow)
+                        K[((size_t)tind * NJ + krow) * NJ + kcol] = (lf_re[n][i] + lf_im[n][i] - rbar[n][i]) / dw[var];
+                c->uht[var][mode] -= dw[var];
+            }
+    }
+}
+
 void or_basis_proj(const hp_basis_tables *t, const double *lin, double *f, double *dx, double *dy, int st) { Basis(*t).proj(lin, f, dx, dy, st); }
 void or_basis_proj_val(const hp_basis_tables *t, const double *lin, double *f, int st) { Basis(*t).proj(lin, f, st); }
 void or_basis_derivr(const hp_basis_tables *t, const double *f, double *d, int st) { Basis(*t).derivr(f, d, st); }

@@ -51,6 +51,7 @@ def lib():
         o.or_basis_proj1d.argtypes = [P, P, P, P]
         o.or_basis_intgrt1d.argtypes = [P, P, P]
         o.or_dpbtrsnu2.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int]
+        o.or_element_jacobian.argtypes = [P, P]
         I = ctypes.c_int
         o.ot_create.restype = P
         o.ot_create.argtypes = [P, P, I, I, I, I, P, P, P, P, P, P, P]
@@ -171,6 +172,15 @@ class Oracle:
     def maxres(self):
         out = np.zeros(self.prob.NV)
         return self.o.or_maxres(self.h, _p(out)), out
+
+
+def element_jacobians(oracle):
+    """tri_hp::element_jacobian of every element of an Oracle (K [ntri][tm*NV][tm*NV])."""
+    pr = oracle.prob
+    nj = pr.NV * (pr.p + 1) * (pr.p + 2) // 2
+    K = np.zeros((pr.mesh.ntri, nj, nj))
+    lib().or_element_jacobian(oracle.h, _p(K))
+    return K
 
 
 class OracleTet:
