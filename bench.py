@@ -261,7 +261,7 @@ def tet_flops_per_element(p, beta_positive=True):
     return 2 * (proj + intg)
 
 
-def c5_sweep(torch, dev, n, p, steps, warmup, timed):
+def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False):
     """3D tet_hp ins: the unit cube split into n^3 hexahedra x 6 tetrahedra (n = 64:
     1,572,864 tetrahedra), p = 3, Re 100, the Ethier-Steinman Beltrami state at the
     vertices plus 1e-3 seeded noise on every coefficient. Times tet_hp::rsdl(nstage)
@@ -328,6 +328,12 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed):
                               "at p = 1", "seconds_incl_preconditioner_setup": sec, "cycles": nc,
                               "ms_per_cycle_incl_setup": 1e3 * sec / max(nc, 1), "drop": float(h[-1]),
                               "drop_history": [float(x) for x in h[::max(1, len(h) // 10)]]}
+    if full_solve:
+        # W-cycles (vwcycle 2) on the same hierarchy to the 1e-10 drop
+        h, sec, nc = H.solve(drop=1e-10, max_cycles=400, vw=2)
+        line["multigrid_full_w_to_1e-10"] = {"seconds": sec, "cycles": nc, "drop": float(h[-1]),
+                                             "reached": bool(h[-1] <= 1e-10), "ms_per_cycle": 1e3 * sec / max(nc, 1),
+                                             "drop_history": [float(x) for x in h[::max(1, len(h) // 10)]]}
     H.close()
     # CPU oracle on a bounded sample
     ps = TetProblem(cube_tets(6), p, mu=1.0 / 100.0).set_beltrami(re=100.0)
@@ -559,6 +565,8 @@ def main():
                          "c4: ins past a cylinder in a channel (curved hole, graded ~150k triangles), learned "
                          "preconditioner trained on Re in [20, 200], judged on held-out Re by the FP64 residual")
     ap.add_argument("--p", type=int, nargs="*", default=None, help="with --sweep: the p values")
+    ap.add_argument("--tet-solve", action="store_true",
+                    help="with --sweep c5: also W-cycles on the full hierarchy to a 1e-10 drop (minutes)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -609,7 +617,7 @@ def main():
     if args.sweep == "c5":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         c5_sweep(torch, dev, args.mesh if args.mesh != N_MESH else 64, (args.p or [3])[0], args.steps, args.warmup,
-                 timed_factory(torch, flush))
+                 timed_factory(torch, flush), full_solve=args.tet_solve)
         return
 
     if args.physics == "ins":
