@@ -279,7 +279,10 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False):
     pr = TetProblem(mesh, p, mu=1.0 / 100.0).set_beltrami(re=100.0)
     import ctypes
     cur = torch.cuda.current_stream()
+    masks, ff = pr.cube_boundary(re=100.0)
     g = TetGPU(pr, device=dev, stream=ctypes.c_void_p(cur.cuda_stream))  # events and kernels on one stream
+    g.set_dirichlet(masks)
+    g.set_flux_faces(ff)
     host_s = _t.perf_counter() - t0
     assert g.setup_preconditioner() == 0
     ns = pr.phys.nstage
@@ -295,6 +298,8 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False):
     fl = tet_flops_per_element(p) * mesh.ntet
     achieved = fl / (rsdl_ms * 1e-3) / 1e12
     line = {"sweep": "c5", "workload": f"tet ins p={p}, {n}^3 x 6 = {mesh.ntet} tetrahedra, Re 100 Beltrami + 1e-3 noise",
+            "boundary": "bdry_ins::inflow (velocity essential, continuity flux) on the six faces, boundary flux "
+                        f"balanced to zero; {len(ff['face_tri'])} flux faces",
             "ndof": pr.ndof, "ntet": mesh.ntet, "host_setup_seconds": host_s, "steps": steps, "warmup": warmup,
             "rsdl_ms": rsdl_ms, "rsdl_gdofs": pr.ndof / rsdl_ms / 1e6, "rsdl_beta0_ms": sum(ms0) / len(ms0),
             "operator_flops_per_tet": tet_flops_per_element(p), "l2_flushed": True,
@@ -303,15 +308,17 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False):
                          "peak_source": "hp_tet_fp64_mma_peak: mma.m8n8k4.f64 chains on every SM, measured in this run"}}
     g.close()
     # smoothing legs: the JACOBI build's update (finite-difference Jacobian diagonal,
-    # omega 0.5) with the velocity fixed on the six faces; cfl 0.5 on every level (the
+    # omega 0.5) with the same boundary layout; cfl 0.5 on every level (the
     # reference's tet defaults 2.2 / 1.5 / 1.0 for p = 1 / 2 / 3 diverge with this smoother
     # at p >= 2)
     from hpb.tet import TetHierarchy
     cfl = {1: 0.5, 2: 0.5, 3: 0.5, 4: 0.5}
     small = 8
     ps = TetProblem(cube_tets(small), p, mu=1.0 / 100.0, cfl=cfl[p]).set_beltrami(re=100.0)
+    masks, ff = ps.cube_boundary(re=100.0)
     gs = TetGPU(ps, device=dev, stream=ctypes.c_void_p(cur.cuda_stream))
-    gs.set_dirichlet(ps.dirichlet_masks())
+    gs.set_dirichlet(masks)
+    gs.set_flux_faces(ff)
     h, sec, nu = gs.solve(drop=1e-10, max_updates=20000, check_every=100)
     line["solve_single_grid_small"] = {"mesh": f"{small}^3 x 6", "ndof": ps.ndof, "seconds": sec, "updates": nu,
                                        "drop": float(h[-1]), "reached": bool(h[-1] <= 1e-10)}
@@ -342,7 +349,9 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False):
     H.close()
     # CPU oracle on a bounded sample
     ps = TetProblem(cube_tets(6), p, mu=1.0 / 100.0).set_beltrami(re=100.0)
+    ff = ps.cube_boundary(re=100.0)[1]
     o = OracleTet(ps)
+    o.set_flux_faces(ff)
     o.setup_preconditioner()
     reps, t2 = 0, _t.perf_counter()
     while _t.perf_counter() - t2 < 10.0:

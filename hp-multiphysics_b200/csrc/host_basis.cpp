@@ -848,6 +848,40 @@ extern "C" int hp_tet_basis_build(int p, hp_tet_tables *out) {
                     t.DZ[q][m] = s * (gx * gy * dgz + t.y1[j] * gx * dgy * gz * t.z0[k]) + t.x0[i] * dx;
                 }
             }
+    // face basis (proj2d / intgrt2d): mode k = sgn gx(x_i, fx) gy(y_j, fy)
+    {
+        const int T2 = 3 + 3 * em + fm;
+        t.T2 = T2;
+        std::vector<int> fx(T2), fy(T2), dyg(T2, 1);  // dyg 0: proj2d's y derivative uses gy
+        std::vector<double> fs(T2, 1.0);
+        fx[0] = 0; fy[0] = 1;
+        fx[1] = 1; fy[1] = 2;
+        fx[2] = 2; fy[2] = 2;
+        const int be2 = em + 3, be3 = 2 * em + 3, bint = 3 + 3 * em;
+        for (int p2 = 3; p2 < em + 3; ++p2) { fx[p2] = p2; fy[p2] = p2; dyg[p2] = 0; }
+        for (int i = 0; i < em; ++i) {
+            fx[be2 + i] = 2; fy[be2 + i] = 3 + em + i;
+            fx[be3 + i] = 1; fy[be3 + i] = 3 + em + i; fs[be3 + i] = (i & 1) ? -1.0 : 1.0;
+        }
+        int ind2 = 0;
+        for (int p2 = 3; p2 < em + 3; ++p2)
+            for (int i = 1; i <= em - p2 + 2; ++i, ++ind2) {
+                fx[bint + ind2] = p2; fy[bint + ind2] = 3 + 2 * em + ind2; dyg[bint + ind2] = 0;
+            }
+        for (int i = 0; i < G; ++i)
+            for (int j = 0; j < G; ++j) {
+                const int q = i * G + j;
+                t.W2[q] = t.wtx[i] * t.wty[j];
+                for (int k = 0; k < T2; ++k) {
+                    const double gx = t.gx[i][fx[k]], dgx = t.dgx[i][fx[k]];
+                    const double gy = t.gy[j][fy[k]], dgy = t.dgy[j][fy[k]];
+                    const double dx = fs[k] * dgx * gy * t.y0[j];
+                    t.F2[q][k] = fs[k] * gx * gy;
+                    t.DX2[q][k] = dx;
+                    t.DY2[q][k] = fs[k] * gx * (dyg[k] ? dgy : gy) + t.x0[i] * dx;
+                }
+            }
+    }
     deriv_operator(G, t.dltx, t.dltx2, t.Ax);
     deriv_operator(G, t.dltx, t.dltx3, t.Bx);
     deriv_operator(G, t.dlty, t.dlty2, t.Ay);

@@ -2,7 +2,7 @@
 // the diagonal element terms) and tet_hp::rsdl with tet_hp_ins::element_rsdl for
 // straight tetrahedra.
 //
-// Reference path (tet_hp/update.cpp:9-118, tet_hp/ins/rsdl.cpp:442-781,
+// Reference path (tet_hp/update.cpp:9-118, tet_hp/ins/rsdl.cpp:442-781, tet_hp/ins/bdry.cpp:16-102,
 // tet_hp/ins/setup_preconditioner.cpp, tet_hp/gtol.cpp:16-82 and 815-873). The
 // basis operators are the dense per-point forms of tet_basis::proj / intgrtrst and
 // the 1D operators of derivr / derivs / derivt (include/hp_tet.h), pinned against
@@ -10,10 +10,11 @@
 //
 // Layout in HBM: one buffer per field (state, res, res_r) holding the vertex, edge,
 // face and interior sections back to back, each [entity][mode][4 variables]; the
-// dense operators (G^3 x T each) are read through the read-only path and stay in
-// L1 / L2. One warp per tetrahedron: lanes own quadrature points for the
-// projection and the pointwise fluxes and (variable, mode) pairs for the
-// integrations; the per-point arrays live in the warp's shared-memory slice.
+// dense operators (G^3 x T each) are stored in DMMA fragment order, read through the
+// read-only path and stay in L1 / L2. One warp per pair of tetrahedra: the
+// projections and integrations run on the FP64 tensor cores, lanes own (tetrahedron,
+// point) pairs for the pointwise fluxes, and the per-point arrays live in the warp's
+// shared-memory slice. Boundary faces with a flux take one warp each.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -55,21 +56,12 @@ struct TetCfg {
     static constexpr int G = P + 1, Q = G * G * G, T = (P + 1) * (P + 2) * (P + 3) / 6;
     static constexpr int EM = P - 1, FM = (P - 1) * (P - 2) / 2, IM = T - 4 - 6 * EM - 4 * FM;
     static constexpr int BM = 4 + 6 * EM + 4 * FM;
-    static constexpr int WPC = 4;                 // warps (tetrahedra in flight) per CTA
-    static constexpr int QL = (Q + 31) / 32;      // quadrature points per lane
-    // per-warp scratch: uht [NV][T]; u [NV][Q]; cvi [3][3][Q]; c3 [3][Q]; df [3][3][Q]
-    static constexpr int S_WARP = NV * T + 25 * Q;
 };
 
 template <typename R, int P>
 struct TetSmall {  // by-value kernel parameter: the 1D derivative operators and factors
     R Ax[P + 1][P + 1], Bx[P + 1][P + 1], Ay[P + 1][P + 1], By[P + 1][P + 1], Az[P + 1][P + 1];
     R y0[P + 1], z0[P + 1];
-};
-
-template <typename R>
-struct TetOps {  // dense operators in device memory, row-major [q][m]; WD* = w * D*
-    const R *F, *DX, *DY, *DZ, *WDX, *WDY, *WDZ;
 };
 
 struct TetMeshD {
@@ -110,208 +102,9 @@ __device__ __forceinline__ R *mode_slot(const TetMeshD &m, const TetFields<R> &g
     return g.i + ((size_t)tind * IM + (mode - C::BM)) * NV + n;
 }
 
-__device__ __forceinline__ void atomic_add_r(double *a, double v) { atomicAdd(a, v); }
-__device__ __forceinline__ void atomic_add_r(float *a, float v) { atomicAdd(a, v); }
 
-// tet_hp::rsdl element loop: res (imaginary terms) and res_r (beta-scaled real terms)
-template <typename R, int P>
-__global__ void __launch_bounds__(TetCfg<P>::WPC * 32)
-    k_tet_rsdl(TetOps<R> ops, TetSmall<R, P> sm, TetMeshD mesh, TetFields<R> ug, TetFields<R> res,
-               TetFields<R> rr, const R *__restrict__ tau, R rho, R mu, R beta) {
-    using C = TetCfg<P>;
-    constexpr int G = C::G, Q = C::Q, T = C::T;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    R *uht = reinterpret_cast<R *>(smem_raw) + warp * C::S_WARP;
-    R *u = uht + NV * T;   // [NV][Q]
-    R *cvi = u + NV * Q;   // [3][3][Q] convective + pressure fluxes
-    R *c3 = cvi + 9 * Q;   // [3][Q] continuity flux, then its SUPG term
-    R *df = c3 + 3 * Q;    // [3][3][Q] viscous flux, then viscous + SUPG
-    for (long tind = (long)blockIdx.x * C::WPC + warp; tind < mesh.ntet; tind += (long)gridDim.x * C::WPC) {
-        const int t = (int)tind;
-        for (int w = lane; w < NV * T; w += 32) {
-            const int n = w / T, m = w - n * T;
-            R s;
-            const R *src = mode_slot<R, P>(mesh, ug, t, m, n, s);
-            uht[n * T + m] = s * *src;
-        }
-        // straight element: ldcrd(n, .) = (v3 - v2, v1 - v2, v0 - v2) / 2
-        R ld[3][3];
-        {
-            const int v0 = mesh.tp[4 * t], v1 = mesh.tp[4 * t + 1], v2 = mesh.tp[4 * t + 2], v3 = mesh.tp[4 * t + 3];
-            for (int n = 0; n < 3; ++n) {
-                const double c2 = mesh.pnts[3 * v2 + n];
-                ld[n][0] = (R)(0.5 * (mesh.pnts[3 * v3 + n] - c2));
-                ld[n][1] = (R)(0.5 * (mesh.pnts[3 * v1 + n] - c2));
-                ld[n][2] = (R)(0.5 * (mesh.pnts[3 * v0 + n] - c2));
-            }
-        }
-        R d[3][3];
-        d[0][0] = ld[1][1] * ld[2][2] - ld[1][2] * ld[2][1];
-        d[0][1] = -ld[0][1] * ld[2][2] + ld[0][2] * ld[2][1];
-        d[0][2] = ld[0][1] * ld[1][2] - ld[0][2] * ld[1][1];
-        d[1][0] = -ld[1][0] * ld[2][2] + ld[1][2] * ld[2][0];
-        d[1][1] = ld[0][0] * ld[2][2] - ld[0][2] * ld[2][0];
-        d[1][2] = -ld[0][0] * ld[1][2] + ld[0][2] * ld[1][0];
-        d[2][0] = ld[1][0] * ld[2][1] - ld[1][1] * ld[2][0];
-        d[2][1] = -ld[0][0] * ld[2][1] + ld[0][1] * ld[2][0];
-        d[2][2] = ld[0][0] * ld[1][1] - ld[0][1] * ld[1][0];
-        const R cjcb = ld[0][0] * (ld[1][1] * ld[2][2] - ld[1][2] * ld[2][1]) -
-                       ld[0][1] * (ld[1][0] * ld[2][2] - ld[2][0] * ld[1][2]) +
-                       ld[0][2] * (ld[1][0] * ld[2][1] - ld[2][0] * ld[1][1]);
-        __syncwarp();
-        // ---- projection and pointwise fluxes (lanes own points)
-        for (int k = 0; k < C::QL; ++k) {
-            const int q = lane + 32 * k;
-            if (q >= Q) break;
-            R uu[NV] = {0, 0, 0, 0}, du[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-            const R *fq = ops.F + (size_t)q * T, *xq = ops.DX + (size_t)q * T, *yq = ops.DY + (size_t)q * T,
-                    *zq = ops.DZ + (size_t)q * T;
-#pragma unroll 4
-            for (int m = 0; m < T; ++m) {
-                const R f = __ldg(fq + m);
-                const R a = __ldg(xq + m), b = __ldg(yq + m), c = __ldg(zq + m);
-#pragma unroll
-                for (int n = 0; n < NV; ++n) uu[n] += f * uht[n * T + m];
-#pragma unroll
-                for (int n = 0; n < 3; ++n) {
-                    const R x = uht[n * T + m];
-                    du[n][0] += a * x;
-                    du[n][1] += b * x;
-                    du[n][2] += c * x;
-                }
-            }
-#pragma unroll
-            for (int n = 0; n < NV; ++n) u[n * Q + q] = uu[n];
-            const R fx = rho * uu[0], fy = rho * uu[1], fz = rho * uu[2];
-            R f3[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                f3[c] = d[c][0] * fx + d[c][1] * fy + d[c][2] * fz;
-                c3[c * Q + q] = f3[c];
-            }
-#pragma unroll
-            for (int n = 0; n < 3; ++n)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) cvi[(n * 3 + c) * Q + q] = uu[n] * f3[c] + d[c][n] * uu[3];
-            if (beta > (R)0) {
-                // df(a,c) = sum_{b,e} visc(a,b)(c,e) du(b,e)  (rsdl.cpp:521-612, 632-670), with
-                // visc(a,a)(c,e) = -mu/J (sum_f d(c)(f) d(e)(f) + d(c)(a) d(e)(a)) and
-                // visc(a,b)(c,e) = -mu/J d(c)(b) d(e)(a) for b != a
-                const R cjcbi = mu / cjcb;
-                R h[3][3];  // h(b,a) = sum_e d(e)(a) du(b,e)
-#pragma unroll
-                for (int b = 0; b < 3; ++b)
-#pragma unroll
-                    for (int a = 0; a < 3; ++a) h[b][a] = d[0][a] * du[b][0] + d[1][a] * du[b][1] + d[2][a] * du[b][2];
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        R s = (R)0;
-#pragma unroll
-                        for (int e = 0; e < 3; ++e) {
-                            const R gce = d[c][0] * d[e][0] + d[c][1] * d[e][1] + d[c][2] * d[e][2];
-                            s += gce * du[a][e];
-                        }
-                        s += d[c][0] * h[0][a] + d[c][1] * h[1][a] + d[c][2] * h[2][a];
-                        df[(a * 3 + c) * Q + q] = -cjcbi * s;
-                    }
-            }
-        }
-        __syncwarp();
-        // ---- imaginary terms: intgrtrst of (cvi, c3), scattered into res
-        for (int w = lane; w < NV * T; w += 32) {
-            const int n = w / T, m = w - n * T;
-            const R *fr = n < 3 ? cvi + (n * 3) * Q : c3;
-            R s = (R)0;
-            for (int q = 0; q < Q; ++q)
-                s += __ldg(ops.WDX + (size_t)q * T + m) * fr[q] + __ldg(ops.WDY + (size_t)q * T + m) * fr[Q + q] +
-                     __ldg(ops.WDZ + (size_t)q * T + m) * fr[2 * Q + q];
-            R sg;
-            R *dst = mode_slot<R, P>(mesh, res, t, m, n, sg);
-            if (m < C::BM) atomic_add_r(dst, -sg * s);
-            else *dst = -s;  // interiors: one writer, res cleared before
-        }
-        if (beta > (R)0) {
-            // ---- strong residual at the owned points: derivatives of the total fluxes
-            R rsd[C::QL][NV];
-            for (int k = 0; k < C::QL; ++k) {
-                const int q = lane + 32 * k;
-                if (q >= Q) break;
-                const int i = q / (G * G), j = (q / G) % G, kk = q % G;
-                const R yz = sm.y0[j] * sm.z0[kk], zz = sm.z0[kk];
-                for (int n = 0; n < NV; ++n) {
-                    // flux component c of variable n at point (i2, j2, k2)
-                    auto fl = [&](int c, int i2, int j2, int k2) -> R {
-                        const int q2 = (i2 * G + j2) * G + k2;
-                        return n < 3 ? cvi[(n * 3 + c) * Q + q2] + df[(n * 3 + c) * Q + q2] : c3[c * Q + q2];
-                    };
-                    R ax = 0, bxs = 0, bxt = 0, ays = 0, byt = 0, azt = 0;
-#pragma unroll
-                    for (int l = 0; l < G; ++l) {
-                        ax += sm.Ax[i][l] * fl(0, l, j, kk);
-                        bxs += sm.Bx[i][l] * fl(1, l, j, kk);
-                        bxt += sm.Bx[i][l] * fl(2, l, j, kk);
-                        ays += sm.Ay[j][l] * fl(1, i, l, kk);
-                        byt += sm.By[j][l] * fl(2, i, l, kk);
-                        azt += sm.Az[kk][l] * fl(2, i, j, l);
-                    }
-                    rsd[k][n] = yz * ax + (yz * bxs + zz * ays) + (yz * bxt + zz * byt + azt);
-                }
-            }
-            __syncwarp();
-            // ---- SUPG terms (rsdl.cpp:693-766), mesh velocity zero
-            const R tau0 = tau[2 * t], tau3 = tau[2 * t + 1];
-            for (int k = 0; k < C::QL; ++k) {
-                const int q = lane + 32 * k;
-                if (q >= Q) break;
-                R tr[NV], uq[3];
-#pragma unroll
-                for (int n = 0; n < 3; ++n) {
-                    tr[n] = tau0 * rsd[k][n];
-                    uq[n] = u[n * Q + q];
-                }
-                tr[3] = tau3 * rsd[k][3];
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        R s = d[c][a] * ((R)2 * uq[a]);
-#pragma unroll
-                        for (int b = 0; b < 3; ++b)
-                            if (b != a) s += d[c][b] * uq[b];
-                        R r = s * tr[a];
-#pragma unroll
-                        for (int b = 0; b < 3; ++b)
-                            if (b != a) r += d[c][b] * uq[a] * tr[b];
-                        r += d[c][a] * tr[3];
-                        df[(a * 3 + c) * Q + q] -= r;
-                    }
-#pragma unroll
-                for (int c = 0; c < 3; ++c) c3[c * Q + q] = -d[c][0] * tr[0] - d[c][1] * tr[1] - d[c][2] * tr[2];
-            }
-            __syncwarp();
-            // ---- real terms: beta * intgrtrst of (df, c3), scattered into res_r
-            for (int w = lane; w < NV * T; w += 32) {
-                const int n = w / T, m = w - n * T;
-                const R *fr = n < 3 ? df + (n * 3) * Q : c3;
-                R s = (R)0;
-                for (int q = 0; q < Q; ++q)
-                    s += __ldg(ops.WDX + (size_t)q * T + m) * fr[q] + __ldg(ops.WDY + (size_t)q * T + m) * fr[Q + q] +
-                         __ldg(ops.WDZ + (size_t)q * T + m) * fr[2 * Q + q];
-                R sg;
-                R *dst = mode_slot<R, P>(mesh, rr, t, m, n, sg);
-                if (m < C::BM) atomic_add_r(dst, -beta * sg * s);
-                else *dst += -beta * s;
-            }
-        }
-        __syncwarp();
-    }
-}
-
-// FP64 tensor-core (DMMA, mma.m8n8k4.f64) form of k_tet_rsdl: one warp takes two
-// tetrahedra, so the 8 rows of an A fragment are (tetrahedron, variable) pairs.
+// tet_hp::rsdl element loop (res: imaginary terms, res_r: beta-scaled real terms) on the
+// FP64 tensor cores (DMMA, mma.m8n8k4.f64): one warp takes two tetrahedra, so the 8 rows of an A fragment are (tetrahedron, variable) pairs.
 //   projection:  C[8 x Q] = U[8 x T] * Op^T[T x Q]   for Op = F, DX, DY, DZ
 //   intgrtrst:   C[8 x T] = Flux[8 x 3Q] * WD[3Q x T] (WD = w * (DX; DY; DZ))
 // The B operands are constant: the host stores them in fragment order (one 8-byte
@@ -681,6 +474,91 @@ __global__ void k_tet_pre(long n, R *res, R *rr, R omb) {
     }
 }
 
+struct TetFacesD {  // boundary faces with a flux
+    int n;
+    const int *tri, *pnt, *seg, *sgn, *kind;  // [n], [n][3], [n][3], [n][3], [n]
+    const double *pbc;                        // [n][G * G]
+};
+
+// hp_face_bdry::rsdl of bdry_ins::neumann / inflow (tet_hp/ins/bdry.cpp:16-102, fluxes
+// tet_hp/ins/bdry_ins.h:85-132), straight faces: one warp per face. Lane k < T2 gathers face
+// mode k (ugtouht2d, tet_hp/gtol.cpp:257-299); lane q < G*G evaluates u, the normal
+// d(x)/dr x d(x)/ds and the flux at face point q; lane k integrates (intgrt2d) and adds into
+// res. ftab = F2, DX2, DY2 [G*G][T2], W2 [G*G].
+template <int P>
+__global__ void __launch_bounds__(128) k_tet_face_flux(TetFacesD fc, const double *__restrict__ ftab, TetMeshD mesh,
+                                                       TetFields<double> u, TetFields<double> res, double rho) {
+    constexpr int G = P + 1, G2 = G * G, EM = P - 1, FM = (P - 1) * (P - 2) / 2, T2 = 3 + 3 * EM + FM;
+    constexpr int EMD = EM > 0 ? EM : 1, FMD = FM > 0 ? FM : 1, WPB = 4;
+    static_assert(G2 <= 32 && T2 <= 32, "one lane per face point and per face mode");
+    __shared__ double sflx[WPB][NV][G2];
+    const double *F2 = ftab, *DX2 = ftab + G2 * T2, *DY2 = ftab + 2 * G2 * T2, *W2 = ftab + 3 * G2 * T2;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (int b = blockIdx.x * WPB + wib; b < fc.n; b += gridDim.x * WPB) {  // warp-uniform
+        const int find = fc.tri[b], kind = fc.kind[b];
+        int pv[3], ps[3], sg[3];
+        for (int i = 0; i < 3; ++i) {
+            pv[i] = fc.pnt[3 * b + i];
+            ps[i] = fc.seg[3 * b + i];
+            sg[i] = fc.sgn[3 * b + i];
+        }
+        double lin[3] = {0.0, 0.0, 0.0};
+        if (lane < 3) {
+            for (int n = 0; n < 3; ++n) lin[n] = u.v[(size_t)pv[lane] * NV + n];
+        } else if (lane < 3 + 3 * EM) {
+            const int i = (lane - 3) / EMD, m = (lane - 3) - i * EMD;
+            const double s = ((m & 1) && sg[i] < 0) ? -1.0 : 1.0;
+            for (int n = 0; n < 3; ++n) lin[n] = s * u.e[((size_t)ps[i] * EMD + m) * NV + n];
+        } else if (lane < T2) {
+            const int k = lane - 3 - 3 * EM;
+            for (int n = 0; n < 3; ++n) lin[n] = u.f[((size_t)find * FMD + k) * NV + n];
+        }
+        double uq[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < T2; ++k) {
+            const double f = lane < G2 ? __ldg(F2 + lane * T2 + k) : 0.0;
+            for (int n = 0; n < 3; ++n) uq[n] += f * __shfl_sync(0xffffffffu, lin[n], k);
+        }
+        if (lane < G2) {
+            double dr[3] = {0.0, 0.0, 0.0}, ds[3] = {0.0, 0.0, 0.0};
+            for (int v = 0; v < 3; ++v) {
+                const double a = __ldg(DX2 + lane * T2 + v), c = __ldg(DY2 + lane * T2 + v);
+                for (int d = 0; d < 3; ++d) {
+                    const double x = mesh.pnts[3 * (size_t)pv[v] + d];
+                    dr[d] += a * x;
+                    ds[d] += c * x;
+                }
+            }
+            const double nrm[3] = {dr[1] * ds[2] - dr[2] * ds[1], dr[2] * ds[0] - dr[0] * ds[2],
+                                   dr[0] * ds[1] - dr[1] * ds[0]};
+            const double mf = rho * (uq[0] * nrm[0] + uq[1] * nrm[1] + uq[2] * nrm[2]);
+            const double pb = kind ? fc.pbc[(size_t)b * G2 + lane] : 0.0;
+            for (int n = 0; n < 3; ++n) sflx[wib][n][lane] = kind ? mf * uq[n] + pb * nrm[n] : 0.0;
+            sflx[wib][3][lane] = mf;
+        }
+        __syncwarp();
+        if (lane < T2) {
+            double r[NV] = {0.0, 0.0, 0.0, 0.0};
+            for (int q = 0; q < G2; ++q) {
+                const double wf = __ldg(W2 + q) * __ldg(F2 + q * T2 + lane);
+                for (int n = 0; n < NV; ++n) r[n] += wf * sflx[wib][n][q];
+            }
+            const int n0 = kind ? 0 : 3;  // inflow: the momentum fluxes are zero
+            if (lane < 3) {
+                for (int n = n0; n < NV; ++n) atomicAdd(res.v + (size_t)pv[lane] * NV + n, r[n]);
+            } else if (lane < 3 + 3 * EM) {
+                const int i = (lane - 3) / EMD, m = (lane - 3) - i * EMD;
+                const double s = ((m & 1) && sg[i] < 0) ? -1.0 : 1.0;
+                for (int n = n0; n < NV; ++n) atomicAdd(res.e + ((size_t)ps[i] * EMD + m) * NV + n, s * r[n]);
+            } else {
+                const int k = lane - 3 - 3 * EM;
+                for (int n = n0; n < NV; ++n) atomicAdd(res.f + ((size_t)find * FMD + k) * NV + n, r[n]);
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // res += res_r
 template <typename R>
 __global__ void k_tet_fold(long n, R *res, const R *rr) {
@@ -835,7 +713,6 @@ struct hp_tet_ctx {
     double *U = nullptr, *RES = nullptr, *RR = nullptr;  // [v | e | f | i]
     double *tau = nullptr, *iprcn = nullptr, *vprcn = nullptr, *eprcn = nullptr, *fprcn = nullptr;
     int *d_err = nullptr;
-    double *ops = nullptr;  // F, DX, DY, DZ, WDX, WDY, WDZ  [Q*T] each
     double *projB = nullptr, *intB = nullptr;  // the same operators in DMMA fragment order
     double *U0 = nullptr, *JD = nullptr, *rbar = nullptr, *part = nullptr;  // update, jacob_diag
     unsigned char *mask = nullptr;  // 1: row fixed by an essential condition
@@ -851,6 +728,10 @@ struct hp_tet_ctx {
     double *RES0 = nullptr, *DRES = nullptr, *UF = nullptr;
     hp_tet_tables tab{};
     bool prcn_ready = false;
+    double *ftab = nullptr;  // face operators F2, DX2, DY2, W2
+    TetFacesD faces{};       // boundary faces with a flux (device arrays below)
+    int *face_int = nullptr;
+    double *face_pbc = nullptr;
     TetFields<double> fields(double *base) const {
         return TetFields<double>{base, base + lv, base + lv + le, base + lv + le + lf};
     }
@@ -912,14 +793,6 @@ int ensure_attrs() {
 
 template <int P>
 int launch_rsdl(hp_tet_ctx *c, int stage) {
-    using C = TetCfg<P>;
-    static_assert(C::S_WARP * C::WPC * 8 <= 227 * 1024, "scratch exceeds shared memory");
-    const size_t smem = (size_t)C::S_WARP * C::WPC * sizeof(double);
-    static bool attr_set = false;
-    if (!attr_set) {
-        TCK(cudaFuncSetAttribute(k_tet_rsdl<double, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
     TetSmall<double, P> sm;
     const hp_tet_tables &t = c->tab;
     for (int i = 0; i <= P; ++i) {
@@ -933,17 +806,16 @@ int launch_rsdl(hp_tet_ctx *c, int stage) {
         sm.y0[i] = t.y0[i];
         sm.z0[i] = t.z0[i];
     }
-    const size_t qt = (size_t)C::Q * C::T;
-    TetOps<double> ops{c->ops, c->ops + qt, c->ops + 2 * qt, c->ops + 3 * qt, c->ops + 4 * qt, c->ops + 5 * qt,
-                       c->ops + 6 * qt};
     const double omb = stage >= c->ph.nstage ? 0.0 : 1.0 - c->ph.beta[stage];
     const double beta = c->ph.beta[stage];
     k_tet_pre<double><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>((long)c->ltot, c->RES,
                                                                                            c->RR, omb);
+    if (c->faces.n > 0)
+        k_tet_face_flux<P><<<std::min(nblk(c->faces.n, 4), c->nsm * 16), 128, 0, c->stream>>>(
+            c->faces, c->ftab, c->mesh, c->fields(c->U), c->fields(c->RES), c->ph.rho);
     using M = TetMma<P>;
     const size_t smem2 = (size_t)M::S_WARP * M::WPC * sizeof(double);
     if (int r = ensure_attrs<P>()) return r;
-    (void)ops;
     const long npair = ((long)c->mesh.ntet + 1) / 2;
     int blocks = std::min(nblk(npair, M::WPC), c->nsm * 32);
     k_tet_rsdl_mma<P, 0><<<blocks, M::WPC * 32, smem2, c->stream>>>(
@@ -1057,21 +929,19 @@ extern "C" int hp_tet_create(const hp_tet_mesh_desc *m, const hp_tet_tables *b, 
         return r;
     }
     TCK(cudaMemset(c->tau, 0, 16 * (size_t)m->ntet));
-    // dense operators; WD* = w(q) * D*(q, m)
-    const int Q = c->Q, T = c->T;
-    std::vector<double> h((size_t)7 * Q * T);
-    for (int q = 0; q < Q; ++q)
-        for (int mm = 0; mm < T; ++mm) {
-            const size_t k = (size_t)q * T + mm, qt = (size_t)Q * T;
-            h[k] = b->F[q][mm];
-            h[qt + k] = b->DX[q][mm];
-            h[2 * qt + k] = b->DY[q][mm];
-            h[3 * qt + k] = b->DZ[q][mm];
-            h[4 * qt + k] = b->w[q] * b->DX[q][mm];
-            h[5 * qt + k] = b->w[q] * b->DY[q][mm];
-            h[6 * qt + k] = b->w[q] * b->DZ[q][mm];
+    {
+        const int G2 = b->G * b->G, T2 = b->T2;
+        std::vector<double> ft((size_t)3 * G2 * T2 + G2);
+        for (int q = 0; q < G2; ++q) {
+            for (int k = 0; k < T2; ++k) {
+                ft[(size_t)q * T2 + k] = b->F2[q][k];
+                ft[(size_t)(G2 + q) * T2 + k] = b->DX2[q][k];
+                ft[(size_t)(2 * G2 + q) * T2 + k] = b->DY2[q][k];
+            }
+            ft[(size_t)3 * G2 * T2 + q] = b->W2[q];
         }
-    if ((r = up(h.data(), 8 * h.size(), (void **)&c->ops))) { hp_tet_destroy(c); return r; }
+        if ((r = up(ft.data(), 8 * ft.size(), (void **)&c->ftab))) { hp_tet_destroy(c); return r; }
+    }
     {
         std::vector<double> pb, ib;
         switch (c->p) {
@@ -1096,10 +966,62 @@ extern "C" int hp_tet_create(const hp_tet_mesh_desc *m, const hp_tet_tables *b, 
     return HP_OK;
 }
 
+extern "C" int hp_tet_set_flux_faces(hp_tet_ctx *c, int nface, const int *face_tri, const int *face_pnt,
+                                     const int *face_seg, const int *face_sgn, const int *kind, const double *pbc) {
+    if (!c || nface < 0 || (nface > 0 && (!face_tri || !face_pnt || !face_seg || !face_sgn || !kind))) {
+        set_err("hp_tet_set_flux_faces: bad arguments");
+        return HP_EINVAL;
+    }
+    const TetMeshD &m = c->mesh;
+    bool any_neumann = false;
+    for (int b = 0; b < nface; ++b) {
+        bool ok = face_tri[b] >= 0 && face_tri[b] < m.ntri && (kind[b] == 0 || kind[b] == 1);
+        for (int i = 0; i < 3; ++i)
+            ok = ok && face_pnt[3 * b + i] >= 0 && face_pnt[3 * b + i] < m.npnt && face_seg[3 * b + i] >= 0 &&
+                 face_seg[3 * b + i] < m.nseg && (face_sgn[3 * b + i] == 1 || face_sgn[3 * b + i] == -1);
+        if (!ok) {
+            set_err("hp_tet_set_flux_faces: face %d has an index out of range or a bad sign / kind", b);
+            return HP_EINVAL;
+        }
+        any_neumann = any_neumann || kind[b] == 1;
+    }
+    if (any_neumann && !pbc) {
+        set_err("hp_tet_set_flux_faces: neumann faces need pbc");
+        return HP_EINVAL;
+    }
+    TCK(cudaSetDevice(c->device));
+    TCK(cudaStreamSynchronize(c->stream));
+    if (c->face_int) cudaFree(c->face_int);
+    if (c->face_pbc) cudaFree(c->face_pbc);
+    c->face_int = nullptr;
+    c->face_pbc = nullptr;
+    c->faces = TetFacesD{};
+    if (nface == 0) return HP_OK;
+    const size_t G2 = (size_t)c->tab.G * c->tab.G;
+    std::vector<int> h((size_t)11 * nface);
+    std::copy(face_tri, face_tri + nface, h.begin());
+    std::copy(face_pnt, face_pnt + 3 * (size_t)nface, h.begin() + nface);
+    std::copy(face_seg, face_seg + 3 * (size_t)nface, h.begin() + 4 * (size_t)nface);
+    std::copy(face_sgn, face_sgn + 3 * (size_t)nface, h.begin() + 7 * (size_t)nface);
+    std::copy(kind, kind + nface, h.begin() + 10 * (size_t)nface);
+    std::vector<double> hp(G2 * nface, 0.0);
+    if (pbc) std::copy(pbc, pbc + G2 * nface, hp.begin());
+    TCK(cudaMalloc((void **)&c->face_int, 4 * h.size()));
+    TCK(cudaMalloc((void **)&c->face_pbc, 8 * hp.size()));
+    TCK(cudaMemcpy(c->face_int, h.data(), 4 * h.size(), cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(c->face_pbc, hp.data(), 8 * hp.size(), cudaMemcpyHostToDevice));
+    const int *d = c->face_int;
+    c->faces = TetFacesD{nface, d, d + nface, d + 4 * (size_t)nface, d + 7 * (size_t)nface, d + 10 * (size_t)nface,
+                         c->face_pbc};
+    return HP_OK;
+}
+
 extern "C" int hp_tet_destroy(hp_tet_ctx *c) {
     if (!c) return HP_EINVAL;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->face_int) cudaFree(c->face_int);
+    if (c->face_pbc) cudaFree(c->face_pbc);
     for (void *p : c->allocs) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;

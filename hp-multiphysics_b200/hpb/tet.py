@@ -18,7 +18,9 @@ class TetTables(ctypes.Structure):
                 [(n, _D * MAXG * MAXG) for n in ("dltx2", "dltx3", "dlty2", "dlty3", "dltz2")] +
                 [(n, _I * MAXT) for n in ("mx", "my", "mz")] + [("msg", _D * MAXT), ("w", _D * MAXQ)] +
                 [(n, _D * MAXT * MAXQ) for n in ("F", "DX", "DY", "DZ")] +
-                [(n, _D * MAXG * MAXG) for n in ("Ax", "Bx", "Ay", "By", "Az")])
+                [(n, _D * MAXG * MAXG) for n in ("Ax", "Bx", "Ay", "By", "Az")] +
+                [("T2", _I)] + [(n, _D * MAXT * (MAXG * MAXG)) for n in ("F2", "DX2", "DY2")] +
+                [("W2", _D * (MAXG * MAXG))])
 
 
 def tables(p):
@@ -43,6 +45,10 @@ def arr(t, name):
         return a[:G ** 3, :T]
     if name == "w":
         return a[:G ** 3]
+    if name in ("F2", "DX2", "DY2"):
+        return a[:G * G, :t.T2]
+    if name == "W2":
+        return a[:G * G]
     if name in ("mx", "my", "mz", "msg"):
         return a[:T]
     if a.ndim == 2:
@@ -129,6 +135,82 @@ class TetProblem:
         mf[f, :3] = 1
         return mv, me, mf
 
+    def face_points(self, faces):
+        """Physical coordinates [nface][G * G][3] of the Gauss points of straight faces
+        (proj2d of the face's vertex coordinates, crdtocht2d)."""
+        F2 = arr(self.tab, "F2")[:, :3]
+        X = self.mesh.pnts[self.mesh.tri_pnt[np.asarray(faces)]]       # (nf, 3, 3)
+        return np.einsum("qv,fvd->fqd", F2, X)
+
+    def flux_faces(self, inflow, neumann=(), pressure=None):
+        """Boundary faces with a flux (bdry_ins::inflow / neumann, tet_hp/ins/bdry_ins.h:85-132)
+        as the arguments of hp_tet_set_flux_faces: `inflow` faces carry the continuity flux,
+        `neumann` faces also the momentum flux with the pressure `pressure(x, y, z)` imposed
+        at their Gauss points."""
+        inflow = np.asarray(inflow, dtype=np.int32)
+        neumann = np.asarray(neumann, dtype=np.int32)
+        faces = np.concatenate([inflow, neumann]).astype(np.int32)
+        seg, sgn = self.mesh.face_edges(faces)
+        kind = np.concatenate([np.zeros(len(inflow), np.int32), np.ones(len(neumann), np.int32)])
+        G2 = self.tab.G ** 2
+        pbc = np.zeros((len(faces), G2))
+        if len(neumann):
+            x = self.face_points(neumann)
+            pbc[len(inflow):] = pressure(x[..., 0], x[..., 1], x[..., 2])
+        return dict(face_tri=faces, face_pnt=np.ascontiguousarray(self.mesh.tri_pnt[faces]),
+                    face_seg=seg, face_sgn=sgn, kind=kind, pbc=np.ascontiguousarray(pbc))
+
+    def boundary_flux(self, ff):
+        """rho times the integral of u_h . n over the faces of `ff` with the face quadrature:
+        the continuity flux summed over the vertex rows (their modes sum to one)."""
+        t, m = self.tab, self.mesh
+        em, fm = t.em, t.fm
+        F2, DX2, DY2, W2 = (arr(t, n) for n in ("F2", "DX2", "DY2", "W2"))
+        faces, pv = ff["face_tri"], ff["face_pnt"]
+        parts = [self.ugv[pv][:, :, :3]]
+        for i in range(3):
+            for k in range(em):
+                sg = ff["face_sgn"][:, i].astype(np.float64) ** k
+                parts.append((self.uge[ff["face_seg"][:, i], k, :3] * sg[:, None])[:, None, :])
+        if fm:
+            parts.append(self.ugf[faces][:, :, :3])
+        uht = np.concatenate(parts, axis=1)                        # (nf, T2, 3)
+        u = np.einsum("qk,fkn->fqn", F2, uht)
+        X = m.pnts[pv]
+        dr = np.einsum("qv,fvd->fqd", DX2[:, :3], X)
+        ds = np.einsum("qv,fvd->fqd", DY2[:, :3], X)
+        return self.phys.rho * float(np.einsum("q,fqd,fqd->", W2, u, np.cross(dr, ds)))
+
+    def balance_inflow(self, ff, lo=0.0):
+        """Shift u at the vertices of the x = lo face so that the discrete boundary flux of
+        `ff` is zero. With velocity essential on every face the vertex continuity rows sum
+        to that flux whatever the interior state, so it must vanish for the residual to
+        reach zero; u on x = lo is normal only to that face, so nothing else changes."""
+        v = np.nonzero(np.abs(self.mesh.pnts[:, 0] - lo) < 1e-12)[0]
+        f0 = self.boundary_flux(ff)
+        self.ugv[v, 0] += 1.0
+        f1 = self.boundary_flux(ff)
+        self.ugv[v, 0] -= 1.0 + f0 / (f1 - f0)
+        return self.boundary_flux(ff)
+
+    def cube_boundary(self, re=100.0, outflow=False):
+        """Unit-cube boundary layouts built from the reference's face types. outflow=False:
+        inflow (velocity essential, continuity flux) on all six faces, with the state's
+        boundary flux balanced to zero (balance_inflow). outflow=True: inflow on five faces
+        and a neumann outflow with the Beltrami pressure imposed at x = 1 (the Beltrami flow
+        crosses that face in both directions). Call before the state is uploaded. Returns
+        (essential masks, flux faces)."""
+        m = self.mesh
+        bf = m.boundary_faces()
+        cx = m.pnts[m.tri_pnt[bf], 0].mean(axis=1)
+        out = bf[cx > 1.0 - 1e-12] if outflow else bf[:0]
+        inf = bf[~np.isin(bf, out)]
+        press = lambda x, y, z: beltrami(x, y, z, re=re)[..., 3]
+        ff = self.flux_faces(inf, out, press)
+        if not outflow:
+            self.balance_inflow(ff)
+        return self.dirichlet_masks(inf), ff
+
     def set_beltrami(self, re=100.0, noise=1e-3, seed=20261209):
         """Vertex values of the Beltrami field, high-order modes zero, plus seeded
         U[-1,1) noise of amplitude `noise` on every coefficient."""
@@ -174,6 +256,7 @@ def _bind():
         lib.hp_tet_sync.argtypes = [P]
         lib.hp_tet_last_error.restype = ctypes.c_char_p
         lib.hp_tet_set_dirichlet.argtypes = [P, P, P, P]
+        lib.hp_tet_set_flux_faces.argtypes = [P, _I, P, P, P, P, P, P]
         lib.hp_tet_jacobian_diagonal.argtypes = [P]
         lib.hp_tet_download_jacobian_diagonal.argtypes = [P, P, P, P, P]
         lib.hp_tet_enqueue_update.argtypes = [P]
@@ -256,6 +339,13 @@ class TetGPU:
         _check(self.lib, self.lib.hp_tet_set_dirichlet(self.h, self._p(mv), self._p(me), self._p(mf)),
                "set_dirichlet")
 
+    def set_flux_faces(self, ff):
+        """Boundary faces with a flux (TetProblem.flux_faces / cube_boundary)."""
+        a = {k: np.ascontiguousarray(v) for k, v in ff.items()}
+        _check(self.lib, self.lib.hp_tet_set_flux_faces(
+            self.h, len(a["face_tri"]), self._p(a["face_tri"]), self._p(a["face_pnt"]), self._p(a["face_seg"]),
+            self._p(a["face_sgn"]), self._p(a["kind"]), self._p(a["pbc"])), "set_flux_faces")
+
     def jacobian_diagonal(self):
         _check(self.lib, self.lib.hp_tet_jacobian_diagonal(self.h), "jacobian_diagonal")
         out = self._out()
@@ -315,9 +405,12 @@ class TetHierarchy:
     """tet multigrid on the unit cube: p-levels p, p-1, ..., 1 on cube_tets(n), then
     h-levels cube_tets(n/2), cube_tets(n/4), ... at p = 1 (the reference decrements
     log2p = p - 1 for tetrahedra; h-levels as tet_mesh coarsening). Every level takes the
-    Beltrami state, essential velocity on the six faces, and `cfl[p]`."""
+    Beltrami state, the boundary layout of TetProblem.cube_boundary (inflow on all six
+    faces with a balanced boundary flux; outflow=True: a neumann outflow at x = 1) and
+    `cfl[p]`."""
 
-    def __init__(self, n, p, hlevels=2, mu=0.01, cfl=None, re=100.0, noise=1e-3, stream=None, fadd=1.0):
+    def __init__(self, n, p, hlevels=2, mu=0.01, cfl=None, re=100.0, noise=1e-3, stream=None, fadd=1.0,
+                 outflow=False):
         import torch
         from .tetmesh import cube_tets
         cfl = cfl or {1: 2.2, 2: 1.5, 3: 1.0, 4: 0.5}
@@ -326,12 +419,15 @@ class TetHierarchy:
             stream = ctypes.c_void_p(self._stream.cuda_stream)
         meshes = [(cube_tets(n), n)] + [(cube_tets(n >> k), n >> k) for k in range(1, hlevels + 1)]
         specs = [(0, q) for q in range(p, 0, -1)] + [(k, 1) for k in range(1, hlevels + 1)]
-        self.probs, self.levels, self.kinds = [], [], []
+        self.probs, self.levels, self.kinds, self.masks = [], [], [], []
         for li, (mi, q) in enumerate(specs):
             pr = TetProblem(meshes[mi][0], q, mu=mu, cfl=cfl[q]).set_beltrami(re=re, noise=noise)
+            masks, ff = pr.cube_boundary(re=re, outflow=outflow)
             g = TetGPU(pr, stream=stream)
-            g.set_dirichlet(pr.dirichlet_masks())
+            g.set_dirichlet(masks)
+            g.set_flux_faces(ff)
             self.probs.append(pr)
+            self.masks.append(masks)
             self.levels.append(g)
         lib = self.levels[0].lib
         lib.hp_tet_mg_attach_p.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]

@@ -87,6 +87,30 @@ class TetMesh:
     def boundary_faces(self):
         return np.nonzero(self.tri_tet[:, 1] < 0)[0].astype(np.int32)
 
+    def face_edges(self, faces):
+        """Edges of the given faces in the face's own frame: face edge i lies opposite face
+        vertex i and runs from face vertex (i+1)%3 to (i+2)%3 (the edge order of
+        tet_basis::proj2d, tet_basis/proj2d.cpp:46-91, and of tet_mesh/refineby2.cpp:142-145);
+        sgn = +1 where the global edge runs that way. Returns seg, sgn [nface][3]."""
+        faces = np.asarray(faces, dtype=np.int64)
+        a = self.tri_pnt[faces].astype(np.int64)
+        n = self.npnt
+        s0 = self.seg_pnt[:, 0].astype(np.int64)
+        s1 = self.seg_pnt[:, 1].astype(np.int64)
+        skey = np.minimum(s0, s1) * n + np.maximum(s0, s1)
+        order = np.argsort(skey)
+        seg = np.empty((len(faces), 3), np.int32)
+        sgn = np.empty((len(faces), 3), np.int32)
+        for i in range(3):
+            b, c = a[:, (i + 1) % 3], a[:, (i + 2) % 3]
+            key = np.minimum(b, c) * n + np.maximum(b, c)
+            pos = order[np.searchsorted(skey, key, sorter=order)]
+            if np.any(skey[pos] != key):
+                raise ValueError("face edge missing from the edge list")
+            seg[:, i] = pos
+            sgn[:, i] = np.where(s0[pos] == b, 1, -1)
+        return seg, sgn
+
     def boundary_entities(self, faces=None):
         """Vertices, edges and faces on the given boundary faces (default: all):
         each face's local edges are found in its tetrahedron (the edges whose two

@@ -8,6 +8,7 @@
  *   tet_basis::derivr / derivs / derivt         tet_basis/proj.cpp:781-911
  *   tet_hp::rsdl + tet_hp_ins::element_rsdl     tet_hp/update.cpp:9, tet_hp/ins/rsdl.cpp:15-785
  *   tet_hp_ins::setup_preconditioner (tau)      tet_hp/ins/setup_preconditioner.cpp
+ *   bdry_ins::neumann / inflow face fluxes      tet_hp/ins/bdry.cpp:16-102
  */
 #ifndef HP_TET_H
 #define HP_TET_H
@@ -57,6 +58,14 @@ typedef struct hp_tet_tables {
     double Ax[HP_TET_MAXG][HP_TET_MAXG], Bx[HP_TET_MAXG][HP_TET_MAXG];
     double Ay[HP_TET_MAXG][HP_TET_MAXG], By[HP_TET_MAXG][HP_TET_MAXG];
     double Az[HP_TET_MAXG][HP_TET_MAXG];
+    /* Face (triangle) basis of tet_basis::proj2d / intgrt2d (tet_basis/proj2d.cpp:20-118,
+     * intgrt2d.cpp:23-113): T2 = 3 + 3 em + fm modes (face vertices 0..2, face edge i
+     * opposite vertex i, face modes) at the G x G points q2 = i * G + j; F2 value, DX2 / DY2
+     * the derivatives proj2d returns (its y derivative of edge-0 and face modes uses gy,
+     * as the reference does), W2 = wtx * wty; intgrt2d: r(k) = sum_q2 W2 F2(q2,k) f(q2). */
+    int T2;
+    double F2[HP_TET_MAXG * HP_TET_MAXG][HP_TET_MAXT], DX2[HP_TET_MAXG * HP_TET_MAXG][HP_TET_MAXT];
+    double DY2[HP_TET_MAXG * HP_TET_MAXG][HP_TET_MAXT], W2[HP_TET_MAXG * HP_TET_MAXG];
 } hp_tet_tables;
 
 /* Builds the tables for 1 <= p <= 4. Returns 0, or -1 for an unsupported p. */
@@ -105,6 +114,18 @@ const char *hp_tet_last_error(void);
  * residual of that (entity, variable) in every mode. */
 int hp_tet_set_dirichlet(hp_tet_ctx *ctx, const unsigned char *mv, const unsigned char *me,
                          const unsigned char *mf);
+/* Boundary faces with a flux, added into res at every rsdl before the element loop
+ * (hp_face_bdry::rsdl of bdry_ins::neumann / inflow, tet_hp/ins/bdry.cpp:16-102, fluxes
+ * tet_hp/ins/bdry_ins.h:85-132; straight faces). Per face b: face_tri [b] its global face;
+ * face_pnt [b][3] its vertices (tri.pnt, with (p1 - p0) x (p2 - p0) pointing out of the
+ * domain); face_seg / face_sgn [b][3] face edge i, opposite face vertex i, and +1 where the
+ * global edge runs from face vertex (i+1)%3 to (i+2)%3, else -1 (tri.seg / tri.sgn); kind [b]
+ * 0 = inflow (continuity flux rho u.n only), 1 = neumann (also rho (u.n) u + p n with the
+ * pressure pbc [b][G*G] at the face's Gauss points, point i * G + j; NULL if no neumann face).
+ * The normal is d(x)/dr x d(x)/ds of the face map, as in neumann::element_rsdl. nface = 0
+ * removes them. */
+int hp_tet_set_flux_faces(hp_tet_ctx *ctx, int nface, const int *face_tri, const int *face_pnt,
+                          const int *face_seg, const int *face_sgn, const int *kind, const double *pbc);
 /* tet_hp::jacobian_diagonal (tet_hp/jacobi.cpp:32-111): finite-difference diagonal of every
  * element Jacobian at stage 0, summed into the global diagonal. Needs tau. */
 int hp_tet_jacobian_diagonal(hp_tet_ctx *ctx);

@@ -6,10 +6,12 @@
 //   tet_hp::ugtouht / lftog             tet_hp/gtol.cpp:16-82, 815-873
 //   tet_hp_ins::element_rsdl (straight) tet_hp/ins/rsdl.cpp:442-781
 //   tet_hp_ins::setup_preconditioner    tet_hp/ins/setup_preconditioner.cpp (diagonal: tau, iprcn)
+//   bdry_ins::neumann / inflow rsdl     tet_hp/ins/bdry.cpp:16-102, bdry_ins.h:85-132
 // with the basis operators of tet_basis in the dense form of hp_tet_tables
 // (pinned against the reference's own proj / intgrt / intgrtrst / derivr / derivs /
 // derivt by tests/test_tet_basis_pin.py). Parity: the stages of the reference's
 // loops are kept; sums over points and modes run in the natural order.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -36,6 +38,10 @@ struct OT {
     std::vector<double> jv, je, jf, ji;               // jacob_diag (tet_hp/jacobi.cpp)
     std::vector<unsigned char> mv, me, mf;            // 1 where a boundary condition fixes the row
     std::vector<double> u0v, u0e, u0f, u0i;           // ug0 of the nstage update
+    // boundary faces with a flux: global face, vertices, edges (opposite each vertex) and
+    // signs [3], kind (0 inflow, 1 neumann), imposed pressure at the face points [G * G]
+    std::vector<int> bf_tri, bf_pnt, bf_seg, bf_sgn, bf_kind;
+    std::vector<double> bf_pbc;
 };
 
 // the face vertices of local face i (tet_mesh/setup.cpp:307-310)
@@ -263,9 +269,83 @@ void scatter_unsigned(const OT &o, int tind, const double lf[NV][HP_TET_MAXT], d
         for (int n = 0; n < NV; ++n) gi[((size_t)tind * t.im + m) * NV + n] += lf[n][indx];
 }
 
+// hp_face_bdry::rsdl of bdry_ins::neumann / inflow (tet_hp/ins/bdry.cpp:16-102): for face b,
+// ugtouht2d (tet_hp/gtol.cpp:257-299), the straight-face coordinates (crdtocht2d), proj2d of
+// the coordinates and the velocity, the flux at every face point with the normal
+// nrm = d(crd)/dr x d(crd)/ds (tet_hp/ins/bdry_ins.h:85-132), intgrt2d, and the sum into res.
+void face_flux(OT &o, int b) {
+    const hp_tet_tables &t = o.t;
+    const int G2 = t.G * t.G, T2 = t.T2, em = t.em, fm = t.fm;
+    const int find = o.bf_tri[b], *pv = &o.bf_pnt[3 * b], *ps = &o.bf_seg[3 * b], *sg = &o.bf_sgn[3 * b];
+    double uht[3][HP_TET_MAXT];
+    for (int v = 0; v < 3; ++v)
+        for (int n = 0; n < 3; ++n) uht[n][v] = o.ugv[(size_t)pv[v] * NV + n];
+    int cnt = 3;
+    for (int i = 0; i < 3; ++i) {
+        int msgn = 1;
+        for (int m = 0; m < em; ++m, ++cnt) {
+            for (int n = 0; n < 3; ++n) uht[n][cnt] = msgn * o.uge[((size_t)ps[i] * em + m) * NV + n];
+            msgn *= sg[i];
+        }
+    }
+    for (int k = 0; k < fm; ++k, ++cnt)
+        for (int n = 0; n < 3; ++n) uht[n][cnt] = o.ugf[((size_t)find * fm + k) * NV + n];
+    double lf[NV][HP_TET_MAXT];
+    for (int n = 0; n < NV; ++n)
+        for (int k = 0; k < T2; ++k) lf[n][k] = 0.0;
+    for (int q = 0; q < G2; ++q) {
+        double dr[3], ds[3], u[3];
+        for (int d = 0; d < 3; ++d) {
+            dr[d] = ds[d] = 0.0;
+            for (int v = 0; v < 3; ++v) {
+                dr[d] += t.DX2[q][v] * o.pnts[3 * (size_t)pv[v] + d];
+                ds[d] += t.DY2[q][v] * o.pnts[3 * (size_t)pv[v] + d];
+            }
+        }
+        const double nrm[3] = {dr[1] * ds[2] - dr[2] * ds[1], dr[2] * ds[0] - dr[0] * ds[2],
+                               dr[0] * ds[1] - dr[1] * ds[0]};
+        for (int n = 0; n < 3; ++n) {
+            u[n] = 0.0;
+            for (int k = 0; k < T2; ++k) u[n] += t.F2[q][k] * uht[n][k];
+        }
+        double flx[NV];
+        flx[3] = o.ph.rho * (u[0] * nrm[0] + u[1] * nrm[1] + u[2] * nrm[2]);
+        for (int n = 0; n < 3; ++n)
+            flx[n] = o.bf_kind[b] ? flx[3] * u[n] + o.bf_pbc[(size_t)b * G2 + q] * nrm[n] : 0.0;
+        for (int n = 0; n < NV; ++n)
+            for (int k = 0; k < T2; ++k) lf[n][k] += t.W2[q] * t.F2[q][k] * flx[n];
+    }
+    for (int v = 0; v < 3; ++v)
+        for (int n = 0; n < NV; ++n) o.rv[(size_t)pv[v] * NV + n] += lf[n][v];
+    int indx = 3;
+    for (int i = 0; i < 3; ++i) {
+        double msgn = 1.0;
+        for (int m = 0; m < em; ++m, ++indx) {
+            for (int n = 0; n < NV; ++n) o.re[((size_t)ps[i] * em + m) * NV + n] += msgn * lf[n][indx];
+            msgn *= sg[i];
+        }
+    }
+    for (int k = 0; k < fm; ++k, ++indx)
+        for (int n = 0; n < NV; ++n) o.rf[((size_t)find * fm + k) * NV + n] += lf[n][indx];
+}
+
 }  // namespace
 
 extern "C" {
+
+// boundary faces with a flux (same arguments as hp_tet_set_flux_faces)
+void ot_set_flux_faces(void *h, int nface, const int *face_tri, const int *face_pnt, const int *face_seg,
+                       const int *face_sgn, const int *kind, const double *pbc) {
+    OT &o = *static_cast<OT *>(h);
+    const size_t G2 = (size_t)o.t.G * o.t.G;
+    o.bf_tri.assign(face_tri, face_tri + nface);
+    o.bf_pnt.assign(face_pnt, face_pnt + 3 * (size_t)nface);
+    o.bf_seg.assign(face_seg, face_seg + 3 * (size_t)nface);
+    o.bf_sgn.assign(face_sgn, face_sgn + 3 * (size_t)nface);
+    o.bf_kind.assign(kind, kind + nface);
+    o.bf_pbc.assign(G2 * nface, 0.0);
+    if (pbc) std::copy(pbc, pbc + G2 * nface, o.bf_pbc.begin());
+}
 
 void *ot_create(const hp_tet_tables *t, const hp_phys_params *ph, int npnt, int nseg, int ntri, int ntet,
                 const double *pnts, const int *tet_pnt, const int *tet_seg, const int *tet_sgn, const int *tet_tri,
@@ -477,13 +557,15 @@ void ot_get_jacobian_diagonal(void *h, double *v, double *e, double *f, double *
     if (!o.ji.empty()) std::memcpy(i, o.ji.data(), o.ji.size() * 8);
 }
 
-// tet_hp::rsdl (update.cpp:9-118) without boundary fluxes and coarse-level terms
+// tet_hp::rsdl (update.cpp:9-118): boundary-face fluxes, then the element loop; no
+// coarse-level terms
 void ot_rsdl(void *h, int stage) {
     OT &o = *static_cast<OT *>(h);
     const double omb = 1.0 - o.ph.beta[stage];
     for (auto *a : {&o.rv, &o.re, &o.rf, &o.ri}) std::fill(a->begin(), a->end(), 0.0);
     for (auto *a : {&o.rrv, &o.rre, &o.rrf, &o.rri})
         for (auto &x : *a) x *= omb;
+    for (size_t b = 0; b < o.bf_tri.size(); ++b) face_flux(o, (int)b);
     double lf_re[NV][HP_TET_MAXT], lf_im[NV][HP_TET_MAXT];
     for (int tind = 0; tind < o.ntet; ++tind) {
         element_rsdl(o, tind, stage, lf_re, lf_im);

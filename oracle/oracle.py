@@ -65,6 +65,7 @@ def lib():
         o.ot_jacobian_diagonal.argtypes = [P]
         o.ot_get_jacobian_diagonal.argtypes = [P, P, P, P, P]
         o.ot_update.argtypes = [P]
+        o.ot_set_flux_faces.argtypes = [P, I, P, P, P, P, P, P]
         _o = o
     return _o
 
@@ -110,6 +111,8 @@ def ref_tet():
         r.ref_tet_intgrt.argtypes = [I, P, P]
         r.ref_tet_intgrtrst.argtypes = [I, P, P, P, P]
         r.ref_tet_deriv.argtypes = [I, I, P, P]
+        r.ref_tet_proj2d.argtypes = [I, P, P, P, P]
+        r.ref_tet_intgrt2d.argtypes = [I, P, P]
         _rt = r
     return _rt
 
@@ -234,6 +237,12 @@ class OracleTet:
     def set_dirichlet(self, masks):
         mv, me, mf = (np.ascontiguousarray(a, dtype=np.uint8) for a in masks)
         lib().ot_set_dirichlet(self.h, _p(mv), _p(me), _p(mf))
+
+    def set_flux_faces(self, ff):
+        a = {k: np.ascontiguousarray(v) for k, v in ff.items()}
+        self._ff = a
+        lib().ot_set_flux_faces(self.h, len(a["face_tri"]), _p(a["face_tri"]), _p(a["face_pnt"]),
+                                _p(a["face_seg"]), _p(a["face_sgn"]), _p(a["kind"]), _p(a["pbc"]))
 
     def jacobian_diagonal(self):
         lib().ot_jacobian_diagonal(self.h)

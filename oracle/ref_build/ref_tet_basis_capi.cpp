@@ -127,4 +127,20 @@ int ref_tet_deriv(int p, int dir, const double *f, double *d) {
     return 0;
 }
 
+/* proj2d with derivatives of face coefficients lin[3 + 3 em + fm]; f(i, j) at i * G + j */
+int ref_tet_proj2d(int p, const double *lin, double *f, double *dx, double *dy) {
+    tet_basis *b = get_tet(p);
+    if (!b) return -1;
+    b->proj2d(const_cast<double *>(lin), f, dx, dy, b->gpx);
+    return 0;
+}
+
+/* intgrt2d: rslt[3 + 3 em + fm] (overwritten) */
+int ref_tet_intgrt2d(int p, double *rslt, const double *f) {
+    tet_basis *b = get_tet(p);
+    if (!b) return -1;
+    b->intgrt2d(rslt, const_cast<double *>(f), b->gpx);
+    return 0;
+}
+
 }  // extern "C"

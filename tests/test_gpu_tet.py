@@ -35,6 +35,46 @@ def test_tet_rsdl_matches_oracle(p):
     g.close()
 
 
+@pytest.mark.parametrize("outflow", [False, True])
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_tet_rsdl_with_face_fluxes_matches_oracle(p, outflow):
+    """The boundary-face fluxes added by rsdl at every stage: bdry_ins::inflow on the six
+    faces, or inflow on five and a neumann outflow with the Beltrami pressure at x = 1."""
+    pr = TetProblem(cube_tets(3), p, mu=0.01).set_beltrami()
+    masks, ff = pr.cube_boundary(outflow=outflow)
+    g, o = TetGPU(pr), OracleTet(pr)
+    g.set_flux_faces(ff)
+    o.set_flux_faces(ff)
+    assert g.setup_preconditioner() == 0 and o.setup_preconditioner() == 0
+    for stage in (pr.phys.nstage, 0, 1):
+        g.rsdl(stage)
+        o.rsdl(stage)
+        assert relerr(g.residual(), o.residual()) < 1e-12, f"res stage {stage}"
+    # the fluxes changed the boundary rows
+    bare = OracleTet(pr)
+    bare.setup_preconditioner()
+    bare.rsdl(1)
+    assert relerr(o.residual(), bare.residual()) > 1e-3
+    g.close()
+
+
+def test_tet_set_flux_faces_rejects_bad_indices():
+    pr = TetProblem(cube_tets(2), 2, mu=0.01).set_beltrami()
+    _, ff = pr.cube_boundary(outflow=True)
+    g = TetGPU(pr)
+    bad = dict(ff)
+    bad["face_seg"] = ff["face_seg"].copy()
+    bad["face_seg"][1, 2] = pr.mesh.nseg
+    with pytest.raises(RuntimeError, match="out of range"):
+        g.set_flux_faces(bad)
+    bad = dict(ff)
+    bad["pbc"] = np.zeros((0, 9))
+    with pytest.raises(RuntimeError, match="pbc"):
+        g.set_flux_faces(bad)
+    g.set_flux_faces(ff)
+    g.close()
+
+
 @pytest.mark.parametrize("p", [1, 2, 3, 4])
 def test_tet_jacobian_diagonal_matches_oracle(p):
     """tet_hp::jacobian_diagonal: finite differences divide rounding by dw ~ 1e-6 |u|, so
@@ -68,6 +108,23 @@ def test_tet_jacobi_updates_match_oracle(p):
     g.close()
 
 
+@pytest.mark.parametrize("p", [2, 3])
+def test_tet_jacobi_updates_with_face_fluxes_match_oracle(p):
+    pr = TetProblem(cube_tets(3), p, mu=0.01).set_beltrami()
+    masks, ff = pr.cube_boundary(outflow=True)
+    g, o = TetGPU(pr), OracleTet(pr)
+    for x in (g, o):
+        x.set_dirichlet(masks)
+        x.set_flux_faces(ff)
+        assert x.setup_preconditioner() == 0
+        x.jacobian_diagonal()
+    for _ in range(3):
+        g.update()
+        o.update()
+    assert relerr(g.state(), o.state()) < 1e-9
+    g.close()
+
+
 def test_tet_multigrid_reduces_residual_and_keeps_essential_values():
     """p-levels 3, 2, 1 and two h-levels (tet_hp mg_restrict / mg_prolongate with the
     FAS source): the residual falls, and the velocity on the boundary faces (essential)
@@ -77,7 +134,7 @@ def test_tet_multigrid_reduces_residual_and_keeps_essential_values():
     u0 = [a.copy() for a in H.probs[0].state]
     hist, sec, cycles = H.solve(drop=1e-10, max_cycles=30, vw=1)
     assert np.all(np.isfinite(hist)) and hist[-1] < 0.2
-    mv, me, mf = (m.astype(bool) for m in H.probs[0].dirichlet_masks())
+    mv, me, mf = (m.astype(bool) for m in H.masks[0])
     u = H.levels[0].state()
     assert np.array_equal(u[0][mv], u0[0][mv])
     assert np.array_equal(u[1][np.broadcast_to(me[:, None, :], u[1].shape)],

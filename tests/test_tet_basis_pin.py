@@ -68,3 +68,26 @@ def test_tet_dense_operators_match_reference_sum_factorisation(p):
             out = np.zeros(Q)
             r.ref_tet_deriv(p, d, ptr(g[d]), ptr(out))
             assert rel(TB.deriv(t, d, g[d]), out) < 1e-13, d
+
+
+@needs_ref
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_tet_face_operators_match_reference_proj2d_intgrt2d(p):
+    """Dense face operators F2 / DX2 / DY2 / W2 against tet_basis::proj2d and intgrt2d."""
+    r = O.ref_tet()
+    t = TB.tables(p)
+    G, T2 = t.G, t.T2
+    assert T2 == 3 + 3 * t.em + t.fm
+    F2, DX2, DY2, W2 = (TB.arr(t, n) for n in ("F2", "DX2", "DY2", "W2"))
+    rng = np.random.default_rng(10 + p)
+    for _ in range(3):
+        lin = rng.uniform(-1, 1, T2)
+        f, dx, dy = (np.zeros(G * G) for _ in range(3))
+        assert r.ref_tet_proj2d(p, ptr(lin), ptr(f), ptr(dx), ptr(dy)) == 0
+        assert rel(F2 @ lin, f) < 1e-13
+        assert rel(DX2 @ lin, dx) < 1e-13
+        assert rel(DY2 @ lin, dy) < 1e-13
+        g = rng.uniform(-1, 1, G * G)
+        res = np.zeros(T2)
+        assert r.ref_tet_intgrt2d(p, ptr(res), ptr(g)) == 0
+        assert rel(F2.T @ (W2 * g), res) < 1e-13

@@ -1,0 +1,138 @@
+"""Boundary-face fluxes of the tet path (bdry_ins::inflow / neumann, tet_hp/ins/bdry.cpp:16-102):
+the face connectivity against a brute-force search, and the oracle's face flux against the
+divergence theorem. For a random modal velocity u_h (every vertex, edge, face and interior
+mode set), the continuity flux rho u_h . n summed over the vertex pressure rows (the vertex
+modes sum to one on every face) is rho times the integral of u_h . n over the boundary, which
+must equal rho times the volume integral of div u_h computed with the 3D operators. Both
+quadratures are exact for these degrees, so the two agree to rounding only if the face gather
+(edges, signs, face modes) gives the trace of the 3D field and the normal points out."""
+import numpy as np
+import pytest
+
+from hpb import tet as TB
+from hpb.tetmesh import cube_tets
+from oracle import oracle as O
+
+
+def test_face_edges_match_brute_force():
+    m = cube_tets(2)
+    bf = m.boundary_faces()
+    seg, sgn = m.face_edges(bf)
+    for f, s, g in zip(bf, seg, sgn):
+        a = m.tri_pnt[f]
+        for i in range(3):
+            b, c = a[(i + 1) % 3], a[(i + 2) % 3]
+            hit = [k for k in range(m.nseg) if set(m.seg_pnt[k]) == {b, c}]
+            assert hit == [s[i]]
+            assert g[i] == (1 if m.seg_pnt[s[i], 0] == b else -1)
+
+
+def test_boundary_face_normals_point_out():
+    m = cube_tets(3)
+    bf = m.boundary_faces()
+    t = m.tri_tet[bf, 0]
+    X = m.pnts[m.tri_pnt[bf]]
+    nrm = np.cross(X[:, 1] - X[:, 0], X[:, 2] - X[:, 0])
+    opp = m.pnts[m.tet_pnt[t]].mean(axis=1)          # centroid of the owning tetrahedron
+    assert np.all(np.einsum("fd,fd->f", nrm, X[:, 0] - opp) > 0)
+
+
+def gather3d(prob, tind):
+    """ugtouht of one tetrahedron (tet_hp/gtol.cpp:16-82): uht [T][4]."""
+    m, t = prob.mesh, prob.tab
+    em, fm, im = t.em, t.fm, t.im
+    v, e, f, i = prob.state
+    out = [v[m.tet_pnt[tind]]]
+    for k in range(6):
+        s, g = m.tet_seg[tind, k], m.tet_sgn[tind, k]
+        out.append(e[s] * (float(g) ** np.arange(em))[:, None])
+    for k in range(4):
+        fa, sg = m.tet_tri[tind, k], -m.tet_rot[tind, k]
+        rows = np.concatenate([np.full(em - r, r) for r in range(1, em)]) if em > 1 else np.zeros(0, int)
+        out.append(f[fa] * (float(sg) ** (rows - 1))[:, None])
+    out.append(i[tind])
+    return np.concatenate(out, axis=0)
+
+
+def volume_divergence(prob):
+    t = prob.tab
+    F, DX, DY, DZ, w = (TB.arr(t, n) for n in ("F", "DX", "DY", "DZ", "w"))
+    m = prob.mesh
+    total, vol = 0.0, 0.0
+    for tind in range(m.ntet):
+        xv = m.pnts[m.tet_pnt[tind]]
+        J = np.stack([D[:, :4] @ xv for D in (DX, DY, DZ)], axis=2)   # J[q][x][r]
+        uht = gather3d(prob, tind)
+        dref = np.stack([D @ uht[:, :3] for D in (DX, DY, DZ)], axis=2)  # [q][var][r]
+        grad = np.einsum("qrx,qnr->qnx", np.linalg.inv(J), dref)        # du_n / dx_x
+        det = np.abs(np.linalg.det(J))
+        total += np.sum(w * det * np.trace(grad, axis1=1, axis2=2))
+        vol += np.sum(w * det)
+    return total, vol
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_face_flux_satisfies_divergence_theorem(p):
+    mesh = cube_tets(2)
+    pr = TB.TetProblem(mesh, p, rho=1.3, mu=0.01).set_beltrami(noise=0.0)
+    rng = np.random.default_rng(40 + p)
+    for a in pr.state:
+        a[:] = rng.uniform(-1, 1, a.shape)
+    div, vol = volume_divergence(pr)
+    assert abs(vol - 1.0) < 1e-12          # the 3D weights integrate the unit cube
+    ff = pr.flux_faces(mesh.boundary_faces())
+    with_f, without = O.OracleTet(pr), O.OracleTet(pr)
+    with_f.set_flux_faces(ff)
+    with_f.rsdl(0)
+    without.rsdl(0)
+    flux = with_f.residual()[0][:, 3] - without.residual()[0][:, 3]
+    assert abs(flux.sum() - 1.3 * div) < 1e-11 * max(1.0, abs(div))
+
+
+def test_neumann_face_flux_of_a_constant_state():
+    """Constant velocity U and imposed pressure P on every face of the cube: the momentum flux
+    summed over the vertex rows is sum over faces of (rho U.n U + P n) = 0, and the x = 1 face
+    alone gives (rho U_x U + P e_x) times its area."""
+    mesh = cube_tets(2)
+    pr = TB.TetProblem(mesh, 3, mu=0.01).set_beltrami(noise=0.0)
+    for a in pr.state:
+        a[:] = 0.0
+    U = np.array([0.3, -0.2, 0.5])
+    pr.ugv[:, :3] = U
+    bf = mesh.boundary_faces()
+    cx = mesh.pnts[mesh.tri_pnt[bf], 0].mean(axis=1)
+    for faces, expect in ((bf, np.zeros(3)), (bf[cx > 1 - 1e-12], 0.3 * U + np.array([2.0, 0, 0]))):
+        ff = pr.flux_faces([], faces, lambda x, y, z: np.full_like(x, 2.0))
+        with_f, without = O.OracleTet(pr), O.OracleTet(pr)
+        with_f.set_flux_faces(ff)
+        with_f.rsdl(0)
+        without.rsdl(0)
+        mom = (with_f.residual()[0] - without.residual()[0])[:, :3].sum(axis=0)
+        assert np.max(np.abs(mom - expect)) < 1e-12
+
+
+@pytest.mark.parametrize("p", [2, 3])
+def test_balanced_inflow_makes_the_continuity_rows_consistent(p):
+    """Velocity essential on all six faces: the vertex pressure rows of the whole residual sum
+    to the boundary flux whatever the interior state, so after balance_inflow they sum to zero,
+    and the host's boundary_flux equals the oracle's face-flux sum before balancing."""
+    pr = TB.TetProblem(cube_tets(3), p, rho=1.1, mu=0.01).set_beltrami()
+    ff = pr.flux_faces(pr.mesh.boundary_faces())
+    phi = pr.boundary_flux(ff)
+    with_f, without = O.OracleTet(pr), O.OracleTet(pr)
+    with_f.set_flux_faces(ff)
+    for o in (with_f, without):
+        assert o.setup_preconditioner() == 0
+        o.rsdl(0)
+    assert abs(phi) > 1e-6
+    fsum = (with_f.residual()[0][:, 3] - without.residual()[0][:, 3]).sum()
+    assert abs(fsum - phi) < 1e-12 * max(1.0, abs(phi))
+    masks, ff = pr.cube_boundary()
+    assert abs(pr.boundary_flux(ff)) < 1e-14
+    o = O.OracleTet(pr)
+    o.set_flux_faces(ff)
+    assert o.setup_preconditioner() == 0
+    for stage in (0, pr.phys.nstage):
+        o.rsdl(stage)
+        rv = o.residual()[0][:, 3]
+        assert abs(rv.sum()) < 1e-13 * np.abs(rv).sum()
