@@ -261,7 +261,7 @@ def tet_flops_per_element(p, beta_positive=True):
     return 2 * (proj + intg)
 
 
-def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False):
+def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=None):
     """3D tet_hp ins: the unit cube split into n^3 hexahedra x 6 tetrahedra (n = 64:
     1,572,864 tetrahedra), p = 3, Re 100, the Ethier-Steinman Beltrami state at the
     vertices plus 1e-3 seeded noise on every coefficient. Times tet_hp::rsdl(nstage)
@@ -337,12 +337,16 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False):
                               "ms_per_cycle_incl_setup": 1e3 * sec / max(nc, 1), "drop": float(h[-1]),
                               "drop_history": [float(x) for x in h[::max(1, len(h) // 10)]]}
     if full_solve:
-        # W-cycles (vwcycle 2) from the initial state on a hierarchy down to 2^3 x 6
+        # W-cycles (vwcycle 2) from the initial state on a hierarchy down to 2^3 x 6 for
+        # n <= 32 and to 8^3 x 6 above (with more levels the W-cycle visits the coarsest
+        # Jacobi-smoothed level 2^levels times per cycle, and at 64^3 down to 2^3 it diverged),
+        # or `hlevels` h-levels
         H.close()
-        hl = max(1, int(round(np.log2(n))) - 1)
+        ln = int(round(np.log2(n)))
+        hl = hlevels or (max(1, ln - 1) if n <= 32 else max(1, ln - 3))
         H = TetHierarchy(n, p, hlevels=hl, mu=1.0 / 100.0, cfl=cfl, stream=ctypes.c_void_p(cur.cuda_stream))
         h, sec, nc = H.solve(drop=1e-10, max_cycles=400, vw=2)
-        line["multigrid_full_w_to_1e-10"] = {"levels": f"p {p}..1, then h-levels down to 2^3 at p = 1",
+        line["multigrid_full_w_to_1e-10"] = {"levels": f"p {p}..1, then h-levels down to {n >> hl}^3 at p = 1",
                                              "seconds": sec, "cycles": nc, "drop": float(h[-1]),
                                              "reached": bool(h[-1] <= 1e-10), "ms_per_cycle": 1e3 * sec / max(nc, 1),
                                              "drop_history": [float(x) for x in h[::max(1, len(h) // 10)]]}
@@ -579,6 +583,9 @@ def main():
                          "c4: ins past a cylinder in a channel (curved hole, graded ~150k triangles), learned "
                          "preconditioner trained on Re in [20, 200], judged on held-out Re by the FP64 residual")
     ap.add_argument("--p", type=int, nargs="*", default=None, help="with --sweep: the p values")
+    ap.add_argument("--tet-hlevels", type=int, default=None,
+                    help="with --sweep c5 --tet-solve: h-levels of the W-cycle hierarchy (default: down to 2^3 "
+                         "for n <= 32, to 8^3 above)")
     ap.add_argument("--tet-solve", action="store_true",
                     help="with --sweep c5: also W-cycles on the full hierarchy to a 1e-10 drop (minutes)")
     args = ap.parse_args()
@@ -631,7 +638,7 @@ def main():
     if args.sweep == "c5":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         c5_sweep(torch, dev, args.mesh if args.mesh != N_MESH else 64, (args.p or [3])[0], args.steps, args.warmup,
-                 timed_factory(torch, flush), full_solve=args.tet_solve)
+                 timed_factory(torch, flush), full_solve=args.tet_solve, hlevels=args.tet_hlevels)
         return
 
     if args.physics == "ins":
