@@ -141,7 +141,7 @@ MG_N = 320
 CD_CFL = {8: 0.3, 6: 0.35, 4: 0.5, 3: 0.6, 2: 0.75, 1: 1.0}
 
 
-def c3_sweep(hpb, dev, n, p, cycles):
+def c3_sweep(hpb, dev, n, p, cycles, arms=None):
     """ins lid-driven cavity, Re 400 (rho 1, mu 1/400), p on an n x n split-square mesh
     (n = 512: 524,288 triangles, 28.3 M DOF at p = 6); u = 1 on the lid, velocity
     Dirichlet on every wall, initial state the boundary field projected plus 1e-3 noise.
@@ -160,6 +160,8 @@ def c3_sweep(hpb, dev, n, p, cycles):
                            ("fp32_defect_correction", {"vw": 2, "mixed": True}, True),
                            ("fp32_defect_correction_autotuned", {"vw": 2, "mixed": True, "tune": True}, True),
                            ("fp64_v_cycle", {"vw": 1}, True), ("fp64_h_levels_only", {"vw": 2}, False)):
+        if arms and name not in arms:
+            continue
         t0 = _t.perf_counter()
         H = MG.build(mk, n=n, p=p, hlevels=3, plevels=plev)
         setup = _t.perf_counter() - t0
@@ -583,6 +585,8 @@ def main():
                          "c4: ins past a cylinder in a channel (curved hole, graded ~150k triangles), learned "
                          "preconditioner trained on Re in [20, 200], judged on held-out Re by the FP64 residual")
     ap.add_argument("--p", type=int, nargs="*", default=None, help="with --sweep: the p values")
+    ap.add_argument("--arms", nargs="*", default=None,
+                    help="with --sweep c3: run only these arms (e.g. fp64_level_by_level fp32_defect_correction)")
     ap.add_argument("--tet-hlevels", type=int, default=None,
                     help="with --sweep c5 --tet-solve: h-levels of the W-cycle hierarchy (default: down to 2^3 "
                          "for n <= 32, to 8^3 above)")
@@ -633,7 +637,7 @@ def main():
         c4_sweep(hpb, dev, args.scale, args.steps)
         return
     if args.sweep == "c3":
-        c3_sweep(hpb, dev, args.mesh if args.mesh != N_MESH else 512, (args.p or [6])[0], args.steps)
+        c3_sweep(hpb, dev, args.mesh if args.mesh != N_MESH else 512, (args.p or [6])[0], args.steps, arms=args.arms)
         return
     if args.sweep == "c5":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")

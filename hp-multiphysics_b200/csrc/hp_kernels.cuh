@@ -100,7 +100,7 @@ struct ElemCfg {
     static constexpr int NPAIR = NV;               // flux pairs integrated by intgrtrs
     static constexpr int NQ = (PHYS == 1 ? 16 : 7);  // per-point scratch values
     static constexpr int WPC = (P <= 4 ? 8 : 4);   // warps per CTA
-    static constexpr int EPW = (P == 1 ? 4 : (P == 2 ? 2 : 1));  // elements per warp (lane groups)
+    static constexpr int EPW = (P == 1 ? 4 : (P <= 3 ? 2 : 1));  // elements per warp (lane groups)
     static constexpr int NB = (PHYS == 1 ? 2 : 0);  // base-state variables gathered in correction form
     // per-warp scratch (in R units)
     static constexpr int S_UHT = (NV + NB) * T;
