@@ -882,6 +882,15 @@ extern "C" int hp_tet_basis_build(int p, hp_tet_tables *out) {
                 }
             }
     }
+    // lumpinv's mass matrix and lumped vertex inverse
+    const int NQ3 = G * G * G;
+    for (int m = 0; m < T; ++m)
+        for (int k = 0; k < T; ++k) {
+            double acc = 0.0;
+            for (int q = 0; q < NQ3; ++q) acc += t.w[q] * t.F[q][m] * t.F[q][k];
+            t.mm[m][k] = acc;
+        }
+    t.vdiag = 1.0 / (t.mm[0][0] + t.mm[0][1] + t.mm[0][2] + t.mm[0][3]);
     deriv_operator(G, t.dltx, t.dltx2, t.Ax);
     deriv_operator(G, t.dltx, t.dltx3, t.Bx);
     deriv_operator(G, t.dlty, t.dlty2, t.Ay);

@@ -619,6 +619,18 @@ __global__ void k_tet_prcn(TetMeshD mesh, const double *ugv, double *tau, double
 
 // tet_hp::update stage, JACOBI build (update.cpp:206-390, jacobi.cpp:14-30): essential rows
 // zeroed, res = 0.5 res / jacob_diag, ug = ug0 - cflalpha res
+// tet_hp::minvrt at p = 1 (its em = 0 branch, tet_hp/setup_preconditioner.cpp:57-74, vprcn
+// pre-inverted as in tet_hp::setup_preconditioner) with the nstage update of tet_hp::update
+// (tet_hp/update.cpp:181-390): res.v *= (1 / vprcn) vdiag, fixed rows zeroed, ug = ug0 - ca res.
+__global__ void k_tet_minvrt1(long n, double *res, const double *vprcn, double vdiag, const unsigned char *mask,
+                              double *u, const double *u0, double ca) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        const double r = mask[k] ? 0.0 : res[k] * ((1.0 / vprcn[k]) * vdiag);
+        res[k] = r;
+        u[k] = u0[k] - ca * r;
+    }
+}
+
 __global__ void k_tet_relax(long n, double *res, const double *jd, const unsigned char *mask, double *u,
                             const double *u0, double ca) {
     for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
@@ -717,6 +729,8 @@ struct hp_tet_ctx {
     double *U0 = nullptr, *JD = nullptr, *rbar = nullptr, *part = nullptr;  // update, jacob_diag
     unsigned char *mask = nullptr;  // 1: row fixed by an essential condition
     bool jd_ready = false;
+    int smoother = 0;  // 0: JACOBI build (jacobi_relaxation), 1: minvrt (p = 1)
+    bool smoother_ready() const { return smoother ? prcn_ready : jd_ready; }
     // multigrid: this level is coarser than `fine` (kind 1: p-level, 2: h-level)
     hp_tet_ctx *fine = nullptr;
     int kind = 0;
@@ -1205,10 +1219,24 @@ extern "C" int hp_tet_download_jacobian_diagonal(hp_tet_ctx *c, double *v, doubl
     return copy_fields(c, c->JD, nullptr, nullptr, nullptr, nullptr, v, e, f, i);
 }
 
+extern "C" int hp_tet_set_smoother(hp_tet_ctx *c, int kind) {
+    if (!c || (kind != 0 && kind != 1)) {
+        set_err("hp_tet_set_smoother: kind 0 (JACOBI build) or 1 (minvrt)");
+        return HP_EINVAL;
+    }
+    if (kind == 1 && c->p != 1) {
+        set_err("hp_tet_set_smoother: tet_hp::minvrt is built for p = 1 only");
+        return HP_EINVAL;
+    }
+    c->smoother = kind;
+    return HP_OK;
+}
+
 extern "C" int hp_tet_enqueue_update(hp_tet_ctx *c) {
     if (!c) return HP_EINVAL;
-    if (!c->jd_ready) {
-        set_err("hp_tet_update needs hp_tet_jacobian_diagonal first");
+    if (!c->smoother_ready()) {
+        set_err(c->smoother ? "hp_tet_update (minvrt) needs hp_tet_setup_preconditioner first"
+                            : "hp_tet_update needs hp_tet_jacobian_diagonal first");
         return HP_ESTATE;
     }
     TCK(cudaMemcpyAsync(c->U0, c->U, 8 * c->ltot, cudaMemcpyDeviceToDevice, c->stream));
@@ -1216,8 +1244,12 @@ extern "C" int hp_tet_enqueue_update(hp_tet_ctx *c) {
         int r = hp_tet_enqueue_rsdl(c, stage);
         if (r) return r;
         const double ca = c->ph.alpha[stage] * c->ph.cfl;
-        k_tet_relax<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
-            (long)c->ltot, c->RES, c->JD, c->mask, c->U, c->U0, ca);
+        if (c->smoother)  // p = 1: the state is the vertex section alone (ltot = lv)
+            k_tet_minvrt1<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+                (long)c->ltot, c->RES, c->vprcn, c->tab.vdiag, c->mask, c->U, c->U0, ca);
+        else
+            k_tet_relax<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+                (long)c->ltot, c->RES, c->JD, c->mask, c->U, c->U0, ca);
     }
     TCK(cudaGetLastError());
     return HP_OK;
@@ -1255,7 +1287,7 @@ extern "C" int hp_tet_solve(hp_tet_ctx *c, double drop, int max_updates, int che
     TCK(cudaEventRecord(e0, c->stream));
     int r = hp_tet_setup_preconditioner(c);
     if (r) return r < 0 ? r : HP_ESTATE;
-    if ((r = hp_tet_jacobian_diagonal(c))) return r;
+    if (!c->smoother && (r = hp_tet_jacobian_diagonal(c))) return r;
     double r0;
     if ((r = hp_tet_resnorm(c, &r0))) return r;
     int nh = 0, nu = 0;
@@ -1401,10 +1433,10 @@ static int tet_cycle(hp_tet_ctx **lv, int n, int lvl, int vw, int itercrsn, int 
     hp_tet_ctx *c = lv[lvl];
     int r;
     for (int vc = 0; vc < vw; ++vc) {
-        if (!c->jd_ready) {
+        if (!c->smoother_ready()) {
             r = hp_tet_setup_preconditioner(c);
             if (r) return r < 0 ? r : HP_ESTATE;
-            if ((r = hp_tet_jacobian_diagonal(c))) return r;
+            if (!c->smoother && (r = hp_tet_jacobian_diagonal(c))) return r;
         }
         for (int it = 0; it < itercrsn; ++it)
             if ((r = hp_tet_enqueue_update(c))) return r;

@@ -20,7 +20,7 @@ class TetTables(ctypes.Structure):
                 [(n, _D * MAXT * MAXQ) for n in ("F", "DX", "DY", "DZ")] +
                 [(n, _D * MAXG * MAXG) for n in ("Ax", "Bx", "Ay", "By", "Az")] +
                 [("T2", _I)] + [(n, _D * MAXT * (MAXG * MAXG)) for n in ("F2", "DX2", "DY2")] +
-                [("W2", _D * (MAXG * MAXG))])
+                [("W2", _D * (MAXG * MAXG)), ("mm", _D * MAXT * MAXT), ("vdiag", _D)])
 
 
 def tables(p):
@@ -49,6 +49,8 @@ def arr(t, name):
         return a[:G * G, :t.T2]
     if name == "W2":
         return a[:G * G]
+    if name == "mm":
+        return a[:T, :T]
     if name in ("mx", "my", "mz", "msg"):
         return a[:T]
     if a.ndim == 2:
@@ -257,6 +259,7 @@ def _bind():
         lib.hp_tet_last_error.restype = ctypes.c_char_p
         lib.hp_tet_set_dirichlet.argtypes = [P, P, P, P]
         lib.hp_tet_set_flux_faces.argtypes = [P, _I, P, P, P, P, P, P]
+        lib.hp_tet_set_smoother.argtypes = [P, _I]
         lib.hp_tet_jacobian_diagonal.argtypes = [P]
         lib.hp_tet_download_jacobian_diagonal.argtypes = [P, P, P, P, P]
         lib.hp_tet_enqueue_update.argtypes = [P]
@@ -339,6 +342,10 @@ class TetGPU:
         _check(self.lib, self.lib.hp_tet_set_dirichlet(self.h, self._p(mv), self._p(me), self._p(mf)),
                "set_dirichlet")
 
+    def set_smoother(self, kind):
+        """0: the JACOBI build's jacobi_relaxation; 1: tet_hp::minvrt (p = 1 only)."""
+        _check(self.lib, self.lib.hp_tet_set_smoother(self.h, kind), "set_smoother")
+
     def set_flux_faces(self, ff):
         """Boundary faces with a flux (TetProblem.flux_faces / cube_boundary)."""
         a = {k: np.ascontiguousarray(v) for k, v in ff.items()}
@@ -407,10 +414,11 @@ class TetHierarchy:
     log2p = p - 1 for tetrahedra; h-levels as tet_mesh coarsening). Every level takes the
     Beltrami state, the boundary layout of TetProblem.cube_boundary (inflow on all six
     faces with a balanced boundary flux; outflow=True: a neumann outflow at x = 1) and
-    `cfl[p]`."""
+    `cfl[p]`; p1_smoother = 1 smooths the p = 1 levels with tet_hp::minvrt instead of the
+    JACOBI build's relaxation."""
 
     def __init__(self, n, p, hlevels=2, mu=0.01, cfl=None, re=100.0, noise=1e-3, stream=None, fadd=1.0,
-                 outflow=False):
+                 outflow=False, p1_smoother=0):
         import torch
         from .tetmesh import cube_tets
         cfl = cfl or {1: 2.2, 2: 1.5, 3: 1.0, 4: 0.5}
@@ -426,6 +434,8 @@ class TetHierarchy:
             g = TetGPU(pr, stream=stream)
             g.set_dirichlet(masks)
             g.set_flux_faces(ff)
+            if q == 1 and p1_smoother:
+                g.set_smoother(p1_smoother)
             self.probs.append(pr)
             self.masks.append(masks)
             self.levels.append(g)

@@ -66,6 +66,12 @@ typedef struct hp_tet_tables {
     int T2;
     double F2[HP_TET_MAXG * HP_TET_MAXG][HP_TET_MAXT], DX2[HP_TET_MAXG * HP_TET_MAXG][HP_TET_MAXT];
     double DY2[HP_TET_MAXG * HP_TET_MAXG][HP_TET_MAXT], W2[HP_TET_MAXG * HP_TET_MAXG];
+    /* tet_basis::lumpinv (tet_basis/initialize.cpp:521-639): the mass matrix
+     * mm(m, k) = sum_q w F(q,m) F(q,k), and vdiag = 1 / (mm(0,0) + mm(0,1) + mm(0,2) + mm(0,3)),
+     * the lumped vertex mass inverse, which is tet_basis::vdiag at p = 1 (at p >= 2 lumpinv
+     * replaces it by a constrained value that is not built). */
+    double mm[HP_TET_MAXT][HP_TET_MAXT];
+    double vdiag;
 } hp_tet_tables;
 
 /* Builds the tables for 1 <= p <= 4. Returns 0, or -1 for an unsupported p. */
@@ -109,6 +115,13 @@ int hp_tet_rsdl(hp_tet_ctx *ctx, int stage);
 int hp_tet_sync(hp_tet_ctx *ctx);
 const char *hp_tet_last_error(void);
 
+/* The smoother of hp_tet_update, hp_tet_solve and hp_tet_solve_mg: kind 0 = the JACOBI
+ * build (jacobian_diagonal + jacobi_relaxation, tet_hp/jacobi.cpp:14-111; the default);
+ * kind 1 = the default build's tet_hp::minvrt (tet_hp/setup_preconditioner.cpp:11-74 with
+ * the inversion of tet_hp::setup_preconditioner, :428-460), built for p = 1, where it is
+ * res.v *= vdiag / vprcn on the rows no essential condition fixes. kind 1 at p > 1 returns
+ * HP_EINVAL. */
+int hp_tet_set_smoother(hp_tet_ctx *ctx, int kind);
 /* Rows fixed by essential conditions (bdry_ins::inflow on boundary faces,
  * tet_hp/ins/bdry_ins.h:141-183): masks [npnt][4], [nseg][4], [ntri][4], 1 = zero the
  * residual of that (entity, variable) in every mode. */

@@ -42,6 +42,7 @@ struct OT {
     // signs [3], kind (0 inflow, 1 neumann), imposed pressure at the face points [G * G]
     std::vector<int> bf_tri, bf_pnt, bf_seg, bf_sgn, bf_kind;
     std::vector<double> bf_pbc;
+    int smoother = 0;  // 0: JACOBI build, 1: minvrt (p = 1)
 };
 
 // the face vertices of local face i (tet_mesh/setup.cpp:307-310)
@@ -530,17 +531,35 @@ static void jacobi_relaxation(OT &o) {
     all_dirichlet(o);
 }
 
+// tet_hp::minvrt at p = 1 (setup_preconditioner.cpp:57-74): vprcn pre-inverted by
+// tet_hp::setup_preconditioner (:451-453), res.v *= vprcn vdiag, then the vertex Dirichlet
+// rows are zeroed; em = 0 ends it.
+static void minvrt_p1(OT &o) {
+    for (size_t k = 0; k < o.rv.size(); ++k) o.rv[k] *= (1.0 / o.vprcn[k]) * o.t.vdiag;
+    all_dirichlet(o);
+}
+
+// 0: the JACOBI build's smoother, 1: minvrt (p = 1 only; -1 otherwise)
+int ot_set_smoother(void *h, int kind) {
+    OT &o = *static_cast<OT *>(h);
+    if (kind != 0 && (kind != 1 || o.t.p != 1)) return -1;
+    o.smoother = kind;
+    return 0;
+}
+
 void ot_rsdl(void *h, int stage);
 
-// tet_hp::update, JACOBI build (update.cpp:181-390): nstage stages of rsdl, boundary
-// zeroing, Jacobi relaxation and ug = ug0 - alpha(stage) cfl res.
+// tet_hp::update (update.cpp:181-390): nstage stages of rsdl, boundary zeroing, the
+// smoother (jacobi_relaxation in the JACOBI build, else minvrt) and
+// ug = ug0 - alpha(stage) cfl res.
 void ot_update(void *h) {
     OT &o = *static_cast<OT *>(h);
     o.u0v = o.ugv; o.u0e = o.uge; o.u0f = o.ugf; o.u0i = o.ugi;
     for (int stage = 0; stage < o.ph.nstage; ++stage) {
         ot_rsdl(h, stage);
         all_dirichlet(o);
-        jacobi_relaxation(o);
+        if (o.smoother) minvrt_p1(o);
+        else jacobi_relaxation(o);
         const double ca = o.ph.alpha[stage] * o.ph.cfl;
         for (size_t k = 0; k < o.ugv.size(); ++k) o.ugv[k] = o.u0v[k] - ca * o.rv[k];
         for (size_t k = 0; k < o.uge.size(); ++k) o.uge[k] = o.u0e[k] - ca * o.re[k];

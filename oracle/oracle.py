@@ -66,6 +66,7 @@ def lib():
         o.ot_get_jacobian_diagonal.argtypes = [P, P, P, P, P]
         o.ot_update.argtypes = [P]
         o.ot_set_flux_faces.argtypes = [P, I, P, P, P, P, P, P]
+        o.ot_set_smoother.argtypes = [P, I]
         _o = o
     return _o
 
@@ -243,6 +244,10 @@ class OracleTet:
         self._ff = a
         lib().ot_set_flux_faces(self.h, len(a["face_tri"]), _p(a["face_tri"]), _p(a["face_pnt"]),
                                 _p(a["face_seg"]), _p(a["face_sgn"]), _p(a["kind"]), _p(a["pbc"]))
+
+    def set_smoother(self, kind):
+        if lib().ot_set_smoother(self.h, kind) != 0:
+            raise ValueError("minvrt is restated for p = 1 only")
 
     def jacobian_diagonal(self):
         lib().ot_jacobian_diagonal(self.h)

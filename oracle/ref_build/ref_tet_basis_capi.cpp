@@ -81,6 +81,8 @@ int ref_tet_get(int p, const char *name, double *out) {
     else if (n == "dlty2") { T2(g, g, i == j ? 0.0 : b->dlty2(i, j)) }
     else if (n == "dlty3") { T2(g, g, i == j ? 0.0 : b->dlty3(i, j)) }
     else if (n == "dltz2") { T2(g, g, i == j ? 0.0 : b->dltz2(i, j)) }
+    else if (n == "mm") { T2(b->tm, b->tm, b->mm(i, j)) }
+    else if (n == "vdiag") { T1(1, b->vdiag) }
     else return -1;
 #undef T1
 #undef T2

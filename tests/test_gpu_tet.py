@@ -140,3 +140,37 @@ def test_tet_multigrid_reduces_residual_and_keeps_essential_values():
     assert np.array_equal(u[1][np.broadcast_to(me[:, None, :], u[1].shape)],
                           u0[1][np.broadcast_to(me[:, None, :], u0[1].shape)])
     H.close()
+
+
+def test_tet_minvrt_p1_updates_match_oracle():
+    """tet_hp::update with tet_hp::minvrt at p = 1 (res.v *= vdiag / vprcn), face fluxes and
+    essential rows, at the reference's p = 1 cfl 2.2."""
+    pr = TetProblem(cube_tets(3), 1, mu=0.01, cfl=2.2).set_beltrami()
+    masks, ff = pr.cube_boundary()
+    g, o = TetGPU(pr), OracleTet(pr)
+    for x in (g, o):
+        x.set_dirichlet(masks)
+        x.set_flux_faces(ff)
+        x.set_smoother(1)
+        assert x.setup_preconditioner() == 0
+    for _ in range(3):
+        g.update()
+        o.update()
+    assert relerr(g.state(), o.state()) < 1e-12
+    g.close()
+
+
+def test_tet_set_smoother_minvrt_needs_p1():
+    pr = TetProblem(cube_tets(2), 2, mu=0.01).set_beltrami()
+    g = TetGPU(pr)
+    with pytest.raises(RuntimeError, match="p = 1"):
+        g.set_smoother(1)
+    g.close()
+
+
+def test_tet_multigrid_with_minvrt_on_p1_levels_reduces_residual():
+    from hpb.tet import TetHierarchy
+    H = TetHierarchy(8, 3, hlevels=2, mu=0.01, cfl={1: 2.2, 2: 0.5, 3: 0.5}, p1_smoother=1)
+    hist, sec, cycles = H.solve(drop=1e-10, max_cycles=30, vw=2)
+    assert np.all(np.isfinite(hist)) and hist[-1] < 1e-2
+    H.close()

@@ -91,3 +91,17 @@ def test_tet_face_operators_match_reference_proj2d_intgrt2d(p):
         res = np.zeros(T2)
         assert r.ref_tet_intgrt2d(p, ptr(res), ptr(g)) == 0
         assert rel(F2.T @ (W2 * g), res) < 1e-13
+
+
+@needs_ref
+@pytest.mark.parametrize("p", [1, 2, 3, 4])
+def test_tet_mass_matrix_and_lumped_vertex_inverse_match_reference_lumpinv(p):
+    r = O.ref_tet()
+    t = TB.tables(p)
+    buf = np.zeros(4096)
+    n = r.ref_tet_get(p, b"mm", ptr(buf))
+    assert n == t.T * t.T
+    assert rel(TB.arr(t, "mm").ravel(), buf[:n]) < 1e-13
+    if p == 1:
+        assert r.ref_tet_get(p, b"vdiag", ptr(buf)) == 1
+        assert abs(t.vdiag - buf[0]) < 1e-13 * abs(buf[0])
