@@ -346,14 +346,15 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=N
         H.close()
         ln = int(round(np.log2(n)))
         hl = hlevels or (max(1, ln - 1) if n <= 32 else max(1, ln - 3))
-        # p1_minvrt: the p = 1 levels smoothed by the default build's tet_hp::minvrt at the
-        # reference's p = 1 cfl (2.2) instead of the JACOBI build's relaxation
-        cflw = {**cfl, **({1: 2.2} if p1_minvrt else {})}
+        # p1_minvrt: the p = 1 and 2 levels smoothed by the default build's tet_hp::minvrt at
+        # the reference's cfl (2.2, 1.5) instead of the JACOBI build's relaxation
+        cflw = {**cfl, **({1: 2.2, 2: 1.5} if p1_minvrt else {})}
         H = TetHierarchy(n, p, hlevels=hl, mu=1.0 / 100.0, cfl=cflw, stream=ctypes.c_void_p(cur.cuda_stream),
-                         p1_smoother=1 if p1_minvrt else 0)
+                         minvrt=p1_minvrt)
         h, sec, nc = H.solve(drop=1e-10, max_cycles=400, vw=2)
         line["multigrid_full_w_to_1e-10"] = {"levels": f"p {p}..1, then h-levels down to {n >> hl}^3 at p = 1",
-                                             "p1_smoother": "minvrt, cfl 2.2" if p1_minvrt else "jacobi, cfl 0.5",
+                                             "low_p_smoother": "minvrt (p = 1, 2; cfl 2.2, 1.5)" if p1_minvrt
+                                             else "jacobi, cfl 0.5",
                                              "seconds": sec, "cycles": nc, "drop": float(h[-1]),
                                              "reached": bool(h[-1] <= 1e-10), "ms_per_cycle": 1e3 * sec / max(nc, 1),
                                              "drop_history": [float(x) for x in h[::max(1, len(h) // 10)]]}
@@ -592,8 +593,8 @@ def main():
     ap.add_argument("--p", type=int, nargs="*", default=None, help="with --sweep: the p values")
     ap.add_argument("--arms", nargs="*", default=None,
                     help="with --sweep c3: run only these arms (e.g. fp64_level_by_level fp32_defect_correction)")
-    ap.add_argument("--tet-p1-minvrt", action="store_true",
-                    help="with --sweep c5 --tet-solve: smooth the p = 1 levels with tet_hp::minvrt (cfl 2.2)")
+    ap.add_argument("--tet-minvrt", action="store_true",
+                    help="with --sweep c5 --tet-solve: smooth the p = 1, 2 levels with tet_hp::minvrt (cfl 2.2, 1.5)")
     ap.add_argument("--tet-hlevels", type=int, default=None,
                     help="with --sweep c5 --tet-solve: h-levels of the W-cycle hierarchy (default: down to 2^3 "
                          "for n <= 32, to 8^3 above)")
@@ -650,7 +651,7 @@ def main():
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         c5_sweep(torch, dev, args.mesh if args.mesh != N_MESH else 64, (args.p or [3])[0], args.steps, args.warmup,
                  timed_factory(torch, flush), full_solve=args.tet_solve, hlevels=args.tet_hlevels,
-                 p1_minvrt=args.tet_p1_minvrt)
+                 p1_minvrt=args.tet_minvrt)
         return
 
     if args.physics == "ins":

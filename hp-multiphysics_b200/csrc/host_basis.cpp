@@ -757,6 +757,105 @@ void deriv_operator(int g, const double *d, const double (*c)[HP_TET_MAXG], doub
 
 }  // namespace
 
+// Gaussian elimination with partial pivoting: solves A x = b (A n x n, row-major, destroyed).
+static bool dense_solve(int n, std::vector<double> &A, std::vector<double> &b) {
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(A[(size_t)r * n + c]) > std::fabs(A[(size_t)piv * n + c])) piv = r;
+        if (A[(size_t)piv * n + c] == 0.0) return false;
+        if (piv != c) {
+            for (int k = 0; k < n; ++k) std::swap(A[(size_t)c * n + k], A[(size_t)piv * n + k]);
+            std::swap(b[c], b[piv]);
+        }
+        for (int r = c + 1; r < n; ++r) {
+            const double f = A[(size_t)r * n + c] / A[(size_t)c * n + c];
+            for (int k = c; k < n; ++k) A[(size_t)r * n + k] -= f * A[(size_t)c * n + k];
+            b[r] -= f * b[c];
+        }
+    }
+    for (int c = n - 1; c >= 0; --c) {
+        double acc = b[c];
+        for (int k = c + 1; k < n; ++k) acc -= A[(size_t)c * n + k] * b[k];
+        b[c] = acc / A[(size_t)c * n + c];
+    }
+    return true;
+}
+
+// The vertex part of tet_basis::lumpinv (tet_basis/initialize.cpp:642-808) for p >= 2: for
+// vertex i, the combination of vertex mode i with the higher modes that touch it (dofs) whose
+// mass products with every lower-order mode (constraints) vanish, except the unit coefficient
+// of vertex mode i. The solution of vertex 3 gives sfmv and ffmv, vertex 0's interior part
+// and sfmv give the constrained vdiag. The constraint and dof lists follow the reference's
+// orderings (vertices, edges by local index, faces, interiors); with p <= 4 both have
+// (em+1)(em+2)(em+3)/6 entries.
+static void tet_vertex_constraints(hp_tet_tables &t) {
+    const int em = t.em, fm = t.fm, im = t.im, bm = t.bm, tm = t.T;
+    std::vector<int> lind;
+    for (int i = 0; i < 4; ++i) lind.push_back(i);
+    for (int m = 0; m < 6; ++m)
+        for (int j = 4 + em * m; j < 3 + em * (m + 1); ++j) lind.push_back(j);
+    for (int m = 0; m < 4; ++m) {
+        int ind2 = 0;
+        for (int i = 1; i <= em - 1; ++i) {
+            for (int j = 1; j <= em - i - 1; ++j) lind.push_back(4 + 6 * em + fm * m + ind2++);
+            ++ind2;
+        }
+    }
+    {
+        int ind2 = 0;
+        for (int i = 1; i <= em - 1; ++i) {
+            for (int j = 1; j <= em - i - 1; ++j) {
+                for (int k = 1; k <= em - i - j - 1; ++k) lind.push_back(bm + ind2++);
+                ++ind2;
+            }
+            ++ind2;
+        }
+    }
+    auto range = [](std::vector<int> &v, int a, int b) { for (int i = a; i < b; ++i) v.push_back(i); };
+    std::vector<int> dind[4];
+    dind[0] = {0}; range(dind[0], 4 + 3 * em, 4 + 6 * em); range(dind[0], 4 + 6 * em + fm, tm);
+    dind[1] = {1}; range(dind[1], 4 + em, 4 + 4 * em); range(dind[1], 4 + 6 * em, 4 + 6 * em + fm);
+    range(dind[1], 4 + 6 * em + 2 * fm, tm);
+    dind[2] = {2}; range(dind[2], 4, 4 + em); range(dind[2], 4 + 2 * em, 4 + 3 * em);
+    range(dind[2], 4 + 4 * em, 4 + 5 * em); range(dind[2], 4 + 6 * em, 4 + 6 * em + 2 * fm);
+    range(dind[2], 4 + 6 * em + 3 * fm, tm);
+    dind[3] = {3}; range(dind[3], 4, 4 + 2 * em); range(dind[3], 4 + 5 * em, 4 + 6 * em);
+    range(dind[3], 4 + 6 * em, 4 + 6 * em + 3 * fm); range(dind[3], bm, tm);
+    const int n = (int)lind.size();
+    std::vector<double> x, ifmb0(std::max(im, 1), 0.0);
+    for (int i = 0; i < 4; ++i) {
+        if ((int)dind[i].size() != n) return;  // not square: beyond the supported p
+        std::vector<double> A((size_t)n * n), b(n, 0.0);
+        for (int j = 0; j < n; ++j)
+            for (int k = 0; k < n; ++k) A[(size_t)j * n + k] = t.mm[lind[j]][dind[i][k]];
+        for (int k = 0; k < n; ++k) A[(size_t)i * n + k] = 0.0;
+        A[(size_t)i * n] = 1.0;
+        b[i] = 1.0;
+        if (!dense_solve(n, A, b)) return;
+        if (i == 0)
+            for (int k = 0; k < im; ++k) ifmb0[k] = -b[k + 3 * em + 3 * fm + 1];
+        x = b;
+    }
+    for (int k = 0; k < em; ++k) {
+        t.sfmv[1][k] = -x[k + 1];
+        t.sfmv[0][k] = -x[k + 1 + em];
+    }
+    for (int k = 0; k < fm; ++k) {
+        t.ffmv[0][k] = 0.0;
+        t.ffmv[1][k] = -x[k + 3 * em + 1 + fm];
+        t.ffmv[2][k] = -x[k + 3 * em + 1 + 2 * fm];
+    }
+    double vd = t.mm[0][0];
+    for (int k = 0; k < em; ++k)
+        vd -= t.sfmv[1][k] * (t.mm[4 + k + 3 * em][0] + t.mm[4 + k + 4 * em][0] + t.mm[4 + k + 5 * em][0]);
+    for (int k = 0; k < fm; ++k)
+        vd -= t.ffmv[0][k] * (t.mm[4 + k + 6 * em + fm][0] + t.mm[4 + k + 6 * em + 2 * fm][0] +
+                              t.mm[4 + k + 6 * em + 3 * fm][0]);
+    for (int k = 0; k < im; ++k) vd -= ifmb0[k] * t.mm[4 + k + 6 * em + 4 * fm][0];
+    t.vdiag = 1.0 / vd;
+}
+
 extern "C" int hp_tet_basis_build(int p, hp_tet_tables *out) {
     if (!out || p < 1 || p > HP_TET_MAXP) return -1;
     hp_tet_tables &t = *out;
@@ -891,6 +990,7 @@ extern "C" int hp_tet_basis_build(int p, hp_tet_tables *out) {
             t.mm[m][k] = acc;
         }
     t.vdiag = 1.0 / (t.mm[0][0] + t.mm[0][1] + t.mm[0][2] + t.mm[0][3]);
+    if (p >= 2) tet_vertex_constraints(t);
     deriv_operator(G, t.dltx, t.dltx2, t.Ax);
     deriv_operator(G, t.dltx, t.dltx3, t.Bx);
     deriv_operator(G, t.dlty, t.dlty2, t.Ay);

@@ -631,6 +631,59 @@ __global__ void k_tet_minvrt1(long n, double *res, const double *vprcn, double v
     }
 }
 
+// tet_hp::minvrt at p = 2 (tet_hp/setup_preconditioner.cpp:16-30, 57-131, 197-221), in four
+// passes. (1) Edge modes removed from their end vertices: res.v -= sfmv(end, k) res.e.
+// The rows fixed by essential conditions were zeroed before minvrt (mask_e: the edge section).
+__global__ void k_tet_minv_e2v(int nseg, int em, const int *seg_pnt, const double *sfmv, double *resv,
+                               const double *rese, const unsigned char *mask_e) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
+        for (int k = 0; k < em; ++k)
+            for (int i = 0; i < 2; ++i) {
+                const int v = seg_pnt[2 * s + i];
+                for (int n = 0; n < NV; ++n) {
+                    const size_t e = ((size_t)s * em + k) * NV + n;
+                    if (!mask_e[e]) atomicAdd(resv + (size_t)v * NV + n, -sfmv[i * (HP_TET_MAXP - 1) + k] * rese[e]);
+                }
+            }
+}
+
+// (2) / (4) res *= (1 / prcn(entity, var)) diag on one section, fixed rows zeroed
+__global__ void k_tet_minv_scale(long n, int modes, double *res, const double *prcn, double diag,
+                                 const unsigned char *mask) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        const long ent = k / ((long)modes * NV), var = k % NV;
+        res[k] = mask[k] ? 0.0 : res[k] * ((1.0 / prcn[ent * NV + var]) * diag);
+    }
+}
+
+// (3) Vertex values (times the element diagonal iprcn) removed from the edge modes:
+// res.e(edge, k) -= sgn^k mm(j, 4 + k + i em) res.v(v_j) iprcn(tet)
+__global__ void k_tet_minv_v2e(TetMeshD m, int em, const double *mm, const double *iprcn, const double *resv,
+                               double *rese) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m.ntet; t += gridDim.x * blockDim.x) {
+        double uh[4][NV];
+        for (int j = 0; j < 4; ++j)
+            for (int n = 0; n < NV; ++n) uh[j][n] = resv[(size_t)m.tp[4 * t + j] * NV + n] * iprcn[(size_t)t * NV + n];
+        for (int i = 0; i < 6; ++i) {
+            const int sind = m.ts[6 * t + i], sg = m.tsg[6 * t + i];
+            for (int j = 0; j < 4; ++j) {
+                double msgn = 1.0;
+                for (int k = 0; k < em; ++k) {
+                    const double c = mm[j * HP_TET_MAXT + 4 + k + i * em];
+                    for (int n = 0; n < NV; ++n) atomicAdd(rese + ((size_t)sind * em + k) * NV + n, -msgn * c * uh[j][n]);
+                    msgn *= sg;
+                }
+            }
+        }
+    }
+}
+
+// ug = ug0 - ca res
+__global__ void k_tet_advance(long n, const double *res, double *u, const double *u0, double ca) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+        u[k] = u0[k] - ca * res[k];
+}
+
 __global__ void k_tet_relax(long n, double *res, const double *jd, const unsigned char *mask, double *u,
                             const double *u0, double ca) {
     for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
@@ -729,7 +782,9 @@ struct hp_tet_ctx {
     double *U0 = nullptr, *JD = nullptr, *rbar = nullptr, *part = nullptr;  // update, jacob_diag
     unsigned char *mask = nullptr;  // 1: row fixed by an essential condition
     bool jd_ready = false;
-    int smoother = 0;  // 0: JACOBI build (jacobi_relaxation), 1: minvrt (p = 1)
+    int smoother = 0;  // 0: JACOBI build (jacobi_relaxation), 1: minvrt (p <= 2)
+    int *seg_pnt = nullptr;           // [nseg][2] edge end points (global direction)
+    double *d_mm = nullptr, *d_sfmv = nullptr;  // lumpinv tables for minvrt
     bool smoother_ready() const { return smoother ? prcn_ready : jd_ready; }
     // multigrid: this level is coarser than `fine` (kind 1: p-level, 2: h-level)
     hp_tet_ctx *fine = nullptr;
@@ -966,6 +1021,25 @@ extern "C" int hp_tet_create(const hp_tet_mesh_desc *m, const hp_tet_tables *b, 
         }
         if ((r = up(pb.data(), 8 * pb.size(), (void **)&c->projB)) ||
             (r = up(ib.data(), 8 * ib.size(), (void **)&c->intB))) {
+            hp_tet_destroy(c);
+            return r;
+        }
+    }
+    {   // edge end points in the global direction (tet_sgn = +1 where the tetrahedron's local
+        // edge runs from its first to its second local vertex the same way) and lumpinv tables
+        static const int VS[6][2] = {{2, 3}, {3, 1}, {2, 1}, {1, 0}, {2, 0}, {3, 0}};
+        std::vector<int> sp(2 * (size_t)m->nseg, -1);
+        for (int t = 0; t < m->ntet; ++t)
+            for (int i = 0; i < 6; ++i) {
+                const int sidx = m->tet_seg[6 * t + i];
+                if (sidx < 0 || sidx >= m->nseg) { set_err("hp_tet_create: tet_seg out of range"); hp_tet_destroy(c); return HP_EINVAL; }
+                const int a = m->tet_pnt[4 * t + VS[i][0]], bb = m->tet_pnt[4 * t + VS[i][1]];
+                sp[2 * (size_t)sidx] = m->tet_sgn[6 * t + i] > 0 ? a : bb;
+                sp[2 * (size_t)sidx + 1] = m->tet_sgn[6 * t + i] > 0 ? bb : a;
+            }
+        if ((r = up(sp.data(), 4 * sp.size(), (void **)&c->seg_pnt)) ||
+            (r = up(&b->mm[0][0], sizeof(b->mm), (void **)&c->d_mm)) ||
+            (r = up(&b->sfmv[0][0], sizeof(b->sfmv), (void **)&c->d_sfmv))) {
             hp_tet_destroy(c);
             return r;
         }
@@ -1224,8 +1298,8 @@ extern "C" int hp_tet_set_smoother(hp_tet_ctx *c, int kind) {
         set_err("hp_tet_set_smoother: kind 0 (JACOBI build) or 1 (minvrt)");
         return HP_EINVAL;
     }
-    if (kind == 1 && c->p != 1) {
-        set_err("hp_tet_set_smoother: tet_hp::minvrt is built for p = 1 only");
+    if (kind == 1 && c->p > 2) {
+        set_err("hp_tet_set_smoother: tet_hp::minvrt is built for p = 1 and 2 only");
         return HP_EINVAL;
     }
     c->smoother = kind;
@@ -1244,10 +1318,24 @@ extern "C" int hp_tet_enqueue_update(hp_tet_ctx *c) {
         int r = hp_tet_enqueue_rsdl(c, stage);
         if (r) return r;
         const double ca = c->ph.alpha[stage] * c->ph.cfl;
-        if (c->smoother)  // p = 1: the state is the vertex section alone (ltot = lv)
+        if (c->smoother && c->p == 1)  // the state is the vertex section alone (ltot = lv)
             k_tet_minvrt1<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
                 (long)c->ltot, c->RES, c->vprcn, c->tab.vdiag, c->mask, c->U, c->U0, ca);
-        else
+        else if (c->smoother) {
+            const int g = c->nsm * 8;
+            double *rv = c->RES, *re = c->RES + c->lv;
+            k_tet_minv_e2v<<<std::min(nblk(c->mesh.nseg, 256), g), 256, 0, c->stream>>>(
+                c->mesh.nseg, c->em, c->seg_pnt, c->d_sfmv, rv, re, c->mask + c->lv);
+            k_tet_minv_scale<<<std::min(nblk((long)c->lv, 256), g), 256, 0, c->stream>>>(
+                (long)c->lv, 1, rv, c->vprcn, c->tab.vdiag, c->mask);
+            k_tet_minv_v2e<<<std::min(nblk(c->mesh.ntet, 128), g), 128, 0, c->stream>>>(
+                c->mesh, c->em, c->d_mm, c->iprcn, rv, re);
+            // p = 2: tet_hp::minvrt sets ediag(0) = 100 before scaling the edge modes
+            k_tet_minv_scale<<<std::min(nblk((long)c->le, 256), g), 256, 0, c->stream>>>(
+                (long)c->le, c->em, re, c->eprcn, 100.0, c->mask + c->lv);
+            k_tet_advance<<<std::min(nblk((long)c->ltot, 256), g), 256, 0, c->stream>>>(
+                (long)c->ltot, c->RES, c->U, c->U0, ca);
+        } else
             k_tet_relax<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
                 (long)c->ltot, c->RES, c->JD, c->mask, c->U, c->U0, ca);
     }

@@ -20,7 +20,8 @@ class TetTables(ctypes.Structure):
                 [(n, _D * MAXT * MAXQ) for n in ("F", "DX", "DY", "DZ")] +
                 [(n, _D * MAXG * MAXG) for n in ("Ax", "Bx", "Ay", "By", "Az")] +
                 [("T2", _I)] + [(n, _D * MAXT * (MAXG * MAXG)) for n in ("F2", "DX2", "DY2")] +
-                [("W2", _D * (MAXG * MAXG)), ("mm", _D * MAXT * MAXT), ("vdiag", _D)])
+                [("W2", _D * (MAXG * MAXG)), ("mm", _D * MAXT * MAXT), ("vdiag", _D),
+                 ("sfmv", _D * (MAXP - 1) * 2), ("ffmv", _D * (MAXP * (MAXP - 1) // 2) * 3)])
 
 
 def tables(p):
@@ -51,6 +52,10 @@ def arr(t, name):
         return a[:G * G]
     if name == "mm":
         return a[:T, :T]
+    if name == "sfmv":
+        return a[:, :t.em]
+    if name == "ffmv":
+        return a[:, :t.fm]
     if name in ("mx", "my", "mz", "msg"):
         return a[:T]
     if a.ndim == 2:
@@ -343,7 +348,7 @@ class TetGPU:
                "set_dirichlet")
 
     def set_smoother(self, kind):
-        """0: the JACOBI build's jacobi_relaxation; 1: tet_hp::minvrt (p = 1 only)."""
+        """0: the JACOBI build's jacobi_relaxation; 1: tet_hp::minvrt (p = 1 and 2)."""
         _check(self.lib, self.lib.hp_tet_set_smoother(self.h, kind), "set_smoother")
 
     def set_flux_faces(self, ff):
@@ -414,11 +419,11 @@ class TetHierarchy:
     log2p = p - 1 for tetrahedra; h-levels as tet_mesh coarsening). Every level takes the
     Beltrami state, the boundary layout of TetProblem.cube_boundary (inflow on all six
     faces with a balanced boundary flux; outflow=True: a neumann outflow at x = 1) and
-    `cfl[p]`; p1_smoother = 1 smooths the p = 1 levels with tet_hp::minvrt instead of the
+    `cfl[p]`; minvrt=True smooths the p = 1 and 2 levels with tet_hp::minvrt instead of the
     JACOBI build's relaxation."""
 
     def __init__(self, n, p, hlevels=2, mu=0.01, cfl=None, re=100.0, noise=1e-3, stream=None, fadd=1.0,
-                 outflow=False, p1_smoother=0):
+                 outflow=False, minvrt=False):
         import torch
         from .tetmesh import cube_tets
         cfl = cfl or {1: 2.2, 2: 1.5, 3: 1.0, 4: 0.5}
@@ -434,8 +439,8 @@ class TetHierarchy:
             g = TetGPU(pr, stream=stream)
             g.set_dirichlet(masks)
             g.set_flux_faces(ff)
-            if q == 1 and p1_smoother:
-                g.set_smoother(p1_smoother)
+            if q <= 2 and minvrt:
+                g.set_smoother(1)
             self.probs.append(pr)
             self.masks.append(masks)
             self.levels.append(g)

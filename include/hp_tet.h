@@ -66,12 +66,14 @@ typedef struct hp_tet_tables {
     int T2;
     double F2[HP_TET_MAXG * HP_TET_MAXG][HP_TET_MAXT], DX2[HP_TET_MAXG * HP_TET_MAXG][HP_TET_MAXT];
     double DY2[HP_TET_MAXG * HP_TET_MAXG][HP_TET_MAXT], W2[HP_TET_MAXG * HP_TET_MAXG];
-    /* tet_basis::lumpinv (tet_basis/initialize.cpp:521-639): the mass matrix
-     * mm(m, k) = sum_q w F(q,m) F(q,k), and vdiag = 1 / (mm(0,0) + mm(0,1) + mm(0,2) + mm(0,3)),
-     * the lumped vertex mass inverse, which is tet_basis::vdiag at p = 1 (at p >= 2 lumpinv
-     * replaces it by a constrained value that is not built). */
+    /* tet_basis::lumpinv (tet_basis/initialize.cpp:521-808): the mass matrix
+     * mm(m, k) = sum_q w F(q,m) F(q,k); at p = 1 vdiag = 1 / (mm(0,0) + ... + mm(0,3)), the
+     * lumped vertex mass inverse; at p >= 2 the vertex constraint systems give sfmv [end][k]
+     * (edge mode k removed from the vertex at edge end 0 / 1), ffmv [i][k] (face modes) and
+     * the constrained vdiag. */
     double mm[HP_TET_MAXT][HP_TET_MAXT];
     double vdiag;
+    double sfmv[2][HP_TET_MAXP - 1], ffmv[3][HP_TET_MAXP * (HP_TET_MAXP - 1) / 2];
 } hp_tet_tables;
 
 /* Builds the tables for 1 <= p <= 4. Returns 0, or -1 for an unsupported p. */

@@ -539,10 +539,54 @@ static void minvrt_p1(OT &o) {
     all_dirichlet(o);
 }
 
-// 0: the JACOBI build's smoother, 1: minvrt (p = 1 only; -1 otherwise)
+// tet_hp::minvrt at p = 2 (setup_preconditioner.cpp:16-30, 57-131, 197-221): edge modes
+// removed from their end vertices with sfmv, the vertex rows scaled by vdiag / vprcn and
+// fixed, the vertex values times the element diagonal removed from the edge modes with the
+// mass matrix, the edge rows scaled by ediag(0) / eprcn (minvrt sets ediag(0) = 100 at p = 2)
+// and fixed.
+static void minvrt_p2(OT &o) {
+    const hp_tet_tables &t = o.t;
+    const int em = t.em;
+    static const int VS[6][2] = {{2, 3}, {3, 1}, {2, 1}, {1, 0}, {2, 0}, {3, 0}};
+    std::vector<int> sp(2 * (size_t)o.nseg);
+    for (int tind = 0; tind < o.ntet; ++tind)
+        for (int i = 0; i < 6; ++i) {
+            const int s = o.ts[6 * tind + i], a = o.tp[4 * tind + VS[i][0]], b = o.tp[4 * tind + VS[i][1]];
+            sp[2 * (size_t)s] = o.tsg[6 * tind + i] > 0 ? a : b;
+            sp[2 * (size_t)s + 1] = o.tsg[6 * tind + i] > 0 ? b : a;
+        }
+    for (int s = 0; s < o.nseg; ++s)
+        for (int k = 0; k < em; ++k)
+            for (int i = 0; i < 2; ++i)
+                for (int n = 0; n < NV; ++n)
+                    o.rv[(size_t)sp[2 * s + i] * NV + n] -= t.sfmv[i][k] * o.re[((size_t)s * em + k) * NV + n];
+    for (size_t k = 0; k < o.rv.size(); ++k) o.rv[k] *= (1.0 / o.vprcn[k]) * t.vdiag;
+    all_dirichlet(o);
+    for (int tind = 0; tind < o.ntet; ++tind) {
+        double uh[4][NV];
+        for (int j = 0; j < 4; ++j)
+            for (int n = 0; n < NV; ++n) uh[j][n] = o.rv[(size_t)o.tp[4 * tind + j] * NV + n] * o.iprcn[(size_t)tind * NV + n];
+        for (int i = 0; i < 6; ++i) {
+            const int s = o.ts[6 * tind + i], sg = o.tsg[6 * tind + i];
+            for (int j = 0; j < 4; ++j) {
+                double msgn = 1.0;
+                for (int k = 0; k < em; ++k) {
+                    for (int n = 0; n < NV; ++n)
+                        o.re[((size_t)s * em + k) * NV + n] -= msgn * t.mm[j][4 + k + i * em] * uh[j][n];
+                    msgn *= sg;
+                }
+            }
+        }
+    }
+    for (int s = 0; s < o.nseg; ++s)
+        for (int n = 0; n < NV; ++n) o.re[((size_t)s * em) * NV + n] *= (1.0 / o.eprcn[(size_t)s * NV + n]) * 100.0;
+    all_dirichlet(o);
+}
+
+// 0: the JACOBI build's smoother, 1: minvrt (p = 1 and 2; -1 otherwise)
 int ot_set_smoother(void *h, int kind) {
     OT &o = *static_cast<OT *>(h);
-    if (kind != 0 && (kind != 1 || o.t.p != 1)) return -1;
+    if (kind != 0 && (kind != 1 || o.t.p > 2)) return -1;
     o.smoother = kind;
     return 0;
 }
@@ -558,8 +602,12 @@ void ot_update(void *h) {
     for (int stage = 0; stage < o.ph.nstage; ++stage) {
         ot_rsdl(h, stage);
         all_dirichlet(o);
-        if (o.smoother) minvrt_p1(o);
-        else jacobi_relaxation(o);
+        if (o.smoother) {
+            if (o.t.p == 1) minvrt_p1(o);
+            else minvrt_p2(o);
+        } else {
+            jacobi_relaxation(o);
+        }
         const double ca = o.ph.alpha[stage] * o.ph.cfl;
         for (size_t k = 0; k < o.ugv.size(); ++k) o.ugv[k] = o.u0v[k] - ca * o.rv[k];
         for (size_t k = 0; k < o.uge.size(); ++k) o.uge[k] = o.u0e[k] - ca * o.re[k];

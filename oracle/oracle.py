@@ -247,7 +247,7 @@ class OracleTet:
 
     def set_smoother(self, kind):
         if lib().ot_set_smoother(self.h, kind) != 0:
-            raise ValueError("minvrt is restated for p = 1 only")
+            raise ValueError("minvrt is restated for p = 1 and 2 only")
 
     def jacobian_diagonal(self):
         lib().ot_jacobian_diagonal(self.h)

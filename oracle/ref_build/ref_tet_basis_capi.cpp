@@ -83,6 +83,8 @@ int ref_tet_get(int p, const char *name, double *out) {
     else if (n == "dltz2") { T2(g, g, i == j ? 0.0 : b->dltz2(i, j)) }
     else if (n == "mm") { T2(b->tm, b->tm, b->mm(i, j)) }
     else if (n == "vdiag") { T1(1, b->vdiag) }
+    else if (n == "sfmv") { T2(2, b->em, b->sfmv(i, j)) }
+    else if (n == "ffmv") { T2(3, b->fm, b->ffmv(i, j)) }
     else return -1;
 #undef T1
 #undef T2

@@ -142,10 +142,12 @@ def test_tet_multigrid_reduces_residual_and_keeps_essential_values():
     H.close()
 
 
-def test_tet_minvrt_p1_updates_match_oracle():
-    """tet_hp::update with tet_hp::minvrt at p = 1 (res.v *= vdiag / vprcn), face fluxes and
-    essential rows, at the reference's p = 1 cfl 2.2."""
-    pr = TetProblem(cube_tets(3), 1, mu=0.01, cfl=2.2).set_beltrami()
+@pytest.mark.parametrize("p,cfl", [(1, 2.2), (2, 1.5)])
+def test_tet_minvrt_updates_match_oracle(p, cfl):
+    """tet_hp::update with tet_hp::minvrt (p = 1: res.v *= vdiag / vprcn; p = 2: also the
+    edge / vertex removals and the edge scaling), face fluxes and essential rows, at the
+    reference's default cfl for that p."""
+    pr = TetProblem(cube_tets(3), p, mu=0.01, cfl=cfl).set_beltrami()
     masks, ff = pr.cube_boundary()
     g, o = TetGPU(pr), OracleTet(pr)
     for x in (g, o):
@@ -160,17 +162,17 @@ def test_tet_minvrt_p1_updates_match_oracle():
     g.close()
 
 
-def test_tet_set_smoother_minvrt_needs_p1():
-    pr = TetProblem(cube_tets(2), 2, mu=0.01).set_beltrami()
+def test_tet_set_smoother_minvrt_needs_p_at_most_2():
+    pr = TetProblem(cube_tets(2), 3, mu=0.01).set_beltrami()
     g = TetGPU(pr)
-    with pytest.raises(RuntimeError, match="p = 1"):
+    with pytest.raises(RuntimeError, match="p = 1 and 2"):
         g.set_smoother(1)
     g.close()
 
 
-def test_tet_multigrid_with_minvrt_on_p1_levels_reduces_residual():
+def test_tet_multigrid_with_minvrt_on_low_p_levels_reduces_residual():
     from hpb.tet import TetHierarchy
-    H = TetHierarchy(8, 3, hlevels=2, mu=0.01, cfl={1: 2.2, 2: 0.5, 3: 0.5}, p1_smoother=1)
+    H = TetHierarchy(8, 3, hlevels=2, mu=0.01, cfl={1: 2.2, 2: 1.5, 3: 0.5}, minvrt=True)
     hist, sec, cycles = H.solve(drop=1e-10, max_cycles=30, vw=2)
     assert np.all(np.isfinite(hist)) and hist[-1] < 1e-2
     H.close()

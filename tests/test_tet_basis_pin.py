@@ -102,6 +102,13 @@ def test_tet_mass_matrix_and_lumped_vertex_inverse_match_reference_lumpinv(p):
     n = r.ref_tet_get(p, b"mm", ptr(buf))
     assert n == t.T * t.T
     assert rel(TB.arr(t, "mm").ravel(), buf[:n]) < 1e-13
-    if p == 1:
-        assert r.ref_tet_get(p, b"vdiag", ptr(buf)) == 1
-        assert abs(t.vdiag - buf[0]) < 1e-13 * abs(buf[0])
+    assert r.ref_tet_get(p, b"vdiag", ptr(buf)) == 1
+    assert abs(t.vdiag - buf[0]) < 1e-11 * abs(buf[0])
+    if p >= 2:
+        n = r.ref_tet_get(p, b"sfmv", ptr(buf))
+        assert n == 2 * t.em
+        assert rel(TB.arr(t, "sfmv").ravel(), buf[:n]) < 1e-11
+    if p >= 3:
+        n = r.ref_tet_get(p, b"ffmv", ptr(buf))
+        assert n == 3 * t.fm
+        assert rel(TB.arr(t, "ffmv").ravel(), buf[:n]) < 1e-11

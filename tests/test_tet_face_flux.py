@@ -138,7 +138,7 @@ def test_balanced_inflow_makes_the_continuity_rows_consistent(p):
         assert abs(rv.sum()) < 1e-13 * np.abs(rv).sum()
 
 
-def test_oracle_minvrt_p1_smoother_converges_and_is_p1_only():
+def test_oracle_minvrt_p1_smoother_converges_and_is_limited_to_low_p():
     """tet_hp::minvrt at p = 1 (the default build's smoother) in the oracle: 200 updates at the
     reference's p = 1 cfl (2.2) reduce the residual by more than 1e4 on a 3^3 x 6 cube."""
     pr = TB.TetProblem(cube_tets(3), 1, mu=0.01, cfl=2.2).set_beltrami()
@@ -158,4 +158,26 @@ def test_oracle_minvrt_p1_smoother_converges_and_is_p1_only():
         o.update()
     assert norm() < 1e-4 * r0
     with pytest.raises(ValueError):
-        O.OracleTet(TB.TetProblem(cube_tets(1), 2, mu=0.01).set_beltrami()).set_smoother(1)
+        O.OracleTet(TB.TetProblem(cube_tets(1), 3, mu=0.01).set_beltrami()).set_smoother(1)
+
+
+def test_oracle_minvrt_p2_smoother_converges():
+    """tet_hp::minvrt at p = 2 in the oracle at the reference's p = 2 cfl (1.5): 200 updates
+    reduce the residual of the free vertex and edge rows by more than 100."""
+    pr = TB.TetProblem(cube_tets(3), 2, mu=0.01, cfl=1.5).set_beltrami()
+    masks, ff = pr.cube_boundary()
+    o = O.OracleTet(pr)
+    o.set_dirichlet(masks)
+    o.set_flux_faces(ff)
+    o.set_smoother(1)
+    assert o.setup_preconditioner() == 0
+    fv, fe = masks[0] == 0, (masks[1] == 0)[:, None, :]
+
+    def norm():
+        o.rsdl(pr.phys.nstage)
+        r = o.residual()
+        return np.sqrt(np.sum(np.where(fv, r[0], 0.0) ** 2) + np.sum(np.where(fe, r[1], 0.0) ** 2))
+    r0 = norm()
+    for _ in range(200):
+        o.update()
+    assert norm() < 1e-2 * r0
