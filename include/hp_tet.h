@@ -119,9 +119,11 @@ const char *hp_tet_last_error(void);
 
 /* The smoother of hp_tet_update, hp_tet_solve and hp_tet_solve_mg: kind 0 = the JACOBI
  * build (jacobian_diagonal + jacobi_relaxation, tet_hp/jacobi.cpp:14-111; the default);
- * kind 1 = the default build's tet_hp::minvrt (tet_hp/setup_preconditioner.cpp:11-74 with
- * the inversion of tet_hp::setup_preconditioner, :428-460), built for p = 1, where it is
- * res.v *= vdiag / vprcn on the rows no essential condition fixes. kind 1 at p > 1 returns
+ * kind 1 = the default build's tet_hp::minvrt (tet_hp/setup_preconditioner.cpp:11-221 with
+ * the inversion of tet_hp::setup_preconditioner, :428-470), built for p = 1 (res.v *= vdiag /
+ * vprcn) and p = 2 (edge modes removed from the vertices with sfmv, vertex scaling, vertex
+ * values times the element diagonal removed from the edge modes with mm, edge scaling by
+ * 100 / eprcn), with the rows no essential condition fixes. kind 1 at p > 2 returns
  * HP_EINVAL. */
 int hp_tet_set_smoother(hp_tet_ctx *ctx, int kind);
 /* Rows fixed by essential conditions (bdry_ins::inflow on boundary faces,
