@@ -126,6 +126,57 @@ class TetMesh:
         return verts, edges, np.unique(faces)
 
 
+def read_msh(path):
+    """Reads a Gmsh 2.x ASCII mesh (the format of the reference's tet test meshes, which it
+    reads through MAdLib): $Nodes 'id x y z', $Elements 'id type ntags tags... nodes' with
+    type 4 = tetrahedron and type 2 = boundary triangle. Returns (TetMesh, groups), groups
+    {elementary entity id (the second tag, the id the reference's input keys b0_f<id>
+    name): array of global face indices}."""
+    with open(path) as f:
+        lines = [ln.strip() for ln in f]
+    k = 0
+    nodes, tets, tris = {}, [], []
+    while k < len(lines):
+        if lines[k] == "$Nodes":
+            n = int(lines[k + 1])
+            for ln in lines[k + 2:k + 2 + n]:
+                a = ln.split()
+                nodes[int(a[0])] = (float(a[1]), float(a[2]), float(a[3]))
+            k += n + 2
+        elif lines[k] == "$Elements":
+            n = int(lines[k + 1])
+            for ln in lines[k + 2:k + 2 + n]:
+                a = [int(x) for x in ln.split()]
+                typ, nt = a[1], a[2]
+                tags, vs = a[3:3 + nt], a[3 + nt:]
+                if typ == 4:
+                    tets.append(vs[:4])
+                elif typ == 2:
+                    tris.append((tags[1] if nt > 1 else tags[0], vs[:3]))
+            k += n + 2
+        else:
+            k += 1
+    if not tets:
+        raise ValueError(f"{path}: no tetrahedra (type 4 elements)")
+    ids = sorted(nodes)
+    index = {nid: i for i, nid in enumerate(ids)}
+    pnts = np.array([nodes[i] for i in ids])
+    mesh = TetMesh(pnts, np.array([[index[v] for v in t] for t in tets]))
+    fk = np.sort(mesh.tri_pnt.astype(np.int64), axis=1)
+    n = mesh.npnt
+    fkey = (fk[:, 0] * n + fk[:, 1]) * n + fk[:, 2]
+    order = np.argsort(fkey)
+    groups = {}
+    for ent, vs in tris:
+        t = sorted(index[v] for v in vs)
+        key = (t[0] * n + t[1]) * n + t[2]
+        pos = order[np.searchsorted(fkey, key, sorter=order)]
+        if fkey[pos] != key:
+            raise ValueError("boundary triangle is not a face of the mesh")
+        groups.setdefault(ent, []).append(pos)
+    return mesh, {g: np.array(v, dtype=np.int32) for g, v in groups.items()}
+
+
 def cube_tets(n, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0)):
     """[lo, hi] box, n^3 hexahedra x 6 tetrahedra around each main diagonal."""
     g = [np.linspace(lo[d], hi[d], n + 1) for d in range(3)]

@@ -176,3 +176,29 @@ def test_tet_multigrid_with_minvrt_on_low_p_levels_reduces_residual():
     hist, sec, cycles = H.solve(drop=1e-10, max_cycles=30, vw=2)
     assert np.all(np.isfinite(hist)) and hist[-1] < 1e-2
     H.close()
+
+
+@pytest.mark.parametrize("p", [2, 3])
+def test_tet_rsdl_and_minvrt_on_a_scrambled_mesh_match_oracle(p):
+    """Residual with face fluxes (and, at p = 2, minvrt updates) on a cube whose interior
+    vertices are jittered and whose vertices are renumbered at random."""
+    from test_tet_face_flux import scrambled_cube
+    pr = TetProblem(scrambled_cube(3, 11), p, mu=0.01, cfl=1.5 if p == 2 else 0.5).set_beltrami()
+    masks, ff = pr.cube_boundary(outflow=True)
+    g, o = TetGPU(pr), OracleTet(pr)
+    for x in (g, o):
+        x.set_dirichlet(masks)
+        x.set_flux_faces(ff)
+        assert x.setup_preconditioner() == 0
+    for stage in (pr.phys.nstage, 0):
+        g.rsdl(stage)
+        o.rsdl(stage)
+        assert relerr(g.residual(), o.residual()) < 1e-12
+    if p == 2:
+        for x in (g, o):
+            x.set_smoother(1)
+        for _ in range(3):
+            g.update()
+            o.update()
+        assert relerr(g.state(), o.state()) < 1e-11
+    g.close()

@@ -9,9 +9,29 @@ quadratures are exact for these degrees, so the two agree to rounding only if th
 import numpy as np
 import pytest
 
+import os
+
 from hpb import tet as TB
-from hpb.tetmesh import cube_tets
+from hpb.tetmesh import TetMesh, cube_tets, read_msh
 from oracle import oracle as O
+
+REF_MSH = "/root/reference/Testing/tet_hp/cd/Multigrid/Inputs/tet{}.msh"
+
+
+def scrambled_cube(n, seed):
+    """cube_tets(n) with the interior vertices jittered by up to 0.2 of a cell and every
+    vertex renumbered at random, so the tetrahedra take all kinds of local orientation."""
+    c = cube_tets(n)
+    rng = np.random.default_rng(seed)
+    pts = c.pnts.copy()
+    inner = np.all((pts > 1e-12) & (pts < 1 - 1e-12), axis=1)
+    pts[inner] += rng.uniform(-0.2, 0.2, (inner.sum(), 3)) / n
+    perm = rng.permutation(c.npnt)
+    newp = np.empty_like(pts)
+    newp[perm] = pts
+    tets = perm[c.tet_pnt]
+    tets = tets[rng.permutation(len(tets))]
+    return TetMesh(newp, tets)
 
 
 def test_face_edges_match_brute_force():
@@ -181,3 +201,44 @@ def test_oracle_minvrt_p2_smoother_converges():
     for _ in range(200):
         o.update()
     assert norm() < 1e-2 * r0
+
+
+def _div_check(mesh, p, seed):
+    pr = TB.TetProblem(mesh, p, rho=1.0, mu=0.01).set_beltrami(noise=0.0)
+    rng = np.random.default_rng(seed)
+    for a in pr.state:
+        a[:] = rng.uniform(-1, 1, a.shape)
+    div, vol = volume_divergence(pr)
+    assert abs(vol - 1.0) < 1e-12
+    ff = pr.flux_faces(mesh.boundary_faces())
+    assert abs(pr.boundary_flux(ff) - div) < 1e-11 * max(1.0, abs(div))
+    with_f, without = O.OracleTet(pr), O.OracleTet(pr)
+    with_f.set_flux_faces(ff)
+    with_f.rsdl(0)
+    without.rsdl(0)
+    flux = with_f.residual()[0][:, 3] - without.residual()[0][:, 3]
+    assert abs(flux.sum() - div) < 1e-11 * max(1.0, abs(div))
+
+
+@pytest.mark.parametrize("p", [2, 3, 4])
+def test_divergence_theorem_on_a_scrambled_mesh(p):
+    """The face gather, face-edge signs and normals on tetrahedra of every local orientation."""
+    _div_check(scrambled_cube(2, 7), p, 70 + p)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_MSH.format(4)), reason="reference meshes absent")
+def test_reference_gmsh_meshes_read_and_satisfy_the_divergence_theorem():
+    """The reference's own tet test meshes (Testing/tet_hp/cd/Multigrid/Inputs/tet{2,4,8}.msh):
+    unit volume, six boundary groups (the input's b0_f<id> keys) that cover the boundary faces,
+    each on one face of the cube; and the face flux of a random p = 3 state on tet4.msh."""
+    for n in (2, 4, 8):
+        m, groups = read_msh(REF_MSH.format(n))
+        assert m.ntet == 6 * n ** 3 and abs(m.vol.sum() / 6 - 1.0) < 1e-12
+        assert sorted(groups) == [5, 14, 18, 22, 26, 27]
+        assert np.array_equal(np.sort(np.concatenate(list(groups.values()))), np.sort(m.boundary_faces()))
+        for faces in groups.values():
+            x = m.pnts[m.tri_pnt[faces]].reshape(-1, 3)
+            assert np.any(np.ptp(x, axis=0) < 1e-9)
+    with pytest.raises(ValueError):
+        read_msh(REF_MSH.format(1))                  # a 2D square: no tetrahedra
+    _div_check(read_msh(REF_MSH.format(4))[0], 3, 90)
