@@ -200,6 +200,36 @@ class TetProblem:
         self.ugv[v, 0] -= 1.0 + f0 / (f1 - f0)
         return self.boundary_flux(ff)
 
+    def group_boundary(self, groups, inflow, outflow=(), pressure=None, balance=True):
+        """Boundary layout from named face groups (hpb.tetmesh.read_msh: the reference's
+        b0_f<id>_hp_type keys): `inflow` / `outflow` are lists of group ids (inflow: velocity
+        essential and the continuity flux; outflow: the neumann flux with `pressure(x, y, z)`
+        imposed). With no outflow group and balance=True the state's boundary flux is balanced
+        to zero on the vertices of the first inflow group, which must be planar. Call before
+        the state is uploaded. Returns (essential masks, flux faces)."""
+        inf = np.concatenate([groups[g] for g in inflow]).astype(np.int32)
+        out = (np.concatenate([groups[g] for g in outflow]).astype(np.int32) if len(outflow)
+               else np.zeros(0, np.int32))
+        ff = self.flux_faces(inf, out, pressure)
+        if not len(out) and balance:
+            self._balance_on(ff, groups[inflow[0]])
+        return self.dirichlet_masks(inf), ff
+
+    def _balance_on(self, ff, faces):
+        """Shift the velocity at the vertices of `faces` (a planar group) along its normal so
+        that the boundary flux of ff is zero; those vertices' normal velocity enters only that
+        group's flux when the neighbouring groups are orthogonal planes."""
+        m = self.mesh
+        X = m.pnts[m.tri_pnt[faces[0]]]
+        nrm = np.cross(X[1] - X[0], X[2] - X[0])
+        nrm /= np.linalg.norm(nrm)
+        v = np.unique(m.tri_pnt[faces].ravel())
+        f0 = self.boundary_flux(ff)
+        self.ugv[v, :3] += nrm
+        f1 = self.boundary_flux(ff)
+        self.ugv[v, :3] -= (1.0 + f0 / (f1 - f0)) * nrm
+        return self.boundary_flux(ff)
+
     def cube_boundary(self, re=100.0, outflow=False):
         """Unit-cube boundary layouts built from the reference's face types. outflow=False:
         inflow (velocity essential, continuity flux) on all six faces, with the state's

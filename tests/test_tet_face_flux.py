@@ -242,3 +242,15 @@ def test_reference_gmsh_meshes_read_and_satisfy_the_divergence_theorem():
     with pytest.raises(ValueError):
         read_msh(REF_MSH.format(1))                  # a 2D square: no tetrahedra
     _div_check(read_msh(REF_MSH.format(4))[0], 3, 90)
+    # inflow on every group by id, boundary flux balanced: the continuity rows are consistent
+    m, groups = read_msh(REF_MSH.format(2))
+    pr = TB.TetProblem(m, 2, mu=0.01).set_beltrami()
+    masks, ff = pr.group_boundary(groups, inflow=sorted(groups))
+    assert abs(pr.boundary_flux(ff)) < 1e-14
+    assert masks[0][:, :3].sum() == 3 * len(np.unique(m.tri_pnt[m.boundary_faces()]))
+    o = O.OracleTet(pr)
+    o.set_flux_faces(ff)
+    assert o.setup_preconditioner() == 0
+    o.rsdl(0)
+    rv = o.residual()[0][:, 3]
+    assert abs(rv.sum()) < 1e-13 * np.abs(rv).sum()
