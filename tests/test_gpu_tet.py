@@ -202,3 +202,31 @@ def test_tet_rsdl_and_minvrt_on_a_scrambled_mesh_match_oracle(p):
             o.update()
         assert relerr(g.state(), o.state()) < 1e-11
     g.close()
+
+
+@pytest.mark.parametrize("p,case,mesh", [(2, "shear", "scrambled"), (4, 1, "cube")])
+def test_tet_exact_steady_solutions_have_zero_residual_on_gpu(p, case, mesh):
+    """The known-answer test of tests/test_tet_face_flux.py on the GPU residual: the
+    interpolant of an exact steady solution has a zero residual on every free row."""
+    from test_tet_face_flux import modal_interpolant, poiseuille, scrambled_cube, shear
+    msh = cube_tets(2) if mesh == "cube" else scrambled_cube(2, 5)
+    pr = TetProblem(msh, p, mu=0.05).set_beltrami(noise=0.0)
+    modal_interpolant(pr, shear if case == "shear" else poiseuille(case, 0.05))
+    ff = pr.flux_faces(msh.boundary_faces())
+    mk = pr.dirichlet_masks(msh.boundary_faces())
+
+    def free_max(state):
+        g = TetGPU(pr)
+        g.upload(*state)
+        g.set_flux_faces(ff)
+        assert g.setup_preconditioner() == 0
+        g.rsdl(pr.phys.nstage)
+        r = g.residual()
+        g.close()
+        parts = [np.where(mk[0], 0.0, r[0]).ravel(), np.where(mk[1][:, None, :], 0.0, r[1]).ravel(), r[3].ravel()]
+        if r[2].size:
+            parts.append(np.where(mk[2][:, None, :], 0.0, r[2]).ravel())
+        return np.max(np.abs(np.concatenate(parts)))
+    rng = np.random.default_rng(3)
+    pert = [a + 1e-3 * rng.uniform(-1, 1, a.shape) for a in pr.state]
+    assert free_max(pr.state) < 1e-9 * free_max(pert)
