@@ -782,6 +782,48 @@ static bool dense_solve(int n, std::vector<double> &A, std::vector<double> &b) {
     return true;
 }
 
+// The edge part of tet_basis::lumpinv at p = 3 (tet_basis/initialize.cpp:846-1040): for edge i
+// and each side of it, its second mode and the adjacent face modes (dofs) combine with its
+// first mode so that the mass products with the first modes of three edges of its cone
+// (constraints, the reference's edgecone table, 1-based edge numbers) vanish. The face
+// coefficients of edges 0..2 give ffms; the last system's edge coefficient gives sfms(0), and
+// mdiag / odiag are the first-mode mass of the combination against edge modes 0 and 2.
+static void tet_edge_cones(hp_tet_tables &t) {
+    const int em = t.em, fm = t.fm;  // 2, 1
+    static const int cone[6][3][2] = {{{2, 3}, {4, 4}, {6, 5}}, {{3, 1}, {4, 5}, {5, 6}}, {{2, 1}, {4, 5}, {6, 6}},
+                                      {{1, 1}, {5, 2}, {6, 3}}, {{2, 1}, {4, 2}, {6, 3}}, {{3, 1}, {4, 2}, {5, 3}}};
+    const int f0 = 4 + 6 * em;
+    const int dind[6][3] = {{5, f0, f0 + fm},          {5 + em, f0, f0 + 2 * fm},     {5 + 2 * em, f0, f0 + 3 * fm},
+                            {5 + 3 * em, f0 + 2 * fm, f0 + 3 * fm}, {5 + 4 * em, f0 + fm, f0 + 3 * fm},
+                            {5 + 5 * em, f0 + fm, f0 + 2 * fm}};
+    std::vector<double> x(3);
+    for (int side = 0; side < 2; ++side)
+        for (int i = 0; i < 6; ++i) {
+            int lind[3];
+            for (int j = 0; j < 3; ++j) lind[j] = 4 + (cone[i][j][side] - 1) * em;
+            std::vector<double> A(9);
+            for (int j = 0; j < 3; ++j) {
+                for (int k = 0; k < 3; ++k) A[j * 3 + k] = t.mm[lind[j]][dind[i][k]];
+                x[j] = -t.mm[lind[j]][4 + i * em];
+            }
+            if (!dense_solve(3, A, x)) return;
+            if (i < 3)
+                for (int k = 0; k < fm; ++k) t.ffms[i][k][side] = x[k + em - 1];
+        }
+    t.sfms0 = -x[0];
+    const int omode = 8;
+    t.mdiag = t.mm[4][4];
+    t.odiag = t.mm[4][omode];
+    for (int k = 1; k < em; ++k) {
+        t.mdiag += t.sfms0 * t.mm[4 + k][4];
+        t.odiag += t.sfms0 * t.mm[4 + k][omode];
+    }
+    for (int k = 0; k < fm; ++k) {
+        t.mdiag += t.ffms[0][k][0] * (t.mm[4 + k + 6 * em][4] + t.mm[4 + k + 6 * em + fm][4]);
+        t.odiag += t.ffms[0][k][0] * (t.mm[4 + k + 6 * em][omode] + t.mm[4 + k + 6 * em + fm][omode]);
+    }
+}
+
 // The vertex part of tet_basis::lumpinv (tet_basis/initialize.cpp:642-808) for p >= 2: for
 // vertex i, the combination of vertex mode i with the higher modes that touch it (dofs) whose
 // mass products with every lower-order mode (constraints) vanish, except the unit coefficient
@@ -991,6 +1033,7 @@ extern "C" int hp_tet_basis_build(int p, hp_tet_tables *out) {
         }
     t.vdiag = 1.0 / (t.mm[0][0] + t.mm[0][1] + t.mm[0][2] + t.mm[0][3]);
     if (p >= 2) tet_vertex_constraints(t);
+    if (p == 3) tet_edge_cones(t);
     deriv_operator(G, t.dltx, t.dltx2, t.Ax);
     deriv_operator(G, t.dltx, t.dltx3, t.Bx);
     deriv_operator(G, t.dlty, t.dlty2, t.Ay);

@@ -21,7 +21,8 @@ class TetTables(ctypes.Structure):
                 [(n, _D * MAXG * MAXG) for n in ("Ax", "Bx", "Ay", "By", "Az")] +
                 [("T2", _I)] + [(n, _D * MAXT * (MAXG * MAXG)) for n in ("F2", "DX2", "DY2")] +
                 [("W2", _D * (MAXG * MAXG)), ("mm", _D * MAXT * MAXT), ("vdiag", _D),
-                 ("sfmv", _D * (MAXP - 1) * 2), ("ffmv", _D * (MAXP * (MAXP - 1) // 2) * 3)])
+                 ("sfmv", _D * (MAXP - 1) * 2), ("ffmv", _D * (MAXP * (MAXP - 1) // 2) * 3),
+                 ("ffms", _D * 2 * (MAXP * (MAXP - 1) // 2) * 3), ("sfms0", _D), ("mdiag", _D), ("odiag", _D)])
 
 
 def tables(p):
@@ -56,6 +57,8 @@ def arr(t, name):
         return a[:, :t.em]
     if name == "ffmv":
         return a[:, :t.fm]
+    if name == "ffms":
+        return a[:, :t.fm, :]
     if name in ("mx", "my", "mz", "msg"):
         return a[:T]
     if a.ndim == 2:

@@ -74,6 +74,11 @@ typedef struct hp_tet_tables {
     double mm[HP_TET_MAXT][HP_TET_MAXT];
     double vdiag;
     double sfmv[2][HP_TET_MAXP - 1], ffmv[3][HP_TET_MAXP * (HP_TET_MAXP - 1) / 2];
+    /* p = 3 only (lumpinv's edge-cone systems, tet_basis/initialize.cpp:846-1040, the tables of
+     * minvrt's vertex-ball edge solve): ffms [face i < 3][k][side], sfms0 = sfms(0), and the
+     * spoke mass coefficients mdiag / odiag; zero at other p. */
+    double ffms[3][HP_TET_MAXP * (HP_TET_MAXP - 1) / 2][2];
+    double sfms0, mdiag, odiag;
 } hp_tet_tables;
 
 /* Builds the tables for 1 <= p <= 4. Returns 0, or -1 for an unsupported p. */

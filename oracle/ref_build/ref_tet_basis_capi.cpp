@@ -85,6 +85,10 @@ int ref_tet_get(int p, const char *name, double *out) {
     else if (n == "vdiag") { T1(1, b->vdiag) }
     else if (n == "sfmv") { T2(2, b->em, b->sfmv(i, j)) }
     else if (n == "ffmv") { T2(3, b->fm, b->ffmv(i, j)) }
+    else if (n == "ffms") { for (int i = 0; i < 3; ++i) for (int k = 0; k < b->fm; ++k) for (int sd = 0; sd < 2; ++sd) out[c++] = b->ffms(i, k, sd); }
+    else if (n == "sfms") { T1(1, b->sfms(0)) }
+    else if (n == "mdiag") { T1(1, b->mdiag) }
+    else if (n == "odiag") { T1(1, b->odiag) }
     else return -1;
 #undef T1
 #undef T2

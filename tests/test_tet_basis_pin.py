@@ -112,3 +112,18 @@ def test_tet_mass_matrix_and_lumped_vertex_inverse_match_reference_lumpinv(p):
         n = r.ref_tet_get(p, b"ffmv", ptr(buf))
         assert n == 3 * t.fm
         assert rel(TB.arr(t, "ffmv").ravel(), buf[:n]) < 1e-11
+
+
+@needs_ref
+def test_tet_edge_cone_tables_match_reference_lumpinv():
+    """p = 3: ffms, sfms(0), mdiag and odiag of lumpinv's edge-cone systems (the tables of
+    tet_hp::minvrt's vertex-ball edge solve and of tet_hp::spoke)."""
+    r = O.ref_tet()
+    t = TB.tables(3)
+    buf = np.zeros(64)
+    n = r.ref_tet_get(3, b"ffms", ptr(buf))
+    assert n == 3 * t.fm * 2
+    assert rel(TB.arr(t, "ffms").ravel(), buf[:n]) < 1e-11
+    for name in ("sfms0", "mdiag", "odiag"):
+        assert r.ref_tet_get(3, (b"sfms" if name == "sfms0" else name.encode()), ptr(buf)) == 1
+        assert abs(getattr(t, name) - buf[0]) < 1e-11 * abs(buf[0]), name
