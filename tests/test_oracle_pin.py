@@ -221,13 +221,16 @@ def test_createsegtri_conventions():
 
 
 def test_abi_exports_every_declared_symbol():
+    import glob
     import re
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     names = set()
-    for h in ("hp_gpu.h", "hp_host.h"):
-        txt = open(os.path.join(root, "include", h)).read()
-        names |= set(re.findall(r"^(?:int|const char \*)\s*(hp_\w+)\(", txt, flags=re.M))
-    assert len(names) > 20
+    headers = sorted(glob.glob(os.path.join(root, "include", "*.h")))
+    assert {os.path.basename(h) for h in headers} >= {"hp_gpu.h", "hp_host.h", "hp_mlp.h", "hp_tet.h"}
+    for h in headers:
+        txt = open(h).read()
+        names |= set(re.findall(r"^(?:int|double|void|const char \*)\s*(hp_\w+)\(", txt, flags=re.M))
+    assert len(names) > 60
     lib = L.lib()
     missing = [n for n in sorted(names) if not hasattr(lib, n)]
     assert not missing, missing
