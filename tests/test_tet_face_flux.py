@@ -357,3 +357,37 @@ def test_exact_steady_solutions_have_zero_residual(p, case, mesh):
     rng = np.random.default_rng(3)
     pert = [a + 1e-3 * rng.uniform(-1, 1, a.shape) for a in pr.state]
     assert exact < 1e-9 * free_residual(pert), exact
+
+
+def test_read_msh_round_trip(tmp_path):
+    """read_msh on a Gmsh 2.2 file written here: cube_tets(2) with its boundary triangles
+    tagged by cube face (elementary ids 11..16), node ids shuffled, extra point / line
+    elements and a $PhysicalNames block that the reader skips."""
+    c = cube_tets(2)
+    rng = np.random.default_rng(1)
+    ids = rng.permutation(c.npnt) + 100                    # file node id of each vertex
+    bf = c.boundary_faces()
+    X = c.pnts[c.tri_pnt[bf]]
+    lines = ["$MeshFormat", "2.2 0 8", "$EndMeshFormat", "$PhysicalNames", "1", '2 1 "wall"',
+             "$EndPhysicalNames", "$Nodes", str(c.npnt)]
+    lines += [f"{ids[i]} {x:.17g} {y:.17g} {z:.17g}" for i, (x, y, z) in enumerate(c.pnts)]
+    lines += ["$EndNodes", "$Elements"]
+    els = [f"15 2 0 1 {ids[0]}", f"1 2 0 2 {ids[0]} {ids[1]}"]
+    want = {}
+    for f, tri in zip(bf, X):
+        d = int(np.argmax(np.ptp(tri, axis=0) < 1e-12))
+        ent = 11 + 2 * d + int(tri[0, d] > 0.5)
+        want.setdefault(ent, []).append(f)
+        els.append("2 2 1 %d %s" % (ent, " ".join(str(ids[v]) for v in c.tri_pnt[f])))
+    els += ["4 2 1 1 %s" % " ".join(str(ids[v]) for v in t) for t in c.tet_pnt]
+    lines += [str(len(els))] + [f"{k + 1} {e}" for k, e in enumerate(els)] + ["$EndElements"]
+    path = tmp_path / "cube.msh"
+    path.write_text("\n".join(lines) + "\n")
+    m, groups = read_msh(str(path))
+    assert (m.npnt, m.nseg, m.ntri, m.ntet) == (c.npnt, c.nseg, c.ntri, c.ntet)
+    assert abs(m.vol.sum() / 6 - 1.0) < 1e-12
+    assert sorted(groups) == sorted(want)
+    # each group is the same set of triangles (by coordinates) as written
+    key = lambda mesh, faces: sorted(tuple(sorted(map(tuple, np.round(mesh.pnts[mesh.tri_pnt[f]], 12)))) for f in faces)
+    for ent in want:
+        assert key(m, groups[ent]) == key(c, want[ent])
