@@ -7,10 +7,14 @@
 //   tet_hp_ins::element_rsdl (straight) tet_hp/ins/rsdl.cpp:442-781
 //   tet_hp_ins::setup_preconditioner    tet_hp/ins/setup_preconditioner.cpp (diagonal: tau, iprcn)
 //   bdry_ins::neumann / inflow rsdl     tet_hp/ins/bdry.cpp:16-102, bdry_ins.h:85-132
+//   tet_hp::jacobian_diagonal, jacobi_relaxation   tet_hp/jacobi.cpp:14-111
+//   tet_hp::minvrt (p = 1 and 2)        tet_hp/setup_preconditioner.cpp:11-221
+//   tet_hp::update                      tet_hp/update.cpp:181-390
 // with the basis operators of tet_basis in the dense form of hp_tet_tables
 // (pinned against the reference's own proj / intgrt / intgrtrst / derivr / derivs /
-// derivt by tests/test_tet_basis_pin.py). Parity: the stages of the reference's
-// loops are kept; sums over points and modes run in the natural order.
+// derivt / proj2d / intgrt2d and lumpinv by tests/test_tet_basis_pin.py). Parity: the
+// stages of the reference's loops are kept; sums over points and modes run in the
+// natural order.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
