@@ -2,21 +2,24 @@
 //
 // hp_gpu_resnorm reduces the residual through a partials buffer that its
 // context allocated with cudaMalloc. Some callers of this library cannot
-// allocate at the moment they need the norm: a solver driver that runs inside a
-// CUDA-graph capture in global capture mode (where cudaMalloc is an illegal
-// call), or an application that gives all device memory to its own pool when it
-// starts and forbids further cudaMalloc/cudaFree. hp_resnorm_noalloc serves
-// them: its only scratch is the file-scope device array below, of fixed size,
-// which every GPU that loads the library keeps until the process exits.
+// allocate at the moment they need the norm: an application that hands all
+// device memory to its own pool when it starts and forbids further
+// cudaMalloc/cudaFree, or a solver embedded in a host program whose memory
+// budget is fixed before the solve begins. hp_resnorm_noalloc serves them: its
+// only scratch is the file-scope device array below, of fixed size, which every
+// GPU that loads the library keeps until the process exits.
 //
 // Host code must not pass the array's name to a kernel (in host code that name
-// is a host-side stand-in, not a device address): the device address is taken
-// once per device with cudaGetSymbolAddress, with that device current, on the
-// first call made on the device. That first call should therefore come before
-// any stream capture. All calls share the one array, so calls whose work
-// overlaps on the GPU (different streams, or different host threads on the same
-// device) race on it and must be serialised by the caller. Every call writes
-// each partial it reads before reading it, so nothing has to start at zero.
+// is a host-side stand-in, not a device address): the device address is looked
+// up with cudaGetSymbolAddress, with the device current, on the first call made
+// in each CUDA context, and kept per context (a new context, e.g. after
+// cudaDeviceReset, gets its own lookup). The call launches two kernels on
+// `stream`, copies the two results to the host and synchronises `stream` before
+// it returns. All calls share the one array, so calls whose work overlaps on
+// the GPU (different streams, or different host threads on the same device)
+// race on it and must be serialised by the caller. Every call writes each
+// partial it reads before reading it, so nothing has to start at zero.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <mutex>
 #include <string>
@@ -32,7 +35,10 @@ constexpr int kThreads = 256;
 static __device__ __align__(256) double g_norm_scratch[2 * HP_NOALLOC_MAX_CHUNKS + 2];
 
 std::mutex g_mu;
-double *g_scratch_dev[64] = {nullptr};  // device address of g_norm_scratch, per device ordinal
+// device address of g_norm_scratch, per device ordinal, valid for the context whose
+// unique id (cuCtxGetId) is g_scratch_ctx[dev]
+double *g_scratch_dev[64] = {nullptr};
+unsigned long long g_scratch_ctx[64] = {0};
 thread_local std::string g_noalloc_err;
 
 __device__ __forceinline__ void block_reduce(double &s, double &m) {
@@ -99,6 +105,32 @@ int fail(int code, const char *msg) {
     return code;
 }
 
+int fail_cuda(const char *what, cudaError_t e) {
+    g_noalloc_err = std::string("hp_resnorm_noalloc: ") + what + ": " + cudaGetErrorString(e);
+    return HP_ECUDA;
+}
+
+// Unique id of the calling thread's current context, through the driver entry points
+// the runtime hands out (the library does not link libcuda itself). Called with g_mu held.
+bool current_context_id(unsigned long long *id) {
+    using get_current_t = CUresult (*)(CUcontext *);
+    using get_id_t = CUresult (*)(CUcontext, unsigned long long *);
+    static get_current_t get_current = nullptr;
+    static get_id_t get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *f0 = nullptr, *f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0, q1;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+            return false;
+        get_current = reinterpret_cast<get_current_t>(f0);
+        get_id = reinterpret_cast<get_id_t>(f1);
+    }
+    CUcontext cu = nullptr;
+    return get_current(&cu) == CUDA_SUCCESS && cu != nullptr && get_id(cu, id) == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" const char *hp_noalloc_last_error(void) { return g_noalloc_err.c_str(); }
@@ -129,27 +161,43 @@ extern "C" int hp_resnorm_noalloc(const double *resv, long long nv, const double
         return HP_OK;
     }
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
-        return fail(HP_ECUDA, "hp_resnorm_noalloc: no current CUDA device");
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail_cuda("no current CUDA device", e);
+    if (dev < 0 || dev >= 64) return fail(HP_ECUDA, "hp_resnorm_noalloc: device ordinal beyond 63");
+    // an error left by an earlier, unrelated call is reported as such, not as this call's
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess) return fail_cuda("a CUDA error was pending before this call", e);
     double *scratch;
     {
-        std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_scratch_dev[dev]) {
+        std::lock_guard<std::mutex> lk(g_mu);  // also guards the driver entry points' lookup
+        // the context's unique id keys the cache; with no context current on this thread,
+        // cudaSetDevice of the current device initialises its primary context (CUDA >= 12)
+        // and makes it current
+        unsigned long long ctx_id = 0;
+        if (!current_context_id(&ctx_id)) {
+            e = cudaSetDevice(dev);
+            if (e != cudaSuccess) return fail_cuda("context initialisation failed", e);
+            if (!current_context_id(&ctx_id)) return fail(HP_ECUDA, "hp_resnorm_noalloc: no current CUDA context");
+        }
+        if (!g_scratch_dev[dev] || g_scratch_ctx[dev] != ctx_id) {
             void *p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_norm_scratch);
-            if (e != cudaSuccess || !p) return fail(HP_ECUDA, "hp_resnorm_noalloc: cudaGetSymbolAddress failed");
+            e = cudaGetSymbolAddress(&p, g_norm_scratch);
+            if (e != cudaSuccess || !p) return fail_cuda("cudaGetSymbolAddress failed", e);
             g_scratch_dev[dev] = static_cast<double *>(p);
+            g_scratch_ctx[dev] = ctx_id;
         }
         scratch = g_scratch_dev[dev];
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     k_chunk_norm<<<(unsigned)nchunks, kThreads, 0, st>>>(resv, nv, ca, ress, ns, cb, resi, ni, scratch);
     k_chunk_final<<<1, kThreads, 0, st>>>((int)nchunks, scratch);
-    if (cudaGetLastError() != cudaSuccess) return fail(HP_ECUDA, "hp_resnorm_noalloc: kernel launch failed");
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_cuda("kernel launch failed", e);
     double out[2];
-    if (cudaMemcpyAsync(out, scratch + 2 * HP_NOALLOC_MAX_CHUNKS, sizeof(out), cudaMemcpyDeviceToHost, st) != cudaSuccess)
-        return fail(HP_ECUDA, "hp_resnorm_noalloc: result copy failed");
-    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(HP_ECUDA, "hp_resnorm_noalloc: stream sync failed");
+    e = cudaMemcpyAsync(out, scratch + 2 * HP_NOALLOC_MAX_CHUNKS, sizeof(out), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return fail_cuda("result copy failed", e);
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail_cuda("stream synchronisation failed", e);
     *l2 = out[0];
     *linf = out[1];
     return HP_OK;

@@ -329,18 +329,21 @@ int hp_gpu_sync(hp_gpu_ctx *ctx);
 const char *hp_gpu_last_error(void);
 
 /* Residual norm that allocates nothing. No counterpart in the reference.
- * For callers that cannot call cudaMalloc when they need the norm: a driver
- * running inside a CUDA-graph capture in global mode, or an application whose
- * device memory all belongs to its own pool. Same result as hp_gpu_resnorm's
- * reduction (sqrt of the sum of squares and max |x| over res.v, res.s, res.i),
- * but over caller-owned device arrays (e.g. from hp_gpu_device_ptrs) and with a
- * fixed static device scratch of HP_NOALLOC_MAX_CHUNKS partials, held by every
- * GPU that loads the library until exit. At most HP_NOALLOC_MAX_CHUNKS chunks
- * of HP_NOALLOC_CHUNK values per call (nv, ns, ni each rounded up to whole
- * chunks); larger inputs return HP_EINVAL with a message from
- * hp_noalloc_last_error(). The first call on a device looks up the scratch's
- * device address and should come before any stream capture. All calls share
- * the scratch: calls that overlap on the GPU race. Synchronises `stream`. */
+ * For callers that cannot call cudaMalloc when they need the norm: an
+ * application that gives all device memory to its own pool at start-up and
+ * forbids further cudaMalloc / cudaFree, or a solver embedded in a host program
+ * whose device-memory budget is fixed before the solve. Same result as
+ * hp_gpu_resnorm's reduction (sqrt of the sum of squares and max |x| over
+ * res.v, res.s, res.i), but over caller-owned device arrays (e.g. from
+ * hp_gpu_device_ptrs) and with a fixed static device scratch of
+ * HP_NOALLOC_MAX_CHUNKS partials, held by every GPU that loads the library until
+ * exit. At most HP_NOALLOC_MAX_CHUNKS chunks of HP_NOALLOC_CHUNK values per call
+ * (nv, ns, ni each rounded up to whole chunks); larger inputs return HP_EINVAL
+ * with a message from hp_noalloc_last_error(). The first call in each CUDA
+ * context looks up the scratch's device address. The call launches two kernels
+ * on `stream`, copies the two results to the host and synchronises `stream`
+ * before returning. All calls share the scratch: calls that overlap on the GPU
+ * race, so the caller serialises them. */
 #define HP_NOALLOC_CHUNK 65536
 #define HP_NOALLOC_MAX_CHUNKS 4096
 int hp_resnorm_noalloc(const double *resv, long long nv, const double *ress, long long ns, const double *resi,

@@ -7,7 +7,9 @@
 * the DPBTRSNU2 restatement against utilities/myblas.c, including its indexing
   quirk;
 * the exactness known-answer test of Testing/tri_hp/conv-diff/Correctness;
-* the split-square mesh against the reference's square7.grd.
+* the split-square mesh against the reference's square7.grd (its golden hash in
+  tests/golden/square7_grd.json, and the file itself when HP_REFERENCE_DIR names
+  the reference checkout).
 """
 import ctypes
 import os
@@ -19,7 +21,9 @@ import hpb
 from hpb import _lib as L
 from oracle import oracle as O
 
-REF_GRD = "/root/reference/Testing/tri_hp/ins/Spatial Accuracy/Inputs/square7.grd"
+REF_DIR = os.environ.get("HP_REFERENCE_DIR")  # reference checkout, for the checks that read its files
+REF_GRD = os.path.join(REF_DIR, "Testing/tri_hp/ins/Spatial Accuracy/Inputs/square7.grd") if REF_DIR else None
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 TABLES = ["gx", "dgx", "wtx", "xp", "x0", "gxwtx", "dgxwtx", "dltx", "dltx1", "gn", "dgn", "wtn", "np", "n0",
           "gnwtn", "gnwtnn0", "dgnwtn", "dltn", "dltn1", "dltn2", "norm", "sfmv", "ifmb", "vdiag", "vfms", "sdiag",
           "sfms", "bfmi", "idiag", "sfmv1d", "vdiag1d", "vfms1d", "sdiag1d"]
@@ -189,21 +193,29 @@ def test_tobasis_spatial_accuracy():
 
 
 def test_square_mesh_matches_square7_grd():
+    import json
+    import sys
+    sys.path.insert(0, GOLDEN)
+    from make_reference_fixtures import tri_keys_sha256
     m = hpb.square_mesh(64)
     assert (m.npnt, m.nseg, m.ntri) == (4225, 12416, 8192)
     assert np.all(m.area2() > 0)
-    if not os.path.exists(REF_GRD):
-        pytest.skip("reference mesh file absent")
+    gold = json.load(open(os.path.join(GOLDEN, "square7_grd.json")))
+    assert (gold["npnt"], gold["nseg"], gold["ntri"]) == (m.npnt, m.nseg, m.ntri)
+    assert tri_keys_sha256(m.pnts, m.tri_pnt, 64) == gold["tri_keys_sha256"]
+
+
+@pytest.mark.skipif(not (REF_GRD and os.path.exists(REF_GRD)), reason="HP_REFERENCE_DIR unset")
+def test_square7_grd_file_matches_its_golden_hash():
+    import json
+    import sys
+    sys.path.insert(0, GOLDEN)
+    from make_reference_fixtures import tri_keys_sha256
+    m = hpb.square_mesh(64)
+    gold = json.load(open(os.path.join(GOLDEN, "square7_grd.json")))
     g = hpb.read_grd(REF_GRD)
     assert (g.npnt, g.nseg, g.ntri) == (m.npnt, m.nseg, m.ntri)
-
-    def tri_set(mesh):
-        q = np.round(mesh.pnts[mesh.tri_pnt] * 64).astype(np.int64)  # [ntri][3][2] integer lattice
-        keys = q[:, :, 0] * 1000 + q[:, :, 1]
-        k = np.sort(keys, axis=1)
-        return set(map(tuple, k))
-
-    assert tri_set(g) == tri_set(m)
+    assert tri_keys_sha256(g.pnts, g.tri_pnt, 64) == gold["tri_keys_sha256"]
 
 
 def test_createsegtri_conventions():

@@ -15,7 +15,8 @@ from hpb import tet as TB
 from hpb.tetmesh import TetMesh, cube_tets, read_msh
 from oracle import oracle as O
 
-REF_MSH = "/root/reference/Testing/tet_hp/cd/Multigrid/Inputs/tet{}.msh"
+REF_DIR = os.environ.get("HP_REFERENCE_DIR")  # reference checkout, for the checks that read its files
+REF_MSH = os.path.join(REF_DIR or "", "Testing/tet_hp/cd/Multigrid/Inputs/tet{}.msh")
 
 
 def scrambled_cube(n, seed):
@@ -226,7 +227,8 @@ def test_divergence_theorem_on_a_scrambled_mesh(p):
     _div_check(scrambled_cube(2, 7), p, 70 + p)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_MSH.format(4)), reason="reference meshes absent")
+@pytest.mark.skipif(not (REF_DIR and os.path.exists(REF_MSH.format(4))),
+                    reason="HP_REFERENCE_DIR unset or its tet meshes absent")
 def test_reference_gmsh_meshes_read_and_satisfy_the_divergence_theorem():
     """The reference's own tet test meshes (Testing/tet_hp/cd/Multigrid/Inputs/tet{2,4,8}.msh):
     unit volume, six boundary groups (the input's b0_f<id> keys) that cover the boundary faces,
