@@ -291,6 +291,17 @@ struct or_ctx {
     std::vector<double> vprcn, sprcn, tprcn, tau;  // tau [ntri][NV] (cd uses column 0)
     // work
     double uht[3][HP_MXTM], lf[3][HP_MXTM];
+    // multigrid: a coarse level (mg_kind 1: p-level of the same mesh, 2: h-level at p = 1)
+    // keeps its fine level, the restricted residual res0, the FAS source dres, the
+    // isfrst flag of mg_source, and for h-levels the transfer weights (ccnnct of the fine
+    // vertices f2c_*, fcnnct of the coarse vertices c2f_*) and vug_frst
+    or_ctx *fine = nullptr;
+    int mg_kind = 0;
+    double fadd = 1.0;
+    bool isfrst = false;
+    std::vector<double> res0v, res0s, res0i, dresv, dress, dresi, vugfrst;
+    std::vector<int> f2c_tri, c2f_tri;
+    std::vector<double> f2c_wt, c2f_wt;
 };
 
 static double tri_area(const or_ctx *c, int t) {  // tri_mesh/tprims.cpp:66-80 (2x area)
@@ -696,7 +707,21 @@ void or_set_prcn(or_ctx *c, const double *vp, const double *sp, const double *tp
     std::copy(tau, tau + c->tau.size(), c->tau.begin());
 }
 
-// tri_hp::rsdl(stage) (nstage.cpp:12-110), one block, fine level
+// tri_hp::mg_source (nstage.cpp:113-129) on a coarse level: on the first residual after
+// mg_restrict (isfrst) the driving term dres = fadd*res0 - res, then res += dres
+static void mg_source(or_ctx *c) {
+    if (c->isfrst) {
+        for (size_t k = 0; k < c->resv.size(); ++k) c->dresv[k] = c->fadd * c->res0v[k] - c->resv[k];
+        for (size_t k = 0; k < c->ress.size(); ++k) c->dress[k] = c->fadd * c->res0s[k] - c->ress[k];
+        for (size_t k = 0; k < c->resi.size(); ++k) c->dresi[k] = c->fadd * c->res0i[k] - c->resi[k];
+        c->isfrst = false;
+    }
+    for (size_t k = 0; k < c->resv.size(); ++k) c->resv[k] += c->dresv[k];
+    for (size_t k = 0; k < c->ress.size(); ++k) c->ress[k] += c->dress[k];
+    for (size_t k = 0; k < c->resi.size(); ++k) c->resi[k] += c->dresi[k];
+}
+
+// tri_hp::rsdl(stage) (nstage.cpp:12-110), one block; on a coarse level with mg_source
 void or_rsdl(or_ctx *c, int stage) {
     const int nstage = c->ph.nstage;
     if (stage < nstage) {
@@ -722,6 +747,7 @@ void or_rsdl(or_ctx *c, int stage) {
     for (size_t k = 0; k < c->ress.size(); ++k) c->ress[k] += c->rrs[k];
     for (size_t k = 0; k < c->resi.size(); ++k) c->resi[k] += c->rri[k];
     bdry_rsdl(c);
+    if (c->mg_kind) mg_source(c);
 }
 
 // tri_hp_{cd,ins}::setup_preconditioner + tri_hp::setup_preconditioner (diagonal)
@@ -959,6 +985,187 @@ double or_maxres(or_ctx *c, double *out) {
     double e = 0.0;
     for (int n = 0; n < NV; ++n) { if (out) out[n] = mx[n]; e = std::max(e, mx[n]); }
     return e;
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid: tri_hp::mg_restrict (movco.cpp:4-106), mg_prolongate (movfin.cpp:7-82) and
+// block::cycle (tri_mesh/blocks.cpp:1267-1348). The reference keeps the p-levels of one
+// mesh in one object whose state ug is shared, so a coarse p-level reads and updates the
+// lower modes of the fine state in place (ugtouht's interior index step sm0 - sm,
+// gtol.cpp:42-52; update's, nstage.cpp:395-406). Here every level is its own context:
+// restriction copies the lower modes in and prolongation copies them back, which is the
+// same arithmetic.
+// ---------------------------------------------------------------------------
+static void mg_alloc(or_ctx *c) {
+    c->res0v.assign(c->ugv.size(), 0.0); c->res0s.assign(c->ugs.size(), 0.0); c->res0i.assign(c->ugi.size(), 0.0);
+    c->dresv.assign(c->ugv.size(), 0.0); c->dress.assign(c->ugs.size(), 0.0); c->dresi.assign(c->ugi.size(), 0.0);
+}
+
+// lower modes of fine-level arrays (v, s [nseg][sm_f][NV], i [ntri][im_f][NV]) to or from a
+// coarse p-level's arrays; interior rows m = 1 .. sm_c - 1 hold sm_c - m coarse modes, and the
+// fine index skips sm_f - sm_c entries after each row (movco.cpp:22-36: the skip is the coarse
+// p, which equals sm_f - sm_c when p halves)
+static void plevel_copy(const or_ctx *c, const or_ctx *f, double *fv, double *fs, double *fi, double *cv,
+                        double *cs, double *ci, bool to_coarse) {
+    const int NV = c->NV, smc = c->sm, smf = f->sm, imc = c->im, imf = f->im;
+    auto mv = [to_coarse](double &fine, double &coarse) {
+        if (to_coarse) coarse = fine;
+        else fine = coarse;
+    };
+    for (int i = 0; i < c->npnt * NV; ++i) mv(fv[i], cv[i]);
+    for (int sd = 0; sd < c->nseg; ++sd)
+        for (int m = 0; m < smc; ++m)
+            for (int n = 0; n < NV; ++n) mv(fs[(sd * smf + m) * NV + n], cs[(sd * smc + m) * NV + n]);
+    if (imc > 0)
+        for (int t = 0; t < c->ntri; ++t) {
+            int indx = 0, indx1 = 0;
+            for (int m = 1; m < smc; ++m) {
+                for (int k = 0; k < smc - m; ++k) {
+                    for (int n = 0; n < NV; ++n)
+                        mv(fi[((size_t)t * imf + indx1) * NV + n], ci[((size_t)t * imc + indx) * NV + n]);
+                    ++indx; ++indx1;
+                }
+                indx1 += smf - smc;
+            }
+        }
+}
+
+// Needs the fine level's full residual rsdl(nstage), which block::cycle evaluates just
+// before mg_restrict (blocks.cpp:1323-1325).
+void or_mg_restrict(or_ctx *c) {
+    or_ctx *f = c->fine;
+    const int NV = c->NV;
+    c->isfrst = true;
+    if (c->mg_kind == 1) {
+        plevel_copy(c, f, f->resv.data(), f->ress.data(), f->resi.data(), c->res0v.data(), c->res0s.data(),
+                    c->res0i.data(), true);
+        plevel_copy(c, f, f->ugv.data(), f->ugs.data(), f->ugi.data(), c->ugv.data(), c->ugs.data(), c->ugi.data(),
+                    true);
+    } else {
+        std::fill(c->res0v.begin(), c->res0v.end(), 0.0);
+        for (int i = 0; i < f->npnt; ++i) {  // movco.cpp:51-58
+            const int tind = c->f2c_tri[i];
+            for (int j = 0; j < 3; ++j) {
+                const int v0 = c->tri_pnt[3 * tind + j];
+                for (int n = 0; n < NV; ++n) c->res0v[v0 * NV + n] += c->f2c_wt[3 * i + j] * f->resv[i * NV + n];
+            }
+        }
+        for (int i = 0; i < c->npnt; ++i) {  // movco.cpp:88-99
+            const int tind = c->c2f_tri[i];
+            for (int n = 0; n < NV; ++n) c->ugv[i * NV + n] = 0.0;
+            for (int j = 0; j < 3; ++j)
+                for (int n = 0; n < NV; ++n)
+                    c->ugv[i * NV + n] += c->c2f_wt[3 * i + j] * f->ugv[f->tri_pnt[3 * tind + j] * NV + n];
+            for (int n = 0; n < NV; ++n) c->vugfrst[i * NV + n] = c->ugv[i * NV + n];
+        }
+    }
+}
+
+void or_mg_prolongate(or_ctx *c) {
+    or_ctx *f = c->fine;
+    const int NV = c->NV;
+    if (c->mg_kind == 1) {
+        plevel_copy(c, f, f->ugv.data(), f->ugs.data(), f->ugi.data(), c->ugv.data(), c->ugs.data(), c->ugi.data(),
+                    false);
+        return;
+    }
+    for (size_t k = 0; k < c->vugfrst.size(); ++k) c->vugfrst[k] -= c->ugv[k];  // movfin.cpp:24
+    for (int i = 0; i < f->npnt; ++i) {                                          // movfin.cpp:33-43, 79
+        const int tind = c->f2c_tri[i];
+        double corr[3] = {0.0, 0.0, 0.0};
+        for (int j = 0; j < 3; ++j) {
+            const int ind = c->tri_pnt[3 * tind + j];
+            for (int n = 0; n < NV; ++n) corr[n] -= c->f2c_wt[3 * i + j] * c->vugfrst[ind * NV + n];
+        }
+        for (int n = 0; n < NV; ++n) f->ugv[i * NV + n] += corr[n];
+    }
+}
+
+int or_mg_attach_p(or_ctx *c, or_ctx *f, double fadd) {
+    if (c->npnt != f->npnt || c->ntri != f->ntri || c->NV != f->NV || c->tm >= f->tm) return -1;
+    c->fine = f; c->mg_kind = 1; c->fadd = fadd;
+    mg_alloc(c);
+    return 0;
+}
+
+int or_mg_attach_h(or_ctx *c, or_ctx *f, const int *f2c_tri, const double *f2c_wt, const int *c2f_tri,
+                   const double *c2f_wt, double fadd) {
+    if (c->sm != 0 || c->NV != f->NV) return -1;
+    c->fine = f; c->mg_kind = 2; c->fadd = fadd;
+    c->f2c_tri.assign(f2c_tri, f2c_tri + f->npnt);
+    c->f2c_wt.assign(f2c_wt, f2c_wt + 3 * f->npnt);
+    c->c2f_tri.assign(c2f_tri, c2f_tri + c->npnt);
+    c->c2f_wt.assign(c2f_wt, c2f_wt + 3 * c->npnt);
+    c->vugfrst.assign(c->ugv.size(), 0.0);
+    mg_alloc(c);
+    return 0;
+}
+
+// block::cycle (blocks.cpp:1267-1348) without the error-control branch; returns the
+// count of bad elements met by a preconditioner set-up (the reference throws)
+static int cycle(or_ctx **lv, int n, int lvl, int vw, int itercrsn, int iterrfne, int eval) {
+    or_ctx *c = lv[lvl];
+    for (int vc = 0; vc < vw; ++vc) {
+        if (eval) { int e = or_setup_preconditioner(c); if (e) return e; }
+        for (int it = 0; it < itercrsn; ++it) or_update(c);
+        if (lvl == n - 1) return 0;
+        or_rsdl(c, c->ph.nstage);
+        or_mg_restrict(lv[lvl + 1]);
+        int e = cycle(lv, n, lvl + 1, vw, itercrsn, iterrfne, eval);
+        if (e) return e;
+        or_mg_prolongate(lv[lvl + 1]);
+        if (eval && iterrfne) { e = or_setup_preconditioner(c); if (e) return e; }
+        for (int it = 0; it < iterrfne; ++it) or_update(c);
+    }
+    return 0;
+}
+
+int or_cycle(or_ctx **lv, int n, int vw, int itercrsn, int iterrfne, int eval) {
+    return cycle(lv, n, 0, vw, itercrsn, iterrfne, eval);
+}
+
+// ||R64(u)||_2 over every v/s/i coefficient of rsdl(nstage) with the rows of essential
+// boundary values zeroed (hp_edge_bdry::vdirichlet / sdirichlet, hp_boundary.cpp:680-704)
+double or_resnorm_essential(or_ctx *c) {
+    or_rsdl(c, c->ph.nstage);
+    const int NV = c->NV;
+    double ss = 0.0;
+    for (int i = 0; i < c->npnt; ++i)
+        for (int n = 0; n < NV; ++n)
+            if (!(c->vess[i] & (1 << n))) ss += c->resv[i * NV + n] * c->resv[i * NV + n];
+    for (int sd = 0; sd < c->nseg; ++sd)
+        for (int m = 0; m < c->sm; ++m)
+            for (int n = 0; n < NV; ++n)
+                if (!(c->sess[sd] & (1 << n))) {
+                    const double r = c->ress[(sd * c->sm + m) * NV + n];
+                    ss += r * r;
+                }
+    for (double r : c->resi) ss += r * r;
+    return std::sqrt(ss);
+}
+
+// Convergence driver of the plain FP64 method (block::go's loop over block::cycle with
+// the reference's preconditioner_interval): cycles until ||R64|| has dropped by `drop`
+// or max_cycles ran; preconditioners on the first cycle and every prcn_every cycles.
+// hist[k] = ||R64|| / ||R64(entry)|| after cycle k (hist[0] = 1). Returns the cycles run,
+// or -(bad elements) when a set-up failed. nlevels = 1 runs itercrsn updates per cycle.
+int or_solve_mg(or_ctx **lv, int n, double drop, int max_cycles, int vw, int itercrsn, int iterrfne,
+                int prcn_every, double *hist, int hist_cap) {
+    int nc = 0, nh = 0;
+    int e = or_setup_preconditioner(lv[0]);
+    if (e) return -e;
+    const double r0 = or_resnorm_essential(lv[0]);
+    if (hist && nh < hist_cap) hist[nh++] = 1.0;
+    while (nc < max_cycles) {
+        const int eval = (nc == 0 || (prcn_every > 0 && nc % prcn_every == 0)) ? 1 : 0;
+        e = cycle(lv, n, 0, vw, itercrsn, iterrfne, eval);
+        if (e) return -e;
+        ++nc;
+        const double d = or_resnorm_essential(lv[0]) / r0;
+        if (hist && nh < hist_cap) hist[nh++] = d;
+        if (!(d == d) || d <= drop) break;
+    }
+    return nc;
 }
 
 // Basis-operator probes for pinning against the reference's tri_basis.

@@ -52,6 +52,15 @@ def lib():
         o.or_basis_intgrt1d.argtypes = [P, P, P]
         o.or_dpbtrsnu2.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int]
         o.or_element_jacobian.argtypes = [P, P]
+        I, D = ctypes.c_int, ctypes.c_double
+        o.or_mg_attach_p.argtypes = [P, P, D]
+        o.or_mg_attach_h.argtypes = [P, P, P, P, P, P, D]
+        o.or_mg_restrict.argtypes = [P]
+        o.or_mg_prolongate.argtypes = [P]
+        o.or_cycle.argtypes = [P, I, I, I, I, I]
+        o.or_resnorm_essential.argtypes = [P]
+        o.or_resnorm_essential.restype = D
+        o.or_solve_mg.argtypes = [P, I, D, I, I, I, I, I, P, I]
         I = ctypes.c_int
         o.ot_create.restype = P
         o.ot_create.argtypes = [P, P, I, I, I, I, P, P, P, P, P, P, P]
@@ -176,6 +185,48 @@ class Oracle:
     def maxres(self):
         out = np.zeros(self.prob.NV)
         return self.o.or_maxres(self.h, _p(out)), out
+
+
+class OracleHierarchy:
+    """The oracle's restatement of a multigrid hierarchy (tri_hp::mg_restrict /
+    mg_prolongate / mg_source and block::cycle): one Oracle per level, levels[0] the
+    finest, each next one a p-level ("p") or an h-level ("h") of the previous, with the
+    same mgconnect transfer weights as hpb.multigrid.Hierarchy."""
+
+    def __init__(self, probs, kinds, fadd=1.0):
+        from hpb.multigrid import connect
+        self.probs = probs
+        self.levels = [Oracle(pr) for pr in probs]
+        self._keep = []
+        o = lib()
+        for l in range(1, len(probs)):
+            c, f = self.levels[l], self.levels[l - 1]
+            if kinds[l] == "p":
+                rc = o.or_mg_attach_p(c.h, f.h, fadd)
+            else:
+                f2c_t, f2c_w = connect(probs[l - 1].mesh, probs[l].mesh)
+                c2f_t, c2f_w = connect(probs[l].mesh, probs[l - 1].mesh)
+                arrs = [np.ascontiguousarray(a) for a in (f2c_t, f2c_w, c2f_t, c2f_w)]
+                self._keep += arrs
+                rc = o.or_mg_attach_h(c.h, f.h, *[_p(a) for a in arrs], fadd)
+            if rc != 0:
+                raise ValueError(f"level {l} cannot be attached as a {kinds[l]}-level")
+
+    def _handles(self):
+        return (ctypes.c_void_p * len(self.levels))(*[lv.h for lv in self.levels])
+
+    def cycle(self, vw=1, itercrsn=2, iterrfne=2, eval_prcn=True):
+        return lib().or_cycle(self._handles(), len(self.levels), vw, itercrsn, iterrfne, int(eval_prcn))
+
+    def solve(self, drop=1e-10, max_cycles=500, vw=1, itercrsn=2, iterrfne=2, prcn_every=1):
+        """Cycles until ||R64|| (essential rows excluded) has dropped by `drop`; returns
+        (hist, cycles) as hpb.multigrid.Hierarchy.solve does (without the time)."""
+        hist = np.zeros(max_cycles + 2)
+        nc = lib().or_solve_mg(self._handles(), len(self.levels), drop, max_cycles, vw, itercrsn, iterrfne,
+                               prcn_every, _p(hist), len(hist))
+        if nc < 0:
+            raise RuntimeError(f"preconditioner set-up met {-nc} bad elements")
+        return hist[:nc + 1], nc
 
 
 def element_jacobians(oracle):
