@@ -1,22 +1,27 @@
 #!/usr/bin/env python
-"""Benchmark of the tri_hp element-residual path on B200 (one process per GPU).
+"""Benchmark of the tri_hp element-residual and multigrid-smoothing path on B200
+(one process per GPU).
 
-Workload (N = 1): scalar convection-diffusion (tri_hp cd, CONST_A), velocity
-(1, 0.5), diffusivity 1e-3, p = 4, Dirichlet data sin(pi x) sin(pi y) on a
-317 x 317 split-square mesh of the unit square (200,978 triangles, 1.61 M
-DOF). Seeded synthetic state: the Dirichlet field projected onto the basis plus
-U[-1,1) * 1e-3 noise (splitmix64). A "step" is one full FP64 residual
-evaluation tri_hp::rsdl(nstage) over the whole mesh, computed from the stored
-cd element operators (built once before the timed steps; the matrix-free
-element kernel is timed beside it); `value` is rsdl GDoF/s
-(whole job, inputs resident in HBM, device time, L2 flushed between steps);
-`e2e` is the same metric through the C-ABI with host buffers (state upload from
-pinned memory + rsdl + residual download every step, wall clock).
+Default workload (N = 1): ins lid-driven cavity, Re 400 (rho 1, mu 1/400), p = 6,
+512 x 512 split squares of the unit square (524,288 triangles, 28.3 M DOF), velocity
+Dirichlet on every wall, u = 1 on the lid; state = the boundary field projected plus
+U[-1,1) * 1e-3 seeded noise (splitmix64). Multigrid hierarchy: p-levels 6 -> 3 -> 1 on
+the fine mesh, then h-levels of 131,072 / 32,768 / 8,192 triangles at p = 1.
+A "step" is one full FP64 residual evaluation tri_hp::rsdl(nstage) of the fine level;
+`value` is its rsdl GDoF/s (whole job, state resident in HBM, device time with CUDA
+events, the 226 MB state exceeds L2 and L2 is flushed between steps as well); `e2e` is
+the same metric through the C-ABI with host buffers (pinned state upload + rsdl +
+residual download every step). `time_to_tol` runs W-cycles from the initial state to a
+1e-10 drop of the FP64 residual: plain FP64, FP32 smoothing inside FP64 defect
+correction, and that plus the learned preconditioner correction. `roofline` relates the
+element kernel to the FP64 tensor-core (DMMA) throughput measured in the same run, with
+the HBM fraction of the compulsory bytes beside it.
 
---gpus N > 1 runs N independent replicas of the same workload (the path does
-not shard across GPUs in this tier): value = sum over ranks.
---impl reference times the CPU oracle (the C++ restatement of the reference's
-rsdl) on the host cores with the same metric.
+--gpus N > 1 runs N independent replicas (the path does not shard across GPUs in this
+tier): value = sum over ranks.
+--impl reference times the CPU oracle (the C++ restatement of the reference's rsdl) on
+all host cores on bounded samples of the same workload.
+--workload cd runs the earlier cd p = 4 line (stored element operators).
 """
 import argparse
 import ctypes
@@ -32,7 +37,85 @@ sys.path.insert(0, ROOT)
 
 N_MESH = 317
 P = 4
-METRIC = "rsdl GDoF/s (FP64 tri_hp::rsdl, cd p=4)"
+METRIC_CD = "rsdl GDoF/s (FP64 tri_hp::rsdl, cd p=4)"
+METRIC = "time to 1e-10 residual drop: learned+FP32 vs plain FP64, 1xB200; rsdl GDoF/s"
+C3_N, C3_P, C3_RE = 512, 6, 400.0
+STRIP_ROWS = 8  # CPU samples: 512 x 8-square strips (8,192 triangles) of the C3 mesh
+
+
+def c3_config():
+    return {"workload": "C3: ins lid-driven cavity Re 400, p=6, 512x512 split squares (524,288 triangles, "
+                        "28.3 M DOF); multigrid p-levels 6,3,1 then h-levels of 131,072 / 32,768 / 8,192 triangles",
+            "physics": "ins", "p": C3_P, "ntri": 2 * C3_N * C3_N, "re": C3_RE, "nstage": 5,
+            "step": "one FP64 tri_hp::rsdl(nstage) of the fine level",
+            "l2": "state (226 MB) and residual exceed L2; L2 also flushed between timed steps (256 MiB write)",
+            "parallelism": "replicas"}
+
+
+def c3_factory(n, p, **kw):
+    import hpb
+    return hpb.lid_cavity_ins(n=n, p=p, re=C3_RE, **kw)
+
+
+def strip_problem(k):
+    """Strip k (from the lid down) of the C3 mesh: 512 x STRIP_ROWS squares with the C3
+    spacing, the lid-cavity state on it (boundary field + 1e-3 noise), p = 6."""
+    import hpb
+    y1 = 1.0 - (k % (C3_N // STRIP_ROWS)) * STRIP_ROWS / C3_N
+    m = hpb.square_mesh(C3_N, 0.0, 1.0, y1 - STRIP_ROWS / C3_N, y1, ny=STRIP_ROWS)
+    return hpb.lid_cavity_ins(p=C3_P, re=C3_RE, mesh=m, seed=20261206 + k)
+
+
+def cpu_strip_worker(args):
+    """One host core: the oracle's rsdl(nstage) on strip k of the C3 mesh; `warmup`
+    untimed then `steps` timed evaluations (steps = 0: until `secs` seconds passed)."""
+    k, steps, warmup, secs = args
+    sys.path.insert(0, os.path.join(ROOT, "hp-multiphysics_b200"))
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle
+    pr = strip_problem(k)
+    o = Oracle(pr)
+    o.setup_preconditioner()
+    for _ in range(max(1, warmup)):
+        o.rsdl(pr.phys.nstage)
+    t0 = time.perf_counter()
+    reps = 0
+    while (reps < steps) if steps > 0 else (time.perf_counter() - t0 < secs):
+        o.rsdl(pr.phys.nstage)
+        reps += 1
+    return pr.ndof * reps, time.perf_counter() - t0, reps
+
+
+def run_cpu_strips(cores, steps, warmup, secs=0.0):
+    """Oracle rsdl GDoF/s over `cores` processes (one strip each, run concurrently)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        res = pool.map(cpu_strip_worker, [(k, steps, warmup, secs) for k in range(cores)])
+    return sum(r[0] for r in res) / max(r[1] for r in res) / 1e9, min(r[2] for r in res)
+
+
+def load_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def ins_flops_per_element(p, beta_positive=True):
+    """Algorithmic FP64 flops of one ins element residual (tri_hp_ins::element_rsdl with
+    the sum-factorised tri_basis operators), from the table the oracle's op-counting
+    build writes (profiles/flops_per_element.json); a loop-count estimate otherwise."""
+    try:
+        t = json.load(open(os.path.join(ROOT, "profiles", "flops_per_element.json")))
+        return float(t["ins"][str(p)]["full" if beta_positive else "imaginary"]), "oracle op count"
+    except Exception:
+        G, X, T = p + 1, p + 2, (p + 1) * (p + 2) // 2
+        projd = G * (4 * T + X) + 6 * G * G * X
+        projv = 2 * G * T + 2 * G * G * X
+        intrs = 2 * G * G + 4 * X * G * G + 4 * T * G
+        der = 2 * G * G + 3 * G * G * (G - 1)
+        return float(2 * projd + projv + 6 * intrs + 6 * der + 100 * G * G), "loop-count estimate"
 
 
 def workload_config():
@@ -472,6 +555,16 @@ def _rel(a, b):
     return float(np.sqrt(sum(np.sum((x - y) ** 2) for x, y in zip(a, b))) / np.sqrt(sum(np.sum(x * x) for x in a)))
 
 
+def _rel_ins_modulo_pressure_level(a, b):
+    """Relative L2 difference of two ins states (v, s, i arrays, variables u, v, p last) after
+    removing the difference of their mean vertex pressure: with velocity given on every wall
+    the pressure is fixed only up to a constant (a constant is the vertex modes alone)."""
+    import numpy as np
+    b = [x.copy() for x in b]
+    b[0][:, 2] += np.mean(a[0][:, 2]) - np.mean(b[0][:, 2])
+    return _rel(a, b)
+
+
 def time_to_tolerance(hpb, dev):
     """Time to a 1e-10 drop of the FP64 residual norm (Dirichlet rows excluded) on cd p=4
     with Dirichlet data -(x-8)^2, velocity (1,0.5), kcond 1e-3, noise 1e-3. `seconds` is
@@ -564,12 +657,208 @@ def time_to_tolerance(hpb, dev):
     return out
 
 
+def kernel_sweep(hpb, dev, n, ps, steps, timed, stream):
+    """FP64 element-kernel time per p on the lid cavity (n x n split squares): the tensor-core
+    (DMMA) and the scalar warp kernel, with the algorithmic flop rate (oracle op count) and
+    the FP64 tensor-core peak measured in the same run."""
+    from hpb._lib import check
+    peak = ctypes.c_double()
+    lib = hpb._lib.lib()
+    lib.hp_tet_fp64_mma_peak.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    check(lib.hp_tet_fp64_mma_peak(dev, 200.0, ctypes.byref(peak)), "fp64 mma peak")
+    for p in ps:
+        pr = hpb.lid_cavity_ins(n=n, p=p, re=C3_RE)
+        g = hpb.GPULevel(pr, device=dev, stream=ctypes.c_void_p(stream.cuda_stream))
+        g.setup_preconditioner()
+        ns = pr.phys.nstage
+        fl_el, src = ins_flops_per_element(p)
+        line = {"sweep": "kernels", "p": p, "ntri": pr.mesh.ntri, "ndof": pr.ndof, "flops_per_element": fl_el,
+                "fp64_tensor_peak_tflops": peak.value}
+        for kind in ("tensor", "scalar"):
+            g.element_kernel(kind)
+            el = lambda: check(lib.hp_gpu_enqueue_element_rsdl(g.h, ns), "element_rsdl")
+            rs = lambda: check(lib.hp_gpu_enqueue_rsdl(g.h, ns), "rsdl")
+            for _ in range(3):
+                rs()
+            k_ms = sum(timed(el, steps, stream)) / steps
+            r_ms = sum(timed(rs, steps, stream)) / steps
+            tf = fl_el * pr.mesh.ntri / (k_ms * 1e-3) / 1e12
+            line[kind] = {"kernel_ms": k_ms, "rsdl_ms": r_ms, "rsdl_gdofs": pr.ndof / (r_ms * 1e-3) / 1e9,
+                          "tflops": tf, "frac_of_fp64_tensor_peak": tf / peak.value}
+        line["speedup_tensor_vs_scalar"] = line["scalar"]["kernel_ms"] / line["tensor"]["kernel_ms"]
+        g.close()
+        print(json.dumps(line), flush=True)
+
+
+def c3_time_to_tol(hpb, dev, stream, max_cycles=150):
+    """C3 W-cycles (vwcycle 2, 2 + 2 updates per level, preconditioners every cycle) from
+    the initial state to a 1e-10 drop of the FP64 residual: plain FP64, FP32 smoothing
+    inside FP64 defect correction, and that plus the learned correction of the Jacobi
+    blocks on the fine level. The network is trained on the GPU on solver-generated
+    samples of 4 lid-cavity instances at other Reynolds numbers (64 x 64 squares, p = 6)."""
+    import numpy as np
+    from hpb import learned as LR
+    from hpb import multigrid as MG
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(20261210)
+    train_re = [float(x) for x in rng.uniform(100.0, 1000.0, 4)]
+    F, T = [], []
+    for k, re in enumerate(train_re):
+        f, tg = LR.solver_samples(lambda: hpb.lid_cavity_ins(n=64, p=C3_P, re=re, seed=500 + k))
+        F.append(f)
+        T.append(tg)
+    net, lh = LR.train(np.concatenate(F), np.concatenate(T), steps=400)
+    out = {"drop": 1e-10, "criterion": "||R64||_2 / ||R64(u0)||_2 over all non-Dirichlet v/s/i rows",
+           "cycle": "W (vwcycle 2), 2+2 multistage updates per level, preconditioners every cycle",
+           "network": {"widths": "17-64-64-64-1", "dtype": "BF16 weights, FP32 accumulation",
+                       "training_re": train_re, "samples": int(sum(len(t) for t in T)),
+                       "training_seconds": time.perf_counter() - t0}}
+    states = {}
+    for name, mixed, learned in (("fp64", False, False), ("fp32_defect_correction", True, False),
+                                 ("learned_fp32", True, True)):
+        H = MG.build(c3_factory, n=C3_N, p=C3_P, hlevels=3, stream=ctypes.c_void_p(stream.cuda_stream))
+        if learned:
+            LR.attach(H.levels[0], net, 1.0)
+        hist, sec, cyc = H.solve(drop=1e-10, max_cycles=max_cycles, vw=2, mixed=mixed, prcn_every=1)
+        states[name] = H.levels[0].state()
+        out[name] = {"seconds": sec, "cycles": cyc, "ms_per_cycle": 1e3 * sec / max(cyc, 1),
+                     "drop": float(hist[-1]), "reached": bool(hist[-1] <= 1e-10),
+                     "rel_l2_state_diff_vs_fp64_modulo_pressure_level":
+                         _rel_ins_modulo_pressure_level(states["fp64"], states[name])}
+        H.close()
+    net.close()
+    out["speedup_learned_fp32_vs_fp64"] = out["fp64"]["seconds"] / out["learned_fp32"]["seconds"]
+    out["speedup_fp32_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_defect_correction"]["seconds"]
+    return out
+
+
+def c3_headline(args, torch, dist, rank, world, dev, stream):
+    import numpy as np
+    import hpb
+    from hpb import multigrid as MG
+    from hpb._lib import check
+    t0 = time.perf_counter()
+    H = MG.build(c3_factory, n=C3_N, p=C3_P, hlevels=3, stream=ctypes.c_void_p(stream.cuda_stream))
+    setup_s = time.perf_counter() - t0
+    fine, pr = H.levels[0], H.probs[0]
+    lib = fine.lib
+    ns = pr.phys.nstage
+    if args.elem:
+        fine.element_kernel(args.elem)
+    check(lib.hp_gpu_setup_preconditioner(fine.h), "setup_preconditioner")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    timed = timed_factory(torch, flush)
+    rsdl = lambda: check(lib.hp_gpu_enqueue_rsdl(fine.h, ns), "rsdl")
+    elem = lambda: check(lib.hp_gpu_enqueue_element_rsdl(fine.h, ns), "element_rsdl")
+    for _ in range(max(3, args.warmup)):
+        rsdl()
+    torch.cuda.synchronize()
+    clk_file = os.path.join(ROOT, f"_clocks_{rank}.csv")
+    clk = sample_clocks(None, clk_file)
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms = timed(rsdl, args.steps, stream)
+    if dist:
+        dist.barrier()
+    t_ms = sum(step_ms)
+    k_ms = sum(timed(elem, args.steps, stream)) / args.steps
+    if clk:
+        clk.terminate()
+        clk.wait()
+    clocks = parse_clocks(clk_file, dev)
+    try:
+        os.remove(clk_file)
+    except OSError:
+        pass
+    peak = ctypes.c_double()
+    lib.hp_tet_fp64_mma_peak.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    check(lib.hp_tet_fp64_mma_peak(dev, 200.0, ctypes.byref(peak)), "fp64 mma peak")
+    # e2e through the C-ABI with host buffers (pinned): upload the state, rsdl, download
+    # the residual, every step
+    hv, hs, hi, rv, rs, ri = (torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy()
+                              for a in (pr.ugv, pr.ugs, pr.ugi) * 2)
+    hv[...] = pr.ugv; hs[...] = pr.ugs; hi[...] = pr.ugi
+    P_ = hpb._lib.ptr
+    e2e_steps = max(3, min(args.steps, 10))
+    for k in range(e2e_steps + 2):
+        if k == 2:
+            torch.cuda.synchronize()
+            te = time.perf_counter()
+        check(lib.hp_gpu_upload_state(fine.h, P_(hv), P_(hs), P_(hi)), "upload")
+        check(lib.hp_gpu_rsdl(fine.h, ns, 0), "rsdl")
+        check(lib.hp_gpu_download_residual(fine.h, P_(rv), P_(rs), P_(ri)), "download")
+    e2e_s = (time.perf_counter() - te) / e2e_steps
+    io_bytes = hv.nbytes + hs.nbytes + hi.nbytes
+    m = pr.mesh
+    ndof = pr.ndof
+    H.close()
+    value, e2e, t_ms, e2e_s = replica_totals(dist, world, ndof, args.steps, t_ms, e2e_s, "cuda")
+    tol = c3_time_to_tol(hpb, dev, stream) if (world == 1 and not args.no_tol) else None
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    fl_el, fl_src = ins_flops_per_element(C3_P)
+    fl = fl_el * m.ntri
+    achieved = fl / (k_ms * 1e-3) / 1e12
+    comp_bytes = 16 * ndof + 36 * m.ntri + 16 * m.npnt
+    peaks = load_peaks()
+    hbm = peaks.get("hbm_gbs")
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs (measured)"
+    if hbm is None:
+        hbm, hbm_src = 6650.0, "fallback 6.65 TB/s (no measured peak file)"
+    traffic = None
+    try:  # DRAM bytes per triangle of the element kernel from an ncu capture, scaled to this launch
+        tr = json.load(open(os.path.join(ROOT, "profiles", "k_rsdl_elem_ins_p6_traffic.json")))
+        traffic = tr["dram_bytes_per_triangle"] * m.ntri
+    except Exception:
+        pass
+    cpu = None
+    if world == 1:
+        cv, reps = run_cpu_strips(1, 0, 1, secs=10.0)
+        cpu = {"value": cv, "unit": "GDoF/s", "cores": 1, "kind": "port",
+               "sample": f"oracle rsdl(nstage) on a 512 x {STRIP_ROWS}-square strip of the C3 mesh "
+                         f"({2 * C3_N * STRIP_ROWS} triangles, p={C3_P}, lid-cavity state), {reps} evaluations "
+                         "in 10 s, 1 core"}
+    launches_per_step = 4  # k_rsdl_pre, k_rsdl_elem, k_rsdl_fold, k_bdry_flux_ins
+    line = {
+        "metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": c3_config(),
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                     "frac": achieved / peak.value, "traffic": traffic, "kernel": "element residual (fine level)",
+                     "kernel_ms": k_ms, "flops_per_element": fl_el, "flops_source": fl_src,
+                     "peak_source": "FP64 tensor-core (DMMA) rate measured in this run by hp_tet_fp64_mma_peak "
+                                    "(MEASURED_PEAKS.json has no FP64 figure)",
+                     "hbm": {"compulsory_bytes": comp_bytes, "achieved_gbs": comp_bytes / (k_ms * 1e-3) / 1e9,
+                             "peak_gbs": hbm, "frac": comp_bytes / (k_ms * 1e-3) / 1e9 / hbm,
+                             "peak_source": hbm_src,
+                             "bytes": "16 NDOF + 36 ntri + 16 npnt (state read, residual written, "
+                                      "connectivity, coordinates)"}},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e, "unit": "GDoF/s", "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+        "gpu_launches": launches_per_step * args.steps,
+        "time_to_tol": tol, "ndof": ndof, "host_setup_seconds": setup_s, "clocks": clocks,
+        "element_kernel": args.elem or "tensor",
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", choices=["c3", "cd"], default="c3",
+                    help="c3 (default): the C3 ins p = 6 line; cd: the cd p = 4 line with stored element operators")
+    ap.add_argument("--no-tol", action="store_true", help="skip the time-to-tolerance legs (profiling runs)")
+    ap.add_argument("--elem", choices=["tensor", "scalar"], default=None,
+                    help="FP64 ins element kernel of the timed fine level (default: the library's, tensor)")
     ap.add_argument("--mesh", type=int, default=N_MESH,
                     help="split-square mesh size n (2 n^2 triangles); smaller cases are for profiler runs")
     ap.add_argument("--quick", action="store_true",
@@ -583,7 +872,7 @@ def main():
                     help="run `steps` multistage updates of the workload in FP64 or FP32 (for profiler runs)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="with --sweep c4: edge-length scale of the channel mesh (1: ~150k triangles)")
-    ap.add_argument("--sweep", choices=["c2", "c3", "c4", "c5"], default=None,
+    ap.add_argument("--sweep", choices=["c2", "c3", "c4", "c5", "kernels"], default=None,
                     help="c2: cd on the seeded 200k-triangle Delaunay mesh, p = 2, 4, 6, 8: rsdl GDoF/s and time "
                          "to a 1e-10 drop, plain FP64 vs FP32 defect correction (one JSON line per p); "
                          "c3: ins lid-driven cavity Re 400, p = 6, 512x512 split squares, V-cycles for --steps "
@@ -609,14 +898,25 @@ def main():
         if rank != 0:
             return
         cores = os.cpu_count() or 1
-        secs = 10.0
-        v, n = run_cpu(cores, secs)
+        if args.workload == "cd":
+            v, n = run_cpu(cores, 10.0)
+            line = {"impl": "reference", "metric": METRIC_CD, "value": v, "unit": "GDoF/s", "n_gpus": args.gpus,
+                    "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+                    "cpu_baseline": {"value": v, "unit": "GDoF/s", "cores": cores, "kind": "port",
+                                     "sample": f"oracle rsdl(nstage) on a {n}x{n} split-square mesh, p={P}, "
+                                               "10 s per core, one process per core"},
+                    "e2e": {"value": v, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line))
+            return
+        v, reps = run_cpu_strips(cores, args.steps, args.warmup)
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GDoF/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(),
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": c3_config(),
                 "cpu_baseline": {"value": v, "unit": "GDoF/s", "cores": cores, "kind": "port",
-                                 "sample": f"oracle rsdl(nstage) on a {n}x{n} split-square mesh, p={P}, "
-                                           f"{secs:.0f} s per core, one process per core"},
+                                 "sample": f"each step: the oracle's rsdl(nstage) on {cores} strips of the C3 mesh "
+                                           f"at once (512 x {STRIP_ROWS} squares, {2 * C3_N * STRIP_ROWS} triangles, "
+                                           f"p={C3_P}, lid-cavity state), one process per core"},
                 "e2e": {"value": v, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -637,6 +937,14 @@ def main():
     stream = torch.cuda.Stream()  # a non-default stream: the update graph is captured on it
     torch.cuda.set_stream(stream)
 
+    if args.sweep is None and args.workload == "c3" and not (args.quick or args.profile):
+        c3_headline(args, torch, dist, rank, world, dev, stream)
+        return
+    if args.sweep == "kernels":
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+        kernel_sweep(hpb, dev, args.mesh if args.mesh != N_MESH else 256, args.p or list(range(1, 9)), args.steps,
+                     timed_factory(torch, flush), stream)
+        return
     if args.sweep == "c2":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         c2_sweep(hpb, dev, args.mesh, args.p or [2, 4, 6, 8], args.steps, timed_factory(torch, flush))
@@ -760,12 +1068,12 @@ def main():
     P_ = hpb._lib.ptr
     for _ in range(2):
         lib.hp_gpu_upload_state(lvl.h, P_(hv), P_(hs), P_(hi))
-        lib.hp_gpu_rsdl(lvl.h, ns)
+        lib.hp_gpu_rsdl(lvl.h, ns, 0)
         lib.hp_gpu_download_residual(lvl.h, P_(rv), P_(rs), P_(ri))
     t0 = time.perf_counter()
     for _ in range(args.steps):
         hpb._lib.check(lib.hp_gpu_upload_state(lvl.h, P_(hv), P_(hs), P_(hi)), "upload")
-        hpb._lib.check(lib.hp_gpu_rsdl(lvl.h, ns), "rsdl")
+        hpb._lib.check(lib.hp_gpu_rsdl(lvl.h, ns, 0), "rsdl")
         hpb._lib.check(lib.hp_gpu_download_residual(lvl.h, P_(rv), P_(rs), P_(ri)), "download")
     e2e_s = (time.perf_counter() - t0) / args.steps
     io_bytes = hv.nbytes + hs.nbytes + hi.nbytes
@@ -812,7 +1120,7 @@ def main():
                                 f"({build_ms:.1f} ms, {2 * op_bytes / 1e9:.2f} GB FP64 + FP32 copy), "
                                 "outside the timed steps")
     line = {
-        "metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC_CD, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,

@@ -1,0 +1,372 @@
+// FP64 ins element residual on the tensor cores (straight triangles).
+//
+// tri_hp::rsdl's element loop (tri_hp/nstage.cpp:52-73: ugtouht, element_rsdl, lftog)
+// with tri_hp_ins::element_rsdl's straight-element branch (tri_hp/ins/rsdl.cpp:259-433)
+// and the tri_basis operators it calls (proj.cpp:22-119, intgrt.cpp:81-158,
+// derivr / derivs proj.cpp:339-402). One warp takes two triangles; the 8 rows of a
+// DMMA fragment (mma.m8n8k4.f64) are (triangle, variable) pairs, variable slot 3
+// unused:
+//   projection  C[8 x GG] = U[8 x T] * Op^T[T x GG]   for Op = value, d/dr, d/ds
+//   intgrtrs    C[8 x T]  = F[8 x 2GG] * W[2GG x T]   (F = [flux_r | flux_s] at the points)
+// The operators are the sum-factorised proj / intgrtrs written out per point (dense),
+// built on the host from the basis tables and stored in fragment order (one coalesced
+// 8-byte read-only load per lane per MMA). Pointwise fluxes, the strong residual
+// (derivr / derivs) and the SUPG terms stay scalar, lanes owning (triangle, point)
+// pairs, on per-warp shared-memory arrays. Vertex and side residuals go to the
+// assembly-by-gather buffers (State::elim / elre) or, without them, FP64 atomics;
+// interior residuals are written directly.
+#pragma once
+#include "hp_kernels.cuh"
+
+namespace hpb {
+
+template <int P>
+struct InsMma {
+    static constexpr int G = P + 1, GG = G * G, X = P + 2, T = (P + 1) * (P + 2) / 2, SM = P - 1,
+                         IM = (P - 1) * (P - 2) / 2, BM = 3 * P, NV = 3;
+    static constexpr int KS = (T + 3) / 4;        // projection k-steps
+    static constexpr int NT = (GG + 7) / 8;       // projection n-tiles
+    static constexpr int KS2 = (2 * GG + 3) / 4;  // intgrtrs k-steps
+    static constexpr int NT2 = (T + 7) / 8;       // intgrtrs n-tiles
+    // flux-pair stride: [flux_r (GG) | flux_s (GG) | zeros], 4 (mod 16) doubles so that the
+    // 4 variable rows a half-warp reads in one A-fragment load fall on distinct banks
+    static constexpr int pad4(int x) { return x + ((4 - x % 16) + 16) % 16; }
+    static constexpr int VS = pad4(KS2 * 4);
+    static constexpr int QP = NT * 8 + 4;  // point-array stride
+    // per triangle: PV [3][QP] u, v, p; PD [4][QP] du/dr, dv/dr, du/ds, dv/ds (the gathered
+    // modes [4][T] before the projection, the strong residual [3][QP] after the fluxes);
+    // FI [3][VS] imaginary flux pairs; FR [3][VS] real flux pairs
+    static constexpr int S_EL = 7 * QP + 6 * VS;
+    static constexpr int WPC = 4;                  // warps per CTA
+    static constexpr int MINB = P <= 4 ? 4 : 3;    // CTAs per SM the register budget allows
+    static constexpr int NG = NT < 8 ? NT : 8;     // projection n-tiles accumulated together
+    static constexpr size_t PROJ_LEN = (size_t)3 * NT * KS * 32, INT_LEN = (size_t)NT2 * KS2 * 32;
+    static_assert(4 * T <= 4 * QP, "gathered modes must fit the PD block");
+};
+
+// The 1D derivative tables of derivr / derivs and the collapsed-coordinate factors.
+template <typename R, int P>
+struct InsSmall {
+    R dltx[P + 1], dltx1[P + 1][P + 1], dltn[P + 1], dltn1[P + 1][P + 1], dltn2[P + 1][P + 1];
+    R n0[P + 1], x0[P + 1];
+};
+template <int P>
+using InsMmaSmall = InsSmall<double, P>;
+template <int P>
+using InsMmaSmallF = InsSmall<float, P>;
+
+__device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <int P>
+__global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
+    k_rsdl_ins_mma(const double *__restrict__ projB, const double *__restrict__ intB, InsMmaSmall<P> small,
+                   Mesh mesh, State<double> st, Phys ph, int stage, int zero_rr) {
+    using M = InsMma<P>;
+    constexpr int G = M::G, GG = M::GG, T = M::T, BM = M::BM, IM = M::IM, NV = 3, QP = M::QP, VS = M::VS;
+    constexpr int SM = (M::SM > 0 ? M::SM : 1);  // side-mode stride (unused when p = 1)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    InsMmaSmall<P> &tb = *reinterpret_cast<InsMmaSmall<P> *>(smem_raw);
+    {
+        const int n4 = sizeof(InsMmaSmall<P>) / 4;
+        const int *src = reinterpret_cast<const int *>(&small);
+        int *dst = reinterpret_cast<int *>(smem_raw);
+        for (int k = threadIdx.x; k < n4; k += blockDim.x) dst[k] = src[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grow = lane >> 2, gcol = lane & 3;
+    const int re_ = grow >> 2, rv = grow & 3;  // fragment row -> (triangle, variable)
+    double *base = reinterpret_cast<double *>(smem_raw + ((sizeof(InsMmaSmall<P>) + 15) / 16) * 16) +
+                   (size_t)warp * 2 * M::S_EL;
+    auto PV = [&](int e) { return base + e * M::S_EL; };
+    auto PD = [&](int e) { return base + e * M::S_EL + 3 * QP; };
+    auto FI = [&](int e) { return base + e * M::S_EL + 7 * QP; };
+    auto FR = [&](int e) { return base + e * M::S_EL + 7 * QP + 3 * VS; };
+    // the K padding of the flux pairs stays zero (their B rows are zero too)
+    for (int e = 0; e < 2; ++e)
+        for (int k = 2 * GG + lane; k < VS; k += 32)
+            for (int v = 0; v < 3; ++v) FI(e)[v * VS + k] = FR(e)[v * VS + k] = 0.0;
+    __syncthreads();
+    const double beta = ph.beta[stage];
+    const double omb = zero_rr ? 0.0 : 1.0 - beta;
+    const double rho = ph.rho, mu = ph.mu;
+    const long ntri = mesh.ntri, npair = (ntri + 1) / 2;
+    for (long pr = (long)blockIdx.x * M::WPC + warp; pr < npair; pr += (long)gridDim.x * M::WPC) {
+        const int t0 = (int)(2 * pr);
+        const bool has1 = t0 + 1 < ntri;
+        // triangle e (0, 1) of the pair and whether it is done here (curved triangles are
+        // done by the curved launch; a missing second triangle repeats the first, unwritten).
+        // Per-triangle values are selected, not indexed, so that they stay in registers.
+        const int ta = t0, tb1 = has1 ? t0 + 1 : t0;
+        const bool acta = !mesh.tri_cv || mesh.tri_cv[ta] < 0;
+        const bool actb = has1 && (!mesh.tri_cv || mesh.tri_cv[tb1] < 0);
+        auto TE = [&](int e) { return e ? tb1 : ta; };
+        auto ACT = [&](int e) { return e ? actb : acta; };
+        __syncwarp();
+        // ---- gather (ugtouht, gtol.cpp:14-55) into the PD block
+        constexpr int NGATH = (2 * NV * T + 31) / 32;
+#pragma unroll
+        for (int k = 0; k < NGATH; ++k) {
+            const int w = lane + 32 * k;
+            if (w >= 2 * NV * T) break;
+            const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
+            double val = 0.0;
+            if (ACT(e)) {
+                const int t = TE(e);
+                if (m < 3) {
+                    val = st.ugv[mesh.tri_pnt[3 * t + m] * NV + n];
+                } else if (m < BM) {
+                    const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
+                    val = st.ugs[(mesh.tri_seg[3 * t + i] * SM + kk) * NV + n];
+                    if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
+                } else {
+                    val = st.ugi[((size_t)t * IM + (m - BM)) * NV + n];
+                }
+            }
+            PD(e)[n * T + m] = val;
+        }
+        // geometry of both triangles: ldcrd(n,0) = (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2, and the
+        // inscribed-radius length scale of the SUPG tau (tri_mesh/tprims.cpp:224-241)
+        double gd[2][4], hh[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int t = TE(e);
+            const int p0 = mesh.tri_pnt[3 * t], p1 = mesh.tri_pnt[3 * t + 1], p2 = mesh.tri_pnt[3 * t + 2];
+            const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
+            const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
+            const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
+            gd[e][0] = 0.5 * (x2d - x1d); gd[e][1] = 0.5 * (x0d - x1d);
+            gd[e][2] = 0.5 * (y2d - y1d); gd[e][3] = 0.5 * (y0d - y1d);
+            const double dx1 = x0d - x2d, dy1 = y0d - y2d, dx2 = x1d - x0d, dy2 = y1d - y0d;
+            const double area = dx1 * dy2 - dy1 * dx2;
+            const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
+                                 sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
+            hh[e] = (area / perim) / (0.25 * (P + 1) * (P + 1));
+        }
+        __syncwarp();
+        // ---- projection on the tensor cores (proj.cpp:22-119 as dense per-point operators)
+        {
+            double a[M::KS];
+#pragma unroll
+            for (int ks = 0; ks < M::KS; ++ks) {
+                const int m = ks * 4 + gcol;
+                a[ks] = (rv < 3 && m < T) ? PD(re_)[rv * T + m] : 0.0;
+            }
+            __syncwarp();  // the gathered modes are dead: PD takes the derivatives
+            const int nop = beta > 0.0 ? 3 : 1;  // derivatives feed the viscous (real) part only
+            for (int op = 0; op < nop; ++op) {
+                double *dst = op == 0 ? (rv < 3 ? PV(re_) + rv * QP : nullptr)
+                                      : (rv < 2 ? PD(re_) + ((op - 1) * 2 + rv) * QP : nullptr);
+#pragma unroll
+                for (int nt0 = 0; nt0 < M::NT; nt0 += M::NG) {
+                    double c[M::NG][2];
+#pragma unroll
+                    for (int g = 0; g < M::NG; ++g) c[g][0] = c[g][1] = 0.0;
+                    const double *b = projB + ((size_t)(op * M::NT + nt0) * M::KS) * 32 + lane;
+#pragma unroll
+                    for (int ks = 0; ks < M::KS; ++ks)
+#pragma unroll
+                        for (int g = 0; g < M::NG; ++g)
+                            if (nt0 + g < M::NT) dmma884(c[g][0], c[g][1], a[ks], __ldg(b + ((size_t)g * M::KS + ks) * 32));
+                    if (dst) {
+#pragma unroll
+                        for (int g = 0; g < M::NG; ++g)
+                            if (nt0 + g < M::NT) {
+                                const int q = (nt0 + g) * 8 + gcol * 2;
+                                dst[q] = c[g][0];
+                                dst[q + 1] = c[g][1];
+                            }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        // ---- pointwise fluxes (ins/rsdl.cpp:259-340), lanes own (triangle, point)
+        for (int w = lane; w < 2 * GG; w += 32) {
+            const int e = w / GG, q = w - e * GG;
+            const double d00 = e ? gd[1][0] : gd[0][0], d01 = e ? gd[1][1] : gd[0][1];
+            const double d10 = e ? gd[1][2] : gd[0][2], d11 = e ? gd[1][3] : gd[0][3];
+            const double u0 = PV(e)[q], u1 = PV(e)[QP + q], pp = PV(e)[2 * QP + q];
+            const double fluxx = rho * u0, fluxy = rho * u1;
+            const double m0 = +d11 * fluxx - d01 * fluxy;
+            const double m1 = -d10 * fluxx + d00 * fluxy;
+            double *fi = FI(e);
+            fi[q] = u0 * m0 + d11 * pp;
+            fi[GG + q] = u0 * m1 - d10 * pp;
+            fi[VS + q] = u1 * m0 - d01 * pp;
+            fi[VS + GG + q] = u1 * m1 + d00 * pp;
+            fi[2 * VS + q] = m0;
+            fi[2 * VS + GG + q] = m1;
+            if (beta > 0.0) {
+                const double dr0 = PD(e)[q], dr1 = PD(e)[QP + q], ds0 = PD(e)[2 * QP + q], ds1 = PD(e)[3 * QP + q];
+                const double cjcb = d00 * d11 - d10 * d01;
+                const double cjcbi = mu / cjcb;
+                const double v0000 = -cjcbi * (2. * d11 * d11 + d01 * d01);
+                const double v0011 = -cjcbi * (2. * d10 * d10 + d00 * d00);
+                const double v0001 = cjcbi * (2. * d11 * d10 + d01 * d00);
+                const double v1100 = -cjcbi * (d11 * d11 + 2. * d01 * d01);
+                const double v1111 = -cjcbi * (d10 * d10 + 2. * d00 * d00);
+                const double v1101 = cjcbi * (d11 * d10 + 2. * d01 * d00);
+                const double v0100 = cjcbi * d01 * d11;
+                const double v0111 = cjcbi * d00 * d10;
+                const double v0101 = -cjcbi * d01 * d10;
+                const double v0110 = -cjcbi * d00 * d11;
+                double *fr = FR(e);
+                fr[q] = v0000 * dr0 + v0100 * dr1 + v0001 * ds0 + v0101 * ds1;
+                fr[GG + q] = v0001 * dr0 + v0110 * dr1 + v0011 * ds0 + v0111 * ds1;
+                fr[VS + q] = v0100 * dr0 + v1100 * dr1 + v0110 * ds0 + v1101 * ds1;
+                fr[VS + GG + q] = v0101 * dr0 + v1101 * dr1 + v0111 * ds0 + v1111 * ds1;
+            }
+        }
+        __syncwarp();
+        // imaginary part -> res (intgrt.cpp:81-158 with the minus sign of the weak divergence)
+        {
+            const double *arow = FI(re_) + (rv < 3 ? rv : 2) * VS;
+            double c[M::NT2][2];
+#pragma unroll
+            for (int nt = 0; nt < M::NT2; ++nt) c[nt][0] = c[nt][1] = 0.0;
+#pragma unroll 5
+            for (int ks = 0; ks < M::KS2; ++ks) {
+                const double a = arow[ks * 4 + gcol];
+#pragma unroll
+                for (int nt = 0; nt < M::NT2; ++nt) dmma884(c[nt][0], c[nt][1], a, __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane));
+            }
+            if (rv < 3 && ACT(re_)) {
+                const int t = TE(re_);
+#pragma unroll
+                for (int nt = 0; nt < M::NT2; ++nt)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int m = nt * 8 + gcol * 2 + h;
+                        if (m >= T) continue;
+                        double val = c[nt][h];
+                        if (m < BM) {
+                            int v = -1, gsi = 0;
+                            if (m < 3) {
+                                v = mesh.tri_pnt[3 * t + m];
+                            } else {
+                                const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
+                                if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
+                                gsi = (mesh.tri_seg[3 * t + i] * SM + kk) * NV + rv;
+                            }
+                            if (st.elim) st.elim[((size_t)t * BM + m) * NV + rv] = val;
+                            else if (v >= 0) atomicAdd(&st.resv[v * NV + rv], val);
+                            else atomicAdd(&st.ress[gsi], val);
+                        } else {
+                            const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
+                            const double src = st.dresi ? st.dresi[gi] : 0.0;
+                            if (beta > 0.0) st.resi[gi] = val + src;
+                            else st.resi[gi] = val + st.rri[gi] * omb + src;  // res_r unchanged when beta = 0
+                        }
+                    }
+            }
+        }
+        if (beta > 0.0) {
+            // ---- strong residual at the points (derivr / derivs, proj.cpp:339-402) into PD
+            for (int w = lane; w < 2 * GG; w += 32) {
+                const int e = w / GG, q = w - e * GG, i = q / G, j = q - i * G;
+                const double *fi = FI(e), *fre = FR(e);
+                const double ln0 = tb.n0[j];
+#pragma unroll
+                for (int n = 0; n < NV; ++n) {
+                    // full fluxes: convective + pressure + viscous (u, v); the mass flux (p)
+                    auto fr_ = [&](int qq) { return n < 2 ? fi[n * VS + qq] + fre[n * VS + qq] : fi[2 * VS + qq]; };
+                    auto fs_ = [&](int qq) {
+                        return n < 2 ? fi[n * VS + GG + qq] + fre[n * VS + GG + qq] : fi[2 * VS + GG + qq];
+                    };
+                    double acc = 0.0;  // rhorbd0 * u + dugdt with bd(0) = 0
+                    {
+                        const double wi = fr_(i * G + j) * tb.dltx[i] * ln0;
+#pragma unroll
+                        for (int qq = 0; qq < G; ++qq)
+                            if (qq != i) acc += (wi + fr_(qq * G + j) * tb.dltx[qq] * ln0) * tb.dltx1[i][qq];
+                    }
+                    {
+                        const double fsij = fs_(i * G + j);
+                        const double wi = fsij * tb.dltx[i] * ln0;
+#pragma unroll
+                        for (int qq = 0; qq < G; ++qq)
+                            if (qq != i) acc += (wi + fs_(qq * G + j) * tb.dltx[qq] * ln0) * tb.dltn1[i][qq];
+                        const double wj = fsij * tb.dltn[j];
+#pragma unroll
+                        for (int qq = 0; qq < G; ++qq)
+                            if (qq != j) acc += (wj + fs_(i * G + qq) * tb.dltn[qq]) * tb.dltn2[j][qq];
+                    }
+                    PD(e)[n * QP + q] = acc;
+                }
+            }
+            __syncwarp();
+            // ---- pointwise SUPG terms (ins/rsdl.cpp:341-431, CALC_TAU2)
+            const double nu = mu / rho;
+            for (int w = lane; w < 2 * GG; w += 32) {
+                const int e = w / GG, q = w - e * GG;
+                const double d00 = e ? gd[1][0] : gd[0][0], d01 = e ? gd[1][1] : gd[0][1];
+                const double d10 = e ? gd[1][2] : gd[0][2], d11 = e ? gd[1][3] : gd[0][3];
+                const double he = e ? hh[1] : hh[0];
+                const double cjcb = d00 * d11 - d10 * d01;
+                const double u0 = PV(e)[q], u1 = PV(e)[QP + q];
+                const double qv = u0 * u0 + u1 * u1;
+                const double t2 = 2. * nu / he;
+                double gam = 3.0 * qv + t2 * t2;
+                if (ph.mu + ph.bd0 == 0.0) gam = (gam > 0.1 ? gam : 0.1);
+                const double tau0 = ph.adis * he / (cjcb * sqrt(gam));
+                const double tau2 = sqrt(qv) * tau0;
+                const double tr0 = tau0 * PD(e)[q], tr1 = tau0 * PD(e)[QP + q], tr2 = tau2 * PD(e)[2 * QP + q];
+                double *fr = FR(e);
+                fr[q] -= (d11 * (2. * u0) - d01 * u1) * tr0 - d01 * u0 * tr1 + d11 * tr2;
+                fr[GG + q] -= (-d10 * (2. * u0) + d00 * u1) * tr0 + d00 * u0 * tr1 - d10 * tr2;
+                fr[VS + q] -= +d11 * u1 * tr0 + (d11 * u0 - d01 * (2. * u1)) * tr1 - d01 * tr2;
+                fr[VS + GG + q] -= -d10 * u1 * tr0 + (-d10 * u0 + d00 * (2. * u1)) * tr1 + d00 * tr2;
+                fr[2 * VS + q] = -(d11 * tr0 - d01 * tr1);
+                fr[2 * VS + GG + q] = -(-d10 * tr0 + d00 * tr1);
+            }
+            __syncwarp();
+            // ---- real part: intgrtrs of the viscous + SUPG fluxes, x beta -> res_r
+            const double *arow = FR(re_) + (rv < 3 ? rv : 2) * VS;
+            double c[M::NT2][2];
+#pragma unroll
+            for (int nt = 0; nt < M::NT2; ++nt) c[nt][0] = c[nt][1] = 0.0;
+#pragma unroll 5
+            for (int ks = 0; ks < M::KS2; ++ks) {
+                const double a = arow[ks * 4 + gcol];
+#pragma unroll
+                for (int nt = 0; nt < M::NT2; ++nt) dmma884(c[nt][0], c[nt][1], a, __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane));
+            }
+            if (rv < 3 && ACT(re_)) {
+                const int t = TE(re_);
+#pragma unroll
+                for (int nt = 0; nt < M::NT2; ++nt)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int m = nt * 8 + gcol * 2 + h;
+                        if (m >= T) continue;
+                        double val = c[nt][h] * beta;
+                        if (m < BM) {
+                            int v = -1, gsi = 0;
+                            if (m < 3) {
+                                v = mesh.tri_pnt[3 * t + m];
+                            } else {
+                                const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
+                                if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
+                                gsi = (mesh.tri_seg[3 * t + i] * SM + kk) * NV + rv;
+                            }
+                            if (st.elre) st.elre[((size_t)t * BM + m) * NV + rv] = val;
+                            else if (v >= 0) atomicAdd(&st.rrv[v * NV + rv], val);
+                            else atomicAdd(&st.rrs[gsi], val);
+                        } else {
+                            const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
+                            const double rr = st.rri[gi] * omb + val;
+                            st.rri[gi] = rr;
+                            st.resi[gi] += rr;
+                        }
+                    }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace hpb

@@ -1,0 +1,391 @@
+// FP32 ins element residual on the tensor cores (TF32 mma.m16n8k8, FP32 accumulation),
+// straight triangles, plain or correction form.
+//
+// The FP32 smoother of the defect correction evaluates the residual in correction form
+// R(b + d) - R(b) + R64(u) about the base state b = fp32(u) (tri_hp::mg_source's shape,
+// tri_hp/nstage.cpp:113-129, with R64 as the source): the convective and pressure fluxes
+// as exact differences F(b + d) - F(b), the viscous flux (linear) of d, the SUPG term with
+// the tau of the base. Same element loop and basis operators as the FP64 tensor-core
+// kernel (hp_elem_mma.cuh; tri_hp/ins/rsdl.cpp:259-433, proj.cpp:22-119,
+// intgrt.cpp:81-158, proj.cpp:339-402), four triangles per warp: the 16 rows of an
+// m16n8k8 fragment are (triangle, variable) pairs. The contractions round their
+// operands to TF32 (10-bit mantissa) and accumulate in FP32: the smoother's residual is
+// accurate to ~1e-3 relative, which the FP64 defect residual absorbs (the converged
+// state is the FP64 one). The base state's point values (u, v) are fixed for a whole
+// correction cycle and are read from State::bpt (k_base_points) instead of being
+// gathered and projected every residual.
+#pragma once
+#include "hp_kernels.cuh"
+
+namespace hpb {
+
+template <int P>
+struct InsTf32 {
+    static constexpr int G = P + 1, GG = G * G, T = (P + 1) * (P + 2) / 2, SM = P - 1,
+                         IM = (P - 1) * (P - 2) / 2, BM = 3 * P, NV = 3;
+    static constexpr int KS = (T + 7) / 8;        // projection k-steps
+    static constexpr int NT = (GG + 7) / 8;       // projection n-tiles
+    static constexpr int KS2 = (2 * GG + 7) / 8;  // intgrtrs k-steps
+    static constexpr int NT2 = (T + 7) / 8;       // intgrtrs n-tiles
+    // flux-pair stride 8 (mod 32) floats and triangle stride 4 (mod 32): the 32 A-fragment
+    // elements a warp loads at once (8 rows = 2 triangles x 4 variables, 4 columns) fall on
+    // distinct banks
+    static constexpr int pad_to(int x, int r) { return x + ((r - x % 32) + 32) % 32; }
+    static constexpr int VS = pad_to(KS2 * 8, 8);
+    static constexpr int QP = NT * 8;
+    static constexpr int S_EL = pad_to(7 * QP + 6 * VS, 4);
+    static constexpr int WPC = 4;
+    static constexpr int MINB = P <= 4 ? 4 : 3;
+    static constexpr int NG = NT < 8 ? NT : 8;
+    // B fragments: two floats per lane per MMA
+    static constexpr size_t PROJ_LEN = (size_t)3 * NT * KS * 64, INT_LEN = (size_t)NT2 * KS2 * 64;
+    static_assert(4 * T <= 4 * QP, "gathered modes must fit the PD block");
+};
+
+__device__ __forceinline__ unsigned f2tf32(float x) {
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], unsigned a0, unsigned a1, unsigned a2, unsigned a3, float2 b) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                 "{%8, %9}, {%0, %1, %2, %3};"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(__float_as_uint(b.x)), "r"(__float_as_uint(b.y)));
+}
+
+// Point values (u, v) of the base state b of every triangle, bpt [ntri][2][GG]: the
+// projection (proj.cpp:121-186 as dense sums) of the gathered base modes.
+template <int P>
+__global__ void k_base_points(const DevTables<float, P> *__restrict__ tb, Mesh mesh, const float *__restrict__ ubv,
+                              const float *__restrict__ ubs, const float *__restrict__ ubi, float *bpt) {
+    constexpr int G = P + 1, GG = G * G, T = (P + 1) * (P + 2) / 2, SM = (P > 1 ? P - 1 : 1),
+                  IM = (P - 1) * (P - 2) / 2, BM = 3 * P, NV = 3;
+    const long item = (long)blockIdx.x * blockDim.x + threadIdx.x;  // (triangle, variable)
+    if (item >= 2L * mesh.ntri) return;
+    const int t = (int)(item >> 1), n = (int)(item & 1);
+    float lin[T];
+#pragma unroll
+    for (int m = 0; m < T; ++m) {
+        float val;
+        if (m < 3) {
+            val = ubv[mesh.tri_pnt[3 * t + m] * NV + n];
+        } else if (m < BM) {
+            const int i = (m - 3) / SM, k = (m - 3) - i * SM;
+            val = ubs[(mesh.tri_seg[3 * t + i] * SM + k) * NV + n];
+            if ((k & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
+        } else {
+            val = ubi[((size_t)t * IM + (m - BM)) * NV + n];
+        }
+        lin[m] = val;
+    }
+    float *out = bpt + ((size_t)t * 2 + n) * GG;
+    for (int q = 0; q < GG; ++q) {
+        const int i = q / G, j = q - i * G;
+        float acc = 0.f;
+#pragma unroll
+        for (int m = 0; m < T; ++m) acc += lin[m] * tb->gn[j][m] * tb->gx[i][ModeCols<P>::col(m)];
+        out[q] = acc;
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
+    k_rsdl_ins_tf32(const float2 *__restrict__ projB, const float2 *__restrict__ intB, InsMmaSmallF<P> small,
+                    Mesh mesh, State<float> st, Phys ph, int stage, int zero_rr, int diff) {
+    using M = InsTf32<P>;
+    constexpr int G = M::G, GG = M::GG, T = M::T, BM = M::BM, IM = M::IM, NV = 3, QP = M::QP, VS = M::VS;
+    constexpr int SM = (M::SM > 0 ? M::SM : 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    InsMmaSmallF<P> &tb = *reinterpret_cast<InsMmaSmallF<P> *>(smem_raw);
+    {
+        const int n4 = sizeof(InsMmaSmallF<P>) / 4;
+        const int *src = reinterpret_cast<const int *>(&small);
+        int *dst = reinterpret_cast<int *>(smem_raw);
+        for (int k = threadIdx.x; k < n4; k += blockDim.x) dst[k] = src[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = lane >> 2, tig = lane & 3;
+    const int ra = grp >> 2, rv = grp & 3;  // fragment row grp -> (triangle ra, variable rv); row grp + 8 -> ra + 2
+    float *base = reinterpret_cast<float *>(smem_raw + ((sizeof(InsMmaSmallF<P>) + 15) / 16) * 16) +
+                  (size_t)warp * 4 * M::S_EL;
+    auto PV = [&](int e) { return base + e * M::S_EL; };
+    auto PD = [&](int e) { return base + e * M::S_EL + 3 * QP; };
+    auto FI = [&](int e) { return base + e * M::S_EL + 7 * QP; };
+    auto FR = [&](int e) { return base + e * M::S_EL + 7 * QP + 3 * VS; };
+    for (int e = 0; e < 4; ++e)
+        for (int k = 2 * GG + lane; k < VS; k += 32)
+            for (int v = 0; v < 3; ++v) FI(e)[v * VS + k] = FR(e)[v * VS + k] = 0.f;
+    __syncthreads();
+    const float beta = (float)ph.beta[stage];
+    const float omb = zero_rr ? 0.f : 1.f - beta;
+    const float rho = (float)ph.rho, mu = (float)ph.mu;
+    const bool corr = diff && st.bpt;
+    const long ntri = mesh.ntri, nquad = (ntri + 3) / 4;
+    for (long pr = (long)blockIdx.x * M::WPC + warp; pr < nquad; pr += (long)gridDim.x * M::WPC) {
+        const int t0 = (int)(4 * pr);
+        // triangle e of the quad (a missing one repeats the first, unwritten); curved
+        // triangles are done by the curved launch
+        unsigned actm = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (t0 + e < ntri && (!mesh.tri_cv || mesh.tri_cv[t0 + e] < 0)) actm |= 1u << e;
+        auto TE = [&](int e) { return t0 + e < ntri ? t0 + e : t0; };
+        auto ACT = [&](int e) { return (actm >> e) & 1u; };
+        __syncwarp();
+        // ---- gather the modes (ugtouht, gtol.cpp:14-55) into the PD block
+        for (int w = lane; w < 4 * NV * T; w += 32) {
+            const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
+            float val = 0.f;
+            if (ACT(e)) {
+                const int t = TE(e);
+                if (m < 3) {
+                    val = st.ugv[mesh.tri_pnt[3 * t + m] * NV + n];
+                } else if (m < BM) {
+                    const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
+                    val = st.ugs[(mesh.tri_seg[3 * t + i] * SM + kk) * NV + n];
+                    if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
+                } else {
+                    val = st.ugi[((size_t)t * IM + (m - BM)) * NV + n];
+                }
+            }
+            PD(e)[n * T + m] = val;
+        }
+        __syncwarp();
+        // ---- projection (TF32): A rows (triangle, variable), B = dense operators
+        {
+            unsigned a[M::KS][4];
+#pragma unroll
+            for (int ks = 0; ks < M::KS; ++ks) {
+                const int m0 = ks * 8 + tig, m1 = m0 + 4;
+                a[ks][0] = f2tf32((rv < 3 && m0 < T) ? PD(ra)[rv * T + m0] : 0.f);
+                a[ks][1] = f2tf32((rv < 3 && m0 < T) ? PD(ra + 2)[rv * T + m0] : 0.f);
+                a[ks][2] = f2tf32((rv < 3 && m1 < T) ? PD(ra)[rv * T + m1] : 0.f);
+                a[ks][3] = f2tf32((rv < 3 && m1 < T) ? PD(ra + 2)[rv * T + m1] : 0.f);
+            }
+            __syncwarp();
+            const int nop = beta > 0.f ? 3 : 1;
+            for (int op = 0; op < nop; ++op) {
+                float *d0, *d1;  // destination rows for triangles ra and ra + 2
+                if (op == 0) {
+                    d0 = rv < 3 ? PV(ra) + rv * QP : nullptr;
+                    d1 = rv < 3 ? PV(ra + 2) + rv * QP : nullptr;
+                } else {
+                    d0 = rv < 2 ? PD(ra) + ((op - 1) * 2 + rv) * QP : nullptr;
+                    d1 = rv < 2 ? PD(ra + 2) + ((op - 1) * 2 + rv) * QP : nullptr;
+                }
+#pragma unroll
+                for (int nt0 = 0; nt0 < M::NT; nt0 += M::NG) {
+                    float c[M::NG][4];
+#pragma unroll
+                    for (int g = 0; g < M::NG; ++g) c[g][0] = c[g][1] = c[g][2] = c[g][3] = 0.f;
+                    const float2 *b = projB + ((size_t)(op * M::NT + nt0) * M::KS) * 32 + lane;
+#pragma unroll
+                    for (int ks = 0; ks < M::KS; ++ks)
+#pragma unroll
+                        for (int g = 0; g < M::NG; ++g)
+                            if (nt0 + g < M::NT)
+                                mma_tf32(c[g], a[ks][0], a[ks][1], a[ks][2], a[ks][3], __ldg(b + ((size_t)g * M::KS + ks) * 32));
+                    if (d0) {
+#pragma unroll
+                        for (int g = 0; g < M::NG; ++g)
+                            if (nt0 + g < M::NT) {
+                                const int q = (nt0 + g) * 8 + tig * 2;
+                                d0[q] = c[g][0]; d0[q + 1] = c[g][1];
+                                d1[q] = c[g][2]; d1[q + 1] = c[g][3];
+                            }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        // ---- pointwise fluxes, lanes own (triangle, point)
+        for (int w = lane; w < 4 * GG; w += 32) {
+            const int e = w / GG, q = w - e * GG;
+            const int t = TE(e);
+            const int p0 = mesh.tri_pnt[3 * t], p1 = mesh.tri_pnt[3 * t + 1], p2 = mesh.tri_pnt[3 * t + 2];
+            const float d00 = (float)(0.5 * (mesh.pnts[2 * p2] - mesh.pnts[2 * p1]));
+            const float d01 = (float)(0.5 * (mesh.pnts[2 * p0] - mesh.pnts[2 * p1]));
+            const float d10 = (float)(0.5 * (mesh.pnts[2 * p2 + 1] - mesh.pnts[2 * p1 + 1]));
+            const float d11 = (float)(0.5 * (mesh.pnts[2 * p0 + 1] - mesh.pnts[2 * p1 + 1]));
+            const float u0 = PV(e)[q], u1 = PV(e)[QP + q], pp = PV(e)[2 * QP + q];
+            const float m0 = +d11 * (rho * u0) - d01 * (rho * u1);
+            const float m1 = -d10 * (rho * u0) + d00 * (rho * u1);
+            float c00, c01, c10, c11;
+            if (corr) {  // F(b + d) - F(b), products expanded
+                const float b0 = st.bpt[((size_t)t * 2) * GG + q], b1 = st.bpt[((size_t)t * 2 + 1) * GG + q];
+                const float mb0 = +d11 * (rho * b0) - d01 * (rho * b1);
+                const float mb1 = -d10 * (rho * b0) + d00 * (rho * b1);
+                const float uf0 = b0 + u0, uf1 = b1 + u1;
+                c00 = uf0 * m0 + u0 * mb0;
+                c01 = uf0 * m1 + u0 * mb1;
+                c10 = uf1 * m0 + u1 * mb0;
+                c11 = uf1 * m1 + u1 * mb1;
+            } else {
+                c00 = u0 * m0; c01 = u0 * m1; c10 = u1 * m0; c11 = u1 * m1;
+            }
+            float *fi = FI(e);
+            fi[q] = c00 + d11 * pp;
+            fi[GG + q] = c01 - d10 * pp;
+            fi[VS + q] = c10 - d01 * pp;
+            fi[VS + GG + q] = c11 + d00 * pp;
+            fi[2 * VS + q] = m0;
+            fi[2 * VS + GG + q] = m1;
+            if (beta > 0.f) {
+                const float dr0 = PD(e)[q], dr1 = PD(e)[QP + q], ds0 = PD(e)[2 * QP + q], ds1 = PD(e)[3 * QP + q];
+                const float cjcb = d00 * d11 - d10 * d01;
+                const float cjcbi = mu / cjcb;
+                const float v0000 = -cjcbi * (2.f * d11 * d11 + d01 * d01);
+                const float v0011 = -cjcbi * (2.f * d10 * d10 + d00 * d00);
+                const float v0001 = cjcbi * (2.f * d11 * d10 + d01 * d00);
+                const float v1100 = -cjcbi * (d11 * d11 + 2.f * d01 * d01);
+                const float v1111 = -cjcbi * (d10 * d10 + 2.f * d00 * d00);
+                const float v1101 = cjcbi * (d11 * d10 + 2.f * d01 * d00);
+                const float v0100 = cjcbi * d01 * d11;
+                const float v0111 = cjcbi * d00 * d10;
+                const float v0101 = -cjcbi * d01 * d10;
+                const float v0110 = -cjcbi * d00 * d11;
+                float *fr = FR(e);
+                fr[q] = v0000 * dr0 + v0100 * dr1 + v0001 * ds0 + v0101 * ds1;
+                fr[GG + q] = v0001 * dr0 + v0110 * dr1 + v0011 * ds0 + v0111 * ds1;
+                fr[VS + q] = v0100 * dr0 + v1100 * dr1 + v0110 * ds0 + v1101 * ds1;
+                fr[VS + GG + q] = v0101 * dr0 + v1101 * dr1 + v0111 * ds0 + v1111 * ds1;
+            }
+        }
+        __syncwarp();
+        // intgrtrs of a flux block (FI or FR) on the tensor cores, then lftog: vertex and
+        // side modes by FP32 atomics, interiors directly. part 0: imaginary -> res;
+        // part 1: real (x beta) -> res_r
+        auto integrate = [&](int part) {
+            const float *r0 = (part ? FR(ra) : FI(ra)) + (rv < 3 ? rv : 2) * VS;
+            const float *r1 = (part ? FR(ra + 2) : FI(ra + 2)) + (rv < 3 ? rv : 2) * VS;
+            float c[M::NT2][4];
+#pragma unroll
+            for (int nt = 0; nt < M::NT2; ++nt) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.f;
+#pragma unroll 4
+            for (int ks = 0; ks < M::KS2; ++ks) {
+                const int k = ks * 8 + tig;
+                const unsigned a0 = f2tf32(r0[k]), a1 = f2tf32(r1[k]), a2 = f2tf32(r0[k + 4]), a3 = f2tf32(r1[k + 4]);
+#pragma unroll
+                for (int nt = 0; nt < M::NT2; ++nt)
+                    mma_tf32(c[nt], a0, a1, a2, a3, __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane));
+            }
+            if (rv >= 3) return;
+#pragma unroll
+            for (int hh = 0; hh < 2; ++hh) {  // rows grp (triangle ra) and grp + 8 (triangle ra + 2)
+                const int e = ra + 2 * hh;
+                if (!ACT(e)) continue;
+                const int t = TE(e);
+#pragma unroll
+                for (int nt = 0; nt < M::NT2; ++nt)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int m = nt * 8 + tig * 2 + h;
+                        if (m >= T) continue;
+                        float val = c[nt][2 * hh + h];
+                        if (part) val *= beta;
+                        if (m < 3) {
+                            atomicAdd((part ? st.rrv : st.resv) + mesh.tri_pnt[3 * t + m] * NV + rv, val);
+                        } else if (m < BM) {
+                            const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
+                            if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
+                            atomicAdd((part ? st.rrs : st.ress) + (mesh.tri_seg[3 * t + i] * SM + kk) * NV + rv, val);
+                        } else {
+                            const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
+                            if (!part) {
+                                const float src = st.dresi ? st.dresi[gi] : 0.f;
+                                if (beta > 0.f) st.resi[gi] = val + src;
+                                else st.resi[gi] = val + st.rri[gi] * omb + src;
+                            } else {
+                                const float rr = st.rri[gi] * omb + val;
+                                st.rri[gi] = rr;
+                                st.resi[gi] += rr;
+                            }
+                        }
+                    }
+            }
+        };
+        integrate(0);
+        if (beta > 0.f) {
+            // ---- strong residual of the full fluxes at the points (derivr / derivs) into PD
+            for (int w = lane; w < 4 * GG; w += 32) {
+                const int e = w / GG, q = w - e * GG, i = q / G, j = q - i * G;
+                const float *fi = FI(e), *fre = FR(e);
+                const float ln0 = tb.n0[j];
+#pragma unroll
+                for (int n = 0; n < NV; ++n) {
+                    auto fr_ = [&](int qq) { return n < 2 ? fi[n * VS + qq] + fre[n * VS + qq] : fi[2 * VS + qq]; };
+                    auto fs_ = [&](int qq) {
+                        return n < 2 ? fi[n * VS + GG + qq] + fre[n * VS + GG + qq] : fi[2 * VS + GG + qq];
+                    };
+                    float acc = 0.f;
+                    {
+                        const float wi = fr_(i * G + j) * tb.dltx[i] * ln0;
+#pragma unroll
+                        for (int qq = 0; qq < G; ++qq)
+                            if (qq != i) acc += (wi + fr_(qq * G + j) * tb.dltx[qq] * ln0) * tb.dltx1[i][qq];
+                    }
+                    {
+                        const float fsij = fs_(i * G + j);
+                        const float wi = fsij * tb.dltx[i] * ln0;
+#pragma unroll
+                        for (int qq = 0; qq < G; ++qq)
+                            if (qq != i) acc += (wi + fs_(qq * G + j) * tb.dltx[qq] * ln0) * tb.dltn1[i][qq];
+                        const float wj = fsij * tb.dltn[j];
+#pragma unroll
+                        for (int qq = 0; qq < G; ++qq)
+                            if (qq != j) acc += (wj + fs_(i * G + qq) * tb.dltn[qq]) * tb.dltn2[j][qq];
+                    }
+                    PD(e)[n * QP + q] = acc;
+                }
+            }
+            __syncwarp();
+            // ---- SUPG with tau of the base state (correction form) or of the state (plain)
+            const float nu = (float)(ph.mu / ph.rho);
+            for (int w = lane; w < 4 * GG; w += 32) {
+                const int e = w / GG, q = w - e * GG;
+                const int t = TE(e);
+                const int p0 = mesh.tri_pnt[3 * t], p1 = mesh.tri_pnt[3 * t + 1], p2 = mesh.tri_pnt[3 * t + 2];
+                const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
+                const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
+                const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
+                const float d00 = (float)(0.5 * (x2d - x1d)), d01 = (float)(0.5 * (x0d - x1d));
+                const float d10 = (float)(0.5 * (y2d - y1d)), d11 = (float)(0.5 * (y0d - y1d));
+                const double dx1 = x0d - x2d, dy1 = y0d - y2d, dx2 = x1d - x0d, dy2 = y1d - y0d;
+                const double area = dx1 * dy2 - dy1 * dx2;
+                const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
+                                     sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
+                const float he = (float)((area / perim) / (0.25 * (P + 1) * (P + 1)));
+                const float cjcb = d00 * d11 - d10 * d01;
+                float u0 = PV(e)[q], u1 = PV(e)[QP + q], qv;
+                if (corr) {
+                    const float b0 = st.bpt[((size_t)t * 2) * GG + q], b1 = st.bpt[((size_t)t * 2 + 1) * GG + q];
+                    qv = b0 * b0 + b1 * b1;
+                    u0 += b0;
+                    u1 += b1;
+                } else {
+                    qv = u0 * u0 + u1 * u1;
+                }
+                const float t2 = 2.f * nu / he;
+                float gam = 3.0f * qv + t2 * t2;
+                if (ph.mu + ph.bd0 == 0.0) gam = (gam > 0.1f ? gam : 0.1f);
+                const float tau0 = (float)ph.adis * he / (cjcb * sqrtf(gam));
+                const float tau2 = sqrtf(qv) * tau0;
+                const float tr0 = tau0 * PD(e)[q], tr1 = tau0 * PD(e)[QP + q], tr2 = tau2 * PD(e)[2 * QP + q];
+                float *fr = FR(e);
+                fr[q] -= (d11 * (2.f * u0) - d01 * u1) * tr0 - d01 * u0 * tr1 + d11 * tr2;
+                fr[GG + q] -= (-d10 * (2.f * u0) + d00 * u1) * tr0 + d00 * u0 * tr1 - d10 * tr2;
+                fr[VS + q] -= +d11 * u1 * tr0 + (d11 * u0 - d01 * (2.f * u1)) * tr1 - d01 * tr2;
+                fr[VS + GG + q] -= -d10 * u1 * tr0 + (-d10 * u0 + d00 * (2.f * u1)) * tr1 + d00 * tr2;
+                fr[2 * VS + q] = -(d11 * tr0 - d01 * tr1);
+                fr[2 * VS + GG + q] = -(-d10 * tr0 + d00 * tr1);
+            }
+            __syncwarp();
+            integrate(1);
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace hpb

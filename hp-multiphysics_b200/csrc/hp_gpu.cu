@@ -2,6 +2,7 @@
 // stream-ordered launches of the element-residual / minvrt / update kernels, and
 // CUDA-graph capture of one multistage update.
 #include <cuda_runtime.h>
+#include <type_traits>
 #include <cstdio>
 #include <cstring>
 #include <cstdarg>
@@ -13,8 +14,11 @@
 #include <cstdint>
 
 #include "hp_gpu.h"
+#include "hp_host.h"
 #include "hp_mlp.h"
 #include "hp_kernels.cuh"
+#include "hp_elem_mma.cuh"
+#include "hp_elem_tf32.cuh"
 
 using namespace hpb;
 
@@ -86,6 +90,113 @@ void fill_tables(const hp_basis_tables &b, DevTables<R, P> &t) {
     t.colstart[X] = c;
 }
 
+// Dense per-point forms of tri_basis::proj (value, d/dr, d/ds; proj.cpp:22-119) and
+// intgrtrs (intgrt.cpp:81-158) for the tensor-core ins kernel, in DMMA fragment order
+// (B operand of mma.m8n8k4 .row.col: lane l holds B[k = l & 3][n = l >> 2]). Point
+// q = i * G + j (i along the x-direction Gauss points, j along eta). With c = the column
+// of mode m in the sum factorisation:
+//   value(q, m) = gn(j, m) gx(i, c)
+//   d/dr (q, m) = n0(j) gn(j, m) dgx(i, c)
+//   d/ds (q, m) = dgn(j, m) gx(i, c) + x0(i) d/dr(q, m)
+//   W_r(q, m)   = -dgxwtx(c, i) gnwtnn0(m, j)
+//   W_s(q, m)   = -(x0(i) dgxwtx(c, i) gnwtnn0(m, j) + gxwtx(c, i) dgnwtn(m, j))
+// so that lf(m) = sum_q flux_r(q) W_r(q, m) + flux_s(q) W_s(q, m) is intgrtrs' result.
+template <int P>
+void build_ins_mma(const hp_basis_tables &b, std::vector<double> &ops, InsMmaSmall<P> &sm) {
+    using M = InsMma<P>;
+    constexpr int G = M::G, GG = M::GG, T = M::T;
+    ops.assign(M::PROJ_LEN + M::INT_LEN, 0.0);
+    for (int op = 0; op < 3; ++op)
+        for (int nt = 0; nt < M::NT; ++nt)
+            for (int ks = 0; ks < M::KS; ++ks)
+                for (int l = 0; l < 32; ++l) {
+                    const int q = nt * 8 + (l >> 2), m = ks * 4 + (l & 3);
+                    if (q >= GG || m >= T) continue;
+                    const int i = q / G, j = q - i * G, c = ModeCols<P>::col(m);
+                    const double dr = b.n0[j] * b.gn[j][m] * b.dgx[i][c];
+                    const double v = op == 0 ? b.gn[j][m] * b.gx[i][c]
+                                             : (op == 1 ? dr : b.dgn[j][m] * b.gx[i][c] + b.x0[i] * dr);
+                    ops[((size_t)(op * M::NT + nt) * M::KS + ks) * 32 + l] = v;
+                }
+    double *ib = ops.data() + M::PROJ_LEN;
+    for (int nt = 0; nt < M::NT2; ++nt)
+        for (int ks = 0; ks < M::KS2; ++ks)
+            for (int l = 0; l < 32; ++l) {
+                const int k = ks * 4 + (l & 3), m = nt * 8 + (l >> 2);
+                if (k >= 2 * GG || m >= T) continue;
+                const int q = k % GG, i = q / G, j = q - i * G, c = ModeCols<P>::col(m);
+                const double w = k < GG ? -b.dgxwtx[c][i] * b.gnwtnn0[m][j]
+                                        : -(b.x0[i] * b.dgxwtx[c][i] * b.gnwtnn0[m][j] + b.gxwtx[c][i] * b.dgnwtn[m][j]);
+                ib[((size_t)nt * M::KS2 + ks) * 32 + l] = w;
+            }
+    for (int i = 0; i < G; ++i) {
+        sm.dltx[i] = b.dltx[i]; sm.dltn[i] = b.dltn[i]; sm.n0[i] = b.n0[i]; sm.x0[i] = b.x0[i];
+        for (int q = 0; q < G; ++q) {
+            sm.dltx1[i][q] = b.dltx1[i][q]; sm.dltn1[i][q] = b.dltn1[i][q]; sm.dltn2[i][q] = b.dltn2[i][q];
+        }
+    }
+}
+
+// TF32 rounding of an operator entry (round to nearest, ties away from zero, as
+// cvt.rna.tf32.f32 does for the A operands)
+float to_tf32(double v) {
+    float f = (float)v;
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    u = (u + 0x1000u) & 0xFFFFE000u;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// The same dense operators as build_ins_mma for the TF32 kernel (mma.m16n8k8 .row.col:
+// lane l holds B[k = l & 3][n = l >> 2] and B[k = (l & 3) + 4][n = l >> 2], stored as one
+// float2 per lane per MMA), rounded to TF32.
+template <int P>
+void build_ins_tf32(const hp_basis_tables &b, std::vector<float> &ops, InsMmaSmallF<P> &sm) {
+    using M = InsTf32<P>;
+    constexpr int G = M::G, GG = M::GG, T = M::T;
+    ops.assign(M::PROJ_LEN + M::INT_LEN, 0.f);
+    auto proj = [&](int op, int q, int m) -> double {
+        if (q >= GG || m >= T) return 0.0;
+        const int i = q / G, j = q - i * G, c = ModeCols<P>::col(m);
+        const double dr = b.n0[j] * b.gn[j][m] * b.dgx[i][c];
+        return op == 0 ? b.gn[j][m] * b.gx[i][c] : (op == 1 ? dr : b.dgn[j][m] * b.gx[i][c] + b.x0[i] * dr);
+    };
+    auto wgt = [&](int k, int m) -> double {
+        if (k >= 2 * GG || m >= T) return 0.0;
+        const int q = k % GG, i = q / G, j = q - i * G, c = ModeCols<P>::col(m);
+        return k < GG ? -b.dgxwtx[c][i] * b.gnwtnn0[m][j]
+                      : -(b.x0[i] * b.dgxwtx[c][i] * b.gnwtnn0[m][j] + b.gxwtx[c][i] * b.dgnwtn[m][j]);
+    };
+    for (int op = 0; op < 3; ++op)
+        for (int nt = 0; nt < M::NT; ++nt)
+            for (int ks = 0; ks < M::KS; ++ks)
+                for (int l = 0; l < 32; ++l) {
+                    const size_t at = (((size_t)(op * M::NT + nt) * M::KS + ks) * 32 + l) * 2;
+                    const int q = nt * 8 + (l >> 2), m = ks * 8 + (l & 3);
+                    ops[at] = to_tf32(proj(op, q, m));
+                    ops[at + 1] = to_tf32(proj(op, q, m + 4));
+                }
+    float *ib = ops.data() + M::PROJ_LEN;
+    for (int nt = 0; nt < M::NT2; ++nt)
+        for (int ks = 0; ks < M::KS2; ++ks)
+            for (int l = 0; l < 32; ++l) {
+                const size_t at = (((size_t)nt * M::KS2 + ks) * 32 + l) * 2;
+                const int k = ks * 8 + (l & 3), m = nt * 8 + (l >> 2);
+                ib[at] = to_tf32(wgt(k, m));
+                ib[at + 1] = to_tf32(wgt(k + 4, m));
+            }
+    for (int i = 0; i < G; ++i) {
+        sm.dltx[i] = (float)b.dltx[i]; sm.dltn[i] = (float)b.dltn[i];
+        sm.n0[i] = (float)b.n0[i]; sm.x0[i] = (float)b.x0[i];
+        for (int q = 0; q < G; ++q) {
+            sm.dltx1[i][q] = (float)b.dltx1[i][q];
+            sm.dltn1[i][q] = (float)b.dltn1[i][q];
+            sm.dltn2[i][q] = (float)b.dltn2[i][q];
+        }
+    }
+}
+
 template <typename R>
 void fill_minv(const hp_basis_tables &b, DevMinv<R> &m) {
     std::memset(&m, 0, sizeof(m));
@@ -138,6 +249,19 @@ struct Launchers {
                        const Tune &, cudaStream_t);
     void (*elem_jac)(const void *tab, const Mesh &, const State<R> &, const Phys &, R *K, R *rbar, int nsm,
                      cudaStream_t);
+    // FP64 ins only: the tensor-core element kernel (k_rsdl_ins_mma) with its operators
+    // (mma_build: dense operators in fragment order + the small derivative tables) and
+    // the curved elements through the scalar kernel
+    // (FP64: DMMA k_rsdl_ins_mma; FP32: TF32 k_rsdl_ins_tf32, plain or correction form)
+    void (*elem_mma)(const void *ops, const void *small, const void *tab, const Mesh &, const State<R> &,
+                     const Phys &, int stage, int zero_rr, int diff, int nsm, const Tune &, cudaStream_t);
+    void (*mma_build)(const hp_basis_tables &, std::vector<unsigned char> &ops, std::vector<unsigned char> &small);
+    // FP32 ins: the base state's point values for the correction form (State::bpt)
+    void (*base_pts)(const void *tab, const Mesh &, const State<R> &, R *bpt, cudaStream_t);
+    int bpt_per_elem;  // 2 GG
+    // tri_hp::l2error on the device (FP64): per-block partials into part
+    void (*l2err)(const void *tab, const double *wtn, const Mesh &, const State<R> &, int NV, const DevField &,
+                  double *part, int blocks, cudaStream_t);
 };
 
 template <typename R, int P, int PHYS>
@@ -253,11 +377,87 @@ struct LaunchImpl {
                      int fold, unsigned long long *slot, int th, cudaStream_t st) {
         k_minv_vert<R, NV><<<nblk(m.npnt, th), th, 0, st>>>(m, s, mt, sm, im, (R)cfla, upd, fold, slot);
     }
+    static constexpr bool HAS_MMA = PHYS == 1;
+    static constexpr bool DBL = std::is_same<R, double>::value;
+    static int mma_smem() {
+        if constexpr (DBL)
+            return (int)(((sizeof(InsMmaSmall<P>) + 15) / 16) * 16 + (size_t)2 * InsMma<P>::S_EL * InsMma<P>::WPC * 8);
+        else
+            return (int)(((sizeof(InsMmaSmallF<P>) + 15) / 16) * 16 + (size_t)4 * InsTf32<P>::S_EL * InsTf32<P>::WPC * 4);
+    }
+    static void elem_mma(const void *ops, const void *small, const void *tab, const Mesh &m, const State<R> &s,
+                         const Phys &ph, int stage, int zero_rr, int diff, int nsm, const Tune &tn, cudaStream_t st) {
+        if constexpr (HAS_MMA) {
+            if constexpr (DBL) {
+                using MM = InsMma<P>;
+                const double *o = static_cast<const double *>(ops);
+                const long npair = ((long)m.ntri + 1) / 2;
+                const int blocks = (int)std::min<long>((npair + MM::WPC - 1) / MM::WPC, (long)nsm * MM::MINB * 4);
+                k_rsdl_ins_mma<P><<<blocks, MM::WPC * 32, mma_smem(), st>>>(
+                    o, o + MM::PROJ_LEN, *static_cast<const InsMmaSmall<P> *>(small), m, s, ph, stage, zero_rr);
+            } else {
+                using MM = InsTf32<P>;
+                const float2 *o = static_cast<const float2 *>(ops);
+                const long nquad = ((long)m.ntri + 3) / 4;
+                const int blocks = (int)std::min<long>((nquad + MM::WPC - 1) / MM::WPC, (long)nsm * MM::MINB * 4);
+                k_rsdl_ins_tf32<P><<<blocks, MM::WPC * 32, mma_smem(), st>>>(
+                    o, o + MM::PROJ_LEN / 2, *static_cast<const InsMmaSmallF<P> *>(small), m, s, ph, stage, zero_rr,
+                    diff);
+            }
+            if (m.ncurved > 0) {
+                constexpr int EPC = C::WPC * C::EPW;
+                const int cap = nsm * tn.elem_cap;
+                k_rsdl_elem<R, P, PHYS, true><<<std::min(nblk(m.ncurved, EPC), cap), C::WPC * 32, smem(), st>>>(
+                    reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, stage, zero_rr, diff, ElemMat<R>{},
+                    ElemJac<R>{});
+            }
+        }
+    }
+    static void mma_build(const hp_basis_tables &b, std::vector<unsigned char> &ops, std::vector<unsigned char> &small) {
+        if constexpr (DBL) {
+            InsMmaSmall<P> sm;
+            std::vector<double> o;
+            build_ins_mma<P>(b, o, sm);
+            ops.resize(o.size() * sizeof(double));
+            std::memcpy(ops.data(), o.data(), ops.size());
+            small.resize(sizeof(sm));
+            std::memcpy(small.data(), &sm, sizeof(sm));
+        } else {
+            InsMmaSmallF<P> sm;
+            std::vector<float> o;
+            build_ins_tf32<P>(b, o, sm);
+            ops.resize(o.size() * sizeof(float));
+            std::memcpy(ops.data(), o.data(), ops.size());
+            small.resize(sizeof(sm));
+            std::memcpy(small.data(), &sm, sizeof(sm));
+        }
+    }
+    static void base_pts(const void *tab, const Mesh &m, const State<R> &s, R *bpt, cudaStream_t st) {
+        if constexpr (HAS_MMA && !DBL)
+            k_base_points<P><<<nblk(2L * m.ntri, 128), 128, 0, st>>>(reinterpret_cast<const DevTables<float, P> *>(tab),
+                                                                     m, s.ubv, s.ubs, s.ubi, bpt);
+    }
     static cudaError_t set_smem_attr() {
         cudaError_t e = cudaFuncSetAttribute(k_rsdl_elem<R, P, PHYS, false>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem());
         if (e != cudaSuccess) return e;
+        if constexpr (HAS_MMA) {
+            if constexpr (DBL)
+                e = cudaFuncSetAttribute(k_rsdl_ins_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, mma_smem());
+            else
+                e = cudaFuncSetAttribute(k_rsdl_ins_tf32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, mma_smem());
+            if (e != cudaSuccess) return e;
+        }
         return cudaFuncSetAttribute(k_rsdl_elem<R, P, PHYS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem());
+    }
+    static void l2err(const void *tab, const double *wtn, const Mesh &m, const State<R> &s, int NV,
+                      const DevField &f, double *part, int blocks, cudaStream_t st) {
+        if constexpr (std::is_same<R, double>::value) {
+            WtN<P> w;
+            for (int j = 0; j <= P; ++j) w.w[j] = wtn[j];
+            k_l2error<P><<<blocks, 128, 0, st>>>(reinterpret_cast<const DevTables<double, P> *>(tab), m, s, NV, f, w,
+                                                 part);
+        }
     }
     static Launchers<R> get() {
         Launchers<R> L;
@@ -274,6 +474,11 @@ struct LaunchImpl {
         L.emat_build = &emat_build;
         L.emat_apply = &emat_apply;
         L.elem_jac = &elem_jac;
+        L.elem_mma = HAS_MMA ? &elem_mma : nullptr;
+        L.mma_build = HAS_MMA ? &mma_build : nullptr;
+        L.base_pts = (HAS_MMA && !DBL) ? &base_pts : nullptr;
+        L.bpt_per_elem = 2 * (P + 1) * (P + 1);
+        L.l2err = std::is_same<R, double>::value ? &l2err : nullptr;
         return L;
     }
 };
@@ -361,6 +566,13 @@ struct hp_gpu_ctx {
     int *f2c_tri = nullptr, *c2f_tri = nullptr;
     double *f2c_wt = nullptr, *c2f_wt = nullptr;
     Tune tune[2];  // launch shapes for FP64 [0] and FP32 [1]
+    // FP64 element kernel: HP_ELEM_TENSOR (ins: k_rsdl_ins_mma) or HP_ELEM_SCALAR (k_rsdl_elem)
+    int elem_kind = 0;
+    void *d_mma = nullptr, *d_mma32 = nullptr;            // dense operators in fragment order (FP64, TF32)
+    std::vector<unsigned char> mma_small, mma_small32;  // derivative tables (kernel parameters)
+    float *d_bpt32 = nullptr;                           // FP32 base point values (correction form)
+    double wtn[HP_MXGP] = {0};                // Gauss-Jacobi weights (l2error)
+    double *d_l2part = nullptr;               // l2error per-block partials
     float tune_ms[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // tuned element-part and minvrt times
     // cd element operators (FP64 built by the element kernel, FP32 converted copy)
     bool emat_on = false, emat_built = false;
@@ -514,10 +726,18 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
         for (int t = 0; t < nt; ++t)
             for (int i = 0; i < 3; ++i) vt_idx[bb[m->tri_pnt[3 * t + i]]++] = 4 * t + i;
     }
-    std::vector<int> vess(np, 0), sess(ns, 0);
+    std::vector<int> vess(np, 0), sess(ns, 0), seg_bdry(ns, -1), vb_idx(2 * (size_t)np, -1);
     for (int e = 0; e < m->nbseg; ++e) {
         int s = m->bseg[e];
         if (s < 0 || s >= ns) { set_err("bseg out of range"); return fail(HP_EINVAL); }
+        if (seg_bdry[s] >= 0) { set_err("segment %d listed twice as a boundary edge", s); return fail(HP_EINVAL); }
+        seg_bdry[s] = e;
+        for (int end = 0; end < 2; ++end) {
+            int *slot = &vb_idx[2 * (size_t)m->seg_pnt[2 * s + end]];
+            if (slot[0] < 0) slot[0] = 2 * e + end;
+            else if (slot[1] < 0) slot[1] = 2 * e + end;
+            else { set_err("vertex %d ends more than two boundary edges", m->seg_pnt[2 * s + end]); return fail(HP_EINVAL); }
+        }
         int mask = m->bseg_kind[e] & 0xFF;
         sess[s] |= mask;
         vess[m->seg_pnt[2 * s]] |= mask;
@@ -542,6 +762,9 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     if ((r = upload(c, &d_sess, sess.data(), sess.size()))) return fail(r);
     if ((r = upload(c, &d_bseg, m->bseg, (size_t)m->nbseg))) return fail(r);
     if ((r = upload(c, &d_bkind, m->bseg_kind, (size_t)m->nbseg))) return fail(r);
+    int *d_sbd, *d_vbi;
+    if ((r = upload(c, &d_sbd, seg_bdry.data(), seg_bdry.size()))) return fail(r);
+    if ((r = upload(c, &d_vbi, vb_idx.data(), vb_idx.size()))) return fail(r);
     std::vector<double> pibc((size_t)std::max(1, m->nbseg) * b->gpx, 0.0);
     if (m->bseg_pibc) std::copy(m->bseg_pibc, m->bseg_pibc + (size_t)m->nbseg * b->gpx, pibc.begin());
     if ((r = upload(c, &d_bpibc, pibc.data(), pibc.size()))) return fail(r);
@@ -552,6 +775,7 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     M.vs_ptr = d_vsp; M.vs_idx = d_vsi; M.vt_ptr = d_vtp; M.vt_idx = d_vti;
     M.vess = d_vess; M.sess = d_sess; M.bseg = d_bseg; M.bkind = d_bkind; M.bpibc = d_bpibc;
     M.tri_cv = nullptr; M.crv_cht = nullptr; M.bcrd = nullptr; M.ncurved = 0; M.crv_tri = nullptr;
+    M.seg_bdry = d_sbd; M.vb_idx = d_vbi;
 
     // curved elements (tri_hp::metric::setinfo, metric.cpp:44-70, for p > 1): the
     // owner triangle of every boundary side with non-zero position modes, with its
@@ -604,6 +828,15 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     std::vector<unsigned char> htab(c->L.tab_bytes);
     c->L.fill(*b, htab.data());
     if ((r = upload(c, (unsigned char **)&c->d_tab, htab.data(), htab.size()))) return fail(r);
+    for (int j = 0; j < b->gpn && j < HP_MXGP; ++j) c->wtn[j] = b->wtn[j];
+    if (c->L.mma_build && c->L32.mma_build) {
+        std::vector<unsigned char> ops, ops32;
+        c->L.mma_build(*b, ops, c->mma_small);
+        c->L32.mma_build(*b, ops32, c->mma_small32);
+        if ((r = upload(c, (unsigned char **)&c->d_mma, ops.data(), ops.size()))) return fail(r);
+        if ((r = upload(c, (unsigned char **)&c->d_mma32, ops32.data(), ops32.size()))) return fail(r);
+        c->elem_kind = HP_ELEM_TENSOR;
+    }
     DevMinv<double> hm;
     fill_minv<double>(*b, hm);
     c->vdiag = b->vdiag;
@@ -628,6 +861,13 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     if ((r = dalloc(c, (void **)&c->st.sprcn, (size_t)ns * NV * 8))) return fail(r);
     if ((r = dalloc(c, (void **)&c->st.tprcn, (size_t)nt * NV * 8))) return fail(r);
     if ((r = dalloc(c, (void **)&c->st.tau, (size_t)nt * NV * 8))) return fail(r);
+    // per-element vertex / side residuals and per-edge boundary fluxes of the FP64
+    // assembly by gather (State::elim)
+    const size_t nel = (size_t)nt * b->bm * NV, nbr = (size_t)std::max(1, m->nbseg) * (b->sm + 2) * NV;
+    if ((r = dalloc(c, (void **)&c->st.elim, nel * 8))) return fail(r);
+    if ((r = dalloc(c, (void **)&c->st.elre, nel * 8))) return fail(r);
+    if ((r = dalloc(c, (void **)&c->st.bres, nbr * 8))) return fail(r);
+    CK(cudaMemsetAsync(c->st.elre, 0, nel * 8, c->stream));
     if ((r = dalloc(c, (void **)&c->d_slot, 4 * 8))) return fail(r);
     CK(cudaMemsetAsync(c->d_slot, 0, 32, c->stream));
     c->hist_cap = 1 << 16;
@@ -721,6 +961,15 @@ static void launch_elem(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab, c
                         int stage, int zero_rr, int diff) {
     if (c->emat_on && c->emat_built && ph.physics == HP_PHYS_CD && !diff)
         L.emat_apply(emat_of(c, R()), c->mesh, st, ph, stage, zero_rr, c->nsm, tune_of(c, R()), c->stream);
+    // FP64: the DMMA kernel; FP32: the TF32 kernel in correction form only (the operand
+    // rounding to TF32 is ~5e-4 of the fluxes, which a plain-form residual near convergence,
+    // much smaller than its fluxes, would not resolve; the correction form has no such
+    // cancellation)
+    else if (c->elem_kind == HP_ELEM_TENSOR && L.elem_mma &&
+             (std::is_same<R, double>::value ? !diff : (diff && st.bpt != nullptr)))
+        L.elem_mma(std::is_same<R, double>::value ? c->d_mma : c->d_mma32,
+                   std::is_same<R, double>::value ? c->mma_small.data() : c->mma_small32.data(), tab, c->mesh, st, ph,
+                   stage, zero_rr, diff, c->nsm, tune_of(c, R()), c->stream);
     else
         L.elem(tab, c->mesh, st, ph, stage, zero_rr, diff, c->nsm, tune_of(c, R()), c->stream);
 }
@@ -732,6 +981,17 @@ static void enqueue_rsdl_t(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab
     const int nstage = ph.nstage;
     const int zero_rr = (stage >= nstage) ? 1 : 0;
     const double omb = zero_rr ? 0.0 : 1.0 - ph.beta[stage];
+    if (st.elim) {
+        // assembly by gather: the element and boundary kernels write per-element and
+        // per-edge values, k_assemble forms res and res_r of the vertices and sides
+        launch_elem<R>(c, L, tab, st, ph, stage, zero_rr, diff);
+        L.bflux(tab, c->mesh, st, ph, diff, c->stream);
+        const long n = (long)c->npnt + (long)c->nseg * c->sm;
+        const int with_b = (ph.physics == HP_PHYS_INS && c->nbseg > 0) ? 1 : 0;
+        k_assemble<R><<<std::min(nblk(n, 256), c->nsm * 16), 256, 0, c->stream>>>(
+            c->mesh, st, c->NV, c->sm, (R)omb, zero_rr, ph.beta[stage] > 0.0 ? 1 : 0, with_b);
+        return;
+    }
     const long n = (long)(c->lv + c->ls);
     k_rsdl_pre<R><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, st.resv, st.ress,
                                                                            st.rrv, st.rrs, (R)omb, zero_rr);
@@ -821,10 +1081,89 @@ extern "C" int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *c, int stage) {
     return check_launch(c);
 }
 
-extern "C" int hp_gpu_rsdl(hp_gpu_ctx *c, int stage) {
-    int r = hp_gpu_enqueue_rsdl(c, stage);
-    if (r) return r;
+static int alloc_mixed(hp_gpu_ctx *c);
+static void mixed_prcn(hp_gpu_ctx *c);
+
+extern "C" int hp_gpu_rsdl(hp_gpu_ctx *c, int stage, int precision) {
+    if (!c) return HP_EINVAL;
+    if (precision == HP_PREC_FP64) {
+        int r = hp_gpu_enqueue_rsdl(c, stage);
+        if (r) return r;
+        return hp_gpu_sync(c);
+    }
+    if (precision != HP_PREC_FP32) { set_err("precision must be HP_PREC_FP64 or HP_PREC_FP32"); return HP_EINVAL; }
+    if (stage < 0 || stage > c->ph.nstage) { set_err("bad stage"); return HP_EINVAL; }
+    if (c->ph.physics == HP_PHYS_CD && c->ph.beta[stage] > 0.0 && !c->prcn_ready) {
+        set_err("cd rsdl needs tau from setup_preconditioner");
+        return HP_ESTATE;
+    }
+    int r;
+    if ((r = fas_first(c))) return r;
+    if ((r = alloc_mixed(c))) return r;
+    // the FP32 element kernels in plain form on fp32(u), with the level's FAS source; the
+    // preconditioner arrays (cd tau) are FP32 copies of the FP64 ones
+    if (c->prcn_ready) mixed_prcn(c);
+    State<float> f = c->s32;
+    f.ubv = f.ubs = f.ubi = nullptr;
+    conv(c, (long)c->lv, c->st.ugv, f.ugv);
+    conv(c, (long)c->ls, c->st.ugs, f.ugs);
+    conv(c, (long)c->li, c->st.ugi, f.ugi);
+    if (c->mg_kind) {
+        conv(c, (long)c->lv, (const double *)c->fasv, (float *)f.dresv);
+        conv(c, (long)c->ls, (const double *)c->fass, (float *)f.dress);
+        if (c->li) conv(c, (long)c->li, (const double *)c->fasi, (float *)f.dresi);
+    } else {
+        f.dresv = f.dress = f.dresi = nullptr;
+    }
+    enqueue_rsdl_t<float>(c, c->L32, c->d_tab32, f, c->ph, stage, 0);
+    const long n = (long)(c->lv + c->ls);
+    k_rsdl_fold<float><<<nblk(n, 256), 256, 0, c->stream>>>((int)c->lv, (int)c->ls, f.resv, f.rrv, f.ress, f.rrs,
+                                                            f.dresv, f.dress);
+    conv(c, (long)c->lv, (const float *)f.resv, c->st.resv);
+    conv(c, (long)c->ls, (const float *)f.ress, c->st.ress);
+    conv(c, (long)c->li, (const float *)f.resi, c->st.resi);
+    if ((r = check_launch(c))) return r;
     return hp_gpu_sync(c);
+}
+
+extern "C" int hp_gpu_l2error(hp_gpu_ctx *c, const hp_field *fld, double *l2, double *linf) {
+    if (!c || !fld || !l2 || !linf) return HP_EINVAL;
+    if (!c->L.l2err) { set_err("l2error not built"); return HP_ENOTSUP; }
+    const int blocks = std::max(1, std::min(c->nsm * 4, nblk(c->ntri, 128)));
+    int r;
+    if (!c->d_l2part && (r = dalloc(c, (void **)&c->d_l2part, (size_t)c->nsm * 4 * 2 * 3 * 8))) return r;
+    double *part = c->d_l2part;
+    DevField f;
+    f.kind = fld->kind;
+    for (int k = 0; k < 4; ++k) f.prm[k] = fld->prm[k];
+    c->L.l2err(c->d_tab, c->wtn, c->mesh, c->st, c->NV, f, part, blocks, c->stream);
+    std::vector<double> h((size_t)blocks * 2 * c->NV);
+    CK(cudaMemcpyAsync(h.data(), part, h.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int n = 0; n < c->NV; ++n) {
+        double a = 0.0, m = 0.0;
+        for (int b = 0; b < blocks; ++b) {
+            a += h[(size_t)b * 2 * c->NV + n];
+            m = std::max(m, h[(size_t)b * 2 * c->NV + c->NV + n]);
+        }
+        l2[n] = std::sqrt(a);
+        linf[n] = m;
+    }
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_set_element_kernel(hp_gpu_ctx *c, int kind) {
+    if (!c || (kind != HP_ELEM_SCALAR && kind != HP_ELEM_TENSOR)) return HP_EINVAL;
+    if (kind == HP_ELEM_TENSOR && !c->d_mma) {
+        set_err("the tensor-core element kernel is built for ins only");
+        return HP_ENOTSUP;
+    }
+    if (c->elem_kind != kind) {  // captured updates hold the old kernel
+        if (c->g_update) { cudaGraphExecDestroy(c->g_update); c->g_update = nullptr; }
+        if (c->g_update32) { cudaGraphExecDestroy(c->g_update32); c->g_update32 = nullptr; }
+    }
+    c->elem_kind = kind;
+    return HP_OK;
 }
 
 static void drop_update_graphs(hp_gpu_ctx *c) {
@@ -886,8 +1225,10 @@ extern "C" int hp_gpu_set_element_matrices(hp_gpu_ctx *c, int on) {
 // Stream-ordered body of setup_preconditioner (capturable: no host synchronisation).
 // Bad elements are counted into d_err, which the caller zeroes and reads.
 static int enqueue_prcn(hp_gpu_ctx *c) {
-    CK(cudaMemsetAsync(c->st.vprcn, 0, (size_t)c->npnt * c->NV * 8, c->stream));
-    CK(cudaMemsetAsync(c->st.sprcn, 0, (size_t)c->nseg * c->NV * 8, c->stream));
+    if (!c->st.elim) {
+        CK(cudaMemsetAsync(c->st.vprcn, 0, (size_t)c->npnt * c->NV * 8, c->stream));
+        CK(cudaMemsetAsync(c->st.sprcn, 0, (size_t)c->nseg * c->NV * 8, c->stream));
+    }
     if (c->net) {
         int r0 = hp_gpu_elem_features(c, c->d_feat);
         if (r0) return r0;
@@ -899,6 +1240,12 @@ static int enqueue_prcn(hp_gpu_ctx *c) {
     }
     launch_prcn(c->p, c->ph.physics, c->d_tab, c->mesh, c->st, c->ph, c->d_err, c->lsc, c->lsc_ld, c->lsc_clamp,
                 c->stream);
+    if (c->st.elim) {  // assembly by gather, inversion fused
+        const long n = (long)c->npnt + (c->p > 1 ? (long)c->nseg : 0);
+        k_prcn_gather<double><<<std::min(nblk(n, 256), c->nsm * 16), 256, 0, c->stream>>>(c->mesh, c->st, c->NV,
+                                                                                        c->p > 1 ? 1 : 0, c->vdiag);
+        return check_launch(c);
+    }
     const int nv = c->npnt * c->NV, ns = (c->p > 1 ? c->nseg * c->NV : 0);
     k_prcn_invert<double><<<nblk(nv + ns, 256), 256, 0, c->stream>>>(nv, ns, c->st.vprcn, c->st.sprcn, c->vdiag);
     return check_launch(c);
@@ -1002,7 +1349,7 @@ static int device_norm(hp_gpu_ctx *c, const double *a, size_t n, double &ss, dou
 
 extern "C" int hp_gpu_resnorm(hp_gpu_ctx *c, double *l2, double *linf) {
     if (!c) return HP_EINVAL;
-    int r = hp_gpu_rsdl(c, c->ph.nstage);
+    int r = hp_gpu_rsdl(c, c->ph.nstage, HP_PREC_FP64);
     if (r) return r;
     double ss = 0.0, mx = 0.0;
     if ((r = device_norm(c, c->st.resv, c->lv, ss, mx))) return r;
@@ -1049,6 +1396,12 @@ static int alloc_mixed(hp_gpu_ctx *c) {
     if ((r = dalloc(c, (void **)&f.sprcn, (size_t)c->nseg * c->NV * 4))) return r;
     if ((r = dalloc(c, (void **)&f.tprcn, (size_t)c->ntri * c->NV * 4))) return r;
     if ((r = dalloc(c, (void **)&f.tau, (size_t)c->ntri * c->NV * 4))) return r;
+    // the base state's point values of the TF32 correction-form kernel (refreshed with the
+    // base by base_points); the pointer is fixed here so that captured updates see it
+    if (c->L32.base_pts && c->d_mma32) {
+        if ((r = dalloc(c, (void **)&c->d_bpt32, (size_t)c->ntri * c->L32.bpt_per_elem * 4))) return r;
+        f.bpt = c->d_bpt32;
+    }
     // res_r is scaled by (1 - beta) before it is first written: it must start finite
     CK(cudaMemsetAsync(f.rrv, 0, c->lv * 4, c->stream));
     if (c->ls) CK(cudaMemsetAsync(f.rrs, 0, c->ls * 4, c->stream));
@@ -1069,6 +1422,11 @@ static void mixed_prcn(hp_gpu_ctx *c) {
     conv(c, (long)c->ntri * c->NV, c->st.tau, f.tau);
 }
 
+// Point values of the FP32 base state (State::bpt) after it changed.
+static void base_points(hp_gpu_ctx *c) {
+    if (c->s32.bpt) c->L32.base_pts(c->d_tab32, c->mesh, c->s32, c->d_bpt32, c->stream);
+}
+
 // Start of one correction cycle: base = fp32(u64), dres = fp32(R64(u64)) (the FP64
 // residual left in res by rsdl(nstage)), correction d = 0, res_r = 0.
 static void mixed_prepare(hp_gpu_ctx *c) {
@@ -1076,6 +1434,7 @@ static void mixed_prepare(hp_gpu_ctx *c) {
     conv(c, (long)c->lv, c->st.ugv, (float *)f.ubv);
     conv(c, (long)c->ls, c->st.ugs, (float *)f.ubs);
     conv(c, (long)c->li, c->st.ugi, (float *)f.ubi);
+    base_points(c);
     conv(c, (long)c->lv, c->st.resv, (float *)f.dresv);
     conv(c, (long)c->ls, c->st.ress, (float *)f.dress);
     if (c->li) conv(c, (long)c->li, c->st.resi, (float *)f.dresi);
@@ -1731,6 +2090,7 @@ static int mixed_levels_setup(hp_gpu_ctx **lv, int n, bool prcn) {
         conv(c, (long)c->lv, c->st.ugv, (float *)f.ubv);
         conv(c, (long)c->ls, c->st.ugs, (float *)f.ubs);
         conv(c, (long)c->li, c->st.ugi, (float *)f.ubi);
+        base_points(c);
     }
     return check_launch(lv[0]);
 }

@@ -62,6 +62,9 @@ struct Mesh {
     const double *bcrd;
     int ncurved;         // number of curved elements
     const int *crv_tri;  // [ncurved] their triangle indices (crv_cht order)
+    // boundary edges seen from the entities: seg_bdry[s] = boundary edge of segment s or -1;
+    // vb_idx[v][2] = 2 e + end of the (at most two) boundary edges ending at vertex v, or -1
+    const int *seg_bdry, *vb_idx;
 };
 
 template <typename R>
@@ -77,6 +80,16 @@ struct State {
     // pointers = plain form.
     const R *ubv, *ubs, *ubi;
     const R *dresv, *dress, *dresi;
+    // Assembly by gather (FP64): when elim != NULL, the element kernels write each
+    // element's vertex and side residuals (lftog's values, side signs applied) to
+    // elim / elre [ntri][BM][NV] (imaginary / beta-scaled real part) and the boundary
+    // fluxes go to bres [nbseg][SM+2][NV] (end 0, end 1, side modes), without atomics;
+    // k_assemble then sums them per vertex and side in a fixed order, so repeated
+    // residual evaluations are bitwise identical. NULL: FP64/FP32 atomics.
+    R *elim, *elre, *bres;
+    // Correction form on the tensor cores: the base state's point values (u, v)
+    // [ntri][2][GG] (k_base_points), fixed for a correction cycle; NULL: not computed.
+    const R *bpt;
 };
 
 __device__ __forceinline__ void atomic_add(double *a, double v) { atomicAdd(a, v); }
@@ -469,8 +482,14 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
             return l0;
         };
         // scatter of one local coefficient of variable n, mode m (lftog, gtol.cpp:364-402)
-        auto scatter = [&](R *gv, R *gs, int n, int m, R val) {
-            if (m < 3) {
+        auto scatter = [&](R *gv, R *gs, R *el, int n, int m, R val) {
+            if (el) {
+                if (m >= 3) {
+                    const int i = (m - 3) / SM, k = (m - 3) - i * SM;
+                    if ((k & 1) && mesh.tri_sgn[3 * tind + i] < 0) val = -val;
+                }
+                el[((size_t)tind * BM + m) * NV + n] = val;
+            } else if (m < 3) {
                 const int v = (m == 0 ? p0 : (m == 1 ? p1 : p2));
                 atomic_add(&gv[v * NV + n], val);
             } else {
@@ -492,7 +511,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
             } else if (jmode) {
                 uht[n * T + m] = val;  // uht is dead after stage I: lf_im collects there
             } else if (m < BM) {
-                scatter(st.resv, st.ress, n, m, val);
+                scatter(st.resv, st.ress, st.elim, n, m, val);
             } else {
                 const size_t gi = ((size_t)tind * IM + (m - BM)) * NV + n;
                 const R src = st.dresi ? st.dresi[gi] : (R)0;
@@ -602,7 +621,7 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
                 } else if (jmode) {
                     uht[n * T + m] += val;
                 } else if (m < BM) {
-                    scatter(st.rrv, st.rrs, n, m, val);
+                    scatter(st.rrv, st.rrs, st.elre, n, m, val);
                 } else {
                     const size_t gi = ((size_t)tind * IM + (m - BM)) * NV + n;
                     const R rr = st.rri[gi] * omb + val;
@@ -730,7 +749,15 @@ __global__ void __launch_bounds__(EmatShape<R, P, RE>::THREADS, 2048 / EmatShape
         if (t >= mesh.ntri) return;
         const R vim = r_s[w];
         const R vre = RE ? r_s[SLOTS + w] : (R)0;
-        if (ms < 3) {
+        if (st.elim && ms < BM) {  // assembly by gather (NV = 1)
+            bool flip = false;
+            if (ms >= 3) {
+                const int i = (ms - 3) / SM, kk = (ms - 3) - i * SM;
+                flip = (kk & 1) && mesh.tri_sgn[3 * t + i] < 0;
+            }
+            st.elim[(size_t)t * BM + ms] = flip ? -vim : vim;
+            if (RE) st.elre[(size_t)t * BM + ms] = flip ? -vre : vre;
+        } else if (ms < 3) {
             const int v = mesh.tri_pnt[3 * t + ms];
             atomic_add(&st.resv[v], vim);
             if (RE) atomic_add(&st.rrv[v], vre);
@@ -870,10 +897,98 @@ __global__ void k_bdry_flux_ins(const DevTables<R, P> *__restrict__ tb, Mesh mes
             for (int m = 3; m < X; ++m) acc[n][m - 1] += tb->gxwtx[m][k] * r;
         }
     }
+    if (st.bres) {  // assembly by gather: k_assemble adds them
+        for (int n = 0; n < NV; ++n)
+            for (int m = 0; m < SM + 2; ++m) st.bres[((size_t)e * (SM + 2) + m) * NV + n] = acc[n][m];
+        return;
+    }
     for (int n = 0; n < NV; ++n) {
         atomic_add(&st.resv[v0 * NV + n], acc[n][0]);
         atomic_add(&st.resv[v1 * NV + n], acc[n][1]);
         for (int m = 0; m < SM; ++m) atomic_add(&st.ress[(sind * SM + m) * NV + n], acc[n][m + 2]);
+    }
+}
+
+// Assembly by gather of rsdl(stage)'s vertex and side residuals (lftog, gtol.cpp:364-402,
+// summed per entity instead of scattered): res = sum of the elements' imaginary parts
+// (+ the boundary fluxes, hp_edge_bdry::rsdl), res_r = (1 - beta) res_r + sum of their
+// real parts (nstage.cpp:21-49; zero_rr: res_r = sum). A vertex sums its triangles in
+// vertex-incidence order, a side its two triangles in seg.tri order, so the result does
+// not depend on the scheduling. One thread per vertex, then one per (side, mode).
+template <typename R>
+__global__ void k_assemble(Mesh mesh, State<R> st, int NV, int SM, R omb, int zero_rr, int with_re, int with_b) {
+    const int BM = 3 + 3 * SM;
+    const long nitems = (long)mesh.npnt + (long)mesh.nseg * SM;
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < nitems; k += (long)gridDim.x * blockDim.x) {
+        if (k < mesh.npnt) {
+            const int v = (int)k, j0 = mesh.vt_ptr[v], j1 = mesh.vt_ptr[v + 1];
+            for (int n = 0; n < NV; ++n) {
+                R sim = (R)0, sre = (R)0;
+                for (int j = j0; j < j1; ++j) {
+                    const int code = mesh.vt_idx[j];
+                    const size_t idx = ((size_t)(code >> 2) * BM + (code & 3)) * NV + n;
+                    sim += st.elim[idx];
+                    if (with_re) sre += st.elre[idx];
+                }
+                if (with_b)
+                    for (int q = 0; q < 2; ++q) {
+                        const int b = mesh.vb_idx[2 * v + q];
+                        if (b >= 0 && (mesh.bkind[b >> 1] & (0xF << 8)) == (1 << 8))
+                            sim += st.bres[((size_t)(b >> 1) * (SM + 2) + (b & 1)) * NV + n];
+                    }
+                st.resv[v * NV + n] = sim;
+                const R r0 = zero_rr ? (R)0 : st.rrv[v * NV + n] * omb;
+                st.rrv[v * NV + n] = with_re ? r0 + sre : r0;
+            }
+        } else {
+            const long q = k - mesh.npnt;
+            const int sd = (int)(q / SM), kk = (int)(q - (long)sd * SM);
+            const int e = with_b ? mesh.seg_bdry[sd] : -1;
+            const bool bf = e >= 0 && (mesh.bkind[e] & (0xF << 8)) == (1 << 8);
+            for (int n = 0; n < NV; ++n) {
+                R sim = (R)0, sre = (R)0;
+                for (int side = 0; side < 2; ++side) {
+                    const int t = mesh.seg_tri[2 * sd + side];
+                    if (t < 0) continue;
+                    const size_t idx = ((size_t)t * BM + 3 + mesh.seg_loc[2 * sd + side] * SM + kk) * NV + n;
+                    sim += st.elim[idx];
+                    if (with_re) sre += st.elre[idx];
+                }
+                if (bf) sim += st.bres[((size_t)e * (SM + 2) + 2 + kk) * NV + n];
+                const size_t g = ((size_t)sd * SM + kk) * NV + n;
+                st.ress[g] = sim;
+                const R r0 = zero_rr ? (R)0 : st.rrs[g] * omb;
+                st.rrs[g] = with_re ? r0 + sre : r0;
+            }
+        }
+    }
+}
+
+// Preconditioner assembly by gather with the inversion of tri_hp::setup_preconditioner
+// (setup_preconditioner.cpp:68-76): vprcn = 1 / (vdiag sum of the vertex's triangles'
+// tprcn), sprcn = 1 / (sum over the side's triangles), in a fixed order.
+template <typename R>
+__global__ void k_prcn_gather(Mesh mesh, State<R> st, int NV, int with_s, R vdiag) {
+    const long nitems = (long)mesh.npnt + (with_s ? (long)mesh.nseg : 0);
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < nitems; k += (long)gridDim.x * blockDim.x) {
+        if (k < mesh.npnt) {
+            const int v = (int)k;
+            for (int n = 0; n < NV; ++n) {
+                R sum = (R)0;
+                for (int j = mesh.vt_ptr[v]; j < mesh.vt_ptr[v + 1]; ++j) sum += st.tprcn[(mesh.vt_idx[j] >> 2) * NV + n];
+                st.vprcn[v * NV + n] = (R)1.0 / (vdiag * sum);
+            }
+        } else {
+            const int sd = (int)(k - mesh.npnt);
+            for (int n = 0; n < NV; ++n) {
+                R sum = (R)0;
+                for (int side = 0; side < 2; ++side) {
+                    const int t = mesh.seg_tri[2 * sd + side];
+                    if (t >= 0) sum += st.tprcn[t * NV + n];
+                }
+                st.sprcn[sd * NV + n] = (R)1.0 / sum;
+            }
+        }
     }
 }
 
@@ -1193,6 +1308,7 @@ __global__ void k_prcn_elem(const DevTables<R, P> *__restrict__ tb, Mesh mesh, S
         }
     }
     for (int n = 0; n < NV; ++n) st.tprcn[t * NV + n] = (R)tp[n];
+    if (st.elim) return;  // assembly by gather: k_prcn_gather sums tprcn per vertex and side
     for (int i = 0; i < 3; ++i) {
         for (int n = 0; n < NV; ++n) atomic_add(&st.vprcn[v[i] * NV + n], (R)tp[n]);
         if (SM > 0) {
@@ -1406,6 +1522,121 @@ __global__ void k_mask_essential(Mesh mesh, R *resv, R *ress, int NV, int sm) {
                 for (int n = 0; n < NV; ++n)
                     if (e & (1 << n)) ress[(s * sm + m) * NV + n] = (R)0;
     }
+}
+// ---------------------------------------------------------------------------
+// tri_hp::l2error (tri_hp/l2error.cpp:13-67) on the device: L2 and L_inf error of the
+// state against an analytic field at the quadrature points, sum err^2 wtx wtn cjcb.
+// Curved elements take their point coordinates from proj_bdry of crdtocht and their
+// Jacobians from calc_metrics, as the reference does.
+// ---------------------------------------------------------------------------
+struct DevField {
+    int kind;
+    double prm[4];
+};
+
+// The built-in closed forms of include/hp_host.h's hp_field kinds.
+__device__ inline double field_value_dev(const DevField &f, int n, double x, double y) {
+    const double PI = 3.14159265358979323846;
+    switch (f.kind) {
+        case 1: {  // Kovasznay, prm[0] = Re
+            const double re = f.prm[0], lda = .5 * re - sqrt(re * re / 4 + 4 * PI * PI);
+            if (n == 0) return 1.0 - cos(2 * PI * y) * exp(lda * x);
+            if (n == 1) return lda / (2 * PI) * sin(2 * PI * y) * exp(lda * x);
+            return -.5 * exp(2. * lda * x);
+        }
+        case 2: return f.prm[0] * sin(PI * x) * sin(PI * y);
+        case 3: return f.prm[0] * (x - f.prm[1]) * (x - f.prm[1]);
+        case 4: return (n == 0 && y >= 1.0 - 1e-12) ? 1.0 : 0.0;
+        case 5: {
+            const double d = hypot(x - f.prm[0], y - f.prm[1]);
+            return (n == 0 && d > f.prm[2] * (1.0 + 1e-9)) ? 1.0 : 0.0;
+        }
+        default: return f.prm[n < 4 ? n : 3];
+    }
+}
+
+template <int P>
+struct WtN {
+    double w[P + 1];
+};
+
+// one thread per element; per-block partials part[block][2 NV] = (sum err^2 per variable,
+// max err per variable), reduced on the host in block order
+template <int P>
+__global__ void __launch_bounds__(128) k_l2error(const DevTables<double, P> *__restrict__ tb, Mesh mesh,
+                                                 State<double> st, int NV, DevField fld, WtN<P> wtn, double *part) {
+    constexpr int G = P + 1, T = (P + 1) * (P + 2) / 2, SM = (P > 1 ? P - 1 : 1), IM = (P - 1) * (P - 2) / 2,
+                  BM = 3 * P;
+    double l2[3] = {0.0, 0.0, 0.0}, mx[3] = {0.0, 0.0, 0.0};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mesh.ntri; t += gridDim.x * blockDim.x) {
+        const int p0 = mesh.tri_pnt[3 * t], p1 = mesh.tri_pnt[3 * t + 1], p2 = mesh.tri_pnt[3 * t + 2];
+        const int cv = mesh.tri_cv ? mesh.tri_cv[t] : -1;
+        const double *cht = cv >= 0 ? mesh.crv_cht + (size_t)cv * 2 * BM : nullptr;
+        const double g00 = 0.5 * (mesh.pnts[2 * p2] - mesh.pnts[2 * p1]);
+        const double g01 = 0.5 * (mesh.pnts[2 * p0] - mesh.pnts[2 * p1]);
+        const double g10 = 0.5 * (mesh.pnts[2 * p2 + 1] - mesh.pnts[2 * p1 + 1]);
+        const double g11 = 0.5 * (mesh.pnts[2 * p0 + 1] - mesh.pnts[2 * p1 + 1]);
+        for (int i = 0; i < G; ++i)
+            for (int j = 0; j < G; ++j) {
+                double x, y, cjcb;
+                if (cht) {  // proj_bdry of the position modes (interior modes zero)
+                    x = y = 0.0;
+                    for (int m = 0; m < BM; ++m) {
+                        const double b = tb->gn[j][m] * tb->gx[i][tb->colof[m]];
+                        x += cht[m] * b;
+                        y += cht[BM + m] * b;
+                    }
+                    double d00, d01, d10, d11;
+                    curved_metrics<double, P>(*tb, cht, i, j, d00, d01, d10, d11);
+                    cjcb = d00 * d11 - d10 * d01;
+                } else {  // proj.cpp:188-199 of the vertex coordinates
+                    const double b0 = tb->gx[i][0] * tb->gn[j][0], b1 = tb->gx[i][1] * tb->gn[j][1],
+                                 b2 = tb->gx[i][2] * tb->gn[j][2];
+                    x = mesh.pnts[2 * p0] * b0 + mesh.pnts[2 * p1] * b1 + mesh.pnts[2 * p2] * b2;
+                    y = mesh.pnts[2 * p0 + 1] * b0 + mesh.pnts[2 * p1 + 1] * b1 + mesh.pnts[2 * p2 + 1] * b2;
+                    cjcb = g00 * g11 - g10 * g01;
+                }
+                const double wt = tb->wtx[i] * wtn.w[j] * cjcb;
+                for (int n = 0; n < NV; ++n) {
+                    double u = 0.0;
+                    for (int m = 0; m < T; ++m) {  // ugtouht + proj
+                        double c;
+                        if (m < 3) {
+                            c = st.ugv[(m == 0 ? p0 : (m == 1 ? p1 : p2)) * NV + n];
+                        } else if (m < BM) {
+                            const int si = (m - 3) / SM, k = (m - 3) - si * SM;
+                            c = st.ugs[(mesh.tri_seg[3 * t + si] * SM + k) * NV + n];
+                            if ((k & 1) && mesh.tri_sgn[3 * t + si] < 0) c = -c;
+                        } else {
+                            c = st.ugi[((size_t)t * IM + (m - BM)) * NV + n];
+                        }
+                        u += c * tb->gn[j][m] * tb->gx[i][tb->colof[m]];
+                    }
+                    const double err = fabs(u - field_value_dev(fld, n, x, y));
+                    if (err >= mx[n]) mx[n] = err;
+                    l2[n] += err * err * wt;
+                }
+            }
+    }
+    __shared__ double sl[3][4], sm_[3][4];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    for (int n = 0; n < 3; ++n) {
+        double a = l2[n], b = mx[n];
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            const double c = __shfl_xor_sync(0xffffffffu, b, o);
+            b = c > b ? c : b;
+        }
+        if (l == 0) { sl[n][w] = a; sm_[n][w] = b; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int n = 0; n < NV; ++n) {
+            double a = 0.0, b = 0.0;
+            for (int q = 0; q < 4; ++q) { a += sl[n][q]; b = sm_[n][q] > b ? sm_[n][q] : b; }
+            part[(size_t)blockIdx.x * 2 * NV + n] = a;
+            part[(size_t)blockIdx.x * 2 * NV + NV + n] = b;
+        }
 }
 }  // namespace hpb
 

@@ -100,7 +100,8 @@ def lib():
                                     _I, P, ctypes.POINTER(P)]
         for name in ("hp_gpu_destroy", "hp_gpu_setup_preconditioner", "hp_gpu_minvrt", "hp_gpu_update", "hp_gpu_sync"):
             getattr(L, name).argtypes = [P]
-        L.hp_gpu_rsdl.argtypes = [P, _I]
+        L.hp_gpu_rsdl.argtypes = [P, _I, _I]
+        L.hp_gpu_l2error.argtypes = [P, P, P, P]
         L.hp_gpu_enqueue_rsdl.argtypes = [P, _I]
         L.hp_gpu_enqueue_update.argtypes = [P]
         L.hp_gpu_enqueue_element_rsdl.argtypes = [P, _I]

@@ -237,14 +237,15 @@ def min_angles(mesh):
     return out
 
 
-def square_mesh(n, x0=0.0, x1=1.0, y0=0.0, y1=1.0):
-    """n x n squares, two counter-clockwise triangles each (diagonal upper-left to lower-right)."""
+def square_mesh(n, x0=0.0, x1=1.0, y0=0.0, y1=1.0, ny=None):
+    """n x ny squares (ny = n by default), two counter-clockwise triangles each (diagonal
+    upper-left to lower-right)."""
+    ny = n if ny is None else ny
     xs = np.linspace(x0, x1, n + 1)
-    ys = np.linspace(y0, y1, n + 1)
+    ys = np.linspace(y0, y1, ny + 1)
     X, Y = np.meshgrid(xs, ys)  # [j][i]
     pnts = np.stack([X.ravel(), Y.ravel()], axis=1)
-    i = np.arange(n)
-    I, J = np.meshgrid(i, i)
+    I, J = np.meshgrid(np.arange(n), np.arange(ny))
     I = I.ravel()
     J = J.ravel()
     va = J * (n + 1) + I

@@ -232,8 +232,17 @@ class GPULevel:
     def setup_preconditioner(self):
         return L.check(self.lib.hp_gpu_setup_preconditioner(self.h), "setup_preconditioner")
 
-    def rsdl(self, stage):
-        L.check(self.lib.hp_gpu_rsdl(self.h, stage), "rsdl")
+    def rsdl(self, stage, precision=0):
+        """tri_hp::rsdl(stage); precision 0 = FP64 kernels, 1 = FP32 kernels (result widened)."""
+        L.check(self.lib.hp_gpu_rsdl(self.h, stage, precision), "rsdl")
+
+    def l2error(self, field=None):
+        """tri_hp::l2error on the device against `field` (default: the problem's field)."""
+        f = self.prob.field if field is None else field
+        l2 = np.zeros(self.prob.NV)
+        li = np.zeros(self.prob.NV)
+        L.check(self.lib.hp_gpu_l2error(self.h, ctypes.byref(f), L.ptr(l2), L.ptr(li)), "l2error")
+        return l2, li
 
     def autotune(self, reps=5):
         """hp_gpu_autotune; returns the chosen shapes and tuned times of FP64 and FP32."""
@@ -258,6 +267,10 @@ class GPULevel:
         self.lib.hp_gpu_element_jacobian.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.check(self.lib.hp_gpu_element_jacobian(self.h, L.ptr(K)), "element_jacobian")
         return K
+
+    def element_kernel(self, kind):
+        """FP64 element kernel: "tensor" (ins default) or "scalar" (hp_gpu_set_element_kernel)."""
+        L.check(self.lib.hp_gpu_set_element_kernel(self.h, {"scalar": 0, "tensor": 1}[kind]), "set_element_kernel")
 
     def element_matrices(self, on=True):
         """cd only: rsdl from stored element operators (hp_gpu_set_element_matrices)."""
@@ -318,9 +331,10 @@ def kovasznay_ins(n=64, p=4, re=100.0, noise=1e-3, seed=20261204, **kw):
     return prob.tobasis(noise=noise, seed=seed)
 
 
-def lid_cavity_ins(n=64, p=4, re=400.0, noise=1e-3, seed=20261206, **kw):
-    """ins lid-driven cavity: u = 1 on the lid, zero on the other walls, velocity essential everywhere."""
-    mesh = square_mesh(n)
+def lid_cavity_ins(n=64, p=4, re=400.0, noise=1e-3, seed=20261206, mesh=None, **kw):
+    """ins lid-driven cavity: u = 1 on the lid (y = 1), zero on the other walls, velocity
+    essential everywhere; on the n x n split-square mesh of the unit square, or `mesh`."""
+    mesh = square_mesh(n) if mesh is None else mesh
     field = L.Field(L.HP_FIELD_LID, (ctypes.c_double * 4)(0, 0, 0, 0))
     walls = mesh.boundary_segments()
     bc = [(walls, 0b011 | L.HP_BC_FLUX_INS_GENERIC)]

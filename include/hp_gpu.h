@@ -154,8 +154,18 @@ int hp_gpu_device_ptrs(hp_gpu_ctx *ctx, double **ugv, double **ugs, double **ugi
                        double **ress, double **resi);
 
 /* tri_hp::rsdl(stage) (tri_hp/nstage.cpp:12-110): residual of the given stage,
- * 0 <= stage <= nstage (stage == nstage: full residual, res_r reset). */
-int hp_gpu_rsdl(hp_gpu_ctx *ctx, int stage);
+ * 0 <= stage <= nstage (stage == nstage: full residual, res_r reset), left in the
+ * context's FP64 res arrays. precision HP_PREC_FP64: the FP64 kernels;
+ * HP_PREC_FP32: the FP32 kernels on fp32 of the state (plain form, with the level's
+ * multigrid source), the result widened to FP64 (res_r is then the FP32 smoother's). */
+int hp_gpu_rsdl(hp_gpu_ctx *ctx, int stage, int precision);
+
+/* tri_hp::l2error (tri_hp/l2error.cpp:13-67) on the device: per variable the L2 norm
+ * sqrt(sum err^2 wtx wtn cjcb) and the max |err| of the state against the analytic
+ * field f (include/hp_host.h) at the quadrature points; curved elements use their
+ * isoparametric coordinates and Jacobians. l2[NV], linf[NV]. */
+struct hp_field;
+int hp_gpu_l2error(hp_gpu_ctx *ctx, const struct hp_field *f, double *l2, double *linf);
 
 /* tri_hp_{ins,cd}::setup_preconditioner + tri_hp::setup_preconditioner
  * (ins/setup_preconditioner.cpp:9-221, cd/setup_preconditioner.cpp:6-97,
@@ -185,6 +195,16 @@ int hp_gpu_maxres(hp_gpu_ctx *ctx, double *out, double *mx);
 /* Unpreconditioned residual norm over all modes: computes rsdl(nstage) and
  * returns sqrt(sum res^2) and max |res| over every v/s/i coefficient. */
 int hp_gpu_resnorm(hp_gpu_ctx *ctx, double *l2, double *linf);
+
+/* FP64 element kernel of rsdl (no counterpart in the reference, which has one CPU
+ * loop, tri_hp/nstage.cpp:52-73). HP_ELEM_TENSOR (the default for ins): projection and
+ * intgrtrs of two triangles per warp on the FP64 tensor cores (mma.m8n8k4.f64) with
+ * dense per-point operators; HP_ELEM_SCALAR: the sum-factorised warp kernel (cd always
+ * uses it). Both give the reference's residual up to rounding. HP_ENOTSUP when the
+ * tensor-core kernel is not built for the context's physics. */
+#define HP_ELEM_SCALAR 0
+#define HP_ELEM_TENSOR 1
+int hp_gpu_set_element_kernel(hp_gpu_ctx *ctx, int kind);
 
 /* Stream-ordered forms without a host synchronisation (for callers that time or
  * capture the work themselves): rsdl(stage) with res_r folded into res, and one

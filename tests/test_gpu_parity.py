@@ -18,10 +18,12 @@ TOLN = 1e-10
 
 
 def tol1(p):
-    """p = 8 runs beyond the reference's "works up to sm = 5" tables: its side and
-    interior static-inversion tables are ill-conditioned and amplify rounding
-    differences of the summation order about tenfold, so 1e-11 there."""
-    return TOL1 if p <= 6 else 1e-11
+    """From p = 5 on, the side and interior static-inversion tables of minvrt are
+    ill-conditioned (the reference's lumpinv systems have fewer equations than unknowns
+    there) and amplify rounding differences of the summation order up to tenfold: the
+    ins tensor-core kernel sums each element's contractions in another order than the
+    sum factorisation (rsdl itself stays within 1e-12), so 1e-11 there."""
+    return TOL1 if p <= 4 else 1e-11
 
 
 def relerr(a, b):
@@ -62,6 +64,47 @@ def test_prcn_rsdl_minvrt(kind, p):
     g.minvrt()
     o.minvrt()
     assert relerr(g.residual(), o.residual()) < tol1(p), "minvrt"
+
+
+def staircase_mesh(n):
+    """The split squares of an n x n grid on or below the anti-diagonal, closed by the
+    lower-left triangles of the diagonal squares: n^2 triangles (odd for odd n)."""
+    pts = [(i, j) for j in range(n + 1) for i in range(n + 1) if i + j <= n]
+    idx = {q: k for k, q in enumerate(pts)}
+    tri = []
+    for J in range(n):
+        for I in range(n - J):
+            va, vb, vd = idx[(I, J)], idx[(I + 1, J)], idx[(I, J + 1)]
+            tri.append((va, vb, vd))
+            if I + J <= n - 2:
+                tri.append((vb, idx[(I + 1, J + 1)], vd))
+    return hpb.Mesh(np.array(pts, dtype=float) / n, np.array(tri, dtype=np.int32))
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("elem", ["tensor", "scalar"])
+def test_ins_element_kernels_match_oracle(p, elem):
+    """Both FP64 ins element kernels (tensor-core DMMA and scalar warp kernel) against the
+    oracle: rsdl at every stage kind (beta = 1, beta = 0, beta in (0, 1)), on a mesh with
+    an odd triangle count (the last warp's second triangle is missing) and on a Delaunay
+    mesh (irregular orientations)."""
+    import ctypes
+    from hpb import _lib as L
+    for mesh in (staircase_mesh(5), hpb.delaunay_square(7, seed=11)):
+        field = L.Field(L.HP_FIELD_KOVASZNAY, (ctypes.c_double * 4)(100.0, 0, 0, 0))
+        b = mesh.boundary_segments()
+        pr = hpb.Problem(mesh, p, L.HP_PHYS_INS, rho=1.0, mu=0.01, field=field,
+                         bc=[(b[::2], 0b011 | L.HP_BC_FLUX_INS_GENERIC),
+                             (b[1::2], L.HP_BC_FLUX_INS_GENERIC)]).tobasis(noise=1e-3, seed=3)
+        g = pr.gpu()
+        g.element_kernel(elem)
+        o = Oracle(pr)
+        assert g.setup_preconditioner() == 0 and o.setup_preconditioner() == 0
+        for stage in (pr.phys.nstage, 0, 1, 2):
+            g.rsdl(stage)
+            o.rsdl(stage)
+            assert relerr(g.residual(), o.residual()) < tol1(p), (mesh.ntri, stage)
+        g.close()
 
 
 @pytest.mark.parametrize("kind,p", [("cd", 2), ("cd", 4), ("ins", 2), ("ins", 4), ("ins", 6)])
