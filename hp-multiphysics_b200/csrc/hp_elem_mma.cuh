@@ -41,6 +41,10 @@ struct InsMma {
     static constexpr int MINB = P <= 4 ? 4 : 3;    // CTAs per SM the register budget allows
     static constexpr int NG = NT < 8 ? NT : 8;     // projection n-tiles accumulated together
     static constexpr size_t PROJ_LEN = (size_t)3 * NT * KS * 32, INT_LEN = (size_t)NT2 * KS2 * 32;
+    // strong residual: C[8 x GG] = [flux_r | flux_s][8 x 2GG] * D[2GG x GG] (derivr + derivs)
+    static constexpr size_t DER_LEN = (size_t)NT * KS2 * 32;
+    static constexpr int IDX = 12;  // staged mesh integers per triangle: pnt[3], seg[3], sgn[3]
+    static constexpr size_t SMEM_IDX = (size_t)WPC * 2 * IDX * sizeof(int);
     static_assert(4 * T <= 4 * QP, "gathered modes must fit the PD block");
 };
 
@@ -61,10 +65,37 @@ __device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double
                  : "d"(a), "d"(b));
 }
 
+// C[8 x N] += A[8 x K] * B[K x N] of one warp's fragment rows, A read from a shared-memory
+// row of K (padded) entries, B in fragment order [nt][ks][lane]; the k-steps alternate
+// between two accumulator sets so that consecutive DMMAs of a tile are independent.
+template <int KS, int NTL>
+__device__ __forceinline__ void warp_gemm(const double *__restrict__ arow, const double *__restrict__ B, int gcol,
+                                          int lane, double (&c)[NTL][2]) {
+    double c2[NTL][2];
+#pragma unroll
+    for (int nt = 0; nt < NTL; ++nt) c[nt][0] = c[nt][1] = c2[nt][0] = c2[nt][1] = 0.0;
+#pragma unroll 4
+    for (int ks = 0; ks < KS; ks += 2) {
+        const double a0 = arow[ks * 4 + gcol];
+        const double a1 = ks + 1 < KS ? arow[(ks + 1) * 4 + gcol] : 0.0;
+#pragma unroll
+        for (int nt = 0; nt < NTL; ++nt) {
+            dmma884(c[nt][0], c[nt][1], a0, __ldg(B + ((size_t)nt * KS + ks) * 32 + lane));
+            if (ks + 1 < KS) dmma884(c2[nt][0], c2[nt][1], a1, __ldg(B + ((size_t)nt * KS + ks + 1) * 32 + lane));
+        }
+    }
+#pragma unroll
+    for (int nt = 0; nt < NTL; ++nt) {
+        c[nt][0] += c2[nt][0];
+        c[nt][1] += c2[nt][1];
+    }
+}
+
 template <int P>
 __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
-    k_rsdl_ins_mma(const double *__restrict__ projB, const double *__restrict__ intB, InsMmaSmall<P> small,
-                   Mesh mesh, State<double> st, Phys ph, int stage, int zero_rr) {
+    k_rsdl_ins_mma(const double *__restrict__ projB, const double *__restrict__ intB,
+                   const double *__restrict__ derB, InsMmaSmall<P> small, Mesh mesh, State<double> st, Phys ph,
+                   int stage, int zero_rr) {
     using M = InsMma<P>;
     constexpr int G = M::G, GG = M::GG, T = M::T, BM = M::BM, IM = M::IM, NV = 3, QP = M::QP, VS = M::VS;
     constexpr int SM = (M::SM > 0 ? M::SM : 1);  // side-mode stride (unused when p = 1)
@@ -81,14 +112,21 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
     const int re_ = grow >> 2, rv = grow & 3;  // fragment row -> (triangle, variable)
     double *base = reinterpret_cast<double *>(smem_raw + ((sizeof(InsMmaSmall<P>) + 15) / 16) * 16) +
                    (size_t)warp * 2 * M::S_EL;
+    int *midx = reinterpret_cast<int *>(reinterpret_cast<double *>(smem_raw + ((sizeof(InsMmaSmall<P>) + 15) / 16) * 16) +
+                                        (size_t)M::WPC * 2 * M::S_EL) + warp * 2 * M::IDX;
+    // per triangle: PV u, v, p at the points; PD the gathered modes, then du/dr, dv/dr,
+    // du/ds, dv/ds, then the strong residual; FI the imaginary flux pairs (convective +
+    // pressure for u, v; the mass flux for p); FX the viscous flux pairs (zero for p), then
+    // the real flux pairs (viscous - SUPG; the continuity SUPG term for p). The strong
+    // residual differentiates FI + FX.
     auto PV = [&](int e) { return base + e * M::S_EL; };
     auto PD = [&](int e) { return base + e * M::S_EL + 3 * QP; };
     auto FI = [&](int e) { return base + e * M::S_EL + 7 * QP; };
-    auto FR = [&](int e) { return base + e * M::S_EL + 7 * QP + 3 * VS; };
+    auto FX = [&](int e) { return base + e * M::S_EL + 7 * QP + 3 * VS; };
     // the K padding of the flux pairs stays zero (their B rows are zero too)
     for (int e = 0; e < 2; ++e)
         for (int k = 2 * GG + lane; k < VS; k += 32)
-            for (int v = 0; v < 3; ++v) FI(e)[v * VS + k] = FR(e)[v * VS + k] = 0.0;
+            for (int v = 0; v < 3; ++v) FI(e)[v * VS + k] = FX(e)[v * VS + k] = 0.0;
     __syncthreads();
     const double beta = ph.beta[stage];
     const double omb = zero_rr ? 0.0 : 1.0 - beta;
@@ -106,6 +144,13 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
         auto TE = [&](int e) { return e ? tb1 : ta; };
         auto ACT = [&](int e) { return e ? actb : acta; };
         __syncwarp();
+        // the pair's connectivity, staged once: pnt[0..2], seg[3..5], sgn[6..8]
+        if (lane < 18) {
+            const int e = lane / 9, k = lane - e * 9, t = TE(e);
+            midx[e * M::IDX + k] = k < 3 ? mesh.tri_pnt[3 * t + k]
+                                         : (k < 6 ? mesh.tri_seg[3 * t + k - 3] : mesh.tri_sgn[3 * t + k - 6]);
+        }
+        __syncwarp();
         // ---- gather (ugtouht, gtol.cpp:14-55) into the PD block
         constexpr int NGATH = (2 * NV * T + 31) / 32;
 #pragma unroll
@@ -113,17 +158,17 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             const int w = lane + 32 * k;
             if (w >= 2 * NV * T) break;
             const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
+            const int *ix = midx + e * M::IDX;
             double val = 0.0;
             if (ACT(e)) {
-                const int t = TE(e);
                 if (m < 3) {
-                    val = st.ugv[mesh.tri_pnt[3 * t + m] * NV + n];
+                    val = st.ugv[ix[m] * NV + n];
                 } else if (m < BM) {
                     const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
-                    val = st.ugs[(mesh.tri_seg[3 * t + i] * SM + kk) * NV + n];
-                    if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
+                    val = st.ugs[(ix[3 + i] * SM + kk) * NV + n];
+                    if ((kk & 1) && ix[6 + i] < 0) val = -val;
                 } else {
-                    val = st.ugi[((size_t)t * IM + (m - BM)) * NV + n];
+                    val = st.ugi[((size_t)TE(e) * IM + (m - BM)) * NV + n];
                 }
             }
             PD(e)[n * T + m] = val;
@@ -133,8 +178,8 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
         double gd[2][4], hh[2];
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-            const int t = TE(e);
-            const int p0 = mesh.tri_pnt[3 * t], p1 = mesh.tri_pnt[3 * t + 1], p2 = mesh.tri_pnt[3 * t + 2];
+            const int *ix = midx + e * M::IDX;
+            const int p0 = ix[0], p1 = ix[1], p2 = ix[2];
             const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
             const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
             const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
@@ -193,11 +238,13 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             const double fluxx = rho * u0, fluxy = rho * u1;
             const double m0 = +d11 * fluxx - d01 * fluxy;
             const double m1 = -d10 * fluxx + d00 * fluxy;
+            const double c00 = u0 * m0 + d11 * pp, c01 = u0 * m1 - d10 * pp;
+            const double c10 = u1 * m0 - d01 * pp, c11 = u1 * m1 + d00 * pp;
             double *fi = FI(e);
-            fi[q] = u0 * m0 + d11 * pp;
-            fi[GG + q] = u0 * m1 - d10 * pp;
-            fi[VS + q] = u1 * m0 - d01 * pp;
-            fi[VS + GG + q] = u1 * m1 + d00 * pp;
+            fi[q] = c00;
+            fi[GG + q] = c01;
+            fi[VS + q] = c10;
+            fi[VS + GG + q] = c11;
             fi[2 * VS + q] = m0;
             fi[2 * VS + GG + q] = m1;
             if (beta > 0.0) {
@@ -214,92 +261,102 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                 const double v0111 = cjcbi * d00 * d10;
                 const double v0101 = -cjcbi * d01 * d10;
                 const double v0110 = -cjcbi * d00 * d11;
-                double *fr = FR(e);
-                fr[q] = v0000 * dr0 + v0100 * dr1 + v0001 * ds0 + v0101 * ds1;
-                fr[GG + q] = v0001 * dr0 + v0110 * dr1 + v0011 * ds0 + v0111 * ds1;
-                fr[VS + q] = v0100 * dr0 + v1100 * dr1 + v0110 * ds0 + v1101 * ds1;
-                fr[VS + GG + q] = v0101 * dr0 + v1101 * dr1 + v0111 * ds0 + v1111 * ds1;
+                double *fx = FX(e);
+                fx[q] = v0000 * dr0 + v0100 * dr1 + v0001 * ds0 + v0101 * ds1;
+                fx[GG + q] = v0001 * dr0 + v0110 * dr1 + v0011 * ds0 + v0111 * ds1;
+                fx[VS + q] = v0100 * dr0 + v1100 * dr1 + v0110 * ds0 + v1101 * ds1;
+                fx[VS + GG + q] = v0101 * dr0 + v1101 * dr1 + v0111 * ds0 + v1111 * ds1;
+                fx[2 * VS + q] = 0.0;
+                fx[2 * VS + GG + q] = 0.0;
             }
         }
         __syncwarp();
-        // imaginary part -> res (intgrt.cpp:81-158 with the minus sign of the weak divergence)
-        {
-            const double *arow = FI(re_) + (rv < 3 ? rv : 2) * VS;
-            double c[M::NT2][2];
+        // lftog of one fragment (rows (triangle, variable), 2 modes per n-tile): vertex and
+        // side modes to the assembly buffers (or atomics), interiors directly
+        auto scatter = [&](const double (&c)[M::NT2][2], int part) {
+            if (rv >= 3 || !ACT(re_)) return;
+            const int t = TE(re_);
+            const int *ix = midx + re_ * M::IDX;
 #pragma unroll
-            for (int nt = 0; nt < M::NT2; ++nt) c[nt][0] = c[nt][1] = 0.0;
-#pragma unroll 5
-            for (int ks = 0; ks < M::KS2; ++ks) {
-                const double a = arow[ks * 4 + gcol];
+            for (int nt = 0; nt < M::NT2; ++nt)
 #pragma unroll
-                for (int nt = 0; nt < M::NT2; ++nt) dmma884(c[nt][0], c[nt][1], a, __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane));
-            }
-            if (rv < 3 && ACT(re_)) {
-                const int t = TE(re_);
-#pragma unroll
-                for (int nt = 0; nt < M::NT2; ++nt)
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int m = nt * 8 + gcol * 2 + h;
-                        if (m >= T) continue;
-                        double val = c[nt][h];
-                        if (m < BM) {
-                            int v = -1, gsi = 0;
-                            if (m < 3) {
-                                v = mesh.tri_pnt[3 * t + m];
-                            } else {
-                                const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
-                                if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
-                                gsi = (mesh.tri_seg[3 * t + i] * SM + kk) * NV + rv;
-                            }
-                            if (st.elim) st.elim[((size_t)t * BM + m) * NV + rv] = val;
-                            else if (v >= 0) atomicAdd(&st.resv[v * NV + rv], val);
-                            else atomicAdd(&st.ress[gsi], val);
-                        } else {
-                            const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
+                for (int h = 0; h < 2; ++h) {
+                    const int m = nt * 8 + gcol * 2 + h;
+                    if (m >= T) continue;
+                    double val = part ? c[nt][h] * beta : c[nt][h];
+                    if (m < BM) {
+                        int gsi = -1;
+                        if (m >= 3) {
+                            const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
+                            if ((kk & 1) && ix[6 + i] < 0) val = -val;
+                            gsi = (ix[3 + i] * SM + kk) * NV + rv;
+                        }
+                        double *el = part ? st.elre : st.elim;
+                        if (el) el[((size_t)t * BM + m) * NV + rv] = val;
+                        else if (gsi < 0) atomicAdd((part ? st.rrv : st.resv) + ix[m] * NV + rv, val);
+                        else atomicAdd((part ? st.rrs : st.ress) + gsi, val);
+                    } else {
+                        const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
+                        if (!part) {
                             const double src = st.dresi ? st.dresi[gi] : 0.0;
                             if (beta > 0.0) st.resi[gi] = val + src;
                             else st.resi[gi] = val + st.rri[gi] * omb + src;  // res_r unchanged when beta = 0
+                        } else {
+                            const double rr = st.rri[gi] * omb + val;
+                            st.rri[gi] = rr;
+                            st.resi[gi] += rr;
                         }
                     }
-            }
+                }
+        };
+        // ---- imaginary part: intgrtrs (intgrt.cpp:81-158, weak divergence with its minus
+        //      sign in the operator) on the tensor cores -> res
+        {
+            double c[M::NT2][2];
+            warp_gemm<M::KS2, M::NT2>(FI(re_) + (rv < 3 ? rv : 2) * VS, intB, gcol, lane, c);
+            scatter(c, 0);
         }
         if (beta > 0.0) {
-            // ---- strong residual at the points (derivr / derivs, proj.cpp:339-402) into PD
-            for (int w = lane; w < 2 * GG; w += 32) {
-                const int e = w / GG, q = w - e * GG, i = q / G, j = q - i * G;
-                const double *fi = FI(e), *fre = FR(e);
-                const double ln0 = tb.n0[j];
+            // ---- strong residual at the points (derivr + derivs of the full fluxes,
+            //      proj.cpp:339-402) on the tensor cores, into PD
+            {
+                constexpr int NTC = M::NT < 8 ? M::NT : 8;
 #pragma unroll
-                for (int n = 0; n < NV; ++n) {
-                    // full fluxes: convective + pressure + viscous (u, v); the mass flux (p)
-                    auto fr_ = [&](int qq) { return n < 2 ? fi[n * VS + qq] + fre[n * VS + qq] : fi[2 * VS + qq]; };
-                    auto fs_ = [&](int qq) {
-                        return n < 2 ? fi[n * VS + GG + qq] + fre[n * VS + GG + qq] : fi[2 * VS + GG + qq];
-                    };
-                    double acc = 0.0;  // rhorbd0 * u + dugdt with bd(0) = 0
-                    {
-                        const double wi = fr_(i * G + j) * tb.dltx[i] * ln0;
+                for (int nt0 = 0; nt0 < M::NT; nt0 += NTC) {
+                    constexpr int NTL = NTC;
+                    double c[NTL][2];
+                    double c2[NTL][2];
 #pragma unroll
-                        for (int qq = 0; qq < G; ++qq)
-                            if (qq != i) acc += (wi + fr_(qq * G + j) * tb.dltx[qq] * ln0) * tb.dltx1[i][qq];
+                    for (int g = 0; g < NTL; ++g) c[g][0] = c[g][1] = c2[g][0] = c2[g][1] = 0.0;
+                    const double *ai = FI(re_) + (rv < 3 ? rv : 2) * VS, *ax = FX(re_) + (rv < 3 ? rv : 2) * VS;
+#pragma unroll 4
+                    for (int ks = 0; ks < M::KS2; ks += 2) {
+                        const int k0 = ks * 4 + gcol, k1 = k0 + 4;
+                        const double a0 = ai[k0] + ax[k0];
+                        const double a1 = ks + 1 < M::KS2 ? ai[k1] + ax[k1] : 0.0;
+#pragma unroll
+                        for (int g = 0; g < NTL; ++g) {
+                            if (nt0 + g >= M::NT) continue;
+                            const double *b = derB + ((size_t)(nt0 + g) * M::KS2 + ks) * 32 + lane;
+                            dmma884(c[g][0], c[g][1], a0, __ldg(b));
+                            if (ks + 1 < M::KS2) dmma884(c2[g][0], c2[g][1], a1, __ldg(b + 32));
+                        }
                     }
-                    {
-                        const double fsij = fs_(i * G + j);
-                        const double wi = fsij * tb.dltx[i] * ln0;
+                    if (rv < 3) {
+                        double *dst = PD(re_) + rv * QP;
 #pragma unroll
-                        for (int qq = 0; qq < G; ++qq)
-                            if (qq != i) acc += (wi + fs_(qq * G + j) * tb.dltx[qq] * ln0) * tb.dltn1[i][qq];
-                        const double wj = fsij * tb.dltn[j];
-#pragma unroll
-                        for (int qq = 0; qq < G; ++qq)
-                            if (qq != j) acc += (wj + fs_(i * G + qq) * tb.dltn[qq]) * tb.dltn2[j][qq];
+                        for (int g = 0; g < NTL; ++g)
+                            if (nt0 + g < M::NT) {
+                                const int q = (nt0 + g) * 8 + gcol * 2;
+                                dst[q] = c[g][0] + c2[g][0];
+                                dst[q + 1] = c[g][1] + c2[g][1];
+                            }
                     }
-                    PD(e)[n * QP + q] = acc;
                 }
             }
             __syncwarp();
-            // ---- pointwise SUPG terms (ins/rsdl.cpp:341-431, CALC_TAU2)
+            // ---- pointwise SUPG terms (ins/rsdl.cpp:341-431, CALC_TAU2): FX becomes the real
+            //      flux pairs, viscous minus SUPG for u, v and the continuity term for p
             const double nu = mu / rho;
             for (int w = lane; w < 2 * GG; w += 32) {
                 const int e = w / GG, q = w - e * GG;
@@ -315,55 +372,19 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                 const double tau0 = ph.adis * he / (cjcb * sqrt(gam));
                 const double tau2 = sqrt(qv) * tau0;
                 const double tr0 = tau0 * PD(e)[q], tr1 = tau0 * PD(e)[QP + q], tr2 = tau2 * PD(e)[2 * QP + q];
-                double *fr = FR(e);
-                fr[q] -= (d11 * (2. * u0) - d01 * u1) * tr0 - d01 * u0 * tr1 + d11 * tr2;
-                fr[GG + q] -= (-d10 * (2. * u0) + d00 * u1) * tr0 + d00 * u0 * tr1 - d10 * tr2;
-                fr[VS + q] -= +d11 * u1 * tr0 + (d11 * u0 - d01 * (2. * u1)) * tr1 - d01 * tr2;
-                fr[VS + GG + q] -= -d10 * u1 * tr0 + (-d10 * u0 + d00 * (2. * u1)) * tr1 + d00 * tr2;
-                fr[2 * VS + q] = -(d11 * tr0 - d01 * tr1);
-                fr[2 * VS + GG + q] = -(-d10 * tr0 + d00 * tr1);
+                double *fx = FX(e);
+                fx[q] -= (d11 * (2. * u0) - d01 * u1) * tr0 - d01 * u0 * tr1 + d11 * tr2;
+                fx[GG + q] -= (-d10 * (2. * u0) + d00 * u1) * tr0 + d00 * u0 * tr1 - d10 * tr2;
+                fx[VS + q] -= +d11 * u1 * tr0 + (d11 * u0 - d01 * (2. * u1)) * tr1 - d01 * tr2;
+                fx[VS + GG + q] -= -d10 * u1 * tr0 + (-d10 * u0 + d00 * (2. * u1)) * tr1 + d00 * tr2;
+                fx[2 * VS + q] = -(d11 * tr0 - d01 * tr1);
+                fx[2 * VS + GG + q] = -(-d10 * tr0 + d00 * tr1);
             }
             __syncwarp();
             // ---- real part: intgrtrs of the viscous + SUPG fluxes, x beta -> res_r
-            const double *arow = FR(re_) + (rv < 3 ? rv : 2) * VS;
             double c[M::NT2][2];
-#pragma unroll
-            for (int nt = 0; nt < M::NT2; ++nt) c[nt][0] = c[nt][1] = 0.0;
-#pragma unroll 5
-            for (int ks = 0; ks < M::KS2; ++ks) {
-                const double a = arow[ks * 4 + gcol];
-#pragma unroll
-                for (int nt = 0; nt < M::NT2; ++nt) dmma884(c[nt][0], c[nt][1], a, __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane));
-            }
-            if (rv < 3 && ACT(re_)) {
-                const int t = TE(re_);
-#pragma unroll
-                for (int nt = 0; nt < M::NT2; ++nt)
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int m = nt * 8 + gcol * 2 + h;
-                        if (m >= T) continue;
-                        double val = c[nt][h] * beta;
-                        if (m < BM) {
-                            int v = -1, gsi = 0;
-                            if (m < 3) {
-                                v = mesh.tri_pnt[3 * t + m];
-                            } else {
-                                const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
-                                if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
-                                gsi = (mesh.tri_seg[3 * t + i] * SM + kk) * NV + rv;
-                            }
-                            if (st.elre) st.elre[((size_t)t * BM + m) * NV + rv] = val;
-                            else if (v >= 0) atomicAdd(&st.rrv[v * NV + rv], val);
-                            else atomicAdd(&st.rrs[gsi], val);
-                        } else {
-                            const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
-                            const double rr = st.rri[gi] * omb + val;
-                            st.rri[gi] = rr;
-                            st.resi[gi] += rr;
-                        }
-                    }
-            }
+            warp_gemm<M::KS2, M::NT2>(FX(re_) + (rv < 3 ? rv : 2) * VS, intB, gcol, lane, c);
+            scatter(c, 1);
         }
         __syncwarp();
     }

@@ -37,8 +37,12 @@ struct InsTf32 {
     static constexpr int WPC = 4;
     static constexpr int MINB = P <= 4 ? 4 : 3;
     static constexpr int NG = NT < 8 ? NT : 8;
-    // B fragments: two floats per lane per MMA
+    // B fragments: two floats per lane per MMA; DER: the strong residual's point-to-point
+    // operator (derivr + derivs), C[16 x GG] = [flux_r | flux_s][16 x 2GG] * D[2GG x GG]
     static constexpr size_t PROJ_LEN = (size_t)3 * NT * KS * 64, INT_LEN = (size_t)NT2 * KS2 * 64;
+    static constexpr size_t DER_LEN = (size_t)NT * KS2 * 64;
+    static constexpr int IDX = 12;  // staged mesh integers per triangle: pnt[3], seg[3], sgn[3]
+    static constexpr size_t SMEM_IDX = (size_t)WPC * 4 * IDX * sizeof(int);
     static_assert(4 * T <= 4 * QP, "gathered modes must fit the PD block");
 };
 
@@ -90,39 +94,59 @@ __global__ void k_base_points(const DevTables<float, P> *__restrict__ tb, Mesh m
     }
 }
 
+// C[16 x 8 NTL] of one warp's fragment rows (triangles ra, ra + 2 at variable rv) from
+// A rows read in shared memory (a0/a2 from ra0, a1/a3 from ra1, plus the optional second
+// rows added in, K padded with zeros) and B in fragment order [nt][ks][lane].
+template <int KS, int NTL>
+__device__ __forceinline__ void warp_gemm_tf32(const float *ra0, const float *ra1, const float *rb0, const float *rb1,
+                                               const float2 *__restrict__ B, int tig, int lane, float (&c)[NTL][4]) {
+#pragma unroll
+    for (int nt = 0; nt < NTL; ++nt) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.f;
+#pragma unroll 4
+    for (int ks = 0; ks < KS; ++ks) {
+        const int k = ks * 8 + tig;
+        float x0 = ra0[k], x1 = ra1[k], x2 = ra0[k + 4], x3 = ra1[k + 4];
+        if (rb0) {
+            x0 += rb0[k]; x1 += rb1[k]; x2 += rb0[k + 4]; x3 += rb1[k + 4];
+        }
+        const unsigned a0 = f2tf32(x0), a1 = f2tf32(x1), a2 = f2tf32(x2), a3 = f2tf32(x3);
+#pragma unroll
+        for (int nt = 0; nt < NTL; ++nt) mma_tf32(c[nt], a0, a1, a2, a3, __ldg(B + ((size_t)nt * KS + ks) * 32 + lane));
+    }
+}
+
 template <int P>
 __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
-    k_rsdl_ins_tf32(const float2 *__restrict__ projB, const float2 *__restrict__ intB, InsMmaSmallF<P> small,
-                    Mesh mesh, State<float> st, Phys ph, int stage, int zero_rr, int diff) {
+    k_rsdl_ins_tf32(const float2 *__restrict__ projB, const float2 *__restrict__ intB,
+                    const float2 *__restrict__ derB, InsMmaSmallF<P> small, Mesh mesh, State<float> st, Phys ph,
+                    int stage, int zero_rr, int diff) {
     using M = InsTf32<P>;
     constexpr int G = M::G, GG = M::GG, T = M::T, BM = M::BM, IM = M::IM, NV = 3, QP = M::QP, VS = M::VS;
     constexpr int SM = (M::SM > 0 ? M::SM : 1);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    InsMmaSmallF<P> &tb = *reinterpret_cast<InsMmaSmallF<P> *>(smem_raw);
-    {
-        const int n4 = sizeof(InsMmaSmallF<P>) / 4;
-        const int *src = reinterpret_cast<const int *>(&small);
-        int *dst = reinterpret_cast<int *>(smem_raw);
-        for (int k = threadIdx.x; k < n4; k += blockDim.x) dst[k] = src[k];
-    }
+    (void)small;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int grp = lane >> 2, tig = lane & 3;
     const int ra = grp >> 2, rv = grp & 3;  // fragment row grp -> (triangle ra, variable rv); row grp + 8 -> ra + 2
-    float *base = reinterpret_cast<float *>(smem_raw + ((sizeof(InsMmaSmallF<P>) + 15) / 16) * 16) +
-                  (size_t)warp * 4 * M::S_EL;
+    float *base = reinterpret_cast<float *>(smem_raw) + (size_t)warp * 4 * M::S_EL;
+    int *midx = reinterpret_cast<int *>(reinterpret_cast<float *>(smem_raw) + (size_t)M::WPC * 4 * M::S_EL) +
+                warp * 4 * M::IDX;
+    // per triangle as in k_rsdl_ins_mma: PV u, v, p; PD modes / derivatives / strong
+    // residual; FI imaginary flux pairs; FX viscous, then real flux pairs
     auto PV = [&](int e) { return base + e * M::S_EL; };
     auto PD = [&](int e) { return base + e * M::S_EL + 3 * QP; };
     auto FI = [&](int e) { return base + e * M::S_EL + 7 * QP; };
-    auto FR = [&](int e) { return base + e * M::S_EL + 7 * QP + 3 * VS; };
+    auto FX = [&](int e) { return base + e * M::S_EL + 7 * QP + 3 * VS; };
     for (int e = 0; e < 4; ++e)
         for (int k = 2 * GG + lane; k < VS; k += 32)
-            for (int v = 0; v < 3; ++v) FI(e)[v * VS + k] = FR(e)[v * VS + k] = 0.f;
+            for (int v = 0; v < 3; ++v) FI(e)[v * VS + k] = FX(e)[v * VS + k] = 0.f;
     __syncthreads();
     const float beta = (float)ph.beta[stage];
     const float omb = zero_rr ? 0.f : 1.f - beta;
     const float rho = (float)ph.rho, mu = (float)ph.mu;
     const bool corr = diff && st.bpt;
     const long ntri = mesh.ntri, nquad = (ntri + 3) / 4;
+    const int rvv = rv < 3 ? rv : 2;  // variable slot 3 repeats slot 2 (its rows are discarded)
     for (long pr = (long)blockIdx.x * M::WPC + warp; pr < nquad; pr += (long)gridDim.x * M::WPC) {
         const int t0 = (int)(4 * pr);
         // triangle e of the quad (a missing one repeats the first, unwritten); curved
@@ -134,20 +158,26 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
         auto TE = [&](int e) { return t0 + e < ntri ? t0 + e : t0; };
         auto ACT = [&](int e) { return (actm >> e) & 1u; };
         __syncwarp();
+        for (int w = lane; w < 36; w += 32) {  // the quad's connectivity: pnt, seg, sgn
+            const int e = w / 9, k = w - e * 9, t = TE(e);
+            midx[e * M::IDX + k] = k < 3 ? mesh.tri_pnt[3 * t + k]
+                                         : (k < 6 ? mesh.tri_seg[3 * t + k - 3] : mesh.tri_sgn[3 * t + k - 6]);
+        }
+        __syncwarp();
         // ---- gather the modes (ugtouht, gtol.cpp:14-55) into the PD block
         for (int w = lane; w < 4 * NV * T; w += 32) {
             const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
+            const int *ix = midx + e * M::IDX;
             float val = 0.f;
             if (ACT(e)) {
-                const int t = TE(e);
                 if (m < 3) {
-                    val = st.ugv[mesh.tri_pnt[3 * t + m] * NV + n];
+                    val = st.ugv[ix[m] * NV + n];
                 } else if (m < BM) {
                     const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
-                    val = st.ugs[(mesh.tri_seg[3 * t + i] * SM + kk) * NV + n];
-                    if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
+                    val = st.ugs[(ix[3 + i] * SM + kk) * NV + n];
+                    if ((kk & 1) && ix[6 + i] < 0) val = -val;
                 } else {
-                    val = st.ugi[((size_t)t * IM + (m - BM)) * NV + n];
+                    val = st.ugi[((size_t)TE(e) * IM + (m - BM)) * NV + n];
                 }
             }
             PD(e)[n * T + m] = val;
@@ -204,7 +234,8 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
         for (int w = lane; w < 4 * GG; w += 32) {
             const int e = w / GG, q = w - e * GG;
             const int t = TE(e);
-            const int p0 = mesh.tri_pnt[3 * t], p1 = mesh.tri_pnt[3 * t + 1], p2 = mesh.tri_pnt[3 * t + 2];
+            const int *ix = midx + e * M::IDX;
+            const int p0 = ix[0], p1 = ix[1], p2 = ix[2];
             const float d00 = (float)(0.5 * (mesh.pnts[2 * p2] - mesh.pnts[2 * p1]));
             const float d01 = (float)(0.5 * (mesh.pnts[2 * p0] - mesh.pnts[2 * p1]));
             const float d10 = (float)(0.5 * (mesh.pnts[2 * p2 + 1] - mesh.pnts[2 * p1 + 1]));
@@ -246,37 +277,26 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                 const float v0111 = cjcbi * d00 * d10;
                 const float v0101 = -cjcbi * d01 * d10;
                 const float v0110 = -cjcbi * d00 * d11;
-                float *fr = FR(e);
-                fr[q] = v0000 * dr0 + v0100 * dr1 + v0001 * ds0 + v0101 * ds1;
-                fr[GG + q] = v0001 * dr0 + v0110 * dr1 + v0011 * ds0 + v0111 * ds1;
-                fr[VS + q] = v0100 * dr0 + v1100 * dr1 + v0110 * ds0 + v1101 * ds1;
-                fr[VS + GG + q] = v0101 * dr0 + v1101 * dr1 + v0111 * ds0 + v1111 * ds1;
+                float *fx = FX(e);
+                fx[q] = v0000 * dr0 + v0100 * dr1 + v0001 * ds0 + v0101 * ds1;
+                fx[GG + q] = v0001 * dr0 + v0110 * dr1 + v0011 * ds0 + v0111 * ds1;
+                fx[VS + q] = v0100 * dr0 + v1100 * dr1 + v0110 * ds0 + v1101 * ds1;
+                fx[VS + GG + q] = v0101 * dr0 + v1101 * dr1 + v0111 * ds0 + v1111 * ds1;
+                fx[2 * VS + q] = 0.f;
+                fx[2 * VS + GG + q] = 0.f;
             }
         }
         __syncwarp();
-        // intgrtrs of a flux block (FI or FR) on the tensor cores, then lftog: vertex and
-        // side modes by FP32 atomics, interiors directly. part 0: imaginary -> res;
-        // part 1: real (x beta) -> res_r
-        auto integrate = [&](int part) {
-            const float *r0 = (part ? FR(ra) : FI(ra)) + (rv < 3 ? rv : 2) * VS;
-            const float *r1 = (part ? FR(ra + 2) : FI(ra + 2)) + (rv < 3 ? rv : 2) * VS;
-            float c[M::NT2][4];
-#pragma unroll
-            for (int nt = 0; nt < M::NT2; ++nt) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.f;
-#pragma unroll 4
-            for (int ks = 0; ks < M::KS2; ++ks) {
-                const int k = ks * 8 + tig;
-                const unsigned a0 = f2tf32(r0[k]), a1 = f2tf32(r1[k]), a2 = f2tf32(r0[k + 4]), a3 = f2tf32(r1[k + 4]);
-#pragma unroll
-                for (int nt = 0; nt < M::NT2; ++nt)
-                    mma_tf32(c[nt], a0, a1, a2, a3, __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane));
-            }
+        // lftog of the two fragment rows a lane holds: vertex and side modes by FP32 atomics,
+        // interiors directly. part 0: imaginary -> res; part 1: real (x beta) -> res_r
+        auto scatter = [&](const float (&c)[M::NT2][4], int part) {
             if (rv >= 3) return;
 #pragma unroll
             for (int hh = 0; hh < 2; ++hh) {  // rows grp (triangle ra) and grp + 8 (triangle ra + 2)
                 const int e = ra + 2 * hh;
                 if (!ACT(e)) continue;
                 const int t = TE(e);
+                const int *ix = midx + e * M::IDX;
 #pragma unroll
                 for (int nt = 0; nt < M::NT2; ++nt)
 #pragma unroll
@@ -286,11 +306,11 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                         float val = c[nt][2 * hh + h];
                         if (part) val *= beta;
                         if (m < 3) {
-                            atomicAdd((part ? st.rrv : st.resv) + mesh.tri_pnt[3 * t + m] * NV + rv, val);
+                            atomicAdd((part ? st.rrv : st.resv) + ix[m] * NV + rv, val);
                         } else if (m < BM) {
                             const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
-                            if ((kk & 1) && mesh.tri_sgn[3 * t + i] < 0) val = -val;
-                            atomicAdd((part ? st.rrs : st.ress) + (mesh.tri_seg[3 * t + i] * SM + kk) * NV + rv, val);
+                            if ((kk & 1) && ix[6 + i] < 0) val = -val;
+                            atomicAdd((part ? st.rrs : st.ress) + (ix[3 + i] * SM + kk) * NV + rv, val);
                         } else {
                             const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
                             if (!part) {
@@ -306,38 +326,32 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                     }
             }
         };
-        integrate(0);
+        {
+            float c[M::NT2][4];
+            warp_gemm_tf32<M::KS2, M::NT2>(FI(ra) + rvv * VS, FI(ra + 2) + rvv * VS, nullptr, nullptr, intB, tig,
+                                            lane, c);
+            scatter(c, 0);
+        }
         if (beta > 0.f) {
-            // ---- strong residual of the full fluxes at the points (derivr / derivs) into PD
-            for (int w = lane; w < 4 * GG; w += 32) {
-                const int e = w / GG, q = w - e * GG, i = q / G, j = q - i * G;
-                const float *fi = FI(e), *fre = FR(e);
-                const float ln0 = tb.n0[j];
+            // ---- strong residual of FI + FX at the points (derivr / derivs) on TF32, into PD
+            {
+                constexpr int NTC = M::NT < 8 ? M::NT : 8;
 #pragma unroll
-                for (int n = 0; n < NV; ++n) {
-                    auto fr_ = [&](int qq) { return n < 2 ? fi[n * VS + qq] + fre[n * VS + qq] : fi[2 * VS + qq]; };
-                    auto fs_ = [&](int qq) {
-                        return n < 2 ? fi[n * VS + GG + qq] + fre[n * VS + GG + qq] : fi[2 * VS + GG + qq];
-                    };
-                    float acc = 0.f;
-                    {
-                        const float wi = fr_(i * G + j) * tb.dltx[i] * ln0;
+                for (int nt0 = 0; nt0 < M::NT; nt0 += NTC) {
+                    float c[NTC][4];
+                    warp_gemm_tf32<M::KS2, NTC>(FI(ra) + rvv * VS, FI(ra + 2) + rvv * VS, FX(ra) + rvv * VS,
+                                                FX(ra + 2) + rvv * VS, derB + (size_t)nt0 * M::KS2 * 32, tig, lane, c);
+                    if (rv < 3) {
 #pragma unroll
-                        for (int qq = 0; qq < G; ++qq)
-                            if (qq != i) acc += (wi + fr_(qq * G + j) * tb.dltx[qq] * ln0) * tb.dltx1[i][qq];
+                        for (int g = 0; g < NTC; ++g)
+                            if (nt0 + g < M::NT) {
+                                const int q = (nt0 + g) * 8 + tig * 2;
+                                PD(ra)[rv * QP + q] = c[g][0];
+                                PD(ra)[rv * QP + q + 1] = c[g][1];
+                                PD(ra + 2)[rv * QP + q] = c[g][2];
+                                PD(ra + 2)[rv * QP + q + 1] = c[g][3];
+                            }
                     }
-                    {
-                        const float fsij = fs_(i * G + j);
-                        const float wi = fsij * tb.dltx[i] * ln0;
-#pragma unroll
-                        for (int qq = 0; qq < G; ++qq)
-                            if (qq != i) acc += (wi + fs_(qq * G + j) * tb.dltx[qq] * ln0) * tb.dltn1[i][qq];
-                        const float wj = fsij * tb.dltn[j];
-#pragma unroll
-                        for (int qq = 0; qq < G; ++qq)
-                            if (qq != j) acc += (wj + fs_(i * G + qq) * tb.dltn[qq]) * tb.dltn2[j][qq];
-                    }
-                    PD(e)[n * QP + q] = acc;
                 }
             }
             __syncwarp();
@@ -346,7 +360,8 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             for (int w = lane; w < 4 * GG; w += 32) {
                 const int e = w / GG, q = w - e * GG;
                 const int t = TE(e);
-                const int p0 = mesh.tri_pnt[3 * t], p1 = mesh.tri_pnt[3 * t + 1], p2 = mesh.tri_pnt[3 * t + 2];
+                const int *ix = midx + e * M::IDX;
+                const int p0 = ix[0], p1 = ix[1], p2 = ix[2];
                 const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
                 const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
                 const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
@@ -373,7 +388,7 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                 const float tau0 = (float)ph.adis * he / (cjcb * sqrtf(gam));
                 const float tau2 = sqrtf(qv) * tau0;
                 const float tr0 = tau0 * PD(e)[q], tr1 = tau0 * PD(e)[QP + q], tr2 = tau2 * PD(e)[2 * QP + q];
-                float *fr = FR(e);
+                float *fr = FX(e);
                 fr[q] -= (d11 * (2.f * u0) - d01 * u1) * tr0 - d01 * u0 * tr1 + d11 * tr2;
                 fr[GG + q] -= (-d10 * (2.f * u0) + d00 * u1) * tr0 + d00 * u0 * tr1 - d10 * tr2;
                 fr[VS + q] -= +d11 * u1 * tr0 + (d11 * u0 - d01 * (2.f * u1)) * tr1 - d01 * tr2;
@@ -382,7 +397,10 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                 fr[2 * VS + GG + q] = -(-d10 * tr0 + d00 * tr1);
             }
             __syncwarp();
-            integrate(1);
+            float c[M::NT2][4];
+            warp_gemm_tf32<M::KS2, M::NT2>(FX(ra) + rvv * VS, FX(ra + 2) + rvv * VS, nullptr, nullptr, intB, tig,
+                                            lane, c);
+            scatter(c, 1);
         }
         __syncwarp();
     }

@@ -101,11 +101,48 @@ void fill_tables(const hp_basis_tables &b, DevTables<R, P> &t) {
 //   W_r(q, m)   = -dgxwtx(c, i) gnwtnn0(m, j)
 //   W_s(q, m)   = -(x0(i) dgxwtx(c, i) gnwtnn0(m, j) + gxwtx(c, i) dgnwtn(m, j))
 // so that lf(m) = sum_q flux_r(q) W_r(q, m) + flux_s(q) W_s(q, m) is intgrtrs' result.
+// The strong residual's point-to-point operator (derivr + derivs, proj.cpp:339-402, as a
+// dense matrix): res(i, j) = sum over input points (q, l) of
+//   flux_r(q, l) Dr[(q, l), (i, j)] + flux_s(q, l) Ds[(q, l), (i, j)], with
+//   Dr = [l == j] n0(j) (q == i ? dltx(i) sum_{q' != i} dltx1(i, q') : dltx(q) dltx1(i, q))
+//   Ds = [l == j] n0(j) (q == i ? dltx(i) sum_{q' != i} dltn1(i, q') : dltx(q) dltn1(i, q))
+//      + [q == i] (l == j ? dltn(j) sum_{l' != j} dltn2(j, l') : dltn(l) dltn2(j, l)).
+inline double strong_op(const hp_basis_tables &b, int G, int k, int qo) {
+    const int GG = G * G;
+    const bool s_part = k >= GG;
+    const int qi = s_part ? k - GG : k;
+    const int q = qi / G, l = qi - q * G, i = qo / G, j = qo - i * G;
+    double v = 0.0;
+    if (l == j) {
+        double t;
+        if (q == i) {
+            double sum = 0.0;
+            for (int qq = 0; qq < G; ++qq)
+                if (qq != i) sum += s_part ? b.dltn1[i][qq] : b.dltx1[i][qq];
+            t = b.dltx[i] * sum;
+        } else {
+            t = b.dltx[q] * (s_part ? b.dltn1[i][q] : b.dltx1[i][q]);
+        }
+        v += b.n0[j] * t;
+    }
+    if (s_part && q == i) {
+        if (l == j) {
+            double sum = 0.0;
+            for (int ll = 0; ll < G; ++ll)
+                if (ll != j) sum += b.dltn2[j][ll];
+            v += b.dltn[j] * sum;
+        } else {
+            v += b.dltn[l] * b.dltn2[j][l];
+        }
+    }
+    return v;
+}
+
 template <int P>
 void build_ins_mma(const hp_basis_tables &b, std::vector<double> &ops, InsMmaSmall<P> &sm) {
     using M = InsMma<P>;
     constexpr int G = M::G, GG = M::GG, T = M::T;
-    ops.assign(M::PROJ_LEN + M::INT_LEN, 0.0);
+    ops.assign(M::PROJ_LEN + M::INT_LEN + M::DER_LEN, 0.0);
     for (int op = 0; op < 3; ++op)
         for (int nt = 0; nt < M::NT; ++nt)
             for (int ks = 0; ks < M::KS; ++ks)
@@ -128,6 +165,14 @@ void build_ins_mma(const hp_basis_tables &b, std::vector<double> &ops, InsMmaSma
                 const double w = k < GG ? -b.dgxwtx[c][i] * b.gnwtnn0[m][j]
                                         : -(b.x0[i] * b.dgxwtx[c][i] * b.gnwtnn0[m][j] + b.gxwtx[c][i] * b.dgnwtn[m][j]);
                 ib[((size_t)nt * M::KS2 + ks) * 32 + l] = w;
+            }
+    double *db = ops.data() + M::PROJ_LEN + M::INT_LEN;
+    for (int nt = 0; nt < M::NT; ++nt)
+        for (int ks = 0; ks < M::KS2; ++ks)
+            for (int l = 0; l < 32; ++l) {
+                const int k = ks * 4 + (l & 3), qo = nt * 8 + (l >> 2);
+                if (k >= 2 * GG || qo >= GG) continue;
+                db[((size_t)nt * M::KS2 + ks) * 32 + l] = strong_op(b, G, k, qo);
             }
     for (int i = 0; i < G; ++i) {
         sm.dltx[i] = b.dltx[i]; sm.dltn[i] = b.dltn[i]; sm.n0[i] = b.n0[i]; sm.x0[i] = b.x0[i];
@@ -155,7 +200,7 @@ template <int P>
 void build_ins_tf32(const hp_basis_tables &b, std::vector<float> &ops, InsMmaSmallF<P> &sm) {
     using M = InsTf32<P>;
     constexpr int G = M::G, GG = M::GG, T = M::T;
-    ops.assign(M::PROJ_LEN + M::INT_LEN, 0.f);
+    ops.assign(M::PROJ_LEN + M::INT_LEN + M::DER_LEN, 0.f);
     auto proj = [&](int op, int q, int m) -> double {
         if (q >= GG || m >= T) return 0.0;
         const int i = q / G, j = q - i * G, c = ModeCols<P>::col(m);
@@ -185,6 +230,16 @@ void build_ins_tf32(const hp_basis_tables &b, std::vector<float> &ops, InsMmaSma
                 const int k = ks * 8 + (l & 3), m = nt * 8 + (l >> 2);
                 ib[at] = to_tf32(wgt(k, m));
                 ib[at + 1] = to_tf32(wgt(k + 4, m));
+            }
+    float *db = ops.data() + M::PROJ_LEN + M::INT_LEN;
+    auto der = [&](int k, int qo) -> double { return (k < 2 * GG && qo < GG) ? strong_op(b, G, k, qo) : 0.0; };
+    for (int nt = 0; nt < M::NT; ++nt)
+        for (int ks = 0; ks < M::KS2; ++ks)
+            for (int l = 0; l < 32; ++l) {
+                const size_t at = (((size_t)nt * M::KS2 + ks) * 32 + l) * 2;
+                const int k = ks * 8 + (l & 3), qo = nt * 8 + (l >> 2);
+                db[at] = to_tf32(der(k, qo));
+                db[at + 1] = to_tf32(der(k + 4, qo));
             }
     for (int i = 0; i < G; ++i) {
         sm.dltx[i] = (float)b.dltx[i]; sm.dltn[i] = (float)b.dltn[i];
@@ -381,9 +436,10 @@ struct LaunchImpl {
     static constexpr bool DBL = std::is_same<R, double>::value;
     static int mma_smem() {
         if constexpr (DBL)
-            return (int)(((sizeof(InsMmaSmall<P>) + 15) / 16) * 16 + (size_t)2 * InsMma<P>::S_EL * InsMma<P>::WPC * 8);
+            return (int)(((sizeof(InsMmaSmall<P>) + 15) / 16) * 16 + (size_t)2 * InsMma<P>::S_EL * InsMma<P>::WPC * 8 +
+                         InsMma<P>::SMEM_IDX);
         else
-            return (int)(((sizeof(InsMmaSmallF<P>) + 15) / 16) * 16 + (size_t)4 * InsTf32<P>::S_EL * InsTf32<P>::WPC * 4);
+            return (int)((size_t)4 * InsTf32<P>::S_EL * InsTf32<P>::WPC * 4 + InsTf32<P>::SMEM_IDX);
     }
     static void elem_mma(const void *ops, const void *small, const void *tab, const Mesh &m, const State<R> &s,
                          const Phys &ph, int stage, int zero_rr, int diff, int nsm, const Tune &tn, cudaStream_t st) {
@@ -394,15 +450,16 @@ struct LaunchImpl {
                 const long npair = ((long)m.ntri + 1) / 2;
                 const int blocks = (int)std::min<long>((npair + MM::WPC - 1) / MM::WPC, (long)nsm * MM::MINB * 4);
                 k_rsdl_ins_mma<P><<<blocks, MM::WPC * 32, mma_smem(), st>>>(
-                    o, o + MM::PROJ_LEN, *static_cast<const InsMmaSmall<P> *>(small), m, s, ph, stage, zero_rr);
+                    o, o + MM::PROJ_LEN, o + MM::PROJ_LEN + MM::INT_LEN, *static_cast<const InsMmaSmall<P> *>(small), m,
+                    s, ph, stage, zero_rr);
             } else {
                 using MM = InsTf32<P>;
                 const float2 *o = static_cast<const float2 *>(ops);
                 const long nquad = ((long)m.ntri + 3) / 4;
                 const int blocks = (int)std::min<long>((nquad + MM::WPC - 1) / MM::WPC, (long)nsm * MM::MINB * 4);
                 k_rsdl_ins_tf32<P><<<blocks, MM::WPC * 32, mma_smem(), st>>>(
-                    o, o + MM::PROJ_LEN / 2, *static_cast<const InsMmaSmallF<P> *>(small), m, s, ph, stage, zero_rr,
-                    diff);
+                    o, o + MM::PROJ_LEN / 2, o + (MM::PROJ_LEN + MM::INT_LEN) / 2,
+                    *static_cast<const InsMmaSmallF<P> *>(small), m, s, ph, stage, zero_rr, diff);
             }
             if (m.ncurved > 0) {
                 constexpr int EPC = C::WPC * C::EPW;
@@ -835,7 +892,10 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
         c->L32.mma_build(*b, ops32, c->mma_small32);
         if ((r = upload(c, (unsigned char **)&c->d_mma, ops.data(), ops.size()))) return fail(r);
         if ((r = upload(c, (unsigned char **)&c->d_mma32, ops32.data(), ops32.size()))) return fail(r);
-        c->elem_kind = HP_ELEM_TENSOR;
+        // at p = 1 and 2 the scalar kernel's lane groups (4 and 2 triangles per warp) are
+        // faster than two triangles per tensor-core warp (measured: 0.080 vs 0.153 ms and
+        // 0.205 vs 0.205 ms for 131k triangles)
+        c->elem_kind = c->p >= 3 ? HP_ELEM_TENSOR : HP_ELEM_SCALAR;
     }
     DevMinv<double> hm;
     fill_minv<double>(*b, hm);

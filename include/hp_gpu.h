@@ -197,11 +197,13 @@ int hp_gpu_maxres(hp_gpu_ctx *ctx, double *out, double *mx);
 int hp_gpu_resnorm(hp_gpu_ctx *ctx, double *l2, double *linf);
 
 /* FP64 element kernel of rsdl (no counterpart in the reference, which has one CPU
- * loop, tri_hp/nstage.cpp:52-73). HP_ELEM_TENSOR (the default for ins): projection and
- * intgrtrs of two triangles per warp on the FP64 tensor cores (mma.m8n8k4.f64) with
- * dense per-point operators; HP_ELEM_SCALAR: the sum-factorised warp kernel (cd always
- * uses it). Both give the reference's residual up to rounding. HP_ENOTSUP when the
- * tensor-core kernel is not built for the context's physics. */
+ * loop, tri_hp/nstage.cpp:52-73). HP_ELEM_TENSOR (the default for ins at p >= 3):
+ * projection, intgrtrs and the strong residual of two triangles per warp on the FP64
+ * tensor cores (mma.m8n8k4.f64) with dense per-point operators, and for the FP32
+ * smoother's correction form four triangles per warp on TF32 (mma.m16n8k8);
+ * HP_ELEM_SCALAR (the default at p <= 2, and cd always): the sum-factorised warp kernel.
+ * Both give the reference's residual up to rounding. HP_ENOTSUP when the tensor-core
+ * kernel is not built for the context's physics. */
 #define HP_ELEM_SCALAR 0
 #define HP_ELEM_TENSOR 1
 int hp_gpu_set_element_kernel(hp_gpu_ctx *ctx, int kind);
