@@ -41,9 +41,12 @@ struct InsMma {
     static constexpr int MINB = P <= 4 ? 4 : 3;    // CTAs per SM the register budget allows
     static constexpr int NG = NT < 8 ? NT : 8;     // projection n-tiles accumulated together
     static constexpr size_t PROJ_LEN = (size_t)3 * NT * KS * 32, INT_LEN = (size_t)NT2 * KS2 * 32;
-    // strong residual: C[8 x GG] = [flux_r | flux_s][8 x 2GG] * D[2GG x GG] (derivr + derivs)
-    static constexpr size_t DER_LEN = (size_t)NT * KS2 * 32;
-    static constexpr int IDX = 12;  // staged mesh integers per triangle: pnt[3], seg[3], sgn[3]
+    // strong residual (derivr + derivs) as tensor products of the 1D derivative operators:
+    // A fragments of Ar | As1 ([MT][2 KR][32], rows i, k = q) and As2 ([MT][KR][32], rows j,
+    // k = l); the point data are the B operands, columns (triangle, variable, point)
+    static constexpr int KR = (G + 3) / 4, MT = (G + 7) / 8, NCOL = 6 * G, NTB = (NCOL + 7) / 8;
+    static constexpr size_t DER_LEN = (size_t)MT * 3 * KR * 32;
+    static constexpr int IDX = 16;  // staged mesh integers per triangle: pnt[3], seg[3], sgn[3], vpos[3], spos[3]
     static constexpr size_t SMEM_IDX = (size_t)WPC * 2 * IDX * sizeof(int);
     static_assert(4 * T <= 4 * QP, "gathered modes must fit the PD block");
 };
@@ -144,11 +147,12 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
         auto TE = [&](int e) { return e ? tb1 : ta; };
         auto ACT = [&](int e) { return e ? actb : acta; };
         __syncwarp();
-        // the pair's connectivity, staged once: pnt[0..2], seg[3..5], sgn[6..8]
-        if (lane < 18) {
-            const int e = lane / 9, k = lane - e * 9, t = TE(e);
-            midx[e * M::IDX + k] = k < 3 ? mesh.tri_pnt[3 * t + k]
-                                         : (k < 6 ? mesh.tri_seg[3 * t + k - 3] : mesh.tri_sgn[3 * t + k - 6]);
+        // the pair's connectivity, staged once: pnt[0..2], seg[3..5], sgn[6..8], and the
+        // assembly slots vpos[9..11], spos[12..14]
+        if (lane < 30) {
+            const int e = lane / 15, k = lane - e * 15, t = TE(e), c = k % 3;
+            const int *src = k < 3 ? mesh.tri_pnt : (k < 6 ? mesh.tri_seg : (k < 9 ? mesh.tri_sgn : (k < 12 ? mesh.vpos : mesh.spos)));
+            midx[e * M::IDX + k] = src ? src[3 * t + c] : 0;
         }
         __syncwarp();
         // ---- gather (ugtouht, gtol.cpp:14-55) into the PD block
@@ -175,7 +179,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
         }
         // geometry of both triangles: ldcrd(n,0) = (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2, and the
         // inscribed-radius length scale of the SUPG tau (tri_mesh/tprims.cpp:224-241)
-        double gd[2][4], hh[2];
+        double gd[2][4], hh[2], gk[2][3];  // gk: mu / |J|, 2 nu / h, adis h / |J|
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
             const int *ix = midx + e * M::IDX;
@@ -190,6 +194,10 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
                                  sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
             hh[e] = (area / perim) / (0.25 * (P + 1) * (P + 1));
+            const double cj = gd[e][0] * gd[e][3] - gd[e][2] * gd[e][1];
+            gk[e][0] = mu / cj;
+            gk[e][1] = 2. * (mu / rho) / hh[e];
+            gk[e][2] = ph.adis * hh[e] / cj;
         }
         __syncwarp();
         // ---- projection on the tensor cores (proj.cpp:22-119 as dense per-point operators)
@@ -249,8 +257,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             fi[2 * VS + GG + q] = m1;
             if (beta > 0.0) {
                 const double dr0 = PD(e)[q], dr1 = PD(e)[QP + q], ds0 = PD(e)[2 * QP + q], ds1 = PD(e)[3 * QP + q];
-                const double cjcb = d00 * d11 - d10 * d01;
-                const double cjcbi = mu / cjcb;
+                const double cjcbi = e ? gk[1][0] : gk[0][0];
                 const double v0000 = -cjcbi * (2. * d11 * d11 + d01 * d01);
                 const double v0011 = -cjcbi * (2. * d10 * d10 + d00 * d00);
                 const double v0001 = cjcbi * (2. * d11 * d10 + d01 * d00);
@@ -292,7 +299,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                             gsi = (ix[3 + i] * SM + kk) * NV + rv;
                         }
                         double *el = part ? st.elre : st.elim;
-                        if (el) el[((size_t)t * BM + m) * NV + rv] = val;
+                        if (el) el[asm_slot(mesh, NV, SM, ix[9 + (m < 3 ? m : 0)], ix[12 + (m < 3 ? 0 : (m - 3) / SM)], m, rv)] = val;
                         else if (gsi < 0) atomicAdd((part ? st.rrv : st.resv) + ix[m] * NV + rv, val);
                         else atomicAdd((part ? st.rrs : st.ress) + gsi, val);
                     } else {
@@ -317,59 +324,95 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             scatter(c, 0);
         }
         if (beta > 0.0) {
-            // ---- strong residual at the points (derivr + derivs of the full fluxes,
-            //      proj.cpp:339-402) on the tensor cores, into PD
+            // ---- strong residual at the points (derivr + derivs of the full fluxes FI + FX,
+            //      proj.cpp:339-402) on the tensor cores as tensor products of the 1D
+            //      operators: res(i, j) = n0(j) (Ar fr + As1 fs)(i, j) + (As2 fs^T)(j, i), the
+            //      columns of the B operand being (triangle, variable, point of the other
+            //      direction); into PD
             {
-                constexpr int NTC = M::NT < 8 ? M::NT : 8;
+                const double *AR = derB, *AS = derB + M::MT * 2 * M::KR * 32;
+                auto col = [&](int n, int &e, int &var, int &j) {
+                    e = n / (3 * G);
+                    const int rem = n - e * 3 * G;
+                    var = rem / G;
+                    j = rem - var * G;
+                };
+                // part 1: rows i, columns (e, var, j)
+#pragma unroll 1
+                for (int nt = 0; nt < M::NTB; ++nt) {
+                    int e, var, j;
+                    const int n = nt * 8 + grow;
+                    col(n < M::NCOL ? n : 0, e, var, j);
+                    const bool colok = n < M::NCOL;
+                    const double *fi = FI(e) + var * VS, *fx = FX(e) + var * VS;
+                    double c[M::MT][2];
 #pragma unroll
-                for (int nt0 = 0; nt0 < M::NT; nt0 += NTC) {
-                    constexpr int NTL = NTC;
-                    double c[NTL][2];
-                    double c2[NTL][2];
+                    for (int mt = 0; mt < M::MT; ++mt) c[mt][0] = c[mt][1] = 0.0;
 #pragma unroll
-                    for (int g = 0; g < NTL; ++g) c[g][0] = c[g][1] = c2[g][0] = c2[g][1] = 0.0;
-                    const double *ai = FI(re_) + (rv < 3 ? rv : 2) * VS, *ax = FX(re_) + (rv < 3 ? rv : 2) * VS;
-#pragma unroll 4
-                    for (int ks = 0; ks < M::KS2; ks += 2) {
-                        const int k0 = ks * 4 + gcol, k1 = k0 + 4;
-                        const double a0 = ai[k0] + ax[k0];
-                        const double a1 = ks + 1 < M::KS2 ? ai[k1] + ax[k1] : 0.0;
+                    for (int ks = 0; ks < 2 * M::KR; ++ks) {
+                        const int blk = ks / M::KR, q = (ks - blk * M::KR) * 4 + gcol;
+                        const int off = blk * GG + q * G + j;
+                        const double bv = (colok && q < G) ? fi[off] + fx[off] : 0.0;
 #pragma unroll
-                        for (int g = 0; g < NTL; ++g) {
-                            if (nt0 + g >= M::NT) continue;
-                            const double *b = derB + ((size_t)(nt0 + g) * M::KS2 + ks) * 32 + lane;
-                            dmma884(c[g][0], c[g][1], a0, __ldg(b));
-                            if (ks + 1 < M::KS2) dmma884(c2[g][0], c2[g][1], a1, __ldg(b + 32));
+                        for (int mt = 0; mt < M::MT; ++mt)
+                            dmma884(c[mt][0], c[mt][1], __ldg(AR + ((size_t)mt * 2 * M::KR + ks) * 32 + lane), bv);
+                    }
+#pragma unroll
+                    for (int mt = 0; mt < M::MT; ++mt)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int i = mt * 8 + grow, nc = nt * 8 + gcol * 2 + h;
+                            if (i >= G || nc >= M::NCOL) continue;
+                            int e2, v2, j2;
+                            col(nc, e2, v2, j2);
+                            PD(e2)[v2 * QP + i * G + j2] = c[mt][h] * tb.n0[j2];
                         }
-                    }
-                    if (rv < 3) {
-                        double *dst = PD(re_) + rv * QP;
+                }
+                __syncwarp();
+                // part 2: rows j, columns (e, var, i)
+#pragma unroll 1
+                for (int nt = 0; nt < M::NTB; ++nt) {
+                    int e, var, i;
+                    const int n = nt * 8 + grow;
+                    col(n < M::NCOL ? n : 0, e, var, i);
+                    const bool colok = n < M::NCOL;
+                    const double *fi = FI(e) + var * VS + GG + i * G, *fx = FX(e) + var * VS + GG + i * G;
+                    double c[M::MT][2];
 #pragma unroll
-                        for (int g = 0; g < NTL; ++g)
-                            if (nt0 + g < M::NT) {
-                                const int q = (nt0 + g) * 8 + gcol * 2;
-                                dst[q] = c[g][0] + c2[g][0];
-                                dst[q + 1] = c[g][1] + c2[g][1];
-                            }
+                    for (int mt = 0; mt < M::MT; ++mt) c[mt][0] = c[mt][1] = 0.0;
+#pragma unroll
+                    for (int ks = 0; ks < M::KR; ++ks) {
+                        const int l = ks * 4 + gcol;
+                        const double bv = (colok && l < G) ? fi[l] + fx[l] : 0.0;
+#pragma unroll
+                        for (int mt = 0; mt < M::MT; ++mt)
+                            dmma884(c[mt][0], c[mt][1], __ldg(AS + ((size_t)mt * M::KR + ks) * 32 + lane), bv);
                     }
+#pragma unroll
+                    for (int mt = 0; mt < M::MT; ++mt)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int j = mt * 8 + grow, nc = nt * 8 + gcol * 2 + h;
+                            if (j >= G || nc >= M::NCOL) continue;
+                            int e2, v2, i2;
+                            col(nc, e2, v2, i2);
+                            PD(e2)[v2 * QP + i2 * G + j] += c[mt][h];
+                        }
                 }
             }
             __syncwarp();
             // ---- pointwise SUPG terms (ins/rsdl.cpp:341-431, CALC_TAU2): FX becomes the real
             //      flux pairs, viscous minus SUPG for u, v and the continuity term for p
-            const double nu = mu / rho;
             for (int w = lane; w < 2 * GG; w += 32) {
                 const int e = w / GG, q = w - e * GG;
                 const double d00 = e ? gd[1][0] : gd[0][0], d01 = e ? gd[1][1] : gd[0][1];
                 const double d10 = e ? gd[1][2] : gd[0][2], d11 = e ? gd[1][3] : gd[0][3];
-                const double he = e ? hh[1] : hh[0];
-                const double cjcb = d00 * d11 - d10 * d01;
                 const double u0 = PV(e)[q], u1 = PV(e)[QP + q];
                 const double qv = u0 * u0 + u1 * u1;
-                const double t2 = 2. * nu / he;
+                const double t2 = e ? gk[1][1] : gk[0][1];
                 double gam = 3.0 * qv + t2 * t2;
                 if (ph.mu + ph.bd0 == 0.0) gam = (gam > 0.1 ? gam : 0.1);
-                const double tau0 = ph.adis * he / (cjcb * sqrt(gam));
+                const double tau0 = (e ? gk[1][2] : gk[0][2]) / sqrt(gam);
                 const double tau2 = sqrt(qv) * tau0;
                 const double tr0 = tau0 * PD(e)[q], tr1 = tau0 * PD(e)[QP + q], tr2 = tau2 * PD(e)[2 * QP + q];
                 double *fx = FX(e);

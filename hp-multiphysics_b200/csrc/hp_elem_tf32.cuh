@@ -37,12 +37,18 @@ struct InsTf32 {
     static constexpr int WPC = 4;
     static constexpr int MINB = P <= 4 ? 4 : 3;
     static constexpr int NG = NT < 8 ? NT : 8;
-    // B fragments: two floats per lane per MMA; DER: the strong residual's point-to-point
-    // operator (derivr + derivs), C[16 x GG] = [flux_r | flux_s][16 x 2GG] * D[2GG x GG]
+    // B fragments: two floats per lane per MMA. DER: the strong residual (derivr + derivs)
+    // as tensor products of the 1D operators, A fragments (four floats per lane per k-step)
+    // of [Ar | As1] (2 KR k-steps) and As2 (KR k-steps); the point data are the B operands,
+    // columns (triangle, variable, point of the other direction)
     static constexpr size_t PROJ_LEN = (size_t)3 * NT * KS * 64, INT_LEN = (size_t)NT2 * KS2 * 64;
-    static constexpr size_t DER_LEN = (size_t)NT * KS2 * 64;
+    static constexpr int KR = (G + 7) / 8, NCOL = 12 * G, NTB = (NCOL + 7) / 8;
+    static_assert(G <= 16, "one m-tile of 16 rows per 1D operator");
+    static constexpr size_t DER_LEN = (size_t)3 * KR * 32 * 4;
     static constexpr int IDX = 12;  // staged mesh integers per triangle: pnt[3], seg[3], sgn[3]
-    static constexpr size_t SMEM_IDX = (size_t)WPC * 4 * IDX * sizeof(int);
+    // per triangle: metrics d00, d01, d10, d11, mu / |J|, 2 nu / h, adis h / |J|, unused
+    static constexpr int GEO = 8;
+    static constexpr size_t SMEM_IDX = (size_t)WPC * 4 * (IDX * sizeof(int) + GEO * sizeof(float));
     static_assert(4 * T <= 4 * QP, "gathered modes must fit the PD block");
 };
 
@@ -124,13 +130,24 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
     constexpr int G = M::G, GG = M::GG, T = M::T, BM = M::BM, IM = M::IM, NV = 3, QP = M::QP, VS = M::VS;
     constexpr int SM = (M::SM > 0 ? M::SM : 1);
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    (void)small;
+    InsMmaSmallF<P> &tb = *reinterpret_cast<InsMmaSmallF<P> *>(smem_raw);
+    {
+        const int n4 = sizeof(InsMmaSmallF<P>) / 4;
+        const int *src = reinterpret_cast<const int *>(&small);
+        int *dst = reinterpret_cast<int *>(smem_raw);
+        for (int k = threadIdx.x; k < n4; k += blockDim.x) dst[k] = src[k];
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int grp = lane >> 2, tig = lane & 3;
     const int ra = grp >> 2, rv = grp & 3;  // fragment row grp -> (triangle ra, variable rv); row grp + 8 -> ra + 2
-    float *base = reinterpret_cast<float *>(smem_raw) + (size_t)warp * 4 * M::S_EL;
-    int *midx = reinterpret_cast<int *>(reinterpret_cast<float *>(smem_raw) + (size_t)M::WPC * 4 * M::S_EL) +
+    constexpr size_t SMALL = ((sizeof(InsMmaSmallF<P>) + 15) / 16) * 16;
+    float *base = reinterpret_cast<float *>(smem_raw + SMALL) + (size_t)warp * 4 * M::S_EL;
+    int *midx = reinterpret_cast<int *>(reinterpret_cast<float *>(smem_raw + SMALL) + (size_t)M::WPC * 4 * M::S_EL) +
                 warp * 4 * M::IDX;
+    float *geo = reinterpret_cast<float *>(reinterpret_cast<int *>(reinterpret_cast<float *>(smem_raw + SMALL) +
+                                                                   (size_t)M::WPC * 4 * M::S_EL) +
+                                           M::WPC * 4 * M::IDX) +
+                 warp * 4 * M::GEO;
     // per triangle as in k_rsdl_ins_mma: PV u, v, p; PD modes / derivatives / strong
     // residual; FI imaginary flux pairs; FX viscous, then real flux pairs
     auto PV = [&](int e) { return base + e * M::S_EL; };
@@ -162,6 +179,26 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             const int e = w / 9, k = w - e * 9, t = TE(e);
             midx[e * M::IDX + k] = k < 3 ? mesh.tri_pnt[3 * t + k]
                                          : (k < 6 ? mesh.tri_seg[3 * t + k - 3] : mesh.tri_sgn[3 * t + k - 6]);
+        }
+        __syncwarp();
+        if (lane < 4) {  // per-triangle geometry: ldcrd metrics and the tau length scale
+            const int *ix = midx + lane * M::IDX;
+            const double x0d = mesh.pnts[2 * ix[0]], y0d = mesh.pnts[2 * ix[0] + 1];
+            const double x1d = mesh.pnts[2 * ix[1]], y1d = mesh.pnts[2 * ix[1] + 1];
+            const double x2d = mesh.pnts[2 * ix[2]], y2d = mesh.pnts[2 * ix[2] + 1];
+            const float d00 = (float)(0.5 * (x2d - x1d)), d01 = (float)(0.5 * (x0d - x1d));
+            const float d10 = (float)(0.5 * (y2d - y1d)), d11 = (float)(0.5 * (y0d - y1d));
+            const double dx1 = x0d - x2d, dy1 = y0d - y2d, dx2 = x1d - x0d, dy2 = y1d - y0d;
+            const double area = dx1 * dy2 - dy1 * dx2;
+            const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
+                                 sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
+            const float he = (float)((area / perim) / (0.25 * (P + 1) * (P + 1)));
+            const float cjcb = d00 * d11 - d10 * d01;
+            float *gg = geo + lane * M::GEO;
+            gg[0] = d00; gg[1] = d01; gg[2] = d10; gg[3] = d11;
+            gg[4] = mu / cjcb;
+            gg[5] = 2.f * (float)(ph.mu / ph.rho) / he;
+            gg[6] = (float)ph.adis * he / cjcb;
         }
         __syncwarp();
         // ---- gather the modes (ugtouht, gtol.cpp:14-55) into the PD block
@@ -234,12 +271,8 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
         for (int w = lane; w < 4 * GG; w += 32) {
             const int e = w / GG, q = w - e * GG;
             const int t = TE(e);
-            const int *ix = midx + e * M::IDX;
-            const int p0 = ix[0], p1 = ix[1], p2 = ix[2];
-            const float d00 = (float)(0.5 * (mesh.pnts[2 * p2] - mesh.pnts[2 * p1]));
-            const float d01 = (float)(0.5 * (mesh.pnts[2 * p0] - mesh.pnts[2 * p1]));
-            const float d10 = (float)(0.5 * (mesh.pnts[2 * p2 + 1] - mesh.pnts[2 * p1 + 1]));
-            const float d11 = (float)(0.5 * (mesh.pnts[2 * p0 + 1] - mesh.pnts[2 * p1 + 1]));
+            const float *gg = geo + e * M::GEO;
+            const float d00 = gg[0], d01 = gg[1], d10 = gg[2], d11 = gg[3];
             const float u0 = PV(e)[q], u1 = PV(e)[QP + q], pp = PV(e)[2 * QP + q];
             const float m0 = +d11 * (rho * u0) - d01 * (rho * u1);
             const float m1 = -d10 * (rho * u0) + d00 * (rho * u1);
@@ -265,8 +298,7 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             fi[2 * VS + GG + q] = m1;
             if (beta > 0.f) {
                 const float dr0 = PD(e)[q], dr1 = PD(e)[QP + q], ds0 = PD(e)[2 * QP + q], ds1 = PD(e)[3 * QP + q];
-                const float cjcb = d00 * d11 - d10 * d01;
-                const float cjcbi = mu / cjcb;
+                const float cjcbi = gg[4];
                 const float v0000 = -cjcbi * (2.f * d11 * d11 + d01 * d01);
                 const float v0011 = -cjcbi * (2.f * d10 * d10 + d00 * d00);
                 const float v0001 = cjcbi * (2.f * d11 * d10 + d01 * d00);
@@ -333,46 +365,71 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             scatter(c, 0);
         }
         if (beta > 0.f) {
-            // ---- strong residual of FI + FX at the points (derivr / derivs) on TF32, into PD
+            // ---- strong residual of FI + FX at the points (derivr / derivs, proj.cpp:339-402)
+            //      on TF32 as tensor products of the 1D operators: part 1 rows i, columns
+            //      (triangle, variable, j): n0(j) (Ar fr + As1 fs); part 2 rows j, columns
+            //      (triangle, variable, i): As2 fs^T; into PD
             {
-                constexpr int NTC = M::NT < 8 ? M::NT : 8;
-#pragma unroll
-                for (int nt0 = 0; nt0 < M::NT; nt0 += NTC) {
-                    float c[NTC][4];
-                    warp_gemm_tf32<M::KS2, NTC>(FI(ra) + rvv * VS, FI(ra + 2) + rvv * VS, FX(ra) + rvv * VS,
-                                                FX(ra + 2) + rvv * VS, derB + (size_t)nt0 * M::KS2 * 32, tig, lane, c);
-                    if (rv < 3) {
-#pragma unroll
-                        for (int g = 0; g < NTC; ++g)
-                            if (nt0 + g < M::NT) {
-                                const int q = (nt0 + g) * 8 + tig * 2;
-                                PD(ra)[rv * QP + q] = c[g][0];
-                                PD(ra)[rv * QP + q + 1] = c[g][1];
-                                PD(ra + 2)[rv * QP + q] = c[g][2];
-                                PD(ra + 2)[rv * QP + q + 1] = c[g][3];
+                const float4 *AR = reinterpret_cast<const float4 *>(derB);
+                const float4 *AS = AR + 2 * M::KR * 32;
+                auto col = [&](int n, int &e, int &var, int &j) {
+                    e = n / (3 * G);
+                    const int rem = n - e * 3 * G;
+                    var = rem / G;
+                    j = rem - var * G;
+                };
+                auto a4 = [&](const float4 v, unsigned (&a)[4]) {
+                    a[0] = __float_as_uint(v.x); a[1] = __float_as_uint(v.y);
+                    a[2] = __float_as_uint(v.z); a[3] = __float_as_uint(v.w);
+                };
+#pragma unroll 1
+                for (int part = 0; part < 2; ++part) {
+                    const int nks = part ? M::KR : 2 * M::KR;
+#pragma unroll 1
+                    for (int nt = 0; nt < M::NTB; ++nt) {
+                        int e, var, x;
+                        const int n = nt * 8 + grp;
+                        col(n < M::NCOL ? n : 0, e, var, x);
+                        const bool colok = n < M::NCOL;
+                        const float *fi = FI(e) + var * VS, *fx = FX(e) + var * VS;
+                        float c[4] = {0.f, 0.f, 0.f, 0.f};
+                        for (int ks = 0; ks < nks; ++ks) {
+                            unsigned a[4];
+                            a4(__ldg((part ? AS : AR) + (size_t)ks * 32 + lane), a);
+                            float2 bv = make_float2(0.f, 0.f);
+                            if (part == 0) {  // k = q of [fr | fs] at column point j = x
+                                const int blk = ks / M::KR, q0 = (ks - blk * M::KR) * 8 + tig, q1 = q0 + 4;
+                                if (colok && q0 < G) bv.x = fi[blk * GG + q0 * G + x] + fx[blk * GG + q0 * G + x];
+                                if (colok && q1 < G) bv.y = fi[blk * GG + q1 * G + x] + fx[blk * GG + q1 * G + x];
+                            } else {  // k = l of fs at column point i = x
+                                const int l0 = ks * 8 + tig, l1 = l0 + 4;
+                                if (colok && l0 < G) bv.x = fi[GG + x * G + l0] + fx[GG + x * G + l0];
+                                if (colok && l1 < G) bv.y = fi[GG + x * G + l1] + fx[GG + x * G + l1];
                             }
+                            bv.x = __uint_as_float(f2tf32(bv.x));
+                            bv.y = __uint_as_float(f2tf32(bv.y));
+                            mma_tf32(c, a[0], a[1], a[2], a[3], bv);
+                        }
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) {
+                            const int row = grp + (r >> 1) * 8, nc = nt * 8 + tig * 2 + (r & 1);
+                            if (row >= G || nc >= M::NCOL) continue;
+                            int e2, v2, x2;
+                            col(nc, e2, v2, x2);
+                            if (part == 0) PD(e2)[v2 * QP + row * G + x2] = c[r] * tb.n0[x2];
+                            else PD(e2)[v2 * QP + x2 * G + row] += c[r];
+                        }
                     }
+                    __syncwarp();
                 }
             }
             __syncwarp();
             // ---- SUPG with tau of the base state (correction form) or of the state (plain)
-            const float nu = (float)(ph.mu / ph.rho);
             for (int w = lane; w < 4 * GG; w += 32) {
                 const int e = w / GG, q = w - e * GG;
                 const int t = TE(e);
-                const int *ix = midx + e * M::IDX;
-                const int p0 = ix[0], p1 = ix[1], p2 = ix[2];
-                const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
-                const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
-                const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
-                const float d00 = (float)(0.5 * (x2d - x1d)), d01 = (float)(0.5 * (x0d - x1d));
-                const float d10 = (float)(0.5 * (y2d - y1d)), d11 = (float)(0.5 * (y0d - y1d));
-                const double dx1 = x0d - x2d, dy1 = y0d - y2d, dx2 = x1d - x0d, dy2 = y1d - y0d;
-                const double area = dx1 * dy2 - dy1 * dx2;
-                const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
-                                     sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
-                const float he = (float)((area / perim) / (0.25 * (P + 1) * (P + 1)));
-                const float cjcb = d00 * d11 - d10 * d01;
+                const float *gg = geo + e * M::GEO;
+                const float d00 = gg[0], d01 = gg[1], d10 = gg[2], d11 = gg[3];
                 float u0 = PV(e)[q], u1 = PV(e)[QP + q], qv;
                 if (corr) {
                     const float b0 = st.bpt[((size_t)t * 2) * GG + q], b1 = st.bpt[((size_t)t * 2 + 1) * GG + q];
@@ -382,10 +439,10 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                 } else {
                     qv = u0 * u0 + u1 * u1;
                 }
-                const float t2 = 2.f * nu / he;
+                const float t2 = gg[5];
                 float gam = 3.0f * qv + t2 * t2;
                 if (ph.mu + ph.bd0 == 0.0) gam = (gam > 0.1f ? gam : 0.1f);
-                const float tau0 = (float)ph.adis * he / (cjcb * sqrtf(gam));
+                const float tau0 = gg[6] * rsqrtf(gam);
                 const float tau2 = sqrtf(qv) * tau0;
                 const float tr0 = tau0 * PD(e)[q], tr1 = tau0 * PD(e)[QP + q], tr2 = tau2 * PD(e)[2 * QP + q];
                 float *fr = FX(e);

@@ -101,41 +101,24 @@ void fill_tables(const hp_basis_tables &b, DevTables<R, P> &t) {
 //   W_r(q, m)   = -dgxwtx(c, i) gnwtnn0(m, j)
 //   W_s(q, m)   = -(x0(i) dgxwtx(c, i) gnwtnn0(m, j) + gxwtx(c, i) dgnwtn(m, j))
 // so that lf(m) = sum_q flux_r(q) W_r(q, m) + flux_s(q) W_s(q, m) is intgrtrs' result.
-// The strong residual's point-to-point operator (derivr + derivs, proj.cpp:339-402, as a
-// dense matrix): res(i, j) = sum over input points (q, l) of
-//   flux_r(q, l) Dr[(q, l), (i, j)] + flux_s(q, l) Ds[(q, l), (i, j)], with
-//   Dr = [l == j] n0(j) (q == i ? dltx(i) sum_{q' != i} dltx1(i, q') : dltx(q) dltx1(i, q))
-//   Ds = [l == j] n0(j) (q == i ? dltx(i) sum_{q' != i} dltn1(i, q') : dltx(q) dltn1(i, q))
-//      + [q == i] (l == j ? dltn(j) sum_{l' != j} dltn2(j, l') : dltn(l) dltn2(j, l)).
-inline double strong_op(const hp_basis_tables &b, int G, int k, int qo) {
-    const int GG = G * G;
-    const bool s_part = k >= GG;
-    const int qi = s_part ? k - GG : k;
-    const int q = qi / G, l = qi - q * G, i = qo / G, j = qo - i * G;
-    double v = 0.0;
-    if (l == j) {
-        double t;
-        if (q == i) {
-            double sum = 0.0;
-            for (int qq = 0; qq < G; ++qq)
-                if (qq != i) sum += s_part ? b.dltn1[i][qq] : b.dltx1[i][qq];
-            t = b.dltx[i] * sum;
-        } else {
-            t = b.dltx[q] * (s_part ? b.dltn1[i][q] : b.dltx1[i][q]);
-        }
-        v += b.n0[j] * t;
-    }
-    if (s_part && q == i) {
-        if (l == j) {
-            double sum = 0.0;
-            for (int ll = 0; ll < G; ++ll)
-                if (ll != j) sum += b.dltn2[j][ll];
-            v += b.dltn[j] * sum;
-        } else {
-            v += b.dltn[l] * b.dltn2[j][l];
-        }
-    }
-    return v;
+// The 1D derivative operators of derivr / derivs (proj.cpp:339-402) as matrices, so that
+// the strong residual at point (i, j) is
+//   res(i, j) = n0(j) (sum_q Ar(i, q) flux_r(q, j) + sum_q As1(i, q) flux_s(q, j))
+//             + sum_l As2(j, l) flux_s(i, l), with (which = 0: Ar, 1: As1, 2: As2)
+//   Ar(i, q)  = q == i ? dltx(i) sum_{q' != i} dltx1(i, q') : dltx(q) dltx1(i, q)
+//   As1(i, q) = q == i ? dltx(i) sum_{q' != i} dltn1(i, q') : dltx(q) dltn1(i, q)
+//   As2(j, l) = l == j ? dltn(j) sum_{l' != j} dltn2(j, l') : dltn(l) dltn2(j, l).
+inline double deriv_op(const hp_basis_tables &b, int G, int which, int r, int k) {
+    if (r >= G || k >= G) return 0.0;
+    auto tab = [&](int a, int c) {
+        return which == 0 ? b.dltx1[a][c] : (which == 1 ? b.dltn1[a][c] : b.dltn2[a][c]);
+    };
+    const double *dl = which == 2 ? b.dltn : b.dltx;
+    if (k != r) return dl[k] * tab(r, k);
+    double sum = 0.0;
+    for (int c = 0; c < G; ++c)
+        if (c != r) sum += tab(r, c);
+    return dl[r] * sum;
 }
 
 template <int P>
@@ -166,14 +149,20 @@ void build_ins_mma(const hp_basis_tables &b, std::vector<double> &ops, InsMmaSma
                                         : -(b.x0[i] * b.dgxwtx[c][i] * b.gnwtnn0[m][j] + b.gxwtx[c][i] * b.dgnwtn[m][j]);
                 ib[((size_t)nt * M::KS2 + ks) * 32 + l] = w;
             }
+    // A fragments of the 1D derivative operators (lane l holds A[row = l >> 2][k = l & 3]):
+    // [Ar | As1] per m-tile over 2 KR k-steps, then As2 over KR k-steps
     double *db = ops.data() + M::PROJ_LEN + M::INT_LEN;
-    for (int nt = 0; nt < M::NT; ++nt)
-        for (int ks = 0; ks < M::KS2; ++ks)
+    for (int mt = 0; mt < M::MT; ++mt)
+        for (int ks = 0; ks < 2 * M::KR; ++ks)
             for (int l = 0; l < 32; ++l) {
-                const int k = ks * 4 + (l & 3), qo = nt * 8 + (l >> 2);
-                if (k >= 2 * GG || qo >= GG) continue;
-                db[((size_t)nt * M::KS2 + ks) * 32 + l] = strong_op(b, G, k, qo);
+                const int blk = ks / M::KR, r = mt * 8 + (l >> 2), k = (ks - blk * M::KR) * 4 + (l & 3);
+                db[((size_t)mt * 2 * M::KR + ks) * 32 + l] = deriv_op(b, G, blk, r, k);
             }
+    double *da = db + M::MT * 2 * M::KR * 32;
+    for (int mt = 0; mt < M::MT; ++mt)
+        for (int ks = 0; ks < M::KR; ++ks)
+            for (int l = 0; l < 32; ++l)
+                da[((size_t)mt * M::KR + ks) * 32 + l] = deriv_op(b, G, 2, mt * 8 + (l >> 2), ks * 4 + (l & 3));
     for (int i = 0; i < G; ++i) {
         sm.dltx[i] = b.dltx[i]; sm.dltn[i] = b.dltn[i]; sm.n0[i] = b.n0[i]; sm.x0[i] = b.x0[i];
         for (int q = 0; q < G; ++q) {
@@ -231,15 +220,19 @@ void build_ins_tf32(const hp_basis_tables &b, std::vector<float> &ops, InsMmaSma
                 ib[at] = to_tf32(wgt(k, m));
                 ib[at + 1] = to_tf32(wgt(k + 4, m));
             }
+    // A fragments of the 1D derivative operators (mma.m16n8k8: lane l holds A[g][t], A[g + 8][t],
+    // A[g][t + 4], A[g + 8][t + 4] with g = l >> 2, t = l & 3 + 8 ks): [Ar | As1] then As2
     float *db = ops.data() + M::PROJ_LEN + M::INT_LEN;
-    auto der = [&](int k, int qo) -> double { return (k < 2 * GG && qo < GG) ? strong_op(b, G, k, qo) : 0.0; };
-    for (int nt = 0; nt < M::NT; ++nt)
-        for (int ks = 0; ks < M::KS2; ++ks)
+    for (int part = 0; part < 2; ++part)
+        for (int ks = 0; ks < (part ? M::KR : 2 * M::KR); ++ks)
             for (int l = 0; l < 32; ++l) {
-                const size_t at = (((size_t)nt * M::KS2 + ks) * 32 + l) * 2;
-                const int k = ks * 8 + (l & 3), qo = nt * 8 + (l >> 2);
-                db[at] = to_tf32(der(k, qo));
-                db[at + 1] = to_tf32(der(k + 4, qo));
+                const int blk = part ? 2 : ks / M::KR, kb = part ? ks : ks - (ks / M::KR) * M::KR;
+                const int g = l >> 2, t = (l & 3) + kb * 8;
+                float *a = db + (((size_t)(part ? 2 * M::KR : 0) + ks) * 32 + l) * 4;
+                a[0] = to_tf32(deriv_op(b, G, blk, g, t));
+                a[1] = to_tf32(deriv_op(b, G, blk, g + 8, t));
+                a[2] = to_tf32(deriv_op(b, G, blk, g, t + 4));
+                a[3] = to_tf32(deriv_op(b, G, blk, g + 8, t + 4));
             }
     for (int i = 0; i < G; ++i) {
         sm.dltx[i] = (float)b.dltx[i]; sm.dltn[i] = (float)b.dltn[i];
@@ -439,7 +432,8 @@ struct LaunchImpl {
             return (int)(((sizeof(InsMmaSmall<P>) + 15) / 16) * 16 + (size_t)2 * InsMma<P>::S_EL * InsMma<P>::WPC * 8 +
                          InsMma<P>::SMEM_IDX);
         else
-            return (int)((size_t)4 * InsTf32<P>::S_EL * InsTf32<P>::WPC * 4 + InsTf32<P>::SMEM_IDX);
+            return (int)(((sizeof(InsMmaSmallF<P>) + 15) / 16) * 16 + (size_t)4 * InsTf32<P>::S_EL * InsTf32<P>::WPC * 4 +
+                         InsTf32<P>::SMEM_IDX);
     }
     static void elem_mma(const void *ops, const void *small, const void *tab, const Mesh &m, const State<R> &s,
                          const Phys &ph, int stage, int zero_rr, int diff, int nsm, const Tune &tn, cudaStream_t st) {
@@ -822,6 +816,22 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     int *d_sbd, *d_vbi;
     if ((r = upload(c, &d_sbd, seg_bdry.data(), seg_bdry.size()))) return fail(r);
     if ((r = upload(c, &d_vbi, vb_idx.data(), vb_idx.size()))) return fail(r);
+    // owner order of the assembly buffers (Mesh::vpos, spos)
+    std::vector<int> vpos(3 * (size_t)nt, -1), spos(3 * (size_t)nt, -1);
+    for (int j = 0; j < vt_ptr[np]; ++j) vpos[3 * (size_t)(vt_idx[j] >> 2) + (vt_idx[j] & 3)] = j;
+    for (int sd = 0; sd < ns; ++sd)
+        for (int k = 0; k < 2; ++k) {
+            const int t = m->seg_tri[2 * sd + k];
+            if (t >= 0) spos[3 * (size_t)t + seg_loc[2 * sd + k]] = 2 * sd + k;
+        }
+    for (size_t q = 0; q < spos.size(); ++q)
+        if (spos[q] < 0 || vpos[q] < 0) {
+            set_err("triangle %zu side %zu is not listed in seg.tri", q / 3, q % 3);
+            return fail(HP_EINVAL);
+        }
+    int *d_vpos, *d_spos;
+    if ((r = upload(c, &d_vpos, vpos.data(), vpos.size()))) return fail(r);
+    if ((r = upload(c, &d_spos, spos.data(), spos.size()))) return fail(r);
     std::vector<double> pibc((size_t)std::max(1, m->nbseg) * b->gpx, 0.0);
     if (m->bseg_pibc) std::copy(m->bseg_pibc, m->bseg_pibc + (size_t)m->nbseg * b->gpx, pibc.begin());
     if ((r = upload(c, &d_bpibc, pibc.data(), pibc.size()))) return fail(r);
@@ -832,7 +842,7 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     M.vs_ptr = d_vsp; M.vs_idx = d_vsi; M.vt_ptr = d_vtp; M.vt_idx = d_vti;
     M.vess = d_vess; M.sess = d_sess; M.bseg = d_bseg; M.bkind = d_bkind; M.bpibc = d_bpibc;
     M.tri_cv = nullptr; M.crv_cht = nullptr; M.bcrd = nullptr; M.ncurved = 0; M.crv_tri = nullptr;
-    M.seg_bdry = d_sbd; M.vb_idx = d_vbi;
+    M.seg_bdry = d_sbd; M.vb_idx = d_vbi; M.vpos = d_vpos; M.spos = d_spos;
 
     // curved elements (tri_hp::metric::setinfo, metric.cpp:44-70, for p > 1): the
     // owner triangle of every boundary side with non-zero position modes, with its
@@ -923,7 +933,8 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     if ((r = dalloc(c, (void **)&c->st.tau, (size_t)nt * NV * 8))) return fail(r);
     // per-element vertex / side residuals and per-edge boundary fluxes of the FP64
     // assembly by gather (State::elim)
-    const size_t nel = (size_t)nt * b->bm * NV, nbr = (size_t)std::max(1, m->nbseg) * (b->sm + 2) * NV;
+    const size_t nel = (size_t)3 * nt * NV + (size_t)2 * ns * std::max(1, b->sm) * NV,
+                 nbr = (size_t)std::max(1, m->nbseg) * (b->sm + 2) * NV;
     if ((r = dalloc(c, (void **)&c->st.elim, nel * 8))) return fail(r);
     if ((r = dalloc(c, (void **)&c->st.elre, nel * 8))) return fail(r);
     if ((r = dalloc(c, (void **)&c->st.bres, nbr * 8))) return fail(r);

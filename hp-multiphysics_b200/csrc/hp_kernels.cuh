@@ -65,7 +65,21 @@ struct Mesh {
     // boundary edges seen from the entities: seg_bdry[s] = boundary edge of segment s or -1;
     // vb_idx[v][2] = 2 e + end of the (at most two) boundary edges ending at vertex v, or -1
     const int *seg_bdry, *vb_idx;
+    // owner order of the assembly buffers: vpos[3 t + c] = position of (t, corner c) in the
+    // vertex-incidence list (vt_idx), spos[3 t + i] = 2 s + k for side i of t being
+    // seg.tri(k) of segment s
+    const int *vpos, *spos;
 };
+
+// Slot of an element's vertex / side residual in the assembly buffers (State::elim,
+// elre): vertex values in vertex-incidence order [3 ntri][NV], then side values in
+// segment order [2 nseg][SM][NV], so that k_assemble reads each vertex's and each side's
+// contributions contiguously.
+__device__ __forceinline__ size_t asm_slot(const Mesh &m, int NV, int SM, int vp, int sp, int mode, int n) {
+    if (mode < 3) return (size_t)vp * NV + n;
+    const int kk = (mode - 3) % SM;
+    return (size_t)3 * m.ntri * NV + ((size_t)sp * SM + kk) * NV + n;
+}
 
 template <typename R>
 struct State {
@@ -484,11 +498,15 @@ __global__ void __launch_bounds__(ElemCfg<R, P, PHYS>::WPC * 32, ElemMinBlocks<R
         // scatter of one local coefficient of variable n, mode m (lftog, gtol.cpp:364-402)
         auto scatter = [&](R *gv, R *gs, R *el, int n, int m, R val) {
             if (el) {
+                int vp = 0, sp = 0;
                 if (m >= 3) {
                     const int i = (m - 3) / SM, k = (m - 3) - i * SM;
                     if ((k & 1) && mesh.tri_sgn[3 * tind + i] < 0) val = -val;
+                    sp = mesh.spos[3 * tind + i];
+                } else {
+                    vp = mesh.vpos[3 * tind + m];
                 }
-                el[((size_t)tind * BM + m) * NV + n] = val;
+                el[asm_slot(mesh, NV, SM, vp, sp, m, n)] = val;
             } else if (m < 3) {
                 const int v = (m == 0 ? p0 : (m == 1 ? p1 : p2));
                 atomic_add(&gv[v * NV + n], val);
@@ -751,12 +769,17 @@ __global__ void __launch_bounds__(EmatShape<R, P, RE>::THREADS, 2048 / EmatShape
         const R vre = RE ? r_s[SLOTS + w] : (R)0;
         if (st.elim && ms < BM) {  // assembly by gather (NV = 1)
             bool flip = false;
+            int vp = 0, sp = 0;
             if (ms >= 3) {
                 const int i = (ms - 3) / SM, kk = (ms - 3) - i * SM;
                 flip = (kk & 1) && mesh.tri_sgn[3 * t + i] < 0;
+                sp = mesh.spos[3 * t + i];
+            } else {
+                vp = mesh.vpos[3 * t + ms];
             }
-            st.elim[(size_t)t * BM + ms] = flip ? -vim : vim;
-            if (RE) st.elre[(size_t)t * BM + ms] = flip ? -vre : vre;
+            const size_t slot = asm_slot(mesh, 1, SM, vp, sp, ms, 0);
+            st.elim[slot] = flip ? -vim : vim;
+            if (RE) st.elre[slot] = flip ? -vre : vre;
         } else if (ms < 3) {
             const int v = mesh.tri_pnt[3 * t + ms];
             atomic_add(&st.resv[v], vim);
@@ -917,18 +940,16 @@ __global__ void k_bdry_flux_ins(const DevTables<R, P> *__restrict__ tb, Mesh mes
 // not depend on the scheduling. One thread per vertex, then one per (side, mode).
 template <typename R>
 __global__ void k_assemble(Mesh mesh, State<R> st, int NV, int SM, R omb, int zero_rr, int with_re, int with_b) {
-    const int BM = 3 + 3 * SM;
+    const size_t soff = (size_t)3 * mesh.ntri * NV;  // side section of the buffers
     const long nitems = (long)mesh.npnt + (long)mesh.nseg * SM;
     for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < nitems; k += (long)gridDim.x * blockDim.x) {
         if (k < mesh.npnt) {
             const int v = (int)k, j0 = mesh.vt_ptr[v], j1 = mesh.vt_ptr[v + 1];
             for (int n = 0; n < NV; ++n) {
                 R sim = (R)0, sre = (R)0;
-                for (int j = j0; j < j1; ++j) {
-                    const int code = mesh.vt_idx[j];
-                    const size_t idx = ((size_t)(code >> 2) * BM + (code & 3)) * NV + n;
-                    sim += st.elim[idx];
-                    if (with_re) sre += st.elre[idx];
+                for (int j = j0; j < j1; ++j) {  // contiguous: the buffers are in incidence order
+                    sim += st.elim[(size_t)j * NV + n];
+                    if (with_re) sre += st.elre[(size_t)j * NV + n];
                 }
                 if (with_b)
                     for (int q = 0; q < 2; ++q) {
@@ -948,9 +969,8 @@ __global__ void k_assemble(Mesh mesh, State<R> st, int NV, int SM, R omb, int ze
             for (int n = 0; n < NV; ++n) {
                 R sim = (R)0, sre = (R)0;
                 for (int side = 0; side < 2; ++side) {
-                    const int t = mesh.seg_tri[2 * sd + side];
-                    if (t < 0) continue;
-                    const size_t idx = ((size_t)t * BM + 3 + mesh.seg_loc[2 * sd + side] * SM + kk) * NV + n;
+                    if (mesh.seg_tri[2 * sd + side] < 0) continue;
+                    const size_t idx = soff + ((size_t)(2 * sd + side) * SM + kk) * NV + n;
                     sim += st.elim[idx];
                     if (with_re) sre += st.elre[idx];
                 }
