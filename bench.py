@@ -432,15 +432,28 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=N
         # p1_minvrt: the p = 1 and 2 levels smoothed by the default build's tet_hp::minvrt at
         # the reference's cfl (2.2, 1.5) instead of the JACOBI build's relaxation
         cflw = {**cfl, **({1: 2.2, 2: 1.5} if p1_minvrt else {})}
-        H = TetHierarchy(n, p, hlevels=hl, mu=1.0 / 100.0, cfl=cflw, stream=ctypes.c_void_p(cur.cuda_stream),
-                         minvrt=p1_minvrt)
-        h, sec, nc = H.solve(drop=1e-10, max_cycles=400, vw=2)
+        arms = {}
+        states = {}
+        for arm, mixed in (("fp64", False), ("fp32_defect_correction", True)):
+            H = TetHierarchy(n, p, hlevels=hl, mu=1.0 / 100.0, cfl=cflw, stream=ctypes.c_void_p(cur.cuda_stream),
+                             minvrt=p1_minvrt)
+            h, sec, nc = H.solve(drop=1e-10, max_cycles=400, vw=2, mixed=mixed)
+            states[arm] = H.levels[0].state()
+            arms[arm] = {"seconds": sec, "cycles": nc, "drop": float(h[-1]), "reached": bool(h[-1] <= 1e-10),
+                         "ms_per_cycle": 1e3 * sec / max(nc, 1),
+                         "drop_history": [float(x) for x in h[::max(1, len(h) // 10)]]}
+            if arm != "fp64":
+                a, b = states["fp64"], [x.copy() for x in states[arm]]
+                b[0][:, 3] += np.mean(a[0][:, 3]) - np.mean(b[0][:, 3])  # free pressure level
+                arms[arm]["rel_l2_state_diff_vs_fp64_modulo_pressure_level"] = float(
+                    np.sqrt(sum(np.sum((x - y) ** 2) for x, y in zip(a, b))) / np.sqrt(sum(np.sum(x * x) for x in a)))
+            H.close()
+            print(json.dumps({"c5_arm": arm, **arms[arm]}), flush=True)
+        arms["speedup_fp32_vs_fp64"] = arms["fp64"]["seconds"] / arms["fp32_defect_correction"]["seconds"]
         line["multigrid_full_w_to_1e-10"] = {"levels": f"p {p}..1, then h-levels down to {n >> hl}^3 at p = 1",
                                              "low_p_smoother": "minvrt (p = 1, 2; cfl 2.2, 1.5)" if p1_minvrt
-                                             else "jacobi, cfl 0.5",
-                                             "seconds": sec, "cycles": nc, "drop": float(h[-1]),
-                                             "reached": bool(h[-1] <= 1e-10), "ms_per_cycle": 1e3 * sec / max(nc, 1),
-                                             "drop_history": [float(x) for x in h[::max(1, len(h) // 10)]]}
+                                             else "jacobi, cfl 0.5", **arms}
+        H = TetHierarchy(n, p, hlevels=1, mu=1.0 / 100.0, cfl=cfl, stream=ctypes.c_void_p(cur.cuda_stream))
     H.close()
     # CPU oracle on a bounded sample
     ps = TetProblem(cube_tets(6), p, mu=1.0 / 100.0).set_beltrami(re=100.0)

@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -622,10 +623,11 @@ __global__ void k_tet_prcn(TetMeshD mesh, const double *ugv, double *tau, double
 // tet_hp::minvrt at p = 1 (its em = 0 branch, tet_hp/setup_preconditioner.cpp:57-74, vprcn
 // pre-inverted as in tet_hp::setup_preconditioner) with the nstage update of tet_hp::update
 // (tet_hp/update.cpp:181-390): res.v *= (1 / vprcn) vdiag, fixed rows zeroed, ug = ug0 - ca res.
-__global__ void k_tet_minvrt1(long n, double *res, const double *vprcn, double vdiag, const unsigned char *mask,
-                              double *u, const double *u0, double ca) {
+template <typename R>
+__global__ void k_tet_minvrt1(long n, R *res, const R *vprcn, R vdiag, const unsigned char *mask, R *u, const R *u0,
+                              R ca) {
     for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
-        const double r = mask[k] ? 0.0 : res[k] * ((1.0 / vprcn[k]) * vdiag);
+        const R r = mask[k] ? (R)0 : res[k] * (((R)1 / vprcn[k]) * vdiag);
         res[k] = r;
         u[k] = u0[k] - ca * r;
     }
@@ -634,8 +636,9 @@ __global__ void k_tet_minvrt1(long n, double *res, const double *vprcn, double v
 // tet_hp::minvrt at p = 2 (tet_hp/setup_preconditioner.cpp:16-30, 57-131, 197-221), in four
 // passes. (1) Edge modes removed from their end vertices: res.v -= sfmv(end, k) res.e.
 // The rows fixed by essential conditions were zeroed before minvrt (mask_e: the edge section).
-__global__ void k_tet_minv_e2v(int nseg, int em, const int *seg_pnt, const double *sfmv, double *resv,
-                               const double *rese, const unsigned char *mask_e) {
+template <typename R>
+__global__ void k_tet_minv_e2v(int nseg, int em, const int *seg_pnt, const R *sfmv, R *resv, const R *rese,
+                               const unsigned char *mask_e) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
         for (int k = 0; k < em; ++k)
             for (int i = 0; i < 2; ++i) {
@@ -648,28 +651,28 @@ __global__ void k_tet_minv_e2v(int nseg, int em, const int *seg_pnt, const doubl
 }
 
 // (2) / (4) res *= (1 / prcn(entity, var)) diag on one section, fixed rows zeroed
-__global__ void k_tet_minv_scale(long n, int modes, double *res, const double *prcn, double diag,
-                                 const unsigned char *mask) {
+template <typename R>
+__global__ void k_tet_minv_scale(long n, int modes, R *res, const R *prcn, R diag, const unsigned char *mask) {
     for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
         const long ent = k / ((long)modes * NV), var = k % NV;
-        res[k] = mask[k] ? 0.0 : res[k] * ((1.0 / prcn[ent * NV + var]) * diag);
+        res[k] = mask[k] ? (R)0 : res[k] * (((R)1 / prcn[ent * NV + var]) * diag);
     }
 }
 
 // (3) Vertex values (times the element diagonal iprcn) removed from the edge modes:
 // res.e(edge, k) -= sgn^k mm(j, 4 + k + i em) res.v(v_j) iprcn(tet)
-__global__ void k_tet_minv_v2e(TetMeshD m, int em, const double *mm, const double *iprcn, const double *resv,
-                               double *rese) {
+template <typename R>
+__global__ void k_tet_minv_v2e(TetMeshD m, int em, const R *mm, const R *iprcn, const R *resv, R *rese) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m.ntet; t += gridDim.x * blockDim.x) {
-        double uh[4][NV];
+        R uh[4][NV];
         for (int j = 0; j < 4; ++j)
             for (int n = 0; n < NV; ++n) uh[j][n] = resv[(size_t)m.tp[4 * t + j] * NV + n] * iprcn[(size_t)t * NV + n];
         for (int i = 0; i < 6; ++i) {
             const int sind = m.ts[6 * t + i], sg = m.tsg[6 * t + i];
             for (int j = 0; j < 4; ++j) {
-                double msgn = 1.0;
+                R msgn = 1;
                 for (int k = 0; k < em; ++k) {
-                    const double c = mm[j * HP_TET_MAXT + 4 + k + i * em];
+                    const R c = mm[j * HP_TET_MAXT + 4 + k + i * em];
                     for (int n = 0; n < NV; ++n) atomicAdd(rese + ((size_t)sind * em + k) * NV + n, -msgn * c * uh[j][n]);
                     msgn *= sg;
                 }
@@ -679,26 +682,28 @@ __global__ void k_tet_minv_v2e(TetMeshD m, int em, const double *mm, const doubl
 }
 
 // ug = ug0 - ca res
-__global__ void k_tet_advance(long n, const double *res, double *u, const double *u0, double ca) {
+template <typename R>
+__global__ void k_tet_advance(long n, const R *res, R *u, const R *u0, R ca) {
     for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
         u[k] = u0[k] - ca * res[k];
 }
 
-__global__ void k_tet_relax(long n, double *res, const double *jd, const unsigned char *mask, double *u,
-                            const double *u0, double ca) {
+template <typename R>
+__global__ void k_tet_relax(long n, R *res, const R *jd, const unsigned char *mask, R *u, const R *u0, R ca) {
     for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
-        const double r = mask[k] ? 0.0 : 0.5 * res[k] / jd[k];
+        const R r = mask[k] ? (R)0 : (R)0.5 * res[k] / jd[k];
         res[k] = r;
         u[k] = u0[k] - ca * r;
     }
 }
 
 // per-block sums of squares of the unmasked residual entries (fixed grid: deterministic)
-__global__ void k_tet_sq(long n, const double *res, const unsigned char *mask, double *part) {
+template <typename R>
+__global__ void k_tet_sq(long n, const R *res, const unsigned char *mask, double *part) {
     __shared__ double sh[256];
     double s = 0.0;
     for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
-        if (!mask[k]) s += res[k] * res[k];
+        if (!mask[k]) s += (double)res[k] * (double)res[k];
     sh[threadIdx.x] = s;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
@@ -710,57 +715,64 @@ __global__ void k_tet_sq(long n, const double *res, const unsigned char *mask, d
 
 // ---- multigrid transfers (tet_hp/mg_restrict.cpp, mg_prolongate.cpp) ----
 // p-levels share the mesh: coarse entry c is fine entry map[c] (mode truncation)
-__global__ void k_tet_p_restrict(long n, const int *map, const double *fu, const double *fres, double *u,
-                                 double *uf, double *res0) {
+template <typename R>
+__global__ void k_tet_p_restrict(long n, const int *map, const R *fu, const R *fres, R *u, R *uf, R *res0) {
     for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-        const double v = fu[map[c]];
+        const R v = fu[map[c]];
         u[c] = v;
         uf[c] = v;
         res0[c] = fres[map[c]];
     }
 }
-__global__ void k_tet_p_prolong(long n, const int *map, const double *u, const double *uf, double *fu) {
+template <typename R>
+__global__ void k_tet_p_prolong(long n, const int *map, const R *u, const R *uf, R *fu) {
     for (long c = (long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x)
         fu[map[c]] += u[c] - uf[c];
 }
 // h-levels at p = 1: vertex values, each point in a tetrahedron of the other mesh
-__global__ void k_tet_h_restrict_state(int ncp, const int *tet, const double *w, const int *ftp, const double *fu,
-                                       double *u, double *uf) {
+template <typename R>
+__global__ void k_tet_h_restrict_state(int ncp, const int *tet, const double *w, const int *ftp, const R *fu, R *u,
+                                       R *uf) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < ncp; v += gridDim.x * blockDim.x)
         for (int n = 0; n < NV; ++n) {
             double s = 0.0;
-            for (int j = 0; j < 4; ++j) s += w[4 * v + j] * fu[(size_t)ftp[4 * tet[v] + j] * NV + n];
-            u[(size_t)v * NV + n] = s;
-            uf[(size_t)v * NV + n] = s;
+            for (int j = 0; j < 4; ++j) s += w[4 * v + j] * (double)fu[(size_t)ftp[4 * tet[v] + j] * NV + n];
+            u[(size_t)v * NV + n] = (R)s;
+            uf[(size_t)v * NV + n] = (R)s;
         }
 }
-__global__ void k_tet_h_restrict_res(int nfp, const int *tet, const double *w, const int *ctp, const double *fres,
-                                     double *res0) {
+template <typename R>
+__global__ void k_tet_h_restrict_res(int nfp, const int *tet, const double *w, const int *ctp, const R *fres,
+                                     R *res0) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nfp; v += gridDim.x * blockDim.x)
         for (int j = 0; j < 4; ++j)
             for (int n = 0; n < NV; ++n)
-                atomicAdd(res0 + (size_t)ctp[4 * tet[v] + j] * NV + n, w[4 * v + j] * fres[(size_t)v * NV + n]);
+                atomicAdd(res0 + (size_t)ctp[4 * tet[v] + j] * NV + n, (R)(w[4 * v + j] * fres[(size_t)v * NV + n]));
 }
-__global__ void k_tet_h_prolong(int nfp, const int *tet, const double *w, const int *ctp, const double *u,
-                                const double *uf, double *fu) {
+template <typename R>
+__global__ void k_tet_h_prolong(int nfp, const int *tet, const double *w, const int *ctp, const R *u, const R *uf,
+                                R *fu) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nfp; v += gridDim.x * blockDim.x)
         for (int n = 0; n < NV; ++n) {
             double s = 0.0;
             for (int j = 0; j < 4; ++j) {
                 const size_t c = (size_t)ctp[4 * tet[v] + j] * NV + n;
-                s += w[4 * v + j] * (u[c] - uf[c]);
+                s += w[4 * v + j] * (double)(u[c] - uf[c]);
             }
-            fu[(size_t)v * NV + n] += s;
+            fu[(size_t)v * NV + n] += (R)s;
         }
 }
 // FAS driving term (tet_hp::rsdl, update.cpp:97-117): on the first residual after a
 // restriction dres = fadd res0 - res; every coarse residual then adds dres
-__global__ void k_tet_fas(long n, double *res, const double *res0, double *dres, double fadd, int first) {
+template <typename R>
+__global__ void k_tet_fas(long n, R *res, const R *res0, R *dres, R fadd, int first) {
     for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
         if (first) dres[k] = fadd * res0[k] - res[k];
         res[k] += dres[k];
     }
 }
+
+#include "hp_tet_mixed.cuh"
 
 int nblk(long n, int b) { return (int)std::max<long>(1, (n + b - 1) / b); }
 
@@ -803,6 +815,23 @@ struct hp_tet_ctx {
     double *face_pbc = nullptr;
     TetFields<double> fields(double *base) const {
         return TetFields<double>{base, base + lv, base + lv + le, base + lv + le + lf};
+    }
+    // FP32 smoother of the mixed-precision solve (hp_tet_solve_mg_mixed): the correction d
+    // (U), its stage copy, residuals, the base state and its point values, the FP32 copies
+    // of the preconditioner (tau, Jacobian diagonal, minvrt's), the source DRES (the FP64
+    // defect on the finest level, the FAS term below), the restricted residual and the
+    // entry correction of a coarse level, and the TF32 operators
+    struct Mixed {
+        float *U = nullptr, *U0 = nullptr, *RES = nullptr, *RR = nullptr, *UB = nullptr, *DRES = nullptr;
+        float *JD = nullptr, *BPT = nullptr, *TAU = nullptr, *RES0 = nullptr, *UF = nullptr;
+        float *vprcn = nullptr, *eprcn = nullptr, *iprcn = nullptr, *mm = nullptr, *sfmv = nullptr;
+        float2 *projB = nullptr, *intB = nullptr;
+        float *F = nullptr;
+        bool fas_pending = false;
+    } mx;
+    bool mixed_ready = false;
+    TetFields<float> fields32(float *base) const {
+        return TetFields<float>{base, base + lv, base + lv + le, base + lv + le + lf};
     }
 };
 
@@ -1563,6 +1592,363 @@ extern "C" int hp_tet_solve_mg(hp_tet_ctx **levels, int nlevels, double drop, in
     hist[nh++] = 1.0;
     while (nc < max_cycles) {
         if ((r = tet_cycle(levels, nlevels, 0, vw, itercrsn, iterrfne))) return r;
+        ++nc;
+        double rn;
+        if ((r = hp_tet_resnorm(f, &rn))) return r;
+        const double d = r0 > 0 ? rn / r0 : 0.0;
+        if (nh < cap) hist[nh++] = d;
+        if (!(d == d) || d <= drop) break;
+    }
+    TCK(cudaEventRecord(e1, f->stream));
+    TCK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    TCK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (nhist) *nhist = nh;
+    if (seconds) *seconds = ms * 1e-3;
+    if (cycles) *cycles = nc;
+    return HP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Multigrid inside FP64 defect correction with FP32 smoothing (the FP32 arm of the 3D
+// workload). Every cycle: the FP64 residual R64(u) of the finest level; the base states
+// (u and its FP64 restriction down the levels) in FP32 with their point values; one FP32
+// cycle of block::cycle (tri_mesh/blocks.cpp:1267-1348) on the correction equation of
+// every level (residual in correction form plus the level's source: R64 on the finest,
+// the FAS term below it), smoothed as the FP64 levels are (tet_hp's JACOBI relaxation,
+// or minvrt at p <= 2); then u += d in FP64. The preconditioners (tau, the Jacobian
+// diagonal, minvrt's) are set up once at the initial state, as in hp_tet_solve_mg, and
+// copied to FP32. Inflow flux faces only (their continuity flux is linear in the state).
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int P>
+void tet_fragments_tf32(const hp_tet_tables &b, std::vector<float> &proj, std::vector<float> &intg,
+                        std::vector<float> &F) {
+    using C = TetCfg<P>;
+    using M = TetTf32<P>;
+    auto tf = [](double v) {
+        float f = (float)v;
+        uint32_t u;
+        std::memcpy(&u, &f, 4);
+        u = (u + 0x1000u) & 0xFFFFE000u;  // round to TF32 (nearest, ties away), as cvt.rna
+        std::memcpy(&f, &u, 4);
+        return f;
+    };
+    proj.assign(M::PROJ_LEN, 0.f);
+    intg.assign(M::INT_LEN, 0.f);
+    const double(*ops[4])[HP_TET_MAXT] = {b.F, b.DX, b.DY, b.DZ};
+    auto op = [&](int o, int q, int m) { return (q < C::Q && m < C::T) ? ops[o][q][m] : 0.0; };
+    auto wd = [&](int k, int m) {
+        if (k >= 3 * C::Q || m >= C::T) return 0.0;
+        const int c = k / C::Q, q = k - c * C::Q;
+        return b.w[q] * ops[1 + c][q][m];
+    };
+    // m16n8k8 B fragments: lane l holds B[k = l & 3][n = l >> 2] and B[k + 4][n]
+    for (int o = 0; o < 4; ++o)
+        for (int nt = 0; nt < M::NT; ++nt)
+            for (int ks = 0; ks < M::KS; ++ks)
+                for (int l = 0; l < 32; ++l) {
+                    const size_t at = ((((size_t)o * M::NT + nt) * M::KS + ks) * 32 + l) * 2;
+                    const int q = nt * 8 + (l >> 2), m = ks * 8 + (l & 3);
+                    proj[at] = tf(op(o, q, m));
+                    proj[at + 1] = tf(op(o, q, m + 4));
+                }
+    for (int nt = 0; nt < M::NT2; ++nt)
+        for (int ks = 0; ks < M::KS2; ++ks)
+            for (int l = 0; l < 32; ++l) {
+                const size_t at = (((size_t)nt * M::KS2 + ks) * 32 + l) * 2;
+                const int k = ks * 8 + (l & 3), m = nt * 8 + (l >> 2);
+                intg[at] = tf(wd(k, m));
+                intg[at + 1] = tf(wd(k + 4, m));
+            }
+    F.assign((size_t)C::Q * C::T, 0.f);
+    for (int q = 0; q < C::Q; ++q)
+        for (int m = 0; m < C::T; ++m) F[(size_t)q * C::T + m] = (float)b.F[q][m];
+}
+
+template <int P>
+TetSmall<float, P> small32(const hp_tet_tables &t) {
+    TetSmall<float, P> sm;
+    for (int i = 0; i <= P; ++i) {
+        for (int j = 0; j <= P; ++j) {
+            sm.Ax[i][j] = (float)t.Ax[i][j];
+            sm.Bx[i][j] = (float)t.Bx[i][j];
+            sm.Ay[i][j] = (float)t.Ay[i][j];
+            sm.By[i][j] = (float)t.By[i][j];
+            sm.Az[i][j] = (float)t.Az[i][j];
+        }
+        sm.y0[i] = (float)t.y0[i];
+        sm.z0[i] = (float)t.z0[i];
+    }
+    return sm;
+}
+
+int mixed_alloc(hp_tet_ctx *c) {
+    if (c->mixed_ready) return HP_OK;
+    hp_tet_ctx::Mixed &x = c->mx;
+    int r;
+    for (float **f : {&x.U, &x.U0, &x.RES, &x.RR, &x.UB, &x.DRES, &x.JD, &x.RES0, &x.UF}) {
+        if ((r = talloc(c, (void **)f, 4 * std::max<size_t>(c->ltot, 1)))) return r;
+        TCK(cudaMemset(*f, 0, 4 * std::max<size_t>(c->ltot, 1)));
+    }
+    if ((r = talloc(c, (void **)&x.BPT, 4 * (size_t)c->mesh.ntet * 3 * c->Q)) ||
+        (r = talloc(c, (void **)&x.TAU, 8 * (size_t)c->mesh.ntet)) ||
+        (r = talloc(c, (void **)&x.iprcn, 16 * (size_t)c->mesh.ntet)) ||
+        (r = talloc(c, (void **)&x.vprcn, 16 * (size_t)c->mesh.npnt)) ||
+        (r = talloc(c, (void **)&x.eprcn, 16 * (size_t)std::max(1, c->mesh.nseg))))
+        return r;
+    {
+        std::vector<float> mm(sizeof(c->tab.mm) / 8), sf(sizeof(c->tab.sfmv) / 8);
+        const double *pm = &c->tab.mm[0][0], *ps = &c->tab.sfmv[0][0];
+        for (size_t k = 0; k < mm.size(); ++k) mm[k] = (float)pm[k];
+        for (size_t k = 0; k < sf.size(); ++k) sf[k] = (float)ps[k];
+        if ((r = talloc(c, (void **)&x.mm, 4 * mm.size())) || (r = talloc(c, (void **)&x.sfmv, 4 * sf.size()))) return r;
+        TCK(cudaMemcpy(x.mm, mm.data(), 4 * mm.size(), cudaMemcpyHostToDevice));
+        TCK(cudaMemcpy(x.sfmv, sf.data(), 4 * sf.size(), cudaMemcpyHostToDevice));
+    }
+    std::vector<float> pb, ib, F;
+    switch (c->p) {
+        case 1: tet_fragments_tf32<1>(c->tab, pb, ib, F); break;
+        case 2: tet_fragments_tf32<2>(c->tab, pb, ib, F); break;
+        case 3: tet_fragments_tf32<3>(c->tab, pb, ib, F); break;
+        case 4: tet_fragments_tf32<4>(c->tab, pb, ib, F); break;
+        default: return HP_EINVAL;
+    }
+    if ((r = talloc(c, (void **)&x.projB, 4 * pb.size())) || (r = talloc(c, (void **)&x.intB, 4 * ib.size())) ||
+        (r = talloc(c, (void **)&x.F, 4 * F.size())))
+        return r;
+    TCK(cudaMemcpy(x.projB, pb.data(), 4 * pb.size(), cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(x.intB, ib.data(), 4 * ib.size(), cudaMemcpyHostToDevice));
+    TCK(cudaMemcpy(x.F, F.data(), 4 * F.size(), cudaMemcpyHostToDevice));
+    c->mixed_ready = true;
+    return HP_OK;
+}
+
+template <typename A, typename B>
+void conv(hp_tet_ctx *c, long n, const A *src, B *dst) {
+    if (n > 0) k_tet_convert<A, B><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>(n, src, dst);
+}
+
+// FP32 copies of the preconditioner set up in FP64 at the base state
+void mixed_prcn(hp_tet_ctx *c) {
+    hp_tet_ctx::Mixed &x = c->mx;
+    conv(c, 2L * c->mesh.ntet, c->tau, x.TAU);
+    conv(c, (long)c->ltot, c->JD, x.JD);
+    conv(c, (long)c->mesh.ntet * NV, c->iprcn, x.iprcn);
+    conv(c, (long)c->mesh.npnt * NV, c->vprcn, x.vprcn);
+    conv(c, (long)c->mesh.nseg * NV, c->eprcn, x.eprcn);
+}
+
+template <int P>
+int base_points(hp_tet_ctx *c) {
+    k_tet_base_points<P><<<nblk(3L * c->mesh.ntet, 128), 128, 0, c->stream>>>(c->mx.F, c->mesh, c->fields32(c->mx.UB),
+                                                                            c->mx.BPT);
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+int base_points_any(hp_tet_ctx *c) {
+    switch (c->p) {
+        case 1: return base_points<1>(c);
+        case 2: return base_points<2>(c);
+        case 3: return base_points<3>(c);
+        case 4: return base_points<4>(c);
+    }
+    return HP_EINVAL;
+}
+
+template <int P>
+int launch_rsdl32(hp_tet_ctx *c, int stage) {
+    using M = TetTf32<P>;
+    static bool attr = false;
+    if (!attr) {
+        TCK(cudaFuncSetAttribute(k_tet_rsdl_tf32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::SMEM));
+        attr = true;
+    }
+    hp_tet_ctx::Mixed &x = c->mx;
+    const float omb = stage >= c->ph.nstage ? 0.f : (float)(1.0 - c->ph.beta[stage]);
+    const float beta = (float)c->ph.beta[stage];
+    const int g = std::min(nblk((long)c->ltot, 256), c->nsm * 8);
+    k_tet_pre<float><<<g, 256, 0, c->stream>>>((long)c->ltot, x.RES, x.RR, omb);
+    if (c->faces.n > 0)
+        k_tet_face_flux32<P><<<std::min(nblk(c->faces.n, 4), c->nsm * 16), 128, 0, c->stream>>>(
+            c->faces, c->ftab, c->mesh, c->fields32(x.U), c->fields32(x.RES), (float)c->ph.rho);
+    const long nquad = ((long)c->mesh.ntet + 3) / 4;
+    k_tet_rsdl_tf32<P><<<std::min(nblk(nquad, M::WPC), c->nsm * 32), M::WPC * 32, M::SMEM, c->stream>>>(
+        x.projB, x.intB, small32<P>(c->tab), c->mesh, c->fields32(x.U), c->fields32(x.RES), c->fields32(x.RR), x.TAU,
+        x.BPT, (float)c->ph.rho, (float)c->ph.mu, beta);
+    k_tet_fold<float><<<g, 256, 0, c->stream>>>((long)c->ltot, x.RES, x.RR);
+    // the source: the FP64 defect on the finest level; the FAS term, formed at the first
+    // residual after a restriction, below it
+    k_tet_fas<float><<<g, 256, 0, c->stream>>>((long)c->ltot, x.RES, x.RES0, x.DRES, (float)c->fadd,
+                                               (c->fine && x.fas_pending) ? 1 : 0);
+    x.fas_pending = false;
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+int rsdl32(hp_tet_ctx *c, int stage) {
+    switch (c->p) {
+        case 1: return launch_rsdl32<1>(c, stage);
+        case 2: return launch_rsdl32<2>(c, stage);
+        case 3: return launch_rsdl32<3>(c, stage);
+        case 4: return launch_rsdl32<4>(c, stage);
+    }
+    return HP_EINVAL;
+}
+
+// tet_hp::update in FP32 on the correction: the stages of hp_tet_enqueue_update
+int update32(hp_tet_ctx *c) {
+    hp_tet_ctx::Mixed &x = c->mx;
+    TCK(cudaMemcpyAsync(x.U0, x.U, 4 * c->ltot, cudaMemcpyDeviceToDevice, c->stream));
+    const int g = std::min(nblk((long)c->ltot, 256), c->nsm * 8);
+    for (int stage = 0; stage < c->ph.nstage; ++stage) {
+        int r = rsdl32(c, stage);
+        if (r) return r;
+        const float ca = (float)(c->ph.alpha[stage] * c->ph.cfl);
+        if (c->smoother && c->p == 1) {
+            k_tet_minvrt1<float><<<g, 256, 0, c->stream>>>((long)c->ltot, x.RES, x.vprcn, (float)c->tab.vdiag, c->mask,
+                                                           x.U, x.U0, ca);
+        } else if (c->smoother) {
+            float *rv = x.RES, *re = x.RES + c->lv;
+            k_tet_minv_e2v<float><<<std::min(nblk(c->mesh.nseg, 256), c->nsm * 8), 256, 0, c->stream>>>(
+                c->mesh.nseg, c->em, c->seg_pnt, x.sfmv, rv, re, c->mask + c->lv);
+            k_tet_minv_scale<float><<<std::min(nblk((long)c->lv, 256), c->nsm * 8), 256, 0, c->stream>>>(
+                (long)c->lv, 1, rv, x.vprcn, (float)c->tab.vdiag, c->mask);
+            k_tet_minv_v2e<float><<<std::min(nblk(c->mesh.ntet, 128), c->nsm * 8), 128, 0, c->stream>>>(
+                c->mesh, c->em, x.mm, x.iprcn, rv, re);
+            k_tet_minv_scale<float><<<std::min(nblk((long)c->le, 256), c->nsm * 8), 256, 0, c->stream>>>(
+                (long)c->le, c->em, re, x.eprcn, 100.f, c->mask + c->lv);
+            k_tet_advance<float><<<g, 256, 0, c->stream>>>((long)c->ltot, x.RES, x.U, x.U0, ca);
+        } else {
+            k_tet_relax<float><<<g, 256, 0, c->stream>>>((long)c->ltot, x.RES, x.JD, c->mask, x.U, x.U0, ca);
+        }
+    }
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+int restrict32(hp_tet_ctx *c) {
+    hp_tet_ctx *f = c->fine;
+    hp_tet_ctx::Mixed &x = c->mx;
+    if (c->kind == 1) {
+        k_tet_p_restrict<float><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+            (long)c->ltot, c->pmap, f->mx.U, f->mx.RES, x.U, x.UF, x.RES0);
+    } else {
+        k_tet_h_restrict_state<float><<<nblk(c->mesh.npnt, 128), 128, 0, c->stream>>>(
+            c->mesh.npnt, c->c2f_tet, c->c2f_w, f->mesh.tp, f->mx.U, x.U, x.UF);
+        TCK(cudaMemsetAsync(x.RES0, 0, 4 * c->ltot, c->stream));
+        k_tet_h_restrict_res<float><<<nblk(f->mesh.npnt, 128), 128, 0, c->stream>>>(
+            f->mesh.npnt, c->f2c_tet, c->f2c_w, c->mesh.tp, f->mx.RES, x.RES0);
+    }
+    TCK(cudaGetLastError());
+    x.fas_pending = true;
+    return HP_OK;
+}
+
+int prolong32(hp_tet_ctx *c) {
+    hp_tet_ctx *f = c->fine;
+    if (c->kind == 1)
+        k_tet_p_prolong<float><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+            (long)c->ltot, c->pmap, c->mx.U, c->mx.UF, f->mx.U);
+    else
+        k_tet_h_prolong<float><<<nblk(f->mesh.npnt, 128), 128, 0, c->stream>>>(f->mesh.npnt, c->f2c_tet, c->f2c_w,
+                                                                              c->mesh.tp, c->mx.U, c->mx.UF, f->mx.U);
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+int cycle32(hp_tet_ctx **lv, int n, int lvl, int vw, int itercrsn, int iterrfne) {
+    hp_tet_ctx *c = lv[lvl];
+    int r;
+    for (int vc = 0; vc < vw; ++vc) {
+        for (int it = 0; it < itercrsn; ++it)
+            if ((r = update32(c))) return r;
+        if (lvl == n - 1) return HP_OK;
+        if ((r = rsdl32(c, c->ph.nstage))) return r;
+        if ((r = restrict32(lv[lvl + 1]))) return r;
+        if ((r = cycle32(lv, n, lvl + 1, vw, itercrsn, iterrfne))) return r;
+        if ((r = prolong32(lv[lvl + 1]))) return r;
+        for (int it = 0; it < iterrfne; ++it)
+            if ((r = update32(c))) return r;
+    }
+    return HP_OK;
+}
+
+// Base states of every level for one correction cycle: the FP64 state restricted down
+// the levels (FP64 transfers), in FP32 with its point values; the corrections start at 0
+int mixed_bases(hp_tet_ctx **lv, int n) {
+    for (int l = 1; l < n; ++l) {
+        hp_tet_ctx *c = lv[l], *f = lv[l - 1];
+        if (c->kind == 1)
+            k_tet_p_restrict<double><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+                (long)c->ltot, c->pmap, f->U, f->RES, c->U, c->UF, c->RES0);
+        else
+            k_tet_h_restrict_state<double><<<nblk(c->mesh.npnt, 128), 128, 0, c->stream>>>(
+                c->mesh.npnt, c->c2f_tet, c->c2f_w, f->mesh.tp, f->U, c->U, c->UF);
+    }
+    for (int l = 0; l < n; ++l) {
+        hp_tet_ctx *c = lv[l];
+        conv(c, (long)c->ltot, c->U, c->mx.UB);
+        int r = base_points_any(c);
+        if (r) return r;
+        TCK(cudaMemsetAsync(c->mx.U, 0, 4 * c->ltot, c->stream));
+    }
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+}  // namespace
+
+extern "C" int hp_tet_solve_mg_mixed(hp_tet_ctx **levels, int nlevels, double drop, int max_cycles, int vw,
+                                     int itercrsn, int iterrfne, double *hist, int cap, int *nhist, double *seconds,
+                                     int *cycles) {
+    if (!levels || nlevels < 1 || drop <= 0 || max_cycles < 1 || vw < 1 || !hist || cap < 1) return HP_EINVAL;
+    for (int l = 1; l < nlevels; ++l)
+        if (!levels[l]->fine || levels[l]->fine != levels[l - 1] || levels[l]->stream != levels[0]->stream) {
+            set_err("hp_tet_solve_mg_mixed: levels must be attached in order and share one stream");
+            return HP_EINVAL;
+        }
+    int r;
+    for (int l = 0; l < nlevels; ++l) {
+        hp_tet_ctx *c = levels[l];
+        std::vector<int> kind(c->faces.n);
+        if (c->faces.n)
+            TCK(cudaMemcpy(kind.data(), c->faces.kind, 4 * (size_t)c->faces.n, cudaMemcpyDeviceToHost));
+        for (int k : kind)
+            if (k != 0) {
+                set_err("hp_tet_solve_mg_mixed: flux faces other than inflow are not built in FP32");
+                return HP_ENOTSUP;
+            }
+        if ((r = mixed_alloc(c))) return r;
+    }
+    hp_tet_ctx *f = levels[0];
+    cudaEvent_t e0, e1;
+    TCK(cudaEventCreate(&e0));
+    TCK(cudaEventCreate(&e1));
+    TCK(cudaEventRecord(e0, f->stream));
+    // preconditioners at the initial state of every level (as hp_tet_solve_mg's first visits)
+    if ((r = mixed_bases(levels, nlevels))) return r;
+    for (int l = 0; l < nlevels; ++l) {
+        hp_tet_ctx *c = levels[l];
+        r = hp_tet_setup_preconditioner(c);
+        if (r) return r < 0 ? r : HP_ESTATE;
+        if (!c->smoother && (r = hp_tet_jacobian_diagonal(c))) return r;
+        mixed_prcn(c);
+    }
+    double r0;
+    if ((r = hp_tet_resnorm(f, &r0))) return r;  // leaves R64(u) in f->RES
+    int nh = 0, nc = 0;
+    hist[nh++] = 1.0;
+    while (nc < max_cycles) {
+        if ((r = mixed_bases(levels, nlevels))) return r;
+        conv(f, (long)f->ltot, f->RES, f->mx.DRES);
+        if ((r = cycle32(levels, nlevels, 0, vw, itercrsn, iterrfne))) return r;
+        k_tet_add_correction<<<std::min(nblk((long)f->ltot, 256), f->nsm * 8), 256, 0, f->stream>>>((long)f->ltot,
+                                                                                                  f->U, f->mx.U);
         ++nc;
         double rn;
         if ((r = hp_tet_resnorm(f, &rn))) return r;

@@ -483,6 +483,7 @@ class TetHierarchy:
         lib.hp_tet_mg_attach_h.argtypes = [P_, P_, P_, P_, P_, P_, ctypes.c_double]
         lib.hp_tet_solve_mg.argtypes = [ctypes.POINTER(P_), _I, ctypes.c_double, _I, _I, _I, _I, P_, _I,
                                         ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I)]
+        lib.hp_tet_solve_mg_mixed.argtypes = lib.hp_tet_solve_mg.argtypes
         self._keep = []
         for li in range(1, len(specs)):
             c, f = self.levels[li], self.levels[li - 1]
@@ -497,14 +498,16 @@ class TetHierarchy:
                                                    c2f[0].ctypes.data, c2f[1].ctypes.data, fadd), "mg_attach_h")
         self.lib = lib
 
-    def solve(self, drop=1e-10, max_cycles=300, vw=1, itercrsn=2, iterrfne=2):
+    def solve(self, drop=1e-10, max_cycles=300, vw=1, itercrsn=2, iterrfne=2, mixed=False):
+        """Cycles to a `drop` of the FP64 residual norm; mixed=True: FP32 (TF32 tensor-core)
+        smoothing inside FP64 defect correction (hp_tet_solve_mg_mixed)."""
         hs = (ctypes.c_void_p * len(self.levels))(*[g.h for g in self.levels])
         hist = np.zeros(max_cycles + 2)
         nh, nc = ctypes.c_int(), ctypes.c_int()
         sec = ctypes.c_double()
-        _check(self.lib, self.lib.hp_tet_solve_mg(hs, len(self.levels), drop, max_cycles, vw, itercrsn, iterrfne,
-                                                  hist.ctypes.data, len(hist), ctypes.byref(nh), ctypes.byref(sec),
-                                                  ctypes.byref(nc)), "solve_mg")
+        fn = self.lib.hp_tet_solve_mg_mixed if mixed else self.lib.hp_tet_solve_mg
+        _check(self.lib, fn(hs, len(self.levels), drop, max_cycles, vw, itercrsn, iterrfne, hist.ctypes.data,
+                            len(hist), ctypes.byref(nh), ctypes.byref(sec), ctypes.byref(nc)), "solve_mg")
         return hist[:nh.value], sec.value, nc.value
 
     def close(self):

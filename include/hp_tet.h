@@ -177,6 +177,18 @@ int hp_tet_mg_attach_h(hp_tet_ctx *coarse, hp_tet_ctx *fine, const int *f2c_tet,
  * preconditioner is set up on its first visit. Levels share one stream. */
 int hp_tet_solve_mg(hp_tet_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
                     int iterrfne, double *hist, int cap, int *nhist, double *seconds, int *cycles);
+/* hp_tet_solve_mg inside FP64 defect correction (no counterpart in the reference): each
+ * cycle takes the FP64 residual R64(u) of the finest level as the source of one FP32
+ * cycle on a correction d about the base state b = fp32(u) of every level (b restricted
+ * down the levels), with the residual in correction form R(b + d) - R(b) + source
+ * (tet_hp::rsdl's element loop on TF32 tensor cores, FP32 accumulation; the FAS term
+ * below the finest level), smoothed as hp_tet_solve_mg smooths (JACOBI relaxation or
+ * minvrt at p <= 2, the preconditioners set up once at the initial state and copied to
+ * FP32); then u += d in FP64. Convergence is judged by the FP64 residual norm, so the
+ * converged state is the FP64 one. Flux faces must be inflow faces (HP_ENOTSUP
+ * otherwise). Arguments as hp_tet_solve_mg. */
+int hp_tet_solve_mg_mixed(hp_tet_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
+                          int iterrfne, double *hist, int cap, int *nhist, double *seconds, int *cycles);
 
 /* Measurement helper (no counterpart in the reference): the FP64 tensor-core
  * (mma.m8n8k4.f64) throughput of this GPU, from independent accumulation chains
