@@ -434,9 +434,35 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=N
         cflw = {**cfl, **({1: 2.2, 2: 1.5} if p1_minvrt else {})}
         arms = {}
         states = {}
-        for arm, mixed in (("fp64", False), ("fp32_defect_correction", True)):
+        # the learned correction of the finest level's smoother, trained on the GPU on the
+        # solver's own samples of 4 smaller instances (8^3 x 6, p, Beltrami at other Re)
+        from hpb import learned as LR
+        from hpb.tet import TetGPU
+        t0 = _t.perf_counter()
+        rng = np.random.default_rng(20261211)
+        train_re = [float(x) for x in rng.uniform(40.0, 250.0, 4)]
+        F, T = [], []
+        for k, re in enumerate(train_re):
+            def level(re=re, k=k):
+                pr_ = TetProblem(cube_tets(8), p, mu=1.0 / re, cfl=cflw[p]).set_beltrami(re=re, seed=700 + k)
+                mk_, ff_ = pr_.cube_boundary(re=re)
+                g_ = TetGPU(pr_, stream=ctypes.c_void_p(cur.cuda_stream))
+                g_.set_dirichlet(mk_)
+                g_.set_flux_faces(ff_)
+                return g_
+            f, tg = LR.tet_solver_samples(level, snapshots=(0, 50, 200))
+            F.append(f)
+            T.append(tg)
+        net, lh = LR.train(np.concatenate(F), np.concatenate(T), steps=400)
+        arms["network"] = {"training_re": train_re, "samples": int(sum(len(t) for t in T)),
+                           "nonzero_targets": float(np.mean(np.concatenate(T) != 0)),
+                           "training_seconds": _t.perf_counter() - t0}
+        for arm, mixed, learned in (("fp64", False, False), ("fp32_defect_correction", True, False),
+                                    ("learned_fp32", True, True)):
             H = TetHierarchy(n, p, hlevels=hl, mu=1.0 / 100.0, cfl=cflw, stream=ctypes.c_void_p(cur.cuda_stream),
                              minvrt=p1_minvrt)
+            if learned:
+                H.levels[0].attach_net(net, 1.0)
             h, sec, nc = H.solve(drop=1e-10, max_cycles=400, vw=2, mixed=mixed)
             states[arm] = H.levels[0].state()
             arms[arm] = {"seconds": sec, "cycles": nc, "drop": float(h[-1]), "reached": bool(h[-1] <= 1e-10),
@@ -449,7 +475,9 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=N
                     np.sqrt(sum(np.sum((x - y) ** 2) for x, y in zip(a, b))) / np.sqrt(sum(np.sum(x * x) for x in a)))
             H.close()
             print(json.dumps({"c5_arm": arm, **arms[arm]}), flush=True)
+        net.close()
         arms["speedup_fp32_vs_fp64"] = arms["fp64"]["seconds"] / arms["fp32_defect_correction"]["seconds"]
+        arms["speedup_learned_fp32_vs_fp64"] = arms["fp64"]["seconds"] / arms["learned_fp32"]["seconds"]
         line["multigrid_full_w_to_1e-10"] = {"levels": f"p {p}..1, then h-levels down to {n >> hl}^3 at p = 1",
                                              "low_p_smoother": "minvrt (p = 1, 2; cfl 2.2, 1.5)" if p1_minvrt
                                              else "jacobi, cfl 0.5", **arms}

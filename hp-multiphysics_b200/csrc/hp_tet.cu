@@ -28,6 +28,7 @@
 
 #include "hp_gpu.h"
 #include "hp_tet.h"
+#include "hp_mlp.h"
 
 namespace {
 
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
     k_tet_rsdl_mma(const double *__restrict__ projB, const double *__restrict__ intB, TetSmall<double, P> sm,
                    TetMeshD mesh, TetFields<double> ug, TetFields<double> res, TetFields<double> rr,
                    const double *__restrict__ tau, double rho, double mu, double beta, double *rbar,
-                   TetFields<double> jd) {
+                   TetFields<double> jd, const float *__restrict__ lsc, float clampv) {
     using C = TetCfg<P>;
     using M = TetMma<P>;
     constexpr int G = C::G, Q = C::Q, T = C::T;
@@ -457,7 +458,14 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
                             if (m != jm[e] || n != jn[e]) continue;
                             double sg;
                             double *dst = mode_slot<double, P>(mesh, jd, te[e], m, n, sg);
-                            atomicAdd(dst, (tot[nt][h2] - rbar[rb]) / dw[e]);
+                            double sc = 1.0;  // learned per-tetrahedron scale of its contribution
+                            if (lsc) {
+                                float c = lsc[te[e]];
+                                c = c > clampv ? clampv : (c < -clampv ? -clampv : c);
+                                if (!(c == c)) c = 0.f;
+                                sc = exp((double)c);
+                            }
+                            atomicAdd(dst, sc * (tot[nt][h2] - rbar[rb]) / dw[e]);
                         }
                     }
             }
@@ -570,7 +578,7 @@ __global__ void k_tet_fold(long n, R *res, const R *rr) {
 // tet_hp_ins::setup_preconditioner, diagonal branch, steady, mesh velocity zero
 __global__ void k_tet_prcn(TetMeshD mesh, const double *ugv, double *tau, double *iprcn, double *vprcn,
                            double *eprcn, double *fprcn, int p, int em, int fm, double rho, double mu, double adis,
-                           double bd0, int *err) {
+                           double bd0, int *err, const float *lsc, float clampv) {
     const int VF[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};
     const double nu = mu / rho;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < mesh.ntet; t += gridDim.x * blockDim.x) {
@@ -605,7 +613,13 @@ __global__ void k_tet_prcn(TetMeshD mesh, const double *ugv, double *tau, double
         tau[2 * t] = adis * h / (jcb * sqrt(gam));
         tau[2 * t + 1] = qmax * tau[2 * t];
         jcb *= 2. * nu * (1. / (h * h) + 1. / (h * h) + 1. / (h * h)) + 3 * lam1 / h;
-        const double ip[NV] = {rho * jcb, rho * jcb, rho * jcb, jcb / gam};
+        double ip[NV] = {rho * jcb, rho * jcb, rho * jcb, jcb / gam};
+        if (lsc) {  // learned per-tetrahedron scale of its diagonal block (minvrt's preconditioner)
+            float cs = lsc[t];
+            cs = cs > clampv ? clampv : (cs < -clampv ? -clampv : cs);
+            if (!(cs == cs)) cs = 0.f;
+            for (int n = 0; n < NV; ++n) ip[n] *= exp((double)cs);
+        }
         for (int n = 0; n < NV; ++n) iprcn[(size_t)t * NV + n] = ip[n];
         for (int i = 0; i < 4; ++i)
             for (int n = 0; n < NV; ++n) atomicAdd(vprcn + (size_t)v[i] * NV + n, ip[n]);
@@ -774,6 +788,82 @@ __global__ void k_tet_fas(long n, R *res, const R *res0, R *dres, R fadd, int fi
 
 #include "hp_tet_mixed.cuh"
 
+// Inputs of the learned correction per tetrahedron (17, the widths of include/hp_mlp.h):
+// per variable (u, v, w, p) the mean and the range of its four vertex values and the rms
+// of its edge, face and interior modes (12); log volume, log longest edge, longest edge^3
+// / volume, log(1 + cell Peclet number of the vertex velocities) (4); p / 4.
+__global__ void k_tet_elem_features(TetMeshD mesh, TetFields<double> u, int p, int em, int fm, int im, double nu,
+                                    float *feat) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= mesh.ntet) return;
+    float *f = feat + (size_t)t * 17;
+    const int *v = mesh.tp + 4 * t;
+    double vmax = 0.0;
+    for (int n = 0; n < NV; ++n) {
+        double sum = 0.0, mx = -1e300, mn = 1e300;
+        for (int j = 0; j < 4; ++j) {
+            const double x = u.v[(size_t)v[j] * NV + n];
+            sum += x;
+            mx = fmax(mx, x);
+            mn = fmin(mn, x);
+        }
+        double ss = 0.0;
+        int cnt = 0;
+        for (int i = 0; i < 6 && em > 0; ++i)
+            for (int k = 0; k < em; ++k, ++cnt) {
+                const double x = u.e[((size_t)mesh.ts[6 * t + i] * em + k) * NV + n];
+                ss += x * x;
+            }
+        for (int i = 0; i < 4 && fm > 0; ++i)
+            for (int k = 0; k < fm; ++k, ++cnt) {
+                const double x = u.f[((size_t)mesh.tt[4 * t + i] * fm + k) * NV + n];
+                ss += x * x;
+            }
+        for (int k = 0; k < im; ++k, ++cnt) {
+            const double x = u.i[((size_t)t * im + k) * NV + n];
+            ss += x * x;
+        }
+        f[3 * n] = (float)(sum / 4.0);
+        f[3 * n + 1] = (float)(mx - mn);
+        f[3 * n + 2] = (float)(cnt > 0 ? sqrt(ss / cnt) : 0.0);
+    }
+    for (int j = 0; j < 4; ++j) {
+        const double *uu = u.v + (size_t)v[j] * NV;
+        vmax = fmax(vmax, sqrt(uu[0] * uu[0] + uu[1] * uu[1] + uu[2] * uu[2]));
+    }
+    double h2 = 0.0;
+    for (int a = 0; a < 4; ++a)
+        for (int b = a + 1; b < 4; ++b) {
+            double d2 = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                const double d = mesh.pnts[3 * v[a] + k] - mesh.pnts[3 * v[b] + k];
+                d2 += d * d;
+            }
+            h2 = fmax(h2, d2);
+        }
+    const double vol = fabs(mesh.vol[t]) / 6.0 + 1e-300, h = sqrt(h2);
+    f[12] = (float)log(vol);
+    f[13] = (float)log(h + 1e-300);
+    f[14] = (float)(h * h2 / vol);
+    f[15] = (float)log1p(vmax * h / (nu > 0 ? nu : 1e-300));
+    f[16] = (float)p / 4.0f;
+}
+
+// Sum of squares of a tetrahedron's own residual coefficients (vertex, edge, face, interior).
+template <int P>
+__global__ void k_tet_elem_resnorm(TetMeshD mesh, TetFields<double> res, double *out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= mesh.ntet) return;
+    double s2 = 0.0;
+    for (int m = 0; m < TetCfg<P>::T; ++m)
+        for (int n = 0; n < NV; ++n) {
+            double sg;
+            const double x = *mode_slot<double, P>(mesh, res, t, m, n, sg);
+            s2 += x * x;
+        }
+    out[t] = s2;
+}
+
 int nblk(long n, int b) { return (int)std::max<long>(1, (n + b - 1) / b); }
 
 }  // namespace
@@ -830,6 +920,12 @@ struct hp_tet_ctx {
         bool fas_pending = false;
     } mx;
     bool mixed_ready = false;
+    // learned correction: a per-tetrahedron log-scale of its contributions to the Jacobian
+    // diagonal (JACOBI smoother) and to minvrt's preconditioner, from a network or given
+    const float *lsc = nullptr;
+    float lsc_clamp = 0.f;
+    hp_mlp *net = nullptr;
+    float *d_feat = nullptr, *d_netout = nullptr;
     TetFields<float> fields32(float *base) const {
         return TetFields<float>{base, base + lv, base + lv + le, base + lv + le + lf};
     }
@@ -918,7 +1014,7 @@ int launch_rsdl(hp_tet_ctx *c, int stage) {
     int blocks = std::min(nblk(npair, M::WPC), c->nsm * 32);
     k_tet_rsdl_mma<P, 0><<<blocks, M::WPC * 32, smem2, c->stream>>>(
         c->projB, c->intB, sm, c->mesh, c->fields(c->U), c->fields(c->RES), c->fields(c->RR), c->tau, c->ph.rho,
-        c->ph.mu, beta, nullptr, TetFields<double>{});
+        c->ph.mu, beta, nullptr, TetFields<double>{}, nullptr, 0.f);
     k_tet_fold<double><<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>((long)c->ltot, c->RES,
                                                                                             c->RR);
     if (c->fine) {
@@ -953,11 +1049,11 @@ int launch_jacdiag(hp_tet_ctx *c) {
     const long n1 = ((long)c->mesh.ntet + 1) / 2, n2 = ((long)c->mesh.ntet * NV * C::T + 1) / 2;
     k_tet_rsdl_mma<P, 1><<<std::min(nblk(n1, M::WPC), c->nsm * 32), M::WPC * 32, M::SMEM, c->stream>>>(
         c->projB, c->intB, sm, c->mesh, c->fields(c->U), c->fields(c->RES), c->fields(c->RR), c->tau, c->ph.rho,
-        c->ph.mu, beta0, c->rbar, c->fields(c->JD));
+        c->ph.mu, beta0, c->rbar, c->fields(c->JD), nullptr, 0.f);
     TCK(cudaMemsetAsync(c->JD, 0, 8 * c->ltot, c->stream));
     k_tet_rsdl_mma<P, 2><<<std::min(nblk(n2, M::WPC), c->nsm * 32), M::WPC * 32, M::SMEM, c->stream>>>(
         c->projB, c->intB, sm, c->mesh, c->fields(c->U), c->fields(c->RES), c->fields(c->RR), c->tau, c->ph.rho,
-        c->ph.mu, beta0, c->rbar, c->fields(c->JD));
+        c->ph.mu, beta0, c->rbar, c->fields(c->JD), c->lsc, c->lsc_clamp);
     TCK(cudaGetLastError());
     return HP_OK;
 }
@@ -1183,15 +1279,21 @@ extern "C" int hp_tet_download_residual(hp_tet_ctx *c, int which, double *v, dou
     return copy_fields(c, which ? c->RR : c->RES, nullptr, nullptr, nullptr, nullptr, v, e, f, i);
 }
 
+static int tet_net_scale(hp_tet_ctx *c);
+
 extern "C" int hp_tet_setup_preconditioner(hp_tet_ctx *c) {
     if (!c) return HP_EINVAL;
+    if (c->net) {
+        int r0 = tet_net_scale(c);
+        if (r0) return r0;
+    }
     TCK(cudaMemsetAsync(c->d_err, 0, 4, c->stream));
     TCK(cudaMemsetAsync(c->vprcn, 0, 32 * (size_t)c->mesh.npnt, c->stream));
     TCK(cudaMemsetAsync(c->eprcn, 0, 32 * (size_t)c->mesh.nseg, c->stream));
     TCK(cudaMemsetAsync(c->fprcn, 0, 32 * (size_t)c->mesh.ntri, c->stream));
     k_tet_prcn<<<std::min(nblk(c->mesh.ntet, 128), c->nsm * 16), 128, 0, c->stream>>>(
         c->mesh, c->U, c->tau, c->iprcn, c->vprcn, c->eprcn, c->fprcn, c->p, c->em, c->fm, c->ph.rho, c->ph.mu,
-        c->ph.adis, c->ph.bd0, c->d_err);
+        c->ph.adis, c->ph.bd0, c->d_err, c->lsc, c->lsc_clamp);
     TCK(cudaGetLastError());
     int herr = 0;
     TCK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1296,6 +1398,10 @@ extern "C" int hp_tet_set_dirichlet(hp_tet_ctx *c, const unsigned char *mv, cons
 
 extern "C" int hp_tet_jacobian_diagonal(hp_tet_ctx *c) {
     if (!c) return HP_EINVAL;
+    if (c->net) {
+        int r0 = tet_net_scale(c);
+        if (r0) return r0;
+    }
     if (!c->prcn_ready) {
         set_err("hp_tet_jacobian_diagonal needs tau from hp_tet_setup_preconditioner");
         return HP_ESTATE;
@@ -1965,5 +2071,65 @@ extern "C" int hp_tet_solve_mg_mixed(hp_tet_ctx **levels, int nlevels, double dr
     if (nhist) *nhist = nh;
     if (seconds) *seconds = ms * 1e-3;
     if (cycles) *cycles = nc;
+    return HP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Learned correction of the tet smoother (no counterpart in the reference)
+// ---------------------------------------------------------------------------
+static int tet_net_scale(hp_tet_ctx *c) {
+    if (!c->d_feat && talloc(c, (void **)&c->d_feat, (size_t)c->mesh.ntet * 17 * 4)) return HP_ECUDA;
+    if (!c->d_netout && talloc(c, (void **)&c->d_netout, (size_t)c->mesh.ntet * 4)) return HP_ECUDA;
+    int r = hp_tet_elem_features(c, c->d_feat);
+    if (r) return r;
+    if (hp_mlp_forward(c->net, c->d_feat, c->mesh.ntet, c->d_netout, c->stream)) {
+        set_err("network forward failed: %s", hp_mlp_last_error());
+        return HP_ECUDA;
+    }
+    c->lsc = c->d_netout;
+    return HP_OK;
+}
+
+extern "C" int hp_tet_elem_features(hp_tet_ctx *c, float *d_feat) {
+    if (!c || !d_feat) return HP_EINVAL;
+    k_tet_elem_features<<<nblk(c->mesh.ntet, 128), 128, 0, c->stream>>>(c->mesh, c->fields(c->U), c->p, c->em, c->fm,
+                                                                       c->im, c->ph.mu / c->ph.rho, d_feat);
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+extern "C" int hp_tet_elem_resnorm(hp_tet_ctx *c, double *d_out) {
+    if (!c || !d_out) return HP_EINVAL;
+    const int g = nblk(c->mesh.ntet, 128);
+    switch (c->p) {
+        case 1: k_tet_elem_resnorm<1><<<g, 128, 0, c->stream>>>(c->mesh, c->fields(c->RES), d_out); break;
+        case 2: k_tet_elem_resnorm<2><<<g, 128, 0, c->stream>>>(c->mesh, c->fields(c->RES), d_out); break;
+        case 3: k_tet_elem_resnorm<3><<<g, 128, 0, c->stream>>>(c->mesh, c->fields(c->RES), d_out); break;
+        case 4: k_tet_elem_resnorm<4><<<g, 128, 0, c->stream>>>(c->mesh, c->fields(c->RES), d_out); break;
+    }
+    TCK(cudaGetLastError());
+    return HP_OK;
+}
+
+extern "C" int hp_tet_set_prcn_scale(hp_tet_ctx *c, const float *d_logscale, float clampv) {
+    if (!c) return HP_EINVAL;
+    c->lsc = d_logscale;
+    c->lsc_clamp = clampv;
+    c->net = nullptr;
+    return HP_OK;
+}
+
+extern "C" int hp_tet_set_prcn_net(hp_tet_ctx *c, hp_mlp *net, float clampv) {
+    if (!c) return HP_EINVAL;
+    if (net) {
+        int nin = 0, nout = 0;
+        if (hp_mlp_dims(net, &nin, &nout) || nin != 17 || nout != 1) {
+            set_err("hp_tet_set_prcn_net: the network must map 17 inputs to 1 output");
+            return HP_EINVAL;
+        }
+    }
+    c->net = net;
+    c->lsc = nullptr;
+    c->lsc_clamp = clampv;
     return HP_OK;
 }

@@ -178,6 +178,63 @@ def solver_samples(prob_factory, scales=(-1.0, -0.6, -0.3, 0.0, 0.3), k_updates=
     return np.concatenate(F), np.concatenate(Tg)
 
 
+def tet_solver_samples(level_factory, scales=(-1.0, -0.6, -0.3, 0.0, 0.3), k_updates=8, margin=0.02,
+                       snapshots=(0,)):
+    """(features, targets) of the tet smoother's learned correction from one instance,
+    generated by the solver as solver_samples does for tri_hp: level_factory() returns a
+    hpb.tet.TetGPU with its boundary set; at each snapshot state (cumulative plain
+    updates), every tetrahedron's target is the global log-scale of the smoother's diagonal
+    (JACOBI: the Jacobian diagonal; minvrt: its diagonal blocks) whose k_updates left that
+    tetrahedron with the smallest residual, 0 where none beats the plain method by margin."""
+    import torch
+    g = level_factory()
+    jacobi = True
+    pr = g.prob
+    ntet = pr.mesh.ntet
+    state = tuple(a.copy() for a in pr.state)
+
+    def prepare():
+        assert g.setup_preconditioner() == 0
+        if jacobi:
+            g.jacobian_diagonal()
+
+    F, Tg = [], []
+    done = 0
+    for snap in sorted(snapshots):
+        if snap > done:
+            g.upload(*state)
+            g.set_prcn_scale(None)
+            prepare()
+            g.iterate(snap - done)
+            state = tuple(g.state())
+            done = snap
+        g.upload(*state)
+        feats = g.elem_features()
+        ratios = []
+        for c in scales:
+            g.upload(*state)
+            sc = torch.full((ntet,), float(c), dtype=torch.float32, device="cuda")
+            torch.cuda.synchronize()
+            g.set_prcn_scale(ctypes.c_void_p(sc.data_ptr()), 1.5)
+            prepare()
+            r0 = g.elem_resnorm()
+            g.iterate(k_updates)
+            rk = g.elem_resnorm()
+            ratios.append(np.sqrt(rk / np.maximum(r0, 1e-300)))
+            g.set_prcn_scale(None)
+            del sc
+        R = np.array(ratios)
+        base = R[list(scales).index(0.0)]
+        best = np.argmin(R, axis=0)
+        tgt = np.array(scales)[best]
+        tgt[(R[best, np.arange(ntet)] > (1.0 - margin) * base) | ~np.isfinite(R).all(axis=0)] = 0.0
+        ok = np.isfinite(feats).all(axis=1)  # a snapshot state the plain smoother blew up gives no samples
+        F.append(feats[ok])
+        Tg.append(tgt[ok].astype(np.float32))
+    g.close()
+    return np.concatenate(F), np.concatenate(Tg)
+
+
 def train(feats, targets, widths=(17, 64, 64, 64, 1), steps=400, batch=4096, lr=2e-3, seed=1, log=None):
     """Trains an MLP on (features, targets) on the GPU; returns (net, loss history)."""
     import torch

@@ -302,6 +302,10 @@ def _bind():
         lib.hp_tet_download_jacobian_diagonal.argtypes = [P, P, P, P, P]
         lib.hp_tet_enqueue_update.argtypes = [P]
         lib.hp_tet_update.argtypes = [P]
+        lib.hp_tet_elem_features.argtypes = [P, P]
+        lib.hp_tet_elem_resnorm.argtypes = [P, P]
+        lib.hp_tet_set_prcn_scale.argtypes = [P, P, ctypes.c_float]
+        lib.hp_tet_set_prcn_net.argtypes = [P, P, ctypes.c_float]
         lib.hp_tet_resnorm.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
         lib.hp_tet_solve.argtypes = [P, ctypes.c_double, _I, _I, P, _I, ctypes.POINTER(_I),
                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_I)]
@@ -400,6 +404,39 @@ class TetGPU:
 
     def update(self):
         _check(self.lib, self.lib.hp_tet_update(self.h), "update")
+
+    def iterate(self, n):
+        for _ in range(n):
+            _check(self.lib, self.lib.hp_tet_enqueue_update(self.h), "update")
+        _check(self.lib, self.lib.hp_tet_sync(self.h), "sync")
+
+    def elem_features(self):
+        """[ntet][17] float32 inputs of the learned correction at the current state."""
+        import torch
+        d = torch.empty((self.prob.mesh.ntet, 17), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        _check(self.lib, self.lib.hp_tet_elem_features(self.h, ctypes.c_void_p(d.data_ptr())), "elem_features")
+        _check(self.lib, self.lib.hp_tet_sync(self.h), "sync")
+        return d.cpu().numpy()
+
+    def elem_resnorm(self):
+        """Per-tetrahedron residual measure of rsdl(nstage) at the current state."""
+        import torch
+        self.rsdl(self.prob.phys.nstage)
+        d = torch.empty(self.prob.mesh.ntet, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        _check(self.lib, self.lib.hp_tet_elem_resnorm(self.h, ctypes.c_void_p(d.data_ptr())), "elem_resnorm")
+        _check(self.lib, self.lib.hp_tet_sync(self.h), "sync")
+        return d.cpu().numpy()
+
+    def set_prcn_scale(self, d_logscale, clamp=1.5):
+        """Per-tetrahedron log-scales (a device pointer or None) of the smoother's diagonal."""
+        _check(self.lib, self.lib.hp_tet_set_prcn_scale(self.h, d_logscale, clamp), "set_prcn_scale")
+
+    def attach_net(self, net, clamp=1.0):
+        """The learned correction (hpb.learned.MLP, 17 -> 1) evaluated at every set-up; None detaches."""
+        _check(self.lib, self.lib.hp_tet_set_prcn_net(self.h, net.h if net is not None else None, clamp),
+               "set_prcn_net")
 
     def resnorm(self):
         r = ctypes.c_double()

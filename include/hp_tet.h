@@ -190,6 +190,25 @@ int hp_tet_solve_mg(hp_tet_ctx **levels, int nlevels, double drop, int max_cycle
 int hp_tet_solve_mg_mixed(hp_tet_ctx **levels, int nlevels, double drop, int max_cycles, int vw, int itercrsn,
                           int iterrfne, double *hist, int cap, int *nhist, double *seconds, int *cycles);
 
+/* Learned correction of the smoother (no counterpart in the reference; the 3D form of
+ * include/hp_mlp.h's hook on tri_hp's preconditioner). A per-tetrahedron log-scale c
+ * (clamped to +-clamp) multiplies that tetrahedron's contributions to the Jacobian
+ * diagonal of the JACOBI smoother (hp_tet_jacobian_diagonal) and to the diagonal blocks
+ * of minvrt's preconditioner (hp_tet_setup_preconditioner), so it changes the local
+ * pseudo-time step, never the residual. hp_tet_set_prcn_scale takes device scales
+ * [ntet] (NULL: none); hp_tet_set_prcn_net a network of 17 inputs and 1 output
+ * (hp_mlp) evaluated at every set-up on hp_tet_elem_features (NULL: none).
+ * hp_tet_elem_features writes the inputs [ntet][17] (per variable the mean and range of
+ * the vertex values and the rms of the edge, face and interior modes; log volume, log
+ * longest edge, longest edge^3 / volume, log(1 + cell Peclet); p / 4);
+ * hp_tet_elem_resnorm the sum of squares of each tetrahedron's residual coefficients
+ * [ntet] (after a residual evaluation). Device pointers, the context's stream. */
+struct hp_mlp;
+int hp_tet_set_prcn_scale(hp_tet_ctx *ctx, const float *d_logscale, float clamp);
+int hp_tet_set_prcn_net(hp_tet_ctx *ctx, struct hp_mlp *net, float clamp);
+int hp_tet_elem_features(hp_tet_ctx *ctx, float *d_feat);
+int hp_tet_elem_resnorm(hp_tet_ctx *ctx, double *d_out);
+
 /* Measurement helper (no counterpart in the reference): the FP64 tensor-core
  * (mma.m8n8k4.f64) throughput of this GPU, from independent accumulation chains
  * on every SM for about `ms` milliseconds. Writes TFLOP/s (2 flops per multiply-add). */
