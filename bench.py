@@ -430,8 +430,9 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=N
         ln = int(round(np.log2(n)))
         hl = hlevels or (max(1, ln - 1) if n <= 32 else max(1, ln - 3))
         # p1_minvrt: the p = 1 and 2 levels smoothed by the default build's tet_hp::minvrt at
-        # the reference's cfl (2.2, 1.5) instead of the JACOBI build's relaxation
-        cflw = {**cfl, **({1: 2.2, 2: 1.5} if p1_minvrt else {})}
+        # the reference's cfl (2.2, 1.5) instead of the JACOBI build's relaxation; "all": every
+        # level, the p = 3 level at its own cfl (1.0)
+        cflw = {**cfl, **({1: 2.2, 2: 1.5} if p1_minvrt else {}), **({3: 1.0} if p1_minvrt == "all" else {})}
         arms = {}
         states = {}
         # the learned correction of the finest level's smoother, trained on the GPU on the
@@ -449,8 +450,10 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=N
                 g_ = TetGPU(pr_, stream=ctypes.c_void_p(cur.cuda_stream))
                 g_.set_dirichlet(mk_)
                 g_.set_flux_faces(ff_)
+                if p1_minvrt == "all":
+                    g_.set_smoother(1)
                 return g_
-            f, tg = LR.tet_solver_samples(level, snapshots=(0, 50, 200))
+            f, tg = LR.tet_solver_samples(level, snapshots=(0, 50, 200), jacobi=p1_minvrt != "all")
             F.append(f)
             T.append(tg)
         net, lh = LR.train(np.concatenate(F), np.concatenate(T), steps=400)
@@ -479,8 +482,10 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=N
         arms["speedup_fp32_vs_fp64"] = arms["fp64"]["seconds"] / arms["fp32_defect_correction"]["seconds"]
         arms["speedup_learned_fp32_vs_fp64"] = arms["fp64"]["seconds"] / arms["learned_fp32"]["seconds"]
         line["multigrid_full_w_to_1e-10"] = {"levels": f"p {p}..1, then h-levels down to {n >> hl}^3 at p = 1",
-                                             "low_p_smoother": "minvrt (p = 1, 2; cfl 2.2, 1.5)" if p1_minvrt
-                                             else "jacobi, cfl 0.5", **arms}
+                                             "low_p_smoother": ("minvrt on every level (cfl 2.2, 1.5, 1.0)"
+                                                                if p1_minvrt == "all" else
+                                                                "minvrt (p = 1, 2; cfl 2.2, 1.5)" if p1_minvrt
+                                                                else "jacobi, cfl 0.5"), **arms}
         H = TetHierarchy(n, p, hlevels=1, mu=1.0 / 100.0, cfl=cfl, stream=ctypes.c_void_p(cur.cuda_stream))
     H.close()
     # CPU oracle on a bounded sample
@@ -863,7 +868,7 @@ def c3_headline(args, torch, dist, rank, world, dev, stream):
                "sample": f"oracle rsdl(nstage) on a 512 x {STRIP_ROWS}-square strip of the C3 mesh "
                          f"({2 * C3_N * STRIP_ROWS} triangles, p={C3_P}, lid-cavity state), {reps} evaluations "
                          "in 10 s, 1 core"}
-    launches_per_step = 4  # k_rsdl_pre, k_rsdl_elem, k_rsdl_fold, k_bdry_flux_ins
+    launches_per_step = 3  # element kernel (k_rsdl_ins_mma or k_rsdl_elem), k_bdry_flux_ins, k_assemble
     line = {
         "metric": METRIC, "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -925,6 +930,8 @@ def main():
                     help="with --sweep c3: run only these arms (e.g. fp64_level_by_level fp32_defect_correction)")
     ap.add_argument("--tet-minvrt", action="store_true",
                     help="with --sweep c5 --tet-solve: smooth the p = 1, 2 levels with tet_hp::minvrt (cfl 2.2, 1.5)")
+    ap.add_argument("--tet-minvrt-all", action="store_true",
+                    help="with --sweep c5 --tet-solve: smooth every level with tet_hp::minvrt (cfl 2.2, 1.5, 1.0)")
     ap.add_argument("--tet-hlevels", type=int, default=None,
                     help="with --sweep c5 --tet-solve: h-levels of the W-cycle hierarchy (default: down to 2^3 "
                          "for n <= 32, to 8^3 above)")
@@ -1000,7 +1007,7 @@ def main():
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         c5_sweep(torch, dev, args.mesh if args.mesh != N_MESH else 64, (args.p or [3])[0], args.steps, args.warmup,
                  timed_factory(torch, flush), full_solve=args.tet_solve, hlevels=args.tet_hlevels,
-                 p1_minvrt=args.tet_minvrt)
+                 p1_minvrt="all" if args.tet_minvrt_all else args.tet_minvrt)
         return
 
     if args.physics == "ins":

@@ -695,6 +695,200 @@ __global__ void k_tet_minv_v2e(TetMeshD m, int em, const R *mm, const R *iprcn, 
     }
 }
 
+// ---- tet_hp::minvrt at p = 3 (tet_hp/setup_preconditioner.cpp:16-354) and its vertex-ball
+// spoke factors (tet_hp::spoke, :530-583). em = 2, fm = 1, im = 0; iprcn is not inverted at
+// im = 0. Faces carry their vertices in the order of the tetrahedron that numbered them and
+// face edge i is the edge opposite face vertex i (tri_pnt / tri_seg below).
+constexpr int SPK_MAX = 64;  // spokes (edges) per vertex the solve kernel takes
+
+// rows fixed by essential conditions zeroed (the vdirichlet / edirichlet / fdirichlet of
+// tet_hp::update before minvrt, and minvrt's own)
+template <typename R>
+__global__ void k_tet_zero_fixed(long n, R *res, const unsigned char *mask) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x)
+        if (mask[k]) res[k] = (R)0;
+}
+
+// face modes removed from the face's vertices: res.v(tri.pnt(i)) -= ffmv(i, k) res.f(k)
+template <typename R>
+__global__ void k_tet_minv_f2v(int ntri, int fm, const int *tri_pnt, const R *ffmv, R *resv, const R *resf) {
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < ntri; f += gridDim.x * blockDim.x)
+        for (int i = 0; i < 3; ++i) {
+            const int v = tri_pnt[3 * f + i];
+            for (int k = 0; k < fm; ++k)
+                for (int n = 0; n < NV; ++n)
+                    atomicAdd(resv + (size_t)v * NV + n,
+                              -ffmv[i * (HP_TET_MAXP * (HP_TET_MAXP - 1) / 2) + k] * resf[((size_t)f * fm + k) * NV + n]);
+        }
+}
+
+// the face modes' share of a tetrahedron's removal: res.f(tri(i), ind) -= msgn mm(row, col(j))
+// u(j) iprcn, with msgn = (-rot)^(m-1) over the face-mode pairs (m, k); col(j) = j for the
+// vertex values (src = 0: u(j) = res.v of vertex j), 4 + j em (src = 1: res.e(seg(j), 0)) or
+// 5 + j em (src = 2: res.e(seg(j), 1)). src = 1 also removes the first edge modes from the
+// higher edge modes: res.e(seg(i), k) -= sgn^k mm(k + 4 + i em, 4 + j em) u(j).
+template <typename R>
+__global__ void k_tet_minv3_remove(TetMeshD m, int em, int fm, int src, const R *mm, const R *iprcn, const R *resv,
+                                   R *rese, R *resf) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m.ntet; t += gridDim.x * blockDim.x) {
+        const int nj = src == 0 ? 4 : 6;
+        R uh[6][NV];
+        for (int j = 0; j < nj; ++j)
+            for (int n = 0; n < NV; ++n) {
+                const R x = src == 0 ? resv[(size_t)m.tp[4 * t + j] * NV + n]
+                                     : rese[((size_t)m.ts[6 * t + j] * em + (src - 1)) * NV + n];
+                uh[j][n] = x * iprcn[(size_t)t * NV + n];
+            }
+        if (src == 0) {
+            for (int i = 0; i < 6; ++i) {
+                const int sind = m.ts[6 * t + i], sg = m.tsg[6 * t + i];
+                for (int j = 0; j < 4; ++j) {
+                    R msgn = 1;
+                    for (int k = 0; k < em; ++k) {
+                        const R c = mm[j * HP_TET_MAXT + 4 + k + i * em];
+                        for (int n = 0; n < NV; ++n)
+                            atomicAdd(rese + ((size_t)sind * em + k) * NV + n, -msgn * c * uh[j][n]);
+                        msgn *= sg;
+                    }
+                }
+            }
+        } else if (src == 1) {
+            for (int i = 0; i < 6; ++i) {
+                const int sind = m.ts[6 * t + i], sg = m.tsg[6 * t + i];
+                for (int j = 0; j < 6; ++j) {
+                    R msgn = (R)sg;
+                    for (int k = 1; k < em; ++k) {
+                        const R c = mm[(k + 4 + i * em) * HP_TET_MAXT + 4 + j * em];
+                        for (int n = 0; n < NV; ++n)
+                            atomicAdd(rese + ((size_t)sind * em + k) * NV + n, -msgn * c * uh[j][n]);
+                        msgn *= sg;
+                    }
+                }
+            }
+        }
+        for (int i = 0; i < 4; ++i) {
+            const int f = m.tt[4 * t + i], sg = -m.trot[4 * t + i];
+            for (int j = 0; j < nj; ++j) {
+                R msgn = 1;
+                int ind = 0;
+                const int col = src == 0 ? j : (src == 1 ? 4 + j * em : 5 + j * em);
+                for (int mm_ = 1; mm_ <= em - 1; ++mm_) {
+                    for (int k = 1; k <= em - mm_; ++k, ++ind) {
+                        const R c = src == 0 ? mm[col * HP_TET_MAXT + 4 + 6 * em + i * fm + ind]
+                                             : mm[(4 + 6 * em + i * fm + ind) * HP_TET_MAXT + col];
+                        for (int n = 0; n < NV; ++n) atomicAdd(resf + ((size_t)f * fm + ind) * NV + n, -msgn * c * uh[j][n]);
+                    }
+                    msgn *= sg;
+                }
+            }
+        }
+    }
+}
+
+// the spoke values of each edge end: w(s, 0 / 1) = e0 +- sfms(0) e1, and e0 = 0
+template <typename R>
+__global__ void k_tet_spoke_w(int nseg, int em, R sfms0, R *rese, R *w) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x)
+        for (int n = 0; n < NV; ++n) {
+            R *e = rese + (size_t)s * em * NV + n;
+            const R e0 = e[0], e1 = e[NV];
+            w[((size_t)s * 2) * NV + n] = e0 + sfms0 * e1;
+            w[((size_t)s * 2 + 1) * NV + n] = e0 - sfms0 * e1;
+            e[0] = (R)0;
+        }
+}
+
+// the face modes' share of the spoke values: edge i of face f takes ffms(i, k, 1) at the end
+// that is face vertex 2 (i = 0) or 0 (i = 1, 2), ffms(i, k, 0) at the other
+template <typename R>
+__global__ void k_tet_spoke_faces(int ntri, int fm, const int *tri_pnt, const int *tri_seg, const int *seg_pnt,
+                                  const R *ffms, const R *resf, R *w) {
+    constexpr int FS = HP_TET_MAXP * (HP_TET_MAXP - 1) / 2;
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < ntri; f += gridDim.x * blockDim.x)
+        for (int i = 0; i < 3; ++i) {
+            const int s = tri_seg[3 * f + i], x = tri_pnt[3 * f + (i == 0 ? 2 : 0)];
+            const int c1 = seg_pnt[2 * s] == x ? 0 : 1;
+            for (int k = 0; k < fm; ++k) {
+                const R a = ffms[(i * FS + k) * 2], b = ffms[(i * FS + k) * 2 + 1];
+                for (int n = 0; n < NV; ++n) {
+                    const R rf = resf[((size_t)f * fm + k) * NV + n];
+                    atomicAdd(w + ((size_t)s * 2 + c1) * NV + n, b * rf);
+                    atomicAdd(w + ((size_t)s * 2 + 1 - c1) * NV + n, a * rf);
+                }
+            }
+        }
+}
+
+// the vertex-ball solve, one thread per (vertex, variable): the spoke values of the vertex's
+// edges, solved with its LU factor (unit lower, upper; no row exchanges: the spoke matrix is
+// diagonally dominant), half of each solution added to the edge's first mode
+template <typename R>
+__global__ void k_tet_spoke_solve(int npnt, int em, const int *vs_ptr, const int *vs_seg, const int *vs_end,
+                                  const long long *fptr, const R *fac, const R *w, R *rese) {
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < (long)npnt * NV; q += (long)gridDim.x * blockDim.x) {
+        const int v = (int)(q / NV), n = (int)(q % NV);
+        const int b = vs_ptr[v], ns = vs_ptr[v + 1] - b;
+        const R *a = fac + fptr[v];
+        R x[SPK_MAX];
+        for (int k = 0; k < ns; ++k) x[k] = w[((size_t)vs_seg[b + k] * 2 + vs_end[b + k]) * NV + n];
+        for (int i = 1; i < ns; ++i) {
+            R sacc = x[i];
+            for (int j = 0; j < i; ++j) sacc -= a[(size_t)i * ns + j] * x[j];
+            x[i] = sacc;
+        }
+        for (int i = ns - 1; i >= 0; --i) {
+            R sacc = x[i];
+            for (int j = i + 1; j < ns; ++j) sacc -= a[(size_t)i * ns + j] * x[j];
+            x[i] = sacc / a[(size_t)i * ns + i];
+        }
+        for (int k = 0; k < ns; ++k) atomicAdd(rese + ((size_t)vs_seg[b + k] * em) * NV + n, x[k] / (R)2);
+    }
+}
+
+// the spoke matrices (tet_hp::spoke): per vertex, summed over its ball with the tetrahedron's
+// iprcn(tind, 0): mdiag on the diagonal of each of its three edges at the vertex, odiag
+// between them; LU-factored in place (no row exchanges), one thread per vertex. err counts
+// vertices with a pivot that is not positive.
+__global__ void k_tet_spoke_factor(int npnt, const int *vs_ptr, const int *vt_ptr, const int *vt_tet, const int *vt_spk,
+                                   const double *iprcn, double mdiag, double odiag, const long long *fptr, double *fac,
+                                   int *err) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < npnt; v += gridDim.x * blockDim.x) {
+        const int ns = vs_ptr[v + 1] - vs_ptr[v];
+        double *a = fac + fptr[v];
+        for (int k = 0; k < ns * ns; ++k) a[k] = 0.0;
+        for (int b = vt_ptr[v]; b < vt_ptr[v + 1]; ++b) {
+            const double jcb = iprcn[(size_t)vt_tet[b] * NV];
+            const int *e0 = vt_spk + 3 * b;
+            for (int j = 0; j < 3; ++j) {
+                a[e0[j] * ns + e0[j]] += jcb * mdiag;
+                for (int k = 0; k < 3; ++k)
+                    if (k != j) a[e0[j] * ns + e0[k]] += jcb * odiag;
+            }
+        }
+        bool ok = true;
+        for (int k = 0; k < ns; ++k) {
+            const double piv = a[k * ns + k];
+            ok = ok && piv > 0.0;
+            for (int i = k + 1; i < ns; ++i) {
+                const double l = a[i * ns + k] / piv;
+                a[i * ns + k] = l;
+                for (int j = k + 1; j < ns; ++j) a[i * ns + j] -= l * a[k * ns + j];
+            }
+        }
+        if (!ok) atomicAdd(err, 1);
+    }
+}
+
+// res *= (1 / prcn(entity, var)) diag on mode `mode` of a section with `modes` per entity, fixed rows zeroed
+template <typename R>
+__global__ void k_tet_minv_scale_mode(long nent, int modes, int mode, R *res, const R *prcn, R diag,
+                                      const unsigned char *mask) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < nent * NV; k += (long)gridDim.x * blockDim.x) {
+        const long ent = k / NV, var = k % NV, idx = (ent * modes + mode) * NV + var;
+        res[idx] = mask[idx] ? (R)0 : res[idx] * (((R)1 / prcn[ent * NV + var]) * diag);
+    }
+}
+
 // ug = ug0 - ca res
 template <typename R>
 __global__ void k_tet_advance(long n, const R *res, R *u, const R *u0, R ca) {
@@ -887,6 +1081,15 @@ struct hp_tet_ctx {
     int smoother = 0;  // 0: JACOBI build (jacobi_relaxation), 1: minvrt (p <= 2)
     int *seg_pnt = nullptr;           // [nseg][2] edge end points (global direction)
     double *d_mm = nullptr, *d_sfmv = nullptr;  // lumpinv tables for minvrt
+    // minvrt at p = 3: face vertices / edges [ntri][3]; per vertex its spokes (edge, end) in
+    // ball order (vs_*), its ball's tetrahedra with their three spokes (vt_*), the offsets of
+    // its LU factor (fptr) and the factors; the spoke values scratch [nseg][2][NV]
+    int *tri_pnt = nullptr, *tri_seg = nullptr, *vs_ptr = nullptr, *vs_seg = nullptr, *vs_end = nullptr;
+    int *vt_ptr = nullptr, *vt_tet = nullptr, *vt_spk = nullptr;
+    long long *fptr = nullptr;
+    long long nfac = 0;
+    int max_spk = 0;
+    double *fac = nullptr, *spk_w = nullptr, *d_ffmv = nullptr, *d_ffms = nullptr;
     bool smoother_ready() const { return smoother ? prcn_ready : jd_ready; }
     // multigrid: this level is coarser than `fine` (kind 1: p-level, 2: h-level)
     hp_tet_ctx *fine = nullptr;
@@ -915,6 +1118,7 @@ struct hp_tet_ctx {
         float *U = nullptr, *U0 = nullptr, *RES = nullptr, *RR = nullptr, *UB = nullptr, *DRES = nullptr;
         float *JD = nullptr, *BPT = nullptr, *TAU = nullptr, *RES0 = nullptr, *UF = nullptr;
         float *vprcn = nullptr, *eprcn = nullptr, *iprcn = nullptr, *mm = nullptr, *sfmv = nullptr;
+        float *fprcn = nullptr, *ffmv = nullptr, *ffms = nullptr, *fac = nullptr, *spk_w = nullptr;
         float2 *projB = nullptr, *intB = nullptr;
         float *F = nullptr;
         bool fas_pending = false;
@@ -1062,6 +1266,95 @@ int launch_jacdiag(hp_tet_ctx *c) {
 
 extern "C" const char *hp_tet_last_error(void) { return g_err.c_str(); }
 
+// The mesh data of minvrt at p = 3. Faces: the vertices of the tetrahedron that numbered the
+// face (rot = +1), in its order VF of that face (tet_mesh::create_tri_from_tet,
+// tet_mesh/setup.cpp:301-374); face edge i is the edge opposite face vertex i. Vertex balls:
+// the tetrahedra at a vertex by index, the vertex's edges numbered in the order the ball's
+// tetrahedra (local edges 0..5) first meet them (tet_hp::spoke, setup_preconditioner.cpp:530-561).
+static int spoke_topology(hp_tet_ctx *c, const hp_tet_mesh_desc *m, const std::vector<int> &sp) {
+    static const int VF[4][3] = {{1, 3, 2}, {0, 2, 3}, {0, 3, 1}, {0, 1, 2}};
+    static const int VS[6][2] = {{2, 3}, {3, 1}, {2, 1}, {1, 0}, {2, 0}, {3, 0}};
+    const int npnt = m->npnt, ntet = m->ntet, ntri = m->ntri;
+    std::vector<int> fp(3 * (size_t)ntri, -1), fs(3 * (size_t)ntri, -1);
+    for (int t = 0; t < ntet; ++t)
+        for (int i = 0; i < 4; ++i) {
+            if (m->tet_rot[4 * t + i] < 0) continue;
+            const int f = m->tet_tri[4 * t + i];
+            if (f < 0 || f >= ntri) { set_err("hp_tet_create: tet_tri out of range"); return HP_EINVAL; }
+            for (int j = 0; j < 3; ++j) fp[3 * (size_t)f + j] = m->tet_pnt[4 * t + VF[i][j]];
+            for (int j = 0; j < 3; ++j) {
+                const int a = VF[i][(j + 1) % 3], bb = VF[i][(j + 2) % 3];
+                for (int e = 0; e < 6; ++e)
+                    if ((VS[e][0] == a && VS[e][1] == bb) || (VS[e][0] == bb && VS[e][1] == a))
+                        fs[3 * (size_t)f + j] = m->tet_seg[6 * t + e];
+            }
+        }
+    for (size_t k = 0; k < fp.size(); ++k)
+        if (fp[k] < 0 || fs[k] < 0) {
+            set_err("hp_tet_create: face %zu is numbered by no tetrahedron (tet_rot +1)", k / 3);
+            return HP_EINVAL;
+        }
+    std::vector<int> vt_ptr(npnt + 1, 0), vt_tet(4 * (size_t)ntet);
+    for (int t = 0; t < ntet; ++t)
+        for (int j = 0; j < 4; ++j) ++vt_ptr[m->tet_pnt[4 * t + j] + 1];
+    for (int v = 0; v < npnt; ++v) vt_ptr[v + 1] += vt_ptr[v];
+    {
+        std::vector<int> fill(vt_ptr.begin(), vt_ptr.end() - 1);
+        for (int t = 0; t < ntet; ++t)
+            for (int j = 0; j < 4; ++j) vt_tet[fill[m->tet_pnt[4 * t + j]]++] = t;
+    }
+    std::vector<int> vs_ptr(npnt + 1, 0), vs_seg, vs_end, vt_spk(3 * (size_t)4 * ntet);
+    std::vector<long long> fptr(npnt + 1, 0);
+    std::vector<int> local(m->nseg, -1);
+    int max_spk = 0;
+    for (int v = 0; v < npnt; ++v) {
+        const int base = (int)vs_seg.size();
+        for (int b = vt_ptr[v]; b < vt_ptr[v + 1]; ++b) {
+            const int t = vt_tet[b];
+            int ind2 = 0;
+            for (int j = 0; j < 6; ++j) {
+                const int sidx = m->tet_seg[6 * t + j];
+                for (int k = 0; k < 2; ++k)
+                    if (sp[2 * (size_t)sidx + k] == v) {
+                        if (local[sidx] < 0) {
+                            local[sidx] = (int)vs_seg.size() - base;
+                            vs_seg.push_back(sidx);
+                            vs_end.push_back(k);
+                        }
+                        if (ind2 < 3) vt_spk[3 * (size_t)b + ind2] = local[sidx];
+                        ++ind2;
+                    }
+            }
+            if (ind2 != 3) { set_err("hp_tet_create: tetrahedron %d does not have three edges at its vertex %d", t, v); return HP_EINVAL; }
+        }
+        const int ns = (int)vs_seg.size() - base;
+        max_spk = std::max(max_spk, ns);
+        vs_ptr[v + 1] = (int)vs_seg.size();
+        fptr[v + 1] = fptr[v] + (long long)ns * ns;
+        for (int k = base; k < (int)vs_seg.size(); ++k) local[vs_seg[k]] = -1;
+    }
+    c->max_spk = max_spk;
+    c->nfac = fptr[npnt];
+    int r;
+    auto up = [&](const void *src, size_t bytes, void **dst) -> int {
+        if ((r = talloc(c, dst, bytes))) return r;
+        if (bytes) TCK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        return HP_OK;
+    };
+    if ((r = up(fp.data(), 4 * fp.size(), (void **)&c->tri_pnt)) || (r = up(fs.data(), 4 * fs.size(), (void **)&c->tri_seg)) ||
+        (r = up(vs_ptr.data(), 4 * vs_ptr.size(), (void **)&c->vs_ptr)) ||
+        (r = up(vs_seg.data(), 4 * vs_seg.size(), (void **)&c->vs_seg)) ||
+        (r = up(vs_end.data(), 4 * vs_end.size(), (void **)&c->vs_end)) ||
+        (r = up(vt_ptr.data(), 4 * vt_ptr.size(), (void **)&c->vt_ptr)) ||
+        (r = up(vt_tet.data(), 4 * vt_tet.size(), (void **)&c->vt_tet)) ||
+        (r = up(vt_spk.data(), 4 * vt_spk.size(), (void **)&c->vt_spk)) ||
+        (r = up(fptr.data(), 8 * fptr.size(), (void **)&c->fptr)) ||
+        (r = up(&c->tab.ffmv[0][0], sizeof(c->tab.ffmv), (void **)&c->d_ffmv)) ||
+        (r = up(&c->tab.ffms[0][0][0], sizeof(c->tab.ffms), (void **)&c->d_ffms)))
+        return r;
+    return HP_OK;
+}
+
 extern "C" int hp_tet_create(const hp_tet_mesh_desc *m, const hp_tet_tables *b, const hp_phys_params *ph, int device,
                              void *stream, hp_tet_ctx **out) {
     if (!m || !b || !ph || !out || b->p < 1 || b->p > HP_TET_MAXP || m->ntet < 1) {
@@ -1165,6 +1458,10 @@ extern "C" int hp_tet_create(const hp_tet_mesh_desc *m, const hp_tet_tables *b, 
         if ((r = up(sp.data(), 4 * sp.size(), (void **)&c->seg_pnt)) ||
             (r = up(&b->mm[0][0], sizeof(b->mm), (void **)&c->d_mm)) ||
             (r = up(&b->sfmv[0][0], sizeof(b->sfmv), (void **)&c->d_sfmv))) {
+            hp_tet_destroy(c);
+            return r;
+        }
+        if (c->p == 3 && (r = spoke_topology(c, m, sp))) {
             hp_tet_destroy(c);
             return r;
         }
@@ -1294,6 +1591,11 @@ extern "C" int hp_tet_setup_preconditioner(hp_tet_ctx *c) {
     k_tet_prcn<<<std::min(nblk(c->mesh.ntet, 128), c->nsm * 16), 128, 0, c->stream>>>(
         c->mesh, c->U, c->tau, c->iprcn, c->vprcn, c->eprcn, c->fprcn, c->p, c->em, c->fm, c->ph.rho, c->ph.mu,
         c->ph.adis, c->ph.bd0, c->d_err, c->lsc, c->lsc_clamp);
+    // minvrt at p = 3: the vertex-ball spoke factors from this iprcn (tet_hp::spoke)
+    if (c->smoother == 1 && c->p == 3)
+        k_tet_spoke_factor<<<nblk(c->mesh.npnt, 128), 128, 0, c->stream>>>(
+            c->mesh.npnt, c->vs_ptr, c->vt_ptr, c->vt_tet, c->vt_spk, c->iprcn, c->tab.mdiag, c->tab.odiag, c->fptr,
+            c->fac, c->d_err);
     TCK(cudaGetLastError());
     int herr = 0;
     TCK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1433,12 +1735,66 @@ extern "C" int hp_tet_set_smoother(hp_tet_ctx *c, int kind) {
         set_err("hp_tet_set_smoother: kind 0 (JACOBI build) or 1 (minvrt)");
         return HP_EINVAL;
     }
-    if (kind == 1 && c->p > 2) {
-        set_err("hp_tet_set_smoother: tet_hp::minvrt is built for p = 1 and 2 only");
+    if (kind == 1 && c->p > 3) {
+        set_err("hp_tet_set_smoother: tet_hp::minvrt is built for p = 1, 2 and 3 only");
         return HP_EINVAL;
+    }
+    if (kind == 1 && c->p == 3 && !c->fac) {
+        if (c->max_spk > SPK_MAX) {
+            set_err("hp_tet_set_smoother: a vertex has %d edges; the vertex-ball solve takes at most %d", c->max_spk,
+                    SPK_MAX);
+            return HP_ENOTSUP;
+        }
+        int r;
+        if ((r = talloc(c, (void **)&c->fac, 8 * (size_t)std::max<long long>(c->nfac, 1))) ||
+            (r = talloc(c, (void **)&c->spk_w, 8 * (size_t)c->mesh.nseg * 2 * NV)))
+            return r;
+        c->prcn_ready = false;  // the spoke factors come with the next preconditioner set-up
     }
     c->smoother = kind;
     return HP_OK;
+}
+
+// tet_hp::minvrt at p = 3 (tet_hp/setup_preconditioner.cpp:16-354) on res, in either precision:
+//  (1) edge and face modes removed from the vertices (sfmv, ffmv), the vertex rows scaled by
+//      vdiag / vprcn and fixed;
+//  (2) the vertex values times iprcn removed from the edge and face modes (mass matrix);
+//  (3) the edges' first modes from the vertex-ball solves: per edge end the spoke value
+//      e0 +- sfms(0) e1 plus the face modes times ffms, solved per vertex with its spoke
+//      factor, half of each end's solution to the edge; fixed edges zeroed;
+//  (4) the first edge modes times iprcn removed from the second edge modes and the faces, the
+//      second edge modes scaled by ediag(1) / eprcn (ediag(1) = 1000 as minvrt sets it at
+//      p = 3) and fixed;
+//  (5) the second edge modes times iprcn removed from the faces (minvrt reads res.e(side, 1)
+//      without the tetrahedron's edge sign there), the faces scaled by fdiag(0) / fprcn
+//      (fdiag(0) = 3000) and fixed.
+// The rows fixed by essential conditions are zeroed first, as tet_hp::update does.
+template <typename R>
+void enqueue_minvrt3(hp_tet_ctx *c, R *res, const R *vprcn, const R *eprcn, const R *fprcn, const R *iprcn,
+                     const R *mm, const R *sfmv, const R *ffmv, const R *ffms, const R *fac, R *w) {
+    const int g = c->nsm * 8, em = c->em, fm = c->fm;
+    const TetMeshD &m = c->mesh;
+    R *rv = res, *re = res + c->lv, *rf = res + c->lv + c->le;
+    const unsigned char *mv = c->mask, *me = c->mask + c->lv, *mf = c->mask + c->lv + c->le;
+    cudaStream_t st = c->stream;
+    k_tet_zero_fixed<R><<<std::min(nblk((long)c->ltot, 256), g), 256, 0, st>>>((long)c->ltot, res, c->mask);
+    k_tet_minv_e2v<R><<<std::min(nblk(m.nseg, 256), g), 256, 0, st>>>(m.nseg, em, c->seg_pnt, sfmv, rv, re, me);
+    k_tet_minv_f2v<R><<<std::min(nblk(m.ntri, 256), g), 256, 0, st>>>(m.ntri, fm, c->tri_pnt, ffmv, rv, rf);
+    k_tet_minv_scale<R><<<std::min(nblk((long)c->lv, 256), g), 256, 0, st>>>((long)c->lv, 1, rv, vprcn,
+                                                                           (R)c->tab.vdiag, mv);
+    k_tet_minv3_remove<R><<<std::min(nblk(m.ntet, 128), g), 128, 0, st>>>(m, em, fm, 0, mm, iprcn, rv, re, rf);
+    k_tet_spoke_w<R><<<std::min(nblk(m.nseg, 256), g), 256, 0, st>>>(m.nseg, em, (R)c->tab.sfms0, re, w);
+    k_tet_spoke_faces<R><<<std::min(nblk(m.ntri, 256), g), 256, 0, st>>>(m.ntri, fm, c->tri_pnt, c->tri_seg,
+                                                                         c->seg_pnt, ffms, rf, w);
+    k_tet_spoke_solve<R><<<std::min(nblk((long)m.npnt * NV, 128), g), 128, 0, st>>>(
+        m.npnt, em, c->vs_ptr, c->vs_seg, c->vs_end, c->fptr, fac, w, re);
+    k_tet_zero_fixed<R><<<std::min(nblk((long)c->le, 256), g), 256, 0, st>>>((long)c->le, re, me);
+    k_tet_minv3_remove<R><<<std::min(nblk(m.ntet, 128), g), 128, 0, st>>>(m, em, fm, 1, mm, iprcn, rv, re, rf);
+    k_tet_minv_scale_mode<R><<<std::min(nblk((long)m.nseg * NV, 256), g), 256, 0, st>>>((long)m.nseg, em, 1, re,
+                                                                                      eprcn, (R)1000, me);
+    k_tet_minv3_remove<R><<<std::min(nblk(m.ntet, 128), g), 128, 0, st>>>(m, em, fm, 2, mm, iprcn, rv, re, rf);
+    k_tet_minv_scale<R><<<std::min(nblk((long)c->lf, 256), g), 256, 0, st>>>((long)c->lf, fm, rf, fprcn, (R)3000,
+                                                                           mf);
 }
 
 extern "C" int hp_tet_enqueue_update(hp_tet_ctx *c) {
@@ -1456,7 +1812,12 @@ extern "C" int hp_tet_enqueue_update(hp_tet_ctx *c) {
         if (c->smoother && c->p == 1)  // the state is the vertex section alone (ltot = lv)
             k_tet_minvrt1<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
                 (long)c->ltot, c->RES, c->vprcn, c->tab.vdiag, c->mask, c->U, c->U0, ca);
-        else if (c->smoother) {
+        else if (c->smoother && c->p == 3) {
+            enqueue_minvrt3<double>(c, c->RES, c->vprcn, c->eprcn, c->fprcn, c->iprcn, c->d_mm, c->d_sfmv, c->d_ffmv,
+                                    c->d_ffms, c->fac, c->spk_w);
+            k_tet_advance<<<std::min(nblk((long)c->ltot, 256), c->nsm * 8), 256, 0, c->stream>>>(
+                (long)c->ltot, c->RES, c->U, c->U0, ca);
+        } else if (c->smoother) {
             const int g = c->nsm * 8;
             double *rv = c->RES, *re = c->RES + c->lv;
             k_tet_minv_e2v<<<std::min(nblk(c->mesh.nseg, 256), g), 256, 0, c->stream>>>(
@@ -1838,14 +2199,33 @@ void conv(hp_tet_ctx *c, long n, const A *src, B *dst) {
     if (n > 0) k_tet_convert<A, B><<<std::min(nblk(n, 256), c->nsm * 8), 256, 0, c->stream>>>(n, src, dst);
 }
 
-// FP32 copies of the preconditioner set up in FP64 at the base state
-void mixed_prcn(hp_tet_ctx *c) {
+// FP32 copies of the preconditioner set up in FP64 at the base state (and, for minvrt at
+// p = 3, of the face diagonals, the face tables and the spoke factors)
+int mixed_prcn(hp_tet_ctx *c) {
     hp_tet_ctx::Mixed &x = c->mx;
     conv(c, 2L * c->mesh.ntet, c->tau, x.TAU);
     conv(c, (long)c->ltot, c->JD, x.JD);
     conv(c, (long)c->mesh.ntet * NV, c->iprcn, x.iprcn);
     conv(c, (long)c->mesh.npnt * NV, c->vprcn, x.vprcn);
     conv(c, (long)c->mesh.nseg * NV, c->eprcn, x.eprcn);
+    if (c->smoother == 1 && c->p == 3 && c->fac) {
+        int r;
+        if (!x.fac) {
+            std::vector<float> ff(sizeof(c->tab.ffmv) / 8), fs(sizeof(c->tab.ffms) / 8);
+            for (size_t k = 0; k < ff.size(); ++k) ff[k] = (float)(&c->tab.ffmv[0][0])[k];
+            for (size_t k = 0; k < fs.size(); ++k) fs[k] = (float)(&c->tab.ffms[0][0][0])[k];
+            if ((r = talloc(c, (void **)&x.fac, 4 * (size_t)std::max<long long>(c->nfac, 1))) ||
+                (r = talloc(c, (void **)&x.spk_w, 4 * (size_t)c->mesh.nseg * 2 * NV)) ||
+                (r = talloc(c, (void **)&x.fprcn, 16 * (size_t)std::max(1, c->mesh.ntri))) ||
+                (r = talloc(c, (void **)&x.ffmv, 4 * ff.size())) || (r = talloc(c, (void **)&x.ffms, 4 * fs.size())))
+                return r;
+            TCK(cudaMemcpy(x.ffmv, ff.data(), 4 * ff.size(), cudaMemcpyHostToDevice));
+            TCK(cudaMemcpy(x.ffms, fs.data(), 4 * fs.size(), cudaMemcpyHostToDevice));
+        }
+        conv(c, (long)c->mesh.ntri * NV, c->fprcn, x.fprcn);
+        conv(c, (long)c->nfac, c->fac, x.fac);
+    }
+    return HP_OK;
 }
 
 template <int P>
@@ -1918,6 +2298,10 @@ int update32(hp_tet_ctx *c) {
         if (c->smoother && c->p == 1) {
             k_tet_minvrt1<float><<<g, 256, 0, c->stream>>>((long)c->ltot, x.RES, x.vprcn, (float)c->tab.vdiag, c->mask,
                                                            x.U, x.U0, ca);
+        } else if (c->smoother && c->p == 3) {
+            enqueue_minvrt3<float>(c, x.RES, x.vprcn, x.eprcn, x.fprcn, x.iprcn, x.mm, x.sfmv, x.ffmv, x.ffms, x.fac,
+                                   x.spk_w);
+            k_tet_advance<float><<<g, 256, 0, c->stream>>>((long)c->ltot, x.RES, x.U, x.U0, ca);
         } else if (c->smoother) {
             float *rv = x.RES, *re = x.RES + c->lv;
             k_tet_minv_e2v<float><<<std::min(nblk(c->mesh.nseg, 256), c->nsm * 8), 256, 0, c->stream>>>(
@@ -2043,7 +2427,7 @@ extern "C" int hp_tet_solve_mg_mixed(hp_tet_ctx **levels, int nlevels, double dr
         r = hp_tet_setup_preconditioner(c);
         if (r) return r < 0 ? r : HP_ESTATE;
         if (!c->smoother && (r = hp_tet_jacobian_diagonal(c))) return r;
-        mixed_prcn(c);
+        if ((r = mixed_prcn(c))) return r;
     }
     double r0;
     if ((r = hp_tet_resnorm(f, &r0))) return r;  // leaves R64(u) in f->RES

@@ -179,16 +179,16 @@ def solver_samples(prob_factory, scales=(-1.0, -0.6, -0.3, 0.0, 0.3), k_updates=
 
 
 def tet_solver_samples(level_factory, scales=(-1.0, -0.6, -0.3, 0.0, 0.3), k_updates=8, margin=0.02,
-                       snapshots=(0,)):
+                       snapshots=(0,), jacobi=True):
     """(features, targets) of the tet smoother's learned correction from one instance,
     generated by the solver as solver_samples does for tri_hp: level_factory() returns a
     hpb.tet.TetGPU with its boundary set; at each snapshot state (cumulative plain
     updates), every tetrahedron's target is the global log-scale of the smoother's diagonal
     (JACOBI: the Jacobian diagonal; minvrt: its diagonal blocks) whose k_updates left that
-    tetrahedron with the smallest residual, 0 where none beats the plain method by margin."""
+    tetrahedron with the smallest residual, 0 where none beats the plain method by margin.
+    jacobi=False: the level smooths with minvrt (its factory called set_smoother(1))."""
     import torch
     g = level_factory()
-    jacobi = True
     pr = g.prob
     ntet = pr.mesh.ntet
     state = tuple(a.copy() for a in pr.state)

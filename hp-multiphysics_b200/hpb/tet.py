@@ -385,7 +385,8 @@ class TetGPU:
                "set_dirichlet")
 
     def set_smoother(self, kind):
-        """0: the JACOBI build's jacobi_relaxation; 1: tet_hp::minvrt (p = 1 and 2)."""
+        """0: the JACOBI build's jacobi_relaxation; 1: tet_hp::minvrt (p = 1, 2 and 3). At
+        p = 3 the vertex-ball spoke factors come with the next setup_preconditioner."""
         _check(self.lib, self.lib.hp_tet_set_smoother(self.h, kind), "set_smoother")
 
     def set_flux_faces(self, ff):
@@ -490,7 +491,7 @@ class TetHierarchy:
     Beltrami state, the boundary layout of TetProblem.cube_boundary (inflow on all six
     faces with a balanced boundary flux; outflow=True: a neumann outflow at x = 1) and
     `cfl[p]`; minvrt=True smooths the p = 1 and 2 levels with tet_hp::minvrt instead of the
-    JACOBI build's relaxation."""
+    JACOBI build's relaxation, minvrt="all" every level (p = 3 included)."""
 
     def __init__(self, n, p, hlevels=2, mu=0.01, cfl=None, re=100.0, noise=1e-3, stream=None, fadd=1.0,
                  outflow=False, minvrt=False):
@@ -509,7 +510,7 @@ class TetHierarchy:
             g = TetGPU(pr, stream=stream)
             g.set_dirichlet(masks)
             g.set_flux_faces(ff)
-            if q <= 2 and minvrt:
+            if minvrt == "all" or (q <= 2 and minvrt):
                 g.set_smoother(1)
             self.probs.append(pr)
             self.masks.append(masks)

@@ -8,7 +8,8 @@
 //   tet_hp_ins::setup_preconditioner    tet_hp/ins/setup_preconditioner.cpp (diagonal: tau, iprcn)
 //   bdry_ins::neumann / inflow rsdl     tet_hp/ins/bdry.cpp:16-102, bdry_ins.h:85-132
 //   tet_hp::jacobian_diagonal, jacobi_relaxation   tet_hp/jacobi.cpp:14-111
-//   tet_hp::minvrt (p = 1 and 2)        tet_hp/setup_preconditioner.cpp:11-221
+//   tet_hp::minvrt (p = 1, 2 and 3)     tet_hp/setup_preconditioner.cpp:11-354
+//   tet_hp::spoke (p = 3)               tet_hp/setup_preconditioner.cpp:530-583
 //   tet_hp::update                      tet_hp/update.cpp:181-390
 // with the basis operators of tet_basis in the dense form of hp_tet_tables
 // (pinned against the reference's own proj / intgrt / intgrtrst / derivr / derivs /
@@ -46,7 +47,7 @@ struct OT {
     // signs [3], kind (0 inflow, 1 neumann), imposed pressure at the face points [G * G]
     std::vector<int> bf_tri, bf_pnt, bf_seg, bf_sgn, bf_kind;
     std::vector<double> bf_pbc;
-    int smoother = 0;  // 0: JACOBI build, 1: minvrt (p = 1)
+    int smoother = 0;  // 0: JACOBI build, 1: minvrt
 };
 
 // the face vertices of local face i (tet_mesh/setup.cpp:307-310)
@@ -587,10 +588,303 @@ static void minvrt_p2(OT &o) {
     all_dirichlet(o);
 }
 
-// 0: the JACOBI build's smoother, 1: minvrt (p = 1 and 2; -1 otherwise)
+// Edge end points in the global direction: tet_sgn = +1 where the tetrahedron's local edge i
+// runs from its first to its second local vertex (VS) the way the global edge does.
+static const int VS[6][2] = {{2, 3}, {3, 1}, {2, 1}, {1, 0}, {2, 0}, {3, 0}};
+static std::vector<int> seg_ends(const OT &o) {
+    std::vector<int> sp(2 * (size_t)o.nseg);
+    for (int tind = 0; tind < o.ntet; ++tind)
+        for (int i = 0; i < 6; ++i) {
+            const int s = o.ts[6 * tind + i], a = o.tp[4 * tind + VS[i][0]], b = o.tp[4 * tind + VS[i][1]];
+            sp[2 * (size_t)s] = o.tsg[6 * tind + i] > 0 ? a : b;
+            sp[2 * (size_t)s + 1] = o.tsg[6 * tind + i] > 0 ? b : a;
+        }
+    return sp;
+}
+
+// Face vertices and edges. A face takes its vertices from the tetrahedron that numbered it
+// (rot = +1), in that tetrahedron's order VF of the face (tet_mesh::create_tri_from_tet,
+// tet_mesh/setup.cpp:301-374); face edge i is the edge opposite face vertex i. That is the
+// numbering tet_basis's face basis uses (proj2d.cpp:46-91), and with it tet_hp::minvrt's
+// face steps (setup_preconditioner.cpp:16-44, 142-175) name the right edge ends.
+static void face_topology(const OT &o, std::vector<int> &fp, std::vector<int> &fs) {
+    fp.assign(3 * (size_t)o.ntri, -1);
+    fs.assign(3 * (size_t)o.ntri, -1);
+    for (int tind = 0; tind < o.ntet; ++tind)
+        for (int i = 0; i < 4; ++i) {
+            if (o.trot[4 * tind + i] < 0) continue;
+            const int f = o.tt[4 * tind + i];
+            for (int j = 0; j < 3; ++j) fp[3 * (size_t)f + j] = o.tp[4 * tind + VF[i][j]];
+            for (int j = 0; j < 3; ++j) {
+                const int a = VF[i][(j + 1) % 3], b = VF[i][(j + 2) % 3];
+                for (int e = 0; e < 6; ++e)
+                    if ((VS[e][0] == a && VS[e][1] == b) || (VS[e][0] == b && VS[e][1] == a))
+                        fs[3 * (size_t)f + j] = o.ts[6 * tind + e];
+            }
+        }
+}
+
+// LU with partial pivoting of an n x n matrix, row-major, in place (the unblocked
+// algorithm of LAPACK's dgetrf); piv[k] = the row swapped with row k. Returns 0, or k + 1
+// when the pivot of column k is zero.
+static int lu_factor(int n, double *a, int *piv) {
+    for (int k = 0; k < n; ++k) {
+        int r = k;
+        for (int i = k + 1; i < n; ++i)
+            if (std::fabs(a[(size_t)i * n + k]) > std::fabs(a[(size_t)r * n + k])) r = i;
+        piv[k] = r;
+        if (a[(size_t)r * n + k] == 0.0) return k + 1;
+        if (r != k)
+            for (int j = 0; j < n; ++j) std::swap(a[(size_t)k * n + j], a[(size_t)r * n + j]);
+        for (int i = k + 1; i < n; ++i) {
+            const double l = a[(size_t)i * n + k] / a[(size_t)k * n + k];
+            a[(size_t)i * n + k] = l;
+            for (int j = k + 1; j < n; ++j) a[(size_t)i * n + j] -= l * a[(size_t)k * n + j];
+        }
+    }
+    return 0;
+}
+
+static void lu_solve(int n, const double *a, const int *piv, double *b) {
+    for (int k = 0; k < n; ++k)
+        if (piv[k] != k) std::swap(b[k], b[piv[k]]);
+    for (int i = 1; i < n; ++i)
+        for (int j = 0; j < i; ++j) b[i] -= a[(size_t)i * n + j] * b[j];
+    for (int i = n - 1; i >= 0; --i) {
+        for (int j = i + 1; j < n; ++j) b[i] -= a[(size_t)i * n + j] * b[j];
+        b[i] /= a[(size_t)i * n + i];
+    }
+}
+
+// tet_hp::spoke (setup_preconditioner.cpp:530-583), p = 3: for every vertex the matrix of its
+// spokes (the edges at the vertex, numbered in the order the vertex ball first meets them:
+// tetrahedra by index, then local edges 0..5), summed over the tetrahedra of the ball with
+// the tetrahedron's iprcn(tind, 0): mdiag on the diagonal of each of its three edges at the
+// vertex, odiag between them; factored by LU. The matrix is symmetric, so the transposed
+// solve of minvrt (dgetrs "T") is the plain one.
+struct Spokes {
+    std::vector<int> ptr, seg, end, fptr, piv;
+    std::vector<double> lu;
+};
+static int spoke(const OT &o, const std::vector<int> &sp, Spokes &S) {
+    std::vector<std::vector<int>> ball(o.npnt);
+    for (int tind = 0; tind < o.ntet; ++tind)
+        for (int j = 0; j < 4; ++j) ball[o.tp[4 * tind + j]].push_back(tind);
+    S.ptr.assign(o.npnt + 1, 0);
+    S.fptr.assign(o.npnt + 1, 0);
+    S.seg.clear(); S.end.clear(); S.lu.clear(); S.piv.clear();
+    std::vector<int> local(o.nseg, -1);
+    for (int v = 0; v < o.npnt; ++v) {
+        const int base = (int)S.seg.size();
+        std::vector<int> tri3;  // per ball tetrahedron: its three spokes
+        for (int tind : ball[v])
+            for (int j = 0; j < 6; ++j) {
+                const int s = o.ts[6 * tind + j];
+                for (int k = 0; k < 2; ++k)
+                    if (sp[2 * (size_t)s + k] == v) {
+                        if (local[s] < 0) {
+                            local[s] = (int)S.seg.size() - base;
+                            S.seg.push_back(s);
+                            S.end.push_back(k);
+                        }
+                        tri3.push_back(local[s]);
+                    }
+            }
+        const int n = (int)S.seg.size() - base;
+        S.ptr[v + 1] = (int)S.seg.size();
+        std::vector<double> a((size_t)n * n, 0.0);
+        for (size_t b = 0; b < ball[v].size(); ++b) {
+            const double jcb = o.iprcn[(size_t)ball[v][b] * NV];
+            const int *e0 = &tri3[3 * b];
+            for (int j = 0; j < 3; ++j) {
+                a[(size_t)e0[j] * n + e0[j]] += jcb * o.t.mdiag;
+                for (int k = 0; k < 3; ++k)
+                    if (k != j) a[(size_t)e0[j] * n + e0[k]] += jcb * o.t.odiag;
+            }
+        }
+        std::vector<int> piv(n);
+        if (lu_factor(n, a.data(), piv.data())) return v + 1;
+        S.lu.insert(S.lu.end(), a.begin(), a.end());
+        S.piv.insert(S.piv.end(), piv.begin(), piv.end());
+        S.fptr[v + 1] = (int)S.lu.size();
+        for (int k = base; k < (int)S.seg.size(); ++k) local[S.seg[k]] = -1;
+    }
+    return 0;
+}
+
+static void edirichlet(OT &o) {
+    if (o.me.empty()) return;
+    for (int e = 0; e < o.nseg; ++e)
+        for (int m = 0; m < o.t.em; ++m)
+            for (int n = 0; n < NV; ++n)
+                if (o.me[(size_t)e * NV + n]) o.re[((size_t)e * o.t.em + m) * NV + n] = 0.0;
+}
+static void fdirichlet(OT &o) {
+    if (o.mf.empty()) return;
+    for (int f = 0; f < o.ntri; ++f)
+        for (int m = 0; m < o.t.fm; ++m)
+            for (int n = 0; n < NV; ++n)
+                if (o.mf[(size_t)f * NV + n]) o.rf[((size_t)f * o.t.fm + m) * NV + n] = 0.0;
+}
+
+// tet_hp::minvrt at p = 3 (setup_preconditioner.cpp:16-354, em = 2, fm = 1, im = 0; iprcn is
+// not inverted at im = 0, tet_hp::setup_preconditioner :463-465):
+//  (1) edge and face modes removed from the vertices (sfmv, ffmv), the vertex rows scaled by
+//      vdiag / vprcn and fixed;
+//  (2) the vertex values times iprcn removed from the edge and face modes (mass matrix);
+//  (3) the edges' first modes from the vertex-ball solves: per edge end the spoke value
+//      e0 +- sfms(0) e1 plus the face modes times ffms, solved per vertex with its spoke
+//      factor, each edge receiving half of each end's solution; fixed edges zeroed;
+//  (4) the first edge modes times iprcn removed from the second edge modes and the faces
+//      (mass matrix), the second edge modes scaled by ediag(1) / eprcn, ediag(1) = 1000 as
+//      minvrt sets it, and fixed;
+//  (5) the second edge modes times iprcn removed from the faces (minvrt takes res.e(side,1)
+//      without the tetrahedron's edge sign here, and so does this restatement), the faces
+//      scaled by fdiag(0) / fprcn, fdiag(0) = 3000, and fixed.
+static void minvrt_p3(OT &o, const Spokes &S, const std::vector<int> &sp, const std::vector<int> &fp,
+                      const std::vector<int> &fs) {
+    const hp_tet_tables &t = o.t;
+    const int em = t.em, fm = t.fm;
+    auto E = [&](int s, int k, int n) -> double & { return o.re[((size_t)s * em + k) * NV + n]; };
+    auto F = [&](int f, int k, int n) -> double & { return o.rf[((size_t)f * fm + k) * NV + n]; };
+    // (1)
+    for (int s = 0; s < o.nseg; ++s)
+        for (int k = 0; k < em; ++k)
+            for (int i = 0; i < 2; ++i)
+                for (int n = 0; n < NV; ++n) o.rv[(size_t)sp[2 * s + i] * NV + n] -= t.sfmv[i][k] * E(s, k, n);
+    for (int f = 0; f < o.ntri; ++f)
+        for (int i = 0; i < 3; ++i)
+            for (int k = 0; k < fm; ++k)
+                for (int n = 0; n < NV; ++n) o.rv[(size_t)fp[3 * f + i] * NV + n] -= t.ffmv[i][k] * F(f, k, n);
+    for (size_t k = 0; k < o.rv.size(); ++k) o.rv[k] *= (1.0 / o.vprcn[k]) * t.vdiag;
+    all_dirichlet(o);
+    // (2)
+    for (int tind = 0; tind < o.ntet; ++tind) {
+        double uh[4][NV];
+        for (int j = 0; j < 4; ++j)
+            for (int n = 0; n < NV; ++n) uh[j][n] = o.rv[(size_t)o.tp[4 * tind + j] * NV + n] * o.iprcn[(size_t)tind * NV + n];
+        for (int i = 0; i < 6; ++i) {
+            const int s = o.ts[6 * tind + i], sg = o.tsg[6 * tind + i];
+            for (int j = 0; j < 4; ++j) {
+                double msgn = 1.0;
+                for (int k = 0; k < em; ++k) {
+                    for (int n = 0; n < NV; ++n) E(s, k, n) -= msgn * t.mm[j][4 + k + i * em] * uh[j][n];
+                    msgn *= sg;
+                }
+            }
+        }
+        for (int i = 0; i < 4; ++i) {
+            const int f = o.tt[4 * tind + i], sg = -o.trot[4 * tind + i];
+            for (int j = 0; j < 4; ++j) {
+                double msgn = 1.0;
+                int ind = 0;
+                for (int m = 1; m <= em - 1; ++m) {
+                    for (int k = 1; k <= em - m; ++k, ++ind)
+                        for (int n = 0; n < NV; ++n) F(f, ind, n) -= msgn * t.mm[j][4 + 6 * em + i * fm + ind] * uh[j][n];
+                    msgn *= sg;
+                }
+            }
+        }
+    }
+    // (3)
+    std::vector<double> w((size_t)o.nseg * 2 * NV);
+    for (int s = 0; s < o.nseg; ++s)
+        for (int n = 0; n < NV; ++n) {
+            w[((size_t)s * 2 + 0) * NV + n] = E(s, 0, n) + t.sfms0 * E(s, 1, n);
+            w[((size_t)s * 2 + 1) * NV + n] = E(s, 0, n) - t.sfms0 * E(s, 1, n);
+            E(s, 0, n) = 0.0;
+        }
+    for (int f = 0; f < o.ntri; ++f)
+        for (int i = 0; i < 3; ++i) {
+            const int s = fs[3 * f + i], x = fp[3 * f + (i == 0 ? 2 : 0)];
+            const int c1 = sp[2 * (size_t)s] == x ? 0 : 1;  // the spoke end that takes ffms(i, k, 1)
+            for (int k = 0; k < fm; ++k)
+                for (int n = 0; n < NV; ++n) {
+                    w[((size_t)s * 2 + c1) * NV + n] += t.ffms[i][k][1] * F(f, k, n);
+                    w[((size_t)s * 2 + 1 - c1) * NV + n] += t.ffms[i][k][0] * F(f, k, n);
+                }
+        }
+    std::vector<double> rhs;
+    for (int v = 0; v < o.npnt; ++v) {
+        const int b = S.ptr[v], nspk = S.ptr[v + 1] - b;
+        rhs.resize(nspk);
+        for (int n = 0; n < NV; ++n) {
+            for (int k = 0; k < nspk; ++k) rhs[k] = w[((size_t)S.seg[b + k] * 2 + S.end[b + k]) * NV + n];
+            lu_solve(nspk, &S.lu[S.fptr[v]], &S.piv[b], rhs.data());
+            for (int k = 0; k < nspk; ++k) E(S.seg[b + k], 0, n) += rhs[k] / 2.0;
+        }
+    }
+    edirichlet(o);
+    // (4)
+    for (int tind = 0; tind < o.ntet; ++tind) {
+        double uh[6][NV];
+        for (int i = 0; i < 6; ++i)
+            for (int n = 0; n < NV; ++n) uh[i][n] = E(o.ts[6 * tind + i], 0, n) * o.iprcn[(size_t)tind * NV + n];
+        for (int i = 0; i < 6; ++i) {
+            const int s = o.ts[6 * tind + i], sg = o.tsg[6 * tind + i];
+            for (int j = 0; j < 6; ++j) {
+                double msgn = sg;
+                for (int k = 1; k < em; ++k) {
+                    for (int n = 0; n < NV; ++n) E(s, k, n) -= msgn * t.mm[k + 4 + i * em][4 + j * em] * uh[j][n];
+                    msgn *= sg;
+                }
+            }
+        }
+        for (int i = 0; i < 4; ++i) {
+            const int f = o.tt[4 * tind + i], sg = -o.trot[4 * tind + i];
+            for (int j = 0; j < 6; ++j) {
+                double msgn = 1.0;
+                int ind = 0;
+                for (int m = 1; m <= em - 1; ++m) {
+                    for (int k = 1; k <= em - m; ++k, ++ind)
+                        for (int n = 0; n < NV; ++n)
+                            F(f, ind, n) -= msgn * t.mm[4 + 6 * em + i * fm + ind][4 + j * em] * uh[j][n];
+                    msgn *= sg;
+                }
+            }
+        }
+    }
+    for (int s = 0; s < o.nseg; ++s)
+        for (int n = 0; n < NV; ++n) E(s, 1, n) *= (1.0 / o.eprcn[(size_t)s * NV + n]) * 1000.0;
+    edirichlet(o);
+    // (5)
+    for (int tind = 0; tind < o.ntet; ++tind) {
+        double uh[6][NV];
+        for (int i = 0; i < 6; ++i)
+            for (int n = 0; n < NV; ++n) uh[i][n] = E(o.ts[6 * tind + i], 1, n) * o.iprcn[(size_t)tind * NV + n];
+        for (int i = 0; i < 4; ++i) {
+            const int f = o.tt[4 * tind + i], sg = -o.trot[4 * tind + i];
+            for (int j = 0; j < 6; ++j) {
+                double msgn = 1.0;
+                int ind = 0;
+                for (int m = 1; m <= em - 1; ++m) {
+                    for (int k = 1; k <= em - m; ++k, ++ind)
+                        for (int n = 0; n < NV; ++n)
+                            F(f, ind, n) -= msgn * t.mm[4 + 6 * em + i * fm + ind][5 + j * em] * uh[j][n];
+                    msgn *= sg;
+                }
+            }
+        }
+    }
+    for (int f = 0; f < o.ntri; ++f)
+        for (int k = 0; k < fm; ++k)
+            for (int n = 0; n < NV; ++n) F(f, k, n) *= (1.0 / o.fprcn[(size_t)f * NV + n]) * 3000.0;
+    fdirichlet(o);
+}
+
+// The face vertices and edges minvrt at p = 3 uses, [ntri][3] each (face_topology).
+void ot_face_topology(void *h, int *fp, int *fs) {
+    const OT &o = *static_cast<const OT *>(h);
+    std::vector<int> a, b;
+    face_topology(o, a, b);
+    std::memcpy(fp, a.data(), a.size() * 4);
+    std::memcpy(fs, b.data(), b.size() * 4);
+}
+
+// 0: the JACOBI build's smoother, 1: minvrt (p = 1, 2 and 3; -1 otherwise)
 int ot_set_smoother(void *h, int kind) {
     OT &o = *static_cast<OT *>(h);
-    if (kind != 0 && (kind != 1 || o.t.p > 2)) return -1;
+    if (kind != 0 && (kind != 1 || o.t.p > 3)) return -1;
     o.smoother = kind;
     return 0;
 }
@@ -603,12 +897,22 @@ void ot_rsdl(void *h, int stage);
 void ot_update(void *h) {
     OT &o = *static_cast<OT *>(h);
     o.u0v = o.ugv; o.u0e = o.uge; o.u0f = o.ugf; o.u0i = o.ugi;
+    // p = 3: the spoke factors of tet_hp::setup_preconditioner, from the iprcn of the last
+    // ot_setup_preconditioner (the same for every stage)
+    Spokes S;
+    std::vector<int> sp, fp, fs;
+    if (o.smoother && o.t.p == 3) {
+        sp = seg_ends(o);
+        face_topology(o, fp, fs);
+        spoke(o, sp, S);
+    }
     for (int stage = 0; stage < o.ph.nstage; ++stage) {
         ot_rsdl(h, stage);
         all_dirichlet(o);
         if (o.smoother) {
             if (o.t.p == 1) minvrt_p1(o);
-            else minvrt_p2(o);
+            else if (o.t.p == 2) minvrt_p2(o);
+            else minvrt_p3(o, S, sp, fp, fs);
         } else {
             jacobi_relaxation(o);
         }

@@ -76,6 +76,7 @@ def lib():
         o.ot_update.argtypes = [P]
         o.ot_set_flux_faces.argtypes = [P, I, P, P, P, P, P, P]
         o.ot_set_smoother.argtypes = [P, I]
+        o.ot_face_topology.argtypes = [P, P, P]
         _o = o
     return _o
 
@@ -298,7 +299,15 @@ class OracleTet:
 
     def set_smoother(self, kind):
         if lib().ot_set_smoother(self.h, kind) != 0:
-            raise ValueError("minvrt is restated for p = 1 and 2 only")
+            raise ValueError("minvrt is restated for p = 1, 2 and 3 only")
+
+    def face_topology(self):
+        """(face vertices, face edges) [ntri][3] that minvrt's face steps use at p = 3."""
+        m = self.prob.mesh
+        fp = np.zeros((m.ntri, 3), np.int32)
+        fs = np.zeros((m.ntri, 3), np.int32)
+        lib().ot_face_topology(self.h, _p(fp), _p(fs))
+        return fp, fs
 
     def jacobian_diagonal(self):
         lib().ot_jacobian_diagonal(self.h)

@@ -142,11 +142,13 @@ def test_tet_multigrid_reduces_residual_and_keeps_essential_values():
     H.close()
 
 
-@pytest.mark.parametrize("p,cfl", [(1, 2.2), (2, 1.5)])
+@pytest.mark.parametrize("p,cfl", [(1, 2.2), (2, 1.5), (3, 1.0)])
 def test_tet_minvrt_updates_match_oracle(p, cfl):
     """tet_hp::update with tet_hp::minvrt (p = 1: res.v *= vdiag / vprcn; p = 2: also the
-    edge / vertex removals and the edge scaling), face fluxes and essential rows, at the
-    reference's default cfl for that p."""
+    edge / vertex removals and the edge scaling; p = 3: also the face removals, the
+    vertex-ball solves of the edges' first modes with the spoke factors, and the second edge
+    modes and the faces), face fluxes and essential rows, at the reference's default cfl for
+    that p."""
     pr = TetProblem(cube_tets(3), p, mu=0.01, cfl=cfl).set_beltrami()
     masks, ff = pr.cube_boundary()
     g, o = TetGPU(pr), OracleTet(pr)
@@ -162,11 +164,35 @@ def test_tet_minvrt_updates_match_oracle(p, cfl):
     g.close()
 
 
-def test_tet_set_smoother_minvrt_needs_p_at_most_2():
-    pr = TetProblem(cube_tets(2), 3, mu=0.01).set_beltrami()
+def test_tet_set_smoother_minvrt_needs_p_at_most_3():
+    pr = TetProblem(cube_tets(2), 4, mu=0.01).set_beltrami()
     g = TetGPU(pr)
-    with pytest.raises(RuntimeError, match="p = 1 and 2"):
+    with pytest.raises(RuntimeError, match="p = 1, 2 and 3"):
         g.set_smoother(1)
+    g.close()
+
+
+def test_tet_minvrt_p3_fixed_rows_stay_and_the_spokes_factor():
+    """minvrt at p = 3 keeps every row fixed by an essential condition at its value, and
+    the preconditioner set-up reports no bad spoke factor."""
+    pr = TetProblem(cube_tets(3), 3, mu=0.01, cfl=1.0).set_beltrami()
+    masks, ff = pr.cube_boundary()
+    g = TetGPU(pr)
+    g.set_dirichlet(masks)
+    g.set_flux_faces(ff)
+    g.set_smoother(1)
+    assert g.setup_preconditioner() == 0
+    u0 = [a.copy() for a in g.state()]
+    for _ in range(2):
+        g.update()
+    u = g.state()
+    mv, me, mf = (np.asarray(a, dtype=bool) for a in masks)
+    assert np.array_equal(u[0][mv], u0[0][mv])
+    assert np.array_equal(u[1][np.broadcast_to(me[:, None, :], u[1].shape)],
+                          u0[1][np.broadcast_to(me[:, None, :], u0[1].shape)])
+    assert np.array_equal(u[2][np.broadcast_to(mf[:, None, :], u[2].shape)],
+                          u0[2][np.broadcast_to(mf[:, None, :], u0[2].shape)])
+    assert all(np.all(np.isfinite(a)) for a in u)
     g.close()
 
 
@@ -180,10 +206,11 @@ def test_tet_multigrid_with_minvrt_on_low_p_levels_reduces_residual():
 
 @pytest.mark.parametrize("p", [2, 3])
 def test_tet_rsdl_and_minvrt_on_a_scrambled_mesh_match_oracle(p):
-    """Residual with face fluxes (and, at p = 2, minvrt updates) on a cube whose interior
-    vertices are jittered and whose vertices are renumbered at random."""
+    """Residual with face fluxes and minvrt updates on a cube whose interior vertices are
+    jittered and whose vertices are renumbered at random (every local orientation of the
+    faces and edges that minvrt's face steps and vertex balls meet)."""
     from test_tet_face_flux import scrambled_cube
-    pr = TetProblem(scrambled_cube(3, 11), p, mu=0.01, cfl=1.5 if p == 2 else 0.5).set_beltrami()
+    pr = TetProblem(scrambled_cube(3, 11), p, mu=0.01, cfl=1.5 if p == 2 else 1.0).set_beltrami()
     masks, ff = pr.cube_boundary(outflow=True)
     g, o = TetGPU(pr), OracleTet(pr)
     for x in (g, o):
@@ -194,9 +221,10 @@ def test_tet_rsdl_and_minvrt_on_a_scrambled_mesh_match_oracle(p):
         g.rsdl(stage)
         o.rsdl(stage)
         assert relerr(g.residual(), o.residual()) < 1e-12
-    if p == 2:
+    if p in (2, 3):
         for x in (g, o):
             x.set_smoother(1)
+            assert x.setup_preconditioner() == 0
         for _ in range(3):
             g.update()
             o.update()

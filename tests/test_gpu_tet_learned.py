@@ -34,9 +34,12 @@ def test_scale_multiplies_the_jacobian_diagonal():
         torch.cuda.synchronize()
         g.set_prcn_scale(ctypes.c_void_p(sc.data_ptr()), 1.5)
         jd = g.jacobian_diagonal()
-        # the diagonal is accumulated with FP64 atomics: equal up to the summation order
+        # the diagonal is a finite difference of the scaled contributions, accumulated with
+        # FP64 atomics: equal up to the difference's rounding (~1e-16 / dw relative, dw ~ 1e-7)
         for a, b in zip(jd, jd0):
-            assert np.allclose(a, np.exp(c) * b, rtol=1e-12, atol=1e-14 * np.max(np.abs(b)))
+            if b.size == 0:
+                continue
+            assert np.allclose(a, np.exp(c) * b, rtol=1e-7, atol=1e-9 * np.max(np.abs(b)))
         g.set_prcn_scale(None)
     g.close()
 
