@@ -346,7 +346,7 @@ def tet_flops_per_element(p, beta_positive=True):
     return 2 * (proj + intg)
 
 
-def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=None, p1_minvrt=False):
+def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=None, p1_minvrt=False, cfl3=None):
     """3D tet_hp ins: the unit cube split into n^3 hexahedra x 6 tetrahedra (n = 64:
     1,572,864 tetrahedra), p = 3, Re 100, the Ethier-Steinman Beltrami state at the
     vertices plus 1e-3 seeded noise on every coefficient. Times tet_hp::rsdl(nstage)
@@ -432,7 +432,7 @@ def c5_sweep(torch, dev, n, p, steps, warmup, timed, full_solve=False, hlevels=N
         # p1_minvrt: the p = 1 and 2 levels smoothed by the default build's tet_hp::minvrt at
         # the reference's cfl (2.2, 1.5) instead of the JACOBI build's relaxation; "all": every
         # level, the p = 3 level at its own cfl (1.0)
-        cflw = {**cfl, **({1: 2.2, 2: 1.5} if p1_minvrt else {}), **({3: 1.0} if p1_minvrt == "all" else {})}
+        cflw = {**cfl, **({1: 2.2, 2: 1.5} if p1_minvrt else {}), **({3: cfl3 or 1.0} if p1_minvrt == "all" else {})}
         arms = {}
         states = {}
         # the learned correction of the finest level's smoother, trained on the GPU on the
@@ -720,7 +720,7 @@ def kernel_sweep(hpb, dev, n, ps, steps, timed, stream):
         fl_el, src = ins_flops_per_element(p)
         line = {"sweep": "kernels", "p": p, "ntri": pr.mesh.ntri, "ndof": pr.ndof, "flops_per_element": fl_el,
                 "fp64_tensor_peak_tflops": peak.value}
-        for kind in ("tensor", "scalar"):
+        for kind in ("tensor", "scalar") + (("point",) if p == 1 else ()):
             g.element_kernel(kind)
             el = lambda: check(lib.hp_gpu_enqueue_element_rsdl(g.h, ns), "element_rsdl")
             rs = lambda: check(lib.hp_gpu_enqueue_rsdl(g.h, ns), "rsdl")
@@ -732,6 +732,8 @@ def kernel_sweep(hpb, dev, n, ps, steps, timed, stream):
             line[kind] = {"kernel_ms": k_ms, "rsdl_ms": r_ms, "rsdl_gdofs": pr.ndof / (r_ms * 1e-3) / 1e9,
                           "tflops": tf, "frac_of_fp64_tensor_peak": tf / peak.value}
         line["speedup_tensor_vs_scalar"] = line["scalar"]["kernel_ms"] / line["tensor"]["kernel_ms"]
+        if "point" in line:
+            line["speedup_point_vs_scalar"] = line["scalar"]["kernel_ms"] / line["point"]["kernel_ms"]
         g.close()
         print(json.dumps(line), flush=True)
 
@@ -932,6 +934,8 @@ def main():
                     help="with --sweep c5 --tet-solve: smooth the p = 1, 2 levels with tet_hp::minvrt (cfl 2.2, 1.5)")
     ap.add_argument("--tet-minvrt-all", action="store_true",
                     help="with --sweep c5 --tet-solve: smooth every level with tet_hp::minvrt (cfl 2.2, 1.5, 1.0)")
+    ap.add_argument("--tet-cfl3", type=float, default=None,
+                    help="with --tet-minvrt-all: the cfl of the p = 3 level (default 1.0, the reference's)")
     ap.add_argument("--tet-hlevels", type=int, default=None,
                     help="with --sweep c5 --tet-solve: h-levels of the W-cycle hierarchy (default: down to 2^3 "
                          "for n <= 32, to 8^3 above)")
@@ -1007,7 +1011,7 @@ def main():
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
         c5_sweep(torch, dev, args.mesh if args.mesh != N_MESH else 64, (args.p or [3])[0], args.steps, args.warmup,
                  timed_factory(torch, flush), full_solve=args.tet_solve, hlevels=args.tet_hlevels,
-                 p1_minvrt="all" if args.tet_minvrt_all else args.tet_minvrt)
+                 p1_minvrt="all" if args.tet_minvrt_all else args.tet_minvrt, cfl3=args.tet_cfl3)
         return
 
     if args.physics == "ins":

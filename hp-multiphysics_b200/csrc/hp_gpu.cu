@@ -18,6 +18,7 @@
 #include "hp_mlp.h"
 #include "hp_kernels.cuh"
 #include "hp_elem_mma.cuh"
+#include "hp_elem_p1.cuh"
 #include "hp_elem_tf32.cuh"
 
 using namespace hpb;
@@ -171,6 +172,31 @@ void build_ins_mma(const hp_basis_tables &b, std::vector<double> &ops, InsMmaSma
     }
 }
 
+// The dense operators of the p = 1 point kernel (k_rsdl_ins_p1), the same entries as
+// build_ins_mma's at G = 2, T = 3, indexed by point q = 2 i + j.
+template <typename R>
+void build_ins_p1(const hp_basis_tables &b, InsP1Ops<R> &o) {
+    constexpr int G = 2;
+    for (int q = 0; q < 4; ++q)
+        for (int m = 0; m < 3; ++m) {
+            const int i = q / G, j = q - i * G, c = ModeCols<1>::col(m);
+            const double dr = b.n0[j] * b.gn[j][m] * b.dgx[i][c];
+            o.V[q][m] = (R)(b.gn[j][m] * b.gx[i][c]);
+            o.DR[q][m] = (R)dr;
+            o.DS[q][m] = (R)(b.dgn[j][m] * b.gx[i][c] + b.x0[i] * dr);
+            o.WR[q][m] = (R)(-b.dgxwtx[c][i] * b.gnwtnn0[m][j]);
+            o.WS[q][m] = (R)(-(b.x0[i] * b.dgxwtx[c][i] * b.gnwtnn0[m][j] + b.gxwtx[c][i] * b.dgnwtn[m][j]));
+        }
+    for (int r = 0; r < G; ++r) {
+        for (int k = 0; k < G; ++k) {
+            o.AR[r][k] = (R)deriv_op(b, G, 0, r, k);
+            o.AS1[r][k] = (R)deriv_op(b, G, 1, r, k);
+            o.AS2[r][k] = (R)deriv_op(b, G, 2, r, k);
+        }
+        o.N0[r] = (R)b.n0[r];
+    }
+}
+
 // TF32 rounding of an operator entry (round to nearest, ties away from zero, as
 // cvt.rna.tf32.f32 does for the A operands)
 float to_tf32(double v) {
@@ -307,6 +333,11 @@ struct Launchers {
     // FP32 ins: the base state's point values for the correction form (State::bpt)
     void (*base_pts)(const void *tab, const Mesh &, const State<R> &, R *bpt, cudaStream_t);
     int bpt_per_elem;  // 2 GG
+    // ins at p = 1: the point kernel (k_rsdl_ins_p1, four lanes per triangle) with its
+    // operators (point_build: InsP1Ops<R>), curved triangles through the scalar kernel
+    void (*elem_point)(const void *ops, const void *tab, const Mesh &, const State<R> &, const Phys &, int stage,
+                       int zero_rr, int diff, int nsm, const Tune &, cudaStream_t);
+    void (*point_build)(const hp_basis_tables &, std::vector<unsigned char> &ops);
     // tri_hp::l2error on the device (FP64): per-block partials into part
     void (*l2err)(const void *tab, const double *wtn, const Mesh &, const State<R> &, int NV, const DevField &,
                   double *part, int blocks, cudaStream_t);
@@ -464,6 +495,29 @@ struct LaunchImpl {
             }
         }
     }
+    static constexpr bool HAS_POINT = PHYS == 1 && P == 1;
+    static void elem_point(const void *ops, const void *tab, const Mesh &m, const State<R> &s, const Phys &ph,
+                           int stage, int zero_rr, int diff, int nsm, const Tune &tn, cudaStream_t st) {
+        if constexpr (HAS_POINT) {
+            const long tri_per_cta = 256 / 4;
+            const int blocks = (int)std::min<long>(((long)m.ntri + tri_per_cta - 1) / tri_per_cta, (long)nsm * 8);
+            k_rsdl_ins_p1<R><<<blocks, 256, 0, st>>>(static_cast<const InsP1Ops<R> *>(ops), m, s, ph, stage, zero_rr,
+                                                     diff);
+            if (m.ncurved > 0) {
+                constexpr int EPC = C::WPC * C::EPW;
+                const int cap = nsm * tn.elem_cap;
+                k_rsdl_elem<R, P, PHYS, true><<<std::min(nblk(m.ncurved, EPC), cap), C::WPC * 32, smem(), st>>>(
+                    reinterpret_cast<const DevTables<R, P> *>(tab), m, s, ph, stage, zero_rr, diff, ElemMat<R>{},
+                    ElemJac<R>{});
+            }
+        }
+    }
+    static void point_build(const hp_basis_tables &b, std::vector<unsigned char> &ops) {
+        InsP1Ops<R> o;
+        build_ins_p1<R>(b, o);
+        ops.resize(sizeof(o));
+        std::memcpy(ops.data(), &o, sizeof(o));
+    }
     static void mma_build(const hp_basis_tables &b, std::vector<unsigned char> &ops, std::vector<unsigned char> &small) {
         if constexpr (DBL) {
             InsMmaSmall<P> sm;
@@ -526,6 +580,8 @@ struct LaunchImpl {
         L.emat_apply = &emat_apply;
         L.elem_jac = &elem_jac;
         L.elem_mma = HAS_MMA ? &elem_mma : nullptr;
+        L.elem_point = HAS_POINT ? &elem_point : nullptr;
+        L.point_build = HAS_POINT ? &point_build : nullptr;
         L.mma_build = HAS_MMA ? &mma_build : nullptr;
         L.base_pts = (HAS_MMA && !DBL) ? &base_pts : nullptr;
         L.bpt_per_elem = 2 * (P + 1) * (P + 1);
@@ -620,6 +676,7 @@ struct hp_gpu_ctx {
     // FP64 element kernel: HP_ELEM_TENSOR (ins: k_rsdl_ins_mma) or HP_ELEM_SCALAR (k_rsdl_elem)
     int elem_kind = 0;
     void *d_mma = nullptr, *d_mma32 = nullptr;            // dense operators in fragment order (FP64, TF32)
+    void *d_p1 = nullptr, *d_p1_32 = nullptr;             // operators of the p = 1 point kernel (FP64, FP32)
     std::vector<unsigned char> mma_small, mma_small32;  // derivative tables (kernel parameters)
     float *d_bpt32 = nullptr;                           // FP32 base point values (correction form)
     double wtn[HP_MXGP] = {0};                // Gauss-Jacobi weights (l2error)
@@ -904,8 +961,16 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
         if ((r = upload(c, (unsigned char **)&c->d_mma32, ops32.data(), ops32.size()))) return fail(r);
         // at p = 1 and 2 the scalar kernel's lane groups (4 and 2 triangles per warp) are
         // faster than two triangles per tensor-core warp (measured: 0.080 vs 0.153 ms and
-        // 0.205 vs 0.205 ms for 131k triangles)
+        // 0.205 vs 0.205 ms for 131k triangles); at p = 1 the point kernel is faster still
         c->elem_kind = c->p >= 3 ? HP_ELEM_TENSOR : HP_ELEM_SCALAR;
+    }
+    if (c->L.point_build && c->L32.point_build) {
+        std::vector<unsigned char> ops, ops32;
+        c->L.point_build(*b, ops);
+        c->L32.point_build(*b, ops32);
+        if ((r = upload(c, (unsigned char **)&c->d_p1, ops.data(), ops.size()))) return fail(r);
+        if ((r = upload(c, (unsigned char **)&c->d_p1_32, ops32.data(), ops32.size()))) return fail(r);
+        c->elem_kind = HP_ELEM_POINT;
     }
     DevMinv<double> hm;
     fill_minv<double>(*b, hm);
@@ -1041,6 +1106,9 @@ static void launch_elem(hp_gpu_ctx *c, const Launchers<R> &L, const void *tab, c
         L.elem_mma(std::is_same<R, double>::value ? c->d_mma : c->d_mma32,
                    std::is_same<R, double>::value ? c->mma_small.data() : c->mma_small32.data(), tab, c->mesh, st, ph,
                    stage, zero_rr, diff, c->nsm, tune_of(c, R()), c->stream);
+    else if (c->elem_kind == HP_ELEM_POINT && L.elem_point)
+        L.elem_point(std::is_same<R, double>::value ? c->d_p1 : c->d_p1_32, tab, c->mesh, st, ph, stage, zero_rr, diff,
+                     c->nsm, tune_of(c, R()), c->stream);
     else
         L.elem(tab, c->mesh, st, ph, stage, zero_rr, diff, c->nsm, tune_of(c, R()), c->stream);
 }
@@ -1224,9 +1292,13 @@ extern "C" int hp_gpu_l2error(hp_gpu_ctx *c, const hp_field *fld, double *l2, do
 }
 
 extern "C" int hp_gpu_set_element_kernel(hp_gpu_ctx *c, int kind) {
-    if (!c || (kind != HP_ELEM_SCALAR && kind != HP_ELEM_TENSOR)) return HP_EINVAL;
+    if (!c || (kind != HP_ELEM_SCALAR && kind != HP_ELEM_TENSOR && kind != HP_ELEM_POINT)) return HP_EINVAL;
     if (kind == HP_ELEM_TENSOR && !c->d_mma) {
         set_err("the tensor-core element kernel is built for ins only");
+        return HP_ENOTSUP;
+    }
+    if (kind == HP_ELEM_POINT && !c->d_p1) {
+        set_err("the point element kernel is built for ins at p = 1 only");
         return HP_ENOTSUP;
     }
     if (c->elem_kind != kind) {  // captured updates hold the old kernel

@@ -269,8 +269,10 @@ class GPULevel:
         return K
 
     def element_kernel(self, kind):
-        """FP64 element kernel: "tensor" (ins default) or "scalar" (hp_gpu_set_element_kernel)."""
-        L.check(self.lib.hp_gpu_set_element_kernel(self.h, {"scalar": 0, "tensor": 1}[kind]), "set_element_kernel")
+        """Element kernel (hp_gpu_set_element_kernel): "tensor" (ins default at p >= 3),
+        "point" (ins default at p = 1) or "scalar"."""
+        L.check(self.lib.hp_gpu_set_element_kernel(self.h, {"scalar": 0, "tensor": 1, "point": 2}[kind]),
+                "set_element_kernel")
 
     def element_matrices(self, on=True):
         """cd only: rsdl from stored element operators (hp_gpu_set_element_matrices)."""

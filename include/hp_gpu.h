@@ -196,16 +196,18 @@ int hp_gpu_maxres(hp_gpu_ctx *ctx, double *out, double *mx);
  * returns sqrt(sum res^2) and max |res| over every v/s/i coefficient. */
 int hp_gpu_resnorm(hp_gpu_ctx *ctx, double *l2, double *linf);
 
-/* FP64 element kernel of rsdl (no counterpart in the reference, which has one CPU
- * loop, tri_hp/nstage.cpp:52-73). HP_ELEM_TENSOR (the default for ins at p >= 3):
- * projection, intgrtrs and the strong residual of two triangles per warp on the FP64
- * tensor cores (mma.m8n8k4.f64) with dense per-point operators, and for the FP32
- * smoother's correction form four triangles per warp on TF32 (mma.m16n8k8);
- * HP_ELEM_SCALAR (the default at p <= 2, and cd always): the sum-factorised warp kernel.
- * Both give the reference's residual up to rounding. HP_ENOTSUP when the tensor-core
- * kernel is not built for the context's physics. */
+/* Element kernel of rsdl (no counterpart in the reference, which has one CPU loop,
+ * tri_hp/nstage.cpp:52-73). HP_ELEM_TENSOR (the default for ins at p >= 3): projection,
+ * intgrtrs and the strong residual of two triangles per warp on the FP64 tensor cores
+ * (mma.m8n8k4.f64) with dense per-point operators, and for the FP32 smoother's
+ * correction form four triangles per warp on TF32 (mma.m16n8k8); HP_ELEM_POINT (the
+ * default for ins at p = 1): four lanes per triangle, one per Gauss point, the point
+ * shares of intgrtrs summed by shuffles; HP_ELEM_SCALAR (the default at p = 2, and cd
+ * always): the sum-factorised warp kernel. All give the reference's residual up to
+ * rounding. HP_ENOTSUP when the kernel is not built for the context's physics and p. */
 #define HP_ELEM_SCALAR 0
 #define HP_ELEM_TENSOR 1
+#define HP_ELEM_POINT 2
 int hp_gpu_set_element_kernel(hp_gpu_ctx *ctx, int kind);
 
 /* Stream-ordered forms without a host synchronisation (for callers that time or

@@ -45,7 +45,7 @@ def test_device_l2error_integrates_curved_elements_exactly():
     g.close()
 
 
-@pytest.mark.parametrize("kind,p", [("ins", 4), ("cd", 4)])
+@pytest.mark.parametrize("kind,p", [("ins", 4), ("ins", 1), ("cd", 4)])
 def test_rsdl_fp32_precision_matches_fp64_to_single_precision(kind, p):
     pr = hpb.kovasznay_ins(n=8, p=p) if kind == "ins" else hpb.cd_sinsin(n=8, p=p, kcond=1e-2)
     g = pr.gpu()

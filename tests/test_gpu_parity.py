@@ -81,13 +81,12 @@ def staircase_mesh(n):
     return hpb.Mesh(np.array(pts, dtype=float) / n, np.array(tri, dtype=np.int32))
 
 
-@pytest.mark.parametrize("p", [1, 2, 3, 4, 5, 6, 7, 8])
-@pytest.mark.parametrize("elem", ["tensor", "scalar"])
+@pytest.mark.parametrize("p,elem", [(p, e) for p in range(1, 9) for e in ("tensor", "scalar")] + [(1, "point")])
 def test_ins_element_kernels_match_oracle(p, elem):
-    """Both FP64 ins element kernels (tensor-core DMMA and scalar warp kernel) against the
-    oracle: rsdl at every stage kind (beta = 1, beta = 0, beta in (0, 1)), on a mesh with
-    an odd triangle count (the last warp's second triangle is missing) and on a Delaunay
-    mesh (irregular orientations)."""
+    """The FP64 ins element kernels (tensor-core DMMA, scalar warp kernel, and at p = 1 the
+    point kernel) against the oracle: rsdl at every stage kind (beta = 1, beta = 0, beta in
+    (0, 1)), on a mesh with an odd triangle count (the last warp's last triangles are
+    missing) and on a Delaunay mesh (irregular orientations)."""
     import ctypes
     from hpb import _lib as L
     for mesh in (staircase_mesh(5), hpb.delaunay_square(7, seed=11)):
