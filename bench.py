@@ -738,7 +738,7 @@ def kernel_sweep(hpb, dev, n, ps, steps, timed, stream):
         print(json.dumps(line), flush=True)
 
 
-def c3_time_to_tol(hpb, dev, stream, max_cycles=150):
+def c3_time_to_tol(hpb, dev, stream, max_cycles=150, snapshots=(0,)):
     """C3 W-cycles (vwcycle 2, 2 + 2 updates per level, preconditioners every cycle) from
     the initial state to a 1e-10 drop of the FP64 residual: plain FP64, FP32 smoothing
     inside FP64 defect correction, and that plus the learned correction of the Jacobi
@@ -752,14 +752,15 @@ def c3_time_to_tol(hpb, dev, stream, max_cycles=150):
     train_re = [float(x) for x in rng.uniform(100.0, 1000.0, 4)]
     F, T = [], []
     for k, re in enumerate(train_re):
-        f, tg = LR.solver_samples(lambda: hpb.lid_cavity_ins(n=64, p=C3_P, re=re, seed=500 + k))
+        f, tg = LR.solver_samples(lambda: hpb.lid_cavity_ins(n=64, p=C3_P, re=re, seed=500 + k), snapshots=snapshots)
         F.append(f)
         T.append(tg)
     net, lh = LR.train(np.concatenate(F), np.concatenate(T), steps=400)
     out = {"drop": 1e-10, "criterion": "||R64||_2 / ||R64(u0)||_2 over all non-Dirichlet v/s/i rows",
            "cycle": "W (vwcycle 2), 2+2 multistage updates per level, preconditioners every cycle",
            "network": {"widths": "17-64-64-64-1", "dtype": "BF16 weights, FP32 accumulation",
-                       "training_re": train_re, "samples": int(sum(len(t) for t in T)),
+                       "training_re": train_re, "samples": int(sum(len(t) for t in T)), "snapshots": list(snapshots),
+                       "nonzero_targets": float(np.mean(np.concatenate(T) != 0)),
                        "training_seconds": time.perf_counter() - t0}}
     states = {}
     for name, mixed, learned in (("fp64", False, False), ("fp32_defect_correction", True, False),
@@ -843,7 +844,7 @@ def c3_headline(args, torch, dist, rank, world, dev, stream):
     ndof = pr.ndof
     H.close()
     value, e2e, t_ms, e2e_s = replica_totals(dist, world, ndof, args.steps, t_ms, e2e_s, "cuda")
-    tol = c3_time_to_tol(hpb, dev, stream) if (world == 1 and not args.no_tol) else None
+    tol = c3_time_to_tol(hpb, dev, stream, snapshots=tuple(args.c3_snapshots)) if (world == 1 and not args.no_tol) else None
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -934,6 +935,8 @@ def main():
                     help="with --sweep c5 --tet-solve: smooth the p = 1, 2 levels with tet_hp::minvrt (cfl 2.2, 1.5)")
     ap.add_argument("--tet-minvrt-all", action="store_true",
                     help="with --sweep c5 --tet-solve: smooth every level with tet_hp::minvrt (cfl 2.2, 1.5, 1.0)")
+    ap.add_argument("--c3-snapshots", type=int, nargs="*", default=[0],
+                    help="plain-update counts of the states the C3 network's training samples come from")
     ap.add_argument("--tet-cfl3", type=float, default=None,
                     help="with --tet-minvrt-all: the cfl of the p = 3 level (default 1.0, the reference's)")
     ap.add_argument("--tet-hlevels", type=int, default=None,
