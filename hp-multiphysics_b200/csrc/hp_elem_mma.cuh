@@ -94,6 +94,26 @@ __device__ __forceinline__ void warp_gemm(const double *__restrict__ arow, const
     }
 }
 
+// The imaginary and the real intgrtrs of the same rows at once: Ca = A_a B, Cb = A_b B with
+// each B fragment loaded once for both (the real part's B is the imaginary part's).
+template <int KS, int NTL>
+__device__ __forceinline__ void warp_gemm2(const double *__restrict__ arow_a, const double *__restrict__ arow_b,
+                                           const double *__restrict__ B, int gcol, int lane, double (&ca)[NTL][2],
+                                           double (&cb)[NTL][2]) {
+#pragma unroll
+    for (int nt = 0; nt < NTL; ++nt) ca[nt][0] = ca[nt][1] = cb[nt][0] = cb[nt][1] = 0.0;
+#pragma unroll 4
+    for (int ks = 0; ks < KS; ++ks) {
+        const double a = arow_a[ks * 4 + gcol], b = arow_b[ks * 4 + gcol];
+#pragma unroll
+        for (int nt = 0; nt < NTL; ++nt) {
+            const double bf = __ldg(B + ((size_t)nt * KS + ks) * 32 + lane);
+            dmma884(ca[nt][0], ca[nt][1], a, bf);
+            dmma884(cb[nt][0], cb[nt][1], b, bf);
+        }
+    }
+}
+
 template <int P>
 __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
     k_rsdl_ins_mma(const double *__restrict__ projB, const double *__restrict__ intB,
@@ -317,13 +337,13 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                 }
         };
         // ---- imaginary part: intgrtrs (intgrt.cpp:81-158, weak divergence with its minus
-        //      sign in the operator) on the tensor cores -> res
-        {
+        //      sign in the operator) on the tensor cores -> res; with a real part (beta > 0)
+        //      it is done together with that one below, sharing the operator loads
+        if (beta == 0.0) {
             double c[M::NT2][2];
             warp_gemm<M::KS2, M::NT2>(FI(re_) + (rv < 3 ? rv : 2) * VS, intB, gcol, lane, c);
             scatter(c, 0);
-        }
-        if (beta > 0.0) {
+        } else {
             // ---- strong residual at the points (derivr + derivs of the full fluxes FI + FX,
             //      proj.cpp:339-402) on the tensor cores as tensor products of the 1D
             //      operators: res(i, j) = n0(j) (Ar fr + As1 fs)(i, j) + (As2 fs^T)(j, i), the
@@ -424,9 +444,12 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                 fx[2 * VS + GG + q] = -(-d10 * tr0 + d00 * tr1);
             }
             __syncwarp();
-            // ---- real part: intgrtrs of the viscous + SUPG fluxes, x beta -> res_r
-            double c[M::NT2][2];
-            warp_gemm<M::KS2, M::NT2>(FX(re_) + (rv < 3 ? rv : 2) * VS, intB, gcol, lane, c);
+            // ---- both parts: intgrtrs of the imaginary pairs -> res, and of the viscous + SUPG
+            //      pairs, x beta -> res_r
+            double ci[M::NT2][2], c[M::NT2][2];
+            warp_gemm2<M::KS2, M::NT2>(FI(re_) + (rv < 3 ? rv : 2) * VS, FX(re_) + (rv < 3 ? rv : 2) * VS, intB, gcol,
+                                       lane, ci, c);
+            scatter(ci, 0);
             scatter(c, 1);
         }
         __syncwarp();

@@ -121,6 +121,29 @@ __device__ __forceinline__ void warp_gemm_tf32(const float *ra0, const float *ra
     }
 }
 
+// Two products with the same B fragments: Ca from rows (ra0, ra1), Cb from rows (rb0, rb1),
+// each B fragment loaded once (the imaginary and the real intgrtrs of the same triangles).
+template <int KS, int NTL>
+__device__ __forceinline__ void warp_gemm2_tf32(const float *ra0, const float *ra1, const float *rb0, const float *rb1,
+                                                const float2 *__restrict__ B, int tig, int lane, float (&ca)[NTL][4],
+                                                float (&cb)[NTL][4]) {
+#pragma unroll
+    for (int nt = 0; nt < NTL; ++nt)
+        ca[nt][0] = ca[nt][1] = ca[nt][2] = ca[nt][3] = cb[nt][0] = cb[nt][1] = cb[nt][2] = cb[nt][3] = 0.f;
+#pragma unroll 2
+    for (int ks = 0; ks < KS; ++ks) {
+        const int k = ks * 8 + tig;
+        const unsigned a0 = f2tf32(ra0[k]), a1 = f2tf32(ra1[k]), a2 = f2tf32(ra0[k + 4]), a3 = f2tf32(ra1[k + 4]);
+        const unsigned b0 = f2tf32(rb0[k]), b1 = f2tf32(rb1[k]), b2 = f2tf32(rb0[k + 4]), b3 = f2tf32(rb1[k + 4]);
+#pragma unroll
+        for (int nt = 0; nt < NTL; ++nt) {
+            const float2 bf = __ldg(B + ((size_t)nt * KS + ks) * 32 + lane);
+            mma_tf32(ca[nt], a0, a1, a2, a3, bf);
+            mma_tf32(cb[nt], b0, b1, b2, b3, bf);
+        }
+    }
+}
+
 template <int P>
 __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
     k_rsdl_ins_tf32(const float2 *__restrict__ projB, const float2 *__restrict__ intB,
@@ -358,13 +381,14 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                     }
             }
         };
-        {
+        // imaginary part -> res; with a real part (beta > 0) it is done together with that one
+        // below, sharing the operator loads
+        if (beta == 0.f) {
             float c[M::NT2][4];
             warp_gemm_tf32<M::KS2, M::NT2>(FI(ra) + rvv * VS, FI(ra + 2) + rvv * VS, nullptr, nullptr, intB, tig,
                                             lane, c);
             scatter(c, 0);
-        }
-        if (beta > 0.f) {
+        } else {
             // ---- strong residual of FI + FX at the points (derivr / derivs, proj.cpp:339-402)
             //      on TF32 as tensor products of the 1D operators: part 1 rows i, columns
             //      (triangle, variable, j): n0(j) (Ar fr + As1 fs); part 2 rows j, columns
@@ -454,9 +478,10 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                 fr[2 * VS + GG + q] = -(-d10 * tr0 + d00 * tr1);
             }
             __syncwarp();
-            float c[M::NT2][4];
-            warp_gemm_tf32<M::KS2, M::NT2>(FX(ra) + rvv * VS, FX(ra + 2) + rvv * VS, nullptr, nullptr, intB, tig,
-                                            lane, c);
+            float ci[M::NT2][4], c[M::NT2][4];
+            warp_gemm2_tf32<M::KS2, M::NT2>(FI(ra) + rvv * VS, FI(ra + 2) + rvv * VS, FX(ra) + rvv * VS,
+                                             FX(ra + 2) + rvv * VS, intB, tig, lane, ci, c);
+            scatter(ci, 0);
             scatter(c, 1);
         }
         __syncwarp();
