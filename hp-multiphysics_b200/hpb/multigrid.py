@@ -60,9 +60,10 @@ def barycentric(pnts, tri_pnt, tris, pts):
     return np.stack([1.0 - w1 - w2, w1, w2], axis=1)
 
 
-def locate(mesh, pts):
+def locate(mesh, pts, strict=True):
     """Containing triangle of each point (tri_mesh::findtri) and its barycentric
-    weights (getwgts). Uses a uniform bucket grid over the triangles."""
+    weights (getwgts). Uses a uniform bucket grid over the triangles. strict=False:
+    points outside the mesh get triangle -1 and NaN weights instead of an error."""
     pts = np.asarray(pts, dtype=np.float64)
     P_ = mesh.pnts
     T = mesh.tri_pnt
@@ -106,7 +107,11 @@ def locate(mesh, pts):
         best_m[qq] = m[better]
         best_t[qq] = t[better]
         best_w[qq] = w[better]
-    if np.any(best_t < 0) or np.any(best_m < -1e-6):
+    if not strict:
+        out = (best_t < 0) | (best_m < -1e-6)
+        best_t[out] = -1
+        best_w[out] = np.nan
+    elif np.any(best_t < 0) or np.any(best_m < -1e-6):
         raise ValueError("point outside the mesh")
     return best_t.astype(np.int32), np.ascontiguousarray(best_w)
 
@@ -237,12 +242,14 @@ def p_sequence(p):
     return seq
 
 
-def build(factory, n, p, hlevels=0, stream=None, cfl=None, plevels=True, **kw):
+def build(factory, n, p, hlevels=0, stream=None, cfl=None, plevels=True, coarsen=None, **kw):
     """Hierarchy for a workload factory(n=..., p=...): p-levels of the fine mesh
     down to p = 1 (unless plevels=False: the fine level goes straight to the h-levels,
     as the reference does with extra_finest_levels = 0), then `hlevels` split-square
-    meshes of n/2, n/4, ... at p = 1. cfl: None (the per-log2p defaults), a number,
-    or a dict p -> cfl."""
+    meshes of n/2, n/4, ... at p = 1. coarsen = a factor (e.g. 1.5): the h-levels are
+    instead made from the level above by hpb.coarsen.coarsen (tri_mesh::coarsen), through
+    factory(mesh=..., p=1). cfl: None (the per-log2p defaults), a number, or a dict
+    p -> cfl."""
     def cf(q):
         if cfl is None:
             return {}
@@ -255,6 +262,10 @@ def build(factory, n, p, hlevels=0, stream=None, cfl=None, plevels=True, **kw):
     m = n
     for _ in range(hlevels):
         m //= 2
-        probs.append(factory(n=m, p=1, **cf(1), **kw))
+        if coarsen:
+            from .coarsen import coarsen as coarsen_mesh
+            probs.append(factory(mesh=coarsen_mesh(probs[-1].mesh, coarsen), p=1, **cf(1), **kw))
+        else:
+            probs.append(factory(n=m, p=1, **cf(1), **kw))
         kinds.append("h")
     return Hierarchy(probs, kinds, stream=stream)

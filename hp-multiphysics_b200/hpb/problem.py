@@ -319,11 +319,12 @@ def _edges_where(mesh, pred):
     return b[pred(mid[:, 0], mid[:, 1])]
 
 
-def kovasznay_ins(n=64, p=4, re=100.0, noise=1e-3, seed=20261204, **kw):
+def kovasznay_ins(n=64, p=4, re=100.0, noise=1e-3, seed=20261204, mesh=None, **kw):
     """2D incompressible Navier-Stokes, Kovasznay flow at Re on an n x n split-square
-    mesh of the unit square; inflow (velocity essential) on left/top/bottom,
-    outflow (generic flux with the analytic pressure) on the right; rho = 1, mu = 1/Re."""
-    mesh = square_mesh(n)
+    mesh of the unit square (or `mesh`, a mesh of the unit square); inflow (velocity
+    essential) on left/top/bottom, outflow (generic flux with the analytic pressure) on the
+    right; rho = 1, mu = 1/Re."""
+    mesh = square_mesh(n) if mesh is None else mesh
     field = L.Field(L.HP_FIELD_KOVASZNAY, (ctypes.c_double * 4)(re, 0, 0, 0))
     eps = 1e-12
     inflow = _edges_where(mesh, lambda x, y: (x < eps) | (y < eps) | (y > 1 - eps))

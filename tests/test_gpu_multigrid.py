@@ -198,3 +198,30 @@ def test_curved_hole_cycles_keep_essential_values_and_converge():
     uv = H.levels[0].state()[0][on_hole, :2]
     assert np.max(np.abs(uv)) == 0.0
     H.close()
+
+
+@pytest.mark.parametrize("kind", ["ins", "cd-delaunay"])
+def test_cycles_on_coarsened_h_levels(kind):
+    """h-levels made from the level above by hpb.coarsen (tri_mesh::coarsen): the cycles
+    reach the 1e-10 drop, in a cycle count close to that of the generated (nested) levels for
+    the structured mesh."""
+    if kind == "ins":
+        def mk(n=16, p=4, mesh=None, **kw):
+            return hpb.kovasznay_ins(n=n, p=p, re=100.0, mesh=mesh, **kw)
+        cfl = None
+    else:
+        def mk(n=24, p=4, mesh=None, **kw):
+            return hpb.cd_sinsin(mesh=mesh if mesh is not None else hpb.delaunay_square(n, seed=n), p=p, kcond=1e-2,
+                                 field=quad(), **kw)
+        cfl = {4: 0.5, 2: 0.75, 1: 1.0}
+    n = 16 if kind == "ins" else 24
+    H = MG.build(mk, n=n, p=4, hlevels=2, cfl=cfl, coarsen=1.5)
+    assert H.levels[-1].prob.mesh.ntri < 0.1 * H.levels[0].prob.mesh.ntri
+    hist, sec, cycles = H.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2)
+    H.close()
+    assert hist[-1] <= 1e-10, hist[-3:]
+    if kind == "ins":
+        H = MG.build(mk, n=n, p=4, hlevels=2, cfl=cfl)
+        h2, s2, c2 = H.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2)
+        H.close()
+        assert cycles <= 1.3 * c2 + 3, (cycles, c2)
