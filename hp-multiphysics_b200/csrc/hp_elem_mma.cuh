@@ -48,6 +48,9 @@ struct InsMma {
     static constexpr size_t DER_LEN = (size_t)MT * 3 * KR * 32;
     static constexpr int IDX = 16;  // staged mesh integers per triangle: pnt[3], seg[3], sgn[3], vpos[3], spos[3]
     static constexpr size_t SMEM_IDX = (size_t)WPC * 2 * IDX * sizeof(int);
+    // per triangle: the metrics d00, d01, d10, d11 (ldcrd), mu / |J|, 2 nu / h, adis h / |J|, unused
+    static constexpr int GEO = 8;
+    static constexpr size_t SMEM_GEO = (size_t)WPC * 2 * GEO * sizeof(double);
     static_assert(4 * T <= 4 * QP, "gathered modes must fit the PD block");
 };
 
@@ -135,8 +138,10 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
     const int re_ = grow >> 2, rv = grow & 3;  // fragment row -> (triangle, variable)
     double *base = reinterpret_cast<double *>(smem_raw + ((sizeof(InsMmaSmall<P>) + 15) / 16) * 16) +
                    (size_t)warp * 2 * M::S_EL;
+    double *geo = reinterpret_cast<double *>(smem_raw + ((sizeof(InsMmaSmall<P>) + 15) / 16) * 16) +
+                  (size_t)M::WPC * 2 * M::S_EL + warp * 2 * M::GEO;
     int *midx = reinterpret_cast<int *>(reinterpret_cast<double *>(smem_raw + ((sizeof(InsMmaSmall<P>) + 15) / 16) * 16) +
-                                        (size_t)M::WPC * 2 * M::S_EL) + warp * 2 * M::IDX;
+                                        (size_t)M::WPC * 2 * (M::S_EL + M::GEO)) + warp * 2 * M::IDX;
     // per triangle: PV u, v, p at the points; PD the gathered modes, then du/dr, dv/dr,
     // du/ds, dv/ds, then the strong residual; FI the imaginary flux pairs (convective +
     // pressure for u, v; the mass flux for p); FX the viscous flux pairs (zero for p), then
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
 #pragma unroll
         for (int k = 0; k < NGATH; ++k) {
             const int w = lane + 32 * k;
-            if (w >= 2 * NV * T) break;
+            if (w >= 2 * NV * T) continue;
             const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
             const int *ix = midx + e * M::IDX;
             double val = 0.0;
@@ -197,27 +202,28 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             }
             PD(e)[n * T + m] = val;
         }
-        // geometry of both triangles: ldcrd(n,0) = (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2, and the
-        // inscribed-radius length scale of the SUPG tau (tri_mesh/tprims.cpp:224-241)
-        double gd[2][4], hh[2], gk[2][3];  // gk: mu / |J|, 2 nu / h, adis h / |J|
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const int *ix = midx + e * M::IDX;
+        // geometry of both triangles, by lanes 0 and 1 into the warp's geo block: ldcrd(n,0) =
+        // (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2, and the inscribed-radius length scale of the
+        // SUPG tau (tri_mesh/tprims.cpp:224-241)
+        if (lane < 2) {
+            const int *ix = midx + lane * M::IDX;
             const int p0 = ix[0], p1 = ix[1], p2 = ix[2];
             const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
             const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
             const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
-            gd[e][0] = 0.5 * (x2d - x1d); gd[e][1] = 0.5 * (x0d - x1d);
-            gd[e][2] = 0.5 * (y2d - y1d); gd[e][3] = 0.5 * (y0d - y1d);
+            double *gg = geo + lane * M::GEO;
+            const double d00 = 0.5 * (x2d - x1d), d01 = 0.5 * (x0d - x1d);
+            const double d10 = 0.5 * (y2d - y1d), d11 = 0.5 * (y0d - y1d);
             const double dx1 = x0d - x2d, dy1 = y0d - y2d, dx2 = x1d - x0d, dy2 = y1d - y0d;
             const double area = dx1 * dy2 - dy1 * dx2;
             const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
                                  sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
-            hh[e] = (area / perim) / (0.25 * (P + 1) * (P + 1));
-            const double cj = gd[e][0] * gd[e][3] - gd[e][2] * gd[e][1];
-            gk[e][0] = mu / cj;
-            gk[e][1] = 2. * (mu / rho) / hh[e];
-            gk[e][2] = ph.adis * hh[e] / cj;
+            const double he = (area / perim) / (0.25 * (P + 1) * (P + 1));
+            const double cj = d00 * d11 - d10 * d01;
+            gg[0] = d00; gg[1] = d01; gg[2] = d10; gg[3] = d11;
+            gg[4] = mu / cj;
+            gg[5] = 2. * (mu / rho) / he;
+            gg[6] = ph.adis * he / cj;
         }
         __syncwarp();
         // ---- projection on the tensor cores (proj.cpp:22-119 as dense per-point operators)
@@ -258,10 +264,13 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
         }
         __syncwarp();
         // ---- pointwise fluxes (ins/rsdl.cpp:259-340), lanes own (triangle, point)
-        for (int w = lane; w < 2 * GG; w += 32) {
+#pragma unroll
+        for (int it = 0; it < (2 * GG + 31) / 32; ++it) {
+            const int w = lane + 32 * it;
+            if (w >= 2 * GG) continue;
             const int e = w / GG, q = w - e * GG;
-            const double d00 = e ? gd[1][0] : gd[0][0], d01 = e ? gd[1][1] : gd[0][1];
-            const double d10 = e ? gd[1][2] : gd[0][2], d11 = e ? gd[1][3] : gd[0][3];
+            const double *gg = geo + e * M::GEO;
+            const double d00 = gg[0], d01 = gg[1], d10 = gg[2], d11 = gg[3];
             const double u0 = PV(e)[q], u1 = PV(e)[QP + q], pp = PV(e)[2 * QP + q];
             const double fluxx = rho * u0, fluxy = rho * u1;
             const double m0 = +d11 * fluxx - d01 * fluxy;
@@ -277,7 +286,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             fi[2 * VS + GG + q] = m1;
             if (beta > 0.0) {
                 const double dr0 = PD(e)[q], dr1 = PD(e)[QP + q], ds0 = PD(e)[2 * QP + q], ds1 = PD(e)[3 * QP + q];
-                const double cjcbi = e ? gk[1][0] : gk[0][0];
+                const double cjcbi = gg[4];
                 const double v0000 = -cjcbi * (2. * d11 * d11 + d01 * d01);
                 const double v0011 = -cjcbi * (2. * d10 * d10 + d00 * d00);
                 const double v0001 = cjcbi * (2. * d11 * d10 + d01 * d00);
@@ -336,6 +345,54 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                     }
                 }
         };
+        // lftog of both parts of one fragment at once (beta > 0): the slot and the side sign
+        // are found once for the imaginary value (-> res) and the beta-scaled real value (->
+        // res_r); interiors: res = im + dres + res_r with res_r = (1 - beta) res_r + re
+        auto scatter2 = [&](const double (&ci)[M::NT2][2], const double (&cr)[M::NT2][2]) {
+            if (rv >= 3 || !ACT(re_)) return;
+            const int t = TE(re_);
+            const int *ix = midx + re_ * M::IDX;
+#pragma unroll
+            for (int nt = 0; nt < M::NT2; ++nt)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int m = nt * 8 + gcol * 2 + h;
+                    if (m >= T) continue;
+                    double vi = ci[nt][h], vr = cr[nt][h] * beta;
+                    if (m < BM) {
+                        size_t slot;
+                        int g;
+                        if (m < 3) {
+                            slot = (size_t)ix[9 + m] * NV + rv;
+                            g = ix[m] * NV + rv;
+                        } else {
+                            const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
+                            if ((kk & 1) && ix[6 + i] < 0) {
+                                vi = -vi;
+                                vr = -vr;
+                            }
+                            slot = (size_t)3 * mesh.ntri * NV + ((size_t)ix[12 + i] * SM + kk) * NV + rv;
+                            g = (ix[3 + i] * SM + kk) * NV + rv;
+                        }
+                        if (st.elim) {
+                            st.elim[slot] = vi;
+                            st.elre[slot] = vr;
+                        } else if (m < 3) {
+                            atomicAdd(st.resv + g, vi);
+                            atomicAdd(st.rrv + g, vr);
+                        } else {
+                            atomicAdd(st.ress + g, vi);
+                            atomicAdd(st.rrs + g, vr);
+                        }
+                    } else {
+                        const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
+                        const double src = st.dresi ? st.dresi[gi] : 0.0;
+                        const double rr = st.rri[gi] * omb + vr;
+                        st.rri[gi] = rr;
+                        st.resi[gi] = (vi + src) + rr;
+                    }
+                }
+        };
         // ---- imaginary part: intgrtrs (intgrt.cpp:81-158, weak divergence with its minus
         //      sign in the operator) on the tensor cores -> res; with a real part (beta > 0)
         //      it is done together with that one below, sharing the operator loads
@@ -357,6 +414,15 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                     var = rem / G;
                     j = rem - var * G;
                 };
+                // the A fragments of the 1D operators, the same for every column tile
+                double ar[M::MT][2 * M::KR], as2[M::MT][M::KR];
+#pragma unroll
+                for (int mt = 0; mt < M::MT; ++mt) {
+#pragma unroll
+                    for (int ks = 0; ks < 2 * M::KR; ++ks) ar[mt][ks] = __ldg(AR + ((size_t)mt * 2 * M::KR + ks) * 32 + lane);
+#pragma unroll
+                    for (int ks = 0; ks < M::KR; ++ks) as2[mt][ks] = __ldg(AS + ((size_t)mt * M::KR + ks) * 32 + lane);
+                }
                 // part 1: rows i, columns (e, var, j)
 #pragma unroll 1
                 for (int nt = 0; nt < M::NTB; ++nt) {
@@ -375,7 +441,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                         const double bv = (colok && q < G) ? fi[off] + fx[off] : 0.0;
 #pragma unroll
                         for (int mt = 0; mt < M::MT; ++mt)
-                            dmma884(c[mt][0], c[mt][1], __ldg(AR + ((size_t)mt * 2 * M::KR + ks) * 32 + lane), bv);
+                            dmma884(c[mt][0], c[mt][1], ar[mt][ks], bv);
                     }
 #pragma unroll
                     for (int mt = 0; mt < M::MT; ++mt)
@@ -406,7 +472,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                         const double bv = (colok && l < G) ? fi[l] + fx[l] : 0.0;
 #pragma unroll
                         for (int mt = 0; mt < M::MT; ++mt)
-                            dmma884(c[mt][0], c[mt][1], __ldg(AS + ((size_t)mt * M::KR + ks) * 32 + lane), bv);
+                            dmma884(c[mt][0], c[mt][1], as2[mt][ks], bv);
                     }
 #pragma unroll
                     for (int mt = 0; mt < M::MT; ++mt)
@@ -423,16 +489,19 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             __syncwarp();
             // ---- pointwise SUPG terms (ins/rsdl.cpp:341-431, CALC_TAU2): FX becomes the real
             //      flux pairs, viscous minus SUPG for u, v and the continuity term for p
-            for (int w = lane; w < 2 * GG; w += 32) {
+#pragma unroll
+            for (int it = 0; it < (2 * GG + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= 2 * GG) continue;
                 const int e = w / GG, q = w - e * GG;
-                const double d00 = e ? gd[1][0] : gd[0][0], d01 = e ? gd[1][1] : gd[0][1];
-                const double d10 = e ? gd[1][2] : gd[0][2], d11 = e ? gd[1][3] : gd[0][3];
+                const double *gg = geo + e * M::GEO;
+                const double d00 = gg[0], d01 = gg[1], d10 = gg[2], d11 = gg[3];
                 const double u0 = PV(e)[q], u1 = PV(e)[QP + q];
                 const double qv = u0 * u0 + u1 * u1;
-                const double t2 = e ? gk[1][1] : gk[0][1];
+                const double t2 = gg[5];
                 double gam = 3.0 * qv + t2 * t2;
                 if (ph.mu + ph.bd0 == 0.0) gam = (gam > 0.1 ? gam : 0.1);
-                const double tau0 = (e ? gk[1][2] : gk[0][2]) / sqrt(gam);
+                const double tau0 = gg[6] / sqrt(gam);
                 const double tau2 = sqrt(qv) * tau0;
                 const double tr0 = tau0 * PD(e)[q], tr1 = tau0 * PD(e)[QP + q], tr2 = tau2 * PD(e)[2 * QP + q];
                 double *fx = FX(e);
@@ -449,8 +518,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             double ci[M::NT2][2], c[M::NT2][2];
             warp_gemm2<M::KS2, M::NT2>(FI(re_) + (rv < 3 ? rv : 2) * VS, FX(re_) + (rv < 3 ? rv : 2) * VS, intB, gcol,
                                        lane, ci, c);
-            scatter(ci, 0);
-            scatter(c, 1);
+            scatter2(ci, c);
         }
         __syncwarp();
     }

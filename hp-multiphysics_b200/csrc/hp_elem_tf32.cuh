@@ -225,7 +225,10 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
         }
         __syncwarp();
         // ---- gather the modes (ugtouht, gtol.cpp:14-55) into the PD block
-        for (int w = lane; w < 4 * NV * T; w += 32) {
+#pragma unroll
+        for (int it = 0; it < (4 * NV * T + 31) / 32; ++it) {
+            const int w = lane + 32 * it;
+            if (w >= 4 * NV * T) continue;
             const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
             const int *ix = midx + e * M::IDX;
             float val = 0.f;
@@ -291,7 +294,10 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
         }
         __syncwarp();
         // ---- pointwise fluxes, lanes own (triangle, point)
-        for (int w = lane; w < 4 * GG; w += 32) {
+#pragma unroll
+        for (int it = 0; it < (4 * GG + 31) / 32; ++it) {
+            const int w = lane + 32 * it;
+            if (w >= 4 * GG) continue;
             const int e = w / GG, q = w - e * GG;
             const int t = TE(e);
             const float *gg = geo + e * M::GEO;
@@ -449,7 +455,10 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             }
             __syncwarp();
             // ---- SUPG with tau of the base state (correction form) or of the state (plain)
-            for (int w = lane; w < 4 * GG; w += 32) {
+#pragma unroll
+            for (int it = 0; it < (4 * GG + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= 4 * GG) continue;
                 const int e = w / GG, q = w - e * GG;
                 const int t = TE(e);
                 const float *gg = geo + e * M::GEO;

@@ -461,7 +461,7 @@ struct LaunchImpl {
     static int mma_smem() {
         if constexpr (DBL)
             return (int)(((sizeof(InsMmaSmall<P>) + 15) / 16) * 16 + (size_t)2 * InsMma<P>::S_EL * InsMma<P>::WPC * 8 +
-                         InsMma<P>::SMEM_IDX);
+                         InsMma<P>::SMEM_GEO + InsMma<P>::SMEM_IDX);
         else
             return (int)(((sizeof(InsMmaSmallF<P>) + 15) / 16) * 16 + (size_t)4 * InsTf32<P>::S_EL * InsTf32<P>::WPC * 4 +
                          InsTf32<P>::SMEM_IDX);
