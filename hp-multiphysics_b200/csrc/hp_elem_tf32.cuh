@@ -387,6 +387,46 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                     }
             }
         };
+        // lftog of both parts at once (beta > 0): the side sign and the index are found once
+        // for the imaginary value (-> res) and the beta-scaled real value (-> res_r);
+        // interiors: res = im + dres + res_r with res_r = (1 - beta) res_r + re
+        auto scatter2 = [&](const float (&ci)[M::NT2][4], const float (&cr)[M::NT2][4]) {
+            if (rv >= 3) return;
+#pragma unroll
+            for (int hh = 0; hh < 2; ++hh) {
+                const int e = ra + 2 * hh;
+                if (!ACT(e)) continue;
+                const int t = TE(e);
+                const int *ix = midx + e * M::IDX;
+#pragma unroll
+                for (int nt = 0; nt < M::NT2; ++nt)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int m = nt * 8 + tig * 2 + h;
+                        if (m >= T) continue;
+                        float vi = ci[nt][2 * hh + h], vr = cr[nt][2 * hh + h] * beta;
+                        if (m < 3) {
+                            atomicAdd(st.resv + ix[m] * NV + rv, vi);
+                            atomicAdd(st.rrv + ix[m] * NV + rv, vr);
+                        } else if (m < BM) {
+                            const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
+                            if ((kk & 1) && ix[6 + i] < 0) {
+                                vi = -vi;
+                                vr = -vr;
+                            }
+                            const int g = (ix[3 + i] * SM + kk) * NV + rv;
+                            atomicAdd(st.ress + g, vi);
+                            atomicAdd(st.rrs + g, vr);
+                        } else {
+                            const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
+                            const float src = st.dresi ? st.dresi[gi] : 0.f;
+                            const float rr = st.rri[gi] * omb + vr;
+                            st.rri[gi] = rr;
+                            st.resi[gi] = (vi + src) + rr;
+                        }
+                    }
+            }
+        };
         // imaginary part -> res; with a real part (beta > 0) it is done together with that one
         // below, sharing the operator loads
         if (beta == 0.f) {
@@ -400,8 +440,7 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             //      (triangle, variable, j): n0(j) (Ar fr + As1 fs); part 2 rows j, columns
             //      (triangle, variable, i): As2 fs^T; into PD
             {
-                const float4 *AR = reinterpret_cast<const float4 *>(derB);
-                const float4 *AS = AR + 2 * M::KR * 32;
+                const float4 *AR = reinterpret_cast<const float4 *>(derB);  // [Ar | As1] then As2
                 auto col = [&](int n, int &e, int &var, int &j) {
                     e = n / (3 * G);
                     const int rem = n - e * 3 * G;
@@ -412,7 +451,11 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                     a[0] = __float_as_uint(v.x); a[1] = __float_as_uint(v.y);
                     a[2] = __float_as_uint(v.z); a[3] = __float_as_uint(v.w);
                 };
-#pragma unroll 1
+                // the A fragments of the 1D operators, the same for every column tile
+                float4 afr[3 * M::KR];
+#pragma unroll
+                for (int k = 0; k < 3 * M::KR; ++k) afr[k] = __ldg(AR + (size_t)k * 32 + lane);
+#pragma unroll
                 for (int part = 0; part < 2; ++part) {
                     const int nks = part ? M::KR : 2 * M::KR;
 #pragma unroll 1
@@ -423,9 +466,10 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                         const bool colok = n < M::NCOL;
                         const float *fi = FI(e) + var * VS, *fx = FX(e) + var * VS;
                         float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
                         for (int ks = 0; ks < nks; ++ks) {
                             unsigned a[4];
-                            a4(__ldg((part ? AS : AR) + (size_t)ks * 32 + lane), a);
+                            a4(afr[(part ? 2 * M::KR : 0) + ks], a);
                             float2 bv = make_float2(0.f, 0.f);
                             if (part == 0) {  // k = q of [fr | fs] at column point j = x
                                 const int blk = ks / M::KR, q0 = (ks - blk * M::KR) * 8 + tig, q1 = q0 + 4;
@@ -490,8 +534,7 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             float ci[M::NT2][4], c[M::NT2][4];
             warp_gemm2_tf32<M::KS2, M::NT2>(FI(ra) + rvv * VS, FI(ra + 2) + rvv * VS, FX(ra) + rvv * VS,
                                              FX(ra + 2) + rvv * VS, intB, tig, lane, ci, c);
-            scatter(ci, 0);
-            scatter(c, 1);
+            scatter2(ci, c);
         }
         __syncwarp();
     }
