@@ -395,54 +395,52 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
             }
             __syncwarp();
         }
-        // ---- intgrtrst on the tensor cores (imaginary into res, real * beta into res_r)
+        // ---- intgrtrst on the tensor cores (imaginary into res, real * beta into res_r); with a
+        //      real part both share each operator fragment load
         {
             const int e = grow >> 2, n = grow & 3;
+            const bool two = beta > 0.0;
             double tot[M::NT2][2];
+            const double *fai = FIM(e) + n * VS, *far = FRE(e) + n * VS;  // [3][Q] = k order
+            double ci[M::NT2][2], cr[M::NT2][2];
 #pragma unroll
-            for (int nt = 0; nt < M::NT2; ++nt) tot[nt][0] = tot[nt][1] = 0.0;
-            for (int part = 0; part < (beta > 0.0 ? 2 : 1); ++part) {
-                const double *fa = (part == 0 ? FIM(e) : FRE(e)) + n * VS;  // [3][Q] = k order
-                // all NT2 n-tiles share each A fragment; two K halves -> 2 * NT2 chains
-                double c[2][M::NT2][2];
-#pragma unroll
-                for (int hh = 0; hh < 2; ++hh)
-#pragma unroll
-                    for (int nt = 0; nt < M::NT2; ++nt) c[hh][nt][0] = c[hh][nt][1] = 0.0;
+            for (int nt = 0; nt < M::NT2; ++nt) ci[nt][0] = ci[nt][1] = cr[nt][0] = cr[nt][1] = 0.0;
 #pragma unroll 2
-                for (int ks = 0; ks < M::KS2; ++ks) {
-                    const int k = ks * 4 + gcol;
-                    const double av = k < 3 * Q ? fa[k] : 0.0;
+            for (int ks = 0; ks < M::KS2; ++ks) {
+                const int k = ks * 4 + gcol;
+                const double ai = k < 3 * Q ? fai[k] : 0.0;
+                const double ar = (two && k < 3 * Q) ? far[k] : 0.0;
 #pragma unroll
-                    for (int nt = 0; nt < M::NT2; ++nt)
-                        dmma(c[ks & 1][nt][0], c[ks & 1][nt][1], av, __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane));
-                }
-                const bool ok = (e == 0 || has1);
                 for (int nt = 0; nt < M::NT2; ++nt) {
-                    // row grow = (e, n); columns m = nt*8 + gcol*2 + {0, 1}
-                    const double c0 = c[0][nt][0] + c[1][nt][0], c1 = c[0][nt][1] + c[1][nt][1];
+                    const double bf = __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane);
+                    dmma(ci[nt][0], ci[nt][1], ai, bf);
+                    if (two) dmma(cr[nt][0], cr[nt][1], ar, bf);
+                }
+            }
+            const bool ok = (e == 0 || has1);
 #pragma unroll
-                    for (int h2 = 0; h2 < 2; ++h2) {
-                        const int m = nt * 8 + gcol * 2 + h2;
-                        if (!ok || m >= T) continue;
-                        const double val = -(h2 ? c1 : c0);
-                        if constexpr (MODE != 0) {
-                            tot[nt][h2] += part == 0 ? val : beta * val;
-                            continue;
-                        }
+            for (int nt = 0; nt < M::NT2; ++nt)
+#pragma unroll
+                for (int h2 = 0; h2 < 2; ++h2) {
+                    // row grow = (e, n); columns m = nt*8 + gcol*2 + {0, 1}
+                    const int m = nt * 8 + gcol * 2 + h2;
+                    tot[nt][h2] = 0.0;
+                    if (!ok || m >= T) continue;
+                    const double vi = -ci[nt][h2], vr = -cr[nt][h2];
+                    if constexpr (MODE != 0) {
+                        tot[nt][h2] = two ? vi + beta * vr : vi;
+                    } else {
                         double sg;
-                        if (part == 0) {
-                            double *dst = mode_slot<double, P>(mesh, res, te[e], m, n, sg);
-                            if (m < C::BM) atomicAdd(dst, sg * val);
-                            else *dst = val;
-                        } else {
-                            double *dst = mode_slot<double, P>(mesh, rr, te[e], m, n, sg);
-                            if (m < C::BM) atomicAdd(dst, beta * sg * val);
-                            else *dst += beta * val;
+                        double *dst = mode_slot<double, P>(mesh, res, te[e], m, n, sg);
+                        if (m < C::BM) atomicAdd(dst, sg * vi);
+                        else *dst = vi;
+                        if (two) {
+                            double *dr = mode_slot<double, P>(mesh, rr, te[e], m, n, sg);
+                            if (m < C::BM) atomicAdd(dr, beta * sg * vr);
+                            else *dr += beta * vr;
                         }
                     }
                 }
-            }
             if constexpr (MODE != 0) {
                 const bool ok = (e == 0 || has1);
 #pragma unroll
