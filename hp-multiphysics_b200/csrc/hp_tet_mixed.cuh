@@ -307,20 +307,30 @@ __global__ void __launch_bounds__(TetTf32<P>::WPC * 32)
             __syncwarp();
         }
         // ---- intgrtrst on TF32 (imaginary into res, real * beta into res_r); lftog
-        for (int part = 0; part < (beta > 0.f ? 2 : 1); ++part) {
-            const float *r0 = (part == 0 ? FIM(ra) : FRE(ra)) + rv * VS;
-            const float *r1 = (part == 0 ? FIM(ra + 2) : FRE(ra + 2)) + rv * VS;
-            float c[M::NT2][4];
+        {
+            // with a real part both products share each operator fragment load
+            const bool two = beta > 0.f;
+            const float *i0 = FIM(ra) + rv * VS, *i1 = FIM(ra + 2) + rv * VS;
+            const float *q0 = FRE(ra) + rv * VS, *q1 = FRE(ra + 2) + rv * VS;
+            float ci[M::NT2][4], cr[M::NT2][4];
 #pragma unroll
-            for (int nt = 0; nt < M::NT2; ++nt) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.f;
-#pragma unroll 4
+            for (int nt = 0; nt < M::NT2; ++nt)
+                ci[nt][0] = ci[nt][1] = ci[nt][2] = ci[nt][3] = cr[nt][0] = cr[nt][1] = cr[nt][2] = cr[nt][3] = 0.f;
+#pragma unroll 2
             for (int ks = 0; ks < M::KS2; ++ks) {
                 const int k = ks * 8 + tig;
-                const unsigned a0 = tet_tf32(r0[k]), a1 = tet_tf32(r1[k]), a2 = tet_tf32(r0[k + 4]),
-                               a3 = tet_tf32(r1[k + 4]);
+                const unsigned a0 = tet_tf32(i0[k]), a1 = tet_tf32(i1[k]), a2 = tet_tf32(i0[k + 4]),
+                               a3 = tet_tf32(i1[k + 4]);
+                unsigned b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+                if (two) {
+                    b0 = tet_tf32(q0[k]); b1 = tet_tf32(q1[k]); b2 = tet_tf32(q0[k + 4]); b3 = tet_tf32(q1[k + 4]);
+                }
 #pragma unroll
-                for (int nt = 0; nt < M::NT2; ++nt)
-                    tet_mma_tf32(c[nt], a0, a1, a2, a3, __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane));
+                for (int nt = 0; nt < M::NT2; ++nt) {
+                    const float2 bf = __ldg(intB + ((size_t)nt * M::KS2 + ks) * 32 + lane);
+                    tet_mma_tf32(ci[nt], a0, a1, a2, a3, bf);
+                    if (two) tet_mma_tf32(cr[nt], b0, b1, b2, b3, bf);
+                }
             }
 #pragma unroll
             for (int hh = 0; hh < 2; ++hh) {
@@ -333,16 +343,15 @@ __global__ void __launch_bounds__(TetTf32<P>::WPC * 32)
                     for (int h2 = 0; h2 < 2; ++h2) {
                         const int m = nt * 8 + tig * 2 + h2;
                         if (m >= T) continue;
-                        const float val = -c[nt][2 * hh + h2];
+                        const float vi = -ci[nt][2 * hh + h2], vr = -cr[nt][2 * hh + h2];
                         float sg;
-                        if (part == 0) {
-                            float *dst = mode_slot<float, P>(mesh, res, t, m, rv, sg);
-                            if (m < C::BM) atomicAdd(dst, sg * val);
-                            else *dst = val;
-                        } else {
-                            float *dst = mode_slot<float, P>(mesh, rr, t, m, rv, sg);
-                            if (m < C::BM) atomicAdd(dst, beta * sg * val);
-                            else *dst += beta * val;
+                        float *dst = mode_slot<float, P>(mesh, res, t, m, rv, sg);
+                        if (m < C::BM) atomicAdd(dst, sg * vi);
+                        else *dst = vi;
+                        if (two) {
+                            float *dr = mode_slot<float, P>(mesh, rr, t, m, rv, sg);
+                            if (m < C::BM) atomicAdd(dr, beta * sg * vr);
+                            else *dr += beta * vr;
                         }
                     }
             }
