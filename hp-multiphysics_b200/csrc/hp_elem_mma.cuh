@@ -186,7 +186,8 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
         for (int k = 0; k < NGATH; ++k) {
             const int w = lane + 32 * k;
             if (w >= 2 * NV * T) continue;
-            const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
+            // item order (triangle, mode, variable): consecutive lanes read consecutive values
+            const int e = w / (NV * T), r = w - e * (NV * T), m = r / NV, n = r - m * NV;
             const int *ix = midx + e * M::IDX;
             double val = 0.0;
             if (ACT(e)) {
@@ -202,28 +203,17 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             }
             PD(e)[n * T + m] = val;
         }
-        // geometry of both triangles, by lanes 0 and 1 into the warp's geo block: ldcrd(n,0) =
-        // (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2, and the inscribed-radius length scale of the
-        // SUPG tau (tri_mesh/tprims.cpp:224-241)
+        // geometry of both triangles into the warp's geo block, from the per-triangle
+        // constants (Mesh::tgeo: ldcrd(n,0) = (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2, 1 / |J|, and
+        // the inscribed-radius length scale of the SUPG tau, tri_mesh/tprims.cpp:224-241)
         if (lane < 2) {
-            const int *ix = midx + lane * M::IDX;
-            const int p0 = ix[0], p1 = ix[1], p2 = ix[2];
-            const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
-            const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
-            const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
+            const double *tg = mesh.tgeo + (size_t)8 * TE(lane);
             double *gg = geo + lane * M::GEO;
-            const double d00 = 0.5 * (x2d - x1d), d01 = 0.5 * (x0d - x1d);
-            const double d10 = 0.5 * (y2d - y1d), d11 = 0.5 * (y0d - y1d);
-            const double dx1 = x0d - x2d, dy1 = y0d - y2d, dx2 = x1d - x0d, dy2 = y1d - y0d;
-            const double area = dx1 * dy2 - dy1 * dx2;
-            const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
-                                 sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
-            const double he = (area / perim) / (0.25 * (P + 1) * (P + 1));
-            const double cj = d00 * d11 - d10 * d01;
-            gg[0] = d00; gg[1] = d01; gg[2] = d10; gg[3] = d11;
-            gg[4] = mu / cj;
-            gg[5] = 2. * (mu / rho) / he;
-            gg[6] = ph.adis * he / cj;
+            const double icj = tg[4], he = tg[5], ihe = tg[6];
+            gg[0] = tg[0]; gg[1] = tg[1]; gg[2] = tg[2]; gg[3] = tg[3];
+            gg[4] = mu * icj;
+            gg[5] = 2. * (mu / rho) * ihe;
+            gg[6] = ph.adis * he * icj;
         }
         __syncwarp();
         // ---- projection on the tensor cores (proj.cpp:22-119 as dense per-point operators)
@@ -424,7 +414,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                     for (int ks = 0; ks < M::KR; ++ks) as2[mt][ks] = __ldg(AS + ((size_t)mt * M::KR + ks) * 32 + lane);
                 }
                 // part 1: rows i, columns (e, var, j)
-#pragma unroll 1
+#pragma unroll
                 for (int nt = 0; nt < M::NTB; ++nt) {
                     int e, var, j;
                     const int n = nt * 8 + grow;
@@ -456,7 +446,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                 }
                 __syncwarp();
                 // part 2: rows j, columns (e, var, i)
-#pragma unroll 1
+#pragma unroll
                 for (int nt = 0; nt < M::NTB; ++nt) {
                     int e, var, i;
                     const int n = nt * 8 + grow;

@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(256, 2)
     constexpr int NV = 3;
     const int lane = threadIdx.x & 31, q = lane & 3, i = q >> 1, j = q & 1;
     const R beta = (R)ph.beta[stage];
-    const R rho = (R)ph.rho, mu = (R)ph.mu;
+    const R rho = (R)ph.rho;
     const bool corr = diff && st.ubv;
     (void)zero_rr;  // no interior modes at p = 1: res_r is folded by the caller's pre / assembly
     // this lane's rows of the operators
@@ -72,11 +72,8 @@ __global__ void __launch_bounds__(256, 2)
             u[n][1] = st.ugv[p1 * NV + n];
             u[n][2] = st.ugv[p2 * NV + n];
         }
-        const double x0d = mesh.pnts[2 * p0], y0d = mesh.pnts[2 * p0 + 1];
-        const double x1d = mesh.pnts[2 * p1], y1d = mesh.pnts[2 * p1 + 1];
-        const double x2d = mesh.pnts[2 * p2], y2d = mesh.pnts[2 * p2 + 1];
-        const R d00 = (R)(0.5 * (x2d - x1d)), d01 = (R)(0.5 * (x0d - x1d));
-        const R d10 = (R)(0.5 * (y2d - y1d)), d11 = (R)(0.5 * (y0d - y1d));
+        const double *tg = mesh.tgeo + (size_t)8 * t;  // per-triangle constants (Mesh::tgeo)
+        const R d00 = (R)tg[0], d01 = (R)tg[1], d10 = (R)tg[2], d11 = (R)tg[3];
         // projection to this lane's point
         R u0 = 0, u1 = 0, pp = 0;
 #pragma unroll
@@ -141,7 +138,7 @@ __global__ void __launch_bounds__(256, 2)
                 dr0 += DR[m] * u[0][m]; dr1 += DR[m] * u[1][m];
                 ds0 += DS[m] * u[0][m]; ds1 += DS[m] * u[1][m];
             }
-            const R cjcbi = mu / (d00 * d11 - d10 * d01);
+            const R cjcbi = (R)(ph.mu * tg[4]);
             const R v0000 = -cjcbi * ((R)2 * d11 * d11 + d01 * d01);
             const R v0011 = -cjcbi * ((R)2 * d10 * d10 + d00 * d00);
             const R v0001 = cjcbi * ((R)2 * d11 * d10 + d01 * d00);
@@ -166,12 +163,6 @@ __global__ void __launch_bounds__(256, 2)
                 res[n] = n0j * (ar_ii * fr + ar_io * fr_oi + as1_ii * fs + as1_io * fs_oi) + (as2_jj * fs + as2_jo * fs_oj);
             }
             // SUPG (ins/rsdl.cpp:341-431, CALC_TAU2), tau of the base in correction form
-            const double dx1 = x0d - x2d, dy1 = y0d - y2d, dx2 = x1d - x0d, dy2 = y1d - y0d;
-            const double area = dx1 * dy2 - dy1 * dx2;
-            const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
-                                 sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
-            const R hh = (R)((area / perim) / (0.25 * 2 * 2));
-            const R cj = d00 * d11 - d10 * d01;
             R a0 = u0, a1 = u1, qv;
             if (corr) {
                 qv = b0 * b0 + b1 * b1;
@@ -180,10 +171,10 @@ __global__ void __launch_bounds__(256, 2)
             } else {
                 qv = u0 * u0 + u1 * u1;
             }
-            const R t2 = (R)2 * (R)(ph.mu / ph.rho) / hh;
+            const R t2 = (R)(2. * (ph.mu / ph.rho) * tg[6]);
             R gam = (R)3 * qv + t2 * t2;
             if (ph.mu + ph.bd0 == 0.0) gam = (gam > (R)0.1 ? gam : (R)0.1);
-            const R tau0 = ((R)ph.adis * hh / cj) / sqrt(gam);
+            const R tau0 = (R)(ph.adis * tg[5] * tg[4]) / sqrt(gam);
             const R tau2 = sqrt(qv) * tau0;
             const R tr0 = tau0 * res[0], tr1 = tau0 * res[1], tr2 = tau2 * res[2];
             fxr[0] -= (d11 * ((R)2 * a0) - d01 * a1) * tr0 - d01 * a0 * tr1 + d11 * tr2;

@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
     __syncthreads();
     const float beta = (float)ph.beta[stage];
     const float omb = zero_rr ? 0.f : 1.f - beta;
-    const float rho = (float)ph.rho, mu = (float)ph.mu;
+    const float rho = (float)ph.rho;
     const bool corr = diff && st.bpt;
     const long ntri = mesh.ntri, nquad = (ntri + 3) / 4;
     const int rvv = rv < 3 ? rv : 2;  // variable slot 3 repeats slot 2 (its rows are discarded)
@@ -204,24 +204,13 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                                          : (k < 6 ? mesh.tri_seg[3 * t + k - 3] : mesh.tri_sgn[3 * t + k - 6]);
         }
         __syncwarp();
-        if (lane < 4) {  // per-triangle geometry: ldcrd metrics and the tau length scale
-            const int *ix = midx + lane * M::IDX;
-            const double x0d = mesh.pnts[2 * ix[0]], y0d = mesh.pnts[2 * ix[0] + 1];
-            const double x1d = mesh.pnts[2 * ix[1]], y1d = mesh.pnts[2 * ix[1] + 1];
-            const double x2d = mesh.pnts[2 * ix[2]], y2d = mesh.pnts[2 * ix[2] + 1];
-            const float d00 = (float)(0.5 * (x2d - x1d)), d01 = (float)(0.5 * (x0d - x1d));
-            const float d10 = (float)(0.5 * (y2d - y1d)), d11 = (float)(0.5 * (y0d - y1d));
-            const double dx1 = x0d - x2d, dy1 = y0d - y2d, dx2 = x1d - x0d, dy2 = y1d - y0d;
-            const double area = dx1 * dy2 - dy1 * dx2;
-            const double perim = sqrt(dx1 * dx1 + dy1 * dy1) + sqrt(dx2 * dx2 + dy2 * dy2) +
-                                 sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
-            const float he = (float)((area / perim) / (0.25 * (P + 1) * (P + 1)));
-            const float cjcb = d00 * d11 - d10 * d01;
+        if (lane < 4) {  // per-triangle geometry (Mesh::tgeo): ldcrd metrics and the tau length scale
+            const double *tg = mesh.tgeo + (size_t)8 * TE(lane);
             float *gg = geo + lane * M::GEO;
-            gg[0] = d00; gg[1] = d01; gg[2] = d10; gg[3] = d11;
-            gg[4] = mu / cjcb;
-            gg[5] = 2.f * (float)(ph.mu / ph.rho) / he;
-            gg[6] = (float)ph.adis * he / cjcb;
+            gg[0] = (float)tg[0]; gg[1] = (float)tg[1]; gg[2] = (float)tg[2]; gg[3] = (float)tg[3];
+            gg[4] = (float)(ph.mu * tg[4]);
+            gg[5] = (float)(2. * (ph.mu / ph.rho) * tg[6]);
+            gg[6] = (float)(ph.adis * tg[5] * tg[4]);
         }
         __syncwarp();
         // ---- gather the modes (ugtouht, gtol.cpp:14-55) into the PD block

@@ -900,6 +900,29 @@ extern "C" int hp_gpu_create(const hp_mesh_desc *m, const hp_basis_tables *b, co
     M.vess = d_vess; M.sess = d_sess; M.bseg = d_bseg; M.bkind = d_bkind; M.bpibc = d_bpibc;
     M.tri_cv = nullptr; M.crv_cht = nullptr; M.bcrd = nullptr; M.ncurved = 0; M.crv_tri = nullptr;
     M.seg_bdry = d_sbd; M.vb_idx = d_vbi; M.vpos = d_vpos; M.spos = d_spos;
+    {   // per-triangle constants of the straight branch (tri_hp_ins::element_rsdl's ldcrd and
+        // the inscribed-radius length scale of tau, tri_mesh/tprims.cpp:224-241)
+        std::vector<double> g((size_t)8 * nt, 0.0);
+        const double pf = 0.25 * (b->p + 1) * (b->p + 1);
+        for (int t = 0; t < nt; ++t) {
+            const double *x0 = m->pnts + 2 * m->tri_pnt[3 * t], *x1 = m->pnts + 2 * m->tri_pnt[3 * t + 1],
+                         *x2 = m->pnts + 2 * m->tri_pnt[3 * t + 2];
+            double *o = &g[(size_t)8 * t];
+            o[0] = 0.5 * (x2[0] - x1[0]); o[1] = 0.5 * (x0[0] - x1[0]);
+            o[2] = 0.5 * (x2[1] - x1[1]); o[3] = 0.5 * (x0[1] - x1[1]);
+            const double dx1 = x0[0] - x2[0], dy1 = x0[1] - x2[1], dx2 = x1[0] - x0[0], dy2 = x1[1] - x0[1];
+            const double area = dx1 * dy2 - dy1 * dx2;
+            const double perim = std::sqrt(dx1 * dx1 + dy1 * dy1) + std::sqrt(dx2 * dx2 + dy2 * dy2) +
+                                 std::sqrt((dx1 + dx2) * (dx1 + dx2) + (dy1 + dy2) * (dy1 + dy2));
+            const double he = (area / perim) / pf;
+            o[4] = 1.0 / (o[0] * o[3] - o[2] * o[1]);
+            o[5] = he;
+            o[6] = 1.0 / he;
+        }
+        double *d_g;
+        if ((r = upload(c, &d_g, g.data(), g.size()))) return fail(r);
+        M.tgeo = d_g;
+    }
 
     // curved elements (tri_hp::metric::setinfo, metric.cpp:44-70, for p > 1): the
     // owner triangle of every boundary side with non-zero position modes, with its

@@ -69,6 +69,9 @@ struct Mesh {
     // vertex-incidence list (vt_idx), spos[3 t + i] = 2 s + k for side i of t being
     // seg.tri(k) of segment s
     const int *vpos, *spos;
+    // per-triangle constants of the straight-element branch [ntri][8]: ldcrd d00, d01, d10,
+    // d11, 1 / |J|, the tau length scale h (inscribed radius / (0.25 (p+1)^2)), 1 / h, unused
+    const double *tgeo;
 };
 
 // Slot of an element's vertex / side residual in the assembly buffers (State::elim,
