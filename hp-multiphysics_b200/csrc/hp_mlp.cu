@@ -9,13 +9,16 @@
 // the forward pass; activations are rounded to BF16 between layers, every dot
 // product accumulates in FP32.
 //
-// Kernels: one thread per sample, the parameters staged in shared memory (all
+// Kernels: inference of the learned corrections' shape (inputs <= 32, hidden layers of
+// 64, one output) on the BF16 tensor cores (k_mlp_forward_mma); other shapes and the
+// training pass one thread per sample, the parameters staged in shared memory (all
 // threads of a warp read the same weight: broadcast, no bank conflicts). The
 // backward pass reduces each weight's per-sample gradient across the warp with
 // shuffles, then across the block in shared memory, then into the global FP32
 // gradient with one atomic per weight per block.
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -125,6 +128,142 @@ __global__ void k_mlp_backward(Dims d, const float *__restrict__ pbf, const floa
     __syncthreads();
     for (int k = threadIdx.x; k < d.nparam; k += blockDim.x) atomicAdd(&grad[k], sg[k]);
     if (threadIdx.x == 0) atomicAdd(loss, 0.5f * sl * inv_n);
+}
+
+// Forward pass on the BF16 tensor cores (mma.sync.m16n8k16, FP32 accumulation) for the
+// shape of the learned corrections: n0 <= 32 inputs, hidden layers of 64, one output.
+// A warp takes 16 samples: each layer's C fragments (+ bias, ReLU, rounded to BF16) are
+// the next layer's A fragments as they sit in the registers (n-tiles 2t and 2t + 1 of the
+// output are k-step t of the next product); the weights are the B operands, staged in
+// shared memory as BF16 with padded rows; the 64 -> 1 output layer is a dot product per
+// sample summed over the four lanes that hold a row. Same arithmetic as forward_one up to
+// the order of the FP32 sums.
+constexpr int kMmaW = 64, kMmaP0 = 40, kMmaPH = 72;  // hidden width; padded row lengths (BF16)
+
+__device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const unsigned *>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                 "{%8, %9}, {%0, %1, %2, %3};"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__global__ void __launch_bounds__(128) k_mlp_forward_mma(Dims d, const float *__restrict__ pbf,
+                                                         const float *__restrict__ mean,
+                                                         const float *__restrict__ istd, const float *__restrict__ X,
+                                                         int n, float *__restrict__ Y) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int nh = d.L - 1;  // hidden layers (each followed by ReLU)
+    __nv_bfloat16 *w0 = reinterpret_cast<__nv_bfloat16 *>(smraw);     // [64][kMmaP0]
+    __nv_bfloat16 *wh = w0 + kMmaW * kMmaP0;                            // [nh-1][64][kMmaPH]
+    float *bias = reinterpret_cast<float *>(wh + (size_t)(nh - 1) * kMmaW * kMmaPH);  // [nh][64]
+    float *wout = bias + nh * kMmaW;                                      // [64], then bout
+    float *smean = wout + kMmaW + 1, *sistd = smean + 32;
+    const int n0 = d.n[0];
+    for (int k = threadIdx.x; k < kMmaW * kMmaP0; k += blockDim.x) {
+        const int o = k / kMmaP0, i = k - o * kMmaP0;
+        w0[k] = __float2bfloat16_rn(i < n0 ? pbf[d.woff[0] + o * n0 + i] : 0.f);
+    }
+    for (int l = 1; l < nh; ++l)
+        for (int k = threadIdx.x; k < kMmaW * kMmaPH; k += blockDim.x) {
+            const int o = k / kMmaPH, i = k - o * kMmaPH;
+            wh[(size_t)(l - 1) * kMmaW * kMmaPH + k] =
+                __float2bfloat16_rn(i < kMmaW ? pbf[d.woff[l] + o * kMmaW + i] : 0.f);
+        }
+    for (int k = threadIdx.x; k < nh * kMmaW; k += blockDim.x) bias[k] = pbf[d.boff[k / kMmaW] + k % kMmaW];
+    for (int k = threadIdx.x; k <= kMmaW; k += blockDim.x) wout[k] = pbf[k < kMmaW ? d.woff[nh] + k : d.boff[nh]];
+    for (int k = threadIdx.x; k < 32; k += blockDim.x) {
+        smean[k] = k < n0 ? mean[k] : 0.f;
+        sistd[k] = k < n0 ? istd[k] : 0.f;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
+    const long step = (long)gridDim.x * (blockDim.x >> 5) * 16;
+    for (long base = ((long)blockIdx.x * (blockDim.x >> 5) + warp) * 16; base < n; base += step) {
+        const long r0 = base + g, r1 = base + g + 8;
+        // layer 0 A fragments: standardised inputs, rounded to BF16, K padded to 32
+        unsigned a[4][4];
+        auto xin = [&](long r, int k) -> float {
+            return (r < n && k < n0) ? (X[(size_t)r * n0 + k] - smean[k]) * sistd[k] : 0.f;
+        };
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            const int k = ks * 16 + 2 * t4;
+            a[ks][0] = pack_bf16(xin(r0, k), xin(r0, k + 1));
+            a[ks][1] = pack_bf16(xin(r1, k), xin(r1, k + 1));
+            a[ks][2] = pack_bf16(xin(r0, k + 8), xin(r0, k + 9));
+            a[ks][3] = pack_bf16(xin(r1, k + 8), xin(r1, k + 9));
+        }
+        float c[8][4];
+        for (int l = 0; l < nh; ++l) {
+            const float *bl = bias + l * kMmaW;
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int col = nt * 8 + 2 * t4;
+                c[nt][0] = c[nt][2] = bl[col];
+                c[nt][1] = c[nt][3] = bl[col + 1];
+            }
+            const int nks = l == 0 ? 2 : 4, ld = l == 0 ? kMmaP0 : kMmaPH;
+            const __nv_bfloat16 *W = l == 0 ? w0 : wh + (size_t)(l - 1) * kMmaW * kMmaPH;
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+                if (ks >= nks) break;
+#pragma unroll
+                for (int nt = 0; nt < 8; ++nt) {
+                    const __nv_bfloat16 *wr = W + (size_t)(nt * 8 + g) * ld + ks * 16 + 2 * t4;
+                    const unsigned b0 = *reinterpret_cast<const unsigned *>(wr);
+                    const unsigned b1 = *reinterpret_cast<const unsigned *>(wr + 8);
+                    mma_bf16(c[nt], a[ks], b0, b1);
+                }
+            }
+            // ReLU, BF16: the next layer's A fragments
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                auto rl = [](float v) { return v > 0.f ? v : 0.f; };
+                a[t][0] = pack_bf16(rl(c[2 * t][0]), rl(c[2 * t][1]));
+                a[t][1] = pack_bf16(rl(c[2 * t][2]), rl(c[2 * t][3]));
+                a[t][2] = pack_bf16(rl(c[2 * t + 1][0]), rl(c[2 * t + 1][1]));
+                a[t][3] = pack_bf16(rl(c[2 * t + 1][2]), rl(c[2 * t + 1][3]));
+            }
+        }
+        // output layer 64 -> 1 on the BF16 activations
+        float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int col = (2 * t + h) * 8 + 2 * t4;
+                const __nv_bfloat162 lo = *reinterpret_cast<const __nv_bfloat162 *>(&a[t][2 * h]);
+                const __nv_bfloat162 hi = *reinterpret_cast<const __nv_bfloat162 *>(&a[t][2 * h + 1]);
+                y0 += wout[col] * __low2float(lo) + wout[col + 1] * __high2float(lo);
+                y1 += wout[col] * __low2float(hi) + wout[col + 1] * __high2float(hi);
+            }
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+        if (t4 == 0) {
+            if (r0 < n) Y[r0] = wout[kMmaW] + y0;
+            if (r1 < n) Y[r1] = wout[kMmaW] + y1;
+        }
+    }
+}
+
+static bool mma_shape(const Dims &d) {
+    if (d.L < 2 || d.n[0] > 32 || d.n[d.L] != 1) return false;
+    for (int l = 1; l < d.L; ++l)
+        if (d.n[l] != kMmaW) return false;
+    return true;
+}
+
+static size_t mma_smem(const Dims &d) {
+    const int nh = d.L - 1;
+    return (size_t)kMmaW * kMmaP0 * 2 + (size_t)(nh - 1) * kMmaW * kMmaPH * 2 + (size_t)nh * kMmaW * 4 +
+           (kMmaW + 1) * 4 + 64 * 4;
 }
 
 __global__ void k_round_bf16(const float *w, float *wb, int n) {
@@ -256,6 +395,16 @@ extern "C" int hp_mlp_forward(hp_mlp *net, const float *d_x, int n, float *d_y, 
     if (!net || (n > 0 && (!d_x || !d_y)) || n < 0) return merr(HP_EINVAL, "bad argument");
     if (n == 0) return HP_OK;
     cudaStream_t st = (cudaStream_t)stream;
+    if (mma_shape(net->d)) {  // the learned corrections' shape: BF16 tensor cores
+        const size_t smm = mma_smem(net->d);
+        if (smm > 48 * 1024)
+            MCK(cudaFuncSetAttribute(k_mlp_forward_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smm));
+        const long groups = ((long)n + 15) / 16;
+        const int blocks = (int)std::min<long>((groups + 3) / 4, 148L * 16);
+        k_mlp_forward_mma<<<blocks, 128, smm, st>>>(net->d, net->wb, net->mean, net->istd, d_x, n, d_y);
+        MCK(cudaGetLastError());
+        return HP_OK;
+    }
     const size_t sm = fwd_smem(net);
     if (sm > 48 * 1024) MCK(cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_mlp_forward<<<(n + kThreads - 1) / kThreads, kThreads, sm, st>>>(net->d, net->wb, net->mean, net->istd, d_x, n,

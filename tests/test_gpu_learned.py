@@ -38,6 +38,29 @@ def test_gradients_match_cpu_oracle():
     assert np.max(np.abs(Y.cpu().numpy() - yo)) < 1e-4 * np.max(np.abs(yo))
 
 
+def test_tensor_core_forward_matches_cpu_oracle():
+    """The learned corrections' shape (17 -> 64 -> 64 -> 64 -> 1) runs its forward pass on the
+    BF16 tensor cores (k_mlp_forward_mma); against the numpy oracle it agrees up to the order
+    of the FP32 sums (an activation within FP32 rounding of a BF16 boundary may round the
+    other way, so the bound is norm-wise), for a sample count that is not a multiple of 16."""
+    import torch
+    widths = (17, 64, 64, 64, 1)
+    net = LR.MLP(widths, seed=5)
+    rng = np.random.default_rng(2)
+    n = 1000 + 7
+    X = rng.normal(size=(n, 17)).astype(np.float32)
+    net.set_norm(X.mean(0), X.std(0))
+    Xd = torch.from_numpy(X).cuda()
+    Y = torch.full((n, 1), np.nan, device="cuda")
+    net.forward(Xd.data_ptr(), Y.data_ptr(), n)
+    torch.cuda.synchronize()
+    y = Y.cpu().numpy()
+    yo = MO.forward(net.params().astype(np.float64), widths, X.mean(0), X.std(0), X)[-1]
+    assert np.all(np.isfinite(y))
+    assert np.linalg.norm(y - yo) / np.linalg.norm(yo) < 2e-3
+    assert np.max(np.abs(y - yo)) < 2e-2 * np.max(np.abs(yo))
+
+
 def test_training_reduces_loss():
     rng = np.random.default_rng(1)
     X = rng.normal(size=(4096, 17)).astype(np.float32)
