@@ -1061,22 +1061,40 @@ extern "C" int hp_gpu_sizes(const hp_gpu_ctx *c, int *nv, int *sm, int *im) {
     return HP_OK;
 }
 
-extern "C" int hp_gpu_upload_state(hp_gpu_ctx *c, const double *v, const double *s, const double *i) {
-    if (!c || !v) return HP_EINVAL;
+extern "C" int hp_gpu_enqueue_upload_state(hp_gpu_ctx *c, const double *v, const double *s, const double *i) {
+    if (!c || !v || (c->ls && !s) || (c->li && !i)) return HP_EINVAL;
     CK(cudaMemcpyAsync(c->st.ugv, v, c->lv * 8, cudaMemcpyHostToDevice, c->stream));
-    if (c->ls) { if (!s) return HP_EINVAL; CK(cudaMemcpyAsync(c->st.ugs, s, c->ls * 8, cudaMemcpyHostToDevice, c->stream)); }
-    if (c->li) { if (!i) return HP_EINVAL; CK(cudaMemcpyAsync(c->st.ugi, i, c->li * 8, cudaMemcpyHostToDevice, c->stream)); }
+    if (c->ls) CK(cudaMemcpyAsync(c->st.ugs, s, c->ls * 8, cudaMemcpyHostToDevice, c->stream));
+    if (c->li) CK(cudaMemcpyAsync(c->st.ugi, i, c->li * 8, cudaMemcpyHostToDevice, c->stream));
+    return HP_OK;
+}
+
+extern "C" int hp_gpu_upload_state(hp_gpu_ctx *c, const double *v, const double *s, const double *i) {
+    const int r = hp_gpu_enqueue_upload_state(c, v, s, i);
+    if (r) return r;
     CK(cudaStreamSynchronize(c->stream));
+    return HP_OK;
+}
+
+static int enqueue_download3(hp_gpu_ctx *c, const double *dv, const double *ds, const double *di, double *v,
+                             double *s, double *i) {
+    if (v) CK(cudaMemcpyAsync(v, dv, c->lv * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (s && c->ls) CK(cudaMemcpyAsync(s, ds, c->ls * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (i && c->li) CK(cudaMemcpyAsync(i, di, c->li * 8, cudaMemcpyDeviceToHost, c->stream));
     return HP_OK;
 }
 
 static int download3(hp_gpu_ctx *c, const double *dv, const double *ds, const double *di, double *v, double *s,
                      double *i) {
-    if (v) CK(cudaMemcpyAsync(v, dv, c->lv * 8, cudaMemcpyDeviceToHost, c->stream));
-    if (s && c->ls) CK(cudaMemcpyAsync(s, ds, c->ls * 8, cudaMemcpyDeviceToHost, c->stream));
-    if (i && c->li) CK(cudaMemcpyAsync(i, di, c->li * 8, cudaMemcpyDeviceToHost, c->stream));
+    const int r = enqueue_download3(c, dv, ds, di, v, s, i);
+    if (r) return r;
     CK(cudaStreamSynchronize(c->stream));
     return HP_OK;
+}
+
+extern "C" int hp_gpu_enqueue_download_residual(hp_gpu_ctx *c, double *v, double *s, double *i) {
+    if (!c) return HP_EINVAL;
+    return enqueue_download3(c, c->st.resv, c->st.ress, c->st.resi, v, s, i);
 }
 
 extern "C" int hp_gpu_download_state(hp_gpu_ctx *c, double *v, double *s, double *i) {

@@ -109,7 +109,7 @@ def lib():
         L.hp_gpu_autotune.argtypes = [P, _I]
         L.hp_gpu_get_tuning.argtypes = [P, P, P]
         L.hp_gpu_sizes.argtypes = [P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]
-        for name in ("hp_gpu_upload_state",):
+        for name in ("hp_gpu_upload_state", "hp_gpu_enqueue_upload_state", "hp_gpu_enqueue_download_residual"):
             getattr(L, name).argtypes = [P, P, P, P]
         for name in ("hp_gpu_download_state", "hp_gpu_download_residual"):
             getattr(L, name).argtypes = [P, P, P, P]

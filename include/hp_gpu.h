@@ -215,6 +215,13 @@ int hp_gpu_set_element_kernel(hp_gpu_ctx *ctx, int kind);
  * update(). */
 int hp_gpu_enqueue_rsdl(hp_gpu_ctx *ctx, int stage);
 int hp_gpu_enqueue_update(hp_gpu_ctx *ctx);
+/* Stream-ordered state upload and residual download: the copies are queued on the
+ * context's stream and the call returns at once. The host arrays must stay valid, and for
+ * the copies to run asynchronously they must be page-locked, until hp_gpu_sync(ctx)
+ * returns. Two contexts on two streams can then overlap one residual's copies with
+ * another's kernels. */
+int hp_gpu_enqueue_upload_state(hp_gpu_ctx *ctx, const double *ugv, const double *ugs, const double *ugi);
+int hp_gpu_enqueue_download_residual(hp_gpu_ctx *ctx, double *resv, double *ress, double *resi);
 /* The element-residual kernel alone (the loop over elements of tri_hp::rsdl,
  * nstage.cpp:52-73: ugtouht, element_rsdl, lftog), for timing it in isolation. */
 int hp_gpu_enqueue_element_rsdl(hp_gpu_ctx *ctx, int stage);

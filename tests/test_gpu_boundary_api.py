@@ -57,3 +57,35 @@ def test_rsdl_fp32_precision_matches_fp64_to_single_precision(kind, p):
     err = np.max(np.abs(out[1] - out[0])) / np.max(np.abs(out[0]))
     assert 0.0 < err < 1e-4, err
     g.close()
+
+
+def test_stream_ordered_upload_rsdl_download_matches_the_synchronous_calls():
+    """hp_gpu_enqueue_upload_state / hp_gpu_enqueue_rsdl / hp_gpu_enqueue_download_residual
+    queued on two contexts of the same level, each with its own pinned buffers, give the
+    residual of the synchronous calls bit for bit."""
+    import ctypes
+    import torch
+    from hpb import _lib as L
+    pr = hpb.kovasznay_ins(n=8, p=4)
+    lib = L.lib()
+    ref = pr.gpu()
+    assert ref.setup_preconditioner() == 0
+    ref.rsdl(pr.phys.nstage)
+    want = ref.residual()
+    ref.close()
+    streams = [torch.cuda.Stream() for _ in range(2)]  # kept alive while the contexts use them
+    ctxs = [pr.gpu(stream=ctypes.c_void_p(s.cuda_stream)) for s in streams]
+    outs = []
+    for g in ctxs:
+        assert g.setup_preconditioner() == 0
+        hin = [torch.from_numpy(a.copy()).pin_memory() for a in (pr.ugv, pr.ugs, pr.ugi)]
+        hout = [torch.empty(a.shape, dtype=torch.float64).pin_memory() for a in (pr.ugv, pr.ugs, pr.ugi)]
+        L.check(lib.hp_gpu_enqueue_upload_state(g.h, *[ctypes.c_void_p(t.data_ptr()) for t in hin]), "up")
+        L.check(lib.hp_gpu_enqueue_rsdl(g.h, pr.phys.nstage), "rsdl")
+        L.check(lib.hp_gpu_enqueue_download_residual(g.h, *[ctypes.c_void_p(t.data_ptr()) for t in hout]), "down")
+        outs.append((hin, hout))
+    for g, (hin, hout) in zip(ctxs, outs):
+        L.check(lib.hp_gpu_sync(g.h), "sync")
+        for a, b in zip(hout, want):
+            assert np.array_equal(a.numpy(), b)
+        g.close()
