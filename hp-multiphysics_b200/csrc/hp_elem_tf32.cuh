@@ -38,13 +38,13 @@ struct InsTf32 {
     static constexpr int MINB = P <= 4 ? 4 : 3;
     static constexpr int NG = NT < 8 ? NT : 8;
     // B fragments: two floats per lane per MMA. DER: the strong residual (derivr + derivs)
-    // as tensor products of the 1D operators, A fragments (four floats per lane per k-step)
-    // of [Ar | As1] (2 KR k-steps) and As2 (KR k-steps); the point data are the B operands,
-    // columns (triangle, variable, point of the other direction)
+    // as tensor products of the 1D operators, transposed so that the point data are the A
+    // operand: rows (triangle, variable, point of the other direction), 16 per m-tile, and
+    // the operators the B operand, B fragments of [Ar | As1]^T (2 KR k-steps) and As2^T (KR
+    // k-steps), NTI n-tiles of 8 operator rows each
     static constexpr size_t PROJ_LEN = (size_t)3 * NT * KS * 64, INT_LEN = (size_t)NT2 * KS2 * 64;
-    static constexpr int KR = (G + 7) / 8, NCOL = 12 * G, NTB = (NCOL + 7) / 8;
-    static_assert(G <= 16, "one m-tile of 16 rows per 1D operator");
-    static constexpr size_t DER_LEN = (size_t)3 * KR * 32 * 4;
+    static constexpr int KR = (G + 7) / 8, NTI = KR, NCOL = 12 * G, MTS = (NCOL + 15) / 16;
+    static constexpr size_t DER_LEN = (size_t)3 * KR * NTI * 64;
     static constexpr int IDX = 12;  // staged mesh integers per triangle: pnt[3], seg[3], sgn[3]
     // per triangle: metrics d00, d01, d10, d11, mu / |J|, 2 nu / h, adis h / |J|, unused
     static constexpr int GEO = 8;
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
         for (int it = 0; it < (4 * NV * T + 31) / 32; ++it) {
             const int w = lane + 32 * it;
             if (w >= 4 * NV * T) continue;
-            const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
+            const int e = w / (NV * T), r = w - e * (NV * T), m = r / NV, n = r - m * NV;  // memory order
             const int *ix = midx + e * M::IDX;
             float val = 0.f;
             if (ACT(e)) {
@@ -425,63 +425,80 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             scatter(c, 0);
         } else {
             // ---- strong residual of FI + FX at the points (derivr / derivs, proj.cpp:339-402)
-            //      on TF32 as tensor products of the 1D operators: part 1 rows i, columns
-            //      (triangle, variable, j): n0(j) (Ar fr + As1 fs); part 2 rows j, columns
-            //      (triangle, variable, i): As2 fs^T; into PD
+            //      on TF32 as tensor products of the 1D operators, the point data as the A
+            //      operand: part 1 rows (triangle, variable, j), k = q of [fr | fs], columns i:
+            //      res(i, j) = n0(j) (Ar fr + As1 fs)(i, j); part 2 rows (triangle, variable, i),
+            //      k = l of fs, columns j: res(i, j) += (As2 fs^T)(j, i); into PD
             {
-                const float4 *AR = reinterpret_cast<const float4 *>(derB);  // [Ar | As1] then As2
                 auto col = [&](int n, int &e, int &var, int &j) {
                     e = n / (3 * G);
                     const int rem = n - e * 3 * G;
                     var = rem / G;
                     j = rem - var * G;
                 };
-                auto a4 = [&](const float4 v, unsigned (&a)[4]) {
-                    a[0] = __float_as_uint(v.x); a[1] = __float_as_uint(v.y);
-                    a[2] = __float_as_uint(v.z); a[3] = __float_as_uint(v.w);
-                };
-                // the A fragments of the 1D operators, the same for every column tile
-                float4 afr[3 * M::KR];
+                // the B fragments of the transposed 1D operators, the same for every m-tile
+                float2 bop[3 * M::KR][M::NTI];
 #pragma unroll
-                for (int k = 0; k < 3 * M::KR; ++k) afr[k] = __ldg(AR + (size_t)k * 32 + lane);
+                for (int k = 0; k < 3 * M::KR; ++k)
+#pragma unroll
+                    for (int nt = 0; nt < M::NTI; ++nt) bop[k][nt] = __ldg(derB + ((size_t)k * M::NTI + nt) * 32 + lane);
 #pragma unroll
                 for (int part = 0; part < 2; ++part) {
                     const int nks = part ? M::KR : 2 * M::KR;
-#pragma unroll 1
-                    for (int nt = 0; nt < M::NTB; ++nt) {
-                        int e, var, x;
-                        const int n = nt * 8 + grp;
-                        col(n < M::NCOL ? n : 0, e, var, x);
-                        const bool colok = n < M::NCOL;
-                        const float *fi = FI(e) + var * VS, *fx = FX(e) + var * VS;
-                        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                    for (int mt = 0; mt < M::MTS; ++mt) {
+                        const int r0 = mt * 16 + grp, r1 = r0 + 8;
+                        const bool ok0 = r0 < M::NCOL, ok1 = r1 < M::NCOL;
+                        int e0, v0, x0, e1, v1, x1;
+                        col(ok0 ? r0 : 0, e0, v0, x0);
+                        col(ok1 ? r1 : 0, e1, v1, x1);
+                        const float *fi0 = FI(e0) + v0 * VS, *fx0 = FX(e0) + v0 * VS;
+                        const float *fi1 = FI(e1) + v1 * VS, *fx1 = FX(e1) + v1 * VS;
+                        float c[M::NTI][4];
+#pragma unroll
+                        for (int nt = 0; nt < M::NTI; ++nt) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.f;
 #pragma unroll
                         for (int ks = 0; ks < nks; ++ks) {
-                            unsigned a[4];
-                            a4(afr[(part ? 2 * M::KR : 0) + ks], a);
-                            float2 bv = make_float2(0.f, 0.f);
-                            if (part == 0) {  // k = q of [fr | fs] at column point j = x
+                            // the offsets of (row, k) in its flux block: k = q (part 1) of
+                            // [fr | fs] at point x, or k = l (part 2) of fs at point x
+                            int o00, o10, o01, o11;
+                            bool k0, k1;
+                            if (part == 0) {
                                 const int blk = ks / M::KR, q0 = (ks - blk * M::KR) * 8 + tig, q1 = q0 + 4;
-                                if (colok && q0 < G) bv.x = fi[blk * GG + q0 * G + x] + fx[blk * GG + q0 * G + x];
-                                if (colok && q1 < G) bv.y = fi[blk * GG + q1 * G + x] + fx[blk * GG + q1 * G + x];
-                            } else {  // k = l of fs at column point i = x
+                                k0 = q0 < G;
+                                k1 = q1 < G;
+                                o00 = blk * GG + q0 * G + x0; o10 = blk * GG + q0 * G + x1;
+                                o01 = blk * GG + q1 * G + x0; o11 = blk * GG + q1 * G + x1;
+                            } else {
                                 const int l0 = ks * 8 + tig, l1 = l0 + 4;
-                                if (colok && l0 < G) bv.x = fi[GG + x * G + l0] + fx[GG + x * G + l0];
-                                if (colok && l1 < G) bv.y = fi[GG + x * G + l1] + fx[GG + x * G + l1];
+                                k0 = l0 < G;
+                                k1 = l1 < G;
+                                o00 = GG + x0 * G + l0; o10 = GG + x1 * G + l0;
+                                o01 = GG + x0 * G + l1; o11 = GG + x1 * G + l1;
                             }
-                            bv.x = __uint_as_float(f2tf32(bv.x));
-                            bv.y = __uint_as_float(f2tf32(bv.y));
-                            mma_tf32(c, a[0], a[1], a[2], a[3], bv);
-                        }
+                            const unsigned a0 = f2tf32((ok0 && k0) ? fi0[o00] + fx0[o00] : 0.f);
+                            const unsigned a1 = f2tf32((ok1 && k0) ? fi1[o10] + fx1[o10] : 0.f);
+                            const unsigned a2 = f2tf32((ok0 && k1) ? fi0[o01] + fx0[o01] : 0.f);
+                            const unsigned a3 = f2tf32((ok1 && k1) ? fi1[o11] + fx1[o11] : 0.f);
 #pragma unroll
-                        for (int r = 0; r < 4; ++r) {
-                            const int row = grp + (r >> 1) * 8, nc = nt * 8 + tig * 2 + (r & 1);
-                            if (row >= G || nc >= M::NCOL) continue;
-                            int e2, v2, x2;
-                            col(nc, e2, v2, x2);
-                            if (part == 0) PD(e2)[v2 * QP + row * G + x2] = c[r] * tb.n0[x2];
-                            else PD(e2)[v2 * QP + x2 * G + row] += c[r];
+                            for (int nt = 0; nt < M::NTI; ++nt)
+                                mma_tf32(c[nt], a0, a1, a2, a3, bop[(part ? 2 * M::KR : 0) + ks][nt]);
                         }
+                        // c[nt][h]: row r0, operator row nt * 8 + 2 tig + h; c[nt][2 + h]: row r1
+#pragma unroll
+                        for (int nt = 0; nt < M::NTI; ++nt)
+#pragma unroll
+                            for (int h = 0; h < 2; ++h) {
+                                const int n = nt * 8 + 2 * tig + h;
+                                if (n >= G) continue;
+                                if (part == 0) {
+                                    if (ok0) PD(e0)[v0 * QP + n * G + x0] = c[nt][h] * tb.n0[x0];
+                                    if (ok1) PD(e1)[v1 * QP + n * G + x1] = c[nt][2 + h] * tb.n0[x1];
+                                } else {
+                                    if (ok0) PD(e0)[v0 * QP + x0 * G + n] += c[nt][h];
+                                    if (ok1) PD(e1)[v1 * QP + x1 * G + n] += c[nt][2 + h];
+                                }
+                            }
                     }
                     __syncwarp();
                 }

@@ -246,19 +246,20 @@ void build_ins_tf32(const hp_basis_tables &b, std::vector<float> &ops, InsMmaSma
                 ib[at] = to_tf32(wgt(k, m));
                 ib[at + 1] = to_tf32(wgt(k + 4, m));
             }
-    // A fragments of the 1D derivative operators (mma.m16n8k8: lane l holds A[g][t], A[g + 8][t],
-    // A[g][t + 4], A[g + 8][t + 4] with g = l >> 2, t = l & 3 + 8 ks): [Ar | As1] then As2
+    // B fragments of the transposed 1D derivative operators (mma.m16n8k8 .col: lane l holds
+    // B[k = t][n = g], B[k = t + 4][n = g] with g = l >> 2 + 8 nt, t = l & 3 + 8 kb and
+    // B[k][n] = A[n][k]): [Ar | As1]^T in 2 KR k-steps, then As2^T in KR k-steps
     float *db = ops.data() + M::PROJ_LEN + M::INT_LEN;
-    for (int part = 0; part < 2; ++part)
-        for (int ks = 0; ks < (part ? M::KR : 2 * M::KR); ++ks)
+    for (int kk = 0; kk < 3 * M::KR; ++kk)
+        for (int nt = 0; nt < M::NTI; ++nt)
             for (int l = 0; l < 32; ++l) {
-                const int blk = part ? 2 : ks / M::KR, kb = part ? ks : ks - (ks / M::KR) * M::KR;
-                const int g = l >> 2, t = (l & 3) + kb * 8;
-                float *a = db + (((size_t)(part ? 2 * M::KR : 0) + ks) * 32 + l) * 4;
-                a[0] = to_tf32(deriv_op(b, G, blk, g, t));
-                a[1] = to_tf32(deriv_op(b, G, blk, g + 8, t));
-                a[2] = to_tf32(deriv_op(b, G, blk, g, t + 4));
-                a[3] = to_tf32(deriv_op(b, G, blk, g + 8, t + 4));
+                const bool part2 = kk >= 2 * M::KR;
+                const int ks = part2 ? kk - 2 * M::KR : kk;
+                const int blk = part2 ? 2 : ks / M::KR, kb = part2 ? ks : ks - (ks / M::KR) * M::KR;
+                const int n = nt * 8 + (l >> 2), k = kb * 8 + (l & 3);
+                float *bb = db + (((size_t)kk * M::NTI + nt) * 32 + l) * 2;
+                bb[0] = to_tf32(deriv_op(b, G, blk, n, k));
+                bb[1] = to_tf32(deriv_op(b, G, blk, n, k + 4));
             }
     for (int i = 0; i < G; ++i) {
         sm.dltx[i] = (float)b.dltx[i]; sm.dltn[i] = (float)b.dltn[i];
