@@ -50,6 +50,7 @@ struct InsTf32 {
     static constexpr int GEO = 8;
     static constexpr size_t SMEM_IDX = (size_t)WPC * 4 * (IDX * sizeof(int) + GEO * sizeof(float));
     static_assert(4 * T <= 4 * QP, "gathered modes must fit the PD block");
+    static_assert(2 * NV * T <= 4 * QP, "the staged residual parts must fit the PD block");
 };
 
 __device__ __forceinline__ unsigned f2tf32(float x) {
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
                     int stage, int zero_rr, int diff) {
     using M = InsTf32<P>;
     constexpr int G = M::G, GG = M::GG, T = M::T, BM = M::BM, IM = M::IM, NV = 3, QP = M::QP, VS = M::VS;
-    constexpr int SM = (M::SM > 0 ? M::SM : 1);
+    constexpr int SM = (M::SM > 0 ? M::SM : 1), IMD = (IM > 0 ? IM : 1);  // divisors
     extern __shared__ __align__(16) unsigned char smem_raw[];
     InsMmaSmallF<P> &tb = *reinterpret_cast<InsMmaSmallF<P> *>(smem_raw);
     {
@@ -213,26 +214,37 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             gg[6] = (float)(ph.adis * tg[5] * tg[4]);
         }
         __syncwarp();
-        // ---- gather the modes (ugtouht, gtol.cpp:14-55) into the PD block
+        // ---- gather the modes (ugtouht, gtol.cpp:14-55) into the PD block, one mode kind per
+        //      loop so that the lanes of an iteration take the same branch: the vertex values,
+        //      the side modes (SM NV consecutive values per side), the interior modes (IM NV
+        //      consecutive values per triangle)
+        {
+            constexpr int NVX = 4 * 3 * NV, NSD = 4 * 3 * M::SM * NV, NIN = 4 * IM * NV;
 #pragma unroll
-        for (int it = 0; it < (4 * NV * T + 31) / 32; ++it) {
-            const int w = lane + 32 * it;
-            if (w >= 4 * NV * T) continue;
-            const int e = w / (NV * T), r = w - e * (NV * T), m = r / NV, n = r - m * NV;  // memory order
-            const int *ix = midx + e * M::IDX;
-            float val = 0.f;
-            if (ACT(e)) {
-                if (m < 3) {
-                    val = st.ugv[ix[m] * NV + n];
-                } else if (m < BM) {
-                    const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
-                    val = st.ugs[(ix[3 + i] * SM + kk) * NV + n];
-                    if ((kk & 1) && ix[6 + i] < 0) val = -val;
-                } else {
-                    val = st.ugi[((size_t)TE(e) * IM + (m - BM)) * NV + n];
-                }
+            for (int it = 0; it < (NVX + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= NVX) continue;
+                const int e = w / (3 * NV), r = w - e * (3 * NV), m = r / NV, n = r - m * NV;
+                PD(e)[n * T + m] = ACT(e) ? st.ugv[midx[e * M::IDX + m] * NV + n] : 0.f;
             }
-            PD(e)[n * T + m] = val;
+#pragma unroll
+            for (int it = 0; it < (NSD + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= NSD) continue;
+                const int b = w / (SM * NV), r = w - b * (SM * NV), e = b / 3, i = b - e * 3, kk = r / NV,
+                          n = r - kk * NV;
+                const int *ix = midx + e * M::IDX;
+                float val = ACT(e) ? st.ugs[ix[3 + i] * (SM * NV) + r] : 0.f;
+                if ((kk & 1) && ix[6 + i] < 0) val = -val;
+                PD(e)[n * T + 3 + i * SM + kk] = val;
+            }
+#pragma unroll
+            for (int it = 0; it < (NIN + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= NIN) continue;
+                const int e = w / (IMD * NV), r = w - e * (IMD * NV), k = r / NV, n = r - k * NV;
+                PD(e)[n * T + BM + k] = ACT(e) ? st.ugi[(size_t)TE(e) * (IMD * NV) + r] : 0.f;
+            }
         }
         __syncwarp();
         // ---- projection (TF32): A rows (triangle, variable), B = dense operators
@@ -337,83 +349,72 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             }
         }
         __syncwarp();
-        // lftog of the two fragment rows a lane holds: vertex and side modes by FP32 atomics,
-        // interiors directly. part 0: imaginary -> res; part 1: real (x beta) -> res_r
-        auto scatter = [&](const float (&c)[M::NT2][4], int part) {
-            if (rv >= 3) return;
+        // lftog (gtol.cpp:364-402) through shared memory: the lanes' fragment values are staged
+        // in the PD block (free after SUPG) as [imaginary | real x beta][variable][mode] per
+        // triangle, then scattered one mode kind per loop: vertex and side modes by FP32
+        // atomics (imaginary -> res, real -> res_r), interiors directly (two parts: res =
+        // im + dres + res_r with res_r = (1 - beta) res_r + re; imaginary only (beta = 0):
+        // res = im + (1 - beta) res_r + dres)
+        auto scatter = [&](const float (&ci)[M::NT2][4], const float (&cr)[M::NT2][4], bool two) {
+            if (rv < 3) {
 #pragma unroll
-            for (int hh = 0; hh < 2; ++hh) {  // rows grp (triangle ra) and grp + 8 (triangle ra + 2)
-                const int e = ra + 2 * hh;
-                if (!ACT(e)) continue;
-                const int t = TE(e);
-                const int *ix = midx + e * M::IDX;
+                for (int hh = 0; hh < 2; ++hh)
 #pragma unroll
-                for (int nt = 0; nt < M::NT2; ++nt)
+                    for (int nt = 0; nt < M::NT2; ++nt)
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int m = nt * 8 + tig * 2 + h;
-                        if (m >= T) continue;
-                        float val = c[nt][2 * hh + h];
-                        if (part) val *= beta;
-                        if (m < 3) {
-                            atomicAdd((part ? st.rrv : st.resv) + ix[m] * NV + rv, val);
-                        } else if (m < BM) {
-                            const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
-                            if ((kk & 1) && ix[6 + i] < 0) val = -val;
-                            atomicAdd((part ? st.rrs : st.ress) + (ix[3 + i] * SM + kk) * NV + rv, val);
-                        } else {
-                            const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
-                            if (!part) {
-                                const float src = st.dresi ? st.dresi[gi] : 0.f;
-                                if (beta > 0.f) st.resi[gi] = val + src;
-                                else st.resi[gi] = val + st.rri[gi] * omb + src;
-                            } else {
-                                const float rr = st.rri[gi] * omb + val;
-                                st.rri[gi] = rr;
-                                st.resi[gi] += rr;
-                            }
+                        for (int h = 0; h < 2; ++h) {
+                            const int m = nt * 8 + tig * 2 + h;
+                            if (m >= T) continue;
+                            float *d = PD(ra + 2 * hh) + rv * T + m;
+                            d[0] = ci[nt][2 * hh + h];
+                            if (two) d[NV * T] = cr[nt][2 * hh + h] * beta;
                         }
-                    }
             }
-        };
-        // lftog of both parts at once (beta > 0): the side sign and the index are found once
-        // for the imaginary value (-> res) and the beta-scaled real value (-> res_r);
-        // interiors: res = im + dres + res_r with res_r = (1 - beta) res_r + re
-        auto scatter2 = [&](const float (&ci)[M::NT2][4], const float (&cr)[M::NT2][4]) {
-            if (rv >= 3) return;
+            __syncwarp();
+            constexpr int NVX = 4 * 3 * NV, NSD = 4 * 3 * M::SM * NV, NIN = 4 * IM * NV;
 #pragma unroll
-            for (int hh = 0; hh < 2; ++hh) {
-                const int e = ra + 2 * hh;
+            for (int it = 0; it < (NVX + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= NVX) continue;
+                const int e = w / (3 * NV), r = w - e * (3 * NV), m = r / NV, n = r - m * NV;
                 if (!ACT(e)) continue;
-                const int t = TE(e);
+                const int g = midx[e * M::IDX + m] * NV + n;
+                atomicAdd(st.resv + g, PD(e)[n * T + m]);
+                if (two) atomicAdd(st.rrv + g, PD(e)[NV * T + n * T + m]);
+            }
+#pragma unroll
+            for (int it = 0; it < (NSD + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= NSD) continue;
+                const int b = w / (SM * NV), r = w - b * (SM * NV), e = b / 3, i = b - e * 3, kk = r / NV,
+                          n = r - kk * NV;
+                if (!ACT(e)) continue;
                 const int *ix = midx + e * M::IDX;
+                const int m = 3 + i * SM + kk, g = ix[3 + i] * (SM * NV) + r;
+                const bool flip = (kk & 1) && ix[6 + i] < 0;
+                const float vi = PD(e)[n * T + m];
+                atomicAdd(st.ress + g, flip ? -vi : vi);
+                if (two) {
+                    const float vr = PD(e)[NV * T + n * T + m];
+                    atomicAdd(st.rrs + g, flip ? -vr : vr);
+                }
+            }
 #pragma unroll
-                for (int nt = 0; nt < M::NT2; ++nt)
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int m = nt * 8 + tig * 2 + h;
-                        if (m >= T) continue;
-                        float vi = ci[nt][2 * hh + h], vr = cr[nt][2 * hh + h] * beta;
-                        if (m < 3) {
-                            atomicAdd(st.resv + ix[m] * NV + rv, vi);
-                            atomicAdd(st.rrv + ix[m] * NV + rv, vr);
-                        } else if (m < BM) {
-                            const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
-                            if ((kk & 1) && ix[6 + i] < 0) {
-                                vi = -vi;
-                                vr = -vr;
-                            }
-                            const int g = (ix[3 + i] * SM + kk) * NV + rv;
-                            atomicAdd(st.ress + g, vi);
-                            atomicAdd(st.rrs + g, vr);
-                        } else {
-                            const size_t gi = ((size_t)t * IM + (m - BM)) * NV + rv;
-                            const float src = st.dresi ? st.dresi[gi] : 0.f;
-                            const float rr = st.rri[gi] * omb + vr;
-                            st.rri[gi] = rr;
-                            st.resi[gi] = (vi + src) + rr;
-                        }
-                    }
+            for (int it = 0; it < (NIN + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= NIN) continue;
+                const int e = w / (IMD * NV), r = w - e * (IMD * NV), k = r / NV, n = r - k * NV;
+                if (!ACT(e)) continue;
+                const size_t gi = (size_t)TE(e) * (IMD * NV) + r;
+                const float vi = PD(e)[n * T + BM + k];
+                const float src = st.dresi ? st.dresi[gi] : 0.f;
+                if (two) {
+                    const float rr = st.rri[gi] * omb + PD(e)[NV * T + n * T + BM + k];
+                    st.rri[gi] = rr;
+                    st.resi[gi] = (vi + src) + rr;
+                } else {
+                    st.resi[gi] = vi + st.rri[gi] * omb + src;
+                }
             }
         };
         // imaginary part -> res; with a real part (beta > 0) it is done together with that one
@@ -422,7 +423,7 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             float c[M::NT2][4];
             warp_gemm_tf32<M::KS2, M::NT2>(FI(ra) + rvv * VS, FI(ra + 2) + rvv * VS, nullptr, nullptr, intB, tig,
                                             lane, c);
-            scatter(c, 0);
+            scatter(c, c, false);
         } else {
             // ---- strong residual of FI + FX at the points (derivr / derivs, proj.cpp:339-402)
             //      on TF32 as tensor products of the 1D operators, the point data as the A
@@ -540,7 +541,7 @@ __global__ void __launch_bounds__(InsTf32<P>::WPC * 32, InsTf32<P>::MINB)
             float ci[M::NT2][4], c[M::NT2][4];
             warp_gemm2_tf32<M::KS2, M::NT2>(FI(ra) + rvv * VS, FI(ra + 2) + rvv * VS, FX(ra) + rvv * VS,
                                              FX(ra + 2) + rvv * VS, intB, tig, lane, ci, c);
-            scatter2(ci, c);
+            scatter(ci, c, true);
         }
         __syncwarp();
     }
