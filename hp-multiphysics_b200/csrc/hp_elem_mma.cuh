@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
     using M = InsMma<P>;
     constexpr int G = M::G, GG = M::GG, T = M::T, BM = M::BM, IM = M::IM, NV = 3, QP = M::QP, VS = M::VS;
     constexpr int SM = (M::SM > 0 ? M::SM : 1);  // side-mode stride (unused when p = 1)
+    constexpr int IMD = (IM > 0 ? IM : 1);        // interior-mode stride (unused when p < 3)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     InsMmaSmall<P> &tb = *reinterpret_cast<InsMmaSmall<P> *>(smem_raw);
     {
@@ -180,28 +181,37 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
             midx[e * M::IDX + k] = src ? src[3 * t + c] : 0;
         }
         __syncwarp();
-        // ---- gather (ugtouht, gtol.cpp:14-55) into the PD block
-        constexpr int NGATH = (2 * NV * T + 31) / 32;
+        // ---- gather (ugtouht, gtol.cpp:14-55) into the PD block, one mode kind per loop so that
+        //      the lanes of an iteration take the same branch and read consecutive values: the
+        //      vertex values, the side modes (SM NV per side), the interior modes (IM NV per
+        //      triangle)
+        {
+            constexpr int NVX = 2 * 3 * NV, NSD = 2 * 3 * M::SM * NV, NIN = 2 * IM * NV;
 #pragma unroll
-        for (int k = 0; k < NGATH; ++k) {
-            const int w = lane + 32 * k;
-            if (w >= 2 * NV * T) continue;
-            // item order (triangle, mode, variable): consecutive lanes read consecutive values
-            const int e = w / (NV * T), r = w - e * (NV * T), m = r / NV, n = r - m * NV;
-            const int *ix = midx + e * M::IDX;
-            double val = 0.0;
-            if (ACT(e)) {
-                if (m < 3) {
-                    val = st.ugv[ix[m] * NV + n];
-                } else if (m < BM) {
-                    const int i = (m - 3) / SM, kk = (m - 3) - i * SM;
-                    val = st.ugs[(ix[3 + i] * SM + kk) * NV + n];
-                    if ((kk & 1) && ix[6 + i] < 0) val = -val;
-                } else {
-                    val = st.ugi[((size_t)TE(e) * IM + (m - BM)) * NV + n];
-                }
+            for (int it = 0; it < (NVX + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= NVX) continue;
+                const int e = w / (3 * NV), r = w - e * (3 * NV), m = r / NV, n = r - m * NV;
+                PD(e)[n * T + m] = ACT(e) ? st.ugv[midx[e * M::IDX + m] * NV + n] : 0.0;
             }
-            PD(e)[n * T + m] = val;
+#pragma unroll
+            for (int it = 0; it < (NSD + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= NSD) continue;
+                const int b = w / (SM * NV), r = w - b * (SM * NV), e = b / 3, i = b - e * 3, kk = r / NV,
+                          n = r - kk * NV;
+                const int *ix = midx + e * M::IDX;
+                double val = ACT(e) ? st.ugs[ix[3 + i] * (SM * NV) + r] : 0.0;
+                if ((kk & 1) && ix[6 + i] < 0) val = -val;
+                PD(e)[n * T + 3 + i * SM + kk] = val;
+            }
+#pragma unroll
+            for (int it = 0; it < (NIN + 31) / 32; ++it) {
+                const int w = lane + 32 * it;
+                if (w >= NIN) continue;
+                const int e = w / (IMD * NV), r = w - e * (IMD * NV), k = r / NV, n = r - k * NV;
+                PD(e)[n * T + BM + k] = ACT(e) ? st.ugi[(size_t)TE(e) * (IMD * NV) + r] : 0.0;
+            }
         }
         // geometry of both triangles into the warp's geo block, from the per-triangle
         // constants (Mesh::tgeo: ldcrd(n,0) = (v2-v1)/2, ldcrd(n,1) = (v0-v1)/2, 1 / |J|, and
@@ -393,9 +403,11 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
         } else {
             // ---- strong residual at the points (derivr + derivs of the full fluxes FI + FX,
             //      proj.cpp:339-402) on the tensor cores as tensor products of the 1D
-            //      operators: res(i, j) = n0(j) (Ar fr + As1 fs)(i, j) + (As2 fs^T)(j, i), the
-            //      columns of the B operand being (triangle, variable, point of the other
-            //      direction); into PD
+            //      operators, the point data as the A operand: part 1 rows (triangle, variable,
+            //      j), k = q of [fr | fs], columns i: res(i, j) = n0(j) (Ar fr + As1 fs)(i, j);
+            //      part 2 rows (triangle, variable, i), k = l of fs, columns j: res(i, j) +=
+            //      (As2 fs^T)(j, i); into PD. The operator fragments are B operands here:
+            //      lane (g, t) holds A[8 nt + g][4 ks + t] = B[k = t][n = g] of the transpose.
             {
                 const double *AR = derB, *AS = derB + M::MT * 2 * M::KR * 32;
                 auto col = [&](int n, int &e, int &var, int &j) {
@@ -404,76 +416,59 @@ __global__ void __launch_bounds__(InsMma<P>::WPC * 32, InsMma<P>::MINB)
                     var = rem / G;
                     j = rem - var * G;
                 };
-                // the A fragments of the 1D operators, the same for every column tile
-                double ar[M::MT][2 * M::KR], as2[M::MT][M::KR];
+                double br[M::MT][2 * M::KR], bs2[M::MT][M::KR];
 #pragma unroll
-                for (int mt = 0; mt < M::MT; ++mt) {
+                for (int nt = 0; nt < M::MT; ++nt) {
 #pragma unroll
-                    for (int ks = 0; ks < 2 * M::KR; ++ks) ar[mt][ks] = __ldg(AR + ((size_t)mt * 2 * M::KR + ks) * 32 + lane);
+                    for (int ks = 0; ks < 2 * M::KR; ++ks) br[nt][ks] = __ldg(AR + ((size_t)nt * 2 * M::KR + ks) * 32 + lane);
 #pragma unroll
-                    for (int ks = 0; ks < M::KR; ++ks) as2[mt][ks] = __ldg(AS + ((size_t)mt * M::KR + ks) * 32 + lane);
+                    for (int ks = 0; ks < M::KR; ++ks) bs2[nt][ks] = __ldg(AS + ((size_t)nt * M::KR + ks) * 32 + lane);
                 }
-                // part 1: rows i, columns (e, var, j)
+                constexpr int MTS = (M::NCOL + 7) / 8;
 #pragma unroll
-                for (int nt = 0; nt < M::NTB; ++nt) {
-                    int e, var, j;
-                    const int n = nt * 8 + grow;
-                    col(n < M::NCOL ? n : 0, e, var, j);
-                    const bool colok = n < M::NCOL;
-                    const double *fi = FI(e) + var * VS, *fx = FX(e) + var * VS;
-                    double c[M::MT][2];
+                for (int part = 0; part < 2; ++part) {
 #pragma unroll
-                    for (int mt = 0; mt < M::MT; ++mt) c[mt][0] = c[mt][1] = 0.0;
+                    for (int mt = 0; mt < MTS; ++mt) {
+                        const int r = mt * 8 + grow;
+                        const bool ok = r < M::NCOL;
+                        int e, var, x;
+                        col(ok ? r : 0, e, var, x);
+                        const double *fi = FI(e) + var * VS, *fx = FX(e) + var * VS;
+                        double c[M::MT][2];
 #pragma unroll
-                    for (int ks = 0; ks < 2 * M::KR; ++ks) {
-                        const int blk = ks / M::KR, q = (ks - blk * M::KR) * 4 + gcol;
-                        const int off = blk * GG + q * G + j;
-                        const double bv = (colok && q < G) ? fi[off] + fx[off] : 0.0;
+                        for (int nt = 0; nt < M::MT; ++nt) c[nt][0] = c[nt][1] = 0.0;
+                        if (part == 0) {
 #pragma unroll
-                        for (int mt = 0; mt < M::MT; ++mt)
-                            dmma884(c[mt][0], c[mt][1], ar[mt][ks], bv);
-                    }
+                            for (int ks = 0; ks < 2 * M::KR; ++ks) {
+                                const int blk = ks / M::KR, q = (ks - blk * M::KR) * 4 + gcol;
+                                const int off = blk * GG + q * G + x;
+                                const double av = (ok && q < G) ? fi[off] + fx[off] : 0.0;
 #pragma unroll
-                    for (int mt = 0; mt < M::MT; ++mt)
+                                for (int nt = 0; nt < M::MT; ++nt) dmma884(c[nt][0], c[nt][1], av, br[nt][ks]);
+                            }
+                        } else {
 #pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int i = mt * 8 + grow, nc = nt * 8 + gcol * 2 + h;
-                            if (i >= G || nc >= M::NCOL) continue;
-                            int e2, v2, j2;
-                            col(nc, e2, v2, j2);
-                            PD(e2)[v2 * QP + i * G + j2] = c[mt][h] * tb.n0[j2];
+                            for (int ks = 0; ks < M::KR; ++ks) {
+                                const int l = ks * 4 + gcol;
+                                const int off = GG + x * G + l;
+                                const double av = (ok && l < G) ? fi[off] + fx[off] : 0.0;
+#pragma unroll
+                                for (int nt = 0; nt < M::MT; ++nt) dmma884(c[nt][0], c[nt][1], av, bs2[nt][ks]);
+                            }
                         }
-                }
-                __syncwarp();
-                // part 2: rows j, columns (e, var, i)
+                        if (ok) {
 #pragma unroll
-                for (int nt = 0; nt < M::NTB; ++nt) {
-                    int e, var, i;
-                    const int n = nt * 8 + grow;
-                    col(n < M::NCOL ? n : 0, e, var, i);
-                    const bool colok = n < M::NCOL;
-                    const double *fi = FI(e) + var * VS + GG + i * G, *fx = FX(e) + var * VS + GG + i * G;
-                    double c[M::MT][2];
+                            for (int nt = 0; nt < M::MT; ++nt)
 #pragma unroll
-                    for (int mt = 0; mt < M::MT; ++mt) c[mt][0] = c[mt][1] = 0.0;
-#pragma unroll
-                    for (int ks = 0; ks < M::KR; ++ks) {
-                        const int l = ks * 4 + gcol;
-                        const double bv = (colok && l < G) ? fi[l] + fx[l] : 0.0;
-#pragma unroll
-                        for (int mt = 0; mt < M::MT; ++mt)
-                            dmma884(c[mt][0], c[mt][1], as2[mt][ks], bv);
-                    }
-#pragma unroll
-                    for (int mt = 0; mt < M::MT; ++mt)
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int j = mt * 8 + grow, nc = nt * 8 + gcol * 2 + h;
-                            if (j >= G || nc >= M::NCOL) continue;
-                            int e2, v2, i2;
-                            col(nc, e2, v2, i2);
-                            PD(e2)[v2 * QP + i2 * G + j] += c[mt][h];
+                                for (int h = 0; h < 2; ++h) {
+                                    const int n = nt * 8 + gcol * 2 + h;
+                                    if (n >= G) continue;
+                                    if (part == 0) PD(e)[var * QP + n * G + x] = c[nt][h] * tb.n0[x];
+                                    else PD(e)[var * QP + x * G + n] += c[nt][h];
+                                }
                         }
+                    }
+                    __syncwarp();
                 }
             }
             __syncwarp();

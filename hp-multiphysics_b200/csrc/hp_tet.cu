@@ -105,6 +105,73 @@ __device__ __forceinline__ R *mode_slot(const TetMeshD &m, const TetFields<R> &g
 }
 
 
+// Row (1-based) of face mode idx in the face's triangle of modes: rows 1 .. EM-1 hold EM-1,
+// EM-2, ... modes (the sign of a face mode is (-rot)^(row-1)).
+template <int EM>
+__device__ __forceinline__ int face_mode_row(int idx) {
+    int row = 1, left = idx;
+    while (left >= EM - row) {
+        left -= EM - row;
+        ++row;
+    }
+    return row;
+}
+
+// ugtouht (tet_hp/gtol.cpp:16-82) of NE tetrahedra into dst(e)[n T + m], one mode kind per
+// loop so that the lanes of an iteration take the same branch and read consecutive values:
+// the vertex values, the edge modes (EM NV per edge), the face modes (FM NV per face), the
+// interior modes (IM NV per tetrahedron). te(e) is tetrahedron e, act(e) whether it is
+// gathered (zeros otherwise). The same values and signs as mode_slot.
+template <typename R, int P, int NE, typename TEF, typename ACTF, typename DSTF>
+__device__ __forceinline__ void tet_gather_kinds(const TetMeshD &mesh, const TetFields<R> &ug, int lane, TEF te,
+                                                 ACTF act, DSTF dst) {
+    using C = TetCfg<P>;
+    constexpr int T = C::T, EM = C::EM, FM = C::FM, IM = C::IM;
+    constexpr int EMD = EM > 0 ? EM : 1, FMD = FM > 0 ? FM : 1, IMD = IM > 0 ? IM : 1;
+    constexpr int NVX = NE * 4 * NV, NED = NE * 6 * EM * NV, NFC = NE * 4 * FM * NV, NIN = NE * IM * NV;
+#pragma unroll
+    for (int it = 0; it < (NVX + 31) / 32; ++it) {
+        const int w = lane + 32 * it;
+        if (w >= NVX) continue;
+        const int e = w / (4 * NV), r = w - e * (4 * NV), m = r / NV, n = r - m * NV;
+        dst(e)[n * T + m] = act(e) ? ug.v[(size_t)mesh.tp[4 * te(e) + m] * NV + n] : (R)0;
+    }
+#pragma unroll
+    for (int it = 0; it < (NED + 31) / 32; ++it) {
+        const int w = lane + 32 * it;
+        if (w >= NED) continue;
+        const int b = w / (EMD * NV), r = w - b * (EMD * NV), e = b / 6, i = b - e * 6, k = r / NV, n = r - k * NV;
+        R v = (R)0;
+        if (act(e)) {
+            const int t = te(e);
+            v = ug.e[(size_t)mesh.ts[6 * t + i] * (EMD * NV) + r];
+            if ((k & 1) && mesh.tsg[6 * t + i] < 0) v = -v;
+        }
+        dst(e)[n * T + 4 + i * EMD + k] = v;
+    }
+#pragma unroll
+    for (int it = 0; it < (NFC + 31) / 32; ++it) {
+        const int w = lane + 32 * it;
+        if (w >= NFC) continue;
+        const int b = w / (FMD * NV), r = w - b * (FMD * NV), e = b / 4, i = b - e * 4, idx = r / NV,
+                  n = r - idx * NV;
+        R v = (R)0;
+        if (act(e)) {
+            const int t = te(e);
+            v = ug.f[(size_t)mesh.tt[4 * t + i] * (FMD * NV) + r];
+            if (((face_mode_row<EM>(idx) - 1) & 1) && mesh.trot[4 * t + i] > 0) v = -v;
+        }
+        dst(e)[n * T + 4 + 6 * EM + i * FMD + idx] = v;
+    }
+#pragma unroll
+    for (int it = 0; it < (NIN + 31) / 32; ++it) {
+        const int w = lane + 32 * it;
+        if (w >= NIN) continue;
+        const int e = w / (IMD * NV), r = w - e * (IMD * NV), k = r / NV, n = r - k * NV;
+        dst(e)[n * T + C::BM + k] = act(e) ? ug.i[(size_t)te(e) * (IMD * NV) + r] : (R)0;
+    }
+}
+
 // tet_hp::rsdl element loop (res: imaginary terms, res_r: beta-scaled real terms) on the
 // FP64 tensor cores (DMMA, mma.m8n8k4.f64): one warp takes two tetrahedra, so the 8 rows of an A fragment are (tetrahedron, variable) pairs.
 //   projection:  C[8 x Q] = U[8 x T] * Op^T[T x Q]   for Op = F, DX, DY, DZ
@@ -180,22 +247,10 @@ __global__ void __launch_bounds__(TetMma<P>::WPC * 32)
             const long it = (e == 1 && has1) ? it0 + 1 : it0;
             te[e] = MODE == 2 ? (int)(it / NJ) : (int)it;
         }
-        // ---- gather both tetrahedra (a missing second one gets zeros); unrolled so that
-        //      the dependent index -> value loads of a lane's entries overlap
-        constexpr int NGATH = (2 * NV * T + 31) / 32;
-#pragma unroll
-        for (int k = 0; k < NGATH; ++k) {
-            const int w = lane + 32 * k;
-            if (w >= 2 * NV * T) break;
-            const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
-            double v = 0.0;
-            if (e == 0 || has1) {
-                double s;
-                const double *src = mode_slot<double, P>(mesh, ug, te[e], m, n, s);
-                v = s * *src;
-            }
-            UHT(e)[n * T + m] = v;
-        }
+        // ---- gather both tetrahedra (a missing second one gets zeros)
+        tet_gather_kinds<double, P, 2>(
+            mesh, ug, lane, [&](int e) { return e ? te[1] : te[0]; }, [&](int e) { return e == 0 || has1; },
+            [&](int e) { return UHT(e); });
         double dw[2] = {0.0, 0.0};
         int jm[2] = {0, 0}, jn[2] = {0, 0};
         if constexpr (MODE == 2) {

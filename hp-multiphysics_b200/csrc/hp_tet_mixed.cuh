@@ -41,6 +41,7 @@ struct TetTf32 {
     static constexpr size_t PROJ_LEN = (size_t)4 * NT * KS * 64, INT_LEN = (size_t)NT2 * KS2 * 64;
     static constexpr size_t SMEM = (size_t)WPC * (4 * S_EL + 4 * GEO) * sizeof(float);
     static_assert(NV * T <= VS && Q <= VS, "modes / pressure must fit fre's variable-3 slot");
+    static_assert(2 * T <= VS, "the staged residual parts must fit the fim block");
 };
 
 __device__ __forceinline__ unsigned tet_tf32(float x) {
@@ -88,16 +89,7 @@ __global__ void __launch_bounds__(TetTf32<P>::WPC * 32)
         auto ACT = [&](int e) { return t0 + e < ntet; };
         __syncwarp();
         // ---- gather d (ugtouht) into the variable-3 slot of fre
-        for (int w = lane; w < 4 * NV * T; w += 32) {
-            const int e = w / (NV * T), r = w - e * (NV * T), n = r / T, m = r - n * T;
-            float v = 0.f;
-            if (ACT(e)) {
-                float s;
-                const float *src = mode_slot<float, P>(mesh, ug, TE(e), m, n, s);
-                v = s * *src;
-            }
-            PV(e)[n * T + m] = v;
-        }
+        tet_gather_kinds<float, P, 4>(mesh, ug, lane, TE, ACT, PV);
         // ---- geometry of the four tetrahedra (lanes 0..3): d(c, k) = the cofactors of
         //      ldcrd, |J| (tet_hp/ins/rsdl.cpp straight branch)
         if (lane < 4) {
@@ -332,28 +324,77 @@ __global__ void __launch_bounds__(TetTf32<P>::WPC * 32)
                     if (two) tet_mma_tf32(cr[nt], b0, b1, b2, b3, bf);
                 }
             }
+            // lftog (tet_hp/gtol.cpp) through shared memory: the lanes' values (-intgrtrst) are
+            // staged in the fim block (free once every lane's products are done) as
+            // [imaginary | real][variable][mode] per tetrahedron, then added one mode kind per
+            // loop: vertex, edge and face modes by FP32 atomics (imaginary -> res, real x beta
+            // -> res_r), interiors directly (res = im, res_r += beta re)
+            __syncwarp();
 #pragma unroll
-            for (int hh = 0; hh < 2; ++hh) {
-                const int e = ra + 2 * hh;
-                if (!ACT(e)) continue;
-                const int t = TE(e);
+            for (int hh = 0; hh < 2; ++hh)
 #pragma unroll
                 for (int nt = 0; nt < M::NT2; ++nt)
 #pragma unroll
                     for (int h2 = 0; h2 < 2; ++h2) {
                         const int m = nt * 8 + tig * 2 + h2;
                         if (m >= T) continue;
-                        const float vi = -ci[nt][2 * hh + h2], vr = -cr[nt][2 * hh + h2];
-                        float sg;
-                        float *dst = mode_slot<float, P>(mesh, res, t, m, rv, sg);
-                        if (m < C::BM) atomicAdd(dst, sg * vi);
-                        else *dst = vi;
-                        if (two) {
-                            float *dr = mode_slot<float, P>(mesh, rr, t, m, rv, sg);
-                            if (m < C::BM) atomicAdd(dr, beta * sg * vr);
-                            else *dr += beta * vr;
-                        }
+                        float *d = FIM(ra + 2 * hh) + rv * T + m;
+                        d[0] = -ci[nt][2 * hh + h2];
+                        if (two) d[NV * T] = -cr[nt][2 * hh + h2];
                     }
+            __syncwarp();
+            {
+                constexpr int EM = C::EM, FM = C::FM, IM = C::IM;
+                constexpr int EMD = EM > 0 ? EM : 1, FMD = FM > 0 ? FM : 1, IMD = IM > 0 ? IM : 1;
+                constexpr int NVX = 4 * 4 * NV, NED = 4 * 6 * EM * NV, NFC = 4 * 4 * FM * NV, NIN = 4 * IM * NV;
+                auto VI = [&](int e, int n, int m) { return FIM(e)[n * T + m]; };
+                auto VR = [&](int e, int n, int m) { return FIM(e)[NV * T + n * T + m]; };
+#pragma unroll
+                for (int it = 0; it < (NVX + 31) / 32; ++it) {
+                    const int w = lane + 32 * it;
+                    if (w >= NVX) continue;
+                    const int e = w / (4 * NV), r = w - e * (4 * NV), m = r / NV, n = r - m * NV;
+                    if (!ACT(e)) continue;
+                    const size_t g = (size_t)mesh.tp[4 * TE(e) + m] * NV + n;
+                    atomicAdd(res.v + g, VI(e, n, m));
+                    if (two) atomicAdd(rr.v + g, beta * VR(e, n, m));
+                }
+#pragma unroll
+                for (int it = 0; it < (NED + 31) / 32; ++it) {
+                    const int w = lane + 32 * it;
+                    if (w >= NED) continue;
+                    const int b = w / (EMD * NV), r = w - b * (EMD * NV), e = b / 6, i = b - e * 6, k = r / NV,
+                              n = r - k * NV;
+                    if (!ACT(e)) continue;
+                    const int t = TE(e), m = 4 + i * EMD + k;
+                    const float sg = ((k & 1) && mesh.tsg[6 * t + i] < 0) ? -1.f : 1.f;
+                    const size_t g = (size_t)mesh.ts[6 * t + i] * (EMD * NV) + r;
+                    atomicAdd(res.e + g, sg * VI(e, n, m));
+                    if (two) atomicAdd(rr.e + g, beta * sg * VR(e, n, m));
+                }
+#pragma unroll
+                for (int it = 0; it < (NFC + 31) / 32; ++it) {
+                    const int w = lane + 32 * it;
+                    if (w >= NFC) continue;
+                    const int b = w / (FMD * NV), r = w - b * (FMD * NV), e = b / 4, i = b - e * 4, idx = r / NV,
+                              n = r - idx * NV;
+                    if (!ACT(e)) continue;
+                    const int t = TE(e), m = 4 + 6 * EM + i * FMD + idx;
+                    const float sg = (((face_mode_row<EM>(idx) - 1) & 1) && mesh.trot[4 * t + i] > 0) ? -1.f : 1.f;
+                    const size_t g = (size_t)mesh.tt[4 * t + i] * (FMD * NV) + r;
+                    atomicAdd(res.f + g, sg * VI(e, n, m));
+                    if (two) atomicAdd(rr.f + g, beta * sg * VR(e, n, m));
+                }
+#pragma unroll
+                for (int it = 0; it < (NIN + 31) / 32; ++it) {
+                    const int w = lane + 32 * it;
+                    if (w >= NIN) continue;
+                    const int e = w / (IMD * NV), r = w - e * (IMD * NV), k = r / NV, n = r - k * NV;
+                    if (!ACT(e)) continue;
+                    const size_t g = (size_t)TE(e) * (IMD * NV) + r;
+                    res.i[g] = VI(e, n, C::BM + k);
+                    if (two) rr.i[g] += beta * VR(e, n, C::BM + k);
+                }
             }
         }
         __syncwarp();
