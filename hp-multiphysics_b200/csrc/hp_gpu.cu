@@ -440,7 +440,8 @@ struct LaunchImpl {
                           int upd, int fold, int th, cudaStream_t st) {
         if constexpr (MODE < SM) {
             if (mode == MODE)
-                k_minv_side<R, NV, SM, MODE><<<nblk(m.nseg, th), th, 0, st>>>(m, s, mt, im, (R)cfla, upd, fold);
+                k_minv_side_flat<R, NV, SM, IM, MODE><<<nblk((long)m.nseg * (SM - MODE) * NV, th), th, 0, st>>>(
+                    m, s, mt, (R)cfla, upd, fold);
             else
                 side_mode<MODE + 1>(m, s, mt, im, mode, cfla, upd, fold, th, st);
         }
@@ -451,11 +452,20 @@ struct LaunchImpl {
     }
     static void intr(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, double cfla, int upd, int th,
                      cudaStream_t st) {
-        if constexpr (IM > 0) k_minv_int<R, NV, SM, IM><<<nblk(m.ntri, th), th, 0, st>>>(m, s, mt, (R)cfla, upd);
+        if constexpr (IM > 0)
+            k_minv_int_flat<R, NV, SM, IM><<<nblk((long)m.ntri * NV, th), th, 0, st>>>(m, s, mt, (R)cfla, upd);
     }
     static void vert(const Mesh &m, const State<R> &s, const DevMinv<R> *mt, int sm, int im, double cfla, int upd,
                      int fold, unsigned long long *slot, int th, cudaStream_t st) {
-        k_minv_vert<R, NV><<<nblk(m.npnt, th), th, 0, st>>>(m, s, mt, sm, im, (R)cfla, upd, fold, slot);
+        if constexpr (SM > 0) {
+            // a lane group per vertex, sized to the vertex's removal terms (about 6 sides x SM
+            // and 6 triangles x IM)
+            constexpr int LPV = SM + IM >= 8 ? 32 : (SM + IM >= 3 ? 8 : 4);
+            k_minv_vert_coop<R, NV, SM, IM, LPV><<<nblk((long)m.npnt * LPV, th), th, 0, st>>>(m, s, mt, (R)cfla, upd,
+                                                                                             fold, slot);
+        } else {
+            k_minv_vert<R, NV><<<nblk(m.npnt, th), th, 0, st>>>(m, s, mt, sm, im, (R)cfla, upd, fold, slot);
+        }
     }
     static constexpr bool HAS_MMA = PHYS == 1;
     static constexpr bool DBL = std::is_same<R, double>::value;

@@ -1072,6 +1072,80 @@ __global__ void k_minv_vert(Mesh mesh, State<R> st, const DevMinv<R> *__restrict
     }
 }
 
+// The vertex phase with LPV lanes per vertex (p >= 2): the lanes split the vertex's
+// (side, mode) and (triangle, interior mode) removal terms, each reading NV consecutive
+// values, and sum them by shuffles in a fixed order, so that a vertex's gather is spread over
+// a lane group instead of one thread's sequential loop. Same result as k_minv_vert up to the
+// order of the removal sums.
+template <typename R, int NV, int SM, int IM, int LPV>
+__global__ void k_minv_vert_coop(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha, int do_update,
+                                 int fold, unsigned long long *maxres_slot) {
+    static_assert(32 % LPV == 0, "lane groups within a warp");
+    const int sub = threadIdx.x % LPV;
+    const long gv = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LPV;
+    const bool active = gv < mesh.npnt;
+    const int v = active ? (int)gv : 0;
+    R acc[NV];
+#pragma unroll
+    for (int n = 0; n < NV; ++n) acc[n] = (R)0;
+    if (active) {
+        if constexpr (SM > 0) {
+            const int q0 = mesh.vs_ptr[v], ns = (mesh.vs_ptr[v + 1] - q0) * SM;
+            for (int w = sub; w < ns; w += LPV) {
+                const int j = w / SM, k = w - j * SM;
+                const int code = mesh.vs_idx[q0 + j], sd = code >> 1, end = code & 1;
+                const R f = mt->sfmv[end][k];
+                const size_t gi = ((size_t)sd * SM + k) * NV;
+#pragma unroll
+                for (int n = 0; n < NV; ++n)
+                    acc[n] += f * (st.ress[gi + n] + (fold ? st.rrs[gi + n] : (R)0) +
+                                   (st.dress ? st.dress[gi + n] : (R)0));
+            }
+        }
+        if constexpr (IM > 0) {
+            const int q0 = mesh.vt_ptr[v], ni = (mesh.vt_ptr[v + 1] - q0) * IM;
+            for (int w = sub; w < ni; w += LPV) {
+                const int j = w / IM, k = w - j * IM;
+                const int code = mesh.vt_idx[q0 + j], t = code >> 2, i = code & 3;
+                const R f = mt->ifmb[i][k];
+                const size_t gi = ((size_t)t * IM + k) * NV;
+#pragma unroll
+                for (int n = 0; n < NV; ++n) acc[n] += f * st.resi[gi + n];
+            }
+        }
+    }
+#pragma unroll
+    for (int o = LPV / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int n = 0; n < NV; ++n) acc[n] += __shfl_xor_sync(0xffffffffu, acc[n], o, LPV);
+    R r[NV];
+#pragma unroll
+    for (int n = 0; n < NV; ++n) r[n] = (R)0;
+    if (active && sub == 0) {
+        const int ess = mesh.vess[v];
+#pragma unroll
+        for (int n = 0; n < NV; ++n) {
+            R x = st.resv[v * NV + n] + (fold ? st.rrv[v * NV + n] : (R)0) + (st.dresv ? st.dresv[v * NV + n] : (R)0);
+            x = (x - acc[n]) * st.vprcn[v * NV + n];
+            if (ess & (1 << n)) x = (R)0;
+            st.resv[v * NV + n] = x;
+            if (do_update) st.ugv[v * NV + n] = st.u0v[v * NV + n] - cflalpha * x;
+            r[n] = x;
+        }
+    }
+    if (maxres_slot) {
+#pragma unroll
+        for (int n = 0; n < NV; ++n) {
+            R a = fabs(r[n]);
+            for (int o = 16; o > 0; o >>= 1) {
+                R b = __shfl_xor_sync(0xffffffffu, a, o);
+                a = a > b ? a : b;
+            }
+            if ((threadIdx.x & 31) == 0) atomicMax(&maxres_slot[n], ord_key(a));
+        }
+    }
+}
+
 // Side phase for mode `mode`: mode 0 assembles res.s + res_r.s and removes the
 // interior and vertex parts; mode > 0 removes the finished mode-1 of the three
 // sides of each adjacent element. Then mode `mode` is finished: preconditioner,
@@ -1159,6 +1233,117 @@ __global__ void k_minv_side(Mesh mesh, State<R> st, const DevMinv<R> *__restrict
             const int gi = (s * SM + mode) * NV + n;
             st.ugs[gi] = st.u0s[gi] - cflalpha * r[mode][n];
         }
+}
+
+// The side phase with one thread per (side, mode >= MODE, variable) output instead of one
+// per side: the same terms subtracted in the same order as k_minv_side (bitwise the same
+// result), spread over (SM - MODE) NV threads per side.
+template <typename R, int NV, int SM, int IM, int MODE>
+__global__ void k_minv_side_flat(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha,
+                                 int do_update, int fold) {
+    constexpr int OUT = (SM - MODE) * NV;
+    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long)mesh.nseg * OUT) return;
+    const int s = (int)(gid / OUT), o = (int)(gid - (long)s * OUT);
+    const int k = MODE + o / NV, n = o - (o / NV) * NV;
+    const size_t gi = ((size_t)s * SM + k) * NV + n;
+    R r;
+    if constexpr (MODE == 0)
+        r = st.ress[gi] + (fold ? st.rrs[gi] : (R)0) + (st.dress ? st.dress[gi] : (R)0);
+    else
+        r = st.ress[gi];
+    for (int side = 0; side < 2; ++side) {
+        const int t = mesh.seg_tri[2 * s + side];
+        if (t < 0) continue;
+        const int i = mesh.seg_loc[2 * s + side];
+        const int sgn_i = mesh.tri_sgn[3 * t + i];
+        if constexpr (MODE == 0) {
+            // interior removal (setup_preconditioner.cpp:131-145)
+            const R msgn = ((k & 1) && sgn_i < 0) ? (R)-1 : (R)1;
+#pragma unroll
+            for (int kk = 0; kk < IM; ++kk) {
+                const R f = msgn * mt->ifmb[3 + i * SM + k][kk];
+                r -= f * st.resi[((size_t)t * IM + kk) * NV + n];
+            }
+            // vertex removal (setup_preconditioner.cpp:192-214)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int vv = mesh.tri_pnt[3 * t + (i + j) % 3];
+                const R uh = st.resv[vv * NV + n] * st.tprcn[t * NV + n];
+                r -= msgn * mt->vfms[j][k] * uh;
+            }
+        } else {
+            // removal of mode-1 from higher modes (setup_preconditioner.cpp:264-284)
+            constexpr int pm = MODE - 1;
+            R msgn = (((pm + 1) & 1) && sgn_i < 0) ? (R)-1 : (R)1;
+            if (sgn_i < 0 && ((k - MODE) & 1)) msgn = -msgn;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int sidx = (i + j) % 3;
+                const int sj = mesh.tri_seg[3 * t + sidx];
+                const int sgj = mesh.tri_sgn[3 * t + sidx];
+                const R sg = ((pm & 1) && sgj < 0) ? (R)-1 : (R)1;
+                const R uh = sg * st.ress[((size_t)sj * SM + pm) * NV + n] * st.tprcn[t * NV + n];
+                const R f = msgn * mt->sfms[pm][k][j];
+                r -= f * uh;
+            }
+        }
+    }
+    if (k == MODE) {
+        r = r * (st.sprcn[s * NV + n] * mt->sdiag[MODE]);
+        if (mesh.sess[s] & (1 << n)) r = (R)0;
+        if (do_update) st.ugs[gi] = st.u0s[gi] - cflalpha * r;
+    }
+    st.ress[gi] = r;
+}
+
+// The interior phase with one thread per (triangle, variable): the variables' banded solves
+// and removals are independent; the same operations in the same order as k_minv_int.
+template <typename R, int NV, int SM, int IM>
+__global__ void k_minv_int_flat(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha,
+                                int do_update) {
+    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long)mesh.ntri * NV) return;
+    const int t = (int)(gid / NV), n = (int)(gid - (long)t * NV);
+    R b[IM];
+#pragma unroll
+    for (int k = 0; k < IM; ++k) b[k] = st.resi[((size_t)t * IM + k) * NV + n];
+#pragma unroll
+    for (int i = 0; i < IM; ++i) {
+        if (i >= 1) b[i] -= mt->idiag[i][0] * b[0];
+        b[i] /= mt->idiag[i][1];
+    }
+#pragma unroll
+    for (int i = IM - 1; i >= 0; --i) {
+        b[i] /= mt->idiag[i][1];
+        if (i >= 1) b[0] -= mt->idiag[i][0] * b[i];
+    }
+    const R tp = st.tprcn[t * NV + n];
+#pragma unroll
+    for (int k = 0; k < IM; ++k) b[k] /= tp;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const R u = st.resv[mesh.tri_pnt[3 * t + i] * NV + n];
+#pragma unroll
+        for (int k = 0; k < IM; ++k) b[k] -= mt->bfmi[i][k] * u;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int sd = mesh.tri_seg[3 * t + i], sg = mesh.tri_sgn[3 * t + i];
+#pragma unroll
+        for (int m = 0; m < SM; ++m) {
+            const R msgn = ((m & 1) && sg < 0) ? (R)-1 : (R)1;
+            const R u = msgn * st.ress[((size_t)sd * SM + m) * NV + n];
+#pragma unroll
+            for (int k = 0; k < IM; ++k) b[k] -= mt->bfmi[3 + i * SM + m][k] * u;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < IM; ++k) {
+        const size_t gi = ((size_t)t * IM + k) * NV + n;
+        st.resi[gi] = b[k];
+        if (do_update) st.ugi[gi] = st.u0i[gi] - cflalpha * b[k];
+    }
 }
 
 // Interior phase (setup_preconditioner.cpp:341-370, DPBTRSNU2 as written in
