@@ -242,14 +242,16 @@ def p_sequence(p):
     return seq
 
 
-def build(factory, n, p, hlevels=0, stream=None, cfl=None, plevels=True, coarsen=None, **kw):
+def build(factory, n, p, hlevels=0, stream=None, cfl=None, plevels=True, coarsen=None, coarsen_method="coarsen",
+          **kw):
     """Hierarchy for a workload factory(n=..., p=...): p-levels of the fine mesh
     down to p = 1 (unless plevels=False: the fine level goes straight to the h-levels,
     as the reference does with extra_finest_levels = 0), then `hlevels` split-square
-    meshes of n/2, n/4, ... at p = 1. coarsen = a factor (e.g. 1.5): the h-levels are
-    instead made from the level above by hpb.coarsen.coarsen (tri_mesh::coarsen), through
-    factory(mesh=..., p=1). cfl: None (the per-log2p defaults), a number, or a dict
-    p -> cfl."""
+    meshes of n/2, n/4, ... at p = 1. coarsen = a factor: the h-levels are instead made
+    from the level above, through factory(mesh=..., p=1), by hpb.coarsen.coarsen
+    (tri_mesh::coarsen, e.g. 1.5) or, with coarsen_method="coarsen2", by
+    hpb.coarsen.coarsen2 (tri_mesh::coarsen2, edge collapse; the reference's multigrid
+    uses 2.0). cfl: None (the per-log2p defaults), a number, or a dict p -> cfl."""
     def cf(q):
         if cfl is None:
             return {}
@@ -263,8 +265,11 @@ def build(factory, n, p, hlevels=0, stream=None, cfl=None, plevels=True, coarsen
     for _ in range(hlevels):
         m //= 2
         if coarsen:
-            from .coarsen import coarsen as coarsen_mesh
-            probs.append(factory(mesh=coarsen_mesh(probs[-1].mesh, coarsen), p=1, **cf(1), **kw))
+            from . import coarsen as C
+            if coarsen_method not in ("coarsen", "coarsen2"):
+                raise ValueError(f"coarsen_method {coarsen_method!r}: 'coarsen' or 'coarsen2'")
+            make = C.coarsen2 if coarsen_method == "coarsen2" else C.coarsen
+            probs.append(factory(mesh=make(probs[-1].mesh, coarsen), p=1, **cf(1), **kw))
         else:
             probs.append(factory(n=m, p=1, **cf(1), **kw))
         kinds.append("h")

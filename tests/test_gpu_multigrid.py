@@ -200,11 +200,13 @@ def test_curved_hole_cycles_keep_essential_values_and_converge():
     H.close()
 
 
-@pytest.mark.parametrize("kind", ["ins", "cd-delaunay"])
-def test_cycles_on_coarsened_h_levels(kind):
-    """h-levels made from the level above by hpb.coarsen (tri_mesh::coarsen): the cycles
-    reach the 1e-10 drop, in a cycle count close to that of the generated (nested) levels for
-    the structured mesh."""
+@pytest.mark.parametrize("kind,method", [("ins", "coarsen"), ("cd-delaunay", "coarsen"), ("ins", "coarsen2"),
+                                         ("cd-delaunay", "coarsen2")])
+def test_cycles_on_coarsened_h_levels(kind, method):
+    """h-levels made from the level above by hpb.coarsen (tri_mesh::coarsen, factor 1.5) or
+    by hpb.coarsen2 (tri_mesh::coarsen2, edge collapse, factor 2): the cycles reach the 1e-10
+    drop, in a cycle count close to that of the generated (nested) levels for the structured
+    mesh."""
     if kind == "ins":
         def mk(n=16, p=4, mesh=None, **kw):
             return hpb.kovasznay_ins(n=n, p=p, re=100.0, mesh=mesh, **kw)
@@ -215,7 +217,8 @@ def test_cycles_on_coarsened_h_levels(kind):
                                  field=quad(), **kw)
         cfl = {4: 0.5, 2: 0.75, 1: 1.0}
     n = 16 if kind == "ins" else 24
-    H = MG.build(mk, n=n, p=4, hlevels=2, cfl=cfl, coarsen=1.5)
+    H = MG.build(mk, n=n, p=4, hlevels=2, cfl=cfl, coarsen=1.5 if method == "coarsen" else 2.0,
+                 coarsen_method=method)
     assert H.levels[-1].prob.mesh.ntri < 0.1 * H.levels[0].prob.mesh.ntri
     hist, sec, cycles = H.solve(drop=1e-10, max_cycles=400, itercrsn=2, iterrfne=2)
     H.close()
