@@ -1146,98 +1146,12 @@ __global__ void k_minv_vert_coop(Mesh mesh, State<R> st, const DevMinv<R> *__res
     }
 }
 
-// Side phase for mode `mode`: mode 0 assembles res.s + res_r.s and removes the
-// interior and vertex parts; mode > 0 removes the finished mode-1 of the three
-// sides of each adjacent element. Then mode `mode` is finished: preconditioner,
-// sdiag, Dirichlet zeroing, update of ug.s.
-// The side mode is a template parameter so that every index into r is a compile-time
-// constant and r stays in registers.
-template <typename R, int NV, int SM, int MODE>
-__global__ void k_minv_side(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, int im, R cflalpha,
-                            int do_update, int fold) {
-    constexpr int mode = MODE;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= mesh.nseg) return;
-    R r[SM][NV];
-    if (mode == 0) {
-        for (int k = 0; k < SM; ++k)
-            for (int n = 0; n < NV; ++n) {
-                const int gi = (s * SM + k) * NV + n;
-                r[k][n] = st.ress[gi] + (fold ? st.rrs[gi] : (R)0) + (st.dress ? st.dress[gi] : (R)0);
-            }
-    } else {
-        for (int k = mode; k < SM; ++k)
-            for (int n = 0; n < NV; ++n) r[k][n] = st.ress[(s * SM + k) * NV + n];
-    }
-    for (int side = 0; side < 2; ++side) {
-        const int t = mesh.seg_tri[2 * s + side];
-        if (t < 0) continue;
-        const int i = mesh.seg_loc[2 * s + side];
-        const int sgn_i = mesh.tri_sgn[3 * t + i];
-        if (mode == 0) {
-            // interior removal (setup_preconditioner.cpp:131-145)
-            for (int k = 0; k < SM; ++k) {
-                const R msgn = ((k & 1) && sgn_i < 0) ? (R)-1 : (R)1;
-                for (int kk = 0; kk < im; ++kk) {
-                    const R f = msgn * mt->ifmb[3 + i * SM + k][kk];
-                    for (int n = 0; n < NV; ++n) r[k][n] -= f * st.resi[((size_t)t * im + kk) * NV + n];
-                }
-            }
-            // vertex removal (setup_preconditioner.cpp:192-214)
-            for (int j = 0; j < 3; ++j) {
-                const int i1 = (i + j) % 3;
-                const int vv = mesh.tri_pnt[3 * t + i1];
-                for (int n = 0; n < NV; ++n) {
-                    const R uh = st.resv[vv * NV + n] * st.tprcn[t * NV + n];
-                    for (int k = 0; k < SM; ++k) {
-                        const R msgn = ((k & 1) && sgn_i < 0) ? (R)-1 : (R)1;
-                        r[k][n] -= msgn * mt->vfms[j][k] * uh;
-                    }
-                }
-            }
-        } else {
-            // removal of mode-1 from higher modes (setup_preconditioner.cpp:264-284)
-            const int pm = mode - 1;
-            R uh[3][NV];  // uh[j]: mode pm of the triangle's side (i + j) % 3
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const int sidx = (i + j) % 3;
-                const int sj = mesh.tri_seg[3 * t + sidx];
-                const int sgj = mesh.tri_sgn[3 * t + sidx];
-                const R sg = ((pm & 1) && sgj < 0) ? (R)-1 : (R)1;
-                for (int n = 0; n < NV; ++n) uh[j][n] = sg * st.ress[(sj * SM + pm) * NV + n] * st.tprcn[t * NV + n];
-            }
-            R msgn = (((pm + 1) & 1) && sgn_i < 0) ? (R)-1 : (R)1;
-#pragma unroll
-            for (int m = mode; m < SM; ++m) {
-#pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const R f = msgn * mt->sfms[pm][m][j];
-                    for (int n = 0; n < NV; ++n) r[m][n] -= f * uh[j][n];
-                }
-                if (sgn_i < 0) msgn = -msgn;
-            }
-        }
-    }
-    const int ess = mesh.sess[s];
-    for (int n = 0; n < NV; ++n) {
-        R v = r[mode][n] * (st.sprcn[s * NV + n] * mt->sdiag[mode]);
-        if (ess & (1 << n)) v = (R)0;
-        r[mode][n] = v;
-    }
-    const int k0 = (mode == 0 ? 0 : mode);
-    for (int k = k0; k < SM; ++k)
-        for (int n = 0; n < NV; ++n) st.ress[(s * SM + k) * NV + n] = r[k][n];
-    if (do_update)
-        for (int n = 0; n < NV; ++n) {
-            const int gi = (s * SM + mode) * NV + n;
-            st.ugs[gi] = st.u0s[gi] - cflalpha * r[mode][n];
-        }
-}
-
-// The side phase with one thread per (side, mode >= MODE, variable) output instead of one
-// per side: the same terms subtracted in the same order as k_minv_side (bitwise the same
-// result), spread over (SM - MODE) NV threads per side.
+// Side phase for mode MODE (setup_preconditioner.cpp:131-340), one thread per (side, mode
+// k >= MODE, variable) output. MODE 0 assembles res.s + res_r.s (+ dres) and removes the
+// interior and vertex parts; MODE > 0 removes the finished mode MODE - 1 of the three sides of
+// each adjacent element. Then mode MODE is finished: preconditioner, sdiag, Dirichlet zeroing,
+// update of ug.s. Each output subtracts its terms in the reference's order (side by side, each
+// side's triangles in seg.tri order).
 template <typename R, int NV, int SM, int IM, int MODE>
 __global__ void k_minv_side_flat(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha,
                                  int do_update, int fold) {
@@ -1297,8 +1211,9 @@ __global__ void k_minv_side_flat(Mesh mesh, State<R> st, const DevMinv<R> *__res
     st.ress[gi] = r;
 }
 
-// The interior phase with one thread per (triangle, variable): the variables' banded solves
-// and removals are independent; the same operations in the same order as k_minv_int.
+// Interior phase (setup_preconditioner.cpp:341-370, DPBTRSNU2 as written in
+// utilities/myblas.c:91-120) + update of ug.i, one thread per (triangle, variable): the
+// variables' banded solves and removals are independent.
 template <typename R, int NV, int SM, int IM>
 __global__ void k_minv_int_flat(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha,
                                 int do_update) {
@@ -1344,56 +1259,6 @@ __global__ void k_minv_int_flat(Mesh mesh, State<R> st, const DevMinv<R> *__rest
         st.resi[gi] = b[k];
         if (do_update) st.ugi[gi] = st.u0i[gi] - cflalpha * b[k];
     }
-}
-
-// Interior phase (setup_preconditioner.cpp:341-370, DPBTRSNU2 as written in
-// utilities/myblas.c:91-120) + update of ug.i.
-template <typename R, int NV, int SM, int IM>
-__global__ void k_minv_int(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha, int do_update) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= mesh.ntri) return;
-    R b[IM][NV];
-    for (int k = 0; k < IM; ++k)
-        for (int n = 0; n < NV; ++n) b[k][n] = st.resi[((size_t)t * IM + k) * NV + n];
-    // DPBTRSNU2(idiag, stride 2, IM, ofdg 1, b, NV)
-    for (int i = 0; i < IM; ++i) {
-        if (i >= 1)
-            for (int n = 0; n < NV; ++n) b[i][n] -= mt->idiag[i][0] * b[0][n];
-        for (int n = 0; n < NV; ++n) b[i][n] /= mt->idiag[i][1];
-    }
-    for (int i = IM - 1; i >= 0; --i) {
-        for (int n = 0; n < NV; ++n) b[i][n] /= mt->idiag[i][1];
-        if (i >= 1)
-            for (int n = 0; n < NV; ++n) b[0][n] -= mt->idiag[i][0] * b[i][n];
-    }
-    R tp[NV];
-    for (int n = 0; n < NV; ++n) tp[n] = st.tprcn[t * NV + n];
-    for (int k = 0; k < IM; ++k)
-        for (int n = 0; n < NV; ++n) b[k][n] /= tp[n];
-    // restouht_bdry and bfmi removal
-    for (int i = 0; i < 3; ++i) {
-        const int vv = mesh.tri_pnt[3 * t + i];
-        for (int n = 0; n < NV; ++n) {
-            const R u = st.resv[vv * NV + n];
-            for (int k = 0; k < IM; ++k) b[k][n] -= mt->bfmi[i][k] * u;
-        }
-    }
-    for (int i = 0; i < 3; ++i) {
-        const int sd = mesh.tri_seg[3 * t + i], sg = mesh.tri_sgn[3 * t + i];
-        for (int m = 0; m < SM; ++m) {
-            const R msgn = ((m & 1) && sg < 0) ? (R)-1 : (R)1;
-            for (int n = 0; n < NV; ++n) {
-                const R u = msgn * st.ress[(sd * SM + m) * NV + n];
-                for (int k = 0; k < IM; ++k) b[k][n] -= mt->bfmi[3 + i * SM + m][k] * u;
-            }
-        }
-    }
-    for (int k = 0; k < IM; ++k)
-        for (int n = 0; n < NV; ++n) {
-            const size_t gi = ((size_t)t * IM + k) * NV + n;
-            st.resi[gi] = b[k][n];
-            if (do_update) st.ugi[gi] = st.u0i[gi] - cflalpha * b[k][n];
-        }
 }
 
 // ---------------------------------------------------------------------------
