@@ -343,7 +343,7 @@ class _AdaptMesh:
         stop = tind
         d = 1
         tris, spokes = [], []
-        while True:
+        for _ in range(2 * len(self.tp) + 2):  # a walk longer than the mesh is a broken ring
             vn = self.tp[tind].index(v)
             t1 = self.tt[tind][(vn + d) % 3]
             if t1 < 0:
@@ -363,6 +363,8 @@ class _AdaptMesh:
             tind = t1
             if tind == stop:
                 break
+        else:
+            raise RuntimeError(f"coarsen2: the triangles around vertex {v} do not close")
         return tris, spokes
 
     def collapse(self, sind, delt):
