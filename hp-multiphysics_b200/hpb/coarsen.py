@@ -18,9 +18,9 @@ level from any fine mesh:
   the set is kept where it lies inside the fine mesh, and every coarse boundary side must be
   one of its edges (checked).
 
-tri_mesh::coarsen2 (coarsen.cpp:248-282), the other route, coarsens by collapsing
-short edges of a copy of the fine mesh. It belongs to the mesh-adaptation machinery
-(yaber, collapse, swap), which is out of scope here.
+tri_mesh::coarsen2 (coarsen.cpp:248-282), the other route and the reference's default for
+its multigrid levels, coarsens by collapsing short edges of a copy of the fine mesh (yaber,
+collapse, swap): `coarsen2` below.
 """
 import numpy as np
 
