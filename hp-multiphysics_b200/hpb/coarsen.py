@@ -710,18 +710,18 @@ def coarsen2(mesh, factor=2.0, tolsize=1.414, corner_deg=30.0):
     X = np.array([am.x[v] for v in keep_p], dtype=np.float64)
     cm = Mesh(X, np.array(tris, dtype=np.int32))
     cm.fine_vertex = np.array(keep_p, dtype=np.int64)
-    # boundary groups of the coarse sides: a coarse boundary side joins two fine vertices of
-    # one chain
-    where = {}
-    for gid, chain, _ in chains:
-        for s in chain:
-            for v in mesh.seg_pnt[s]:
-                where.setdefault(int(v), set()).add(gid)
+    # boundary groups of the coarse sides: a coarse boundary side replaces the run of fine
+    # boundary sides from its first vertex along the chain, so it takes the group of the fine
+    # side that starts there (boundary sides run with the domain on their left)
     groups = {}
-    for s in cm.boundary_segments():
-        a, b = (int(cm.fine_vertex[v]) for v in cm.seg_pnt[s])
-        g = where.get(a, set()) & where.get(b, set())
-        if g:
-            groups.setdefault(min(g), []).append(int(s))
-    cm.groups = groups if getattr(mesh, "groups", None) else {}
+    fine_groups = getattr(mesh, "groups", None)
+    if fine_groups:
+        gid_of = {int(sd): gid for gid, segs in fine_groups.items() for sd in segs}
+        start = {int(mesh.seg_pnt[sd, 0]): int(sd) for sd in mesh.boundary_segments()}
+        for sd in cm.boundary_segments():
+            a = int(cm.fine_vertex[cm.seg_pnt[sd, 0]])
+            g = gid_of.get(start.get(a, -1))
+            if g is not None:
+                groups.setdefault(g, []).append(int(sd))
+    cm.groups = groups
     return cm

@@ -84,3 +84,23 @@ def test_reference_grd_meshes_coarsen2_with_their_groups(k):
     for gid, segs in g.groups.items():
         ends = {int(g.seg_pnt[s, 0]) for s in segs} ^ {int(g.seg_pnt[s, 1]) for s in segs}
         assert ends <= set(c.fine_vertex.tolist())
+
+
+@pytest.mark.skipif(not REF_DIR, reason="HP_REFERENCE_DIR (reference checkout) not set")
+@pytest.mark.parametrize("rel", ["Testing/tri_hp/conv-diff/Correctness/Inputs/tim.0.grd",
+                                 "Testing/tri_hp/conv-diff/Correctness/Inputs/tim.1.grd",
+                                 "Testing/tri_mesh/wind phased/Inputs/wind_b0.grd",
+                                 "Testing/tri_hp/ins/Time Accuracy/Taylor/Inputs/square32.grd"])
+def test_reference_test_meshes_coarsen2(rel):
+    """The reference's own test meshes (holes, curved and grouped boundaries): valid coarse
+    meshes whose every boundary side keeps the group of the fine side it starts on."""
+    g = read_grd(os.path.join(REF_DIR, rel))
+    c = coarsen2(g)
+    assert np.all(c.area2() > 0)
+    fv = c.fine_vertex
+    assert np.all(c.pnts == g.pnts[fv])
+    assert c.ntri < g.ntri
+    if g.groups:
+        assert set(c.groups) == set(g.groups)
+        flat = sorted(s for segs in c.groups.values() for s in segs)
+        assert flat == sorted(c.boundary_segments().tolist())
