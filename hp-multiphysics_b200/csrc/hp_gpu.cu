@@ -440,8 +440,8 @@ struct LaunchImpl {
                           int upd, int fold, int th, cudaStream_t st) {
         if constexpr (MODE < SM) {
             if (mode == MODE)
-                k_minv_side_flat<R, NV, SM, IM, MODE><<<nblk((long)m.nseg * (SM - MODE) * NV, th), th, 0, st>>>(
-                    m, s, mt, (R)cfla, upd, fold);
+                k_minv_side_vn<R, NV, SM, IM, MODE><<<nblk((long)m.nseg * NV, th), th, 0, st>>>(m, s, mt, (R)cfla, upd,
+                                                                                             fold);
             else
                 side_mode<MODE + 1>(m, s, mt, im, mode, cfla, upd, fold, th, st);
         }

@@ -1211,6 +1211,97 @@ __global__ void k_minv_side_flat(Mesh mesh, State<R> st, const DevMinv<R> *__res
     st.ress[gi] = r;
 }
 
+// The same side phase with one thread per (side, variable), its modes k >= MODE in
+// registers: the values a side's modes share (the triangles' interior modes and vertex
+// values in mode 0, the three sides' finished mode MODE - 1 in the others) are read once per
+// thread instead of once per mode, and the tables come from shared memory, staged per block.
+// Each output subtracts the same terms in the same order as k_minv_side_flat.
+template <typename R, int NV, int SM, int IM, int MODE>
+__global__ void k_minv_side_vn(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha,
+                               int do_update, int fold) {
+    constexpr int I1 = IM > 0 ? IM : 1, NK = SM - MODE;
+    __shared__ R s_ifmb[3 * SM][I1], s_vfms[3][SM], s_sfms[SM][3], s_sdiag;
+    for (int x = threadIdx.x; x < 3 * SM * I1; x += blockDim.x)
+        s_ifmb[x / I1][x % I1] = IM > 0 ? mt->ifmb[3 + x / I1][x % I1] : (R)0;
+    for (int x = threadIdx.x; x < 3 * SM; x += blockDim.x) {
+        s_vfms[x / SM][x % SM] = mt->vfms[x / SM][x % SM];
+        s_sfms[x / 3][x % 3] = MODE > 0 ? mt->sfms[MODE > 0 ? MODE - 1 : 0][x / 3][x % 3] : (R)0;
+    }
+    if (threadIdx.x == 0) s_sdiag = mt->sdiag[MODE];
+    __syncthreads();
+    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= (long)mesh.nseg * NV) return;
+    const int s = (int)(gid / NV), n = (int)(gid - (long)s * NV);
+    const size_t g0 = (size_t)s * SM * NV + n;  // mode k at g0 + k NV
+    R r[NK];
+#pragma unroll
+    for (int q = 0; q < NK; ++q) {
+        const size_t gi = g0 + (size_t)(MODE + q) * NV;
+        if constexpr (MODE == 0)
+            r[q] = st.ress[gi] + (fold ? st.rrs[gi] : (R)0) + (st.dress ? st.dress[gi] : (R)0);
+        else
+            r[q] = st.ress[gi];
+    }
+    for (int side = 0; side < 2; ++side) {
+        const int t = mesh.seg_tri[2 * s + side];
+        if (t < 0) continue;
+        const int i = mesh.seg_loc[2 * s + side];
+        const bool neg = mesh.tri_sgn[3 * t + i] < 0;
+        const R tp = st.tprcn[t * NV + n];
+        if constexpr (MODE == 0) {
+            // interior removal (setup_preconditioner.cpp:131-145)
+            R ri[I1];
+#pragma unroll
+            for (int kk = 0; kk < IM; ++kk) ri[kk] = st.resi[((size_t)t * IM + kk) * NV + n];
+            R uh[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) uh[j] = st.resv[mesh.tri_pnt[3 * t + (i + j) % 3] * NV + n] * tp;
+#pragma unroll
+            for (int k = 0; k < SM; ++k) {
+                const R msgn = ((k & 1) && neg) ? (R)-1 : (R)1;
+#pragma unroll
+                for (int kk = 0; kk < IM; ++kk) {
+                    const R f = msgn * s_ifmb[i * SM + k][kk];
+                    r[k] -= f * ri[kk];
+                }
+                // vertex removal (setup_preconditioner.cpp:192-214)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) r[k] -= msgn * s_vfms[j][k] * uh[j];
+            }
+        } else {
+            // removal of mode-1 from higher modes (setup_preconditioner.cpp:264-284)
+            constexpr int pm = MODE - 1;
+            R uh[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int sidx = (i + j) % 3;
+                const int sj = mesh.tri_seg[3 * t + sidx];
+                const int sgj = mesh.tri_sgn[3 * t + sidx];
+                const R sg = ((pm & 1) && sgj < 0) ? (R)-1 : (R)1;
+                uh[j] = sg * st.ress[((size_t)sj * SM + pm) * NV + n] * tp;
+            }
+            R msgn = (((pm + 1) & 1) && neg) ? (R)-1 : (R)1;
+#pragma unroll
+            for (int q = 0; q < NK; ++q) {
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const R f = msgn * s_sfms[MODE + q][j];
+                    r[q] -= f * uh[j];
+                }
+                if (neg) msgn = -msgn;
+            }
+        }
+    }
+    {
+        R v = r[0] * (st.sprcn[s * NV + n] * s_sdiag);
+        if (mesh.sess[s] & (1 << n)) v = (R)0;
+        r[0] = v;
+        if (do_update) st.ugs[g0 + (size_t)MODE * NV] = st.u0s[g0 + (size_t)MODE * NV] - cflalpha * v;
+    }
+#pragma unroll
+    for (int q = 0; q < NK; ++q) st.ress[g0 + (size_t)(MODE + q) * NV] = r[q];
+}
+
 // Interior phase (setup_preconditioner.cpp:341-370, DPBTRSNU2 as written in
 // utilities/myblas.c:91-120) + update of ug.i, one thread per (triangle, variable): the
 // variables' banded solves and removals are independent.
