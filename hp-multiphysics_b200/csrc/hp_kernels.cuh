@@ -1081,6 +1081,11 @@ template <typename R, int NV, int SM, int IM, int LPV>
 __global__ void k_minv_vert_coop(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha, int do_update,
                                  int fold, unsigned long long *maxres_slot) {
     static_assert(32 % LPV == 0, "lane groups within a warp");
+    constexpr int S1 = SM > 0 ? SM : 1, I1 = IM > 0 ? IM : 1;
+    __shared__ R s_sfmv[2][S1], s_ifmb[3][I1];  // the tables, staged per block
+    for (int x = threadIdx.x; x < 2 * S1; x += blockDim.x) s_sfmv[x / S1][x % S1] = SM > 0 ? mt->sfmv[x / S1][x % S1] : (R)0;
+    for (int x = threadIdx.x; x < 3 * I1; x += blockDim.x) s_ifmb[x / I1][x % I1] = IM > 0 ? mt->ifmb[x / I1][x % I1] : (R)0;
+    __syncthreads();
     const int sub = threadIdx.x % LPV;
     const long gv = ((long)blockIdx.x * blockDim.x + threadIdx.x) / LPV;
     const bool active = gv < mesh.npnt;
@@ -1094,7 +1099,7 @@ __global__ void k_minv_vert_coop(Mesh mesh, State<R> st, const DevMinv<R> *__res
             for (int w = sub; w < ns; w += LPV) {
                 const int j = w / SM, k = w - j * SM;
                 const int code = mesh.vs_idx[q0 + j], sd = code >> 1, end = code & 1;
-                const R f = mt->sfmv[end][k];
+                const R f = s_sfmv[end][k];
                 const size_t gi = ((size_t)sd * SM + k) * NV;
 #pragma unroll
                 for (int n = 0; n < NV; ++n)
@@ -1107,7 +1112,7 @@ __global__ void k_minv_vert_coop(Mesh mesh, State<R> st, const DevMinv<R> *__res
             for (int w = sub; w < ni; w += LPV) {
                 const int j = w / IM, k = w - j * IM;
                 const int code = mesh.vt_idx[q0 + j], t = code >> 2, i = code & 3;
-                const R f = mt->ifmb[i][k];
+                const R f = s_ifmb[i][k];
                 const size_t gi = ((size_t)t * IM + k) * NV;
 #pragma unroll
                 for (int n = 0; n < NV; ++n) acc[n] += f * st.resi[gi + n];
@@ -1146,76 +1151,15 @@ __global__ void k_minv_vert_coop(Mesh mesh, State<R> st, const DevMinv<R> *__res
     }
 }
 
-// Side phase for mode MODE (setup_preconditioner.cpp:131-340), one thread per (side, mode
-// k >= MODE, variable) output. MODE 0 assembles res.s + res_r.s (+ dres) and removes the
-// interior and vertex parts; MODE > 0 removes the finished mode MODE - 1 of the three sides of
-// each adjacent element. Then mode MODE is finished: preconditioner, sdiag, Dirichlet zeroing,
-// update of ug.s. Each output subtracts its terms in the reference's order (side by side, each
-// side's triangles in seg.tri order).
-template <typename R, int NV, int SM, int IM, int MODE>
-__global__ void k_minv_side_flat(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha,
-                                 int do_update, int fold) {
-    constexpr int OUT = (SM - MODE) * NV;
-    const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (long)mesh.nseg * OUT) return;
-    const int s = (int)(gid / OUT), o = (int)(gid - (long)s * OUT);
-    const int k = MODE + o / NV, n = o - (o / NV) * NV;
-    const size_t gi = ((size_t)s * SM + k) * NV + n;
-    R r;
-    if constexpr (MODE == 0)
-        r = st.ress[gi] + (fold ? st.rrs[gi] : (R)0) + (st.dress ? st.dress[gi] : (R)0);
-    else
-        r = st.ress[gi];
-    for (int side = 0; side < 2; ++side) {
-        const int t = mesh.seg_tri[2 * s + side];
-        if (t < 0) continue;
-        const int i = mesh.seg_loc[2 * s + side];
-        const int sgn_i = mesh.tri_sgn[3 * t + i];
-        if constexpr (MODE == 0) {
-            // interior removal (setup_preconditioner.cpp:131-145)
-            const R msgn = ((k & 1) && sgn_i < 0) ? (R)-1 : (R)1;
-#pragma unroll
-            for (int kk = 0; kk < IM; ++kk) {
-                const R f = msgn * mt->ifmb[3 + i * SM + k][kk];
-                r -= f * st.resi[((size_t)t * IM + kk) * NV + n];
-            }
-            // vertex removal (setup_preconditioner.cpp:192-214)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const int vv = mesh.tri_pnt[3 * t + (i + j) % 3];
-                const R uh = st.resv[vv * NV + n] * st.tprcn[t * NV + n];
-                r -= msgn * mt->vfms[j][k] * uh;
-            }
-        } else {
-            // removal of mode-1 from higher modes (setup_preconditioner.cpp:264-284)
-            constexpr int pm = MODE - 1;
-            R msgn = (((pm + 1) & 1) && sgn_i < 0) ? (R)-1 : (R)1;
-            if (sgn_i < 0 && ((k - MODE) & 1)) msgn = -msgn;
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const int sidx = (i + j) % 3;
-                const int sj = mesh.tri_seg[3 * t + sidx];
-                const int sgj = mesh.tri_sgn[3 * t + sidx];
-                const R sg = ((pm & 1) && sgj < 0) ? (R)-1 : (R)1;
-                const R uh = sg * st.ress[((size_t)sj * SM + pm) * NV + n] * st.tprcn[t * NV + n];
-                const R f = msgn * mt->sfms[pm][k][j];
-                r -= f * uh;
-            }
-        }
-    }
-    if (k == MODE) {
-        r = r * (st.sprcn[s * NV + n] * mt->sdiag[MODE]);
-        if (mesh.sess[s] & (1 << n)) r = (R)0;
-        if (do_update) st.ugs[gi] = st.u0s[gi] - cflalpha * r;
-    }
-    st.ress[gi] = r;
-}
-
-// The same side phase with one thread per (side, variable), its modes k >= MODE in
-// registers: the values a side's modes share (the triangles' interior modes and vertex
-// values in mode 0, the three sides' finished mode MODE - 1 in the others) are read once per
-// thread instead of once per mode, and the tables come from shared memory, staged per block.
-// Each output subtracts the same terms in the same order as k_minv_side_flat.
+// Side phase for mode MODE (setup_preconditioner.cpp:131-340), one thread per (side,
+// variable) with its modes k >= MODE in registers. MODE 0 assembles res.s + res_r.s (+ dres)
+// and removes the interior and vertex parts; MODE > 0 removes the finished mode MODE - 1 of the
+// three sides of each adjacent element. Then mode MODE is finished: preconditioner, sdiag,
+// Dirichlet zeroing, update of ug.s. The values a side's modes share (the triangles' interior
+// modes and vertex values in mode 0, the three sides' mode MODE - 1 in the others) are read
+// once per thread, and the tables come from shared memory, staged per block. Each output
+// subtracts its terms in the reference's order (side by side, each side's triangles in
+// seg.tri order).
 template <typename R, int NV, int SM, int IM, int MODE>
 __global__ void k_minv_side_vn(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha,
                                int do_update, int fold) {
@@ -1308,6 +1252,11 @@ __global__ void k_minv_side_vn(Mesh mesh, State<R> st, const DevMinv<R> *__restr
 template <typename R, int NV, int SM, int IM>
 __global__ void k_minv_int_flat(Mesh mesh, State<R> st, const DevMinv<R> *__restrict__ mt, R cflalpha,
                                 int do_update) {
+    // the tables in shared memory, staged per block
+    __shared__ R s_bfmi[3 + 3 * SM][IM], s_idiag[IM][2];
+    for (int x = threadIdx.x; x < (3 + 3 * SM) * IM; x += blockDim.x) s_bfmi[x / IM][x % IM] = mt->bfmi[x / IM][x % IM];
+    for (int x = threadIdx.x; x < 2 * IM; x += blockDim.x) s_idiag[x / 2][x % 2] = mt->idiag[x / 2][x % 2];
+    __syncthreads();
     const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= (long)mesh.ntri * NV) return;
     const int t = (int)(gid / NV), n = (int)(gid - (long)t * NV);
@@ -1316,13 +1265,13 @@ __global__ void k_minv_int_flat(Mesh mesh, State<R> st, const DevMinv<R> *__rest
     for (int k = 0; k < IM; ++k) b[k] = st.resi[((size_t)t * IM + k) * NV + n];
 #pragma unroll
     for (int i = 0; i < IM; ++i) {
-        if (i >= 1) b[i] -= mt->idiag[i][0] * b[0];
-        b[i] /= mt->idiag[i][1];
+        if (i >= 1) b[i] -= s_idiag[i][0] * b[0];
+        b[i] /= s_idiag[i][1];
     }
 #pragma unroll
     for (int i = IM - 1; i >= 0; --i) {
-        b[i] /= mt->idiag[i][1];
-        if (i >= 1) b[0] -= mt->idiag[i][0] * b[i];
+        b[i] /= s_idiag[i][1];
+        if (i >= 1) b[0] -= s_idiag[i][0] * b[i];
     }
     const R tp = st.tprcn[t * NV + n];
 #pragma unroll
@@ -1331,7 +1280,7 @@ __global__ void k_minv_int_flat(Mesh mesh, State<R> st, const DevMinv<R> *__rest
     for (int i = 0; i < 3; ++i) {
         const R u = st.resv[mesh.tri_pnt[3 * t + i] * NV + n];
 #pragma unroll
-        for (int k = 0; k < IM; ++k) b[k] -= mt->bfmi[i][k] * u;
+        for (int k = 0; k < IM; ++k) b[k] -= s_bfmi[i][k] * u;
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
@@ -1341,7 +1290,7 @@ __global__ void k_minv_int_flat(Mesh mesh, State<R> st, const DevMinv<R> *__rest
             const R msgn = ((m & 1) && sg < 0) ? (R)-1 : (R)1;
             const R u = msgn * st.ress[((size_t)sd * SM + m) * NV + n];
 #pragma unroll
-            for (int k = 0; k < IM; ++k) b[k] -= mt->bfmi[3 + i * SM + m][k] * u;
+            for (int k = 0; k < IM; ++k) b[k] -= s_bfmi[3 + i * SM + m][k] * u;
         }
     }
 #pragma unroll
