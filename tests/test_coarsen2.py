@@ -104,3 +104,14 @@ def test_reference_test_meshes_coarsen2(rel):
         assert set(c.groups) == set(g.groups)
         flat = sorted(s for segs in c.groups.values() for s in segs)
         assert flat == sorted(c.boundary_segments().tolist())
+
+
+def test_build_rejects_an_unknown_coarsening_route():
+    import hpb
+    from hpb import multigrid as MG
+
+    def mk(n=8, p=2, mesh=None, **kw):
+        return hpb.kovasznay_ins(n=n, p=p, mesh=mesh, **kw)
+
+    with pytest.raises(ValueError, match="coarsen_method"):
+        MG.build(mk, n=8, p=2, hlevels=1, coarsen=2.0, coarsen_method="collapse")
